@@ -1,0 +1,541 @@
+// driver.cpp -- standalone driver over the C ABI (hipft_run).
+//
+// Mirrors `program HIPFT` (src/hipft.f90:869-968) for the flux-transport
+// path: setup (reading hipft.in, realization parameters, the initial map or
+// a validation map, flows, diffusion, data-assimilation list), then per step
+// update_step -> flux_transport_step -> time += dt -> data assimilation ->
+// analysis -> history output, until time_end.  History files use the
+// reference's names and Fortran formats (src/hipft.f90:1616-1646, 2633-2634).
+// Map files (HDF5 output) are not written.
+#include <cfloat>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/hipft_gpu.h"
+#include "namelist.h"
+
+namespace hipft {
+namespace {
+
+constexpr double c_pi = 3.1415926535897932;
+constexpr double c_pi_two = 1.5707963267948966;
+constexpr double c_pi_four = 0.7853981633974483;
+constexpr double c_twopi = 6.2831853071795864;
+constexpr double c_threepi_two = 4.71238898038469;
+constexpr double c_km_s_to_rs_hr = 0.005172413793103448;
+
+// Fortran 1PE23.15E3: sign column, one digit, 15 decimals, 3-digit exponent.
+std::string fmt_e(double v) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%.15E", v);
+  std::string s(b);
+  size_t e = s.find('E');
+  std::string mant = s.substr(0, e);
+  int ex = std::atoi(s.c_str() + e + 1);
+  char eb[16];
+  std::snprintf(eb, sizeof eb, "E%c%03d", ex < 0 ? '-' : '+', ex < 0 ? -ex : ex);
+  std::string r = mant + eb;
+  while (r.size() < 23) r = " " + r;
+  return r;
+}
+std::string rjust(const std::string &s, size_t w) { return s.size() >= w ? s : std::string(w - s.size(), ' ') + s; }
+std::string fmt_i(long v, int w) { return rjust(std::to_string(v), (size_t)w); }
+
+// Y_lm by the first modified forward column recursion of Holmes &
+// Featherstone (2002), as tesseral_spherical_harmonic (src/hipft.f90:2390-2533).
+// Y is (np, nt) with phi fastest.
+void spherical_harmonic(int m, int l, const std::vector<double> &pv, const std::vector<double> &tv,
+                        std::vector<double> &Y) {
+  const double lpi = 3.141592653589793;
+  int am = std::abs(m), nt = (int)tv.size(), np = (int)pv.size();
+  std::vector<double> ct(nt), P(nt, 1.0), Pm(nt, 0.0);
+  for (int i = 0; i < nt; ++i) ct[i] = std::cos(tv[i]);
+  if (am > 0) {
+    for (int i = 0; i < nt; ++i) P[i] = std::sqrt(3.0);
+    for (int im = 2; im <= am; ++im)
+      for (int i = 0; i < nt; ++i) P[i] = std::sqrt((2.0 * im + 1.0) / (2.0 * im)) * P[i];
+  }
+  for (int il = am + 1; il <= l; ++il) {
+    double a = std::sqrt(((2.0 * il - 1.0) * (2.0 * il + 1.0)) / (double)((il - am) * (il + am)));
+    double b = std::sqrt(((2.0 * il + 1.0) * (il + am - 1.0) * (il - am - 1.0)) /
+                         ((il - am) * (il + am) * (2.0 * il - 3.0)));
+    for (int i = 0; i < nt; ++i) {
+      double Pl = a * ct[i] * P[i] - b * Pm[i];
+      Pm[i] = P[i];
+      P[i] = Pl;
+    }
+  }
+  double norm = 1.0 / std::sqrt(4.0 * lpi);
+  for (int i = 0; i < nt; ++i) {
+    double s = std::sin(tv[i]), sp = 1.0;
+    for (int q = 0; q < am; ++q) sp *= s;
+    P[i] = (((am % 2) ? -1.0 : 1.0) * sp) * norm * P[i];
+  }
+  int pos = (m + 1 >= 0) ? 1 : 0;
+  Y.assign((size_t)np * nt, 0.0);
+  for (int j = 0; j < nt; ++j)
+    for (int i = 0; i < np; ++i)
+      Y[(size_t)j * np + i] = P[j] * (pos * std::cos(m * pv[i]) + (1.0 - pos) * std::sin(am * pv[i]));
+}
+
+struct DAList {
+  std::vector<double> times;  // hours since the first map
+  std::vector<std::string> files;
+};
+
+bool read_da_list(const std::string &path, DAList &L, std::string &err) {
+  std::ifstream in(path);
+  if (!in) {
+    err = "cannot open assimilation map list " + path;
+    return false;
+  }
+  std::string line;
+  std::getline(in, line);  // header row
+  std::vector<double> jd;
+  while (std::getline(in, line)) {
+    std::istringstream ss(line);
+    std::string req, act, file;
+    double j;
+    if (!(ss >> req >> act >> j >> file)) continue;
+    jd.push_back(j);
+    L.files.push_back(file);
+  }
+  if (jd.empty()) {
+    err = "empty assimilation map list " + path;
+    return false;
+  }
+  for (double j : jd) L.times.push_back(24.0 * j - 24.0 * jd[0]);
+  return true;
+}
+
+struct Run {
+  Namelist nl;
+  std::string dir;
+  hipft_gpu *h = nullptr;
+  int nr = 0;
+  // time stepping state (globals / flows / diffusion modules)
+  double time = 0.0, dtime_global = 0.0, dtmax_flow = 0.0, dtime_advection_used = 0.0;
+  long ntime = 0, idx_hist = 0, idx_out = 0;
+  bool timestep_needs_updating = true, timestep_flow_needs_updating = true, time_step_changed = false;
+  bool output_current_map = false;
+  double dt_euler = 0.0;
+  int64_t niters = 0, subcycles = 0;
+  // DA
+  DAList da;
+  bool da_active = false;
+  int da_idx = 0;
+  double time_of_next_input_map = 0.0;
+  std::vector<double> hist;
+  std::string err;
+
+  std::string path(const std::string &f) const {
+    if (f.empty() || f[0] == '/') return f;
+    return dir + "/" + f;
+  }
+  std::string rname(const char *kind, int i) const {
+    char b[64];
+    std::snprintf(b, sizeof b, "hipft_history_%s_r%06d.out", kind, i);
+    return path(b);
+  }
+
+  bool history_due() const {
+    if (nl.output_history_time_cadence > 0.0)
+      return time >= nl.time_start + (double)idx_hist * nl.output_history_time_cadence;
+    return true;
+  }
+
+  // analysis_step + output_histories (src/hipft.f90:3135-3145, 2637-2690)
+  int analysis_and_history() {
+    if (!history_due()) return HIPFT_OK;
+    int rc = hipft_gpu_analysis(h, time, hist.data());
+    if (rc) return rc;
+    idx_hist++;
+    for (int i = 1; i <= nr; ++i) {
+      FILE *fn = std::fopen(rname("num", i).c_str(), "a");
+      FILE *fs = std::fopen(rname("sol", i).c_str(), "a");
+      if (!fn || !fs) {
+        if (fn) std::fclose(fn);
+        if (fs) std::fclose(fs);
+        return HIPFT_EIO;
+      }
+      std::string ln = fmt_i(ntime, 10) + " " + fmt_e(time) + " " + fmt_e(dtime_global) + " " + fmt_e(dtmax_flow) +
+                       " " + fmt_e(dtime_advection_used) + " " + fmt_e(dt_euler) + " " + fmt_i((long)niters, 15) +
+                       " " + fmt_i((long)subcycles, 15) + "\n";
+      std::fputs(ln.c_str(), fn);
+      std::string ls = fmt_i(ntime, 10) + " " + fmt_e(time) + " ";
+      const double *v = &hist[(size_t)(i - 1) * 14];
+      for (int q = 0; q < 14; ++q) ls += fmt_e(v[q]) + " ";
+      ls += "\n";
+      std::fputs(ls.c_str(), fs);
+      std::fclose(fn);
+      std::fclose(fs);
+    }
+    return HIPFT_OK;
+  }
+
+  void output_map_index() {
+    if (nl.output_map_idx_cadence > 0 && ntime % nl.output_map_idx_cadence == 0) output_current_map = true;
+    if (nl.output_map_time_cadence > 0.0 &&
+        time >= nl.time_start + (double)(idx_out - (nl.output_map_idx_start - 1)) * nl.output_map_time_cadence)
+      output_current_map = true;
+    if (output_current_map) {
+      idx_out++;
+      output_current_map = false;
+    }
+  }
+
+  // update_timestep (src/hipft.f90:4308-4461)
+  int update_timestep() {
+    if (timestep_needs_updating) {
+      dtime_global = nl.time_end - time;
+      time_step_changed = true;
+      if (nl.advance_flow) {
+        dtmax_flow = DBL_MAX;
+        if (timestep_flow_needs_updating) {
+          int rc = hipft_gpu_flow_dtmax(h, &dtmax_flow);
+          if (rc) return rc;
+          timestep_flow_needs_updating = false;
+        }
+        if (dtmax_flow < dtime_global) dtime_global = dtmax_flow;
+      }
+      if (nl.dt_max < dtime_global) dtime_global = nl.dt_max;
+      if (dtime_global < nl.dt_min) std::fprintf(stderr, "   UPDATE_TIMESTEP: Warning! Time step is smaller than DTMIN!\n");
+      timestep_needs_updating = false;
+    }
+    if (nl.output_map_time_cadence > 0.0) {
+      double tn = nl.time_start + (double)(idx_out - (nl.output_map_idx_start - 1)) * nl.output_map_time_cadence;
+      if (time + dtime_global >= tn) {
+        dtime_global = tn - time;
+        timestep_needs_updating = timestep_flow_needs_updating = time_step_changed = true;
+      }
+    }
+    if (da_active && time + dtime_global >= time_of_next_input_map) {
+      dtime_global = time_of_next_input_map - time;
+      timestep_needs_updating = timestep_flow_needs_updating = time_step_changed = true;
+    }
+    if (time + dtime_global >= nl.time_end) {
+      dtime_global = nl.time_end - time;
+      timestep_needs_updating = false;
+      time_step_changed = true;
+    }
+    return HIPFT_OK;
+  }
+
+  static void cycle_cb(void *user, int, double time_stepped, double, int64_t s, int64_t sc) {
+    Run *r = (Run *)user;
+    if (r->nl.verbose <= 1) return;
+    r->niters = s;
+    r->subcycles = sc;
+    double tt = r->time;
+    r->time = r->time + time_stepped;
+    int rc = r->analysis_and_history();
+    if (rc && r->err.empty()) r->err = "history output inside the diffusion step failed";
+    r->time = tt;
+  }
+
+  int apply_data_assimilation() {
+    if (!(da_active && time >= time_of_next_input_map)) return HIPFT_OK;
+    std::string f = nl.assimilate_data_map_root_dir + "/" + da.files[da_idx];
+    if (f[0] != '/') f = path(f);
+    int nd = 0;
+    int64_t dims[3];
+    int rc = hipft_h5_read(f.c_str(), &nd, dims, nullptr, nullptr, nullptr, nullptr);
+    if (rc) {
+      err = "cannot read assimilation map " + f;
+      return rc;
+    }
+    std::vector<double> data((size_t)(dims[0] * dims[1] * dims[2]));
+    rc = hipft_h5_read(f.c_str(), &nd, dims, data.data(), nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    hipft_info inf;
+    hipft_gpu_info(h, &inf);
+    if (dims[0] != inf.npm - 1 || dims[1] != inf.ntm || dims[2] < 3) {
+      err = "assimilation map size does not match the run's grid";
+      return HIPFT_EINVAL;
+    }
+    hipft_da_opts o{};
+    o.add = nl.assimilate_data_add;
+    o.custom_from_mu = nl.assimilate_data_custom_from_mu;
+    o.balance_flux = nl.assimilate_data_balance_flux;
+    o.mult_fac = nl.assimilate_data_mult_fac;
+    o.mu_power = nl.assimilate_data_mu_powers.data();
+    o.mu_limit = nl.assimilate_data_mu_limits.data();
+    o.lat_limit = nl.assimilate_data_lat_limits.data();
+    rc = hipft_gpu_assimilate(h, data.data(), &o);
+    if (rc) return rc;
+    da_idx++;
+    if (da_idx >= (int)da.files.size()) da_active = false;
+    else time_of_next_input_map = da.times[da_idx];
+    return HIPFT_OK;
+  }
+
+  int setup(int device) {
+    nr = nl.n_realizations;
+    hist.assign((size_t)nr * 14, 0.0);
+    if (nl.advance_source) {
+      err = "sources (advance_source) are not part of this library";
+      return HIPFT_EINVAL;
+    }
+    if (nl.use_flow_from_files) {
+      err = "flows from files are not supported yet";
+      return HIPFT_EINVAL;
+    }
+    if (!nl.diffusion_coef_filename.empty()) {
+      err = "diffusion_coef_filename is not supported yet";
+      return HIPFT_EINVAL;
+    }
+    // initial condition (load_initial_condition, src/hipft.f90:1741-2187)
+    int n1, n2;
+    std::vector<double> s1, s2, f_local;
+    if (nl.initial_map_filename.empty()) {
+      n1 = nl.res_np;
+      n2 = nl.res_nt;
+      double d1 = c_twopi / (n1 - 1), d2 = c_pi / (n2 - 1);
+      for (int i = 1; i <= n1; ++i) s1.push_back((i - 1) * d1);
+      for (int i = 1; i <= n2; ++i) s2.push_back((i - 1) * d2);
+      f_local.assign((size_t)n1 * n2 * nr, 0.0);
+    } else {
+      int nd = 0;
+      int64_t dims[3];
+      std::string f = path(nl.initial_map_filename);
+      int rc = hipft_h5_read(f.c_str(), &nd, dims, nullptr, nullptr, nullptr, nullptr);
+      if (rc) {
+        err = "cannot read the initial map " + f;
+        return rc;
+      }
+      n1 = (int)dims[0];
+      n2 = (int)dims[1];
+      std::vector<double> all((size_t)(dims[0] * dims[1] * dims[2]));
+      s1.resize(n1);
+      s2.resize(n2);
+      rc = hipft_h5_read(f.c_str(), &nd, dims, all.data(), s1.data(), s2.data(), nullptr);
+      if (rc) return rc;
+      f_local.assign((size_t)n1 * n2 * nr, 0.0);
+      size_t plane = (size_t)n1 * n2;
+      if (nd == 2) {
+        for (int i = 0; i < nr; ++i) std::copy(all.begin(), all.begin() + plane, f_local.begin() + plane * i);
+      } else {
+        if (dims[2] != nr) {
+          err = "number of realizations in the input map differs from n_realizations";
+          return HIPFT_EINVAL;
+        }
+        f_local = all;
+      }
+    }
+    double vt_const = nl.flow_vt_const, vp_omega = nl.flow_vp_rigid_omega;
+    std::vector<double> fval_u0;
+    size_t plane = (size_t)n1 * n2;
+    if (nl.validation_run == 1) {
+      std::vector<double> Y0, Y5;
+      spherical_harmonic(0, 6, s1, s2, Y0);
+      spherical_harmonic(5, 6, s1, s2, Y5);
+      fval_u0.assign(plane * nr, 0.0);
+      for (int i = 0; i < nr; ++i)
+        for (size_t q = 0; q < plane; ++q) fval_u0[plane * i + q] = Y0[q] + std::sqrt(14.0 / 11.0) * Y5[q];
+      f_local = fval_u0;
+    } else if (nl.validation_run == 2) {
+      if (std::fabs(vt_const) > 0.0) vt_const = (c_pi_two / (nl.time_end - nl.time_start)) / c_km_s_to_rs_hr;
+      if (std::fabs(vp_omega) > 0.0) vp_omega = (c_twopi / (nl.time_end - nl.time_start)) / c_km_s_to_rs_hr;
+      double w = nl.validation_run_width;
+      for (int i = 0; i < nr; ++i)
+        for (int j = 1; j <= n2; ++j) {
+          double sti = (j > 1 && j < n2) ? 1.0 / std::sin(s2[j - 1]) : 0.0;
+          for (int k = 1; k <= n1; ++k) {
+            double a = s2[j - 1] - c_pi_four, b1 = s1[k - 1] - c_pi_two, b2 = s1[k - 1] - c_threepi_two;
+            f_local[plane * i + (size_t)(j - 1) * n1 + (k - 1)] =
+                -sti * std::exp(-(a * a) / w - (b1 * b1) / w) + sti * std::exp(-(a * a) / w - (b2 * b2) / w);
+          }
+        }
+    }
+    hipft_grid g{};
+    g.ntm = n2;
+    g.npm1 = n1;
+    g.nr = nr;
+    g.device = device;
+    g.t = s2.data();
+    g.p = s1.data();
+    hipft_params P{};
+    P.advance_flow = nl.advance_flow;
+    P.flow_num_method = nl.flow_num_method;
+    P.upwind = nl.upwind;
+    P.weno_eps = nl.weno_eps;
+    P.strang_splitting = nl.strang_splitting;
+    P.advance_diffusion = nl.advance_diffusion;
+    P.diffusion_num_method = nl.diffusion_num_method;
+    P.diffusion_subcycles = nl.diffusion_subcycles;
+    P.diffusion_coef_grid = nl.diffusion_coef_grid;
+    P.diffusion_coef_factor = nl.diffusion_coef_factor;
+    P.diffusion_coef_constants = nl.diffusion_coef_constants.data();
+    P.pole_flux_lat_limit = nl.pole_flux_lat_limit;
+    P.verbose = nl.verbose;
+    int rc = hipft_gpu_create(&g, &P, &h);
+    if (rc) {
+      err = "hipft_gpu_create failed";
+      return rc;
+    }
+    rc = hipft_gpu_load_initial_map(h, f_local.data(), nl.initial_map_flux_balance, nl.initial_map_mult_fac);
+    if (rc) return rc;
+    if (nl.validation_run == 1) rc = hipft_gpu_set_validation(h, 1, fval_u0.data(), 0, 0, 0, nl.time_start);
+    else if (nl.validation_run == 2)
+      rc = hipft_gpu_set_validation(h, 2, nullptr, nl.validation_run_width, vt_const, vp_omega, nl.time_start);
+    if (rc) return rc;
+    if (nl.advance_flow) {
+      hipft_flow_def d{};
+      d.flow_dr_model = nl.flow_dr_model;
+      d.flow_mf_model = nl.flow_mf_model;
+      d.dr_p0 = nl.flow_dr_coef_p0_values.data();
+      d.dr_p2 = nl.flow_dr_coef_p2_values.data();
+      d.dr_p4 = nl.flow_dr_coef_p4_values.data();
+      d.mf_p1 = nl.flow_mf_coef_p1_values.data();
+      d.mf_p3 = nl.flow_mf_coef_p3_values.data();
+      d.mf_p5 = nl.flow_mf_coef_p5_values.data();
+      d.flow_vp_rigid_omega = vp_omega;
+      d.flow_vt_const = vt_const;
+      d.flow_rigid_omega = nl.flow_rigid_omega;
+      d.flow_attenuate = nl.flow_attenuate;
+      d.flow_attenuate_values = nl.flow_attenuate_values.data();
+      rc = hipft_gpu_set_flow(h, &d);
+      if (rc) return rc;
+    }
+    hipft_info inf;
+    hipft_gpu_info(h, &inf);
+    dt_euler = inf.dtime_diffusion_euler;
+    subcycles = nl.diffusion_subcycles;
+    time = nl.time_start;
+    idx_out = nl.output_map_idx_start - 1;
+    if (nl.output_map_idx_cadence > 0 || nl.output_map_time_cadence > 0.0) output_current_map = true;
+    if (nl.assimilate_data) {
+      if (!read_da_list(path(nl.assimilate_data_map_list_filename), da, err)) return HIPFT_EIO;
+      // load_data_assimilation time bookkeeping (src/hipft.f90:4017-4042)
+      int best = 0;
+      double bd = DBL_MAX;
+      for (size_t q = 0; q < da.times.size(); ++q) {
+        double d = std::fabs(da.times[q] - nl.time_start);
+        if (d < bd) { bd = d; best = (int)q; }
+      }
+      da_active = true;
+      if (nl.time_start <= 0.0) {
+        da_idx = 0;
+        time_of_next_input_map = 0.0;
+      } else if (nl.time_start > da.times.back()) {
+        da_active = false;
+      } else if (nl.time_start <= da.times[best]) {
+        da_idx = best;
+        time_of_next_input_map = da.times[best];
+      } else {
+        da_idx = best + 1;
+        time_of_next_input_map = da.times[best + 1];
+      }
+    }
+    // history files with headers (create_and_open_output_log_files, src/hipft.f90:1601-1648)
+    const char *numh[] = {"TIME", "DTIME", "DTIME_ADV_STB", "DTIME_ADV_USED", "DTIME_DIFF_STB", "N_DIFF_PER_STEP",
+                          "N_DIFF_CYCLES"};
+    const char *solh[] = {"TIME", "BR_MIN", "BR_MAX", "BR_ABS_MIN", "FLUX_POSITIVE", "FLUX_NEGATIVE",
+                          "NPOLE_FLUX_POSITIVE", "NPOLE_FLUX_NEGATIVE", "SPOLE_FLUX_POSITIVE",
+                          "SPOLE_FLUX_NEGATIVE", "NPOLE_AREA", "SPOLE_AREA", "EQ_DIPOLE", "AX_DIPOLE",
+                          "VALIDATION_ERR_HHabs"};
+    for (int i = 1; i <= nr; ++i) {
+      FILE *fn = std::fopen(rname("num", i).c_str(), "w");
+      FILE *fs = std::fopen(rname("sol", i).c_str(), "w");
+      if (!fn || !fs) {
+        if (fn) std::fclose(fn);
+        if (fs) std::fclose(fs);
+        err = "cannot create history files in " + dir;
+        return HIPFT_EIO;
+      }
+      std::string a = rjust("STEP", 10) + " ";
+      for (auto *s : numh) a += rjust(s, 22) + " ";
+      std::fputs((a + "\n").c_str(), fn);
+      std::string b = rjust("STEP", 10) + " ";
+      for (auto *s : solh) b += rjust(s, 22) + " ";
+      std::fputs((b + "\n").c_str(), fs);
+      std::fclose(fn);
+      std::fclose(fs);
+    }
+    rc = analysis_and_history();
+    if (rc) return rc;
+    output_map_index();
+    return HIPFT_OK;
+  }
+
+  int main_loop() {
+    for (;;) {
+      ntime++;
+      if (nl.advance_flow) {
+        int upd = 0;
+        int rc = hipft_gpu_update_flow(h, &upd);
+        if (rc) return rc;
+        if (upd) timestep_flow_needs_updating = timestep_needs_updating = true;
+      }
+      int rc = update_timestep();
+      if (rc) return rc;
+      hipft_diffusion_info di{};
+      double dtl = dtime_global;
+      if (nl.advance_flow) dtime_advection_used = nl.strang_splitting ? dtl * 0.5 : dtl;
+      rc = hipft_gpu_flux_transport_step(h, dtl, &Run::cycle_cb, this, nl.advance_diffusion ? &di : nullptr);
+      if (rc) return rc;
+      if (!err.empty()) return HIPFT_EIO;
+      if (nl.advance_diffusion) {
+        niters = di.sts_s;
+        subcycles = di.subcycles;
+      }
+      time = time + dtime_global;
+      rc = apply_data_assimilation();
+      if (rc) return rc;
+      rc = analysis_and_history();
+      if (rc) return rc;
+      output_map_index();
+      if (nl.verbose >= 0) {
+        std::printf(" Completed step: %10ld  Time: %14.3f / %14.3f  dt: %12.6f\n", ntime, time, nl.time_end,
+                    dtime_global);
+      }
+      if (time >= nl.time_end) break;
+      FILE *stop = std::fopen(path("STOPRUN").c_str(), "r");
+      if (stop) {
+        std::fclose(stop);
+        std::printf(" ### NOTE: The run was stopped prematurely via STOPRUN!\n");
+        break;
+      }
+    }
+    return HIPFT_OK;
+  }
+};
+
+}  // namespace
+}  // namespace hipft
+
+extern "C" int hipft_run_field(const char *namelist_path, const char *run_dir, int device, double *f_out,
+                               size_t f_len) {
+  if (!namelist_path || !run_dir) return HIPFT_EINVAL;
+  hipft::Run r;
+  r.dir = run_dir;
+  std::string err;
+  if (!hipft::read_namelist(namelist_path, r.nl, err)) {
+    std::fprintf(stderr, "### ERROR in READ_INPUT_FILE: %s\n", err.c_str());
+    return HIPFT_EINVAL;
+  }
+  int rc = r.setup(device);
+  if (rc == HIPFT_OK) rc = r.main_loop();
+  if (rc == HIPFT_OK && f_out) {
+    hipft_info inf;
+    hipft_gpu_info(r.h, &inf);
+    if (f_len != (size_t)inf.ntm * inf.npm * inf.nr) rc = HIPFT_EINVAL;
+    else rc = hipft_gpu_get_field(r.h, f_out);
+  }
+  if (rc != HIPFT_OK) {
+    char msg[512] = "";
+    if (r.h) hipft_gpu_last_error(r.h, msg, sizeof msg);
+    std::fprintf(stderr, "### ERROR in HIPFT (code %d): %s %s\n", rc, r.err.c_str(), msg);
+  }
+  hipft_gpu_destroy(r.h);
+  return rc;
+}
+
+extern "C" int hipft_run(const char *namelist_path, const char *run_dir, int device) {
+  return hipft_run_field(namelist_path, run_dir, device, nullptr, 0);
+}

@@ -1,0 +1,1186 @@
+// hipft_gpu.cu -- host side of the B200 flux-transport library (C ABI in
+// include/hipft_gpu.h).  Owns all device state behind an opaque handle and
+// sequences the kernels of kernels.cuh the way HipFT's Fortran routines
+// sequence their do-concurrent loops (src/hipft.f90).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/hipft_gpu.h"
+#include "kernels.cuh"
+
+using namespace hipft;
+
+namespace {
+
+// Constants of the reference (src/hipft.f90:83-136).
+constexpr double c_pi = 3.1415926535897932;
+constexpr double c_pi_i = 0.3183098861837907;
+constexpr double c_twopi = 6.2831853071795864;
+constexpr double c_pi_two = 1.5707963267948966;
+constexpr double c_threepi_two = 4.71238898038469;
+constexpr double c_d2r = 0.017453292519943295;
+constexpr double c_rsun_cm2 = 4.84416e21;
+constexpr double c_km_s_to_rs_hr = 0.005172413793103448;
+constexpr double c_m_s_to_rs_hr = 5.172413793103448e-06;
+constexpr double c_safety = 0.95;
+constexpr double c_three_quarter = 0.75;
+constexpr double c_quarter = 0.25;
+constexpr double c_sixth = 0.16666666666666666;
+constexpr double c_two_third = 0.66666666666666666;
+constexpr double c_third = 0.33333333333333333;
+
+constexpr int kNBuf = 4;  // current field + 3 scratch fields
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+double pow3(double c) { return c * c * c; }
+double pow5(double c) { return c * c * c * c * c; }
+
+}  // namespace
+
+struct hipft_gpu {
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int ntm = 0, npm = 0, npm1 = 0, nt = 0, np = 0, nr = 0, ldt = 0, ldv = 0;
+  int64_t plane = 0;
+  size_t fieldn = 0;
+  hipft_params P{};
+  std::vector<double> Dc;
+  int adv_time = 3, adv_space = 2;
+  // host mesh, 1-based (element 0 unused)
+  std::vector<double> t, p, th, ph, dt, dth, dp, dph, dt_i, dth_i, dp_i, dph_i, st, sth, ct, cth, st_i, sth_i;
+  std::vector<void *> allocs;
+  size_t dev_bytes = 0;
+  Mesh M{};
+  DiffCoef DC{};
+  Weno W{};
+  Flow FL{};
+  double bc_flow_n = 0, bc_flow_s = 0, bc_diff_n = 0, bc_diff_s = 0;
+  // fields
+  double *buf[kNBuf] = {};
+  int cur = 0;
+  bool field_set = false;
+  // flows
+  bool have_flow = false, flow_needs_updating = false, flow2d = false;
+  hipft_flow_def fdef{};
+  std::vector<double> f_p0, f_p2, f_p4, f_p1, f_p3, f_p5, f_att;
+  double *d_vt1 = nullptr, *d_vp1 = nullptr, *d_at1 = nullptr, *d_ap1 = nullptr;
+  double *d_vt = nullptr, *d_vp = nullptr, *d_at = nullptr, *d_ap = nullptr;
+  double *d_trig = nullptr, *d_atten = nullptr;
+  // diffusion
+  double dt_euler = 0.0;
+  bool auto_sc = false;
+  int64_t sts_s = 0, n_euler = 0, subcycles_state = 0;
+  std::vector<double> sts_uj, sts_vj, sts_ubj, sts_gj, sts_b;
+  // scratch
+  double *d_ring = nullptr;
+  unsigned long long *d_bits = nullptr;
+  double *d_part = nullptr;
+  size_t part_cap = 0;
+  double *h_pin = nullptr;
+  // analysis
+  double *d_anw = nullptr;
+  unsigned char *d_masks = nullptr;
+  std::vector<double> da_t, da_p;
+  int vmode = 0;
+  double *d_fval_u0 = nullptr, *d_vscale = nullptr, *d_vgauss = nullptr;
+  double vwidth = 0.03, vt_const = 0.0, vp_omega = 0.0, vtime_start = 0.0;
+  // assimilation
+  double *d_da = nullptr, *d_daopt = nullptr;
+  int *d_tidx = nullptr;
+  std::string err;
+  int64_t launches = 0, cell_updates = 0;
+};
+
+// ------------------------------------------------------------------ errors
+static int fail(hipft_gpu *h, int code, const char *fmt, ...) {
+  char msg[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(msg, sizeof msg, fmt, ap);
+  va_end(ap);
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CK(h, call)                                                                         \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail((h), HIPFT_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,              \
+                  cudaGetErrorString(e_));                                                  \
+  } while (0)
+
+#define LAUNCHED(h)                                                                         \
+  do {                                                                                      \
+    (h)->launches++;                                                                        \
+    cudaError_t e_ = cudaPeekAtLastError();                                                 \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail((h), HIPFT_ECUDA, "%s:%d kernel launch: %s", __FILE__, __LINE__,          \
+                  cudaGetErrorString(e_));                                                  \
+  } while (0)
+
+template <typename T>
+static int dalloc(hipft_gpu *h, T **p, size_t n) {
+  size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  cudaError_t e = cudaMalloc((void **)p, bytes);
+  if (e != cudaSuccess) return fail(h, HIPFT_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  h->allocs.push_back((void *)*p);
+  h->dev_bytes += bytes;
+  return HIPFT_OK;
+}
+
+template <typename T>
+static int upload(hipft_gpu *h, T *d, const std::vector<T> &v) {
+  CK(h, cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, h->stream));
+  return HIPFT_OK;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_ != HIPFT_OK) return rc_; \
+  } while (0)
+
+// ------------------------------------------------------------- set_mesh
+// src/hipft.f90:6495-6653, restated on 1-based host vectors.
+static int set_mesh(hipft_gpu *h, const double *tin, const double *pin) {
+  const double eps = 1.e-5;
+  int ntm = h->ntm, npm = h->npm, nt = h->nt, np = h->np, npm1 = h->npm1, ntm1 = h->ntm;
+  auto &t = h->t, &p = h->p;
+  t.assign(ntm + 1, 0.0);
+  p.assign(npm + 1, 0.0);
+  for (int j = 1; j <= ntm; ++j) t[j] = tin[j - 1];
+  for (int k = 1; k <= npm1; ++k) p[k] = pin[k - 1];
+  p[npm1 + 1] = p[2] + c_twopi;
+  if (std::fabs(t[1]) > eps || std::fabs(t[ntm] - c_pi) > eps || std::fabs(p[1]) > eps ||
+      std::fabs(p[npm - 1] - c_twopi) > eps)
+    return fail(h, HIPFT_EINVAL, "set_mesh: the mesh does not cover the sphere (t in [0,pi], p in [0,2pi])");
+  h->th.assign(nt + 1, 0); h->dth.assign(nt + 1, 0); h->dth_i.assign(nt + 1, 0);
+  h->sth.assign(nt + 1, 0); h->sth_i.assign(nt + 1, 0); h->cth.assign(nt + 1, 0);
+  h->dt.assign(ntm + 1, 0); h->dt_i.assign(ntm + 1, 0); h->st.assign(ntm + 1, 0);
+  h->st_i.assign(ntm + 1, 0); h->ct.assign(ntm + 1, 0);
+  h->ph.assign(np + 1, 0); h->dph.assign(np + 1, 0); h->dph_i.assign(np + 1, 0);
+  h->dp.assign(npm + 1, 0); h->dp_i.assign(npm + 1, 0);
+  auto &th = h->th, &dth = h->dth, &dt = h->dt, &ph = h->ph, &dph = h->dph, &dp = h->dp;
+  for (int i = 2; i <= ntm1; ++i) {
+    th[i] = 0.5 * (t[i] + t[i - 1]);
+    dth[i] = t[i] - t[i - 1];
+  }
+  th[1] = th[2] - dth[2];
+  th[nt] = th[ntm1] + dth[ntm1];
+  dth[1] = dth[2];
+  dth[nt] = dth[ntm1];
+  for (int i = 1; i <= nt; ++i) h->dth_i[i] = 1.0 / dth[i];
+  for (int i = 1; i <= ntm; ++i) {
+    dt[i] = th[i + 1] - th[i];
+    h->dt_i[i] = 1.0 / dt[i];
+  }
+  for (int i = 1; i <= ntm; ++i) h->st[i] = std::sin(t[i]);
+  h->st[1] = 0.0;
+  h->st[ntm] = 0.0;
+  for (int i = 1; i <= ntm; ++i) h->ct[i] = std::cos(t[i]);
+  h->ct[1] = 1.0;
+  h->ct[ntm] = 1.0;
+  for (int i = 2; i <= ntm - 1; ++i) h->st_i[i] = 1.0 / h->st[i];
+  for (int i = 1; i <= nt; ++i) h->sth[i] = std::sin(std::fabs(th[i]));
+  for (int i = 2; i <= ntm1; ++i) h->sth_i[i] = 1.0 / h->sth[i];
+  for (int i = 1; i <= nt; ++i) h->cth[i] = std::cos(th[i]);
+  for (int i = 2; i <= np; ++i) {
+    ph[i] = 0.5 * (p[i] + p[i - 1]);
+    dph[i] = p[i] - p[i - 1];
+  }
+  ph[1] = ph[npm1] - c_twopi;
+  dph[1] = dph[npm1];
+  for (int i = 1; i <= np; ++i) h->dph_i[i] = 1.0 / dph[i];
+  for (int i = 1; i <= npm - 1; ++i) dp[i] = ph[i + 1] - ph[i];
+  dp[npm] = dp[2];
+  for (int i = 1; i <= npm; ++i) h->dp_i[i] = 1.0 / dp[i];
+  return HIPFT_OK;
+}
+
+// load_weno grid weights (src/hipft.f90:6893-6932); 7 theta + 7 phi arrays.
+static void weno_weights(const hipft_gpu *h, std::vector<double> wt[7], std::vector<double> wp[7]) {
+  int nt = h->nt, np = h->np, ntm = h->ntm, npm = h->npm;
+  for (int q = 0; q < 7; ++q) {
+    wt[q].assign(nt + 2, 0.0);
+    wp[q].assign(np + 2, 0.0);
+  }
+  for (int j = 1; j <= ntm; ++j) wt[6][j] = (h->P.weno_eps <= 0.0) ? h->dt[j] : h->P.weno_eps;
+  for (int k = 1; k <= npm; ++k) wp[6][k] = (h->P.weno_eps <= 0.0) ? h->dp[k] : h->P.weno_eps;
+  auto fill = [](std::vector<double> *w, const std::vector<double> &d, int lo, int hi) {
+    for (int j = lo; j <= hi; ++j) {
+      double tot = d[j - 1] + d[j] + d[j + 1];
+      w[0][j] = d[j] / (d[j] + d[j + 1]);          // D_C_CP
+      w[1][j] = d[j] / (d[j - 1] + d[j]);          // D_C_MC
+      w[2][j] = d[j - 1] / tot;                    // D_M_T
+      w[3][j] = (d[j] + d[j + 1]) / tot;           // D_CP_T
+      w[4][j] = d[j + 1] / tot;                    // D_P_T
+      w[5][j] = (d[j - 1] + d[j]) / tot;           // D_MC_T
+    }
+  };
+  fill(wt, h->dt, 2, nt - 2);
+  fill(wp, h->dp, 2, np - 1);
+  for (int q = 0; q < 6; ++q) {
+    wp[q][1] = wp[q][np - 1];
+    wp[q][np] = wp[q][2];
+  }
+}
+
+// Scratch buffer n (0,1,2) other than the current field.
+static int scratch(const hipft_gpu *h, int n) {
+  int c = 0;
+  for (int b = 0; b < kNBuf; ++b) {
+    if (b == h->cur) continue;
+    if (c == n) return b;
+    ++c;
+  }
+  return -1;
+}
+
+static dim3 stage_grid(const hipft_gpu *h, int tj, int tk) {
+  return dim3((unsigned)((h->ntm + tj - 1) / tj), (unsigned)((h->npm - 2 + tk - 1) / tk), (unsigned)h->nr);
+}
+
+static int ensure_part(hipft_gpu *h, size_t n) {
+  if (n <= h->part_cap) return HIPFT_OK;
+  if (h->d_part) {
+    cudaFree(h->d_part);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)h->d_part), h->allocs.end());
+  }
+  h->d_part = nullptr;
+  TRY(dalloc(h, &h->d_part, n));
+  h->part_cap = n;
+  return HIPFT_OK;
+}
+
+static int sync_read(hipft_gpu *h, const void *dsrc, size_t bytes) {
+  CK(h, cudaMemcpyAsync(h->h_pin, dsrc, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+// ------------------------------------------------------------- kernels glue
+static int ring_diffusion(hipft_gpu *h, const double *x) {
+  k_ring_diffusion<<<h->nr, 256, 0, h->stream>>>(h->M, h->DC, x, h->d_ring);
+  LAUNCHED(h);
+  return HIPFT_OK;
+}
+
+template <int MODE>
+static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
+                           double *out, double *out2, StageCoef sc, unsigned long long *absmax) {
+  dim3 blk(32, 8);
+  k_diffusion_stage<MODE><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->DC, x, ykm2, u0, dty0, out, out2,
+                                                                       h->d_ring, h->bc_diff_n, h->bc_diff_s, sc,
+                                                                       absmax);
+  LAUNCHED(h);
+  return HIPFT_OK;
+}
+
+static int advection_stage(hipft_gpu *h, const double *x, const double *f0, double *out, AdvCombine cb) {
+  k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
+  LAUNCHED(h);
+  dim3 blk(32, 8);
+  if (h->adv_space == 2)
+    k_advection_stage<32, 8, true><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out,
+                                                                                 h->d_ring, h->bc_flow_n,
+                                                                                 h->bc_flow_s, cb);
+  else
+    k_advection_stage<32, 8, false><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out,
+                                                                                  h->d_ring, h->bc_flow_n,
+                                                                                  h->bc_flow_s, cb);
+  LAUNCHED(h);
+  h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr;
+  return HIPFT_OK;
+}
+
+// ---------------------------------------------------------------- create
+extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hipft_gpu **out) {
+  if (!g || !prm || !out || !g->t || !g->p) return HIPFT_EINVAL;
+  *out = nullptr;
+  if (g->ntm < 4 || g->npm1 < 5 || g->nr < 1) return HIPFT_EINVAL;
+  if (prm->advance_diffusion && !prm->diffusion_coef_constants) return HIPFT_EINVAL;
+  if (prm->advance_flow && (prm->flow_num_method < 1 || prm->flow_num_method > 4)) return HIPFT_EINVAL;
+  if (prm->advance_diffusion && (prm->diffusion_num_method < 1 || prm->diffusion_num_method > 3))
+    return HIPFT_EINVAL;
+  hipft_gpu *h = new hipft_gpu();
+  h->dev = g->device;
+  h->P = *prm;
+  h->P.diffusion_coef_constants = nullptr;
+  h->ntm = g->ntm;
+  h->npm1 = g->npm1;
+  h->npm = g->npm1 + 1;
+  h->nt = g->ntm + 1;
+  h->np = g->npm1 + 1;
+  h->nr = g->nr;
+  h->ldt = round_up(h->ntm, 16);
+  h->ldv = round_up(h->nt, 16);
+  h->plane = (int64_t)h->ldt * h->npm;
+  h->fieldn = (size_t)h->plane * h->nr;
+  if (prm->advance_diffusion) h->Dc.assign(prm->diffusion_coef_constants, prm->diffusion_coef_constants + g->nr);
+  int fm = prm->flow_num_method;
+  h->adv_time = (fm == 1) ? 1 : (fm == 4 ? 3 : 2);
+  h->adv_space = (fm <= 2) ? 1 : 2;
+  h->subcycles_state = prm->diffusion_subcycles;
+  auto bail = [&](int rc) {
+    std::string e = h->err;
+    hipft_gpu_destroy(h);
+    (void)e;
+    return rc;
+  };
+  cudaError_t ce = cudaSetDevice(h->dev);
+  if (ce != cudaSuccess) {
+    fail(h, HIPFT_ECUDA, "cudaSetDevice(%d): %s", h->dev, cudaGetErrorString(ce));
+    return bail(HIPFT_ECUDA);
+  }
+  ce = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) return bail(HIPFT_ECUDA);
+  h->own_stream = true;
+  int rc = set_mesh(h, g->t, g->p);
+  if (rc) return bail(rc);
+  int ntm = h->ntm, npm = h->npm, nt = h->nt, np = h->np, nr = h->nr;
+
+  // 1-D mesh arrays on the device (one allocation, 1-based slices)
+  std::vector<const std::vector<double> *> arrs = {&h->dt_i, &h->dth_i, &h->dp_i, &h->dph_i, &h->st_i,
+                                                   &h->sth,  &h->dp,    &h->dth,  &h->dph};
+  size_t tot = 0;
+  for (auto *a : arrs) tot += a->size();
+  double *dm = nullptr;
+  if ((rc = dalloc(h, &dm, tot))) return bail(rc);
+  std::vector<double> packed;
+  packed.reserve(tot);
+  std::vector<size_t> offs;
+  for (auto *a : arrs) {
+    offs.push_back(packed.size());
+    packed.insert(packed.end(), a->begin(), a->end());
+  }
+  if ((rc = upload(h, dm, packed))) return bail(rc);
+  h->M.ntm = ntm; h->M.npm = npm; h->M.nt = nt; h->M.np = np; h->M.nr = nr; h->M.ldt = h->ldt;
+  h->M.plane = h->plane;
+  h->M.dt_i = dm + offs[0]; h->M.dth_i = dm + offs[1]; h->M.dp_i = dm + offs[2]; h->M.dph_i = dm + offs[3];
+  h->M.st_i = dm + offs[4]; h->M.sth = dm + offs[5]; h->M.dp = dm + offs[6]; h->M.dth = dm + offs[7];
+  h->M.dph = dm + offs[8];
+
+  // fields
+  for (int b = 0; b < kNBuf; ++b) {
+    if ((rc = dalloc(h, &h->buf[b], h->fieldn))) return bail(rc);
+    if (cudaMemsetAsync(h->buf[b], 0, h->fieldn * sizeof(double), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
+  }
+  if ((rc = dalloc(h, &h->d_ring, 2 * (size_t)nr))) return bail(rc);
+  if ((rc = dalloc(h, &h->d_bits, 4))) return bail(rc);
+  if (cudaMallocHost((void **)&h->h_pin, sizeof(double) * std::max<size_t>(64, (size_t)nr * kNPart)) !=
+      cudaSuccess)
+    return bail(fail(h, HIPFT_ENOMEM, "cudaMallocHost failed"));
+
+  // diffusion: D constants, Gershgorin dt (load_diffusion, src/hipft.f90:6655-6844)
+  std::vector<double> dfac(nr + 1, 0.0);
+  if (prm->advance_diffusion)
+    for (int i = 1; i <= nr; ++i)
+      dfac[i] = prm->diffusion_coef_grid ? h->Dc[i - 1] : prm->diffusion_coef_factor * h->Dc[i - 1];
+  double *d_dfac = nullptr;
+  if ((rc = dalloc(h, &d_dfac, nr + 1))) return bail(rc);
+  if ((rc = upload(h, d_dfac, dfac))) return bail(rc);
+  h->DC.dfac = d_dfac;
+  h->DC.factor = prm->diffusion_coef_factor;
+  h->DC.grid = prm->diffusion_coef_grid;
+  h->bc_diff_n = c_pi_i * h->dth_i[2] * h->dth_i[2];
+  h->bc_diff_s = c_pi_i * h->dth_i[nt - 1] * h->dth_i[nt - 1];
+  h->auto_sc = (prm->diffusion_subcycles == 0);
+  if (prm->advance_diffusion) {
+    if (cudaMemsetAsync(h->d_bits, 0, sizeof(unsigned long long), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
+    dim3 blk(32, 8);
+    dim3 grd((unsigned)((ntm - 2 + 31) / 32), (unsigned)((npm - 2 + 7) / 8), (unsigned)nr);
+    k_gershgorin<<<grd, blk, 0, h->stream>>>(h->M, h->DC, h->d_bits);
+    h->launches++;
+    if (cudaPeekAtLastError() != cudaSuccess) return bail(fail(h, HIPFT_ECUDA, "k_gershgorin launch failed"));
+    if ((rc = sync_read(h, h->d_bits, sizeof(unsigned long long)))) return bail(rc);
+    unsigned long long bits;
+    std::memcpy(&bits, h->h_pin, 8);
+    double max_eig;
+    std::memcpy(&max_eig, &bits, 8);
+    h->dt_euler = c_safety * (2.0 / max_eig);
+  }
+
+  // flows and WENO (load_flows src/hipft.f90:2535-2564, load_weno 6846)
+  h->bc_flow_n = 2.0 * h->dth_i[2] * c_pi_i;
+  h->bc_flow_s = 2.0 * h->dth_i[nt - 1] * c_pi_i;
+  if (prm->advance_flow) {
+    std::vector<double> wt[7], wp[7];
+    weno_weights(h, wt, wp);
+    std::vector<double> pk;
+    std::vector<size_t> wo;
+    for (int q = 0; q < 7; ++q) { wo.push_back(pk.size()); pk.insert(pk.end(), wt[q].begin(), wt[q].end()); }
+    for (int q = 0; q < 7; ++q) { wo.push_back(pk.size()); pk.insert(pk.end(), wp[q].begin(), wp[q].end()); }
+    double *dw = nullptr;
+    if ((rc = dalloc(h, &dw, pk.size()))) return bail(rc);
+    if ((rc = upload(h, dw, pk))) return bail(rc);
+    h->W.cpt = dw + wo[0]; h->W.mct = dw + wo[1]; h->W.mt = dw + wo[2]; h->W.cptt = dw + wo[3];
+    h->W.pt = dw + wo[4]; h->W.mctt = dw + wo[5]; h->W.epst = dw + wo[6];
+    h->W.cpp = dw + wo[7]; h->W.mcp = dw + wo[8]; h->W.mp = dw + wo[9]; h->W.cptp = dw + wo[10];
+    h->W.pp = dw + wo[11]; h->W.mctp = dw + wo[12]; h->W.epsp = dw + wo[13];
+    if ((rc = dalloc(h, &h->d_vt1, (size_t)nr * (nt + 1)))) return bail(rc);
+    if ((rc = dalloc(h, &h->d_vp1, (size_t)nr * (ntm + 1)))) return bail(rc);
+    if ((rc = dalloc(h, &h->d_at1, (size_t)nr * (ntm + 1)))) return bail(rc);
+    if ((rc = dalloc(h, &h->d_ap1, (size_t)nr * (ntm + 1)))) return bail(rc);
+    h->FL.vt1 = h->d_vt1; h->FL.vp1 = h->d_vp1; h->FL.at1 = h->d_at1; h->FL.ap1 = h->d_ap1;
+    h->FL.ldv = h->ldv;
+    h->FL.vplane = (int64_t)h->ldv * npm;
+    h->FL.upwind = prm->upwind;
+    // zero flow until set_flow
+    std::vector<double> z1((size_t)nr * (nt + 1), 0.0), z2((size_t)nr * (ntm + 1), 0.0);
+    if ((rc = upload(h, h->d_vt1, z1)) || (rc = upload(h, h->d_vp1, z2)) || (rc = upload(h, h->d_at1, z2)) ||
+        (rc = upload(h, h->d_ap1, z2)))
+      return bail(rc);
+  }
+
+  // analysis weights (src/hipft.f90:3230-3257; get_flux 8712-8732)
+  {
+    std::vector<double> w(6 * (size_t)(std::max(ntm, npm) + 1), 0.0);
+    size_t L = (size_t)std::max(ntm, npm) + 1;
+    double *da_t = &w[0], *sn_t = &w[L], *cs_t = &w[2 * L], *da_p = &w[3 * L], *cs_p = &w[4 * L], *sn_p = &w[5 * L];
+    for (int j = 1; j <= ntm; ++j) {
+      double tav, sn, cs, d;
+      if (j == 1) {
+        tav = 0.5 * (h->t[1] + h->t[2]);
+        sn = std::sin(tav); cs = std::cos(tav); d = h->dth[2];
+        da_t[j] = 0.25 * sn * d;
+      } else if (j == ntm) {
+        tav = 0.5 * (h->t[ntm] + h->t[ntm - 1]);
+        sn = std::sin(tav); cs = std::cos(tav); d = h->dth[ntm];
+        da_t[j] = 0.25 * sn * d;
+      } else {
+        sn = std::sin(h->t[j]); cs = std::cos(h->t[j]); d = h->dt[j];
+        da_t[j] = sn * d;
+      }
+      sn_t[j] = sn;
+      cs_t[j] = cs;
+    }
+    for (int k = 1; k <= npm - 1; ++k) {
+      if (k == 1) da_p[k] = 0.5 * h->dph[1];
+      else if (k == npm - 1) da_p[k] = 0.5 * h->dph[npm - 1];
+      else da_p[k] = h->dp[k];
+      cs_p[k] = std::cos(h->p[k]);
+      sn_p[k] = std::sin(h->p[k]);
+    }
+    h->da_t.assign(da_t, da_t + ntm + 1);
+    h->da_p.assign(da_p, da_p + npm);
+    if ((rc = dalloc(h, &h->d_anw, w.size()))) return bail(rc);
+    if ((rc = upload(h, h->d_anw, w))) return bail(rc);
+    std::vector<unsigned char> masks(2 * (size_t)(ntm + 1), 0);
+    for (int j = 1; j <= ntm; ++j) {
+      masks[j] = (h->t[j] <= prm->pole_flux_lat_limit * c_d2r) ? 1 : 0;
+      masks[ntm + 1 + j] = (h->t[j] >= c_pi - prm->pole_flux_lat_limit * c_d2r) ? 1 : 0;
+    }
+    if ((rc = dalloc(h, &h->d_masks, masks.size()))) return bail(rc);
+    if (cudaMemcpyAsync(h->d_masks, masks.data(), masks.size(), cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+      return bail(HIPFT_ECUDA);
+    if ((rc = dalloc(h, &h->d_vscale, nr + 1))) return bail(rc);
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(fail(h, HIPFT_ECUDA, "create: sync failed"));
+  *out = h;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_destroy(hipft_gpu *h) {
+  if (!h) return HIPFT_OK;
+  cudaSetDevice(h->dev);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->h_pin) cudaFreeHost(h->h_pin);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_last_error(const hipft_gpu *h, char *buf, size_t len) {
+  if (!buf || !len) return HIPFT_EINVAL;
+  const char *m = h ? h->err.c_str() : "no handle";
+  std::snprintf(buf, len, "%s", m);
+  return HIPFT_OK;
+}
+
+extern "C" const char *hipft_gpu_version(void) { return "hipft_b200 0.1.0 (sm_100a, fp64)"; }
+
+// ------------------------------------------------------------- field I/O
+extern "C" int hipft_gpu_set_field(hipft_gpu *h, const double *f) {
+  if (!h || !f) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaMemcpy2DAsync(h->buf[h->cur], (size_t)h->ldt * sizeof(double), f, (size_t)h->ntm * sizeof(double),
+                          (size_t)h->ntm * sizeof(double), (size_t)h->npm * h->nr, cudaMemcpyHostToDevice,
+                          h->stream));
+  h->field_set = true;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_get_field(hipft_gpu *h, double *f) {
+  if (!h || !f) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaMemcpy2DAsync(f, (size_t)h->ntm * sizeof(double), h->buf[h->cur], (size_t)h->ldt * sizeof(double),
+                          (size_t)h->ntm * sizeof(double), (size_t)h->npm * h->nr, cudaMemcpyDeviceToHost,
+                          h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+// get_flux of a host (ntm,npm) slab (src/hipft.f90:8706-8738).
+static void host_flux(const hipft_gpu *h, const double *map, double &fp, double &fm) {
+  fp = 0.0;
+  fm = 0.0;
+  for (int k = 1; k <= h->npm - 1; ++k)
+    for (int j = 1; j <= h->ntm; ++j) {
+      double fv = map[(size_t)(k - 1) * h->ntm + (j - 1)] * h->da_t[j] * h->da_p[k];
+      if (fv > 0.0) fp = fp + fv; else fm = fm + fv;
+    }
+}
+
+extern "C" int hipft_gpu_load_initial_map(hipft_gpu *h, const double *map_pt, int flux_balance, double mult_fac) {
+  if (!h || !map_pt) return HIPFT_EINVAL;
+  int ntm = h->ntm, npm = h->npm, npm1 = h->npm1, nr = h->nr;
+  std::vector<double> f((size_t)ntm * npm * nr);
+  auto F = [&](int j, int k, int i) -> double & { return f[((size_t)(i - 1) * npm + (k - 1)) * ntm + (j - 1)]; };
+  for (int i = 1; i <= nr; ++i)
+    for (int k = 1; k <= npm1; ++k)
+      for (int j = 1; j <= ntm; ++j) F(j, k, i) = map_pt[((size_t)(i - 1) * ntm + (j - 1)) * npm1 + (k - 1)];
+  for (int i = 1; i <= nr; ++i)
+    for (int j = 1; j <= ntm; ++j) {
+      F(j, 1, i) = 0.5 * (F(j, 1, i) + F(j, npm1, i));
+      F(j, npm1, i) = F(j, 1, i);
+      F(j, npm1 + 1, i) = F(j, 2, i);
+    }
+  for (int i = 1; i <= nr; ++i) {
+    double fn1 = 0.0, fs1 = 0.0;
+    for (int k = 2; k <= npm - 1; ++k) {
+      fn1 = fn1 + F(1, k, i) * h->dp[k];
+      fs1 = fs1 + F(ntm, k, i) * h->dp[k];
+    }
+    for (int k = 1; k <= npm; ++k) {
+      F(1, k, i) = fn1 * 0.15915494309189535;
+      F(ntm, k, i) = fs1 * 0.15915494309189535;
+    }
+  }
+  if (flux_balance)
+    for (int i = 1; i <= nr; ++i) {
+      double *slab = &f[(size_t)(i - 1) * npm * ntm];
+      double fp, fm;
+      host_flux(h, slab, fp, fm);
+      if (fm + fp == 0.0) continue;
+      double ratio = std::sqrt(std::fabs(fp / fm));
+      for (size_t q = 0; q < (size_t)npm * ntm; ++q) slab[q] = (slab[q] > 0) ? slab[q] / ratio : slab[q] * ratio;
+    }
+  for (auto &v : f) v = mult_fac * v;
+  return hipft_gpu_set_field(h, f.data());
+}
+
+// ------------------------------------------------------------------ flows
+extern "C" int hipft_gpu_set_flow(hipft_gpu *h, const hipft_flow_def *def) {
+  if (!h || !def) return HIPFT_EINVAL;
+  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "set_flow: advance_flow is off for this handle");
+  int nr = h->nr;
+  auto take = [&](std::vector<double> &v, const double *src, double dflt) {
+    v.assign(nr, dflt);
+    if (src) std::copy(src, src + nr, v.begin());
+  };
+  if ((def->flow_dr_model == 1 && (!def->dr_p0 || !def->dr_p2 || !def->dr_p4)) ||
+      (def->flow_mf_model == 1 && (!def->mf_p1 || !def->mf_p3 || !def->mf_p5)) ||
+      (def->flow_attenuate && !def->flow_attenuate_values))
+    return fail(h, HIPFT_EINVAL, "set_flow: missing per-realization coefficients");
+  take(h->f_p0, def->dr_p0, 0); take(h->f_p2, def->dr_p2, 0); take(h->f_p4, def->dr_p4, 0);
+  take(h->f_p1, def->mf_p1, 0); take(h->f_p3, def->mf_p3, 0); take(h->f_p5, def->mf_p5, 0);
+  take(h->f_att, def->flow_attenuate_values, 0);
+  h->fdef = *def;
+  h->have_flow = true;
+  h->flow_needs_updating = true;
+  h->flow2d = def->flow_attenuate || def->flow_rigid_omega != 0.0;
+  return HIPFT_OK;
+}
+
+// 1-D analytic parts of vt (theta faces) and vp (phi faces), per
+// realization, in the order update_flow adds them (src/hipft.f90:3409-3437).
+static void analytic_profiles(const hipft_gpu *h, std::vector<double> &vt1, std::vector<double> &vp1) {
+  int nt = h->nt, ntm = h->ntm, nr = h->nr;
+  const hipft_flow_def &d = h->fdef;
+  vt1.assign((size_t)nr * (nt + 1), 0.0);
+  vp1.assign((size_t)nr * (ntm + 1), 0.0);
+  for (int i = 1; i <= nr; ++i) {
+    double *vt = &vt1[(size_t)(i - 1) * (nt + 1)];
+    double *vp = &vp1[(size_t)(i - 1) * (ntm + 1)];
+    if (d.flow_mf_model == 1)
+      for (int j = 1; j <= nt; ++j) {
+        double c = h->cth[j];
+        vt[j] = vt[j] - c_m_s_to_rs_hr * h->sth[j] *
+                            (h->f_p1[i - 1] * c + h->f_p3[i - 1] * pow3(c) + h->f_p5[i - 1] * pow5(c));
+      }
+    if (d.flow_dr_model == 1)
+      for (int j = 1; j <= ntm; ++j) {
+        double c = h->ct[j];
+        double c2 = c * c, c4 = c2 * c2;
+        vp[j] = vp[j] + c_m_s_to_rs_hr * h->st[j] * (h->f_p0[i - 1] + h->f_p2[i - 1] * c2 + h->f_p4[i - 1] * c4);
+      }
+    if (d.flow_vp_rigid_omega != 0.0)
+      for (int j = 1; j <= ntm; ++j) vp[j] = vp[j] + d.flow_vp_rigid_omega * c_km_s_to_rs_hr * h->st[j];
+    if (d.flow_vt_const != 0.0)
+      for (int j = 1; j <= nt; ++j) vt[j] = vt[j] + d.flow_vt_const * c_km_s_to_rs_hr;
+  }
+}
+
+extern "C" int hipft_gpu_update_flow(hipft_gpu *h, int *updated) {
+  if (!h) return HIPFT_EINVAL;
+  if (updated) *updated = 0;
+  if (!h->have_flow || !h->flow_needs_updating) return HIPFT_OK;
+  CK(h, cudaSetDevice(h->dev));
+  h->flow_needs_updating = false;
+  int nt = h->nt, ntm = h->ntm, nr = h->nr, npm = h->npm;
+  std::vector<double> vt1, vp1;
+  analytic_profiles(h, vt1, vp1);
+  TRY(upload(h, h->d_vt1, vt1));
+  TRY(upload(h, h->d_vp1, vp1));
+  if (!h->flow2d) {
+    // set_lf_alpha on theta-only profiles (src/hipft.f90:6968-7037)
+    std::vector<double> at1((size_t)nr * (ntm + 1), 0.0), ap1((size_t)nr * (ntm + 1), 0.0);
+    for (int i = 1; i <= nr; ++i) {
+      const double *vt = &vt1[(size_t)(i - 1) * (nt + 1)];
+      const double *vp = &vp1[(size_t)(i - 1) * (ntm + 1)];
+      double *at = &at1[(size_t)(i - 1) * (ntm + 1)];
+      double *ap = &ap1[(size_t)(i - 1) * (ntm + 1)];
+      auto A = [&](int j) { return std::fabs(vt[j]); };
+      for (int j = 3; j <= nt - 3; ++j)
+        at[j] = std::max(std::max(std::max(std::max(std::max(A(j - 2), A(j - 1)), A(j)), A(j + 1)), A(j + 2)), A(j + 3));
+      at[1] = std::max(std::max(std::max(A(1), A(2)), A(3)), A(4));
+      at[2] = std::max(std::max(std::max(std::max(A(1), A(2)), A(3)), A(4)), A(5));
+      { int j = nt - 2; at[j] = std::max(std::max(std::max(std::max(A(j - 2), A(j - 1)), A(j)), A(j + 1)), A(j + 2)); }
+      { int j = nt - 1; at[j] = std::max(std::max(std::max(A(j - 2), A(j - 1)), A(j)), A(j + 1)); }
+      for (int j = 2; j <= ntm - 1; ++j) ap[j] = std::fabs(vp[j]);
+    }
+    TRY(upload(h, h->d_at1, at1));
+    TRY(upload(h, h->d_ap1, ap1));
+    h->FL.flow2d = 0;
+  } else {
+    if (!h->d_vt) {
+      size_t n2 = (size_t)h->ldv * npm * nr;
+      TRY(dalloc(h, &h->d_vt, n2));
+      TRY(dalloc(h, &h->d_vp, n2));
+      TRY(dalloc(h, &h->d_at, n2));
+      TRY(dalloc(h, &h->d_ap, n2));
+      CK(h, cudaMemsetAsync(h->d_at, 0, n2 * sizeof(double), h->stream));
+      CK(h, cudaMemsetAsync(h->d_ap, 0, n2 * sizeof(double), h->stream));
+      // cos(p), sin(p), cos(ph), theta metrics (1-based), attenuation factors
+      size_t L = (size_t)std::max(npm, nt) + 2;
+      std::vector<double> trig(7 * L, 0.0);
+      for (int k = 1; k <= npm; ++k) {
+        trig[k] = std::cos(h->p[k]);
+        trig[L + k] = std::sin(h->p[k]);
+        trig[2 * L + k] = std::cos(h->ph[k]);
+      }
+      for (int j = 1; j <= nt; ++j) { trig[3 * L + j] = h->cth[j]; trig[4 * L + j] = h->sth[j]; }
+      for (int j = 1; j <= ntm; ++j) { trig[5 * L + j] = h->ct[j]; trig[6 * L + j] = h->st[j]; }
+      TRY(dalloc(h, &h->d_trig, trig.size()));
+      TRY(upload(h, h->d_trig, trig));
+      std::vector<double> att(nr + 1, 0.0);
+      for (int i = 1; i <= nr; ++i)
+        att[i] = (h->f_att[i - 1] > 0.0) ? 1.0 / h->f_att[i - 1] : DBL_MAX;
+      TRY(dalloc(h, &h->d_atten, nr + 1));
+      TRY(upload(h, h->d_atten, att));
+    }
+    if (h->fdef.flow_attenuate && !h->field_set) return fail(h, HIPFT_ESTATE, "update_flow: attenuation needs the field");
+    size_t L = (size_t)std::max(npm, nt) + 2;
+    Flow2DBuild b{};
+    b.vt1 = h->d_vt1; b.vp1 = h->d_vp1;
+    b.cosp = h->d_trig; b.sinp = h->d_trig + L; b.cosph = h->d_trig + 2 * L;
+    b.cth = h->d_trig + 3 * L; b.sth = h->d_trig + 4 * L; b.ct = h->d_trig + 5 * L; b.st = h->d_trig + 6 * L;
+    b.vrigid = h->fdef.flow_rigid_omega * c_km_s_to_rs_hr;
+    b.attenuate = h->fdef.flow_attenuate;
+    b.atten_i = h->d_atten;
+    dim3 blk(32, 8), grd((unsigned)((nt + 31) / 32), (unsigned)((npm + 7) / 8), (unsigned)nr);
+    k_flow_build<<<grd, blk, 0, h->stream>>>(h->M, b, h->ldv, h->buf[h->cur], h->d_vt, h->d_vp);
+    LAUNCHED(h);
+    if (h->fdef.flow_attenuate) {
+      k_seam<<<dim3((unsigned)((nt + 127) / 128), (unsigned)nr), 128, 0, h->stream>>>(h->M, nt, h->ldv, h->d_vt);
+      LAUNCHED(h);
+      k_seam<<<dim3((unsigned)((ntm + 127) / 128), (unsigned)nr), 128, 0, h->stream>>>(h->M, ntm, h->ldv, h->d_vp);
+      LAUNCHED(h);
+      h->flow_needs_updating = true;  // Br changes every step (src/hipft.f90:3514)
+    }
+    if (h->adv_space == 2) {
+      dim3 g2((unsigned)((ntm + 31) / 32), (unsigned)((npm + 7) / 8), (unsigned)nr);
+      k_lf_alpha<<<g2, blk, 0, h->stream>>>(h->M, h->ldv, h->d_vt, h->d_vp, h->d_at, h->d_ap);
+      LAUNCHED(h);
+    }
+    h->FL.vt = h->d_vt; h->FL.vp = h->d_vp; h->FL.at = h->d_at; h->FL.ap = h->d_ap;
+    h->FL.flow2d = 1;
+  }
+  if (updated) *updated = 1;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_flow_dtmax(hipft_gpu *h, double *dtmax) {
+  if (!h || !dtmax) return HIPFT_EINVAL;
+  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "flow_dtmax: advance_flow is off");
+  CK(h, cudaSetDevice(h->dev));
+  unsigned long long init = 0x7fefffffffffffffULL;  // DBL_MAX bits
+  CK(h, cudaMemcpyAsync(h->d_bits + 1, &init, 8, cudaMemcpyHostToDevice, h->stream));
+  dim3 blk(32, 8), grd((unsigned)((h->ntm - 2 + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)h->nr);
+  k_flow_dtmax<<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->d_bits + 1);
+  LAUNCHED(h);
+  TRY(sync_read(h, h->d_bits + 1, 8));
+  double d;
+  std::memcpy(&d, h->h_pin, 8);
+  d = c_safety * d;
+  if (h->P.strang_splitting) d = 2.0 * d;
+  if (h->adv_time == 3) d = 2.0 * d;
+  *dtmax = d;
+  return HIPFT_OK;
+}
+
+// ------------------------------------------------------------- advection
+extern "C" int hipft_gpu_advection_step(hipft_gpu *h, double dt) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "advection_step before set_field");
+  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "advection_step: advance_flow is off");
+  CK(h, cudaSetDevice(h->dev));
+  double *f = h->buf[h->cur];
+  int ia = scratch(h, 0), ib = scratch(h, 1);
+  double *A = h->buf[ia], *B = h->buf[ib];
+  if (h->adv_time == 1) {  // FE (src/hipft.f90:7440-7444)
+    TRY(advection_stage(h, f, nullptr, A, AdvCombine{0, 0.0, 0.0, dt}));
+    h->cur = ia;
+  } else if (h->adv_time == 2) {  // SSPRK(3,3) (7486-7505)
+    TRY(advection_stage(h, f, nullptr, A, AdvCombine{0, 0.0, 0.0, dt}));
+    TRY(advection_stage(h, A, f, B, AdvCombine{1, c_three_quarter, c_quarter, c_quarter * dt}));
+    TRY(advection_stage(h, B, f, f, AdvCombine{1, c_third, c_two_third, c_two_third * dt}));
+  } else {  // SSPRK(4,3) (7552-7574)
+    TRY(advection_stage(h, f, nullptr, A, AdvCombine{0, 0.0, 0.0, 0.5 * dt}));
+    TRY(advection_stage(h, A, nullptr, B, AdvCombine{0, 0.0, 0.0, 0.5 * dt}));
+    TRY(advection_stage(h, B, f, A, AdvCombine{1, c_two_third, c_third, c_sixth * dt}));
+    TRY(advection_stage(h, A, nullptr, f, AdvCombine{0, 0.0, 0.0, 0.5 * dt}));
+  }
+  return HIPFT_OK;
+}
+
+// ------------------------------------------------------------- diffusion
+// load_sts_rkl2 / load_sts_rkg2 (src/hipft.f90:5244-5475).
+static void load_sts(hipft_gpu *h, double dtl) {
+  int64_t s;
+  if (h->P.diffusion_num_method == 2)
+    s = (int64_t)std::ceil(0.5 * (std::sqrt(9.0 + 16.0 * (dtl / h->dt_euler)) - 1.0));
+  else
+    s = (int64_t)std::ceil(0.5 * (std::sqrt(25.0 + 24.0 * (dtl / h->dt_euler)) - 3.0));
+  if (s < 3) s = 3;
+  if (s % 2 == 0) s = s + 1;
+  h->sts_s = s;
+  auto &b = h->sts_b, &uj = h->sts_uj, &vj = h->sts_vj, &ubj = h->sts_ubj, &gj = h->sts_gj;
+  b.assign(s + 1, 0); uj.assign(s + 1, 0); vj.assign(s + 1, 0); ubj.assign(s + 1, 0); gj.assign(s + 1, 0);
+  if (h->P.diffusion_num_method == 2) {
+    double w = 4.0 / (double)(s * s + s - 2);
+    b[1] = 1.0 / 3.0; b[2] = 1.0 / 3.0;
+    uj[1] = -9999.0; vj[1] = -9999.0; ubj[1] = 4.0 / (3.0 * (double)(s * s + s - 2)); gj[1] = -9999.0;
+    uj[2] = 3.0 / 2.0; vj[2] = -0.5; ubj[2] = uj[2] * w; gj[2] = -w;
+    for (int64_t j = 3; j <= s; ++j) {
+      b[j] = ((double)(j * j + j) - 2.0) / (2.0 * (double)j * (double)(j + 1));
+      double r1 = b[j] / b[j - 1], r2 = b[j] / b[j - 2];
+      uj[j] = r1 * (2.0 - 1.0 / (double)j);
+      vj[j] = r2 * (1.0 / (double)j - 1.0);
+      ubj[j] = uj[j] * w;
+      gj[j] = (b[j - 1] - 1.0) * ubj[j];
+    }
+  } else {
+    double w = 6.0 / (double)((s + 4) * (s - 1));
+    b[1] = 1.0 / 3.0; b[2] = 1.0 / 15.0;
+    uj[1] = 1.0; vj[1] = -9999.0; ubj[1] = w; gj[1] = -9999.0;
+    uj[2] = 1.0 / 2.0; vj[2] = -1.0 / 10.0; ubj[2] = uj[2] * w; gj[2] = 0.0;
+    for (int64_t j = 3; j <= s; ++j) {
+      b[j] = (4.0 * (double)(j - 1) * (double)(j + 4)) /
+             (3.0 * (double)j * (double)(j + 1) * (double)(j + 2) * (double)(j + 3));
+      double r1 = b[j] / b[j - 1], r2 = b[j] / b[j - 2];
+      uj[j] = r1 * (2.0 + 1.0 / (double)j);
+      vj[j] = -r2 * (1.0 / (double)j + 1.0);
+      ubj[j] = uj[j] * w;
+      gj[j] = (0.5 * (double)j * ((double)j + 1.0) * b[j - 1] - 1.0) * ubj[j];
+    }
+  }
+}
+
+// diffusion_step_sts_cd (src/hipft.f90:5163-5242): stage 1 then the
+// s-1 fused stages, rotating three scratch fields.
+static int sts_super_step(hipft_gpu *h, double dtl) {
+  load_sts(h, dtl);
+  int u0 = h->cur, idty = scratch(h, 0), ia = scratch(h, 1), ib = scratch(h, 2);
+  TRY(ring_diffusion(h, h->buf[u0]));
+  TRY(diffusion_stage<MODE_STS1>(h, h->buf[u0], nullptr, nullptr, nullptr, h->buf[ia], h->buf[idty],
+                                 StageCoef{dtl, h->sts_ubj[1], 0, 0, 0}, nullptr));
+  int ykm1 = ia, ykm2 = u0;
+  for (int64_t k = 2; k <= h->sts_s; ++k) {
+    TRY(ring_diffusion(h, h->buf[ykm1]));
+    int out = (k == 2) ? ib : ykm2;
+    double uj = h->sts_uj[k], vj = h->sts_vj[k];
+    StageCoef sc{uj, vj, 1.0 - uj - vj, h->sts_ubj[k] * dtl, h->sts_gj[k]};
+    TRY(diffusion_stage<MODE_STSK>(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[out], nullptr,
+                                   sc, nullptr));
+    ykm2 = ykm1;
+    ykm1 = out;
+  }
+  h->cur = ykm1;
+  h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr * h->sts_s;
+  return HIPFT_OK;
+}
+
+// diffusion_step_fe_cd (src/hipft.f90:7352-7407).
+static int euler_steps(hipft_gpu *h, double dtl) {
+  int64_t n = (int64_t)std::ceil(dtl / h->dt_euler);
+  h->n_euler = n;
+  double dte = dtl / (double)n;
+  for (int64_t c = 0; c < n; ++c) {
+    int o = scratch(h, 0);
+    TRY(ring_diffusion(h, h->buf[h->cur]));
+    TRY(diffusion_stage<MODE_EULER>(h, h->buf[h->cur], nullptr, nullptr, nullptr, h->buf[o], nullptr,
+                                    StageCoef{dte, 0, 0, 0, 0}, nullptr));
+    h->cur = o;
+  }
+  h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr * n;
+  return HIPFT_OK;
+}
+
+// get_dtime_diffusion_ptl (src/hipft.f90:5042-5161).
+static int ptl_dt(hipft_gpu *h, double *dtl) {
+  double dtime_in = *dtl;
+  double *f = h->buf[h->cur], *af = h->buf[scratch(h, 0)];
+  CK(h, cudaMemsetAsync(h->d_bits, 0, 2 * sizeof(unsigned long long), h->stream));
+  TRY(ring_diffusion(h, f));
+  TRY(diffusion_stage<MODE_AX>(h, f, nullptr, nullptr, nullptr, af, nullptr, StageCoef{}, h->d_bits));
+  TRY(sync_read(h, h->d_bits, 8));
+  double axabsmax;
+  std::memcpy(&axabsmax, h->h_pin, 8);
+  double d = DBL_MAX;
+  if (axabsmax > 0.0) {
+    unsigned long long init = 0x7fefffffffffffffULL;
+    CK(h, cudaMemcpyAsync(h->d_bits + 1, &init, 8, cudaMemcpyHostToDevice, h->stream));
+    dim3 blk(32, 8);
+    k_ptl<<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, f, af, h->d_bits, h->d_bits + 1);
+    LAUNCHED(h);
+    TRY(sync_read(h, h->d_bits + 1, 8));
+    std::memcpy(&d, h->h_pin, 8);
+    d = 0.95 * d;
+    if (d < dtime_in) d = dtime_in;
+  }
+  *dtl = d;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_diffusion_step(hipft_gpu *h, double dtl, hipft_cycle_cb cb, void *user,
+                                        hipft_diffusion_info *info) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "diffusion_step before set_field");
+  if (!h->P.advance_diffusion) return fail(h, HIPFT_ESTATE, "diffusion_step: advance_diffusion is off");
+  CK(h, cudaSetDevice(h->dev));
+  const int max_sc = 60;
+  int64_t stages0 = h->cell_updates;
+  int i = 1;
+  bool done = false;
+  double time_stepped = 0.0;
+  double dtl2 = h->auto_sc ? 0.0 : dtl / (double)h->P.diffusion_subcycles;
+  for (;;) {
+    if (h->auto_sc) TRY(ptl_dt(h, &dtl2));
+    if (h->auto_sc && time_stepped + dtl2 >= dtl) {
+      dtl2 = dtl - time_stepped;
+      done = true;
+    }
+    if (h->auto_sc && i == max_sc - 1) {
+      dtl2 = dtl - time_stepped;
+      done = true;
+    }
+    if (h->auto_sc && h->P.verbose > 0) h->subcycles_state = (int64_t)std::ceil((dtl - time_stepped) / dtl2);
+    if (h->P.diffusion_num_method == 1) TRY(euler_steps(h, dtl2));
+    else TRY(sts_super_step(h, dtl2));
+    time_stepped = time_stepped + dtl2;
+    if (cb) {
+      CK(h, cudaStreamSynchronize(h->stream));
+      cb(user, i, time_stepped, dtl2, h->P.diffusion_num_method == 1 ? h->n_euler : h->sts_s, h->subcycles_state);
+    }
+    if (!h->auto_sc && i == h->P.diffusion_subcycles) done = true;
+    if (done) break;
+    i = i + 1;
+  }
+  if (h->auto_sc) h->subcycles_state = i;
+  if (info) {
+    info->dtime_diffusion_euler = h->dt_euler;
+    info->sts_s = (h->P.diffusion_num_method == 1) ? h->n_euler : h->sts_s;
+    info->subcycles = h->subcycles_state;
+    int64_t cells = (int64_t)h->ntm * (h->npm - 2) * h->nr;
+    info->total_stages = cells ? (h->cell_updates - stages0) / cells : 0;
+  }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_flux_transport_step(hipft_gpu *h, double dt, hipft_cycle_cb cb, void *user,
+                                             hipft_diffusion_info *info) {
+  if (!h) return HIPFT_EINVAL;
+  if (h->P.strang_splitting) {
+    double half = dt * 0.5;
+    if (h->P.advance_flow) TRY(hipft_gpu_advection_step(h, half));
+    if (h->P.advance_diffusion) TRY(hipft_gpu_diffusion_step(h, dt, cb, user, info));
+    if (h->P.advance_flow) TRY(hipft_gpu_advection_step(h, half));
+  } else {
+    if (h->P.advance_flow) TRY(hipft_gpu_advection_step(h, dt));
+    if (h->P.advance_diffusion) TRY(hipft_gpu_diffusion_step(h, dt, cb, user, info));
+  }
+  return HIPFT_OK;
+}
+
+// ------------------------------------------------------------ assimilation
+extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o) {
+  if (!h || !data3_pt || !o) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "assimilate before set_field");
+  if (!o->lat_limit || (o->custom_from_mu && (!o->mu_power || !o->mu_limit)))
+    return fail(h, HIPFT_EINVAL, "assimilate: missing per-realization options");
+  CK(h, cudaSetDevice(h->dev));
+  int ntm = h->ntm, npm1 = h->npm1, nr = h->nr;
+  size_t nd = (size_t)npm1 * ntm * 3;
+  if (!h->d_da) {
+    TRY(dalloc(h, &h->d_da, nd));
+    TRY(dalloc(h, &h->d_daopt, 3 * (size_t)(nr + 1)));
+    TRY(dalloc(h, &h->d_tidx, 2 * (size_t)(nr + 1)));
+  }
+  CK(h, cudaMemcpyAsync(h->d_da, data3_pt, nd * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  std::vector<double> opt(3 * (size_t)(nr + 1), 0.0);
+  std::vector<int> tidx(2 * (size_t)(nr + 1), -1);
+  for (int i = 1; i <= nr; ++i) {
+    opt[i] = o->mu_power ? o->mu_power[i - 1] : 0.0;
+    opt[(nr + 1) + i] = o->mu_limit ? o->mu_limit[i - 1] : 0.0;
+    opt[2 * (nr + 1) + i] = o->lat_limit[i - 1];
+    // lat-limit indices (load_data_assimilation, src/hipft.f90:4066-4079)
+    int t0 = -1, t1 = -1;
+    for (int j = 1; j <= ntm; ++j)
+      if (h->t[j] >= o->lat_limit[i - 1] * c_d2r && t0 == -1) t0 = j;
+    for (int j = ntm; j >= 1; --j)
+      if (h->t[j] <= (c_pi - o->lat_limit[i - 1] * c_d2r) && t1 == -1) t1 = j;
+    tidx[i] = t0;
+    tidx[(nr + 1) + i] = t1;
+  }
+  TRY(upload(h, h->d_daopt, opt));
+  CK(h, cudaMemcpyAsync(h->d_tidx, tidx.data(), tidx.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  DAArgs a{};
+  a.data = h->d_da;
+  a.mu_power = h->d_daopt;
+  a.mu_limit = h->d_daopt + (nr + 1);
+  a.lat_limit = h->d_daopt + 2 * (nr + 1);
+  a.tidx0 = h->d_tidx;
+  a.tidx1 = h->d_tidx + (nr + 1);
+  a.add = o->add;
+  a.custom_from_mu = o->custom_from_mu;
+  a.mult_fac = o->mult_fac;
+  double *f = h->buf[h->cur], *delta = h->buf[scratch(h, 0)];
+  dim3 blk(32, 8), grd((unsigned)((ntm + 31) / 32), (unsigned)((npm1 + 31) / 32), (unsigned)nr);
+  k_da_delta<<<grd, blk, 0, h->stream>>>(h->M, a, f, delta);
+  LAUNCHED(h);
+  const double *ratio = nullptr;
+  if (o->balance_flux) {
+    int cpb = 16, nb = (h->npm - 1 + cpb - 1) / cpb;
+    TRY(ensure_part(h, (size_t)nr * nb * 2 + (nr + 1)));
+    double *da_t = h->d_anw, *da_p = h->d_anw + 3 * ((size_t)std::max(ntm, h->npm) + 1);
+    k_flux_partial<<<dim3((unsigned)nb, (unsigned)nr), 256, 0, h->stream>>>(h->M, da_t, da_p, delta, 1, h->d_part,
+                                                                            cpb);
+    LAUNCHED(h);
+    std::vector<double> part((size_t)nr * nb * 2);
+    CK(h, cudaMemcpyAsync(part.data(), h->d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    std::vector<double> r(nr + 1, 1.0);
+    for (int i = 0; i < nr; ++i) {
+      double fp = 0.0, fm = 0.0;
+      for (int b = 0; b < nb; ++b) {
+        fp = fp + part[((size_t)i * nb + b) * 2];
+        fm = fm + part[((size_t)i * nb + b) * 2 + 1];
+      }
+      r[i + 1] = (fm + fp == 0.0) ? 1.0 : std::sqrt(std::fabs(fp / fm));
+    }
+    double *dr = h->d_part + (size_t)nr * nb * 2;
+    TRY(upload(h, dr, r));
+    ratio = dr;
+  }
+  dim3 g2((unsigned)((ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)nr);
+  k_da_apply<<<g2, blk, 0, h->stream>>>(h->M, delta, f, ratio);
+  LAUNCHED(h);
+  return HIPFT_OK;
+}
+
+// ------------------------------------------------------------ diagnostics
+extern "C" int hipft_gpu_set_validation(hipft_gpu *h, int mode, const double *fval_u0_pt, double width,
+                                        double vt_const, double vp_omega, double time_start) {
+  if (!h || mode < 0 || mode > 2) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  h->vmode = mode;
+  h->vwidth = width;
+  h->vt_const = vt_const;
+  h->vp_omega = vp_omega;
+  h->vtime_start = time_start;
+  if (mode == 1) {
+    if (!fval_u0_pt) return HIPFT_EINVAL;
+    if (!h->P.advance_diffusion) return fail(h, HIPFT_ESTATE, "validation 1 needs diffusion coefficients");
+    size_t n = (size_t)h->npm1 * h->ntm * h->nr;
+    if (!h->d_fval_u0) TRY(dalloc(h, &h->d_fval_u0, n));
+    CK(h, cudaMemcpyAsync(h->d_fval_u0, fval_u0_pt, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  if (mode == 2 && !h->d_vgauss) {
+    // theta scale, phi scale and st_i (1-based) for the analytic Gaussians
+    size_t L = (size_t)std::max(h->npm, h->nt) + 2;
+    std::vector<double> v(3 * L, 0.0);
+    for (int j = 1; j <= h->ntm; ++j) {
+      v[j] = h->t[j];
+      v[2 * L + j] = h->st_i[j];
+    }
+    for (int k = 1; k <= h->npm; ++k) v[L + k] = h->p[k];
+    TRY(dalloc(h, &h->d_vgauss, v.size()));
+    TRY(upload(h, h->d_vgauss, v));
+  }
+  return HIPFT_OK;
+}
+
+// Fortran MODULO for reals.
+static double fmodulo(double a, double p) { return a - std::floor(a / p) * p; }
+
+extern "C" int hipft_gpu_analysis(hipft_gpu *h, double time, double *hist) {
+  if (!h || !hist) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "analysis before set_field");
+  CK(h, cudaSetDevice(h->dev));
+  int ntm = h->ntm, npm = h->npm, nr = h->nr;
+  AnalysisArgs a{};
+  size_t L = (size_t)std::max(ntm, npm) + 1;
+  a.da_t = h->d_anw; a.sn_t = h->d_anw + L; a.cs_t = h->d_anw + 2 * L;
+  a.da_p = h->d_anw + 3 * L; a.cs_p = h->d_anw + 4 * L; a.sn_p = h->d_anw + 5 * L;
+  a.pn = h->d_masks; a.ps = h->d_masks + (ntm + 1);
+  a.vmode = h->vmode;
+  if (h->vmode == 1) {
+    // fval = fval_u0 * exp(-42 D factor (time - time_start))  (src/hipft.f90:3156-3159)
+    std::vector<double> sc(nr + 1, 0.0);
+    for (int i = 1; i <= nr; ++i)
+      sc[i] = std::exp(-42.0 * h->Dc[i - 1] * h->P.diffusion_coef_factor * (time - h->vtime_start));
+    TRY(upload(h, h->d_vscale, sc));
+    a.fval_u0 = h->d_fval_u0;
+    a.vscale = h->d_vscale;
+  } else if (h->vmode == 2) {
+    size_t G = (size_t)std::max(h->npm, h->nt) + 2;
+    a.t = h->d_vgauss; a.p = h->d_vgauss + G; a.st_i = h->d_vgauss + 2 * G;
+    a.vtt = h->vt_const * c_km_s_to_rs_hr * (time - h->vtime_start);
+    a.vpt = h->vp_omega * c_km_s_to_rs_hr * (time - h->vtime_start);
+    a.p1 = fmodulo(c_pi_two + a.vpt, c_twopi);
+    a.p2 = fmodulo(c_threepi_two + a.vpt, c_twopi);
+    a.width = h->vwidth;
+  }
+  const int cpb = 8;
+  int nb = (npm - 1 + cpb - 1) / cpb;
+  TRY(ensure_part(h, (size_t)nr * nb * kNPart + (size_t)nr * kNPart));
+  double *fin = h->d_part + (size_t)nr * nb * kNPart;
+  k_analysis_partial<256><<<dim3((unsigned)nb, (unsigned)nr), 256, 0, h->stream>>>(h->M, a, h->buf[h->cur],
+                                                                                    h->d_part, cpb);
+  LAUNCHED(h);
+  k_analysis_final<<<(nr * kNPart + 127) / 128, 128, 0, h->stream>>>(nb, nr, h->d_part, fin);
+  LAUNCHED(h);
+  TRY(sync_read(h, fin, (size_t)nr * kNPart * sizeof(double)));
+  for (int i = 0; i < nr; ++i) {
+    const double *v = h->h_pin + (size_t)i * kNPart;
+    double *o = hist + (size_t)i * 14;
+    o[0] = v[0]; o[1] = v[1]; o[2] = v[2];
+    double verr = v[3], sumfval2 = v[4];
+    o[13] = (sumfval2 == 0.0) ? std::sqrt(verr / (double)((int64_t)ntm * (npm - 1))) : std::sqrt(verr / sumfval2);
+    o[3] = c_rsun_cm2 * v[5]; o[4] = c_rsun_cm2 * v[6];
+    o[5] = c_rsun_cm2 * v[7]; o[6] = c_rsun_cm2 * v[8];
+    o[7] = c_rsun_cm2 * v[9]; o[8] = c_rsun_cm2 * v[10];
+    o[9] = c_rsun_cm2 * v[11]; o[10] = c_rsun_cm2 * v[12];
+    o[12] = c_three_quarter * c_pi_i * v[15];
+    double e1 = c_three_quarter * c_pi_i * v[13], e2 = c_three_quarter * c_pi_i * v[14];
+    o[11] = std::sqrt(e1 * e1 + e2 * e2);
+  }
+  return HIPFT_OK;
+}
+
+static int flux_of(hipft_gpu *h, const double *a, std::vector<double> &fp, std::vector<double> &fm) {
+  int nr = h->nr;
+  const int cpb = 16;
+  int nb = (h->npm - 1 + cpb - 1) / cpb;
+  TRY(ensure_part(h, (size_t)nr * nb * 2 + (nr + 1)));
+  size_t L = (size_t)std::max(h->ntm, h->npm) + 1;
+  k_flux_partial<<<dim3((unsigned)nb, (unsigned)nr), 256, 0, h->stream>>>(h->M, h->d_anw, h->d_anw + 3 * L, a, 0,
+                                                                          h->d_part, cpb);
+  LAUNCHED(h);
+  std::vector<double> part((size_t)nr * nb * 2);
+  CK(h, cudaMemcpyAsync(part.data(), h->d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  fp.assign(nr, 0.0);
+  fm.assign(nr, 0.0);
+  for (int i = 0; i < nr; ++i)
+    for (int b = 0; b < nb; ++b) {
+      fp[i] = fp[i] + part[((size_t)i * nb + b) * 2];
+      fm[i] = fm[i] + part[((size_t)i * nb + b) * 2 + 1];
+    }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_get_flux(hipft_gpu *h, double *flux_p, double *flux_m) {
+  if (!h || !flux_p || !flux_m) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "get_flux before set_field");
+  CK(h, cudaSetDevice(h->dev));
+  std::vector<double> fp, fm;
+  TRY(flux_of(h, h->buf[h->cur], fp, fm));
+  std::copy(fp.begin(), fp.end(), flux_p);
+  std::copy(fm.begin(), fm.end(), flux_m);
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_balance_flux(hipft_gpu *h) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "balance_flux before set_field");
+  CK(h, cudaSetDevice(h->dev));
+  std::vector<double> fp, fm;
+  TRY(flux_of(h, h->buf[h->cur], fp, fm));
+  std::vector<double> r(h->nr + 1, 1.0);
+  for (int i = 0; i < h->nr; ++i) r[i + 1] = (fm[i] + fp[i] == 0.0) ? 1.0 : std::sqrt(std::fabs(fp[i] / fm[i]));
+  size_t L = (size_t)h->nr * ((h->npm - 1 + 15) / 16) * 2;
+  double *dr = h->d_part + L;
+  TRY(upload(h, dr, r));
+  dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)h->nr);
+  k_scale_balance<<<grd, blk, 0, h->stream>>>(h->M, h->buf[h->cur], dr);
+  LAUNCHED(h);
+  CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_info(const hipft_gpu *h, hipft_info *info) {
+  if (!h || !info) return HIPFT_EINVAL;
+  info->ntm = h->ntm;
+  info->npm = h->npm;
+  info->nr = h->nr;
+  info->ldt = h->ldt;
+  info->dtime_diffusion_euler = h->dt_euler;
+  info->sts_s = (h->P.diffusion_num_method == 1) ? h->n_euler : h->sts_s;
+  info->kernel_launches = h->launches;
+  info->cell_stage_updates = h->cell_updates;
+  info->device_bytes = h->dev_bytes;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_set_stream(hipft_gpu *h, void *s) {
+  if (!h) return HIPFT_EINVAL;
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (s) {
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->own_stream = false;
+    h->stream = (cudaStream_t)s;
+  } else if (!h->own_stream) {
+    CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_synchronize(hipft_gpu *h) {
+  if (!h) return HIPFT_EINVAL;
+  CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}

@@ -1,0 +1,834 @@
+// kernels.cuh -- device code of the flux-transport step (sm_100a, FP64).
+//
+// Layout: a field is f(j,k,i) with j = theta (1..ntm), k = phi (1..npm,
+// two-point periodic overlap), i = realization (1..nr), stored theta-fastest
+// with a padded theta stride `ldt` (a multiple of 16 doubles, 128 B) so every
+// phi column starts on a 128-byte boundary.  Index formulas below keep the
+// reference's 1-based j,k,i so each expression can be read against
+// src/hipft.f90 line by line; 1-D mesh arrays are stored with an unused
+// element 0 for the same reason.
+//
+// Every arithmetic expression is written in the reference's left-to-right
+// order and the library is compiled with --fmad=false, so stencil values are
+// bit-identical to the CPU restatement given identical inputs.  The only
+// order-dependent operations are the ring sums at the poles and the
+// diagnostic sums; both use a fixed reduction tree (deterministic run to run).
+#pragma once
+#include <cstdint>
+
+namespace hipft {
+
+constexpr double kHalf = 0.5;
+constexpr double kOne = 1.0;
+constexpr double kTwo = 2.0;
+constexpr double kFour = 4.0;
+
+// ---------------------------------------------------------------- meshes
+struct Mesh {
+  int ntm, npm, nt, np, nr, ldt;
+  int64_t plane;  // ldt * npm
+  // 1-based device arrays (element 0 unused)
+  const double *dt_i, *dth_i, *dp_i, *dph_i, *st_i, *sth, *dp, *dth, *dph;
+};
+
+__device__ __forceinline__ int64_t fidx(const Mesh &m, int j, int k, int i) {
+  return (int64_t)(i - 1) * m.plane + (int64_t)(k - 1) * m.ldt + (j - 1);
+}
+
+// ------------------------------------------------------------ diffusion
+// Diffusion coefficient on the half-half mesh, load_diffusion
+// (src/hipft.f90:6687-6820): factor * (constant [+ grid term]).
+struct DiffCoef {
+  const double *dfac;  // [nr+1] factor*constant (no grid) or constant (grid)
+  double factor;
+  int grid;
+};
+
+__device__ __forceinline__ double dcoef(const Mesh &m, const DiffCoef &c, int j, int k, int i) {
+  if (!c.grid) return c.dfac[i];
+  double a = m.dth[j], b = m.dph[k] * m.sth[j];
+  return c.factor * (c.dfac[i] + (a * a + b * b));
+}
+
+// 5-point coefficients, load_diffusion_matrix (src/hipft.f90:4958-4980).
+struct Coef5 {
+  double c1, c2, c3, c4, c5;
+};
+
+__device__ __forceinline__ Coef5 coef5(const Mesh &m, const DiffCoef &c, int j, int k, int i) {
+  double Djk = dcoef(m, c, j, k, i), Dj1k = dcoef(m, c, j + 1, k, i);
+  double Djk1 = dcoef(m, c, j, k + 1, i), Dj1k1 = dcoef(m, c, j + 1, k + 1, i);
+  Coef5 r;
+  r.c1 = kHalf * (Djk + Dj1k) * m.dph_i[k] * m.dp_i[k] * m.st_i[j] * m.st_i[j];
+  r.c2 = kHalf * (Djk + Djk1) * m.dth_i[j] * m.dt_i[j] * m.st_i[j] * m.sth[j];
+  r.c4 = kHalf * (Dj1k + Dj1k1) * m.dth_i[j + 1] * m.dt_i[j] * m.st_i[j] * m.sth[j + 1];
+  r.c5 = kHalf * (Djk1 + Dj1k1) * m.dph_i[k + 1] * m.dp_i[k] * m.st_i[j] * m.st_i[j];
+  r.c3 = -(r.c1 + r.c2 + r.c4 + r.c5);
+  return r;
+}
+
+// Deterministic block sum of two values (blockDim.x*blockDim.y threads,
+// multiple of 32, at most 1024).  Result valid in thread 0.
+__device__ __forceinline__ void block_sum2(double &a, double &b, double *sh) {
+  const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  const int nthr = blockDim.x * blockDim.y;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int w = tid >> 5, l = tid & 31, nw = nthr >> 5;
+  if (l == 0) {
+    sh[2 * w] = a;
+    sh[2 * w + 1] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    a = (l < nw) ? sh[2 * l] : 0.0;
+    b = (l < nw) ? sh[2 * l + 1] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+  }
+  __syncthreads();
+}
+
+// Pole ring sums of the diffusion operator, diffusion_operator_cd
+// (src/hipft.f90:7969-7979).  One block per realization; ring[2(i-1)] = fn,
+// ring[2(i-1)+1] = fs.
+__global__ void k_ring_diffusion(Mesh m, DiffCoef c, const double *__restrict__ x,
+                                 double *__restrict__ ring) {
+  __shared__ double sh[64];
+  const int i = blockIdx.x + 1;
+  double fn = 0.0, fs = 0.0;
+  for (int k = 2 + threadIdx.x; k <= m.npm - 1; k += blockDim.x) {
+    double x1 = x[fidx(m, 1, k, i)], x2 = x[fidx(m, 2, k, i)];
+    double xa = x[fidx(m, m.ntm - 1, k, i)], xb = x[fidx(m, m.ntm, k, i)];
+    fn = fn + (dcoef(m, c, 1, k, i) + dcoef(m, c, 2, k, i)) * (x2 - x1) * m.dp[k];
+    fs = fs + (dcoef(m, c, m.nt - 1, k, i) + dcoef(m, c, m.nt, k, i)) * (xb - xa) * m.dp[k];
+  }
+  block_sum2(fn, fs, sh);
+  if (threadIdx.x == 0) {
+    ring[2 * (i - 1)] = fn;
+    ring[2 * (i - 1) + 1] = fs;
+  }
+}
+
+// One diffusion stage: y = A x at (j,k,i) fused with the stage combine.
+//   MODE_AX    : out = A x                          (PTL's Af, F:5097)
+//   MODE_STS1  : out2 = dt*(A x); out = x + ubj1*out2 (F:5211-5218)
+//   MODE_STSK  : out = uj*x + vj*ykm2 + c*u0 + ubjdt*(A x) + gj*dty0, written
+//                over ykm2 (F:5224-5235)
+//   MODE_EULER : out = x + dte*(A x)                  (F:7396-7399)
+enum { MODE_AX = 0, MODE_STS1 = 1, MODE_STSK = 2, MODE_EULER = 3 };
+
+struct StageCoef {
+  double a, b, c, d, e;  // meaning depends on the mode
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_diffusion_stage(
+    Mesh m, DiffCoef dc, const double *__restrict__ x, const double *ykm2, const double *__restrict__ u0,
+    const double *__restrict__ dty0, double *out, double *out2, const double *__restrict__ ring, double bcn,
+    double bcs, StageCoef sc, unsigned long long *absmax_bits) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  double ax = 0.0;
+  bool active = (j <= m.ntm && k <= m.npm - 1);
+  int64_t q = 0;
+  if (active) {
+    q = fidx(m, j, k, i);
+    if (j == 1) {
+      ax = ring[2 * (i - 1)] * bcn;
+    } else if (j == m.ntm) {
+      ax = -ring[2 * (i - 1) + 1] * bcs;
+    } else {
+      Coef5 cf = coef5(m, dc, j, k, i);
+      ax = cf.c1 * x[q - m.ldt] + cf.c2 * x[q - 1] + cf.c3 * x[q] + cf.c4 * x[q + 1] + cf.c5 * x[q + m.ldt];
+    }
+    double y;
+    if (MODE == MODE_AX) {
+      y = ax;
+    } else if (MODE == MODE_STS1) {
+      double d0 = sc.a * ax;  // dt * (A f)
+      y = x[q] + sc.b * d0;   // f + ubj(1)*dty0
+      out2[q] = d0;
+      if (k == 2) out2[q + (int64_t)(m.npm - 2) * m.ldt] = d0;
+      if (k == m.npm - 1) out2[q - (int64_t)(m.npm - 2) * m.ldt] = d0;
+    } else if (MODE == MODE_STSK) {
+      y = sc.a * x[q] + sc.b * ykm2[q] + sc.c * u0[q] + sc.d * ax + sc.e * dty0[q];
+    } else {
+      y = x[q] + sc.a * ax;
+    }
+    out[q] = y;
+    if (k == 2) out[q + (int64_t)(m.npm - 2) * m.ldt] = y;
+    if (k == m.npm - 1) out[q - (int64_t)(m.npm - 2) * m.ldt] = y;
+  }
+  if (MODE == MODE_AX && absmax_bits) {
+    // max |Af| over |f| > fmin (src/hipft.f90:5097-5102): non-negative
+    // doubles order like their bit patterns.
+    double v = (active && fabs(x[q]) > 1e-14) ? fabs(ax) : 0.0;
+    unsigned long long b = __double_as_longlong(v);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long t = __shfl_down_sync(0xffffffffu, b, o);
+      b = t > b ? t : b;
+    }
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(absmax_bits, b);
+  }
+}
+
+// PTL candidates at the argmax cells (src/hipft.f90:5108-5135).
+__global__ void k_ptl(Mesh m, const double *__restrict__ f, const double *__restrict__ af,
+                      const unsigned long long *absmax_bits, unsigned long long *ptl_bits) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  if (j < 2 || j > m.ntm - 1 || k > m.npm - 1) return;
+  const double fmin_v = 1e-14;
+  double axabsmax = __longlong_as_double(*absmax_bits);
+  int64_t q = fidx(m, j, k, i);
+  if (!(axabsmax == fabs(af[q]) && fabs(f[q]) > fmin_v)) return;
+  double best = 1.7976931348623157e308;
+  const int64_t nb[4] = {-1, 1, -(int64_t)m.ldt, (int64_t)m.ldt};
+#pragma unroll
+  for (int n = 0; n < 4; ++n) {
+    double du = f[q] - f[q + nb[n]];
+    double df = af[q] - af[q + nb[n]];
+    if (du * df < -fmin_v) best = fmin(-du / df, best);
+  }
+  if (best < 1.7976931348623157e308) atomicMin(ptl_bits, (unsigned long long)__double_as_longlong(best));
+}
+
+// Gershgorin bound, get_dtime_diffusion_euler (src/hipft.f90:5019-5025).
+__global__ void k_gershgorin(Mesh m, DiffCoef dc, unsigned long long *max_bits) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  double g = 0.0;
+  if (j <= m.ntm - 1 && k <= m.npm - 1) {
+    Coef5 c = coef5(m, dc, j, k, i);
+    g = 0.0;
+    g = g + fabs(c.c1);
+    g = g + fabs(c.c2);
+    g = g + fabs(c.c3);
+    g = g + fabs(c.c4);
+    g = g + fabs(c.c5);
+  }
+  unsigned long long b = __double_as_longlong(g);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long t = __shfl_down_sync(0xffffffffu, b, o);
+    b = t > b ? t : b;
+  }
+  if ((threadIdx.x & 31) == 0 && b) atomicMax(max_bits, b);
+}
+
+// ------------------------------------------------------------ advection
+// Velocities either as 1-D theta profiles per realization (analytic flows,
+// identical in every phi column) or as full 2-D arrays (attenuated or rotated
+// flows).  vt lives on theta faces (nt per column), vp on phi faces (np).
+struct Flow {
+  int flow2d;
+  // 1-D: [nr][nt+1] / [nr][ntm+1], 1-based inside each row
+  const double *vt1, *vp1, *at1, *ap1;
+  // 2-D: vt(nt,npm,nr), vp(ntm,np,nr), at/ap(ntm,npm,nr), all with theta
+  // stride ldv >= nt (np == npm, so one plane size serves all four)
+  const double *vt, *vp, *at, *ap;
+  int ldv;
+  int64_t vplane;  // ldv * npm
+  double upwind;
+};
+
+__device__ __forceinline__ double vt_at(const Mesh &m, const Flow &fl, int j, int k, int i) {
+  if (fl.flow2d) return fl.vt[(int64_t)(i - 1) * fl.vplane + (int64_t)(k - 1) * fl.ldv + (j - 1)];
+  return fl.vt1[(int64_t)(i - 1) * (m.nt + 1) + j];
+}
+__device__ __forceinline__ double vp_at(const Mesh &m, const Flow &fl, int j, int k, int i) {
+  if (fl.flow2d) return fl.vp[(int64_t)(i - 1) * fl.vplane + (int64_t)(k - 1) * fl.ldv + (j - 1)];
+  return fl.vp1[(int64_t)(i - 1) * (m.ntm + 1) + j];
+}
+__device__ __forceinline__ double at_at(const Mesh &m, const Flow &fl, int j, int k, int i) {
+  if (fl.flow2d) return fl.at[(int64_t)(i - 1) * fl.vplane + (int64_t)(k - 1) * fl.ldv + (j - 1)];
+  return fl.at1[(int64_t)(i - 1) * (m.ntm + 1) + j];
+}
+__device__ __forceinline__ double ap_at(const Mesh &m, const Flow &fl, int j, int k, int i) {
+  if (fl.flow2d) return fl.ap[(int64_t)(i - 1) * fl.vplane + (int64_t)(k - 1) * fl.ldv + (j - 1)];
+  return fl.ap1[(int64_t)(i - 1) * (m.ntm + 1) + j];
+}
+
+// 1-D WENO weights (load_weno, src/hipft.f90:6905-6932), 1-based.
+struct Weno {
+  const double *cpt, *mct, *mt, *cptt, *pt, *mctt, *epst;  // theta: D_C_CPt, D_C_MCt, D_M_Tt, D_CP_Tt, D_P_Tt, D_MC_Tt, eps
+  const double *cpp, *mcp, *mp, *cptp, *pp, *mctp, *epsp;  // phi
+};
+
+// WENO3 face flux (src/hipft.f90:7775-7801).  LN*: LN(j-2), LN(j-1), LN(j);
+// LP*: LP(j-1), LP(j), LP(j+1); weights at indices j-1 (m1) and j (0).
+__device__ __forceinline__ double weno_face(double LNm2, double LNm1, double LN0, double LPm1, double LP0,
+                                            double LPp1, double DCMC_m1, double DCMC_0, double DCCP_m1,
+                                            double DCCP_0, double DPT_m1, double DMCT_m1, double DMT_0,
+                                            double DCPT_0, double eps_m1, double eps_0) {
+  double p0m = (kOne + DCMC_m1) * LNm1 - DCMC_m1 * LNm2;
+  double p1m = DCMC_0 * LNm1 + DCCP_m1 * LN0;
+  double p0p = (kOne + DCCP_0) * LP0 - DCCP_0 * LPp1;
+  double p1p = DCCP_m1 * LP0 + DCMC_0 * LPm1;
+  double t0 = DCMC_m1 * (LNm1 - LNm2), t1 = DCCP_m1 * (LN0 - LNm1);
+  double t2 = DCCP_0 * (LPp1 - LP0), t3 = DCMC_0 * (LP0 - LPm1);
+  double B0m = kFour * (t0 * t0), B1m = kFour * (t1 * t1);
+  double B0p = kFour * (t2 * t2), B1p = kFour * (t3 * t3);
+  double e0 = eps_m1 + B0m, e1 = eps_m1 + B1m, e2 = eps_0 + B0p, e3 = eps_0 + B1p;
+  double w0m = DPT_m1 / (e0 * e0);
+  double w1m = DMCT_m1 / (e1 * e1);
+  double w0p = DMT_0 / (e2 * e2);
+  double w1p = DCPT_0 / (e3 * e3);
+  double wm_sum = w0m + w1m, wp_sum = w0p + w1p;
+  double OM0m = w0m / wm_sum, OM1m = w1m / wm_sum;
+  double OM0p = w0p / wp_sum, OM1p = w1p / wp_sum;
+  double um = OM0m * p0m + OM1m * p1m;
+  double up = OM0p * p0p + OM1p * p1p;
+  return up + um;
+}
+
+// First-order upwind face flux (src/hipft.f90:7649-7651, 7809-7815).
+__device__ __forceinline__ double upwind_flux(double v, double upw, double xhi, double xlo) {
+  double cct = copysign(upw, v);
+  return v * kHalf * ((kOne - cct) * xhi + (kOne + cct) * xlo);
+}
+
+// Pole ring sums of the advection operator (src/hipft.f90:7902-7915): theta
+// fluxes through faces 2 and nt-1 (upwind in both operators).
+__global__ void k_ring_advection(Mesh m, Flow fl, const double *__restrict__ x, double *__restrict__ ring) {
+  __shared__ double sh[64];
+  const int i = blockIdx.x + 1;
+  double fn = 0.0, fs = 0.0;
+  for (int k = 2 + threadIdx.x; k <= m.npm - 1; k += blockDim.x) {
+    double ftn = upwind_flux(vt_at(m, fl, 2, k, i), fl.upwind, x[fidx(m, 2, k, i)], x[fidx(m, 1, k, i)]);
+    double fts = upwind_flux(vt_at(m, fl, m.nt - 1, k, i), fl.upwind, x[fidx(m, m.ntm, k, i)],
+                             x[fidx(m, m.ntm - 1, k, i)]);
+    fn = fn + ftn * m.dp[k];
+    fs = fs + fts * m.dp[k];
+  }
+  block_sum2(fn, fs, sh);
+  if (threadIdx.x == 0) {
+    ring[2 * (i - 1)] = fn;
+    ring[2 * (i - 1) + 1] = fs;
+  }
+}
+
+// Stage combine of the explicit integrators (src/hipft.f90:7440-7578):
+//   mode 0: out = x - C*aop
+//   mode 1: out = A*f0 + B*x - C*aop
+struct AdvCombine {
+  int mode;
+  double A, B, C;
+};
+
+// Phi cell index with the reference's periodic pad (LP(j,0) = LP(j,npm-2),
+// LP(j,npm) = LP(j,2), src/hipft.f90:7840-7845).
+__device__ __forceinline__ int wrap_cell(const Mesh &m, int c) {
+  if (c < 1) return c + (m.npm - 2);
+  if (c > m.npm - 1) return c - (m.npm - 2);
+  return c;
+}
+
+// Tile of TJ x TK cells; block is TJ x TK threads.
+template <int TJ, int TK>
+struct AdvSmem {
+  double x[TJ + 4][TK + 4];  // rows j0-2..j0+TJ+1, cols k0-2..k0+TK+1
+  double ft[TJ + 1][TK];     // theta faces j0..j0+TJ
+  double fp[TJ][TK + 1];     // phi faces k0..k0+TK
+};
+
+// One explicit advection stage over a tile: face fluxes (WENO3 or upwind),
+// divergence (src/hipft.f90:7890-7898), pole rows from the ring sums, seam,
+// and the integrator's combine.
+template <int TJ, int TK, bool WENO>
+__global__ void __launch_bounds__(TJ *TK) k_advection_stage(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
+                                                            const double *__restrict__ f0, double *out,
+                                                            const double *__restrict__ ring, double bcn, double bcs,
+                                                            AdvCombine cb) {
+  __shared__ AdvSmem<TJ, TK> s;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + ty * TJ;
+  const int j0 = blockIdx.x * TJ + 1;
+  const int k0 = blockIdx.y * TK + 2;
+  const int i = blockIdx.z + 1;
+  const int ntm = m.ntm, npm = m.npm;
+
+  // x tile with halo 2 (theta clipped to 1..ntm, phi wrapped periodically).
+  for (int e = tid; e < (TJ + 4) * (TK + 4); e += TJ * TK) {
+    int a = e % (TJ + 4), b = e / (TJ + 4);
+    int j = j0 - 2 + a, k = wrap_cell(m, k0 - 2 + b);
+    double v = 0.0;
+    if (j >= 1 && j <= ntm) v = x[fidx(m, j, k, i)];
+    s.x[a][b] = v;
+  }
+  __syncthreads();
+
+  // theta faces j = j0 .. j0+TJ for columns k0..k0+TK-1
+  for (int e = tid; e < (TJ + 1) * TK; e += TJ * TK) {
+    int a = e % (TJ + 1), b = e / (TJ + 1);
+    int jf = j0 + a, k = k0 + b;
+    double F = 0.0;
+    if (k <= npm - 1 && jf >= 2 && jf <= ntm) {
+      double xa = s.x[a + 2][b + 2], xb = s.x[a + 1][b + 2];  // x(jf), x(jf-1)
+      if (!WENO || jf == 2 || jf == ntm) {
+        F = upwind_flux(vt_at(m, fl, jf, k, i), fl.upwind, xa, xb);
+      } else {
+        // LP(c) = half*x(c)*(vt(c+1)-alpha_t(c)), LN(c) = half*x(c)*(vt(c)+alpha_t(c))
+        double LN[3], LP[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          int c = jf - 2 + d;  // LN at jf-2, jf-1, jf
+          double xc = s.x[a + d][b + 2];
+          LN[d] = kHalf * xc * (vt_at(m, fl, c, k, i) + at_at(m, fl, c, k, i));
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          int c = jf - 1 + d;  // LP at jf-1, jf, jf+1
+          double xc = s.x[a + 1 + d][b + 2];
+          LP[d] = kHalf * xc * (vt_at(m, fl, c + 1, k, i) - at_at(m, fl, c, k, i));
+        }
+        F = weno_face(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mct[jf - 1], wn.mct[jf], wn.cpt[jf - 1],
+                      wn.cpt[jf], wn.pt[jf - 1], wn.mctt[jf - 1], wn.mt[jf], wn.cptt[jf], wn.epst[jf - 1],
+                      wn.epst[jf]);
+      }
+    }
+    s.ft[a][b] = F;
+  }
+
+  // phi faces k = k0 .. k0+TK for rows j0..j0+TJ-1 (interior rows only).
+  // Face npm is the seam copy of face 2 (src/hipft.f90:7882): its stencil
+  // cells are the seam copies of face 2's cells, and it takes face 2's
+  // weights (index kw).
+  for (int e = tid; e < TJ * (TK + 1); e += TJ * TK) {
+    int a = e % TJ, b = e / TJ;
+    int j = j0 + a;
+    int kf = k0 + b;
+    double F = 0.0;
+    if (j >= 2 && j <= ntm - 1 && kf <= npm) {
+      int kw = (kf == npm) ? 2 : kf;
+      int bb = b + 2;  // smem column of cell kf
+      if (!WENO) {
+        F = upwind_flux(vp_at(m, fl, j, kw, i), fl.upwind, s.x[a + 2][bb], s.x[a + 2][bb - 1]);
+      } else {
+        double LN[3], LP[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          int c = wrap_cell(m, kf - 2 + d);
+          double xc = s.x[a + 2][bb - 2 + d];
+          LN[d] = kHalf * xc * (vp_at(m, fl, j, c, i) + ap_at(m, fl, j, c, i));
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          int c = wrap_cell(m, kf - 1 + d);
+          double xc = s.x[a + 2][bb - 1 + d];
+          LP[d] = kHalf * xc * (vp_at(m, fl, j, c + 1, i) - ap_at(m, fl, j, c, i));
+        }
+        F = weno_face(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mcp[kw - 1], wn.mcp[kw], wn.cpp[kw - 1],
+                      wn.cpp[kw], wn.pp[kw - 1], wn.mctp[kw - 1], wn.mp[kw], wn.cptp[kw], wn.epsp[kw - 1],
+                      wn.epsp[kw]);
+      }
+    }
+    s.fp[a][b] = F;
+  }
+  __syncthreads();
+
+  const int j = j0 + tx, k = k0 + ty;
+  if (j > ntm || k > npm - 1) return;
+  double aop;
+  if (j == 1) {
+    aop = ring[2 * (i - 1)] * bcn;
+  } else if (j == ntm) {
+    aop = -ring[2 * (i - 1) + 1] * bcs;
+  } else {
+    aop = ((m.sth[j + 1] * s.ft[tx + 1][ty] - m.sth[j] * s.ft[tx][ty]) * m.st_i[j] * m.dt_i[j] +
+           (s.fp[tx][ty + 1] - s.fp[tx][ty]) * m.st_i[j] * m.dp_i[k]);
+  }
+  int64_t q = fidx(m, j, k, i);
+  double xv = s.x[tx + 2][ty + 2];
+  double y;
+  if (cb.mode == 0) {
+    y = xv - cb.C * aop;
+  } else {
+    y = cb.A * f0[q] + cb.B * xv - cb.C * aop;
+  }
+  out[q] = y;
+  if (k == 2) out[q + (int64_t)(npm - 2) * m.ldt] = y;
+  if (k == npm - 1) out[q - (int64_t)(npm - 2) * m.ldt] = y;
+}
+
+// CFL limit, get_flow_dtmax (src/hipft.f90:7321-7327): min over interior
+// cells of half/max(kdotv, tiny); positive doubles order like their bits.
+__global__ void k_flow_dtmax(Mesh m, Flow fl, unsigned long long *min_bits) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  double dtv = 1.7976931348623157e308;
+  if (j <= m.ntm - 1 && k <= m.npm - 1) {
+    double kdotv = fmax(fabs(vt_at(m, fl, j, k, i)), fabs(vt_at(m, fl, j + 1, k, i))) * m.dt_i[j] +
+                   fmax(fabs(vp_at(m, fl, j, k, i)), fabs(vp_at(m, fl, j, k + 1, i))) * m.st_i[j] * m.dp_i[k];
+    dtv = kHalf / fmax(kdotv, 2.2250738585072014e-308);
+  }
+  unsigned long long b = __double_as_longlong(dtv);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long t = __shfl_down_sync(0xffffffffu, b, o);
+    b = t < b ? t : b;
+  }
+  if ((threadIdx.x & 31) == 0) atomicMin(min_bits, b);
+}
+
+// 2-D flow build (update_flow, src/hipft.f90:3393-3519): theta/phi profiles
+// from the analytic models (1-D, computed on the host), the rotated rigid
+// rotation, and Br attenuation.  One thread per (j,k,i) of the larger of
+// the vt (nt x npm) and vp (ntm x np) grids.
+struct Flow2DBuild {
+  const double *vt1, *vp1;  // analytic 1-D parts, [nr][nt+1], [nr][ntm+1]
+  const double *cth, *sth, *ct, *st;  // 1-based
+  const double *cosp, *sinp, *cosph;  // cos(p(k)), sin(p(k)), cos(ph(k)), 1-based
+  double vrigid;      // flow_rigid_omega * km_s_to_rs_hr (0: off)
+  int attenuate;
+  const double *atten_i;  // [nr+1]
+};
+
+__device__ __forceinline__ double sgn1(double b) { return copysign(1.0, b); }
+
+__global__ void k_flow_build(Mesh m, Flow2DBuild b, int ldv, const double *__restrict__ f, double *vt,
+                             double *vp) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int i = blockIdx.z + 1;
+  const int64_t base = ((int64_t)(i - 1) * m.npm + (k - 1)) * ldv + (j - 1);
+  if (j <= m.nt && k <= m.npm) {
+    double v = b.vt1[(int64_t)(i - 1) * (m.nt + 1) + j];
+    if (b.vrigid != 0.0) {
+      double cp = b.cosp[k], c = b.cth[j], sv = b.sth[j];
+      double acp = fabs(cp);
+      double p1 = -2 * c * fabs(sv * cp);
+      double p2 = (cp * c * c - cp) * acp * acp * acp;
+      double p3 = (-3 * cp * c * c + 2 * cp) * acp;
+      double p4 = sgn1(cp) * c * c;
+      double p5 = 2 * acp * acp * acp * c * fabs(sv);
+      double p6 = (-cp * cp * cp * cp + 3 * cp * cp - 1) * c * c;
+      double p7 = (-2 * cp * cp * cp * sv + 2 * sv * cp) * c;
+      double p8 = cp * cp * cp * cp - 2 * cp * cp + 1;
+      double p9 = fabs(sv * cp) * b.sinp[k] * b.vrigid;
+      double p10 = (cp * cp * cp * cp - 3 * cp * cp + 1) * c * c;
+      double p11 = (2 * cp * cp * cp * sv - 2 * sv * cp) * c;
+      double p12 = cp * cp * cp * cp + 2 * cp * cp;
+      v = v + (-((p1 + (p2 + p3 + p4) * sgn1(sv) + p5 + p6 + p7 + p8) * p9) / sqrt(p10 + p11 - p12));
+      if (fabs(v) > 1.0e5 || fabs(v) < -1.0e-5) v = 0;
+    }
+    if (b.attenuate && k >= 2 && k <= m.npm - 1 && j >= 2 && j <= m.nt - 1) {
+      double ba = fmax(fabs(f[fidx(m, j - 1, k, i)]), fabs(f[fidx(m, j, k, i)]));
+      v = v * (kOne - tanh(ba * b.atten_i[i]));
+    }
+    vt[base] = v;
+  }
+  if (j <= m.ntm && k <= m.np) {
+    double v = b.vp1[(int64_t)(i - 1) * (m.ntm + 1) + j];
+    if (b.vrigid != 0.0) {
+      double cph = b.cosph[k], c = b.ct[j], sv = b.st[j];
+      double p1 = b.vrigid * (cph * cph * c + sv * cph - c) * sgn1(cph) * fabs(sv);
+      double p2 = (cph * cph * cph * cph - 3 * cph * cph + 1) * c * c;
+      double p3 = (2 * cph * cph * cph * sv - 2 * sv * cph) * c;
+      double p4 = cph * cph * cph * cph + 2 * cph * cph;
+      v = v - p1 / sqrt(p2 + p3 - p4);
+      if (fabs(v) > 1.0e5 || fabs(v) < -1.0e-5) v = 0;
+    }
+    if (b.attenuate && k >= 2 && k <= m.np - 1) {
+      double ba = fmax(fabs(f[fidx(m, j, k - 1, i)]), fabs(f[fidx(m, j, k, i)]));
+      v = v * (kOne - tanh(ba * b.atten_i[i]));
+    }
+    vp[base] = v;
+  }
+}
+
+// Periodic seam of a (n1 rows) x npm x nr array with stride ldt
+// (set_periodic_bc_3d, src/hipft.f90:4920-4923).
+__global__ void k_seam(Mesh m, int n1, int ld, double *a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int i = blockIdx.y + 1;
+  if (j > n1) return;
+  int64_t b = (int64_t)(i - 1) * m.npm * ld + (j - 1);
+  a[b] = a[b + (int64_t)(m.npm - 2) * ld];
+  a[b + (int64_t)(m.npm - 1) * ld] = a[b + (int64_t)ld];
+}
+
+// Local Lax-Friedrichs alpha from 2-D velocities (set_lf_alpha,
+// src/hipft.f90:6968-7046).
+__global__ void k_lf_alpha(Mesh m, int ldv, const double *__restrict__ vt, const double *__restrict__ vp,
+                           double *at, double *ap) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int i = blockIdx.z + 1;
+  const int nt = m.nt, np = m.np;
+  if (j > m.ntm || k > m.npm) return;
+  const int64_t col = ((int64_t)(i - 1) * m.npm + (k - 1)) * ldv;
+  auto VT = [&](int jj) { return fabs(vt[col + (jj - 1)]); };
+  double a;
+  if (j >= 3 && j <= nt - 3)
+    a = fmax(fmax(fmax(fmax(fmax(VT(j - 2), VT(j - 1)), VT(j)), VT(j + 1)), VT(j + 2)), VT(j + 3));
+  else if (j == 1)
+    a = fmax(fmax(fmax(VT(j), VT(j + 1)), VT(j + 2)), VT(j + 3));
+  else if (j == 2)
+    a = fmax(fmax(fmax(fmax(VT(j - 1), VT(j)), VT(j + 1)), VT(j + 2)), VT(j + 3));
+  else if (j == nt - 2)
+    a = fmax(fmax(fmax(fmax(VT(j - 2), VT(j - 1)), VT(j)), VT(j + 1)), VT(j + 2));
+  else
+    a = fmax(fmax(fmax(VT(j - 2), VT(j - 1)), VT(j)), VT(j + 1));
+  at[col + (j - 1)] = a;
+  // alpha_p on interior rows and columns 2..np-1; columns 1 and npm by seam.
+  double b = 0.0;
+  if (j >= 2 && j <= m.ntm - 1) {
+    const int64_t rb = (int64_t)(i - 1) * m.npm * ldv + (j - 1);
+    auto VP = [&](int kk) { return fabs(vp[rb + (int64_t)(kk - 1) * ldv]); };
+    int kk = k;
+    if (kk == 1) kk = np - 1;
+    if (kk == np) kk = 2;
+    if (kk >= 3 && kk <= np - 3)
+      b = fmax(fmax(fmax(fmax(fmax(VP(kk - 2), VP(kk - 1)), VP(kk)), VP(kk + 1)), VP(kk + 2)), VP(kk + 3));
+    else if (kk == 2)
+      b = fmax(fmax(fmax(fmax(fmax(VP(np - 2), VP(kk - 1)), VP(kk)), VP(kk + 1)), VP(kk + 2)), VP(kk + 3));
+    else if (kk == np - 2)
+      b = fmax(fmax(fmax(fmax(fmax(VP(kk - 2), VP(kk - 1)), VP(kk)), VP(kk + 1)), VP(kk + 2)), VP(3));
+    else
+      b = fmax(fmax(fmax(fmax(fmax(VP(kk - 2), VP(kk - 1)), VP(kk)), VP(kk + 1)), VP(3)), VP(4));
+  }
+  ap[col + (j - 1)] = b;
+}
+
+// ------------------------------------------------------------- analysis
+// Per-realization diagnostics of analysis_step (src/hipft.f90:3183-3325).
+// Stage 1: each block reduces a slab of phi columns into 15 partials
+// (min, max, min|.|, verr, sumfval2, fluxp, fluxm, fluxp_pn, fluxm_pn,
+// fluxp_ps, fluxm_ps, area_pn, area_ps, eqd1, eqd2, axd -> 16 slots).
+constexpr int kNPart = 16;
+
+struct AnalysisArgs {
+  const double *da_t, *sn_t, *cs_t;        // [ntm+1], 1-based
+  const double *da_p, *cs_p, *sn_p;        // [npm+1], 1-based
+  const unsigned char *pn, *ps;            // [ntm+1] polar-cap masks
+  int vmode;                               // validation mode 0/1/2
+  const double *fval_u0;                   // PT (npm1, ntm, nr)
+  const double *vscale;                    // [nr+1] mode-1 decay factors
+  const double *t, *p, *st_i;              // 1-based, mode 2
+  double vtt, vpt, width, p1, p2;
+};
+
+__device__ __forceinline__ double fval_at(const Mesh &m, const AnalysisArgs &a, int jphi, int jth, int i) {
+  if (a.vmode == 1) {
+    int npm1 = m.npm - 1;
+    return a.fval_u0[((int64_t)(i - 1) * m.ntm + (jth - 1)) * npm1 + (jphi - 1)] * a.vscale[i];
+  }
+  // mode 2: two Gaussians (src/hipft.f90:3162-3174)
+  double tt = a.t[jth] - 0.7853981633974483 - a.vtt;
+  double b1 = a.p[jphi] - a.p1, b2 = a.p[jphi] - a.p2;
+  return -a.st_i[jth] * exp(-(tt * tt) / a.width - (b1 * b1) / a.width) +
+         a.st_i[jth] * exp(-(tt * tt) / a.width - (b2 * b2) / a.width);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_analysis_partial(Mesh m, AnalysisArgs a, const double *__restrict__ f,
+                                                         double *part, int cols_per_block) {
+  __shared__ double sh[kNPart][NT / 32];
+  const int i = blockIdx.y + 1;
+  const int kb = blockIdx.x * cols_per_block + 1;
+  const int ke = min(kb + cols_per_block - 1, m.npm - 1);
+  double v[kNPart];
+  v[0] = 1.7976931348623157e308;  // min
+  v[1] = 2.2250738585072014e-308; // max starts at tiny (small_value)
+  v[2] = 1.7976931348623157e308;  // min |f|
+#pragma unroll
+  for (int q = 3; q < kNPart; ++q) v[q] = 0.0;
+  const int ncell = (ke - kb + 1) * m.ntm;
+  for (int e = threadIdx.x; e < ncell; e += NT) {
+    int k = kb + e / m.ntm, j = 1 + e % m.ntm;
+    double fj = f[fidx(m, j, k, i)];
+    if (k <= m.npm - 2) {
+      v[0] = fmin(fj, v[0]);
+      v[1] = fmax(fj, v[1]);
+      v[2] = fmin(fabs(fj), v[2]);
+      double fv = 0.0, fval;
+      if (a.vmode == 0) {
+        fval = fj;
+      } else {
+        fval = fval_at(m, a, k, j, i);
+      }
+      double d = fj - fval;
+      v[3] = v[3] + d * d;
+      v[4] = v[4] + fabs(fj) * fabs(fval);
+      (void)fv;
+    }
+    double dat = a.da_t[j], dap = a.da_p[k];
+    double fv = fj * dat * dap;
+    if (fv > 0.) v[5] = v[5] + fv; else v[6] = v[6] + fv;
+    if (a.pn[j]) {
+      if (fv > 0.) v[7] = v[7] + fv; else v[8] = v[8] + fv;
+      v[11] = v[11] + dat * dap;
+    }
+    if (a.ps[j]) {
+      if (fv > 0.) v[9] = v[9] + fv; else v[10] = v[10] + fv;
+      v[12] = v[12] + dat * dap;
+    }
+    v[13] = v[13] + fj * a.sn_t[j] * a.cs_p[k] * dat * dap;
+    v[14] = v[14] + fj * a.sn_t[j] * a.sn_p[k] * dat * dap;
+    v[15] = v[15] + fj * a.cs_t[j] * dat * dap;
+  }
+  const int l = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < kNPart; ++q) {
+    double x = v[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double y = __shfl_down_sync(0xffffffffu, x, o);
+      if (q == 0 || q == 2) x = fmin(x, y);
+      else if (q == 1) x = fmax(x, y);
+      else x = x + y;
+    }
+    if (l == 0) sh[q][w] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNPart) {
+    int q = threadIdx.x;
+    double x = sh[q][0];
+    for (int ww = 1; ww < NT / 32; ++ww) {
+      double y = sh[q][ww];
+      if (q == 0 || q == 2) x = fmin(x, y);
+      else if (q == 1) x = fmax(x, y);
+      else x = x + y;
+    }
+    part[((int64_t)(i - 1) * gridDim.x + blockIdx.x) * kNPart + q] = x;
+  }
+}
+
+// Stage 2: one thread per (realization, slot) reduces the block partials in
+// block order (deterministic).
+__global__ void k_analysis_final(int nblocks, int nr, const double *__restrict__ part, double *out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nr * kNPart) return;
+  const int i = t / kNPart, q = t % kNPart;
+  double x = part[((int64_t)i * nblocks) * kNPart + q];
+  for (int b = 1; b < nblocks; ++b) {
+    double y = part[((int64_t)i * nblocks + b) * kNPart + q];
+    if (q == 0 || q == 2) x = fmin(x, y);
+    else if (q == 1) x = fmax(x, y);
+    else x = x + y;
+  }
+  out[(int64_t)i * kNPart + q] = x;
+}
+
+// -------------------------------------------------------- assimilation
+// Increment of assimilate_new_data (src/hipft.f90:4111-4120) with the mu
+// weights, latitude caps and scaling of apply_data_assimilation
+// (4242-4271).  The PT map (phi fastest) is read through a 32x32 shared
+// tile so both the map and the field are accessed coalesced.
+struct DAArgs {
+  const double *data;   // (npm1, ntm, 3) PT
+  const double *mu_power, *mu_limit, *lat_limit;  // [nr+1]
+  const int *tidx0, *tidx1;                        // [nr+1]
+  int add, custom_from_mu;
+  double mult_fac;
+};
+
+__global__ void k_da_delta(Mesh m, DAArgs a, const double *__restrict__ f, double *delta) {
+  __shared__ double sd[32][33], sw[32][33];
+  const int npm1 = m.npm - 1;
+  const int i = blockIdx.z + 1;
+  const int j0 = blockIdx.x * 32 + 1;   // theta tile start
+  const int k0 = blockIdx.y * 32 + 1;   // phi tile start
+  const int64_t slice = (int64_t)npm1 * m.ntm;
+  // load: thread (tx,ty) reads phi = k0+tx, theta = j0+ty+8r
+  for (int r = 0; r < 4; ++r) {
+    int jt = j0 + threadIdx.y + 8 * r, kp = k0 + threadIdx.x;
+    double d = 0.0, w = 0.0;
+    if (jt <= m.ntm && kp <= npm1) {
+      int64_t q = (int64_t)(jt - 1) * npm1 + (kp - 1);
+      d = a.data[q];
+      if (a.custom_from_mu) {
+        double mu = a.data[2 * slice + q];
+        w = (mu > a.mu_limit[i]) ? pow(mu, a.mu_power[i]) : 0.0;
+      } else {
+        w = a.data[slice + q];
+      }
+      if (a.lat_limit[i] > 0 && (jt <= a.tidx0[i] || jt >= a.tidx1[i])) w = 0.0;
+      d = a.mult_fac * d;
+    }
+    sd[threadIdx.y + 8 * r][threadIdx.x] = d;
+    sw[threadIdx.y + 8 * r][threadIdx.x] = w;
+  }
+  __syncthreads();
+  // compute: thread (tx,ty) handles theta = j0+tx, phi = k0+ty+8r
+  for (int r = 0; r < 4; ++r) {
+    int jt = j0 + threadIdx.x, kp = k0 + threadIdx.y + 8 * r;
+    if (jt > m.ntm || kp > npm1) continue;
+    double d = sd[threadIdx.x][threadIdx.y + 8 * r], w = sw[threadIdx.x][threadIdx.y + 8 * r];
+    int64_t q = fidx(m, jt, kp, i);
+    double dv = a.add ? w * d : w * (d - f[q]);
+    delta[q] = dv;
+  }
+}
+
+// f += delta (src/hipft.f90:4138-4141) over every point including the seam,
+// with the delta's seam taken first (4121) -- both done by reading the seam
+// source columns directly; an optional per-realization scale implements
+// balance_flux of the increment (8794-8801).
+__global__ void k_da_apply(Mesh m, const double *__restrict__ delta, double *f, const double *ratio) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm) return;
+  int ks = k;
+  if (k == 1) ks = m.npm - 1;
+  if (k == m.npm) ks = 2;
+  double d = delta[fidx(m, j, ks, i)];
+  if (ratio) {
+    double r = ratio[i];
+    d = (d > 0) ? d / r : d * r;
+  }
+  int64_t q = fidx(m, j, k, i);
+  f[q] = f[q] + d;
+}
+
+// get_flux (src/hipft.f90:8706-8738) partial sums per block; the host
+// finishes the per-realization sums in block order.
+__global__ void k_flux_partial(Mesh m, const double *__restrict__ da_t, const double *__restrict__ da_p,
+                               const double *__restrict__ a, int seam_src, double *part, int cols_per_block) {
+  __shared__ double sh[64];
+  const int i = blockIdx.y + 1;
+  const int kb = blockIdx.x * cols_per_block + 1;
+  const int ke = min(kb + cols_per_block - 1, m.npm - 1);
+  double fp = 0.0, fm = 0.0;
+  const int ncell = (ke - kb + 1) * m.ntm;
+  for (int e = threadIdx.x; e < ncell; e += blockDim.x) {
+    int k = kb + e / m.ntm, j = 1 + e % m.ntm;
+    int ks = k;
+    if (seam_src && k == 1) ks = m.npm - 1;
+    double fv = a[fidx(m, j, ks, i)] * da_t[j] * da_p[k];
+    if (fv > 0.0) fp = fp + fv; else fm = fm + fv;
+  }
+  block_sum2(fp, fm, sh);
+  if (threadIdx.x == 0) {
+    part[((int64_t)(i - 1) * gridDim.x + blockIdx.x) * 2] = fp;
+    part[((int64_t)(i - 1) * gridDim.x + blockIdx.x) * 2 + 1] = fm;
+  }
+}
+
+// Multiplicative balance (src/hipft.f90:8794-8801) of the whole array.
+__global__ void k_scale_balance(Mesh m, double *a, const double *ratio) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm) return;
+  double r = ratio[i];
+  int64_t q = fidx(m, j, k, i);
+  double br = a[q];
+  a[q] = (br > 0) ? br / r : br * r;
+}
+
+}  // namespace hipft

@@ -1,0 +1,232 @@
+/*
+ * hipft_gpu.h -- C ABI of the B200 (sm_100a) flux-transport library.
+ *
+ * Drop-in for the hot-path subroutines of HipFT (src/hipft.f90, v1.19.3).
+ * HipFT keeps its solver state in Fortran module arrays; this library keeps
+ * the same state on the GPU behind an opaque handle.  Every entry point takes
+ * plain host pointers and sizes, copies what it needs, and returns an int
+ * status (HIPFT_OK = 0).  Host buffers are only borrowed for the duration of
+ * a call.  A handle is used from one host thread (the reference runs
+ * MPI_THREAD_FUNNELED, src/hipft.f90:1090).
+ *
+ * Field layout at the ABI is the reference's: f(ntm, npm, nr) in Fortran
+ * column-major order, theta fastest, with the two-point periodic overlap in
+ * phi (npm = npm1 + 1; column 1 == column npm-1, column npm == column 2),
+ * src/hipft.f90:2114-2126.  Data-assimilation maps are the reference's
+ * (npm1, ntm, 3) phi-fastest slices [data, weight, mu], src/hipft.f90:4234.
+ *
+ * Each declaration cites the reference routine it replaces.
+ */
+#ifndef HIPFT_GPU_H
+#define HIPFT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference prints and calls endrun(.true.)
+ * (src/hipft.f90:970-1004); a Fortran shim maps a nonzero status to that. */
+enum {
+  HIPFT_OK = 0,
+  HIPFT_EINVAL = 1,   /* bad argument or size                              */
+  HIPFT_ECUDA = 2,    /* CUDA runtime error (message in hipft_gpu_last_error) */
+  HIPFT_ETIMEOUT = 3, /* a bounded device wait gave up                     */
+  HIPFT_ENAN = 4,     /* non-finite value detected                          */
+  HIPFT_ESTATE = 5,   /* call out of order (e.g. step before set_field)     */
+  HIPFT_EIO = 6,      /* file could not be read/written                     */
+  HIPFT_ENOMEM = 7    /* device allocation failed                           */
+};
+
+typedef struct hipft_gpu hipft_gpu;
+
+/* Mesh and realization count.  Replaces set_mesh's inputs
+ * (src/hipft.f90:6495-6653): t(ntm1) and p(npm1) are the map scales. */
+typedef struct {
+  int ntm;          /* theta points including both poles                    */
+  int npm1;         /* phi points including 0 and 2*pi (one-point overlap)  */
+  int nr;           /* realizations held by this handle                     */
+  int device;       /* CUDA device ordinal                                  */
+  const double *t;  /* [ntm]  theta scale, t[0]=0, t[ntm-1]=pi              */
+  const double *p;  /* [npm1] phi scale,   p[0]=0, p[npm1-1]=2*pi           */
+} hipft_grid;
+
+/* Numerical-method switches with the reference's namelist names and
+ * meanings (src/hipft.f90:580-700, presets 8583-8608). */
+typedef struct {
+  int advance_flow;
+  int flow_num_method;        /* 1 FE+UW, 2 SSPRK33+UW, 3 SSPRK33+WENO3, 4 SSPRK43+WENO3 */
+  double upwind;              /* upwind coefficient (1 = full upwind)        */
+  double weno_eps;            /* <=0: epsilon = cell width                    */
+  int strang_splitting;       /* 1: A(dt/2) D(dt) A(dt/2), else A(dt) D(dt)   */
+  int advance_diffusion;
+  int diffusion_num_method;   /* 1 Euler, 2 RKL2, 3 RKG2                      */
+  int diffusion_subcycles;    /* 0 = automatic (PTL) subcycling               */
+  int diffusion_coef_grid;    /* add grid-based diffusion                      */
+  double diffusion_coef_factor; /* km^2/s -> Rs^2/hr by default               */
+  const double *diffusion_coef_constants; /* [nr], km^2/s                     */
+  double pole_flux_lat_limit; /* degrees, for the polar-flux diagnostics       */
+  int verbose;
+} hipft_params;
+
+/* Analytic / prescribed flow definition (update_flow, src/hipft.f90:3371-3523;
+ * add_flow_*_analytic 7219-7285).  Per-realization vectors have length nr
+ * and may be NULL when their model is off. */
+typedef struct {
+  int flow_dr_model;          /* 1: vp += st*(p0 + p2 ct^2 + p4 ct^4) [m/s]   */
+  int flow_mf_model;          /* 1: vt -= sth*(p1 c + p3 c^3 + p5 c^5) [m/s]  */
+  const double *dr_p0, *dr_p2, *dr_p4;
+  const double *mf_p1, *mf_p3, *mf_p5;
+  double flow_vp_rigid_omega; /* km/s, vp += omega*st                          */
+  double flow_vt_const;       /* km/s                                          */
+  double flow_rigid_omega;    /* km/s, rotated rigid rotation (2-D)            */
+  int flow_attenuate;         /* attenuate by tanh(|Br|/value) each step       */
+  const double *flow_attenuate_values; /* [nr], Gauss                          */
+} hipft_flow_def;
+
+/* Data-assimilation options (apply_data_assimilation, src/hipft.f90:4148-4306;
+ * assimilate_new_data 4083-4146). */
+typedef struct {
+  int add;                    /* assimilate_data_add: f += w*d instead of blend */
+  int custom_from_mu;         /* weight = mu^power where mu > limit, else 0    */
+  int balance_flux;           /* multiplicative balance of the increment       */
+  double mult_fac;            /* assimilate_data_mult_fac                      */
+  const double *mu_power;     /* [nr]                                          */
+  const double *mu_limit;     /* [nr]                                          */
+  const double *lat_limit;    /* [nr] degrees; <=0 disables the cap mask       */
+} hipft_da_opts;
+
+/* What one diffusion_step did (history columns, src/hipft.f90:2666-2670). */
+typedef struct {
+  double dtime_diffusion_euler; /* Gershgorin explicit-Euler limit            */
+  int64_t sts_s;                /* stages in the last super-step (or Euler cycles) */
+  int64_t subcycles;            /* diffusion cycles taken (or its diagnostic)  */
+  int64_t total_stages;         /* stage launches summed over the call         */
+} hipft_diffusion_info;
+
+/* Called after each diffusion cycle (the reference's verbose>1 per-cycle
+ * analysis + history output, src/hipft.f90:4659-4669).  time_stepped is the
+ * amount of the step covered so far; subcycle_diag is the
+ * CEILING((dt - time_stepped)/dt_cycle) diagnostic. */
+typedef void (*hipft_cycle_cb)(void *user, int cycle, double time_stepped, double dt_cycle,
+                               int64_t sts_s, int64_t subcycle_diag);
+
+/* ---- lifecycle ------------------------------------------------------- */
+
+/* setup's device part: set_mesh (6495), load_flows (2535) + load_weno (6846),
+ * load_diffusion (6655) + load_diffusion_matrix (4927) +
+ * get_dtime_diffusion_euler (4985).  Allocates all device memory. */
+int hipft_gpu_create(const hipft_grid *grid, const hipft_params *params, hipft_gpu **out);
+int hipft_gpu_destroy(hipft_gpu *h);
+/* Copies the last error message (NUL terminated). */
+int hipft_gpu_last_error(const hipft_gpu *h, char *buf, size_t len);
+/* Library version string and the device it was built for ("sm_100a"). */
+const char *hipft_gpu_version(void);
+
+/* ---- field I/O ---------------------------------------------------------- */
+
+/* f(ntm, npm, nr), theta fastest (replaces `!$omp target enter data
+ * map(to:f)`, src/hipft.f90:2159). */
+int hipft_gpu_set_field(hipft_gpu *h, const double *f);
+/* Copies f back (replaces `!$omp target update from`, src/hipft.f90:2844). */
+int hipft_gpu_get_field(hipft_gpu *h, double *f);
+/* Initial map in the file's PT layout (npm1, ntm, nr): transpose, periodic
+ * fix-up, m=0 poles, optional balance, multiply (src/hipft.f90:2116-2172). */
+int hipft_gpu_load_initial_map(hipft_gpu *h, const double *map_pt, int flux_balance,
+                               double mult_fac);
+
+/* ---- flows -------------------------------------------------------------- */
+
+/* Stores the flow definition; marks the flow for (re)building. */
+int hipft_gpu_set_flow(hipft_gpu *h, const hipft_flow_def *def);
+/* update_flow (src/hipft.f90:3371): rebuilds vt, vp (and the WENO LF alpha,
+ * set_lf_alpha 6940) when needed.  *updated = 1 when the flow changed, which
+ * tells the caller to recompute the CFL limit. */
+int hipft_gpu_update_flow(hipft_gpu *h, int *updated);
+/* get_flow_dtmax (src/hipft.f90:7287-7350): CFL limit over all cells and
+ * realizations, x2 for Strang splitting, x2 for SSPRK(4,3). */
+int hipft_gpu_flow_dtmax(hipft_gpu *h, double *dtmax);
+
+/* ---- the time step -------------------------------------------------------- */
+
+/* advection_step (src/hipft.f90:4509) with FE / SSPRK(3,3) / SSPRK(4,3)
+ * (7409-7582) over upwind or WENO3 operators (7615-7925). */
+int hipft_gpu_advection_step(hipft_gpu *h, double dt);
+/* diffusion_step (src/hipft.f90:4551): subcycling (fixed or PTL,
+ * get_dtime_diffusion_ptl 5042) of Euler / RKL2 / RKG2 (5163-5475) through
+ * diffusion_operator_cd (7927).  cb may be NULL. */
+int hipft_gpu_diffusion_step(hipft_gpu *h, double dt, hipft_cycle_cb cb, void *user,
+                             hipft_diffusion_info *info);
+/* flux_transport_step (src/hipft.f90:4463): Strang A(dt/2) D(dt) A(dt/2) or
+ * Lie A(dt) D(dt), as selected at create time. */
+int hipft_gpu_flux_transport_step(hipft_gpu *h, double dt, hipft_cycle_cb cb, void *user,
+                                  hipft_diffusion_info *info);
+
+/* ---- data assimilation --------------------------------------------------- */
+
+/* Blend one observed map into every realization: per-realization mu-power
+ * weights and latitude caps, mult factor, f += w*(d - f) (or w*d), seam,
+ * optional balance.  data3_pt: (npm1, ntm, 3) phi fastest. */
+int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *opts);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Validation modes of analysis_step (src/hipft.f90:3148-3175):
+ * mode 1: fval = fval_u0_pt * exp(-42 D factor (time - time_start));
+ *         fval_u0_pt is (npm1, ntm, nr) PT.
+ * mode 2: analytic Gaussian pair moved by vt_const / vp_omega (km/s). */
+int hipft_gpu_set_validation(hipft_gpu *h, int mode, const double *fval_u0_pt, double width,
+                             double vt_const, double vp_omega, double time_start);
+/* analysis_step (src/hipft.f90:3098-3336): hist is [nr][14] =
+ * BR_MIN, BR_MAX, BR_ABS_MIN, FLUX_POSITIVE, FLUX_NEGATIVE,
+ * NPOLE_FLUX_POSITIVE, NPOLE_FLUX_NEGATIVE, SPOLE_FLUX_POSITIVE,
+ * SPOLE_FLUX_NEGATIVE, NPOLE_AREA, SPOLE_AREA, EQ_DIPOLE, AX_DIPOLE,
+ * VALIDATION_ERR_HHabs. */
+int hipft_gpu_analysis(hipft_gpu *h, double time, double *hist);
+/* get_flux (src/hipft.f90:8672): flux_p[nr], flux_m[nr] of the field. */
+int hipft_gpu_get_flux(hipft_gpu *h, double *flux_p, double *flux_m);
+/* balance_flux (src/hipft.f90:8752) on every realization of the field. */
+int hipft_gpu_balance_flux(hipft_gpu *h);
+
+/* ---- introspection --------------------------------------------------------- */
+
+typedef struct {
+  int ntm, npm, nr, ldt;        /* ldt: padded theta stride on the device     */
+  double dtime_diffusion_euler;
+  int64_t sts_s;
+  int64_t kernel_launches;      /* launches of this library's kernels so far  */
+  int64_t cell_stage_updates;   /* unique cells x stages advanced so far      */
+  size_t device_bytes;          /* device memory held by the handle           */
+} hipft_info;
+int hipft_gpu_info(const hipft_gpu *h, hipft_info *info);
+/* Runs subsequent work on a caller-owned cudaStream_t (NULL: the handle's). */
+int hipft_gpu_set_stream(hipft_gpu *h, void *cuda_stream);
+int hipft_gpu_synchronize(hipft_gpu *h);
+
+/* ---- standalone driver ----------------------------------------------------- */
+
+/* Runs `program HIPFT` (src/hipft.f90:869-968) for the hot-path subset: reads
+ * the hipft.in namelist at `namelist_path`, resolves file names relative to
+ * `run_dir`, writes hipft_history_{num,sol}_rNNNNNN.out (formats of
+ * src/hipft.f90:1616-1646, 2633-2634) into `run_dir`. */
+int hipft_run(const char *namelist_path, const char *run_dir, int device);
+/* Same, and copies the final field f(ntm, npm, nr) into f_out when f_len
+ * equals ntm*npm*nr (the data of the reference's hipft_brmap_final.h5,
+ * wrap_it_up src/hipft.f90:1381-1412, before its PT transpose). */
+int hipft_run_field(const char *namelist_path, const char *run_dir, int device, double *f_out, size_t f_len);
+
+/* ---- map files ------------------------------------------------------------- */
+
+/* Minimal reader of the reference's HDF5 maps (rdh5, src/hipft.f90:5678):
+ * dataset "Data" plus scales "dim1".."dim3".  Sizes first (pass NULL
+ * buffers), then data.  dims are Fortran order (fastest first); unused
+ * dims are 1.  Data is converted to double. */
+int hipft_h5_read(const char *path, int *ndim, int64_t dims[3], double *data, double *s1,
+                  double *s2, double *s3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HIPFT_GPU_H */
