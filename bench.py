@@ -1,0 +1,344 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 Gcell-updates/s of HipFT's flux-transport step on B200.
+
+Workload (default "batched64_1024x2048"): 64 realizations on a 1024 x 2048
+(theta x phi) grid whose theta spacing is halved within 15 degrees of each
+pole; per-realization diffusion D log-U(100, 1000) km^2/s, meridional flow
+v0 U(10, 20) m/s and differential rotation B, C x U(0.9, 1.1) (seed 1);
+WENO3-CS(h) + SSPRK(4,3) advection Strang-split with RKG2 super-time-stepped
+diffusion (automatic PTL subcycling), assimilation of a synthetic observed
+map every 24 model hours (mu^4 weights, mu > 0.1), diagnostics every step.
+A step is one flux-transport time step at the CFL-limited dt over all
+realizations.  Unit of work: one unique grid point of one realization
+advanced through one stage (one RKG2 stage or one SSPRK stage).
+
+Timing: W untimed warm-up steps, then K steps between CUDA events on the
+library's stream (inputs resident in HBM; each field is 1.07 GB, far above
+the 126 MB L2, so no flush is needed), max over ranks.  `e2e` repeats K steps
+through the C ABI with the field copied host->device before and
+device->host after every step.  Multi-GPU: realizations are split across
+ranks (block split, low ranks take the remainder) and every rank advances its
+own share independently -- weak scaling, no data-path collective.
+
+`--impl reference` times the CPU oracle (the restatement of the reference's
+solver in oracle/, all host threads) on a bounded sample of the same
+workload: one realization, one flux-transport step per bench step.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 Gcell-updates/s"
+UNIT = "Gcell-updates/s"
+STS_BYTES_PER_CELL = 40  # RKG2 stage k>=2: read Y_{k-1}, Y_{k-2}, u0, dty0; write Y_k
+
+WORKLOADS = {
+    "batched64_1024x2048": dict(ntm=1024, npm1=2049, nr=64, seed=1),
+    "single_1024x2048": dict(ntm=1024, npm1=2049, nr=1, seed=0),
+    "batched8_1024x2048": dict(ntm=1024, npm1=2049, nr=8, seed=1),
+    "small_128x256": dict(ntm=128, npm1=257, nr=4, seed=1),
+}
+
+
+def split_realizations(nr: int, world: int, rank: int):
+    """Block split of realizations over ranks, remainder to the low ranks
+    (src/hipft.f90:1033-1050).  Returns (first index, count)."""
+    base, rem = divmod(nr, world)
+    cnt = base + (1 if rank < rem else 0)
+    first = rank * base + min(rank, rem)
+    return first, cnt
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.tmp.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.tmp.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(wl: dict):
+    from hipft_b200 import synthetic as S
+    t = S.refined_theta(wl["ntm"])
+    p = S.uniform_phi(wl["npm1"])
+    br = S.bipole_map(t, p, wl["seed"])
+    prm = S.batched_params(wl["nr"], wl["seed"])
+    return t, p, br, prm
+
+
+def oracle_sample(t, p, br, prm, dt, index: int = 0):
+    """One flux-transport step of one realization on the CPU oracle (at the
+    given dt, or at its own CFL-limited dt when dt is None); returns
+    (cell_updates, seconds)."""
+    from oracle import oracle as O
+    q = dict(O.DEFAULTS)
+    q.update(n_realizations=1, advance_flow=True, flow_dr_model=1, flow_mf_model=1,
+             advance_diffusion=True, strang_splitting=True, flow_num_method=4)
+    if dt is None:
+        q.update(time_end=1.0e9)
+    else:
+        q.update(time_end=dt, dt_max=dt)
+    raw = {k: v for k, v in q.items()}
+    raw.update({
+        "diffusion_coef_constants": [float(prm["diffusion_coef_constants"][index])],
+        "flow_dr_coef_p0_values": [float(prm["dr_p0"][index])], "flow_dr_coef_p2_values": [float(prm["dr_p2"][index])],
+        "flow_dr_coef_p4_values": [float(prm["dr_p4"][index])], "flow_mf_coef_p1_values": [float(prm["mf_p1"][index])],
+        "flow_mf_coef_p3_values": [float(prm["mf_p3"][index])], "flow_mf_coef_p5_values": [float(prm["mf_p5"][index])],
+    })
+    pp = O.process_parameters(raw)
+    m = np.ascontiguousarray(br[None])
+    t0 = time.perf_counter()
+    r = O.run(pp, map_pt=m, s1=p, s2=t, want_field=False, hist_cap=16, max_steps=1)
+    sec = time.perf_counter() - t0
+    return r["cell_updates"], sec
+
+
+def host_threads() -> int:
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def run_reference(args, wl, name):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from hipft_b200 import synthetic as S  # noqa: F401  (inputs only)
+    t, p, br, prm = make_inputs(wl)
+    vals = []
+    total = 0.0
+    for k in range(args.warmup + args.steps):
+        cells, sec = oracle_sample(t, p, br, prm, None, index=k % wl["nr"])
+        if k >= args.warmup:
+            vals.append(cells / sec / 1e9)
+            total += sec
+    v = float(np.mean(vals))
+    sample = (f"one realization (cycling through the {wl['nr']}), one Strang flux-transport step at its "
+              f"CFL-limited dt on the {wl['ntm']}x{wl['npm1'] - 1} grid, per bench step")
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / max(args.steps, 1),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": name, "grid": [wl["ntm"], wl["npm1"] - 1], "realizations": wl["nr"]},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": host_threads(), "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def run_gpu(args, wl, name):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import hipft_b200 as H
+    from hipft_b200 import synthetic as S
+
+    t, p, br, prm = make_inputs(wl)
+    first, nrl = split_realizations(wl["nr"], world, rank)
+    sl = slice(first, first + nrl)
+    g = H.HipftGPU(t, p, nrl, device=local, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                   advance_diffusion=True, diffusion_coef_constants=prm["diffusion_coef_constants"][sl])
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    g.load_initial_map(np.broadcast_to(br, (nrl,) + br.shape))
+    g.set_flow(dr_model=1, mf_model=1, dr_p0=prm["dr_p0"][sl], dr_p2=prm["dr_p2"][sl], dr_p4=prm["dr_p4"][sl],
+               mf_p1=prm["mf_p1"][sl], mf_p3=prm["mf_p3"][sl], mf_p5=prm["mf_p5"][sl])
+    g.update_flow()
+    dt = g.flow_dtmax()
+    ntm, npm = g.ntm, g.npm
+    # assimilation maps for every 24 h boundary the run will cross
+    n_total = args.warmup + 2 * args.steps + 2
+    da_times = [24.0 * k for k in range(1, int(n_total * dt / 24.0) + 2)]
+    da_maps = {tt: S.observed_map(t, p, tt, wl["seed"]) for tt in da_times}
+    state = {"time": 0.0, "da": 0}
+
+    def step():
+        g.flux_transport_step(dt)
+        state["time"] += dt
+        if state["da"] < len(da_times) and state["time"] >= da_times[state["da"]]:
+            g.assimilate(da_maps[da_times[state["da"]]], custom_from_mu=True, mu_power=prm["mu_power"][sl],
+                         mu_limit=prm["mu_limit"][sl], lat_limit=prm["lat_limit"][sl])
+            state["da"] += 1
+        g.analysis(state["time"])
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    i0 = g.info()
+    g.set_profiling(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    i1 = g.info()
+    sts_n, sts_ms = g.kernel_time(0)
+    adv_n, adv_ms = g.kernel_time(1)
+    ring_n, ring_ms = g.kernel_time(2)
+    oth_n, oth_ms = g.kernel_time(3)
+    g.set_profiling(False)
+    cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
+    launches = int(i1.kernel_launches - i0.kernel_launches)
+
+    # end to end through the C ABI with host buffers
+    f_host = torch.empty((nrl, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
+    g.get_field(f_host)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    i2 = g.info()
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        g.set_field(f_host)
+        step()
+        g.get_field(f_host)
+    w1 = time.perf_counter()
+    i3 = g.info()
+    e2e_ms = (w1 - w0) * 1e3
+    e2e_cells = float(i3.cell_stage_updates - i2.cell_stage_updates)
+
+    if dist:
+        tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        cc = torch.tensor([cells, e2e_cells, float(launches)], dtype=torch.float64, device="cuda")
+        dist.all_reduce(cc, op=dist.ReduceOp.SUM)
+        ms, e2e_ms = float(tt[0]), float(tt[1])
+        cells, e2e_cells, launches = float(cc[0]), float(cc[1]), int(cc[2])
+
+    peak, peak_kind = measured_peak()
+    bytes_per_launch = STS_BYTES_PER_CELL * ntm * (npm - 2) * nrl
+    sts_avg_ms = sts_ms / max(sts_n, 1)
+    achieved = bytes_per_launch / (sts_avg_ms * 1e-3) / 1e9 if sts_n else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "sts_stage_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            tj = json.load(fh)
+        traffic = tj["dram_bytes_per_cell"] * ntm * (npm - 2) * nrl
+    out = {
+        "metric": METRIC, "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": name, "grid": [ntm, npm - 2], "realizations": wl["nr"],
+                   "realizations_per_gpu": nrl, "dt_hours": dt, "parallelism": f"realizations/{world}",
+                   "method": "WENO3+SSPRK(4,3) Strang-split with RKG2 (PTL subcycles), DA every 24 h",
+                   "l2": "inputs larger than L2 (%.2f GB per field), no flush" % (ntm * npm * nrl * 8 / 1e9)},
+        "roofline": {"bound": "hbm", "kernel": "k_diffusion_stage<MODE_STSK> (fused RKG2 stage)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "launches": sts_n, "avg_launch_ms": sts_avg_ms,
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "share_of_step": sts_ms / ms if ms > 0 else None,
+                     "other_kernels_ms": {"advection_stage": adv_ms, "ring_sums": ring_ms, "other": oth_ms},
+                     "other_kernels_launches": {"advection_stage": adv_n, "ring_sums": ring_n, "other": oth_n}},
+        "e2e": {"value": e2e_cells / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+                "h2d_bytes_per_step": ntm * npm * nrl * 8, "d2h_bytes_per_step": ntm * npm * nrl * 8},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cells_c, sec_c = oracle_sample(t, p, br, prm, dt, index=0)
+        out["cpu_baseline"] = {"value": cells_c / sec_c / 1e9, "unit": UNIT, "cores": host_threads(),
+                               "kind": "port",
+                               "sample": f"CPU oracle, one realization, one Strang flux-transport step of dt={dt:.4f} h "
+                                         f"({sec_c:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(out))
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="hipft", choices=["hipft", "reference"])
+    ap.add_argument("--workload", default="batched64_1024x2048", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, wl, args.workload)
+    return run_gpu(args, wl, args.workload)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

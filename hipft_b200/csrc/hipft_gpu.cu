@@ -98,6 +98,40 @@ struct hipft_gpu {
   int *d_tidx = nullptr;
   std::string err;
   int64_t launches = 0, cell_updates = 0;
+  // optional per-kernel event timing
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pending[HIPFT_K_NKINDS];
+  double prof_ms[HIPFT_K_NKINDS] = {};
+  int64_t prof_n[HIPFT_K_NKINDS] = {};
+};
+
+// Event pair around one launch when profiling (returns the stop event).
+struct ProfScope {
+  hipft_gpu *h;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  static cudaEvent_t take(hipft_gpu *h) {
+    if (!h->ev_pool.empty()) {
+      cudaEvent_t e = h->ev_pool.back();
+      h->ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+  }
+  ProfScope(hipft_gpu *hh, int k) : h(hh), kind(k) {
+    if (!h->profiling) return;
+    a = take(h);
+    b = take(h);
+    if (a) cudaEventRecord(a, h->stream);
+  }
+  ~ProfScope() {
+    if (!h->profiling || !a || !b) return;
+    cudaEventRecord(b, h->stream);
+    h->ev_pending[kind].push_back({a, b});
+  }
 };
 
 // ------------------------------------------------------------------ errors
@@ -270,6 +304,7 @@ static int sync_read(hipft_gpu *h, const void *dsrc, size_t bytes) {
 
 // ------------------------------------------------------------- kernels glue
 static int ring_diffusion(hipft_gpu *h, const double *x) {
+  ProfScope ps(h, HIPFT_K_RING);
   k_ring_diffusion<<<h->nr, 256, 0, h->stream>>>(h->M, h->DC, x, h->d_ring);
   LAUNCHED(h);
   return HIPFT_OK;
@@ -279,6 +314,7 @@ template <int MODE>
 static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
                            double *out, double *out2, StageCoef sc, unsigned long long *absmax) {
   dim3 blk(32, 8);
+  ProfScope ps(h, MODE == MODE_STSK ? HIPFT_K_STS : HIPFT_K_OTHER);
   k_diffusion_stage<MODE><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->DC, x, ykm2, u0, dty0, out, out2,
                                                                        h->d_ring, h->bc_diff_n, h->bc_diff_s, sc,
                                                                        absmax);
@@ -287,9 +323,13 @@ static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, co
 }
 
 static int advection_stage(hipft_gpu *h, const double *x, const double *f0, double *out, AdvCombine cb) {
-  k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
-  LAUNCHED(h);
+  {
+    ProfScope ps(h, HIPFT_K_RING);
+    k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
+    LAUNCHED(h);
+  }
   dim3 blk(32, 8);
+  ProfScope ps(h, HIPFT_K_ADV);
   if (h->adv_space == 2)
     k_advection_stage<32, 8, true><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out,
                                                                                  h->d_ring, h->bc_flow_n,
@@ -494,6 +534,12 @@ extern "C" int hipft_gpu_destroy(hipft_gpu *h) {
   if (!h) return HIPFT_OK;
   cudaSetDevice(h->dev);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto &v : h->ev_pending)
+    for (auto &pr : v) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  for (auto e : h->ev_pool) cudaEventDestroy(e);
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1182,5 +1228,41 @@ extern "C" int hipft_gpu_set_stream(hipft_gpu *h, void *s) {
 extern "C" int hipft_gpu_synchronize(hipft_gpu *h) {
   if (!h) return HIPFT_EINVAL;
   CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+// Folds finished event pairs into the per-kind totals.
+static int prof_collect(hipft_gpu *h) {
+  CK(h, cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < HIPFT_K_NKINDS; ++k) {
+    for (auto &pr : h->ev_pending[k]) {
+      float ms = 0.f;
+      CK(h, cudaEventElapsedTime(&ms, pr.first, pr.second));
+      h->prof_ms[k] += ms;
+      h->prof_n[k] += 1;
+      h->ev_pool.push_back(pr.first);
+      h->ev_pool.push_back(pr.second);
+    }
+    h->ev_pending[k].clear();
+  }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_set_profiling(hipft_gpu *h, int on) {
+  if (!h) return HIPFT_EINVAL;
+  TRY(prof_collect(h));
+  for (int k = 0; k < HIPFT_K_NKINDS; ++k) {
+    h->prof_ms[k] = 0.0;
+    h->prof_n[k] = 0;
+  }
+  h->profiling = on != 0;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_kernel_time(hipft_gpu *h, int kind, int64_t *launches, double *total_ms) {
+  if (!h || kind < 0 || kind >= HIPFT_K_NKINDS || !launches || !total_ms) return HIPFT_EINVAL;
+  TRY(prof_collect(h));
+  *launches = h->prof_n[kind];
+  *total_ms = h->prof_ms[kind];
   return HIPFT_OK;
 }

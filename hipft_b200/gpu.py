@@ -96,6 +96,9 @@ SIGNATURES = [
     ("hipft_gpu_get_flux", ctypes.c_int, [_H, DPTR, DPTR]),
     ("hipft_gpu_balance_flux", ctypes.c_int, [_H]),
     ("hipft_gpu_info", ctypes.c_int, [_H, ctypes.POINTER(Info)]),
+    ("hipft_gpu_set_profiling", ctypes.c_int, [_H, ctypes.c_int]),
+    ("hipft_gpu_kernel_time", ctypes.c_int, [_H, ctypes.c_int, ctypes.POINTER(ctypes.c_int64),
+                                             ctypes.POINTER(ctypes.c_double)]),
     ("hipft_gpu_set_stream", ctypes.c_int, [_H, ctypes.c_void_p]),
     ("hipft_gpu_synchronize", ctypes.c_int, [_H]),
     ("hipft_run", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
@@ -318,6 +321,16 @@ class HipftGPU:
         i = Info()
         self._ck(self.L.hipft_gpu_info(self.h, ctypes.byref(i)), "info")
         return i
+
+    def set_profiling(self, on: bool):
+        """Per-kernel CUDA-event timing on the handle's stream (resets the counters)."""
+        self._ck(self.L.hipft_gpu_set_profiling(self.h, int(on)), "set_profiling")
+
+    def kernel_time(self, kind: int):
+        """(launches, total ms) of kernel kind 0 STS stage, 1 advection stage, 2 ring sums, 3 other."""
+        n, ms = ctypes.c_int64(0), ctypes.c_double(0.0)
+        self._ck(self.L.hipft_gpu_kernel_time(self.h, int(kind), ctypes.byref(n), ctypes.byref(ms)), "kernel_time")
+        return n.value, ms.value
 
     def set_stream(self, stream_ptr: int):
         self._ck(self.L.hipft_gpu_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "set_stream")

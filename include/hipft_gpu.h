@@ -201,6 +201,15 @@ typedef struct {
   size_t device_bytes;          /* device memory held by the handle           */
 } hipft_info;
 int hipft_gpu_info(const hipft_gpu *h, hipft_info *info);
+/* Per-kernel timing with CUDA events on the handle's stream.  Kinds:
+ * 0 RKG2/RKL2 stage (the fused Laplacian + combine), 1 advection stage
+ * (fused WENO3/upwind operator + SSPRK combine), 2 pole-ring sums,
+ * 3 everything else.  Enabling resets the counters. */
+enum { HIPFT_K_STS = 0, HIPFT_K_ADV = 1, HIPFT_K_RING = 2, HIPFT_K_OTHER = 3, HIPFT_K_NKINDS = 4 };
+int hipft_gpu_set_profiling(hipft_gpu *h, int on);
+/* Launch count and summed device time (ms) of one kernel kind since
+ * profiling was enabled (synchronizes the stream). */
+int hipft_gpu_kernel_time(hipft_gpu *h, int kind, int64_t *launches, double *total_ms);
 /* Runs subsequent work on a caller-owned cudaStream_t (NULL: the handle's). */
 int hipft_gpu_set_stream(hipft_gpu *h, void *cuda_stream);
 int hipft_gpu_synchronize(hipft_gpu *h);

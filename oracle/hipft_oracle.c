@@ -133,6 +133,7 @@ typedef struct {
   int da_active;
   int *tidx0, *tidx1;
   orc_hist *hist;
+  double cell_updates; /* unique cells x stages advanced (for throughput) */
 } orc;
 
 #define A3(a, j, k, i, n1, n2) \
@@ -833,6 +834,7 @@ static void advection_operator_weno3(orc *S, const double *x, double *aop) {
 }
 
 static void advection_operator(orc *S, const double *x, double *aop) {
+  S->cell_updates += (double)S->ntm * (S->npm - 2) * S->nr;
   if (S->adv_space == 1) advection_operator_upwind(S, x, aop);
   else advection_operator_weno3(S, x, aop);
 }
@@ -1054,6 +1056,7 @@ static void diffusion_step_sts_cd(orc *S, double dtl) {
     dty0[q] = dtl * dty0[q];
     ukm1[q] = f[q] + S->sts_ubj[1] * dty0[q];
   }
+  S->cell_updates += (double)S->ntm * (S->npm - 2) * S->nr * (double)S->sts_s;
   for (long k = 2; k <= S->sts_s; k++) {
     diffusion_operator_cd(S, ukm1, ykm1);
     double uj = S->sts_uj[k], vj = S->sts_vj[k], ubj = S->sts_ubj[k], gj = S->sts_gj[k];
@@ -1075,6 +1078,7 @@ static void diffusion_step_fe_cd(orc *S, double dtl) {
   long nc = (long)ceil(r);
   S->n_stable_diffusion_cycles = nc;
   double dte = dtl / (double)nc;
+  S->cell_updates += (double)S->ntm * (S->npm - 2) * S->nr * (double)nc;
   for (long i = 1; i <= nc; i++) {
     diffusion_operator_cd(S, S->f, fold);
     for (size_t q = 0; q < n; q++) S->f[q] = S->f[q] + dte * fold[q];
@@ -1430,6 +1434,7 @@ int orc_run(const orc_params *P, int n1, int n2, const double *s1in, const doubl
   if (timing_out) {
     timing_out[0] = (double)S->ntime;
     timing_out[1] = S->time;
+    timing_out[2] = S->cell_updates;
   }
   return 0;
 }

@@ -254,7 +254,7 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
         raise RuntimeError(f"oracle failed with code {rc}")
     n = min(h.nrows, hist_cap)
     return dict(sol=sol[:n].copy(), num=num[:n].copy(), f=f, nsteps=int(tinfo[0]),
-                time=float(tinfo[1]))
+                time=float(tinfo[1]), cell_updates=float(tinfo[2]))
 
 
 def read_history(path: str) -> np.ndarray:
