@@ -81,7 +81,13 @@ struct hipft_gpu {
   int64_t sts_s = 0, n_euler = 0, subcycles_state = 0;
   std::vector<double> sts_uj, sts_vj, sts_ubj, sts_gj, sts_b;
   // scratch
-  double *d_ring = nullptr;
+  double *d_ring = nullptr;            // ring sums for kernels that take them from a launch of their own
+  double *d_ringbuf[2] = {};           // diffusion ring of a stage's input / output (fused path)
+  int ring_cur = 0;
+  bool dring_valid = false;            // d_ringbuf[ring_cur] holds the ring of the current field
+  double *d_rpart = nullptr;
+  unsigned int *d_rcount = nullptr;
+  int nkb = 0;
   unsigned long long *d_bits = nullptr;
   double *d_part = nullptr;
   size_t part_cap = 0;
@@ -303,20 +309,52 @@ static int sync_read(hipft_gpu *h, const void *dsrc, size_t bytes) {
 }
 
 // ------------------------------------------------------------- kernels glue
-static int ring_diffusion(hipft_gpu *h, const double *x) {
+static int ring_diffusion(hipft_gpu *h, const double *x, double *ring) {
   ProfScope ps(h, HIPFT_K_RING);
-  k_ring_diffusion<<<h->nr, 256, 0, h->stream>>>(h->M, h->DC, x, h->d_ring);
+  k_ring_diffusion<<<h->nr, 256, 0, h->stream>>>(h->M, h->DC, x, ring);
   LAUNCHED(h);
+  return HIPFT_OK;
+}
+
+// Diffusion ring sums of the current field, reused while the field is
+// unchanged (the fused stages leave the ring of their output behind).
+static int current_dring(hipft_gpu *h, const double **ring) {
+  if (!h->dring_valid) {
+    TRY(ring_diffusion(h, h->buf[h->cur], h->d_ringbuf[h->ring_cur]));
+    h->dring_valid = true;
+  }
+  *ring = h->d_ringbuf[h->ring_cur];
+  return HIPFT_OK;
+}
+
+constexpr int kKPT = 8;  // phi columns per thread in the fused stage kernel
+
+template <int MODE>
+static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
+                        double *out, double *out2, StageCoef sc) {
+  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, h->nkb};
+  // shift the theta-to-lane map by one row when row ntm-1 would be a warp's last lane
+  const int jshift = ((h->ntm - 2) % 32 == 31) ? 1 : 0;
+  dim3 grd((unsigned)((h->ntm + jshift + 127) / 128), (unsigned)h->nkb, (unsigned)h->nr);
+  {
+    ProfScope ps(h, MODE == MODE_STSK ? HIPFT_K_STS : HIPFT_K_OTHER);
+    k_sts_stage_v2<MODE, kKPT><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
+                                                           h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
+                                                           sc, ro, jshift);
+    LAUNCHED(h);
+  }
+  h->ring_cur = 1 - h->ring_cur;  // the output's ring is now current
   return HIPFT_OK;
 }
 
 template <int MODE>
 static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
-                           double *out, double *out2, StageCoef sc, unsigned long long *absmax) {
+                           double *out, double *out2, const double *ring, StageCoef sc,
+                           unsigned long long *absmax) {
   dim3 blk(32, 8);
   ProfScope ps(h, MODE == MODE_STSK ? HIPFT_K_STS : HIPFT_K_OTHER);
   k_diffusion_stage<MODE><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->DC, x, ykm2, u0, dty0, out, out2,
-                                                                       h->d_ring, h->bc_diff_n, h->bc_diff_s, sc,
+                                                                       ring, h->bc_diff_n, h->bc_diff_s, sc,
                                                                        absmax);
   LAUNCHED(h);
   return HIPFT_OK;
@@ -416,6 +454,12 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
     if (cudaMemsetAsync(h->buf[b], 0, h->fieldn * sizeof(double), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   }
   if ((rc = dalloc(h, &h->d_ring, 2 * (size_t)nr))) return bail(rc);
+  h->nkb = (npm - 2 + kKPT - 1) / kKPT;
+  if ((rc = dalloc(h, &h->d_ringbuf[0], 2 * (size_t)nr))) return bail(rc);
+  if ((rc = dalloc(h, &h->d_ringbuf[1], 2 * (size_t)nr))) return bail(rc);
+  if ((rc = dalloc(h, &h->d_rpart, 2 * (size_t)nr * h->nkb))) return bail(rc);
+  if ((rc = dalloc(h, &h->d_rcount, (size_t)nr))) return bail(rc);
+  if (cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned int) * nr, h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   if ((rc = dalloc(h, &h->d_bits, 4))) return bail(rc);
   if (cudaMallocHost((void **)&h->h_pin, sizeof(double) * std::max<size_t>(64, (size_t)nr * kNPart)) !=
       cudaSuccess)
@@ -564,6 +608,7 @@ extern "C" int hipft_gpu_set_field(hipft_gpu *h, const double *f) {
                           (size_t)h->ntm * sizeof(double), (size_t)h->npm * h->nr, cudaMemcpyHostToDevice,
                           h->stream));
   h->field_set = true;
+  h->dring_valid = false;
   return HIPFT_OK;
 }
 
@@ -792,6 +837,7 @@ extern "C" int hipft_gpu_advection_step(hipft_gpu *h, double dt) {
   if (!h->field_set) return fail(h, HIPFT_ESTATE, "advection_step before set_field");
   if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "advection_step: advance_flow is off");
   CK(h, cudaSetDevice(h->dev));
+  h->dring_valid = false;
   double *f = h->buf[h->cur];
   int ia = scratch(h, 0), ib = scratch(h, 1);
   double *A = h->buf[ia], *B = h->buf[ib];
@@ -859,21 +905,35 @@ static void load_sts(hipft_gpu *h, double dtl) {
 static int sts_super_step(hipft_gpu *h, double dtl) {
   load_sts(h, dtl);
   int u0 = h->cur, idty = scratch(h, 0), ia = scratch(h, 1), ib = scratch(h, 2);
-  TRY(ring_diffusion(h, h->buf[u0]));
-  TRY(diffusion_stage<MODE_STS1>(h, h->buf[u0], nullptr, nullptr, nullptr, h->buf[ia], h->buf[idty],
-                                 StageCoef{dtl, h->sts_ubj[1], 0, 0, 0}, nullptr));
+  const bool fused = !h->DC.grid;
+  if (fused) {
+    const double *r0;
+    TRY(current_dring(h, &r0));
+    TRY(sts_stage_v2<MODE_STS1>(h, h->buf[u0], nullptr, nullptr, nullptr, h->buf[ia], h->buf[idty],
+                                StageCoef{dtl, h->sts_ubj[1], 0, 0, 0}));
+  } else {
+    TRY(ring_diffusion(h, h->buf[u0], h->d_ring));
+    TRY(diffusion_stage<MODE_STS1>(h, h->buf[u0], nullptr, nullptr, nullptr, h->buf[ia], h->buf[idty], h->d_ring,
+                                   StageCoef{dtl, h->sts_ubj[1], 0, 0, 0}, nullptr));
+  }
   int ykm1 = ia, ykm2 = u0;
   for (int64_t k = 2; k <= h->sts_s; ++k) {
-    TRY(ring_diffusion(h, h->buf[ykm1]));
     int out = (k == 2) ? ib : ykm2;
     double uj = h->sts_uj[k], vj = h->sts_vj[k];
     StageCoef sc{uj, vj, 1.0 - uj - vj, h->sts_ubj[k] * dtl, h->sts_gj[k]};
-    TRY(diffusion_stage<MODE_STSK>(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[out], nullptr,
-                                   sc, nullptr));
+    if (fused) {
+      TRY(sts_stage_v2<MODE_STSK>(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[out], nullptr,
+                                  sc));
+    } else {
+      TRY(ring_diffusion(h, h->buf[ykm1], h->d_ring));
+      TRY(diffusion_stage<MODE_STSK>(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[out],
+                                     nullptr, h->d_ring, sc, nullptr));
+    }
     ykm2 = ykm1;
     ykm1 = out;
   }
   h->cur = ykm1;
+  h->dring_valid = fused;  // the last fused stage left the ring of the new field
   h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr * h->sts_s;
   return HIPFT_OK;
 }
@@ -885,10 +945,20 @@ static int euler_steps(hipft_gpu *h, double dtl) {
   double dte = dtl / (double)n;
   for (int64_t c = 0; c < n; ++c) {
     int o = scratch(h, 0);
-    TRY(ring_diffusion(h, h->buf[h->cur]));
-    TRY(diffusion_stage<MODE_EULER>(h, h->buf[h->cur], nullptr, nullptr, nullptr, h->buf[o], nullptr,
-                                    StageCoef{dte, 0, 0, 0, 0}, nullptr));
-    h->cur = o;
+    if (!h->DC.grid) {
+      const double *r0;
+      TRY(current_dring(h, &r0));
+      TRY(sts_stage_v2<MODE_EULER>(h, h->buf[h->cur], nullptr, nullptr, nullptr, h->buf[o], nullptr,
+                                   StageCoef{dte, 0, 0, 0, 0}));
+      h->cur = o;
+      h->dring_valid = true;
+    } else {
+      TRY(ring_diffusion(h, h->buf[h->cur], h->d_ring));
+      TRY(diffusion_stage<MODE_EULER>(h, h->buf[h->cur], nullptr, nullptr, nullptr, h->buf[o], nullptr, h->d_ring,
+                                      StageCoef{dte, 0, 0, 0, 0}, nullptr));
+      h->cur = o;
+      h->dring_valid = false;
+    }
   }
   h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr * n;
   return HIPFT_OK;
@@ -899,8 +969,9 @@ static int ptl_dt(hipft_gpu *h, double *dtl) {
   double dtime_in = *dtl;
   double *f = h->buf[h->cur], *af = h->buf[scratch(h, 0)];
   CK(h, cudaMemsetAsync(h->d_bits, 0, 2 * sizeof(unsigned long long), h->stream));
-  TRY(ring_diffusion(h, f));
-  TRY(diffusion_stage<MODE_AX>(h, f, nullptr, nullptr, nullptr, af, nullptr, StageCoef{}, h->d_bits));
+  const double *ring;
+  TRY(current_dring(h, &ring));
+  TRY(diffusion_stage<MODE_AX>(h, f, nullptr, nullptr, nullptr, af, nullptr, ring, StageCoef{}, h->d_bits));
   TRY(sync_read(h, h->d_bits, 8));
   double axabsmax;
   std::memcpy(&axabsmax, h->h_pin, 8);
@@ -1053,6 +1124,7 @@ extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const 
   dim3 g2((unsigned)((ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)nr);
   k_da_apply<<<g2, blk, 0, h->stream>>>(h->M, delta, f, ratio);
   LAUNCHED(h);
+  h->dring_valid = false;
   return HIPFT_OK;
 }
 
@@ -1193,6 +1265,7 @@ extern "C" int hipft_gpu_balance_flux(hipft_gpu *h) {
   dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)h->nr);
   k_scale_balance<<<grd, blk, 0, h->stream>>>(h->M, h->buf[h->cur], dr);
   LAUNCHED(h);
+  h->dring_valid = false;
   CK(h, cudaStreamSynchronize(h->stream));
   return HIPFT_OK;
 }

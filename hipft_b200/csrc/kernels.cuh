@@ -832,3 +832,161 @@ __global__ void k_scale_balance(Mesh m, double *a, const double *ratio) {
 }
 
 }  // namespace hipft
+
+namespace hipft {
+
+// ------------------------------------------------------ RKG2 stage, v2
+// Fused RKG2/RKL2 stage for a diffusion coefficient that is constant per
+// realization (the diffusion_coef_constant path of load_diffusion).  Each
+// thread owns one theta row j and marches over KPT consecutive phi columns;
+// all of its loads are issued before any arithmetic so that 5*KPT+2
+// independent requests per thread are in flight.  The 5-point coefficients
+// are assembled from per-row and per-column factors in exactly the operation
+// order of load_diffusion_matrix (src/hipft.f90:4962-4979), so values are
+// bit-identical to the general kernel.
+//
+// The pole-ring sums of the *output* (needed by the next stage's pole rows,
+// src/hipft.f90:7969-7979) are fused: the threads owning rows 2 and ntm-1
+// add their KPT terms in column order, write one partial per phi block, and
+// the last contributor of each realization (atomic counter, no waiting)
+// reduces the partials in block order with a fixed shuffle tree and writes
+// ring_out.  Nothing spins, so no wait needs a bound.
+struct RingOut {
+  double *ring;          // [2*nr] (fn, fs) of the output field
+  double *part;          // [2][nr][nkb] partial sums
+  unsigned int *count;   // [nr] contribution counters (left at 0)
+  int nkb;               // phi blocks per realization
+};
+
+template <int MODE, int KPT>
+__global__ void __launch_bounds__(128, 4) k_sts_stage_v2(Mesh m, const double *__restrict__ dfac,
+                                                     const double *__restrict__ x, const double *ykm2,
+                                                     const double *__restrict__ u0, const double *__restrict__ dty0,
+                                                     double *out, double *out2, const double *__restrict__ ring_in,
+                                                     double bcn, double bcs, StageCoef sc, RingOut ro, int jshift) {
+  const int lane = threadIdx.x & 31;
+  // jshift (0 or 1) keeps rows ntm-1 and ntm in one warp; rows 1 and 2 always are.
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1 - jshift;
+  const int kb = blockIdx.y;
+  const int k0 = kb * KPT + 2;
+  const int i = blockIdx.z + 1;
+  const int ntm = m.ntm, npm = m.npm;
+  const int nk = min(KPT, npm - 1 - k0 + 1);  // columns in this block (k0..k0+nk-1 <= npm-1)
+  const bool row = (j >= 1 && j <= ntm);
+  const bool interior = row && j >= 2 && j <= ntm - 1;
+  const int64_t ld = m.ldt;
+  const int64_t q0 = (int64_t)(i - 1) * m.plane + (int64_t)(k0 - 1) * ld + (j - 1);
+  const double Dr = dfac[i];
+  const double Dh = kHalf * (Dr + Dr);  // half*(D(j,k)+D(j+1,k)) of a constant D
+
+  // ---- loads (all independent, issued before any store)
+  double xv[KPT + 2], xe[KPT], y2[KPT], uu[KPT], dd[KPT];
+#pragma unroll
+  for (int c = 0; c < KPT + 2; ++c) {
+    int kc = k0 - 1 + c;
+    xv[c] = (row && kc <= npm) ? x[q0 + (int64_t)(c - 1) * ld] : 0.0;
+  }
+#pragma unroll
+  for (int c = 0; c < KPT; ++c) {
+    bool ok = row && c < nk;
+    int64_t q = q0 + (int64_t)c * ld;
+    // theta neighbours across warp boundaries: lane 0 needs x(j-1), lane 31 x(j+1)
+    double e = 0.0;
+    if (ok && interior && (lane == 0 || lane == 31)) e = (lane == 0) ? x[q - 1] : x[q + 1];
+    xe[c] = e;
+    if (MODE == MODE_STSK) {
+      y2[c] = ok ? ykm2[q] : 0.0;
+      uu[c] = ok ? u0[q] : 0.0;
+      dd[c] = ok ? dty0[q] : 0.0;
+    }
+  }
+  // per-row factors
+  double sti = 0, c2 = 0, c4 = 0;
+  if (interior) {
+    sti = m.st_i[j];
+    c2 = Dh * m.dth_i[j] * m.dt_i[j] * sti * m.sth[j];
+    c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * sti * m.sth[j + 1];
+  }
+  const bool north = (j == 2), south = (j == ntm - 1);
+  double rn_acc = 0.0;  // ring partial (north or south) over this block's columns
+  const double ax_n = ring_in[2 * (i - 1)] * bcn;
+  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
+#pragma unroll
+  for (int c = 0; c < KPT; ++c) {
+    const int k = k0 + c;
+    const bool active = row && c < nk;
+    double xc = xv[c + 1];
+    double up = __shfl_up_sync(0xffffffffu, xc, 1);
+    double dn = __shfl_down_sync(0xffffffffu, xc, 1);
+    double xjm = (lane == 0) ? xe[c] : up;
+    double xjp = (lane == 31) ? xe[c] : dn;
+    double ax;
+    if (j == 1) {
+      ax = ax_n;
+    } else if (j == ntm) {
+      ax = ax_s;
+    } else {
+      double pk = m.dph_i[min(k, npm)], pk1 = m.dph_i[min(k + 1, npm)], dpi = m.dp_i[min(k, npm)];
+      double c1 = Dh * pk * dpi * sti * sti;
+      double c5 = Dh * pk1 * dpi * sti * sti;
+      double c3 = -(c1 + c2 + c4 + c5);
+      ax = c1 * xv[c] + c2 * xjm + c3 * xc + c4 * xjp + c5 * xv[c + 2];
+    }
+    double y, d0 = 0.0;
+    if (MODE == MODE_STS1) {
+      d0 = sc.a * ax;
+      y = xc + sc.b * d0;
+    } else if (MODE == MODE_STSK) {
+      y = sc.a * xc + sc.b * y2[c] + sc.c * uu[c] + sc.d * ax + sc.e * dd[c];
+    } else {  // MODE_EULER
+      y = xc + sc.a * ax;
+    }
+    // ring terms of the output, ((D(1,k)+D(2,k))*(y(2,k)-y(1,k)))*dp(k), with
+    // the pole-row output taken from the neighbouring lane
+    double yup = __shfl_up_sync(0xffffffffu, y, 1);
+    double ydn = __shfl_down_sync(0xffffffffu, y, 1);
+    if (!active) continue;
+    if (north) rn_acc = rn_acc + (Dr + Dr) * (y - yup) * m.dp[k];
+    if (south) rn_acc = rn_acc + (Dr + Dr) * (ydn - y) * m.dp[k];
+    const int64_t q = q0 + (int64_t)c * ld;
+    out[q] = y;
+    if (k == 2) out[q + (int64_t)(npm - 2) * ld] = y;
+    if (k == npm - 1) out[q - (int64_t)(npm - 2) * ld] = y;
+    if (MODE == MODE_STS1) {
+      out2[q] = d0;
+      if (k == 2) out2[q + (int64_t)(npm - 2) * ld] = d0;
+      if (k == npm - 1) out2[q - (int64_t)(npm - 2) * ld] = d0;
+    }
+  }
+  // ---- publish ring partials; the last contributor of realization i reduces
+  const bool contrib = (north || south) && row;
+  unsigned int last = 0;
+  if (contrib) {
+    ro.part[((int64_t)(south ? 1 : 0) * m.nr + (i - 1)) * ro.nkb + kb] = rn_acc;
+    __threadfence();
+    unsigned int old = atomicAdd(&ro.count[i - 1], 1u);
+    last = (old == 2u * (unsigned)ro.nkb - 1u) ? 1u : 0u;
+  }
+  // broadcast "last" to the contributor's warp (all lanes reach this point)
+  unsigned int src_mask = __ballot_sync(0xffffffffu, last != 0);
+  if (src_mask) {
+    __threadfence();
+    double sn = 0.0, ss = 0.0;
+    for (int b = lane; b < ro.nkb; b += 32) {
+      sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + b]);
+      ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sn += __shfl_down_sync(0xffffffffu, sn, o);
+      ss += __shfl_down_sync(0xffffffffu, ss, o);
+    }
+    if (lane == 0) {
+      ro.ring[2 * (i - 1)] = sn;
+      ro.ring[2 * (i - 1) + 1] = ss;
+      ro.count[i - 1] = 0u;
+    }
+  }
+}
+
+}  // namespace hipft
