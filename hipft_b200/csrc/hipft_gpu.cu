@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -327,20 +328,44 @@ static int current_dring(hipft_gpu *h, const double **ring) {
   return HIPFT_OK;
 }
 
-constexpr int kKPT = 8;  // phi columns per thread in the fused stage kernel
+constexpr int kKPT = 8;   // phi columns per thread, fused stage kernel v2 (one row per thread)
+constexpr int kKPT3 = 4;  // phi columns per thread, v3 (two rows per thread)
+
+// Fused stage kernel variant: 3 (row pairs, 16-byte accesses; default) or
+// 2 (one row per thread); HIPFT_STS_KERNEL selects it for A/B timing.
+static int sts_kernel_variant() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_STS_KERNEL");
+    v = (e && std::atoi(e) == 2) ? 2 : 3;
+  }
+  return v;
+}
 
 template <int MODE>
 static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
                         double *out, double *out2, StageCoef sc) {
-  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, h->nkb};
-  // shift the theta-to-lane map by one row when row ntm-1 would be a warp's last lane
-  const int jshift = ((h->ntm - 2) % 32 == 31) ? 1 : 0;
-  dim3 grd((unsigned)((h->ntm + jshift + 127) / 128), (unsigned)h->nkb, (unsigned)h->nr);
+  const int kpt = (sts_kernel_variant() == 2) ? kKPT : kKPT3;
+  const int nkb = (h->npm - 2 + kpt - 1) / kpt;
+  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkb};
   {
     ProfScope ps(h, MODE == MODE_STSK ? HIPFT_K_STS : HIPFT_K_OTHER);
-    k_sts_stage_v2<MODE, kKPT><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
-                                                           h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
-                                                           sc, ro, jshift);
+    if (sts_kernel_variant() == 2) {
+      // shift the theta-to-lane map by one row when row ntm-1 would be a warp's last lane
+      const int jshift = ((h->ntm - 2) % 32 == 31) ? 1 : 0;
+      dim3 grd((unsigned)((h->ntm + jshift + 127) / 128), (unsigned)nkb, (unsigned)h->nr);
+      k_sts_stage_v2<MODE, kKPT><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
+                                                             h->d_ringbuf[h->ring_cur], h->bc_diff_n,
+                                                             h->bc_diff_s, sc, ro, jshift);
+    } else {
+      // odd ntm: keep the thread owning row ntm off lane 0 (row ntm-1 is its left neighbour)
+      const int jshift = (h->ntm % 2 == 1 && ((h->ntm - 1) / 2) % 32 == 0) ? 1 : 0;
+      const int nthr = (h->ntm + 2 * jshift + 1) / 2;
+      dim3 grd((unsigned)((nthr + 127) / 128), (unsigned)nkb, (unsigned)h->nr);
+      k_sts_stage_v3<MODE, kKPT3><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
+                                                             h->d_ringbuf[h->ring_cur], h->bc_diff_n,
+                                                             h->bc_diff_s, sc, ro, jshift);
+    }
     LAUNCHED(h);
   }
   h->ring_cur = 1 - h->ring_cur;  // the output's ring is now current
@@ -454,7 +479,7 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
     if (cudaMemsetAsync(h->buf[b], 0, h->fieldn * sizeof(double), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   }
   if ((rc = dalloc(h, &h->d_ring, 2 * (size_t)nr))) return bail(rc);
-  h->nkb = (npm - 2 + kKPT - 1) / kKPT;
+  h->nkb = (npm - 2 + kKPT3 - 1) / kKPT3;  // partial slots for the smaller phi block
   if ((rc = dalloc(h, &h->d_ringbuf[0], 2 * (size_t)nr))) return bail(rc);
   if ((rc = dalloc(h, &h->d_ringbuf[1], 2 * (size_t)nr))) return bail(rc);
   if ((rc = dalloc(h, &h->d_rpart, 2 * (size_t)nr * h->nkb))) return bail(rc);

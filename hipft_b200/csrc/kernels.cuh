@@ -990,3 +990,173 @@ __global__ void __launch_bounds__(128, 4) k_sts_stage_v2(Mesh m, const double *_
 }
 
 }  // namespace hipft
+
+namespace hipft {
+
+// ------------------------------------------------------ RKG2 stage, v3
+// As k_sts_stage_v2, but every thread owns two adjacent theta rows and moves
+// them with 16-byte loads and stores, so a warp touches 512 contiguous bytes
+// per array and phi column (twice the DRAM burst of v2) with half the load
+// instructions.  Row pairs start at an odd row (j = 2t+1, 2t+2) so the pole
+// pairs (1,2) and (ntm-1,ntm) stay inside one thread when ntm is even, and
+// inside one warp otherwise (handled with shuffles).  Requires ldt even.
+template <int MODE, int KPT>
+__global__ void __launch_bounds__(128, 4) k_sts_stage_v3(Mesh m, const double *__restrict__ dfac,
+                                                        const double *__restrict__ x, const double *ykm2,
+                                                        const double *__restrict__ u0,
+                                                        const double *__restrict__ dty0, double *out, double *out2,
+                                                        const double *__restrict__ ring_in, double bcn, double bcs,
+                                                        StageCoef sc, RingOut ro, int jshift) {
+  const int lane = threadIdx.x & 31;
+  // thread t owns rows ja = 2t+1-2*jshift and ja+1; for odd ntm, jshift moves
+  // the thread owning row ntm off lane 0 so row ntm-1 is in the same warp
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ja = 2 * t + 1 - 2 * jshift;
+  const int kb = blockIdx.y;
+  const int k0 = kb * KPT + 2;
+  const int i = blockIdx.z + 1;
+  const int ntm = m.ntm, npm = m.npm;
+  const int nk = min(KPT, npm - 1 - k0 + 1);
+  const bool rowa = (ja >= 1 && ja <= ntm), rowb = (ja + 1 >= 1 && ja + 1 <= ntm);
+  const bool any = rowa || rowb;
+  const int64_t ld = m.ldt;
+  // 16-byte aligned pair offset (ja-1 is even)
+  const int64_t q0 = (int64_t)(i - 1) * m.plane + (int64_t)(k0 - 1) * ld + (ja - 1);
+  const double Dr = dfac[i];
+  const double Dh = kHalf * (Dr + Dr);
+
+  double2 xv[KPT + 2], y2[KPT], uu[KPT], dd[KPT];
+  double xe[KPT];
+#pragma unroll
+  for (int c = 0; c < KPT + 2; ++c) {
+    int kc = k0 - 1 + c;
+    xv[c] = (any && ja >= 1 && kc <= npm) ? *reinterpret_cast<const double2 *>(&x[q0 + (int64_t)(c - 1) * ld])
+                                          : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int c = 0; c < KPT; ++c) {
+    bool ok = any && ja >= 1 && c < nk;
+    int64_t q = q0 + (int64_t)c * ld;
+    double e = 0.0;
+    // lane 0 needs x(ja-1), lane 31 needs x(ja+2)
+    if (ok && lane == 0 && ja >= 2) e = x[q - 1];
+    if (ok && lane == 31 && ja + 2 <= ntm) e = x[q + 2];
+    xe[c] = e;
+    if (MODE == MODE_STSK) {
+      y2[c] = ok ? *reinterpret_cast<const double2 *>(&ykm2[q]) : make_double2(0.0, 0.0);
+      uu[c] = ok ? *reinterpret_cast<const double2 *>(&u0[q]) : make_double2(0.0, 0.0);
+      dd[c] = ok ? *reinterpret_cast<const double2 *>(&dty0[q]) : make_double2(0.0, 0.0);
+    }
+  }
+  // per-row factors for rows ja (a) and ja+1 (b)
+  const int jb = ja + 1;
+  const bool ia = rowa && ja >= 2 && ja <= ntm - 1, ib = rowb && jb >= 2 && jb <= ntm - 1;
+  double sta = 0, c2a = 0, c4a = 0, stb = 0, c2b = 0, c4b = 0;
+  if (ia) {
+    sta = m.st_i[ja];
+    c2a = Dh * m.dth_i[ja] * m.dt_i[ja] * sta * m.sth[ja];
+    c4a = Dh * m.dth_i[ja + 1] * m.dt_i[ja] * sta * m.sth[ja + 1];
+  }
+  if (ib) {
+    stb = m.st_i[jb];
+    c2b = Dh * m.dth_i[jb] * m.dt_i[jb] * stb * m.sth[jb];
+    c4b = Dh * m.dth_i[jb + 1] * m.dt_i[jb] * stb * m.sth[jb + 1];
+  }
+  double rn_acc = 0.0;
+  const double ax_n = ring_in[2 * (i - 1)] * bcn;
+  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
+#pragma unroll
+  for (int c = 0; c < KPT; ++c) {
+    const int k = k0 + c;
+    const bool active = any && c < nk;
+    double2 xc = xv[c + 1];
+    double left = __shfl_up_sync(0xffffffffu, xc.y, 1);    // x(ja-1)
+    double right = __shfl_down_sync(0xffffffffu, xc.x, 1); // x(jb+1)
+    double xjm_a = (lane == 0) ? xe[c] : left;
+    double xjp_b = (lane == 31) ? xe[c] : right;
+    double pk = m.dph_i[min(k, npm)], pk1 = m.dph_i[min(k + 1, npm)], dpi = m.dp_i[min(k, npm)];
+    double axa, axb;
+    if (ja == 1) {
+      axa = ax_n;
+    } else if (ja == ntm) {
+      axa = ax_s;
+    } else {
+      double c1 = Dh * pk * dpi * sta * sta;
+      double c5 = Dh * pk1 * dpi * sta * sta;
+      double c3 = -(c1 + c2a + c4a + c5);
+      axa = c1 * xv[c].x + c2a * xjm_a + c3 * xc.x + c4a * xc.y + c5 * xv[c + 2].x;
+    }
+    if (jb == 1) {
+      axb = ax_n;
+    } else if (jb == ntm) {
+      axb = ax_s;
+    } else {
+      double c1 = Dh * pk * dpi * stb * stb;
+      double c5 = Dh * pk1 * dpi * stb * stb;
+      double c3 = -(c1 + c2b + c4b + c5);
+      axb = c1 * xv[c].y + c2b * xc.x + c3 * xc.y + c4b * xjp_b + c5 * xv[c + 2].y;
+    }
+    double ya, yb, da = 0.0, db = 0.0;
+    if (MODE == MODE_STS1) {
+      da = sc.a * axa;
+      ya = xc.x + sc.b * da;
+      db = sc.a * axb;
+      yb = xc.y + sc.b * db;
+    } else if (MODE == MODE_STSK) {
+      ya = sc.a * xc.x + sc.b * y2[c].x + sc.c * uu[c].x + sc.d * axa + sc.e * dd[c].x;
+      yb = sc.a * xc.y + sc.b * y2[c].y + sc.c * uu[c].y + sc.d * axb + sc.e * dd[c].y;
+    } else {
+      ya = xc.x + sc.a * axa;
+      yb = xc.y + sc.a * axb;
+    }
+    // ring terms of the output: rows (1,2) and (ntm-1,ntm)
+    double yb_prev = __shfl_up_sync(0xffffffffu, yb, 1);  // y(ja-1), for odd ntm
+    if (!active) continue;
+    if (ja == 1) rn_acc = rn_acc + (Dr + Dr) * (yb - ya) * m.dp[k];
+    if (jb == ntm) rn_acc = rn_acc + (Dr + Dr) * (yb - ya) * m.dp[k];
+    if (ja == ntm) rn_acc = rn_acc + (Dr + Dr) * (ya - yb_prev) * m.dp[k];
+    const int64_t q = q0 + (int64_t)c * ld;
+    double2 yv = make_double2(ya, yb);
+    // rows beyond ntm (padding) are written too: they lie inside the padded column
+    *reinterpret_cast<double2 *>(&out[q]) = yv;
+    if (k == 2) *reinterpret_cast<double2 *>(&out[q + (int64_t)(npm - 2) * ld]) = yv;
+    if (k == npm - 1) *reinterpret_cast<double2 *>(&out[q - (int64_t)(npm - 2) * ld]) = yv;
+    if (MODE == MODE_STS1) {
+      double2 dv = make_double2(da, db);
+      *reinterpret_cast<double2 *>(&out2[q]) = dv;
+      if (k == 2) *reinterpret_cast<double2 *>(&out2[q + (int64_t)(npm - 2) * ld]) = dv;
+      if (k == npm - 1) *reinterpret_cast<double2 *>(&out2[q - (int64_t)(npm - 2) * ld]) = dv;
+    }
+  }
+  // contributors: the thread owning row 1 (north) and the one owning row ntm (south)
+  const bool north = (ja == 1), south = (jb == ntm) || (ja == ntm);
+  unsigned int last = 0;
+  if ((north || south) && any) {
+    // a thread owning both poles (ntm == 2) cannot occur: ntm >= 4
+    ro.part[((int64_t)(south ? 1 : 0) * m.nr + (i - 1)) * ro.nkb + kb] = rn_acc;
+    __threadfence();
+    unsigned int old = atomicAdd(&ro.count[i - 1], 1u);
+    last = (old == 2u * (unsigned)ro.nkb - 1u) ? 1u : 0u;
+  }
+  unsigned int src_mask = __ballot_sync(0xffffffffu, last != 0);
+  if (src_mask) {
+    __threadfence();
+    double sn = 0.0, ss = 0.0;
+    for (int b = lane; b < ro.nkb; b += 32) {
+      sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + b]);
+      ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sn += __shfl_down_sync(0xffffffffu, sn, o);
+      ss += __shfl_down_sync(0xffffffffu, ss, o);
+    }
+    if (lane == 0) {
+      ro.ring[2 * (i - 1)] = sn;
+      ro.ring[2 * (i - 1) + 1] = ss;
+      ro.count[i - 1] = 0u;
+    }
+  }
+}
+
+}  // namespace hipft
