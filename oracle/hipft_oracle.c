@@ -1225,11 +1225,11 @@ static void load_data_assimilation(orc *S) {
   }
 }
 
-static void apply_data_assimilation(orc *S) {
+/* The blend of one map (npm1, ntm, 3) into every realization
+ * (src/hipft.f90:4228-4271, 4083-4146). */
+static void da_blend(orc *S, const double *map) {
   const orc_params *P = S->P;
-  if (!(S->da_active && S->time >= S->time_of_next_input_map)) return;
   int ntm = S->ntm, npm = S->npm, npm1 = S->npm1, nr = S->nr;
-  const double *map = S->da_maps + (size_t)S->da_idx * npm1 * ntm * 3; /* (npm1,ntm,3) */
   size_t plane = (size_t)npm1 * ntm;
   double *w = dalloc(plane), *d = dalloc(plane);
   double *deltaf = dalloc((size_t)ntm * npm * nr);
@@ -1263,6 +1263,12 @@ static void apply_data_assimilation(orc *S) {
   for (size_t q = 0; q < n; q++) S->f[q] = S->f[q] + deltaf[q];
   set_periodic_bc_3d(S->f, ntm, npm, nr);
   free(w); free(d); free(deltaf);
+}
+
+static void apply_data_assimilation(orc *S) {
+  if (!(S->da_active && S->time >= S->time_of_next_input_map)) return;
+  const double *map = S->da_maps + (size_t)S->da_idx * S->npm1 * S->ntm * 3; /* (npm1,ntm,3) */
+  da_blend(S, map);
   S->da_idx++;
   if (S->da_idx >= S->n_da) S->da_active = 0;
   else S->time_of_next_input_map = S->da_times[S->da_idx];
@@ -1444,4 +1450,37 @@ void orc_sizes(const orc_params *P, int n1, int n2, int *ntm, int *npm) {
   if (n1 <= 0) { n1 = P->res_np; n2 = P->res_nt; }
   *ntm = n2;
   *npm = n1 + 1;
+}
+
+/* One assimilation blend on a given field (test entry point): t[ntm], p[npm1]
+ * scales, f (ntm, npm1+1, nr) theta fastest updated in place, map3
+ * (npm1, ntm, 3).  Returns 0 on success. */
+int orc_da_blend(const orc_params *P, int ntm, int npm1, const double *t, const double *p, double *f,
+                 const double *map3) {
+  orc Sx;
+  orc *S = &Sx;
+  memset(S, 0, sizeof(*S));
+  S->P = P;
+  S->nr = P->n_realizations;
+  S->ntm1 = ntm; S->npm1 = npm1;
+  S->ntm = ntm; S->npm = npm1 + 1; S->nt = ntm + 1; S->np = npm1 + 1;
+  S->t = dalloc(ntm); S->p = dalloc(S->npm);
+  for (int j = 1; j <= ntm; j++) V1(S->t, j) = t[j - 1];
+  for (int k = 1; k <= npm1; k++) V1(S->p, k) = p[k - 1];
+  V1(S->p, npm1 + 1) = V1(S->p, 2) + twopi;
+  if (set_mesh(S)) return -1;
+  S->f = f;
+  S->n_da = 1;
+  S->da_times = NULL;
+  S->tidx0 = (int *)calloc(S->nr, sizeof(int));
+  S->tidx1 = (int *)calloc(S->nr, sizeof(int));
+  for (int r = 0; r < S->nr; r++) {
+    S->tidx0[r] = -1; S->tidx1[r] = -1;
+    for (int j = 1; j <= S->ntm; j++)
+      if (V1(S->t, j) >= P->assimilate_data_lat_limits[r] * d2r && S->tidx0[r] == -1) S->tidx0[r] = j;
+    for (int j = S->ntm; j >= 1; j--)
+      if (V1(S->t, j) <= (pi - P->assimilate_data_lat_limits[r] * d2r) && S->tidx1[r] == -1) S->tidx1[r] = j;
+  }
+  da_blend(S, map3);
+  return 0;
 }

@@ -201,15 +201,7 @@ def _ptr(a):
     return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
 
 
-def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
-        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True):
-    """Run the oracle on processed parameters ``p``.
-
-    map_pt: (nr, ntm, npm1) C-order array (i.e. Fortran (npm1,ntm,nr)), or None.
-    Returns dict(sol=(rows,nr,16), num=(rows,nr,8), f=(nr,npm,ntm) or None).
-    """
-    L = lib()
-    nr = int(p["n_realizations"])
+def _params_struct(p: dict):
     keep = []
     c = OrcParams()
     for name, typ in OrcParams._fields_:
@@ -221,6 +213,19 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
             setattr(c, name, int(p[name]))
         else:
             setattr(c, name, float(p[name]))
+    return c, keep
+
+
+def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
+        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True):
+    """Run the oracle on processed parameters ``p``.
+
+    map_pt: (nr, ntm, npm1) C-order array (i.e. Fortran (npm1,ntm,nr)), or None.
+    Returns dict(sol=(rows,nr,16), num=(rows,nr,8), f=(nr,npm,ntm) or None).
+    """
+    L = lib()
+    nr = int(p["n_realizations"])
+    c, keep = _params_struct(p)
     if map_pt is not None:
         map_pt = np.ascontiguousarray(map_pt, dtype=np.float64)
         n2, n1 = map_pt.shape[-2], map_pt.shape[-1]
@@ -255,6 +260,23 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
     n = min(h.nrows, hist_cap)
     return dict(sol=sol[:n].copy(), num=num[:n].copy(), f=f, nsteps=int(tinfo[0]),
                 time=float(tinfo[1]), cell_updates=float(tinfo[2]))
+
+
+def da_blend(p: dict, t, ph, f, map3):
+    """One assimilation blend of map3 (3, ntm, npm1) into f (nr, npm, ntm) (in place)."""
+    L = lib()
+    L.orc_da_blend.restype = ctypes.c_int
+    L.orc_da_blend.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    c, keep = _params_struct(p)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    ph = np.ascontiguousarray(ph, dtype=np.float64)
+    m = np.ascontiguousarray(map3, dtype=np.float64)
+    assert f.flags["C_CONTIGUOUS"] and f.dtype == np.float64
+    rc = L.orc_da_blend(ctypes.byref(c), len(t), len(ph), _ptr(t), _ptr(ph), _ptr(f), _ptr(m))
+    if rc:
+        raise RuntimeError("oracle da_blend failed")
+    return f
 
 
 def read_history(path: str) -> np.ndarray:
