@@ -1364,3 +1364,154 @@ extern "C" int hipft_gpu_kernel_time(hipft_gpu *h, int kind, int64_t *launches, 
   *total_ms = h->prof_ms[kind];
   return HIPFT_OK;
 }
+
+// ======================================================================
+// hipft_get_flux_noalloc: get_flux (src/hipft.f90:8672) for callers that
+// cannot allocate GPU memory.
+//
+// Some callers own every byte of device memory themselves: a Fortran code
+// that keeps its maps device-resident through OpenMP `target enter data`
+// mappings (HipFT's own model) and hands over `use_device_ptr` addresses, or
+// a host application that runs the GPU from a fixed, pre-reserved arena.
+// They cannot let a library call cudaMalloc.  This entry point takes the
+// field as a device pointer and keeps all of its scratch -- the mesh scales,
+// the cell-area weights, the per-block partial sums and the per-realization
+// results -- in one file-scope __device__ array, g_na_scratch, of fixed size
+// (kNaScratchDoubles doubles, about 1.6 MB), which every GPU that loads this
+// library holds until the process exits.
+//
+// Limits: ntm <= kNaMaxNtm, npm1 <= kNaMaxNpm1, nr <= kNaMaxNr, and the
+// partial sums (2 * nr * ceil((npm1)/16)) must fit kNaMaxPart; larger
+// requests return HIPFT_EINVAL.  The array is shared by every call on a
+// device and keeps the last call's contents, so calls that overlap on the GPU
+// (different streams, or different host threads) race; serialise them.
+// The first call on a device looks up the array's device address with
+// cudaGetSymbolAddress (with that device current) and caches it; make that
+// first call before any stream capture.
+// ======================================================================
+#include <mutex>
+
+namespace {
+constexpr int kNaMaxNtm = 16384;
+constexpr int kNaMaxNpm1 = 16384;
+constexpr int kNaMaxNr = 2000;
+constexpr int kNaMaxPart = 1 << 17;
+constexpr int kNaMaxDevices = 64;
+// layout (doubles): t[kNaMaxNtm+2] p[kNaMaxNpm1+2] da_t[kNaMaxNtm+2] da_p[kNaMaxNpm1+2] part[kNaMaxPart] out[2*kNaMaxNr]
+constexpr size_t kNaOffT = 0;
+constexpr size_t kNaOffP = kNaOffT + kNaMaxNtm + 2;
+constexpr size_t kNaOffDaT = kNaOffP + kNaMaxNpm1 + 2;
+constexpr size_t kNaOffDaP = kNaOffDaT + kNaMaxNtm + 2;
+constexpr size_t kNaOffPart = kNaOffDaP + kNaMaxNpm1 + 2;
+constexpr size_t kNaOffOut = kNaOffPart + kNaMaxPart;
+constexpr size_t kNaScratchDoubles = kNaOffOut + 2 * kNaMaxNr;
+std::mutex g_na_mutex;
+double *g_na_dev_ptr[kNaMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) double g_na_scratch[kNaScratchDoubles];
+
+// Cell-area weights of get_flux (src/hipft.f90:8712-8732) from the raw
+// scales, computed with set_mesh's definitions (6579-6641); 1-based.
+__global__ void k_na_weights(int ntm, int npm1, const double *t, const double *p, double *da_t, double *da_p) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n <= ntm) {
+    const int j = n;
+    double v;
+    if (j == 1) {
+      v = 0.25 * sin(0.5 * (t[1] + t[2])) * (t[2] - t[1]);
+    } else if (j == ntm) {
+      v = 0.25 * sin(0.5 * (t[ntm] + t[ntm - 1])) * (t[ntm] - t[ntm - 1]);
+    } else {
+      double thj = 0.5 * (t[j] + t[j - 1]), thj1 = 0.5 * (t[j + 1] + t[j]);
+      v = sin(t[j]) * (thj1 - thj);
+    }
+    da_t[j] = v;
+  }
+  if (n <= npm1) {
+    const int k = n;
+    double v;
+    if (k == 1 || k == npm1) {
+      v = 0.5 * (p[npm1] - p[npm1 - 1]);
+    } else {
+      double phk = 0.5 * (p[k] + p[k - 1]), phk1 = 0.5 * (p[k + 1] + p[k]);
+      v = phk1 - phk;
+    }
+    da_p[k] = v;
+  }
+}
+
+// Per-realization totals of the block partials, in block order.
+__global__ void k_na_flux_final(int nb, int nr, const double *part, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nr) return;
+  double fp = 0.0, fm = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    fp = fp + part[((int64_t)i * nb + b) * 2];
+    fm = fm + part[((int64_t)i * nb + b) * 2 + 1];
+  }
+  out[2 * i] = fp;
+  out[2 * i + 1] = fm;
+}
+
+static int na_fail(char *err, size_t len, int code, const char *msg) {
+  if (err && len) std::snprintf(err, len, "hipft_get_flux_noalloc: %s", msg);
+  return code;
+}
+
+extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, int nr, int ldt, const double *t,
+                                      const double *p, double *flux_p, double *flux_m, void *cuda_stream,
+                                      char *err, size_t err_len) {
+  if (!f_dev || !t || !p || !flux_p || !flux_m) return na_fail(err, err_len, HIPFT_EINVAL, "null argument");
+  if (ntm < 4 || npm1 < 5 || nr < 1 || ldt < ntm)
+    return na_fail(err, err_len, HIPFT_EINVAL, "sizes out of range (ntm >= 4, npm1 >= 5, nr >= 1, ldt >= ntm)");
+  const int cpb = 16;
+  const int npm = npm1 + 1;
+  const int nb = (npm - 1 + cpb - 1) / cpb;
+  if (ntm > kNaMaxNtm || npm1 > kNaMaxNpm1 || nr > kNaMaxNr || (size_t)2 * nr * nb > (size_t)kNaMaxPart)
+    return na_fail(err, err_len, HIPFT_EINVAL,
+                   "grid too large for the fixed scratch (ntm <= 16384, npm1 <= 16384, nr <= 2000, "
+                   "2*nr*ceil(npm1/16) <= 131072)");
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices)
+    return na_fail(err, err_len, HIPFT_ECUDA, "no usable current device");
+  double *base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_na_mutex);
+    if (!g_na_dev_ptr[dev]) {
+      double *ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_na_scratch);
+      if (e != cudaSuccess || !ptr) return na_fail(err, err_len, HIPFT_ECUDA, cudaGetErrorString(e));
+      g_na_dev_ptr[dev] = ptr;
+    }
+    base = g_na_dev_ptr[dev];
+  }
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  double *dt = base + kNaOffT, *dp = base + kNaOffP, *dat = base + kNaOffDaT, *dap = base + kNaOffDaP;
+  double *part = base + kNaOffPart, *out = base + kNaOffOut;
+  // 1-based scales
+  if (cudaMemcpyAsync(dt + 1, t, sizeof(double) * ntm, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(dp + 1, p, sizeof(double) * npm1, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return na_fail(err, err_len, HIPFT_ECUDA, "copy of the scales failed");
+  int nmax = ntm > npm1 ? ntm : npm1;
+  k_na_weights<<<(nmax + 255) / 256, 256, 0, s>>>(ntm, npm1, dt, dp, dat, dap);
+  Mesh m{};
+  m.ntm = ntm;
+  m.npm = npm;
+  m.nt = ntm + 1;
+  m.np = npm;
+  m.nr = nr;
+  m.ldt = ldt;
+  m.plane = (int64_t)ldt * npm;
+  k_flux_partial<<<dim3((unsigned)nb, (unsigned)nr), 256, 0, s>>>(m, dat, dap, f_dev, 0, part, cpb);
+  k_na_flux_final<<<(nr + 127) / 128, 128, 0, s>>>(nb, nr, part, out);
+  if (cudaPeekAtLastError() != cudaSuccess) return na_fail(err, err_len, HIPFT_ECUDA, "kernel launch failed");
+  if (cudaMemcpy2DAsync(flux_p, sizeof(double), out, 2 * sizeof(double), sizeof(double), (size_t)nr,
+                        cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemcpy2DAsync(flux_m, sizeof(double), out + 1, 2 * sizeof(double), sizeof(double), (size_t)nr,
+                        cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return na_fail(err, err_len, HIPFT_ECUDA, "copy of the results failed");
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return na_fail(err, err_len, HIPFT_ECUDA, cudaGetErrorString(e));
+  return HIPFT_OK;
+}

@@ -103,6 +103,9 @@ SIGNATURES = [
     ("hipft_gpu_synchronize", ctypes.c_int, [_H]),
     ("hipft_run", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int]),
     ("hipft_run_field", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, DPTR, ctypes.c_size_t]),
+    ("hipft_get_flux_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              DPTR, DPTR, DPTR, DPTR, ctypes.c_void_p, ctypes.c_char_p,
+                                              ctypes.c_size_t]),
     ("hipft_h5_read", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
                                      DPTR, DPTR, DPTR, DPTR]),
 ]

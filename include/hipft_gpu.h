@@ -214,6 +214,25 @@ int hipft_gpu_kernel_time(hipft_gpu *h, int kind, int64_t *launches, double *tot
 int hipft_gpu_set_stream(hipft_gpu *h, void *cuda_stream);
 int hipft_gpu_synchronize(hipft_gpu *h);
 
+/* ---- allocation-free flux integral ------------------------------------------ */
+
+/* No counterpart in the reference: get_flux (src/hipft.f90:8672) for callers
+ * that cannot allocate GPU memory -- e.g. a Fortran code whose maps live in
+ * OpenMP `target enter data` mappings and are handed over as use_device_ptr
+ * addresses, or an application that runs the GPU from a fixed arena.  It
+ * allocates nothing: f_dev is the caller's device field f(j,k,i) at
+ * f_dev[((i-1)*(npm1+1) + (k-1))*ldt + (j-1)] (ldt >= ntm), t/p are the host
+ * scales, flux_p/flux_m receive nr values each.  Its scratch is one
+ * file-scope device array of about 1.6 MB that every GPU loading the library
+ * keeps until exit; it bounds the sizes to ntm <= 16384, npm1 <= 16384,
+ * nr <= 2000 and 2*nr*ceil(npm1/16) <= 131072 (else HIPFT_EINVAL).  Calls
+ * share that scratch, so calls that overlap on the GPU race.  The first call
+ * on a device looks up the scratch address (do it before any stream
+ * capture).  err (may be NULL) receives a message on failure. */
+int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, int nr, int ldt, const double *t,
+                           const double *p, double *flux_p, double *flux_m, void *cuda_stream, char *err,
+                           size_t err_len);
+
 /* ---- standalone driver ----------------------------------------------------- */
 
 /* Runs `program HIPFT` (src/hipft.f90:869-968) for the hot-path subset: reads
