@@ -53,15 +53,6 @@ WORKLOADS = {
 }
 
 
-def split_realizations(nr: int, world: int, rank: int):
-    """Block split of realizations over ranks, remainder to the low ranks
-    (src/hipft.f90:1033-1050).  Returns (first index, count)."""
-    base, rem = divmod(nr, world)
-    cnt = base + (1 if rank < rem else 0)
-    first = rank * base + min(rank, rem)
-    return first, cnt
-
-
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -199,6 +190,7 @@ def run_gpu(args, wl, name):
     torch.cuda.set_device(local)
     import hipft_b200 as H
     from hipft_b200 import synthetic as S
+    from hipft_b200.parallel import reduce_timing, split_realizations
 
     t, p, br, prm = make_inputs(wl)
     first, nrl = split_realizations(wl["nr"], world, rank)
@@ -272,12 +264,10 @@ def run_gpu(args, wl, name):
     e2e_cells = float(i3.cell_stage_updates - i2.cell_stage_updates)
 
     if dist:
-        tt = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        cc = torch.tensor([cells, e2e_cells, float(launches)], dtype=torch.float64, device="cuda")
-        dist.all_reduce(cc, op=dist.ReduceOp.SUM)
-        ms, e2e_ms = float(tt[0]), float(tt[1])
-        cells, e2e_cells, launches = float(cc[0]), float(cc[1]), int(cc[2])
+        ms, cells = reduce_timing(dist, "cuda", ms, cells)
+        e2e_ms, e2e_cells = reduce_timing(dist, "cuda", e2e_ms, e2e_cells)
+        _, launches = reduce_timing(dist, "cuda", 0.0, float(launches))
+        launches = int(launches)
 
     peak, peak_kind = measured_peak()
     bytes_per_launch = STS_BYTES_PER_CELL * ntm * (npm - 2) * nrl

@@ -38,7 +38,7 @@ constexpr double c_sixth = 0.16666666666666666;
 constexpr double c_two_third = 0.66666666666666666;
 constexpr double c_third = 0.33333333333333333;
 
-constexpr int kNBuf = 4;  // current field + 3 scratch fields
+constexpr int kNBuf = 6;  // current field + 5 scratch fields (two-stage RKG2 needs two fresh outputs)
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 double pow3(double c) { return c * c * c; }
@@ -89,6 +89,7 @@ struct hipft_gpu {
   double *d_rpart = nullptr;
   unsigned int *d_rcount = nullptr;
   int nkb = 0;
+  int *d_err = nullptr;   // set by kernels whose bounded waits gave up
   unsigned long long *d_bits = nullptr;
   double *d_part = nullptr;
   size_t part_cap = 0;
@@ -372,6 +373,32 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
+// Two-stage kernel on/off (HIPFT_STS_PAIR=0 disables it, for A/B timing).
+static bool sts_pairs_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_STS_PAIR");
+    v = (e && std::atoi(e) == 0) ? 0 : 1;
+  }
+  return v == 1;
+}
+
+static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
+                    double *out_k, double *out_k1, StageCoef ca, StageCoef cb) {
+  const int nkt = (h->npm - 2 + kPK - 1) / kPK;
+  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
+  dim3 grd((unsigned)((h->ntm + kPJ - 1) / kPJ), (unsigned)nkt, (unsigned)h->nr);
+  {
+    ProfScope ps(h, HIPFT_K_STS);
+    k_sts_pair<<<grd, kPThreads, kPairSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1,
+                                                          h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
+                                                          PairArgs{ca, cb, h->d_err}, ro);
+    LAUNCHED(h);
+  }
+  h->ring_cur = 1 - h->ring_cur;
+  return HIPFT_OK;
+}
+
 template <int MODE>
 static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
                            double *out, double *out2, const double *ring, StageCoef sc,
@@ -484,6 +511,10 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   if ((rc = dalloc(h, &h->d_ringbuf[1], 2 * (size_t)nr))) return bail(rc);
   if ((rc = dalloc(h, &h->d_rpart, 2 * (size_t)nr * h->nkb))) return bail(rc);
   if ((rc = dalloc(h, &h->d_rcount, (size_t)nr))) return bail(rc);
+  if ((rc = dalloc(h, &h->d_err, 1))) return bail(rc);
+  if (cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
+  if (cudaFuncSetAttribute(k_sts_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem) != cudaSuccess)
+    return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernel"));
   if (cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned int) * nr, h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   if ((rc = dalloc(h, &h->d_bits, 4))) return bail(rc);
   if (cudaMallocHost((void **)&h->h_pin, sizeof(double) * std::max<size_t>(64, (size_t)nr * kNPart)) !=
@@ -942,10 +973,30 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
                                    StageCoef{dtl, h->sts_ubj[1], 0, 0, 0}, nullptr));
   }
   int ykm1 = ia, ykm2 = u0;
-  for (int64_t k = 2; k <= h->sts_s; ++k) {
-    int out = (k == 2) ? ib : ykm2;
+  auto coef = [&](int64_t k) {
     double uj = h->sts_uj[k], vj = h->sts_vj[k];
-    StageCoef sc{uj, vj, 1.0 - uj - vj, h->sts_ubj[k] * dtl, h->sts_gj[k]};
+    return StageCoef{uj, vj, 1.0 - uj - vj, h->sts_ubj[k] * dtl, h->sts_gj[k]};
+  };
+  // a buffer not holding u0, dty0, Y_{k-1}, Y_{k-2} (or `avoid`)
+  auto free_buf = [&](int avoid) {
+    for (int b = 0; b < kNBuf; ++b)
+      if (b != u0 && b != idty && b != ykm1 && b != ykm2 && b != avoid) return b;
+    return -1;
+  };
+  (void)ib;
+  int64_t k = 2;
+  while (k <= h->sts_s) {
+    if (fused && sts_pairs_enabled() && k + 1 <= h->sts_s) {
+      int bk = free_buf(-1), bk1 = free_buf(bk);
+      TRY(sts_pair(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[bk], h->buf[bk1], coef(k),
+                   coef(k + 1)));
+      ykm2 = bk;
+      ykm1 = bk1;
+      k += 2;
+      continue;
+    }
+    int out = (ykm2 == u0) ? free_buf(-1) : ykm2;
+    StageCoef sc = coef(k);
     if (fused) {
       TRY(sts_stage_v2<MODE_STSK>(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[out], nullptr,
                                   sc));
@@ -956,6 +1007,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
     }
     ykm2 = ykm1;
     ykm1 = out;
+    k += 1;
   }
   h->cur = ykm1;
   h->dring_valid = fused;  // the last fused stage left the ring of the new field
@@ -1051,6 +1103,16 @@ extern "C" int hipft_gpu_diffusion_step(hipft_gpu *h, double dtl, hipft_cycle_cb
     i = i + 1;
   }
   if (h->auto_sc) h->subcycles_state = i;
+  {
+    int ev = 0;
+    CK(h, cudaMemcpyAsync(&ev, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    if (ev) {
+      CK(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+      CK(h, cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned int) * h->nr, h->stream));
+      return fail(h, HIPFT_ETIMEOUT, "diffusion_step: a bounded wait for staged tiles gave up");
+    }
+  }
   if (info) {
     info->dtime_diffusion_euler = h->dt_euler;
     info->sts_s = (h->P.diffusion_num_method == 1) ? h->n_euler : h->sts_s;

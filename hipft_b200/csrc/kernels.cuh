@@ -1160,3 +1160,276 @@ __global__ void __launch_bounds__(128, 4) k_sts_stage_v3(Mesh m, const double *_
 }
 
 }  // namespace hipft
+
+namespace hipft {
+
+// ---------------------------------------------------- bulk-copy helpers
+// 1-D TMA (cp.async.bulk) global -> shared copies completed on an mbarrier.
+// Every copy is 16-byte aligned at both ends and a multiple of 16 bytes.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t phase) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false if the copies did not land within the limit.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+
+// ------------------------------------------- two RKG2 stages per launch
+// Temporal blocking of stages k and k+1 (src/hipft.f90:5222-5237) for a
+// constant-per-realization D.  A CTA owns a tile of TJ theta rows x TK phi
+// columns.  Phase 1 stages, with 1-D TMA copies of whole theta runs, Y_{k-1}
+// on the tile plus a halo of 2 and Y_{k-2}, u0, dty0 plus a halo of 1 in
+// shared memory (phi halos wrap periodically; theta runs are clipped at the
+// poles).  Phase 2 computes Y_k on the tile plus a halo of 1 in shared memory
+// (in place of Y_{k-2}) and writes its tile; phase 3 computes Y_{k+1} on the
+// tile from shared memory and writes it.  Per cell and stage pair the HBM
+// traffic is 4 reads + 2 writes instead of 2 x (4 reads + 1 write).
+//
+// The pole rows of Y_{k+1} need ring sums over all phi of the intermediate
+// Y_k (src/hipft.f90:7969-7979).  CTAs holding rows 1-2 / ntm-1..ntm publish
+// per-tile partials of those sums; the last of them (atomic counter, no
+// waiting) reduces the partials in tile order, computes both pole rows of
+// Y_{k+1} for every phi column, then the ring sums of Y_{k+1} for the next
+// launch.
+constexpr int kPJ = 128;          // theta rows per tile
+constexpr int kPK = 16;           // phi columns per tile
+constexpr int kPR = kPJ + 4;      // shared rows per column (halo 2 each side)
+constexpr int kPC = kPK + 4;      // shared columns (halo 2 each side)
+constexpr int kPThreads = 256;
+constexpr size_t kPairSmem = (size_t)4 * kPC * kPR * sizeof(double) + 64;
+
+struct PairArgs {
+  StageCoef ca, cb;     // stages k and k+1
+  int *err;             // set to 1 when a bounded wait gives up
+};
+
+__global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double *__restrict__ dfac,
+                                                           const double *__restrict__ ykm1,
+                                                           const double *__restrict__ ykm2,
+                                                           const double *__restrict__ u0,
+                                                           const double *__restrict__ dty0, double *out_k,
+                                                           double *out_k1, const double *__restrict__ ring_in,
+                                                           double bcn, double bcs, PairArgs pa, RingOut ro) {
+  extern __shared__ __align__(128) double psm[];
+  double *sX1 = psm;                   // Y_{k-1}
+  double *sYk = psm + kPC * kPR;       // Y_{k-2}, overwritten by Y_k
+  double *sU = psm + 2 * kPC * kPR;    // u0
+  double *sD = psm + 3 * kPC * kPR;    // dty0
+  uint64_t *bar = reinterpret_cast<uint64_t *>(psm + 4 * kPC * kPR);
+  __shared__ double red[2][kPThreads / 32];
+  __shared__ int s_last;
+
+  const int tid = threadIdx.x;
+  const int ntm = m.ntm, npm = m.npm;
+  const int64_t ld = m.ldt;
+  const int j0 = blockIdx.x * kPJ + 1;
+  const int kt = blockIdx.y;
+  const int k0 = kt * kPK + 2;
+  const int i = blockIdx.z + 1;
+  const int nk = min(kPK, npm - 1 - k0 + 1);  // interior columns of this tile
+  const int64_t pbase = (int64_t)(i - 1) * m.plane;
+  auto sidx = [](int c, int r) { return c * kPR + r; };  // c: column k0-2+c, r: row j0-2+r
+  auto wrapc = [&](int c) {
+    if (c < 1) return c + (npm - 2);
+    if (c > npm) return c - (npm - 2);
+    return c;
+  };
+
+  // ---- phase 1: TMA loads of whole theta runs
+  const int rs = max(1, j0 - 2);
+  const int re = min((int)ld, j0 + kPJ + 1);
+  const uint32_t run_bytes = (uint32_t)(re - rs + 1) * 8u;
+  const int roff = rs - (j0 - 2);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t ncopy = (uint32_t)(nk + 4) + 3u * (uint32_t)(nk + 2);
+    mbar_expect_tx(bar, ncopy * run_bytes);
+    for (int c = 0; c < nk + 4; ++c) {
+      const int kg = wrapc(k0 - 2 + c);
+      bulk_load(&sX1[sidx(c, roff)], ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1), run_bytes, bar);
+    }
+    for (int c = 1; c < nk + 3; ++c) {
+      const int kg = wrapc(k0 - 2 + c);
+      const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
+      bulk_load(&sYk[sidx(c, roff)], ykm2 + g, run_bytes, bar);
+      bulk_load(&sU[sidx(c, roff)], u0 + g, run_bytes, bar);
+      bulk_load(&sD[sidx(c, roff)], dty0 + g, run_bytes, bar);
+    }
+  }
+  const double Dr = dfac[i];
+  const double Dh = kHalf * (Dr + Dr);
+  const double ax_n = ring_in[2 * (i - 1)] * bcn;
+  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
+  if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
+    if (tid == 0) atomicExch(pa.err, 1);
+    mbar_wait_bounded(bar, 0, 1u << 22);  // let copies still in flight land before exiting
+    return;
+  }
+
+  // ---- phase 2: Y_k on rows j0-1..j0+TJ, columns k0-1..k0+nk (shared, in place of Y_{k-2})
+  const int nr2 = kPJ + 2, nc2 = nk + 2;
+  for (int e = tid; e < nr2 * nc2; e += kPThreads) {
+    const int r = 1 + e % nr2;  // shared row
+    const int c = 1 + e / nr2;  // shared column
+    const int j = j0 - 2 + r;
+    if (j < 1 || j > ntm) continue;
+    const int kw = wrapc(k0 - 2 + c) == npm ? 2 : (wrapc(k0 - 2 + c) == 1 ? npm - 1 : wrapc(k0 - 2 + c));
+    double ax;
+    if (j == 1) {
+      ax = ax_n;
+    } else if (j == ntm) {
+      ax = ax_s;
+    } else {
+      const double sti = m.st_i[j];
+      const double c1 = Dh * m.dph_i[kw] * m.dp_i[kw] * sti * sti;
+      const double c2 = Dh * m.dth_i[j] * m.dt_i[j] * sti * m.sth[j];
+      const double c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * sti * m.sth[j + 1];
+      const double c5 = Dh * m.dph_i[kw + 1] * m.dp_i[kw] * sti * sti;
+      const double c3 = -(c1 + c2 + c4 + c5);
+      ax = c1 * sX1[sidx(c - 1, r)] + c2 * sX1[sidx(c, r - 1)] + c3 * sX1[sidx(c, r)] +
+           c4 * sX1[sidx(c, r + 1)] + c5 * sX1[sidx(c + 1, r)];
+    }
+    const StageCoef &s = pa.ca;
+    const double y = s.a * sX1[sidx(c, r)] + s.b * sYk[sidx(c, r)] + s.c * sU[sidx(c, r)] + s.d * ax +
+                     s.e * sD[sidx(c, r)];
+    sYk[sidx(c, r)] = y;
+    // tile interior goes to HBM (plus its seam copies)
+    if (r >= 2 && r < 2 + kPJ && c >= 2 && c < 2 + nk) {
+      const int k = k0 - 2 + c;
+      const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
+      out_k[q] = y;
+      if (k == 2) out_k[q + (int64_t)(npm - 2) * ld] = y;
+      if (k == npm - 1) out_k[q - (int64_t)(npm - 2) * ld] = y;
+    }
+  }
+  __syncthreads();
+
+  // ---- ring partials of Y_k over this tile's columns
+  // The CTAs whose tile holds row 2 (north) or row ntm-1 (south) publish
+  // ring partials; they also write rows 2 and ntm-1 of Y_{k+1}, which the
+  // last of them reads back below.
+  const bool has_n = (j0 == 1);
+  const bool has_s = (ntm - 1 >= j0 && ntm - 1 <= j0 + kPJ - 1);
+  if (tid == 0 && (has_n || has_s)) {
+    if (has_n) {
+      double acc = 0.0;
+      for (int c = 2; c < 2 + nk; ++c)
+        acc = acc + (Dr + Dr) * (sYk[sidx(c, 3)] - sYk[sidx(c, 2)]) * m.dp[k0 - 2 + c];
+      ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
+    }
+    if (has_s) {
+      const int rS = ntm - (j0 - 2);
+      double acc = 0.0;
+      for (int c = 2; c < 2 + nk; ++c)
+        acc = acc + (Dr + Dr) * (sYk[sidx(c, rS)] - sYk[sidx(c, rS - 1)]) * m.dp[k0 - 2 + c];
+      ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
+    }
+  }
+
+  // ---- phase 3: Y_{k+1} on the tile interior (pole rows are finished below)
+  for (int e = tid; e < kPJ * nk; e += kPThreads) {
+    const int r = 2 + e % kPJ;
+    const int c = 2 + e / kPJ;
+    const int j = j0 - 2 + r;
+    if (j < 2 || j > ntm - 1) continue;
+    const int k = k0 - 2 + c;
+    const double sti = m.st_i[j];
+    const double c1 = Dh * m.dph_i[k] * m.dp_i[k] * sti * sti;
+    const double c2 = Dh * m.dth_i[j] * m.dt_i[j] * sti * m.sth[j];
+    const double c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * sti * m.sth[j + 1];
+    const double c5 = Dh * m.dph_i[k + 1] * m.dp_i[k] * sti * sti;
+    const double c3 = -(c1 + c2 + c4 + c5);
+    const double ax = c1 * sYk[sidx(c - 1, r)] + c2 * sYk[sidx(c, r - 1)] + c3 * sYk[sidx(c, r)] +
+                      c4 * sYk[sidx(c, r + 1)] + c5 * sYk[sidx(c + 1, r)];
+    const StageCoef &s = pa.cb;
+    const double y = s.a * sYk[sidx(c, r)] + s.b * sX1[sidx(c, r)] + s.c * sU[sidx(c, r)] + s.d * ax +
+                     s.e * sD[sidx(c, r)];
+    const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
+    out_k1[q] = y;
+    if (k == 2) out_k1[q + (int64_t)(npm - 2) * ld] = y;
+    if (k == npm - 1) out_k1[q - (int64_t)(npm - 2) * ld] = y;
+  }
+
+  // ---- publish: the last pole-holding CTA of realization i finishes the poles
+  const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
+  if (contrib == 0) return;
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned int old = atomicAdd(&ro.count[i - 1], (unsigned)contrib);
+    s_last = (old + (unsigned)contrib == 2u * (unsigned)ro.nkb) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // ring sums of Y_k in tile order (fixed tree)
+  double sn = 0.0, ss = 0.0;
+  for (int b = tid; b < ro.nkb; b += kPThreads) {
+    sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + b]);
+    ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
+  }
+  block_sum2(sn, ss, &red[0][0]);
+  __shared__ double s_ring[2];
+  if (tid == 0) {
+    s_ring[0] = sn;
+    s_ring[1] = ss;
+  }
+  __syncthreads();
+  const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
+  // pole rows of Y_{k+1} for every column, then the ring sums of Y_{k+1}
+  const StageCoef &s = pa.cb;
+  double rn = 0.0, rsum = 0.0;
+  for (int k = 1 + tid; k <= npm; k += kPThreads) {
+    const int64_t qn = pbase + (int64_t)(k - 1) * ld;  // row 1
+    const int64_t qs = qn + (ntm - 1);                 // row ntm
+    // Y_k at the pole rows, recomputed from the inputs (stage k's pole rows
+    // use the input's ring sums), so no other CTA's stores are needed here
+    const StageCoef &sa = pa.ca;
+    const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
+    const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
+    const double yn = s.a * ykn + s.b * ykm1[qn] + s.c * u0[qn] + s.d * axn1 + s.e * dty0[qn];
+    const double ys = s.a * yks + s.b * ykm1[qs] + s.c * u0[qs] + s.d * axs1 + s.e * dty0[qs];
+    out_k1[qn] = yn;
+    out_k1[qs] = ys;
+    if (k >= 2 && k <= npm - 1) {
+      rn = rn + (Dr + Dr) * (__ldcg(&out_k1[qn + 1]) - yn) * m.dp[k];
+      rsum = rsum + (Dr + Dr) * (ys - __ldcg(&out_k1[qs - 1])) * m.dp[k];
+    }
+  }
+  block_sum2(rn, rsum, &red[0][0]);
+  if (tid == 0) {
+    ro.ring[2 * (i - 1)] = rn;
+    ro.ring[2 * (i - 1) + 1] = rsum;
+    ro.count[i - 1] = 0u;
+  }
+}
+
+}  // namespace hipft
