@@ -373,12 +373,13 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
-// Two-stage kernel on/off (HIPFT_STS_PAIR=0 disables it, for A/B timing).
+// Two RKG2 stages per launch (k_sts_pair) when HIPFT_STS_PAIR=1; off by
+// default until it is faster than the single-stage kernel.
 static bool sts_pairs_enabled() {
   static int v = -1;
   if (v < 0) {
     const char *e = std::getenv("HIPFT_STS_PAIR");
-    v = (e && std::atoi(e) == 0) ? 0 : 1;
+    v = (e && std::atoi(e) == 1) ? 1 : 0;
   }
   return v == 1;
 }
