@@ -245,6 +245,7 @@ def run_gpu(args, wl, name):
     g.set_profiling(False)
     cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
     launches = int(i1.kernel_launches - i0.kernel_launches)
+    rkg2_stages = int(i1.rkg2_stages - i0.rkg2_stages)
 
     # end to end through the C ABI with host buffers
     f_host = torch.empty((nrl, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
@@ -270,15 +271,20 @@ def run_gpu(args, wl, name):
         launches = int(launches)
 
     peak, peak_kind = measured_peak()
-    bytes_per_launch = STS_BYTES_PER_CELL * ntm * (npm - 2) * nrl
+    # Algorithmic bytes: 40 B per unique cell per RKG2 stage (read Y_{k-1},
+    # Y_{k-2}, u0, dty0; write Y_k), times the stages one launch advances.
+    stages_per_launch = rkg2_stages / max(sts_n, 1)
+    bytes_per_launch = STS_BYTES_PER_CELL * ntm * (npm - 2) * nrl * stages_per_launch
     sts_avg_ms = sts_ms / max(sts_n, 1)
     achieved = bytes_per_launch / (sts_avg_ms * 1e-3) / 1e9 if sts_n else None
-    traffic = None
+    traffic, traffic_src = None, None
     tpath = os.path.join(ROOT, "profiles", "sts_stage_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as fh:
             tj = json.load(fh)
-        traffic = tj["dram_bytes_per_cell"] * ntm * (npm - 2) * nrl
+        if abs(tj.get("stages_per_launch", 1) - stages_per_launch) < 1e-9:
+            traffic = tj["dram_bytes_per_cell"] * ntm * (npm - 2) * nrl
+            traffic_src = tj["source"]
     out = {
         "metric": METRIC, "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -287,7 +293,10 @@ def run_gpu(args, wl, name):
                    "realizations_per_gpu": nrl, "dt_hours": dt, "parallelism": f"realizations/{world}",
                    "method": "WENO3+SSPRK(4,3) Strang-split with RKG2 (PTL subcycles), DA every 24 h",
                    "l2": "inputs larger than L2 (%.2f GB per field), no flush" % (ntm * npm * nrl * 8 / 1e9)},
-        "roofline": {"bound": "hbm", "kernel": "k_diffusion_stage<MODE_STSK> (fused RKG2 stage)",
+        "roofline": {"bound": "hbm",
+                     "kernel": ("k_sts_pair (two fused RKG2 stages per launch)" if stages_per_launch > 1.5
+                                else "k_sts_stage_v3<MODE_STSK> (fused RKG2 stage)"),
+                     "stages_per_launch": stages_per_launch, "traffic_source": traffic_src,
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "launches": sts_n, "avg_launch_ms": sts_avg_ms,

@@ -106,6 +106,7 @@ struct hipft_gpu {
   int *d_tidx = nullptr;
   std::string err;
   int64_t launches = 0, cell_updates = 0;
+  int64_t rkg2_stages = 0;  // RKG2/RKL2 stages k >= 2 run (fused kernels)
   // optional per-kernel event timing
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -373,13 +374,13 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
-// Two RKG2 stages per launch (k_sts_pair) when HIPFT_STS_PAIR=1; off by
-// default until it is faster than the single-stage kernel.
+// Two RKG2 stages per launch (k_sts_pair); HIPFT_STS_PAIR=0 falls back to
+// one stage per launch (A/B timing).
 static bool sts_pairs_enabled() {
   static int v = -1;
   if (v < 0) {
     const char *e = std::getenv("HIPFT_STS_PAIR");
-    v = (e && std::atoi(e) == 1) ? 1 : 0;
+    v = (e && std::atoi(e) == 0) ? 0 : 1;
   }
   return v == 1;
 }
@@ -994,6 +995,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
       ykm2 = bk;
       ykm1 = bk1;
       k += 2;
+      h->rkg2_stages += 2;
       continue;
     }
     int out = (ykm2 == u0) ? free_buf(-1) : ykm2;
@@ -1009,6 +1011,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
     ykm2 = ykm1;
     ykm1 = out;
     k += 1;
+    h->rkg2_stages += 1;
   }
   h->cur = ykm1;
   h->dring_valid = fused;  // the last fused stage left the ring of the new field
@@ -1369,6 +1372,7 @@ extern "C" int hipft_gpu_info(const hipft_gpu *h, hipft_info *info) {
   info->kernel_launches = h->launches;
   info->cell_stage_updates = h->cell_updates;
   info->device_bytes = h->dev_bytes;
+  info->rkg2_stages = h->rkg2_stages;
   return HIPFT_OK;
 }
 

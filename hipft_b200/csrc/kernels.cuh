@@ -1216,18 +1216,19 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase,
 // Y_{k+1} for every phi column, then the ring sums of Y_{k+1} for the next
 // launch.
 constexpr int kPJ = 128;          // theta rows per tile
-constexpr int kPK = 16;           // phi columns per tile
+constexpr int kPK = 8;            // phi columns per tile
 constexpr int kPR = kPJ + 4;      // shared rows per column (halo 2 each side)
 constexpr int kPC = kPK + 4;      // shared columns (halo 2 each side)
 constexpr int kPThreads = 256;
-constexpr size_t kPairSmem = (size_t)4 * kPC * kPR * sizeof(double) + 64;
+// 4 staged arrays, per-row tables (st_i, c2, c4), per-column tables (P1, P5), mbarrier
+constexpr size_t kPairSmem = ((size_t)4 * kPC * kPR + 3 * kPR + 2 * kPC) * sizeof(double) + 64;
 
 struct PairArgs {
   StageCoef ca, cb;     // stages k and k+1
   int *err;             // set to 1 when a bounded wait gives up
 };
 
-__global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double *__restrict__ dfac,
+__global__ void __launch_bounds__(kPThreads, 4) k_sts_pair(Mesh m, const double *__restrict__ dfac,
                                                            const double *__restrict__ ykm1,
                                                            const double *__restrict__ ykm2,
                                                            const double *__restrict__ u0,
@@ -1239,8 +1240,14 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double 
   double *sYk = psm + kPC * kPR;       // Y_{k-2}, overwritten by Y_k
   double *sU = psm + 2 * kPC * kPR;    // u0
   double *sD = psm + 3 * kPC * kPR;    // dty0
-  uint64_t *bar = reinterpret_cast<uint64_t *>(psm + 4 * kPC * kPR);
+  double *tST = psm + 4 * kPC * kPR;   // st_i(j) per shared row
+  double *tC2 = tST + kPR;             // c2(j)
+  double *tC4 = tC2 + kPR;             // c4(j)
+  double *tP1 = tC4 + kPR;             // (Dh*dph_i(k))*dp_i(k) per shared column
+  double *tP5 = tP1 + kPC;             // (Dh*dph_i(k+1))*dp_i(k)
+  uint64_t *bar = reinterpret_cast<uint64_t *>(tP5 + kPC);
   __shared__ double red[2][kPThreads / 32];
+  __shared__ double s_ring[2];
   __shared__ int s_last;
 
   const int tid = threadIdx.x;
@@ -1252,7 +1259,7 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double 
   const int i = blockIdx.z + 1;
   const int nk = min(kPK, npm - 1 - k0 + 1);  // interior columns of this tile
   const int64_t pbase = (int64_t)(i - 1) * m.plane;
-  auto sidx = [](int c, int r) { return c * kPR + r; };  // c: column k0-2+c, r: row j0-2+r
+#define SIDX(c, r) ((c) * kPR + (r))       // c: column k0-2+c, r: row j0-2+r
   auto wrapc = [&](int c) {
     if (c < 1) return c + (npm - 2);
     if (c > npm) return c - (npm - 2);
@@ -1274,55 +1281,74 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double 
     mbar_expect_tx(bar, ncopy * run_bytes);
     for (int c = 0; c < nk + 4; ++c) {
       const int kg = wrapc(k0 - 2 + c);
-      bulk_load(&sX1[sidx(c, roff)], ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1), run_bytes, bar);
+      bulk_load(&sX1[SIDX(c, roff)], ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1), run_bytes, bar);
     }
     for (int c = 1; c < nk + 3; ++c) {
       const int kg = wrapc(k0 - 2 + c);
       const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
-      bulk_load(&sYk[sidx(c, roff)], ykm2 + g, run_bytes, bar);
-      bulk_load(&sU[sidx(c, roff)], u0 + g, run_bytes, bar);
-      bulk_load(&sD[sidx(c, roff)], dty0 + g, run_bytes, bar);
+      bulk_load(&sYk[SIDX(c, roff)], ykm2 + g, run_bytes, bar);
+      bulk_load(&sU[SIDX(c, roff)], u0 + g, run_bytes, bar);
+      bulk_load(&sD[SIDX(c, roff)], dty0 + g, run_bytes, bar);
     }
   }
   const double Dr = dfac[i];
   const double Dh = kHalf * (Dr + Dr);
   const double ax_n = ring_in[2 * (i - 1)] * bcn;
   const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
-  if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
+  // coefficient tables, in load_diffusion_matrix's operation order, while the copies fly
+  for (int r = tid; r < kPR; r += kPThreads) {
+    const int j = j0 - 2 + r;
+    double st = 0.0, c2 = 0.0, c4 = 0.0;
+    if (j >= 2 && j <= ntm - 1) {
+      st = m.st_i[j];
+      c2 = Dh * m.dth_i[j] * m.dt_i[j] * st * m.sth[j];
+      c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * st * m.sth[j + 1];
+    }
+    tST[r] = st;
+    tC2[r] = c2;
+    tC4[r] = c4;
+  }
+  for (int c = tid; c < kPC; c += kPThreads) {
+    const int kc = wrapc(k0 - 2 + c);
+    const int kw = kc == npm ? 2 : (kc == 1 ? npm - 1 : kc);  // seam columns take their twins' metrics
+    tP1[c] = Dh * m.dph_i[kw] * m.dp_i[kw];
+    tP5[c] = Dh * m.dph_i[kw + 1] * m.dp_i[kw];
+  }
+  const bool landed = mbar_wait_bounded(bar, 0, 1u << 22);
+  if (!landed) {
     if (tid == 0) atomicExch(pa.err, 1);
     mbar_wait_bounded(bar, 0, 1u << 22);  // let copies still in flight land before exiting
     return;
   }
+  __syncthreads();  // tables visible
 
   // ---- phase 2: Y_k on rows j0-1..j0+TJ, columns k0-1..k0+nk (shared, in place of Y_{k-2})
   const int nr2 = kPJ + 2, nc2 = nk + 2;
+  const StageCoef sa = pa.ca;
   for (int e = tid; e < nr2 * nc2; e += kPThreads) {
     const int r = 1 + e % nr2;  // shared row
     const int c = 1 + e / nr2;  // shared column
     const int j = j0 - 2 + r;
     if (j < 1 || j > ntm) continue;
-    const int kw = wrapc(k0 - 2 + c) == npm ? 2 : (wrapc(k0 - 2 + c) == 1 ? npm - 1 : wrapc(k0 - 2 + c));
     double ax;
     if (j == 1) {
       ax = ax_n;
     } else if (j == ntm) {
       ax = ax_s;
     } else {
-      const double sti = m.st_i[j];
-      const double c1 = Dh * m.dph_i[kw] * m.dp_i[kw] * sti * sti;
-      const double c2 = Dh * m.dth_i[j] * m.dt_i[j] * sti * m.sth[j];
-      const double c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * sti * m.sth[j + 1];
-      const double c5 = Dh * m.dph_i[kw + 1] * m.dp_i[kw] * sti * sti;
+      const double sti = tST[r];
+      const double c1 = tP1[c] * sti * sti;
+      const double c2 = tC2[r];
+      const double c4 = tC4[r];
+      const double c5 = tP5[c] * sti * sti;
       const double c3 = -(c1 + c2 + c4 + c5);
-      ax = c1 * sX1[sidx(c - 1, r)] + c2 * sX1[sidx(c, r - 1)] + c3 * sX1[sidx(c, r)] +
-           c4 * sX1[sidx(c, r + 1)] + c5 * sX1[sidx(c + 1, r)];
+      ax = c1 * sX1[SIDX(c - 1, r)] + c2 * sX1[SIDX(c, r - 1)] + c3 * sX1[SIDX(c, r)] +
+           c4 * sX1[SIDX(c, r + 1)] + c5 * sX1[SIDX(c + 1, r)];
     }
-    const StageCoef &s = pa.ca;
-    const double y = s.a * sX1[sidx(c, r)] + s.b * sYk[sidx(c, r)] + s.c * sU[sidx(c, r)] + s.d * ax +
-                     s.e * sD[sidx(c, r)];
-    sYk[sidx(c, r)] = y;
-    // tile interior goes to HBM (plus its seam copies)
-    if (r >= 2 && r < 2 + kPJ && c >= 2 && c < 2 + nk) {
+    const double y = sa.a * sX1[SIDX(c, r)] + sa.b * sYk[SIDX(c, r)] + sa.c * sU[SIDX(c, r)] + sa.d * ax +
+                     sa.e * sD[SIDX(c, r)];
+    sYk[SIDX(c, r)] = y;
+    if (r >= 2 && r < 2 + kPJ && c >= 2 && c < 2 + nk) {  // tile interior goes to HBM (+ seam copies)
       const int k = k0 - 2 + c;
       const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
       out_k[q] = y;
@@ -1332,51 +1358,51 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double 
   }
   __syncthreads();
 
-  // ---- ring partials of Y_k over this tile's columns
-  // The CTAs whose tile holds row 2 (north) or row ntm-1 (south) publish
-  // ring partials; they also write rows 2 and ntm-1 of Y_{k+1}, which the
-  // last of them reads back below.
+  // ---- ring partials of Y_k over this tile's columns.  The CTAs whose tile
+  // holds row 2 (north) or row ntm-1 (south) publish; they also write rows 2
+  // and ntm-1 of Y_{k+1}, which the last of them reads back below.
   const bool has_n = (j0 == 1);
   const bool has_s = (ntm - 1 >= j0 && ntm - 1 <= j0 + kPJ - 1);
   if (tid == 0 && (has_n || has_s)) {
     if (has_n) {
       double acc = 0.0;
       for (int c = 2; c < 2 + nk; ++c)
-        acc = acc + (Dr + Dr) * (sYk[sidx(c, 3)] - sYk[sidx(c, 2)]) * m.dp[k0 - 2 + c];
+        acc = acc + (Dr + Dr) * (sYk[SIDX(c, 3)] - sYk[SIDX(c, 2)]) * m.dp[k0 - 2 + c];
       ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
     }
     if (has_s) {
       const int rS = ntm - (j0 - 2);
       double acc = 0.0;
       for (int c = 2; c < 2 + nk; ++c)
-        acc = acc + (Dr + Dr) * (sYk[sidx(c, rS)] - sYk[sidx(c, rS - 1)]) * m.dp[k0 - 2 + c];
+        acc = acc + (Dr + Dr) * (sYk[SIDX(c, rS)] - sYk[SIDX(c, rS - 1)]) * m.dp[k0 - 2 + c];
       ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
     }
   }
 
   // ---- phase 3: Y_{k+1} on the tile interior (pole rows are finished below)
+  const StageCoef sb = pa.cb;
   for (int e = tid; e < kPJ * nk; e += kPThreads) {
     const int r = 2 + e % kPJ;
     const int c = 2 + e / kPJ;
     const int j = j0 - 2 + r;
     if (j < 2 || j > ntm - 1) continue;
     const int k = k0 - 2 + c;
-    const double sti = m.st_i[j];
-    const double c1 = Dh * m.dph_i[k] * m.dp_i[k] * sti * sti;
-    const double c2 = Dh * m.dth_i[j] * m.dt_i[j] * sti * m.sth[j];
-    const double c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * sti * m.sth[j + 1];
-    const double c5 = Dh * m.dph_i[k + 1] * m.dp_i[k] * sti * sti;
+    const double sti = tST[r];
+    const double c1 = tP1[c] * sti * sti;
+    const double c2 = tC2[r];
+    const double c4 = tC4[r];
+    const double c5 = tP5[c] * sti * sti;
     const double c3 = -(c1 + c2 + c4 + c5);
-    const double ax = c1 * sYk[sidx(c - 1, r)] + c2 * sYk[sidx(c, r - 1)] + c3 * sYk[sidx(c, r)] +
-                      c4 * sYk[sidx(c, r + 1)] + c5 * sYk[sidx(c + 1, r)];
-    const StageCoef &s = pa.cb;
-    const double y = s.a * sYk[sidx(c, r)] + s.b * sX1[sidx(c, r)] + s.c * sU[sidx(c, r)] + s.d * ax +
-                     s.e * sD[sidx(c, r)];
+    const double ax = c1 * sYk[SIDX(c - 1, r)] + c2 * sYk[SIDX(c, r - 1)] + c3 * sYk[SIDX(c, r)] +
+                      c4 * sYk[SIDX(c, r + 1)] + c5 * sYk[SIDX(c + 1, r)];
+    const double y = sb.a * sYk[SIDX(c, r)] + sb.b * sX1[SIDX(c, r)] + sb.c * sU[SIDX(c, r)] + sb.d * ax +
+                     sb.e * sD[SIDX(c, r)];
     const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
     out_k1[q] = y;
     if (k == 2) out_k1[q + (int64_t)(npm - 2) * ld] = y;
     if (k == npm - 1) out_k1[q - (int64_t)(npm - 2) * ld] = y;
   }
+#undef SIDX
 
   // ---- publish: the last pole-holding CTA of realization i finishes the poles
   const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
@@ -1397,7 +1423,6 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double 
     ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
   }
   block_sum2(sn, ss, &red[0][0]);
-  __shared__ double s_ring[2];
   if (tid == 0) {
     s_ring[0] = sn;
     s_ring[1] = ss;
@@ -1405,18 +1430,16 @@ __global__ void __launch_bounds__(kPThreads, 2) k_sts_pair(Mesh m, const double 
   __syncthreads();
   const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
   // pole rows of Y_{k+1} for every column, then the ring sums of Y_{k+1}
-  const StageCoef &s = pa.cb;
   double rn = 0.0, rsum = 0.0;
   for (int k = 1 + tid; k <= npm; k += kPThreads) {
     const int64_t qn = pbase + (int64_t)(k - 1) * ld;  // row 1
     const int64_t qs = qn + (ntm - 1);                 // row ntm
     // Y_k at the pole rows, recomputed from the inputs (stage k's pole rows
     // use the input's ring sums), so no other CTA's stores are needed here
-    const StageCoef &sa = pa.ca;
     const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
     const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
-    const double yn = s.a * ykn + s.b * ykm1[qn] + s.c * u0[qn] + s.d * axn1 + s.e * dty0[qn];
-    const double ys = s.a * yks + s.b * ykm1[qs] + s.c * u0[qs] + s.d * axs1 + s.e * dty0[qs];
+    const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];
+    const double ys = sb.a * yks + sb.b * ykm1[qs] + sb.c * u0[qs] + sb.d * axs1 + sb.e * dty0[qs];
     out_k1[qn] = yn;
     out_k1[qs] = ys;
     if (k >= 2 && k <= npm - 1) {

@@ -65,7 +65,7 @@ class Info(ctypes.Structure):
     _fields_ = [("ntm", ctypes.c_int), ("npm", ctypes.c_int), ("nr", ctypes.c_int), ("ldt", ctypes.c_int),
                 ("dtime_diffusion_euler", ctypes.c_double), ("sts_s", ctypes.c_int64),
                 ("kernel_launches", ctypes.c_int64), ("cell_stage_updates", ctypes.c_int64),
-                ("device_bytes", ctypes.c_size_t)]
+                ("device_bytes", ctypes.c_size_t), ("rkg2_stages", ctypes.c_int64)]
 
 
 CYCLE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int64,

@@ -199,10 +199,12 @@ typedef struct {
   int64_t kernel_launches;      /* launches of this library's kernels so far  */
   int64_t cell_stage_updates;   /* unique cells x stages advanced so far      */
   size_t device_bytes;          /* device memory held by the handle           */
+  int64_t rkg2_stages;          /* super-step stages k >= 2 run so far         */
 } hipft_info;
 int hipft_gpu_info(const hipft_gpu *h, hipft_info *info);
 /* Per-kernel timing with CUDA events on the handle's stream.  Kinds:
- * 0 RKG2/RKL2 stage (the fused Laplacian + combine), 1 advection stage
+ * 0 RKG2/RKL2 stages k >= 2 (the fused Laplacian + combine kernels, one
+ * or two stages per launch), 1 advection stage
  * (fused WENO3/upwind operator + SSPRK combine), 2 pole-ring sums,
  * 3 everything else.  Enabling resets the counters. */
 enum { HIPFT_K_STS = 0, HIPFT_K_ADV = 1, HIPFT_K_RING = 2, HIPFT_K_OTHER = 3, HIPFT_K_NKINDS = 4 };

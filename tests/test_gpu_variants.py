@@ -1,0 +1,55 @@
+"""Parity of the alternative fused RKG2 stage kernels against the oracle.
+
+The library picks its RKG2 stage kernel from the environment at first use
+(HIPFT_STS_PAIR=1: two stages per launch with TMA-staged tiles;
+HIPFT_STS_KERNEL=2: one theta row per thread), so each variant runs the
+standalone driver in a fresh subprocess; final fields must match the oracle
+to FIELD_TOL."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import cases
+import test_gpu_features as F
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-12
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "v2": {"HIPFT_STS_KERNEL": "2"}}
+RUNS = ["diffuse_soccer", "rkg2_auto_ntm33", "rkg2_auto_ntm161", "strang_dr_mf_diff"]
+
+
+def _setup(name, tmp_path):
+    if name in cases.CASES:
+        src = cases.input_dir(name)
+        text = open(os.path.join(src, "hipft.in")).read()
+        r = cases.oracle_case(name)
+    else:
+        d = dict(F.BASE)
+        d.update(F.CASES[name])
+        text = F._namelist(d)
+        r = O.run(O.process_parameters(O.parse_namelist(text)))
+    (tmp_path / "hipft.in").write_text(text)
+    return r
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+@pytest.mark.parametrize("name", RUNS)
+def test_stage_kernel_variant_parity(variant, name, tmp_path):
+    r = _setup(name, tmp_path)
+    out = tmp_path / "f.npy"
+    code = ("import sys, numpy as np; sys.path.insert(0, %r); import hipft_b200 as H; "
+            "np.save(%r, H.run_field(%r, %r, %r))" % (ROOT, str(out), str(tmp_path / "hipft.in"), str(tmp_path),
+                                                      tuple(r["f"].shape)))
+    env = dict(os.environ)
+    env.update(VARIANTS[variant])
+    res = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    f = np.load(out)
+    err = np.abs(f - r["f"]).max() / np.abs(r["f"]).max()
+    assert err <= FIELD_TOL, f"{variant}/{name}: field rel max-norm {err:.3e}"
