@@ -90,6 +90,7 @@ struct hipft_gpu {
   unsigned int *d_rcount = nullptr;
   int nkb = 0;
   int *d_err = nullptr;   // set by kernels whose bounded waits gave up
+  int num_sms = 148;
   unsigned long long *d_bits = nullptr;
   double *d_part = nullptr;
   size_t part_cap = 0;
@@ -374,27 +375,106 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
-// Two RKG2 stages per launch (k_sts_pair); HIPFT_STS_PAIR=0 falls back to
-// one stage per launch (A/B timing).
-static bool sts_pairs_enabled() {
+// Two RKG2 stages per launch: HIPFT_STS_PAIR=1 (default) one CTA per tile
+// (k_sts_pair), 2 persistent double-buffered CTAs (k_sts_pair_p), 3 one CTA
+// per tile with row-marching arithmetic (k_sts_pair_march), 0 one stage per
+// launch (A/B timing).
+static int sts_pair_variant() {
   static int v = -1;
   if (v < 0) {
     const char *e = std::getenv("HIPFT_STS_PAIR");
-    v = (e && std::atoi(e) == 0) ? 0 : 1;
+    v = e ? std::atoi(e) : 1;
+    if (v < 0 || v > 3) v = 1;
   }
-  return v == 1;
+  return v;
+}
+static bool sts_pairs_enabled() { return sts_pair_variant() != 0; }
+
+// Tile shape of the two-stage kernel (theta rows x phi columns), picked by
+// HIPFT_PAIR_TILE ("128x8" default) for tuning sweeps.
+struct PairShape {
+  const char *name;
+  int tj, tk;
+  size_t smem;
+  void (*launch)(dim3, cudaStream_t, const Mesh &, const double *, const double *, const double *, const double *,
+                 const double *, double *, double *, const double *, double, double, const PairArgs &,
+                 const RingOut &);
+};
+
+template <int TJ, int TK, int MINB>
+static void launch_pair(dim3 g, cudaStream_t s, const Mesh &m, const double *dfac, const double *ykm1,
+                        const double *ykm2, const double *u0, const double *dty0, double *ok, double *ok1,
+                        const double *rin, double bcn, double bcs, const PairArgs &pa, const RingOut &ro) {
+  k_sts_pair<TJ, TK, MINB><<<g, kPThreads, pair_smem_bytes<TJ, TK>(), s>>>(m, dfac, ykm1, ykm2, u0, dty0, ok, ok1,
+                                                                          rin, bcn, bcs, pa, ro);
+}
+
+template <int TJ, int TK, int MINB>
+static cudaError_t pair_attr() {
+  return cudaFuncSetAttribute(k_sts_pair<TJ, TK, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)pair_smem_bytes<TJ, TK>());
+}
+
+static const PairShape kPairShapes[] = {
+    {"128x8", 128, 8, pair_smem_bytes<128, 8>(), launch_pair<128, 8, 4>},
+    {"128x4", 128, 4, pair_smem_bytes<128, 4>(), launch_pair<128, 4, 4>},
+    {"64x8", 64, 8, pair_smem_bytes<64, 8>(), launch_pair<64, 8, 4>},
+    {"64x16", 64, 16, pair_smem_bytes<64, 16>(), launch_pair<64, 16, 4>},
+    {"128x16", 128, 16, pair_smem_bytes<128, 16>(), launch_pair<128, 16, 2>},
+    {"256x8", 256, 8, pair_smem_bytes<256, 8>(), launch_pair<256, 8, 2>},
+    {"256x4", 256, 4, pair_smem_bytes<256, 4>(), launch_pair<256, 4, 3>},
+};
+
+static cudaError_t pair_attrs_all() {
+  cudaError_t e;
+  if ((e = pair_attr<128, 8, 4>()) != cudaSuccess) return e;
+  if ((e = pair_attr<128, 4, 4>()) != cudaSuccess) return e;
+  if ((e = pair_attr<64, 8, 4>()) != cudaSuccess) return e;
+  if ((e = pair_attr<64, 16, 4>()) != cudaSuccess) return e;
+  if ((e = pair_attr<128, 16, 2>()) != cudaSuccess) return e;
+  if ((e = pair_attr<256, 8, 2>()) != cudaSuccess) return e;
+  return pair_attr<256, 4, 3>();
+}
+
+static const PairShape &pair_shape() {
+  static int idx = -1;
+  if (idx < 0) {
+    idx = 0;
+    const char *e = std::getenv("HIPFT_PAIR_TILE");
+    if (e)
+      for (int q = 0; q < (int)(sizeof(kPairShapes) / sizeof(kPairShapes[0])); ++q)
+        if (std::strcmp(e, kPairShapes[q].name) == 0) idx = q;
+  }
+  return kPairShapes[idx];
 }
 
 static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
                     double *out_k, double *out_k1, StageCoef ca, StageCoef cb) {
-  const int nkt = (h->npm - 2 + kPK - 1) / kPK;
+  const PairShape &ps_ = pair_shape();
+  const int tk = (sts_pair_variant() >= 2) ? kPK : ps_.tk;
+  const int tj = (sts_pair_variant() >= 2) ? kPJ : ps_.tj;
+  const int nkt = (h->npm - 2 + tk - 1) / tk;
   RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
-  dim3 grd((unsigned)((h->ntm + kPJ - 1) / kPJ), (unsigned)nkt, (unsigned)h->nr);
+  const int ntj = (h->ntm + tj - 1) / tj;
   {
     ProfScope ps(h, HIPFT_K_STS);
-    k_sts_pair<<<grd, kPThreads, kPairSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1,
-                                                          h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
-                                                          PairArgs{ca, cb, h->d_err}, ro);
+    if (sts_pair_variant() == 3) {
+      dim3 grd((unsigned)ntj, (unsigned)nkt, (unsigned)h->nr);
+      k_sts_pair_march<<<grd, 256, kMarchSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1,
+                                                             h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
+                                                             PairArgs{ca, cb, h->d_err}, ro);
+    } else if (sts_pair_variant() == 2) {
+      const int ntiles = ntj * nkt * h->nr;
+      const int grid = std::min(ntiles, 2 * h->num_sms);
+      k_sts_pair_p<<<grid, kPThreads, kPairSmemP, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
+                                                                out_k1, h->d_ringbuf[h->ring_cur], h->bc_diff_n,
+                                                                h->bc_diff_s, PairArgs{ca, cb, h->d_err}, ro,
+                                                                ntiles);
+    } else {
+      dim3 grd((unsigned)ntj, (unsigned)nkt, (unsigned)h->nr);
+      ps_.launch(grd, h->stream, h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, h->d_ringbuf[h->ring_cur],
+                 h->bc_diff_n, h->bc_diff_s, PairArgs{ca, cb, h->d_err}, ro);
+    }
     LAUNCHED(h);
   }
   h->ring_cur = 1 - h->ring_cur;
@@ -515,8 +595,14 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   if ((rc = dalloc(h, &h->d_rcount, (size_t)nr))) return bail(rc);
   if ((rc = dalloc(h, &h->d_err, 1))) return bail(rc);
   if (cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
-  if (cudaFuncSetAttribute(k_sts_pair, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmem) != cudaSuccess)
-    return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernel"));
+  if (pair_attrs_all() != cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMarchSmem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemP) !=
+          cudaSuccess)
+    return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernels"));
+  if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->num_sms < 1)
+    h->num_sms = 148;
   if (cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned int) * nr, h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   if ((rc = dalloc(h, &h->d_bits, 4))) return bail(rc);
   if (cudaMallocHost((void **)&h->h_pin, sizeof(double) * std::max<size_t>(64, (size_t)nr * kNPart)) !=

@@ -1,8 +1,9 @@
 """Parity of the alternative fused RKG2 stage kernels against the oracle.
 
 The library picks its RKG2 stage kernel from the environment at first use
-(HIPFT_STS_PAIR=1: two stages per launch with TMA-staged tiles;
-HIPFT_STS_KERNEL=2: one theta row per thread), so each variant runs the
+(HIPFT_STS_PAIR=1: two stages per launch with TMA-staged tiles; =2: the same,
+persistent and double-buffered; =0: one stage per launch, two theta rows per
+thread, or one row per thread with HIPFT_STS_KERNEL=2), so each variant runs the
 standalone driver in a fresh subprocess; final fields must match the oracle
 to FIELD_TOL."""
 import os
@@ -20,7 +21,10 @@ pytestmark = pytest.mark.gpu
 
 FIELD_TOL = 1e-12
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "v2": {"HIPFT_STS_KERNEL": "2"}}
+VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "pair_persistent": {"HIPFT_STS_PAIR": "2"},
+            "pair_64x16": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "64x16"}, "pair_march": {"HIPFT_STS_PAIR": "3"},
+            "pair_256x4": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "256x4"},
+            "single_v3": {"HIPFT_STS_PAIR": "0"}, "single_v2": {"HIPFT_STS_PAIR": "0", "HIPFT_STS_KERNEL": "2"}}
 RUNS = ["diffuse_soccer", "rkg2_auto_ntm33", "rkg2_auto_ntm161", "strang_dr_mf_diff"]
 
 
