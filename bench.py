@@ -44,6 +44,10 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 Gcell-updates/s"
 UNIT = "Gcell-updates/s"
 STS_BYTES_PER_CELL = 40  # RKG2 stage k>=2: read Y_{k-1}, Y_{k-2}, u0, dty0; write Y_k
+# two-stage kernel per HIPFT_STS_PAIR value (the library's default is 4); the
+# timed region of a "launch" is the kernel plus, for 4, its pole-row launch
+STS_KERNELS = {"1": "k_sts_pair", "2": "k_sts_pair_p", "3": "k_sts_pair_march",
+               "4": "k_sts_pair_ws+k_pair_poles"}
 
 WORKLOADS = {
     "batched64_1024x2048": dict(ntm=1024, npm1=2049, nr=64, seed=1),
@@ -278,11 +282,13 @@ def run_gpu(args, wl, name):
     sts_avg_ms = sts_ms / max(sts_n, 1)
     achieved = bytes_per_launch / (sts_avg_ms * 1e-3) / 1e9 if sts_n else None
     traffic, traffic_src = None, None
+    sts_kernel = STS_KERNELS.get(os.environ.get("HIPFT_STS_PAIR", "4"), STS_KERNELS["4"]) if stages_per_launch > 1.5 \
+        else "k_sts_stage_v3"
     tpath = os.path.join(ROOT, "profiles", "sts_stage_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as fh:
             tj = json.load(fh)
-        if abs(tj.get("stages_per_launch", 1) - stages_per_launch) < 1e-9:
+        if abs(tj.get("stages_per_launch", 1) - stages_per_launch) < 1e-9 and tj.get("kernel") == sts_kernel:
             traffic = tj["dram_bytes_per_cell"] * ntm * (npm - 2) * nrl
             traffic_src = tj["source"]
     out = {
@@ -294,8 +300,8 @@ def run_gpu(args, wl, name):
                    "method": "WENO3+SSPRK(4,3) Strang-split with RKG2 (PTL subcycles), DA every 24 h",
                    "l2": "inputs larger than L2 (%.2f GB per field), no flush" % (ntm * npm * nrl * 8 / 1e9)},
         "roofline": {"bound": "hbm",
-                     "kernel": ("k_sts_pair (two fused RKG2 stages per launch)" if stages_per_launch > 1.5
-                                else "k_sts_stage_v3<MODE_STSK> (fused RKG2 stage)"),
+                     "kernel": sts_kernel, "kernel_role": ("two fused RKG2 stages per launch"
+                                                           if stages_per_launch > 1.5 else "one fused RKG2 stage"),
                      "stages_per_launch": stages_per_launch, "traffic_source": traffic_src,
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,

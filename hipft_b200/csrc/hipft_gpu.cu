@@ -16,6 +16,7 @@
 
 #include "../../include/hipft_gpu.h"
 #include "kernels.cuh"
+#include "sts_pair_ws.cuh"
 
 using namespace hipft;
 
@@ -89,6 +90,9 @@ struct hipft_gpu {
   double *d_rpart = nullptr;
   unsigned int *d_rcount = nullptr;
   int nkb = 0;
+  PairTables ptab{};        // coefficient tables of the warp-specialised two-stage kernel
+  PoleScratch pole{};       // chunk shares of the ring sums for k_pair_poles
+  int pole_nch = 0;
   int *d_err = nullptr;   // set by kernels whose bounded waits gave up
   int num_sms = 148;
   unsigned long long *d_bits = nullptr;
@@ -375,20 +379,31 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
-// Two RKG2 stages per launch: HIPFT_STS_PAIR=1 (default) one CTA per tile
-// (k_sts_pair), 2 persistent double-buffered CTAs (k_sts_pair_p), 3 one CTA
-// per tile with row-marching arithmetic (k_sts_pair_march), 0 one stage per
-// launch (A/B timing).
+// Two RKG2 stages per launch: HIPFT_STS_PAIR=4 (default) persistent
+// warp-specialised CTAs (k_sts_pair_ws, then k_pair_poles), 1 one CTA per
+// tile (k_sts_pair), 2 persistent double-buffered CTAs (k_sts_pair_p), 3 one
+// CTA per tile with row-marching arithmetic (k_sts_pair_march), 0 one stage
+// per launch (A/B timing).
 static int sts_pair_variant() {
   static int v = -1;
   if (v < 0) {
     const char *e = std::getenv("HIPFT_STS_PAIR");
-    v = e ? std::atoi(e) : 1;
-    if (v < 0 || v > 3) v = 1;
+    v = e ? std::atoi(e) : 4;
+    if (v < 0 || v > 4) v = 4;
   }
   return v;
 }
 static bool sts_pairs_enabled() { return sts_pair_variant() != 0; }
+// HIPFT_WS_POLES=1: k_sts_pair_ws finishes the pole rows itself (last
+// pole-holding tile); default 0: a separate k_pair_poles launch does.
+static bool ws_inline_poles() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_WS_POLES");
+    v = (e && std::atoi(e) == 1) ? 1 : 0;
+  }
+  return v == 1;
+}
 
 // Tile shape of the two-stage kernel (theta rows x phi columns), picked by
 // HIPFT_PAIR_TILE ("128x8" default) for tuning sweeps.
@@ -453,12 +468,30 @@ static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const 
   const PairShape &ps_ = pair_shape();
   const int tk = (sts_pair_variant() >= 2) ? kPK : ps_.tk;
   const int tj = (sts_pair_variant() >= 2) ? kPJ : ps_.tj;
+  static_assert(kWK == kPK && kWJ == kPJ, "the two-stage variants share one tile shape");
   const int nkt = (h->npm - 2 + tk - 1) / tk;
   RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
   const int ntj = (h->ntm + tj - 1) / tj;
   {
     ProfScope ps(h, HIPFT_K_STS);
-    if (sts_pair_variant() == 3) {
+    if (sts_pair_variant() == 4) {
+      const int grid = std::min(h->ptab.ntiles, 2 * h->num_sms);
+      const PairArgs pa{ca, cb, h->d_err};
+      const double *rin = h->d_ringbuf[h->ring_cur];
+      if (ws_inline_poles()) {
+        k_sts_pair_ws<true><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
+                                                                    out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
+                                                                    h->ptab);
+      } else {
+        k_sts_pair_ws<false><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
+                                                                     out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
+                                                                     h->ptab);
+        LAUNCHED(h);
+        dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
+        k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
+                                                         h->bc_diff_n, h->bc_diff_s, pa, ro, h->pole);
+      }
+    } else if (sts_pair_variant() == 3) {
       dim3 grd((unsigned)ntj, (unsigned)nkt, (unsigned)h->nr);
       k_sts_pair_march<<<grd, 256, kMarchSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1,
                                                              h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
@@ -599,6 +632,10 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
       cudaFuncSetAttribute(k_sts_pair_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMarchSmem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_sts_pair_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemP) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_ws<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess)
     return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernels"));
   if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->num_sms < 1)
@@ -620,6 +657,27 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   h->DC.dfac = d_dfac;
   h->DC.factor = prm->diffusion_coef_factor;
   h->DC.grid = prm->diffusion_coef_grid;
+  if (prm->advance_diffusion && !prm->diffusion_coef_grid) {
+    PairTables &pt = h->ptab;
+    pt.nb = (ntm + kWJ - 1) / kWJ;
+    pt.nkt = (npm - 2 + kWK - 1) / kWK;
+    pt.ntiles = pt.nb * pt.nkt * nr;
+    pt.LR = pt.nb * kWJ + 4;
+    pt.LC = pt.nkt * kWK + 4;
+    double *tab = nullptr;
+    const size_t nrow = (size_t)nr * pt.LR * 4, ncol = (size_t)nr * pt.LC * 2;
+    if ((rc = dalloc(h, &tab, nrow + ncol))) return bail(rc);
+    pt.row = tab;
+    pt.col = tab + nrow;
+    k_pair_tables<<<2 * h->num_sms, 256, 0, h->stream>>>(h->M, d_dfac, pt.LR, pt.LC, tab, tab + nrow);
+    h->launches++;
+    if (cudaPeekAtLastError() != cudaSuccess) return bail(fail(h, HIPFT_ECUDA, "k_pair_tables launch failed"));
+    h->pole_nch = (npm + kPoleThreads - 1) / kPoleThreads;
+    if ((rc = dalloc(h, &h->pole.part, (size_t)nr * h->pole_nch * 2))) return bail(rc);
+    if ((rc = dalloc(h, &h->pole.count, (size_t)nr))) return bail(rc);
+    if (cudaMemsetAsync(h->pole.count, 0, sizeof(unsigned int) * nr, h->stream) != cudaSuccess)
+      return bail(HIPFT_ECUDA);
+  }
   h->bc_diff_n = c_pi_i * h->dth_i[2] * h->dth_i[2];
   h->bc_diff_s = c_pi_i * h->dth_i[nt - 1] * h->dth_i[nt - 1];
   h->auto_sc = (prm->diffusion_subcycles == 0);

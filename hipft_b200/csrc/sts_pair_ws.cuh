@@ -1,0 +1,597 @@
+// Two RKG2 stages per launch, persistent and warp-specialised.
+//
+// Same tiles and the same arithmetic as k_sts_pair (stages k and k+1 of
+// diffusion_step_sts_cd, src/hipft.f90:5222-5237, with the 5-point operator of
+// diffusion_operator_cd, src/hipft.f90:7927-7984), organised so that HBM is
+// busy while the SMs compute:
+//
+//  * one producer warp walks the CTA's tiles and fills a ring of two tile
+//    buffers with 1-D bulk copies (cp.async.bulk): Y_{k-1} on the tile plus a
+//    halo of 2, Y_{k-2}, u0 and dty0 plus a halo of 1, and the tile's rows and
+//    columns of two coefficient tables precomputed in HBM (k_pair_tables);
+//    each buffer has a "full" mbarrier (copies landed) and an "empty" one (all
+//    consumers done reading it); every wait is bounded and reports through the
+//    error flag;
+//  * eight consumer warps compute Y_k on the tile plus a halo of 1 into a
+//    shared array of their own, then Y_{k+1} on the tile.  A consumer thread
+//    owns one theta row and half of the tile's phi columns and marches along
+//    phi with a three-value register window, so a cell costs six shared loads
+//    per stage.  The consumers synchronise with named barrier 1 only.
+//
+// Tiles are walked phi tile fastest, so every CTA sees every theta block.
+// Shared memory per CTA: 2 x 48.8 KB buffers + 10.6 KB for Y_k = 108 KB, two
+// CTAs per SM.  Tiles holding rows 2 / ntm-1 publish ring partials of Y_k; the
+// pole rows of Y_{k+1} and its ring sums are finished either by the last of
+// those tiles (atomic counter, no waiting; INLINE_POLES) or by k_pair_poles in
+// a launch of its own.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace hipft {
+
+constexpr int kWJ = 128;                  // theta rows per tile
+constexpr int kWK = 8;                    // phi columns per tile
+constexpr int kWR = kWJ + 4;              // shared rows per column (theta halo 2)
+constexpr int kWNB = 2;                   // tile buffers
+constexpr int kWCons = 256;               // consumer threads
+constexpr int kWThreads = kWCons + 32;    // + the producer warp
+// doubles, offsets within one tile buffer
+constexpr int kWX1 = 0;                        // Y_{k-1}: kWK+4 columns (shared columns 0..kWK+3)
+constexpr int kWY2 = kWX1 + (kWK + 4) * kWR;   // Y_{k-2}: kWK+2 columns (shared columns 1..kWK+2)
+constexpr int kWU = kWY2 + (kWK + 2) * kWR;    // u0
+constexpr int kWD = kWU + (kWK + 2) * kWR;     // dty0
+constexpr int kWRT = kWD + (kWK + 2) * kWR;    // rows: {st_i, c2, c4, 0} per shared row
+constexpr int kWCT = kWRT + 4 * kWR;           // columns: {P1, P5} per shared column
+constexpr int kWBuf = kWCT + 2 * (kWK + 4);
+constexpr int kWYk = kWNB * kWBuf;             // Y_k: kWK+2 columns, consumers only
+constexpr int kWEnd = kWYk + (kWK + 2) * kWR;
+constexpr size_t kWSmem = (size_t)kWEnd * sizeof(double) + 2 * kWNB * sizeof(uint64_t);
+static_assert(kWX1 % 2 == 0 && kWY2 % 2 == 0 && kWU % 2 == 0 && kWD % 2 == 0 && kWRT % 2 == 0 &&
+                  kWCT % 2 == 0 && kWBuf % 2 == 0 && kWYk % 2 == 0 && kWEnd % 2 == 0,
+              "every bulk-copy destination must be 16-byte aligned");
+static_assert((kWR * 8) % 16 == 0, "column stride must keep 16-byte alignment");
+
+// Coefficient tables of the two-stage kernels, in load_diffusion_matrix's
+// operation order (src/hipft.f90:6880-6920) for a per-realization constant D:
+//   rows    [nr][LR][4]: entry jj holds theta row j = jj-1:
+//           {st_i(j), Dh dth_i(j) dt_i(j) st_i(j) sth(j), Dh dth_i(j+1) dt_i(j) st_i(j) sth(j+1), 0}
+//           for 2 <= j <= ntm-1, zeros elsewhere;
+//   columns [nr][LC][2]: entry kk holds phi column kk mapped onto the interior
+//           column kw in 2..npm-1 it duplicates: {Dh dph_i(kw) dp_i(kw), Dh dph_i(kw+1) dp_i(kw)}.
+__global__ void k_pair_tables(Mesh m, const double *__restrict__ dfac, int LR, int LC, double *rowtab,
+                              double *coltab) {
+  const int64_t nrow = (int64_t)m.nr * LR, ncol = (int64_t)m.nr * LC;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nrow + ncol;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    if (e < nrow) {
+      const int i = (int)(e / LR) + 1, j = (int)(e % LR) - 1;
+      const double Dr = dfac[i];
+      const double Dh = kHalf * (Dr + Dr);
+      double st = 0.0, c2 = 0.0, c4 = 0.0;
+      if (j >= 2 && j <= m.ntm - 1) {
+        st = m.st_i[j];
+        c2 = Dh * m.dth_i[j] * m.dt_i[j] * st * m.sth[j];
+        c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * st * m.sth[j + 1];
+      }
+      double *o = rowtab + e * 4;
+      o[0] = st;
+      o[1] = c2;
+      o[2] = c4;
+      o[3] = 0.0;
+    } else {
+      const int64_t f = e - nrow;
+      const int i = (int)(f / LC) + 1, kk = (int)(f % LC);
+      const int n2 = m.npm - 2;
+      const int kw = ((kk - 2) % n2 + n2) % n2 + 2;
+      const double Dr = dfac[i];
+      const double Dh = kHalf * (Dr + Dr);
+      coltab[2 * f] = Dh * m.dph_i[kw] * m.dp_i[kw];
+      coltab[2 * f + 1] = Dh * m.dph_i[kw + 1] * m.dp_i[kw];
+    }
+  }
+}
+
+__device__ __forceinline__ void cons_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+// true on every consumer thread if p is true on any of them (named barrier 1)
+__device__ __forceinline__ bool cons_any(bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred q, o;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred o, 1, 256, q;\n selp.u32 %0, 1, 0, o;\n}"
+      : "=r"(r)
+      : "r"((uint32_t)p)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// fixed-tree sum of two values over the 256 consumer threads; result in thread 0
+__device__ __forceinline__ void cons_sum2(double &a, double &b, double *sh) {
+  const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if (l == 0) {
+    sh[2 * w] = a;
+    sh[2 * w + 1] = b;
+  }
+  cons_sync();
+  if (w == 0) {
+    a = (l < kWCons / 32) ? sh[2 * l] : 0.0;
+    b = (l < kWCons / 32) ? sh[2 * l + 1] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+  }
+  cons_sync();
+}
+
+__device__ __forceinline__ int wrap_col(int c, int npm) {
+  if (c < 1) return c + (npm - 2);
+  if (c > npm) return c - (npm - 2);
+  return c;
+}
+
+struct PairTables {
+  const double *row, *col;  // k_pair_tables output
+  int LR, LC;               // entries per realization
+  int nb, nkt, ntiles;      // theta blocks, phi tiles, all tiles
+};
+
+template <bool INLINE_POLES>
+__global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const double *__restrict__ dfac,
+                                                             const double *__restrict__ ykm1,
+                                                             const double *__restrict__ ykm2,
+                                                             const double *__restrict__ u0,
+                                                             const double *__restrict__ dty0, double *out_k,
+                                                             double *out_k1, const double *__restrict__ ring_in,
+                                                             double bcn, double bcs, PairArgs pa, RingOut ro,
+                                                             PairTables pt) {
+  extern __shared__ __align__(128) double wsm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(wsm + kWEnd);
+  uint64_t *empty = full + kWNB;
+  __shared__ double red[16];
+  __shared__ double s_ring[2];
+  __shared__ int s_last;
+
+  const int tid = threadIdx.x;
+  const int ntm = m.ntm, npm = m.npm;
+  const int64_t ld = m.ldt;
+  if (tid == 0) {
+    for (int b = 0; b < kWNB; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], kWCons);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (tid >= kWCons) {
+    // ------------------------------------------------------------ producer
+    const int lane = tid - kWCons;
+    int n = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
+      const int b = n % kWNB, u = n / kWNB;
+      if (u >= 1 && !mbar_wait_bounded(&empty[b], (uint32_t)((u - 1) & 1), 1u << 22)) {
+        ok = false;
+        break;
+      }
+      const int kt = t % pt.nkt, rest = t / pt.nkt;
+      const int rb = rest % pt.nb, i = rest / pt.nb + 1;
+      const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
+      const int nk = min(kWK, npm - 1 - k0 + 1);
+      const int rs = max(1, j0 - 2), re = min((int)ld, j0 + kWJ + 1);
+      const uint32_t run = (uint32_t)(re - rs + 1) * 8u;
+      const int roff = rs - (j0 - 2);
+      const int64_t pbase = (int64_t)(i - 1) * m.plane;
+      double *B = wsm + b * kWBuf;
+      const int nx = nk + 4, ny = nk + 2, ncp = nx + 3 * ny + 2;
+      if (lane == 0)
+        mbar_expect_tx(&full[b], (uint32_t)(nx + 3 * ny) * run + (uint32_t)(kWR * 32 + (kWK + 4) * 16));
+      __syncwarp();
+      for (int q = lane; q < ncp; q += 32) {
+        const double *src;
+        double *dst;
+        uint32_t bytes = run;
+        if (q < nx) {
+          const int kg = wrap_col(k0 - 2 + q, npm);
+          src = ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1);
+          dst = B + kWX1 + q * kWR + roff;
+        } else if (q < nx + 3 * ny) {
+          const int qq = q - nx, a = qq / ny, c = 1 + qq % ny;
+          const int kg = wrap_col(k0 - 2 + c, npm);
+          const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
+          src = (a == 0 ? ykm2 : (a == 1 ? u0 : dty0)) + g;
+          dst = B + (a == 0 ? kWY2 : (a == 1 ? kWU : kWD)) + (c - 1) * kWR + roff;
+        } else if (q == nx + 3 * ny) {
+          src = pt.row + ((int64_t)(i - 1) * pt.LR + (int64_t)rb * kWJ) * 4;
+          dst = B + kWRT;
+          bytes = kWR * 32;
+        } else {
+          src = pt.col + ((int64_t)(i - 1) * pt.LC + (int64_t)kt * kWK) * 2;
+          dst = B + kWCT;
+          bytes = (kWK + 4) * 16;
+        }
+        bulk_load(dst, src, bytes, &full[b]);
+      }
+    }
+    if (!ok && lane == 0) atomicExch(pa.err, 1);
+    // every issued copy lands before this warp exits (tiles 0..n-1 were issued)
+    for (int b = 0; b < kWNB; ++b) {
+      int last = n - 1;
+      while (last >= 0 && last % kWNB != b) --last;
+      if (last >= 0) mbar_wait_bounded(&full[b], (uint32_t)((last / kWNB) & 1), 1u << 22);
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const int lane = tid & 31, w = tid >> 5;
+  const int h = tid >> 7;            // column half of the tile
+  const int r2 = 1 + (tid & 127);    // stage-k shared row (rows 129, 130 by the last 20 threads)
+  const int r3 = r2 + 1;             // stage-k+1 shared row
+  const StageCoef sa = pa.ca, sb = pa.cb;
+  double *sYk = wsm + kWYk;          // column c of the tile at (c-1)*kWR
+  int n = 0;
+  for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
+    const int b = n % kWNB, u = n / kWNB;
+    const int kt = t % pt.nkt, rest = t / pt.nkt;
+    const int rb = rest % pt.nb, i = rest / pt.nb + 1;
+    const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
+    const int nk = min(kWK, npm - 1 - k0 + 1);
+    const int64_t pbase = (int64_t)(i - 1) * m.plane;
+    const double Dr = dfac[i];
+    const double ax_n = ring_in[2 * (i - 1)] * bcn;
+    const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
+    const bool landed = mbar_wait_bounded(&full[b], (uint32_t)(u & 1), 1u << 22);
+    // one vote: every consumer stops together; also orders the previous
+    // tile's reads of sYk before this tile's writes
+    if (cons_any(!landed)) {
+      if (tid == 0) atomicExch(pa.err, 1);
+      break;
+    }
+    const double *B = wsm + b * kWBuf;
+    const double *X1 = B + kWX1, *Y2 = B + kWY2, *U = B + kWU, *D = B + kWD, *RT = B + kWRT;
+    const double2 *CT = reinterpret_cast<const double2 *>(B + kWCT);
+    const int64_t seam = (int64_t)(npm - 2) * ld;
+
+    // ---------------------------------------------- stage k: Y_k into sYk
+    if (nk == kWK) {
+      {
+        const int r = r2, j = j0 - 2 + r;
+        const bool rowst = (j >= 1 && j <= ntm) && r >= 2;
+        const bool pole = (j == 1 || j == ntm);
+        const double axp = (j == 1) ? ax_n : ax_s;
+        const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+        const int cb = 1 + 5 * h;  // columns cb..cb+4
+        const double *x = X1 + cb * kWR + r;
+        const double *y2 = Y2 + (cb - 1) * kWR + r, *uu = U + (cb - 1) * kWR + r, *dd = D + (cb - 1) * kWR + r;
+        double *yk = sYk + (cb - 1) * kWR + r;
+        const double2 *ct = CT + cb;
+        double *g = out_k + pbase + (int64_t)(k0 - 3 + cb) * ld + (j - 1);
+        // all five cells before any shared store, so that the five
+        // arithmetic chains can overlap (a store to sYk would otherwise
+        // order every later shared load after it)
+        double y[5];
+        double xl = x[-kWR], xc = x[0];
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+          const double xr = x[(s + 1) * kWR];
+          const double up = x[s * kWR - 1], dn = x[s * kWR + 1];
+          double ax;
+          if (pole) {
+            ax = axp;
+          } else {
+            const double2 P = ct[s];
+            const double c1 = P.x * sti * sti;
+            const double c5 = P.y * sti * sti;
+            const double c3 = -(c1 + c2 + c4 + c5);
+            ax = c1 * xl + c2 * up + c3 * xc + c4 * dn + c5 * xr;
+          }
+          y[s] = sa.a * xc + sa.b * y2[s * kWR] + sa.c * uu[s * kWR] + sa.d * ax + sa.e * dd[s * kWR];
+          xl = xc;
+          xc = xr;
+        }
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+          const int c = cb + s;
+          yk[s * kWR] = y[s];
+          if (rowst && c >= 2 && c <= kWK + 1) {
+            double *gq = g + (int64_t)s * ld;
+            *gq = y[s];
+            const int k = k0 - 2 + c;
+            if (k == 2) gq[seam] = y[s];
+            if (k == npm - 1) gq[-seam] = y[s];
+          }
+        }
+      }
+      if (tid >= kWCons - 2 * (kWK + 2)) {  // shared rows kWJ+1, kWJ+2 (one cell each)
+        const int e = tid - (kWCons - 2 * (kWK + 2));
+        const int r = kWJ + 1 + (e & 1), c = 1 + (e >> 1);
+        const int j = j0 - 2 + r;
+        if (j >= 1 && j <= ntm) {
+          double ax;
+          if (j == 1) {
+            ax = ax_n;
+          } else if (j == ntm) {
+            ax = ax_s;
+          } else {
+            const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+            const double2 P = CT[c];
+            const double c1 = P.x * sti * sti;
+            const double c5 = P.y * sti * sti;
+            const double c3 = -(c1 + c2 + c4 + c5);
+            ax = c1 * X1[(c - 1) * kWR + r] + c2 * X1[c * kWR + r - 1] + c3 * X1[c * kWR + r] +
+                 c4 * X1[c * kWR + r + 1] + c5 * X1[(c + 1) * kWR + r];
+          }
+          const double y = sa.a * X1[c * kWR + r] + sa.b * Y2[(c - 1) * kWR + r] + sa.c * U[(c - 1) * kWR + r] +
+                           sa.d * ax + sa.e * D[(c - 1) * kWR + r];
+          sYk[(c - 1) * kWR + r] = y;
+          if (r == kWJ + 1 && c >= 2 && c <= kWK + 1) {
+            const int k = k0 - 2 + c;
+            double *gq = out_k + pbase + (int64_t)(k - 1) * ld + (j - 1);
+            *gq = y;
+            if (k == 2) gq[seam] = y;
+            if (k == npm - 1) gq[-seam] = y;
+          }
+        }
+      }
+    } else {
+      const int nr2 = kWJ + 2, nc2 = nk + 2;
+      for (int e = tid; e < nr2 * nc2; e += kWCons) {
+        const int r = 1 + e % nr2, c = 1 + e / nr2;
+        const int j = j0 - 2 + r;
+        if (j < 1 || j > ntm) continue;
+        double ax;
+        if (j == 1) {
+          ax = ax_n;
+        } else if (j == ntm) {
+          ax = ax_s;
+        } else {
+          const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+          const double2 P = CT[c];
+          const double c1 = P.x * sti * sti;
+          const double c5 = P.y * sti * sti;
+          const double c3 = -(c1 + c2 + c4 + c5);
+          ax = c1 * X1[(c - 1) * kWR + r] + c2 * X1[c * kWR + r - 1] + c3 * X1[c * kWR + r] +
+               c4 * X1[c * kWR + r + 1] + c5 * X1[(c + 1) * kWR + r];
+        }
+        const double y = sa.a * X1[c * kWR + r] + sa.b * Y2[(c - 1) * kWR + r] + sa.c * U[(c - 1) * kWR + r] +
+                         sa.d * ax + sa.e * D[(c - 1) * kWR + r];
+        sYk[(c - 1) * kWR + r] = y;
+        if (r >= 2 && r < 2 + kWJ && c >= 2 && c < 2 + nk) {
+          const int k = k0 - 2 + c;
+          double *gq = out_k + pbase + (int64_t)(k - 1) * ld + (j - 1);
+          *gq = y;
+          if (k == 2) gq[seam] = y;
+          if (k == npm - 1) gq[-seam] = y;
+        }
+      }
+    }
+    cons_sync();
+
+    // ---- ring partials of Y_k over this tile's columns (fixed tree over columns)
+    const bool has_n = (j0 == 1);
+    const bool has_s = (ntm - 1 >= j0 && ntm - 1 <= j0 + kWJ - 1);
+    if ((w == 0 && has_n) || (w == 1 && has_s)) {
+      const int ra = (w == 0) ? 3 : ntm - (j0 - 2);  // (row 2 - row 1) or (row ntm - row ntm-1)
+      double v = 0.0;
+      if (lane < nk) {
+        const int c = 2 + lane;
+        v = (Dr + Dr) * (sYk[(c - 1) * kWR + ra] - sYk[(c - 1) * kWR + ra - 1]) * m.dp[k0 - 2 + c];
+      }
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if (lane == 0) ro.part[((int64_t)w * m.nr + (i - 1)) * ro.nkb + kt] = v;
+    }
+
+    // -------------------------------------- stage k+1: Y_{k+1} to HBM
+    if (nk == kWK) {
+      const int r = r3, j = j0 - 2 + r;
+      const bool rowok = (j >= 2 && j <= ntm - 1);
+      const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+      const int cb = 2 + 4 * h;  // columns cb..cb+3
+      const double *yk = sYk + (cb - 1) * kWR + r;
+      const double *x1 = X1 + cb * kWR + r, *uu = U + (cb - 1) * kWR + r, *dd = D + (cb - 1) * kWR + r;
+      const double2 *ct = CT + cb;
+      double *g = out_k1 + pbase + (int64_t)(k0 - 3 + cb) * ld + (j - 1);
+      double xl = yk[-kWR], xc = yk[0];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const int c = cb + s;
+        const double xr = yk[(s + 1) * kWR];
+        const double up = yk[s * kWR - 1], dn = yk[s * kWR + 1];
+        const double2 P = ct[s];
+        const double c1 = P.x * sti * sti;
+        const double c5 = P.y * sti * sti;
+        const double c3 = -(c1 + c2 + c4 + c5);
+        const double ax = c1 * xl + c2 * up + c3 * xc + c4 * dn + c5 * xr;
+        const double y = sb.a * xc + sb.b * x1[s * kWR] + sb.c * uu[s * kWR] + sb.d * ax + sb.e * dd[s * kWR];
+        if (rowok) {
+          double *gq = g + (int64_t)s * ld;
+          *gq = y;
+          const int k = k0 - 2 + c;
+          if (k == 2) gq[seam] = y;
+          if (k == npm - 1) gq[-seam] = y;
+        }
+        xl = xc;
+        xc = xr;
+      }
+    } else {
+      for (int e = tid; e < kWJ * nk; e += kWCons) {
+        const int r = 2 + e % kWJ, c = 2 + e / kWJ;
+        const int j = j0 - 2 + r;
+        if (j < 2 || j > ntm - 1) continue;
+        const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+        const double2 P = CT[c];
+        const double c1 = P.x * sti * sti;
+        const double c5 = P.y * sti * sti;
+        const double c3 = -(c1 + c2 + c4 + c5);
+        const double ax = c1 * sYk[(c - 2) * kWR + r] + c2 * sYk[(c - 1) * kWR + r - 1] +
+                          c3 * sYk[(c - 1) * kWR + r] + c4 * sYk[(c - 1) * kWR + r + 1] + c5 * sYk[c * kWR + r];
+        const double y = sb.a * sYk[(c - 1) * kWR + r] + sb.b * X1[c * kWR + r] + sb.c * U[(c - 1) * kWR + r] +
+                         sb.d * ax + sb.e * D[(c - 1) * kWR + r];
+        const int k = k0 - 2 + c;
+        double *gq = out_k1 + pbase + (int64_t)(k - 1) * ld + (j - 1);
+        *gq = y;
+        if (k == 2) gq[seam] = y;
+        if (k == npm - 1) gq[-seam] = y;
+      }
+    }
+    mbar_arrive(&empty[b]);  // this thread is done with buffer b
+
+    // ---- the last pole-holding tile of realization i finishes the poles
+    // (or k_pair_poles does, in a launch of its own)
+    const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
+    if (INLINE_POLES && contrib) {
+      __threadfence();
+      cons_sync();
+      if (tid == 0) {
+        const unsigned int old = atomicAdd(&ro.count[i - 1], (unsigned)contrib);
+        s_last = (old + (unsigned)contrib == 2u * (unsigned)ro.nkb) ? 1 : 0;
+      }
+      cons_sync();
+      if (s_last) {
+        __threadfence();
+        double sn = 0.0, ss = 0.0;
+        for (int q = tid; q < ro.nkb; q += kWCons) {
+          sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + q]);
+          ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + q]);
+        }
+        cons_sum2(sn, ss, red);
+        if (tid == 0) {
+          s_ring[0] = sn;
+          s_ring[1] = ss;
+        }
+        cons_sync();
+        const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
+        double rn = 0.0, rsum = 0.0;
+        for (int k = 1 + tid; k <= npm; k += kWCons) {
+          const int64_t qn = pbase + (int64_t)(k - 1) * ld;  // row 1
+          const int64_t qs = qn + (ntm - 1);                 // row ntm
+          // Y_k at the pole rows, recomputed from the inputs
+          const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
+          const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
+          const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];
+          const double ys = sb.a * yks + sb.b * ykm1[qs] + sb.c * u0[qs] + sb.d * axs1 + sb.e * dty0[qs];
+          out_k1[qn] = yn;
+          out_k1[qs] = ys;
+          if (k >= 2 && k <= npm - 1) {
+            rn = rn + (Dr + Dr) * (__ldcg(&out_k1[qn + 1]) - yn) * m.dp[k];
+            rsum = rsum + (Dr + Dr) * (ys - __ldcg(&out_k1[qs - 1])) * m.dp[k];
+          }
+        }
+        cons_sum2(rn, rsum, red);
+        if (tid == 0) {
+          ro.ring[2 * (i - 1)] = rn;
+          ro.ring[2 * (i - 1) + 1] = rsum;
+          ro.count[i - 1] = 0u;
+        }
+      }
+    }
+  }
+}
+
+// Pole rows of Y_{k+1} and the ring sums of Y_{k+1}, after
+// k_sts_pair_ws<false>.  Grid (realization, chunk of kPoleThreads phi
+// columns).  Every block sums the ring partials of Y_k that the pole tiles
+// wrote (tile order, the same fixed tree in every block), computes the pole
+// rows of Y_{k+1} for its columns by stage k+1's combine (src/hipft.f90:
+// 5224-5235) with Y_k at the poles recomputed from the inputs, and writes its
+// chunk's share of the ring sums of Y_{k+1} (src/hipft.f90:7969-7979); the
+// last block of a realization (atomic counter, no waiting) adds the chunks in
+// order and leaves the ring sums for the next launch.
+constexpr int kPoleThreads = 256;
+struct PoleScratch {
+  double *part;          // [nr][nch][2] chunk shares of the ring sums
+  unsigned int *count;   // [nr] blocks done, reset by the last one
+};
+__global__ void __launch_bounds__(kPoleThreads) k_pair_poles(Mesh m, const double *__restrict__ dfac,
+                                                            const double *__restrict__ ykm1,
+                                                            const double *__restrict__ ykm2,
+                                                            const double *__restrict__ u0,
+                                                            const double *__restrict__ dty0, double *out_k1,
+                                                            const double *__restrict__ ring_in, double bcn,
+                                                            double bcs, PairArgs pa, RingOut ro, PoleScratch ps) {
+  __shared__ double sh[2 * (kPoleThreads / 32)];
+  __shared__ double s_ring[2];
+  __shared__ int s_last;
+  const int tid = threadIdx.x, i = blockIdx.x + 1, ch = blockIdx.y, nch = gridDim.y;
+  const int ntm = m.ntm, npm = m.npm;
+  const int64_t ld = m.ldt, pbase = (int64_t)(i - 1) * m.plane;
+  const StageCoef sa = pa.ca, sb = pa.cb;
+  const double Dr = dfac[i];
+  const double ax_n = ring_in[2 * (i - 1)] * bcn;
+  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
+  // this block's column: its inputs are loaded before the ring reduction
+  const int k = 1 + ch * kPoleThreads + tid;
+  const bool kin = (k <= npm);
+  const int64_t qn = pbase + (int64_t)(kin ? k - 1 : 0) * ld;  // row 1
+  const int64_t qs = qn + (ntm - 1);                           // row ntm
+  double a1n = 0, a2n = 0, aun = 0, adn = 0, a1s = 0, a2s = 0, aus = 0, ads = 0, y2 = 0, ym = 0, dpk = 0;
+  if (kin) {
+    a1n = ykm1[qn]; a2n = ykm2[qn]; aun = u0[qn]; adn = dty0[qn];
+    a1s = ykm1[qs]; a2s = ykm2[qs]; aus = u0[qs]; ads = dty0[qs];
+    y2 = out_k1[qn + 1];
+    ym = out_k1[qs - 1];
+    dpk = m.dp[k];
+  }
+  double sn = 0.0, ss = 0.0;
+  for (int q = tid; q < ro.nkb; q += kPoleThreads) {
+    sn = sn + ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + q];
+    ss = ss + ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + q];
+  }
+  block_sum2(sn, ss, sh);
+  if (tid == 0) {
+    s_ring[0] = sn;
+    s_ring[1] = ss;
+  }
+  __syncthreads();
+  const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
+  double rn = 0.0, rsum = 0.0;
+  if (kin) {
+    const double ykn = sa.a * a1n + sa.b * a2n + sa.c * aun + sa.d * ax_n + sa.e * adn;
+    const double yks = sa.a * a1s + sa.b * a2s + sa.c * aus + sa.d * ax_s + sa.e * ads;
+    const double yn = sb.a * ykn + sb.b * a1n + sb.c * aun + sb.d * axn1 + sb.e * adn;
+    const double ys = sb.a * yks + sb.b * a1s + sb.c * aus + sb.d * axs1 + sb.e * ads;
+    out_k1[qn] = yn;
+    out_k1[qs] = ys;
+    if (k >= 2 && k <= npm - 1) {
+      rn = (Dr + Dr) * (y2 - yn) * dpk;
+      rsum = (Dr + Dr) * (ys - ym) * dpk;
+    }
+  }
+  block_sum2(rn, rsum, sh);
+  if (tid == 0) {
+    double *pp = ps.part + ((int64_t)(i - 1) * nch + ch) * 2;
+    pp[0] = rn;
+    pp[1] = rsum;
+    __threadfence();
+    const unsigned int old = atomicAdd(&ps.count[i - 1], 1u);
+    s_last = (old == (unsigned)nch - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  if (tid == 0) {
+    __threadfence();
+    double tn = 0.0, ts = 0.0;
+    for (int c = 0; c < nch; ++c) {
+      tn = tn + __ldcg(&ps.part[((int64_t)(i - 1) * nch + c) * 2]);
+      ts = ts + __ldcg(&ps.part[((int64_t)(i - 1) * nch + c) * 2 + 1]);
+    }
+    ro.ring[2 * (i - 1)] = tn;
+    ro.ring[2 * (i - 1) + 1] = ts;
+    ps.count[i - 1] = 0u;
+  }
+}
+
+}  // namespace hipft

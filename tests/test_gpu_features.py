@@ -31,6 +31,11 @@ CASES = {
                             validation_run=1),
     "rkg2_auto_ntm161": dict(res_nt=161, res_np=101, n_realizations=3, advance_diffusion=True,
                              diffusion_coef_constants=[300.0, 600.0, 50.0], validation_run=1),
+    # theta rows 128 | 129 and 129 | 130 straddle a 128-row tile boundary at the south pole
+    "rkg2_ntm129_np65": dict(res_nt=129, res_np=65, advance_diffusion=True, diffusion_coef_constants=[500.0, 120.0],
+                             validation_run=1),
+    "rkg2_ntm130_np96": dict(res_nt=130, res_np=96, advance_diffusion=True, diffusion_coef_constants=[80.0, 700.0],
+                             validation_run=1),
     "rkl2_fixed_sc": dict(advance_diffusion=True, diffusion_num_method=2, diffusion_subcycles=3,
                           diffusion_coef_constants=[250.0, 500.0], validation_run=1),
     "euler_fixed_sc": dict(res_nt=20, res_np=37, advance_diffusion=True, diffusion_num_method=1,
