@@ -3,6 +3,6 @@
 The CUDA library (libhipft_gpu.so, include/hipft_gpu.h) holds the kernels
 and the driver; :mod:`hipft_b200.gpu` is its ctypes binding.
 """
-from .gpu import HipftGPU, HipftError, h5_read, lib, run, run_field  # noqa: F401
+from .gpu import HipftGPU, HipftError, h5_read, h5_write, lib, run, run_field  # noqa: F401
 
-__all__ = ["HipftGPU", "HipftError", "h5_read", "lib", "run", "run_field"]
+__all__ = ["HipftGPU", "HipftError", "h5_read", "h5_write", "lib", "run", "run_field"]

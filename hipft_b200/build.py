@@ -18,7 +18,7 @@ LIB = os.path.join(PKG, "libhipft_gpu.so")
 EXE = os.path.join(PKG, "bin", "hipft")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["hipft_gpu.cu"]
-CXX_SOURCES = ["namelist.cpp", "h5lite.cpp", "driver.cpp"]
+CXX_SOURCES = ["namelist.cpp", "h5lite.cpp", "h5write.cpp", "driver.cpp"]
 HEADERS = ["kernels.cuh", "sts_pair_ws.cuh", "namelist.h"]
 
 

@@ -4,12 +4,19 @@
 // path: setup (reading hipft.in, realization parameters, the initial map or
 // a validation map, flows, diffusion, data-assimilation list), then per step
 // update_step -> flux_transport_step -> time += dt -> data assimilation ->
-// analysis -> history output, until time_end.  History files use the
-// reference's names and Fortran formats (src/hipft.f90:1616-1646, 2633-2634).
-// Map files (HDF5 output) are not written.
+// analysis -> history output -> map output, until time_end.  History files
+// use the reference's names and Fortran formats (src/hipft.f90:1616-1646,
+// 2633-2634); maps are written as the reference's write_map does
+// (src/hipft.f90:2801-2917): <root>_initial.h5 after setup, numbered maps in
+// output_map_directory at the output cadence (listed in
+// hipft_output_map_list.out, src/hipft.f90:2700-2798), <root>_final.h5 at the
+// end, and for validation runs the analytic maps of src/hipft.f90:1891-2102.
+#include <sys/stat.h>
+
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -94,14 +101,32 @@ bool read_da_list(const std::string &path, DAList &L, std::string &err) {
     err = "cannot open assimilation map list " + path;
     return false;
   }
+  // rows as READ(...,'(A19,1X,A19,1X,F13.5,1X,A)') reads them
+  // (src/hipft.f90:3987-4001): two 19-character date fields, the actual
+  // Julian day in columns 41-53 and the map's relative path after column 54,
+  // whatever single character separates the fields (blank or comma)
   std::string line;
   std::getline(in, line);  // header row
   std::vector<double> jd;
   while (std::getline(in, line)) {
-    std::istringstream ss(line);
-    std::string req, act, file;
-    double j;
-    if (!(ss >> req >> act >> j >> file)) continue;
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    if (line.find_first_not_of(" \t") == std::string::npos) continue;
+    if (line.size() < 55) {
+      err = "malformed row in assimilation map list " + path + ": " + line;
+      return false;
+    }
+    std::string f13 = line.substr(40, 13), digits;
+    for (char c : f13)
+      if (c != ' ') digits += (c == 'd' || c == 'D') ? 'E' : c;  // blanks are ignored in a numeric field
+    char *end = nullptr;
+    double j = std::strtod(digits.c_str(), &end);
+    if (digits.empty() || *end != '\0') {
+      err = "bad Julian day in assimilation map list " + path + ": " + f13;
+      return false;
+    }
+    if (digits.find_first_of(".eEdD") == std::string::npos) j /= 1.0e5;  // F13.5 without a point
+    std::string file = line.substr(54);
+    while (!file.empty() && (file.back() == ' ' || file.back() == '\t')) file.pop_back();
     jd.push_back(j);
     L.files.push_back(file);
   }
@@ -113,9 +138,39 @@ bool read_da_list(const std::string &path, DAList &L, std::string &err) {
   return true;
 }
 
+// Fortran 1PE25.15 (two-digit exponent): right-justified in 25 columns.
+std::string fmt_pe25(double v) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%.15E", v);
+  return rjust(b, 25);
+}
+
+// mkdir -p of a relative or absolute directory
+bool make_dirs(const std::string &d) {
+  std::string cur;
+  size_t i = 0;
+  while (i <= d.size()) {
+    size_t j = d.find('/', i);
+    if (j == std::string::npos) j = d.size();
+    cur = d.substr(0, j);
+    if (!cur.empty()) {
+      struct stat st;
+      if (stat(cur.c_str(), &st) != 0) {
+        if (mkdir(cur.c_str(), 0755) != 0) return false;
+      } else if (!S_ISDIR(st.st_mode)) {
+        return false;
+      }
+    }
+    i = j + 1;
+  }
+  return true;
+}
+
 struct Run {
   Namelist nl;
   std::string dir;
+  std::string map_dir;             // output_map_directory (relative to the run directory)
+  std::vector<double> pscale, tscale;  // the map scales: p(1:npm1), t(1:ntm)
   hipft_gpu *h = nullptr;
   int nr = 0;
   // time stepping state (globals / flows / diffusion modules)
@@ -178,15 +233,70 @@ struct Run {
     return HIPFT_OK;
   }
 
-  void output_map_index() {
+  // write_2d_file / write_3d_file (src/hipft.f90:6353-6493): PT data
+  // (n1, n2[, n3]) with scales s1, s2 and realization numbers 1..n3.
+  int write_pt(const std::string &fname, int n1, int n2, int n3, const double *f, const double *s1,
+               const double *s2, bool two_d) {
+    std::vector<double> s3(n3);
+    for (int i = 0; i < n3; ++i) s3[i] = (double)(i + 1);
+    int64_t dims[3] = {n1, n2, two_d ? 1 : n3};
+    int rc = hipft_h5_write(path(fname).c_str(), two_d ? 2 : 3, dims, f, s1, s2, two_d ? nullptr : s3.data(),
+                            nl.output_single_precision ? 1 : 0);
+    if (rc) err = "cannot write the map file " + path(fname);
+    return rc;
+  }
+
+  // write_map (src/hipft.f90:2801-2917): the current field, flux-balanced
+  // on a copy when output_map_flux_balance, as PT with one-point phi overlap.
+  int write_map(const std::string &fname) {
+    hipft_info inf;
+    hipft_gpu_info(h, &inf);
+    const int ntm = inf.ntm, npm = inf.npm, npm1 = npm - 1;
+    std::vector<double> f((size_t)ntm * npm * nr);
+    int rc = hipft_gpu_get_field(h, f.data());
+    if (rc) return rc;
+    if (nl.output_map_flux_balance) {
+      // balance_flux (src/hipft.f90:8752-8807) on the copy
+      std::vector<double> fp(nr), fm(nr);
+      rc = hipft_gpu_get_flux(h, fp.data(), fm.data());
+      if (rc) return rc;
+      for (int i = 0; i < nr; ++i) {
+        if (fm[i] + fp[i] == 0.0) continue;
+        const double ratio = std::sqrt(std::fabs(fp[i] / fm[i]));
+        double *a = &f[(size_t)i * ntm * npm];
+        for (size_t q = 0; q < (size_t)ntm * npm; ++q) a[q] = (a[q] > 0) ? a[q] / ratio : a[q] * ratio;
+      }
+    }
+    std::vector<double> fout((size_t)npm1 * ntm * nr);
+    for (int i = 0; i < nr; ++i)
+      for (int j = 0; j < ntm; ++j)
+        for (int k = 0; k < npm1; ++k)
+          fout[((size_t)i * ntm + j) * npm1 + k] = f[((size_t)i * npm + k) * ntm + j];
+    return write_pt(fname, npm1, ntm, nr, fout.data(), pscale.data(), tscale.data(),
+                    nl.output_map_2d && nl.n_realizations == 1);
+  }
+
+  // output_map (src/hipft.f90:2700-2798)
+  int output_map() {
     if (nl.output_map_idx_cadence > 0 && ntime % nl.output_map_idx_cadence == 0) output_current_map = true;
     if (nl.output_map_time_cadence > 0.0 &&
         time >= nl.time_start + (double)(idx_out - (nl.output_map_idx_start - 1)) * nl.output_map_time_cadence)
       output_current_map = true;
     if (output_current_map) {
       idx_out++;
+      char idx[32];
+      std::snprintf(idx, sizeof idx, "%06ld", idx_out);
+      const std::string base = nl.output_map_root_filename + "_idx" + idx + ".h5";
+      int rc = write_map(map_dir + "/" + base);
+      if (rc) return rc;
       output_current_map = false;
+      FILE *fl = std::fopen(path("hipft_output_map_list.out").c_str(), "a");
+      if (!fl) return HIPFT_EIO;
+      std::string ln = fmt_i(idx_out, 10) + "   " + fmt_pe25(time) + "    " + base + "\n";
+      std::fputs(ln.c_str(), fl);
+      std::fclose(fl);
     }
+    return HIPFT_OK;
   }
 
   // update_timestep (src/hipft.f90:4308-4461)
@@ -330,6 +440,7 @@ struct Run {
     double vt_const = nl.flow_vt_const, vp_omega = nl.flow_vp_rigid_omega;
     std::vector<double> fval_u0;
     size_t plane = (size_t)n1 * n2;
+    const bool two_d = nl.output_map_2d && nl.n_realizations == 1;
     if (nl.validation_run == 1) {
       std::vector<double> Y0, Y5;
       spherical_harmonic(0, 6, s1, s2, Y0);
@@ -337,11 +448,28 @@ struct Run {
       fval_u0.assign(plane * nr, 0.0);
       for (int i = 0; i < nr; ++i)
         for (size_t q = 0; q < plane; ++q) fval_u0[plane * i + q] = Y0[q] + std::sqrt(14.0 / 11.0) * Y5[q];
+      // initial and final analytic maps (src/hipft.f90:1921-2031)
+      int rc = write_pt(nl.output_map_root_filename + "_initial_0.h5", n1, n2, nr, fval_u0.data(), s1.data(),
+                        s2.data(), two_d);
+      if (rc) return rc;
+      std::vector<double> fa(plane * nr);
+      for (int i = 0; i < nr; ++i)
+        for (size_t q = 0; q < plane; ++q)
+          fa[plane * i + q] = fval_u0[plane * i + q] * std::exp(-42.0 * nl.diffusion_coef_constants[i] *
+                                                                nl.diffusion_coef_factor * nl.time_end);
+      rc = write_pt(nl.output_map_root_filename + "_final_analytic.h5", n1, n2, nr, fa.data(), s1.data(),
+                    s2.data(), two_d);
+      if (rc) return rc;
       f_local = fval_u0;
     } else if (nl.validation_run == 2) {
-      if (std::fabs(vt_const) > 0.0) vt_const = (c_pi_two / (nl.time_end - nl.time_start)) / c_km_s_to_rs_hr;
+      double vt_end_loc = c_pi_four;
+      if (std::fabs(vt_const) > 0.0) {
+        vt_const = (c_pi_two / (nl.time_end - nl.time_start)) / c_km_s_to_rs_hr;
+        vt_end_loc = 3.0 * c_pi_four;
+      }
       if (std::fabs(vp_omega) > 0.0) vp_omega = (c_twopi / (nl.time_end - nl.time_start)) / c_km_s_to_rs_hr;
       double w = nl.validation_run_width;
+      std::vector<double> fa(plane);
       for (int i = 0; i < nr; ++i)
         for (int j = 1; j <= n2; ++j) {
           double sti = (j > 1 && j < n2) ? 1.0 / std::sin(s2[j - 1]) : 0.0;
@@ -349,9 +477,20 @@ struct Run {
             double a = s2[j - 1] - c_pi_four, b1 = s1[k - 1] - c_pi_two, b2 = s1[k - 1] - c_threepi_two;
             f_local[plane * i + (size_t)(j - 1) * n1 + (k - 1)] =
                 -sti * std::exp(-(a * a) / w - (b1 * b1) / w) + sti * std::exp(-(a * a) / w - (b2 * b2) / w);
+            if (i == 0) {
+              double e = s2[j - 1] - vt_end_loc;
+              fa[(size_t)(j - 1) * n1 + (k - 1)] =
+                  -sti * std::exp(-(e * e) / w - (b1 * b1) / w) + sti * std::exp(-(e * e) / w - (b2 * b2) / w);
+            }
           }
         }
+      // final analytic map of the first realization (src/hipft.f90:2062-2097)
+      int rc = write_pt(nl.output_map_root_filename + "_final_analytic.h5", n1, n2, 1, fa.data(), s1.data(),
+                        s2.data(), true);
+      if (rc) return rc;
     }
+    pscale = s1;
+    tscale = s2;
     hipft_grid g{};
     g.ntm = n2;
     g.npm1 = n1;
@@ -379,6 +518,8 @@ struct Run {
       return rc;
     }
     rc = hipft_gpu_load_initial_map(h, f_local.data(), nl.initial_map_flux_balance, nl.initial_map_mult_fac);
+    if (rc) return rc;
+    rc = write_map(nl.output_map_root_filename + "_initial.h5");  // src/hipft.f90:2185
     if (rc) return rc;
     if (nl.validation_run == 1) rc = hipft_gpu_set_validation(h, 1, fval_u0.data(), 0, 0, 0, nl.time_start);
     else if (nl.validation_run == 2)
@@ -408,7 +549,23 @@ struct Run {
     subcycles = nl.diffusion_subcycles;
     time = nl.time_start;
     idx_out = nl.output_map_idx_start - 1;
-    if (nl.output_map_idx_cadence > 0 || nl.output_map_time_cadence > 0.0) output_current_map = true;
+    if (nl.output_map_idx_cadence > 0 || nl.output_map_time_cadence > 0.0) {
+      output_current_map = true;
+      // output directory and map list (src/hipft.f90:1194-1210, 1654-1664)
+      map_dir = nl.output_map_directory;
+      if (!make_dirs(path(map_dir))) {
+        std::printf(" ### Could not make map output subdirectory, using ./\n");
+        map_dir = ".";
+      }
+      FILE *fl = std::fopen(path("hipft_output_map_list.out").c_str(), "w");
+      if (!fl) {
+        err = "cannot create hipft_output_map_list.out in " + dir;
+        return HIPFT_EIO;
+      }
+      std::string hdr = rjust("IDX", 10) + " " + rjust("TIME", 25) + " FILENAME\n";
+      std::fputs(hdr.c_str(), fl);
+      std::fclose(fl);
+    }
     if (nl.assimilate_data) {
       if (!read_da_list(path(nl.assimilate_data_map_list_filename), da, err)) return HIPFT_EIO;
       // load_data_assimilation time bookkeeping (src/hipft.f90:4017-4042)
@@ -459,8 +616,7 @@ struct Run {
     }
     rc = analysis_and_history();
     if (rc) return rc;
-    output_map_index();
-    return HIPFT_OK;
+    return output_map();
   }
 
   int main_loop() {
@@ -489,7 +645,8 @@ struct Run {
       if (rc) return rc;
       rc = analysis_and_history();
       if (rc) return rc;
-      output_map_index();
+      rc = output_map();
+      if (rc) return rc;
       if (nl.verbose >= 0) {
         std::printf(" Completed step: %10ld  Time: %14.3f / %14.3f  dt: %12.6f\n", ntime, time, nl.time_end,
                     dtime_global);
@@ -521,6 +678,7 @@ extern "C" int hipft_run_field(const char *namelist_path, const char *run_dir, i
   }
   int rc = r.setup(device);
   if (rc == HIPFT_OK) rc = r.main_loop();
+  if (rc == HIPFT_OK) rc = r.write_map(r.nl.output_map_root_filename + "_final.h5");  // wrap_it_up
   if (rc == HIPFT_OK && f_out) {
     hipft_info inf;
     hipft_gpu_info(r.h, &inf);

@@ -108,6 +108,8 @@ SIGNATURES = [
                                               ctypes.c_size_t]),
     ("hipft_h5_read", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
                                      DPTR, DPTR, DPTR, DPTR]),
+    ("hipft_h5_write", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), DPTR, DPTR,
+                                      DPTR, DPTR, ctypes.c_int]),
 ]
 
 _lib = None
@@ -155,6 +157,27 @@ def h5_read(path: str):
         raise HipftError(rc, "hipft_h5_read", path)
     shape = tuple(reversed(n[: nd.value]))
     return data.reshape(shape), sc[: nd.value]
+
+
+def h5_write(path: str, data: np.ndarray, scales, single_precision: bool = True) -> None:
+    """Write a HipFT HDF5 map as the reference's wrh5 does.  ``data`` is in
+    C order (shape (n3, n2, n1) for Fortran (n1, n2, n3)); ``scales`` lists
+    the Fortran-order scales (n1 values first)."""
+    L = lib()
+    a = np.ascontiguousarray(data, dtype=np.float64)
+    nd = a.ndim
+    if not 1 <= nd <= 3 or len(scales) != nd:
+        raise ValueError("data must have 1-3 dimensions and one scale per dimension")
+    fdims = list(reversed(a.shape))
+    sc = [np.ascontiguousarray(x, dtype=np.float64) for x in scales]
+    for x, n in zip(sc, fdims):
+        if x.shape != (n,):
+            raise ValueError("scale length does not match its dimension")
+    dims = (ctypes.c_int64 * 3)(*(fdims + [1] * (3 - nd)))
+    ptr = [_p(x) for x in sc] + [None] * (3 - nd)
+    rc = L.hipft_h5_write(path.encode(), nd, dims, _p(a), ptr[0], ptr[1], ptr[2], 1 if single_precision else 0)
+    if rc:
+        raise HipftError(rc, "hipft_h5_write", path)
 
 
 def run(namelist: str, run_dir: str, device: int = 0) -> int:

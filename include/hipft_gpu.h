@@ -256,6 +256,15 @@ int hipft_run_field(const char *namelist_path, const char *run_dir, int device, 
 int hipft_h5_read(const char *path, int *ndim, int64_t dims[3], double *data, double *s1,
                   double *s2, double *s3);
 
+/* Writer of the reference's HDF5 maps (wrh5, src/hipft.f90:6155-6351):
+ * dataset "Data" (float32 when single_precision, else float64) of Fortran
+ * dimensions dims[0..ndim-1] (dims[0] varies fastest in `data`) and scale
+ * datasets "dim1".."dimN" (s1..s3, converted like the data) attached to it
+ * as HDF5 dimension scales.  Returns HIPFT_EIO when the file cannot be
+ * written. */
+int hipft_h5_write(const char *path, int ndim, const int64_t dims[3], const double *data, const double *s1,
+                   const double *s2, const double *s3, int single_precision);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,7 @@ typedef struct {
       *flow_mf_coef_p3_values, *flow_mf_coef_p5_values,
       *assimilate_data_lat_limits, *assimilate_data_mu_powers,
       *assimilate_data_mu_limits;
+  int output_map_flux_balance;
 } orc_params;
 
 /* History rows, one block of nr rows per output event.
@@ -92,6 +93,12 @@ typedef struct {
 typedef struct {
   long cap, nrows;
   double *sol, *num;
+  /* maps the reference writes (write_map F:2801-2917), as f(ntm,npm,nr),
+   * flux-balanced copies when output_map_flux_balance; NULL = not kept.
+   * maps[map_cap]: numbered outputs with their index and time. */
+  long map_cap, n_maps;
+  long *map_idx;
+  double *map_time, *maps, *map_initial, *map_final;
 } orc_hist;
 
 /* ------------------------------------------------------------------ state */
@@ -1274,7 +1281,17 @@ static void apply_data_assimilation(orc *S) {
   else S->time_of_next_input_map = S->da_times[S->da_idx];
 }
 
-/* output_map bookkeeping only (F:2726-2742): the map index drives dt cuts. */
+/* write_map's copy of f (F:2829-2843): balanced per realization if asked. */
+static void capture_map(orc *S, double *dst) {
+  if (!dst) return;
+  const size_t plane = (size_t)S->ntm * S->npm;
+  memcpy(dst, S->f, sizeof(double) * plane * S->nr);
+  if (S->P->output_map_flux_balance)
+    for (int i = 1; i <= S->nr; i++) balance_flux(S, dst + (size_t)(i - 1) * plane);
+}
+
+/* output_map (F:2700-2798): the map index drives dt cuts; the maps
+ * themselves are kept in the history struct when it asks for them. */
 static void output_map_index(orc *S) {
   const orc_params *P = S->P;
   if (P->output_map_idx_cadence > 0 && S->ntime % P->output_map_idx_cadence == 0) S->output_current_map = 1;
@@ -1283,6 +1300,13 @@ static void output_map_index(orc *S) {
     S->output_current_map = 1;
   if (S->output_current_map) {
     S->idx_out++;
+    orc_hist *H = S->hist;
+    if (H && H->maps && H->n_maps < H->map_cap) {
+      capture_map(S, H->maps + (size_t)H->n_maps * S->ntm * S->npm * S->nr);
+      H->map_idx[H->n_maps] = S->idx_out;
+      H->map_time[H->n_maps] = S->time;
+      H->n_maps++;
+    }
     S->output_current_map = 0;
   }
 }
@@ -1390,6 +1414,7 @@ int orc_run(const orc_params *P, int n1, int n2, const double *s1in, const doubl
   if (P->initial_map_flux_balance)
     for (int i = 1; i <= nr; i++) balance_flux(S, S->f + (size_t)(i - 1) * ntm * npm);
   for (size_t q = 0; q < (size_t)ntm * npm * nr; q++) S->f[q] = P->initial_map_mult_fac * S->f[q];
+  if (hist) capture_map(S, hist->map_initial); /* <root>_initial.h5, F:2185 */
   free(s1); free(s2); free(f_local);
 
   S->time = P->time_start;
@@ -1437,6 +1462,7 @@ int orc_run(const orc_params *P, int n1, int n2, const double *s1in, const doubl
     if (max_steps > 0 && S->ntime >= max_steps) break;
   }
   if (f_out) memcpy(f_out, S->f, sizeof(double) * (size_t)ntm * npm * nr);
+  if (hist) capture_map(S, hist->map_final); /* <root>_final.h5, F:1390 */
   if (timing_out) {
     timing_out[0] = (double)S->ntime;
     timing_out[1] = S->time;

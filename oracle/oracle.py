@@ -29,7 +29,8 @@ DEFAULTS = dict(
     initial_map_mult_fac=1.0,
     output_map_idx_start=1, output_map_idx_cadence=0,
     output_map_time_cadence=0.0, output_history_time_cadence=0.0,
-    output_single_precision=True,
+    output_single_precision=True, output_map_flux_balance=False, output_map_2d=True,
+    output_map_root_filename="hipft_brmap", output_map_directory="output_maps",
     time_start=0.0, time_end=1.0, dt_min=1.0e-15,
     dt_max=float(np.finfo(np.float64).max),
     strang_splitting=False, pole_flux_lat_limit=30.0,
@@ -163,13 +164,20 @@ class OrcParams(ctypes.Structure):
         "diffusion_coef_constants", "flow_attenuate_values",
         "flow_dr_coef_p0_values", "flow_dr_coef_p2_values", "flow_dr_coef_p4_values",
         "flow_mf_coef_p1_values", "flow_mf_coef_p3_values", "flow_mf_coef_p5_values",
-        "assimilate_data_lat_limits", "assimilate_data_mu_powers", "assimilate_data_mu_limits")]
+        "assimilate_data_lat_limits", "assimilate_data_mu_powers", "assimilate_data_mu_limits")] + [
+        ("output_map_flux_balance", ctypes.c_int)]
 
 
 class OrcHist(ctypes.Structure):
     _fields_ = [("cap", ctypes.c_long), ("nrows", ctypes.c_long),
                 ("sol", ctypes.POINTER(ctypes.c_double)),
-                ("num", ctypes.POINTER(ctypes.c_double))]
+                ("num", ctypes.POINTER(ctypes.c_double)),
+                ("map_cap", ctypes.c_long), ("n_maps", ctypes.c_long),
+                ("map_idx", ctypes.POINTER(ctypes.c_long)),
+                ("map_time", ctypes.POINTER(ctypes.c_double)),
+                ("maps", ctypes.POINTER(ctypes.c_double)),
+                ("map_initial", ctypes.POINTER(ctypes.c_double)),
+                ("map_final", ctypes.POINTER(ctypes.c_double))]
 
 
 _lib = None
@@ -217,11 +225,14 @@ def _params_struct(p: dict):
 
 
 def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
-        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True):
+        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True, map_cap: int = 0):
     """Run the oracle on processed parameters ``p``.
 
     map_pt: (nr, ntm, npm1) C-order array (i.e. Fortran (npm1,ntm,nr)), or None.
     Returns dict(sol=(rows,nr,16), num=(rows,nr,8), f=(nr,npm,ntm) or None).
+    With map_cap > 0 also maps=(n,nr,npm,ntm), map_idx, map_time (the numbered
+    map outputs, at most map_cap) and map_initial, map_final (nr,npm,ntm): the
+    fields write_map writes, flux-balanced when output_map_flux_balance.
     """
     L = lib()
     nr = int(p["n_realizations"])
@@ -244,6 +255,18 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
     h.cap = hist_cap
     h.sol = sol.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     h.num = num.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    maps = None
+    if map_cap > 0:
+        maps = np.zeros((map_cap, nr, npm, ntm))
+        map_idx = np.zeros(map_cap, dtype=np.int64)
+        map_time = np.zeros(map_cap)
+        map_initial = np.zeros((nr, npm, ntm))
+        map_final = np.zeros((nr, npm, ntm))
+        dptr = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        h.map_cap = map_cap
+        h.map_idx = map_idx.ctypes.data_as(ctypes.POINTER(ctypes.c_long))
+        h.map_time, h.maps = dptr(map_time), dptr(maps)
+        h.map_initial, h.map_final = dptr(map_initial), dptr(map_final)
     f = np.zeros((nr, npm, ntm)) if want_field else None
     n_da = 0
     if da_times is not None:
@@ -258,8 +281,13 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
     if rc != 0:
         raise RuntimeError(f"oracle failed with code {rc}")
     n = min(h.nrows, hist_cap)
-    return dict(sol=sol[:n].copy(), num=num[:n].copy(), f=f, nsteps=int(tinfo[0]),
-                time=float(tinfo[1]), cell_updates=float(tinfo[2]))
+    out = dict(sol=sol[:n].copy(), num=num[:n].copy(), f=f, nsteps=int(tinfo[0]),
+               time=float(tinfo[1]), cell_updates=float(tinfo[2]))
+    if maps is not None:
+        m = int(h.n_maps)
+        out.update(maps=maps[:m], map_idx=map_idx[:m], map_time=map_time[:m], map_initial=map_initial,
+                   map_final=map_final)
+    return out
 
 
 def da_blend(p: dict, t, ph, f, map3):

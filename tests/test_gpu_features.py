@@ -67,6 +67,8 @@ CASES = {
 
 def _namelist(d: dict) -> str:
     def fmt(v):
+        if isinstance(v, str):
+            return "'" + v + "'"
         if isinstance(v, bool):
             return ".true." if v else ".false."
         if isinstance(v, (list, tuple)):
