@@ -166,8 +166,68 @@ bool make_dirs(const std::string &d) {
   return true;
 }
 
+// Flow list of use_flow_from_files, read as READ(...,'(F11.5,1X,A11,1X,A11)')
+// reads it (src/hipft.f90:3735-3746): the Julian day in columns 1-11, the
+// theta-velocity file in 13-23 and the phi-velocity file in 25-35.
+struct FlowFiles {
+  std::vector<double> times;  // flow_from_files_times, hours
+  std::vector<std::string> vt, vp;
+  int idx = 0;  // current entry, 1-based
+  double t_cur = 0.0, t_next = 0.0, dt_last = 0.0;
+};
+
+// A Fortran F edit field: blanks ignored, D exponents, implied decimals.
+bool f_field(const std::string &fld, int decimals, double &v) {
+  std::string digits;
+  for (char c : fld)
+    if (c != ' ') digits += (c == 'd' || c == 'D') ? 'E' : c;
+  if (digits.empty()) return false;
+  char *end = nullptr;
+  v = std::strtod(digits.c_str(), &end);
+  if (*end != '\0') return false;
+  if (digits.find_first_of(".eE") == std::string::npos) v /= std::pow(10.0, decimals);
+  return true;
+}
+
+std::string a_field(const std::string &line, size_t pos, size_t n) {
+  std::string f = pos < line.size() ? line.substr(pos, n) : std::string();
+  while (!f.empty() && (f.back() == ' ' || f.back() == '\t')) f.pop_back();
+  return f;
+}
+
+bool read_flow_list(const std::string &path, FlowFiles &L, std::string &err) {
+  std::ifstream in(path);
+  if (!in) {
+    err = "cannot open flow list " + path;
+    return false;
+  }
+  std::string line;
+  std::getline(in, line);  // header row
+  while (std::getline(in, line)) {
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    if (line.find_first_not_of(" \t") == std::string::npos) continue;
+    double jd;
+    if (!f_field(line.substr(0, 11), 5, jd)) {
+      err = "bad Julian day in flow list " + path + ": " + line;
+      return false;
+    }
+    L.times.push_back(24.0 * jd);
+    L.vt.push_back(a_field(line, 12, 11));
+    L.vp.push_back(a_field(line, 24, 11));
+  }
+  if (L.times.size() < 2) {
+    err = "the flow list " + path + " needs at least two entries";
+    return false;
+  }
+  // src/hipft.f90:3750-3753, in place and in order: entries after the first
+  // subtract the already-zeroed first one (no effect when the list starts at 0)
+  for (size_t i = 0; i < L.times.size(); ++i) L.times[i] = L.times[i] - L.times[0];
+  return true;
+}
+
 struct Run {
   Namelist nl;
+  FlowFiles ff;
   std::string dir;
   std::string map_dir;             // output_map_directory (relative to the run directory)
   std::vector<double> pscale, tscale;  // the map scales: p(1:npm1), t(1:ntm)
@@ -230,6 +290,68 @@ struct Run {
       std::fclose(fn);
       std::fclose(fs);
     }
+    return HIPFT_OK;
+  }
+
+  // read_2d_file of one flow pair and hand it to the library
+  // (add_flow_from_files src/hipft.f90:3578-3634, load_flow_from_files 3765-3800)
+  int read_flow_pair(int idx, int at_load) {
+    hipft_info inf;
+    hipft_gpu_info(h, &inf);
+    const int64_t ntm = inf.ntm, nt = ntm + 1, np = inf.npm, npm1 = inf.npm - 1;
+    std::vector<double> vt, vp;
+    const std::string *names[2] = {&ff.vt[idx - 1], &ff.vp[idx - 1]};
+    std::vector<double> *dst[2] = {&vt, &vp};
+    const int64_t want[2][2] = {{npm1, nt}, {np, ntm}};
+    for (int q = 0; q < 2; ++q) {
+      std::string f = nl.flow_root_dir + "/" + *names[q];
+      if (f[0] != '/') f = path(f);
+      int nd = 0;
+      int64_t dims[3];
+      int rc = hipft_h5_read(f.c_str(), &nd, dims, nullptr, nullptr, nullptr, nullptr);
+      if (rc || nd != 2 || dims[0] != want[q][0] || dims[1] != want[q][1]) {
+        err = "cannot read flow file " + f + " as a 2D map of the run's grid";
+        return rc ? rc : HIPFT_EINVAL;
+      }
+      dst[q]->resize((size_t)(dims[0] * dims[1]));
+      rc = hipft_h5_read(f.c_str(), &nd, dims, dst[q]->data(), nullptr, nullptr, nullptr);
+      if (rc) return rc;
+    }
+    return hipft_gpu_set_flow_from_files(h, vt.data(), vp.data(), at_load);
+  }
+
+  // load_flow_from_files (src/hipft.f90:3675-3800)
+  int load_flow_from_files() {
+    if (!read_flow_list(path(nl.flow_list_filename), ff, err)) return HIPFT_EIO;
+    const int n = (int)ff.times.size();
+    const double span = ff.times[n - 1] - ff.times[0];
+    const double tsf = nl.time_start - std::floor(nl.time_start / span) * span;  // MODULO
+    int idx = 0;
+    for (int i = 1; i < n; ++i)
+      if (std::fabs(ff.times[i] - tsf) < std::fabs(ff.times[idx] - tsf)) idx = i;
+    idx += 1;
+    if (ff.times[idx - 1] > tsf) idx -= 1;
+    ff.idx = idx;
+    int rc = read_flow_pair(idx, 1);
+    if (rc) return rc;
+    ff.dt_last = ff.times[n - 1] - ff.times[n - 2];
+    ff.t_cur = nl.time_start - tsf + ff.times[idx - 1];
+    const double delta = (idx + 1 > n) ? ff.dt_last : ff.times[idx] - ff.times[idx - 1];
+    ff.t_next = ff.t_cur + delta;
+    return HIPFT_OK;
+  }
+
+  // the file part of add_flow_from_files (src/hipft.f90:3552-3658)
+  int advance_flow_files() {
+    if (!(nl.advance_flow && nl.use_flow_from_files) || time < ff.t_next) return HIPFT_OK;
+    const int n = (int)ff.times.size();
+    ff.idx += 1;
+    if (ff.idx > n) ff.idx = 1;
+    int rc = read_flow_pair(ff.idx, 0);
+    if (rc) return rc;
+    ff.t_cur = ff.t_next;
+    const double delta = (ff.idx + 1 > n) ? ff.dt_last : ff.times[ff.idx] - ff.times[ff.idx - 1];
+    ff.t_next = ff.t_cur + delta;
     return HIPFT_OK;
   }
 
@@ -328,6 +450,10 @@ struct Run {
       dtime_global = time_of_next_input_map - time;
       timestep_needs_updating = timestep_flow_needs_updating = time_step_changed = true;
     }
+    if (nl.advance_flow && nl.use_flow_from_files && time + dtime_global >= ff.t_next) {  // src/hipft.f90:4415
+      dtime_global = ff.t_next - time;
+      timestep_needs_updating = timestep_flow_needs_updating = time_step_changed = true;
+    }
     if (time + dtime_global >= nl.time_end) {
       dtime_global = nl.time_end - time;
       timestep_needs_updating = false;
@@ -389,10 +515,6 @@ struct Run {
     hist.assign((size_t)nr * 14, 0.0);
     if (nl.advance_source) {
       err = "sources (advance_source) are not part of this library";
-      return HIPFT_EINVAL;
-    }
-    if (nl.use_flow_from_files) {
-      err = "flows from files are not supported yet";
       return HIPFT_EINVAL;
     }
     if (!nl.diffusion_coef_filename.empty()) {
@@ -542,6 +664,10 @@ struct Run {
       d.flow_attenuate_values = nl.flow_attenuate_values.data();
       rc = hipft_gpu_set_flow(h, &d);
       if (rc) return rc;
+      if (nl.use_flow_from_files) {
+        rc = load_flow_from_files();
+        if (rc) return rc;
+      }
     }
     hipft_info inf;
     hipft_gpu_info(h, &inf);
@@ -624,7 +750,9 @@ struct Run {
       ntime++;
       if (nl.advance_flow) {
         int upd = 0;
-        int rc = hipft_gpu_update_flow(h, &upd);
+        int rc = advance_flow_files();
+        if (rc) return rc;
+        rc = hipft_gpu_update_flow(h, &upd);
         if (rc) return rc;
         if (upd) timestep_flow_needs_updating = timestep_needs_updating = true;
       }

@@ -72,6 +72,9 @@ struct hipft_gpu {
   bool field_set = false;
   // flows
   bool have_flow = false, flow_needs_updating = false, flow2d = false;
+  bool have_file_flow = false;               // flows from files are the base of vt, vp
+  double *d_vtf = nullptr, *d_vpf = nullptr;  // [npm][nt+1], [np][ntm+1]
+  double *d_fterms = nullptr;                 // analytic terms applied over the file flow
   hipft_flow_def fdef{};
   std::vector<double> f_p0, f_p2, f_p4, f_p1, f_p3, f_p5, f_att;
   double *d_vt1 = nullptr, *d_vp1 = nullptr, *d_at1 = nullptr, *d_ap1 = nullptr;
@@ -571,7 +574,10 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   h->ldv = round_up(h->nt, 16);
   h->plane = (int64_t)h->ldt * h->npm;
   h->fieldn = (size_t)h->plane * h->nr;
-  if (prm->advance_diffusion) h->Dc.assign(prm->diffusion_coef_constants, prm->diffusion_coef_constants + g->nr);
+  // the per-realization constants also set validation run 1's decay rate
+  // (src/hipft.f90:3156-3159), diffusion or not
+  if (prm->diffusion_coef_constants)
+    h->Dc.assign(prm->diffusion_coef_constants, prm->diffusion_coef_constants + g->nr);
   int fm = prm->flow_num_method;
   h->adv_time = (fm == 1) ? 1 : (fm == 4 ? 3 : 2);
   h->adv_space = (fm <= 2) ? 1 : 2;
@@ -925,10 +931,42 @@ static void analytic_profiles(const hipft_gpu *h, std::vector<double> &vt1, std:
   }
 }
 
+extern "C" int hipft_gpu_set_flow_from_files(hipft_gpu *h, const double *vt_pt, const double *vp_pt,
+                                             int at_load) {
+  if (!h || !vt_pt || !vp_pt) return HIPFT_EINVAL;
+  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "set_flow_from_files: advance_flow is off for this handle");
+  CK(h, cudaSetDevice(h->dev));
+  const int nt = h->nt, ntm = h->ntm, npm = h->npm, np = h->np, npm1 = h->npm1;
+  std::vector<double> vt((size_t)npm * (nt + 1), 0.0), vp((size_t)np * (ntm + 1), 0.0);
+  auto T = [&](int j, int k) -> double & { return vt[(size_t)(k - 1) * (nt + 1) + j]; };
+  auto P = [&](int j, int k) -> double & { return vp[(size_t)(k - 1) * (ntm + 1) + j]; };
+  for (int k = 1; k <= npm1; ++k)
+    for (int j = 1; j <= nt; ++j) T(j, k) = c_m_s_to_rs_hr * vt_pt[(size_t)(j - 1) * npm1 + (k - 1)];
+  for (int k = 1; k <= np; ++k)
+    for (int j = 1; j <= ntm; ++j) P(j, k) = c_m_s_to_rs_hr * vp_pt[(size_t)(j - 1) * np + (k - 1)];
+  if (at_load) {
+    for (int j = 1; j <= nt; ++j) T(j, npm) = T(j, 2);  // src/hipft.f90:3789
+  } else {                                             // set_periodic_bc_3d, src/hipft.f90:3604, 3634
+    for (int j = 1; j <= nt; ++j) { T(j, 1) = T(j, npm - 1); T(j, npm) = T(j, 2); }
+    for (int j = 1; j <= ntm; ++j) { P(j, 1) = P(j, np - 1); P(j, np) = P(j, 2); }
+  }
+  if (!h->d_vtf) {
+    TRY(dalloc(h, &h->d_vtf, vt.size()));
+    TRY(dalloc(h, &h->d_vpf, vp.size()));
+  }
+  TRY(upload(h, h->d_vtf, vt));
+  TRY(upload(h, h->d_vpf, vp));
+  CK(h, cudaStreamSynchronize(h->stream));  // the host staging vectors go out of scope
+  h->have_file_flow = true;
+  h->flow2d = true;
+  h->flow_needs_updating = true;
+  return HIPFT_OK;
+}
+
 extern "C" int hipft_gpu_update_flow(hipft_gpu *h, int *updated) {
   if (!h) return HIPFT_EINVAL;
   if (updated) *updated = 0;
-  if (!h->have_flow || !h->flow_needs_updating) return HIPFT_OK;
+  if (!(h->have_flow || h->have_file_flow) || !h->flow_needs_updating) return HIPFT_OK;
   CK(h, cudaSetDevice(h->dev));
   h->flow_needs_updating = false;
   int nt = h->nt, ntm = h->ntm, nr = h->nr, npm = h->npm;
@@ -992,6 +1030,36 @@ extern "C" int hipft_gpu_update_flow(hipft_gpu *h, int *updated) {
     b.vrigid = h->fdef.flow_rigid_omega * c_km_s_to_rs_hr;
     b.attenuate = h->fdef.flow_attenuate;
     b.atten_i = h->d_atten;
+    if (h->have_file_flow) {
+      // the analytic terms one by one, as update_flow adds them over the
+      // file flow (src/hipft.f90:3416-3437, 7219-7285)
+      const hipft_flow_def &d = h->fdef;
+      const size_t nT = (size_t)nr * (nt + 1), nP = (size_t)nr * (ntm + 1);
+      std::vector<double> terms(nT + nP + (size_t)(ntm + 1), 0.0);
+      double *tmf = terms.data(), *vdr = tmf + nT, *vrg = vdr + nP;
+      for (int i = 1; i <= nr; ++i) {
+        for (int j = 1; j <= nt; ++j) {
+          double c = h->cth[j];
+          tmf[(size_t)(i - 1) * (nt + 1) + j] =
+              c_m_s_to_rs_hr * h->sth[j] * (h->f_p1[i - 1] * c + h->f_p3[i - 1] * pow3(c) + h->f_p5[i - 1] * pow5(c));
+        }
+        for (int j = 1; j <= ntm; ++j) {
+          double c = h->ct[j];
+          double c2 = c * c, c4 = c2 * c2;
+          vdr[(size_t)(i - 1) * (ntm + 1) + j] =
+              c_m_s_to_rs_hr * h->st[j] * (h->f_p0[i - 1] + h->f_p2[i - 1] * c2 + h->f_p4[i - 1] * c4);
+        }
+      }
+      for (int j = 1; j <= ntm; ++j) vrg[j] = d.flow_vp_rigid_omega * c_km_s_to_rs_hr * h->st[j];
+      if (!h->d_fterms) TRY(dalloc(h, &h->d_fterms, terms.size()));
+      TRY(upload(h, h->d_fterms, terms));
+      b.vtf = h->d_vtf;
+      b.vpf = h->d_vpf;
+      b.tmf = (d.flow_mf_model == 1) ? h->d_fterms : nullptr;
+      b.vdr = (d.flow_dr_model == 1) ? h->d_fterms + nT : nullptr;
+      b.vrg = (d.flow_vp_rigid_omega != 0.0) ? h->d_fterms + nT + nP : nullptr;
+      b.vtc = (d.flow_vt_const != 0.0) ? d.flow_vt_const * c_km_s_to_rs_hr : 0.0;
+    }
     dim3 blk(32, 8), grd((unsigned)((nt + 31) / 32), (unsigned)((npm + 7) / 8), (unsigned)nr);
     k_flow_build<<<grd, blk, 0, h->stream>>>(h->M, b, h->ldv, h->buf[h->cur], h->d_vt, h->d_vp);
     LAUNCHED(h);
@@ -1002,6 +1070,7 @@ extern "C" int hipft_gpu_update_flow(hipft_gpu *h, int *updated) {
       LAUNCHED(h);
       h->flow_needs_updating = true;  // Br changes every step (src/hipft.f90:3514)
     }
+    if (h->have_file_flow) h->flow_needs_updating = true;  // src/hipft.f90:3423
     if (h->adv_space == 2) {
       dim3 g2((unsigned)((ntm + 31) / 32), (unsigned)((npm + 7) / 8), (unsigned)nr);
       k_lf_alpha<<<g2, blk, 0, h->stream>>>(h->M, h->ldv, h->d_vt, h->d_vp, h->d_at, h->d_ap);
@@ -1375,7 +1444,8 @@ extern "C" int hipft_gpu_set_validation(hipft_gpu *h, int mode, const double *fv
   h->vtime_start = time_start;
   if (mode == 1) {
     if (!fval_u0_pt) return HIPFT_EINVAL;
-    if (!h->P.advance_diffusion) return fail(h, HIPFT_ESTATE, "validation 1 needs diffusion coefficients");
+    if ((int)h->Dc.size() != h->nr)
+      return fail(h, HIPFT_ESTATE, "validation 1 needs the diffusion coefficient constants");
     size_t n = (size_t)h->npm1 * h->ntm * h->nr;
     if (!h->d_fval_u0) TRY(dalloc(h, &h->d_fval_u0, n));
     CK(h, cudaMemcpyAsync(h->d_fval_u0, fval_u0_pt, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));

@@ -489,6 +489,14 @@ __global__ void k_flow_dtmax(Mesh m, Flow fl, unsigned long long *min_bits) {
 // the vt (nt x npm) and vp (ntm x np) grids.
 struct Flow2DBuild {
   const double *vt1, *vp1;  // analytic 1-D parts, [nr][nt+1], [nr][ntm+1]
+  // flows from files (shared by all realizations): when vtf is set, v starts
+  // from vtf[k][j] ([npm][nt+1]) / vpf[k][j] ([np][ntm+1]) and the analytic
+  // terms are applied one by one in update_flow's order instead of vt1/vp1
+  const double *vtf, *vpf;
+  const double *tmf;   // meridional term to subtract, [nr][nt+1] (NULL: model off)
+  const double *vdr;   // differential rotation term to add, [nr][ntm+1] (NULL: off)
+  const double *vrg;   // rigid rotation term to add, [ntm+1] (NULL: off)
+  double vtc;          // constant theta velocity (0: off)
   const double *cth, *sth, *ct, *st;  // 1-based
   const double *cosp, *sinp, *cosph;  // cos(p(k)), sin(p(k)), cos(ph(k)), 1-based
   double vrigid;      // flow_rigid_omega * km_s_to_rs_hr (0: off)
@@ -505,7 +513,14 @@ __global__ void k_flow_build(Mesh m, Flow2DBuild b, int ldv, const double *__res
   const int i = blockIdx.z + 1;
   const int64_t base = ((int64_t)(i - 1) * m.npm + (k - 1)) * ldv + (j - 1);
   if (j <= m.nt && k <= m.npm) {
-    double v = b.vt1[(int64_t)(i - 1) * (m.nt + 1) + j];
+    double v;
+    if (b.vtf) {
+      v = b.vtf[(int64_t)(k - 1) * (m.nt + 1) + j];
+      if (b.tmf) v = v - b.tmf[(int64_t)(i - 1) * (m.nt + 1) + j];
+      if (b.vtc != 0.0) v = v + b.vtc;
+    } else {
+      v = b.vt1[(int64_t)(i - 1) * (m.nt + 1) + j];
+    }
     if (b.vrigid != 0.0) {
       double cp = b.cosp[k], c = b.cth[j], sv = b.sth[j];
       double acp = fabs(cp);
@@ -531,7 +546,14 @@ __global__ void k_flow_build(Mesh m, Flow2DBuild b, int ldv, const double *__res
     vt[base] = v;
   }
   if (j <= m.ntm && k <= m.np) {
-    double v = b.vp1[(int64_t)(i - 1) * (m.ntm + 1) + j];
+    double v;
+    if (b.vpf) {
+      v = b.vpf[(int64_t)(k - 1) * (m.ntm + 1) + j];
+      if (b.vdr) v = v + b.vdr[(int64_t)(i - 1) * (m.ntm + 1) + j];
+      if (b.vrg) v = v + b.vrg[j];
+    } else {
+      v = b.vp1[(int64_t)(i - 1) * (m.ntm + 1) + j];
+    }
     if (b.vrigid != 0.0) {
       double cph = b.cosph[k], c = b.ct[j], sv = b.st[j];
       double p1 = b.vrigid * (cph * cph * c + sv * cph - c) * sgn1(cph) * fabs(sv);

@@ -252,7 +252,8 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"assimilate_data_map_list_filename", &nl.assimilate_data_map_list_filename},
       {"assimilate_data_map_root_dir", &nl.assimilate_data_map_root_dir},
       {"output_flows_directory", nullptr}, {"output_flows_root_filename", nullptr},
-      {"flow_list_filename", nullptr}, {"flow_root_dir", nullptr}, {"source_filename", nullptr}};
+      {"flow_list_filename", &nl.flow_list_filename}, {"flow_root_dir", &nl.flow_root_dir},
+      {"source_filename", nullptr}};
   std::map<std::string, int> ignored_ints = {{"source_rfe_model", 0}, {"source_rfe_seed", 0}};
 
   for (const auto &a : assigns) {

@@ -43,6 +43,7 @@ struct Namelist {
   double flow_mf_coef_p1_value = 22.0, flow_mf_coef_p3_value = 11.0,
          flow_mf_coef_p5_value = -28.0;
   bool use_flow_from_files = false;
+  std::string flow_list_filename, flow_root_dir = ".";
   int flow_num_method = 4;
   double upwind = 1.0, weno_eps = 0.0;
   bool advance_diffusion = false;

@@ -66,7 +66,7 @@ typedef struct {
   int diffusion_subcycles;    /* 0 = automatic (PTL) subcycling               */
   int diffusion_coef_grid;    /* add grid-based diffusion                      */
   double diffusion_coef_factor; /* km^2/s -> Rs^2/hr by default               */
-  const double *diffusion_coef_constants; /* [nr], km^2/s                     */
+  const double *diffusion_coef_constants; /* [nr], km^2/s; also validation 1   */
   double pole_flux_lat_limit; /* degrees, for the polar-flux diagnostics       */
   int verbose;
 } hipft_params;
@@ -145,6 +145,16 @@ int hipft_gpu_set_flow(hipft_gpu *h, const hipft_flow_def *def);
  * set_lf_alpha 6940) when needed.  *updated = 1 when the flow changed, which
  * tells the caller to recompute the CFL limit. */
 int hipft_gpu_update_flow(hipft_gpu *h, int *updated);
+/* Flows from files (use_flow_from_files): the 2-D flow, shared by all
+ * realizations, that update_flow starts from before adding the analytic
+ * models (flow_from_files_current_vt/vp of add_flow_from_files,
+ * src/hipft.f90:3525-3673, and load_flow_from_files, 3675-3800).
+ * vt_pt: the theta-velocity file as read, (npm1, nt) phi fastest, in m/s;
+ * vp_pt: the phi-velocity file, (np, ntm).  at_load != 0 applies the
+ * load-time phi rule (vt column npm = column 2), else the update rule
+ * (set_periodic_bc_3d on both).  The flow is then rebuilt at every
+ * update_flow, as the reference does while flows come from files. */
+int hipft_gpu_set_flow_from_files(hipft_gpu *h, const double *vt_pt, const double *vp_pt, int at_load);
 /* get_flow_dtmax (src/hipft.f90:7287-7350): CFL limit over all cells and
  * realizations, x2 for Strang splitting, x2 for SSPRK(4,3). */
 int hipft_gpu_flow_dtmax(hipft_gpu *h, double *dtmax);

@@ -85,6 +85,10 @@ typedef struct {
       *assimilate_data_lat_limits, *assimilate_data_mu_powers,
       *assimilate_data_mu_limits;
   int output_map_flux_balance;
+  /* flows from files (use_flow_from_files): the list's Julian days and the
+   * files' contents in PT order, vt (npm1, nt) and vp (np, ntm) per entry, m/s */
+  int use_flow_from_files, n_flows;
+  const double *flow_jd, *flow_vt, *flow_vp;
 } orc_params;
 
 /* History rows, one block of nr rows per output event.
@@ -121,6 +125,10 @@ typedef struct {
   double *D_C_CPt, *D_C_MCt, *D_M_Tt, *D_CP_Tt, *D_P_Tt, *D_MC_Tt, *weno_eps_t;
   double *D_C_CPp, *D_C_MCp, *D_M_Tp, *D_CP_Tp, *D_P_Tp, *D_MC_Tp, *weno_eps_p;
   double *atten_i;
+  /* flows from files: current pair (flow_from_files_current_vt/vp) and times */
+  double *fvt, *fvp, *flow_times;
+  int flow_idx;
+  double time_of_current_input_flow, time_of_next_input_flow, flow_dt_last;
   /* diffusion */
   double *dcoef, *coef; /* dcoef (nt,np,nr); coef (2:ntm-1,2:npm-1,5,nr) */
   double bc_diffusion_npole_fac, bc_diffusion_spole_fac;
@@ -536,6 +544,76 @@ static void set_lf_alpha(orc *S) {
 
 /* --------------------------------------------------------- update_flow
  * F:3371-3523 with add_flow_*_analytic F:7219-7285 */
+/* One pair of flow files into fvt, fvp: add_flow_from_files F:3578-3634
+ * (at_load = 0: set_periodic_bc_3d on both) and load_flow_from_files
+ * F:3775-3800 (at_load = 1: only vt's column npm from column 2). */
+static void read_flow_pair(orc *S, int idx, int at_load) {
+  const orc_params *P = S->P;
+  int nt = S->nt, ntm = S->ntm, npm = S->npm, np = S->np, npm1 = S->npm1, nr = S->nr;
+  const double *ft = P->flow_vt + (size_t)(idx - 1) * npm1 * nt;
+  const double *fp = P->flow_vp + (size_t)(idx - 1) * np * ntm;
+  for (int k = 1; k <= nr; k++) {
+    for (int j = 1; j <= npm1; j++)
+      for (int i = 1; i <= nt; i++)
+        A3(S->fvt, i, j, k, nt, npm) = m_s_to_rs_hr * ft[(size_t)(i - 1) * npm1 + (j - 1)];
+    for (int j = 1; j <= np; j++)
+      for (int i = 1; i <= ntm; i++)
+        A3(S->fvp, i, j, k, ntm, np) = m_s_to_rs_hr * fp[(size_t)(i - 1) * np + (j - 1)];
+  }
+  if (at_load) {
+    for (int k = 1; k <= nr; k++)
+      for (int i = 1; i <= nt; i++) A3(S->fvt, i, npm, k, nt, npm) = A3(S->fvt, i, 2, k, nt, npm);
+  } else {
+    set_periodic_bc_3d(S->fvt, nt, npm, nr);
+    set_periodic_bc_3d(S->fvp, ntm, np, nr);
+  }
+}
+
+/* load_flow_from_files F:3675-3800 (times as the reference computes them). */
+static void load_flow_from_files(orc *S) {
+  const orc_params *P = S->P;
+  int n = P->n_flows;
+  S->flow_times = dalloc(n);
+  for (int i = 0; i < n; i++) S->flow_times[i] = twentyfour * P->flow_jd[i];
+  /* F:3750-3753: in place and in order, so entries after the first subtract
+   * the already-zeroed first entry (no effect when the list starts at 0) */
+  for (int i = 0; i < n; i++) S->flow_times[i] = S->flow_times[i] - S->flow_times[0];
+  double span = S->flow_times[n - 1] - S->flow_times[0];
+  double tsf = P->time_start - floor(P->time_start / span) * span; /* MODULO */
+  int idx = 0;
+  double best = fabs(S->flow_times[0] - tsf);
+  for (int i = 1; i < n; i++)
+    if (fabs(S->flow_times[i] - tsf) < best) { best = fabs(S->flow_times[i] - tsf); idx = i; }
+  idx += 1; /* 1-based */
+  if (S->flow_times[idx - 1] > tsf) idx -= 1;
+  S->flow_idx = idx;
+  S->fvt = dalloc((size_t)S->nt * S->npm * S->nr);
+  S->fvp = dalloc((size_t)S->ntm * S->np * S->nr);
+  read_flow_pair(S, idx, 1);
+  S->flow_dt_last = S->flow_times[n - 1] - S->flow_times[n - 2];
+  S->time_of_current_input_flow = P->time_start - tsf + S->flow_times[idx - 1];
+  double delta = (idx + 1 > n) ? S->flow_dt_last : S->flow_times[idx] - S->flow_times[idx - 1];
+  S->time_of_next_input_flow = S->time_of_current_input_flow + delta;
+}
+
+/* add_flow_from_files F:3525-3673 */
+static void add_flow_from_files(orc *S) {
+  const orc_params *P = S->P;
+  int n = P->n_flows;
+  if (S->time >= S->time_of_next_input_flow) {
+    S->flow_idx += 1;
+    if (S->flow_idx > n) S->flow_idx = 1;
+    read_flow_pair(S, S->flow_idx, 0);
+    S->time_of_current_input_flow = S->time_of_next_input_flow;
+    double delta = (S->flow_idx + 1 > n) ? S->flow_dt_last
+                                         : S->flow_times[S->flow_idx] - S->flow_times[S->flow_idx - 1];
+    S->time_of_next_input_flow = S->time_of_current_input_flow + delta;
+  }
+  size_t nv = (size_t)S->nt * S->npm * S->nr, np_ = (size_t)S->ntm * S->np * S->nr;
+  for (size_t q = 0; q < nv; q++) S->vt[q] = S->vt[q] + S->fvt[q];
+  for (size_t q = 0; q < np_; q++) S->vp[q] = S->vp[q] + S->fvp[q];
+}
+
 static void update_flow(orc *S) {
   const orc_params *P = S->P;
   int nt = S->nt, np = S->np, ntm = S->ntm, npm = S->npm, nr = S->nr;
@@ -545,6 +623,10 @@ static void update_flow(orc *S) {
   S->timestep_needs_updating = 1;
   memset(S->vt, 0, sizeof(double) * (size_t)nt * npm * nr);
   memset(S->vp, 0, sizeof(double) * (size_t)ntm * np * nr);
+  if (P->use_flow_from_files) { /* F:3417-3420: first, it overwrites */
+    add_flow_from_files(S);
+    S->flow_needs_updating = 1;
+  }
   if (P->flow_mf_model == 1) {
     for (int i = 1; i <= nr; i++)
       for (int k = 1; k <= npm; k++)
@@ -1183,6 +1265,15 @@ static void update_timestep(orc *S) {
       S->time_step_changed = 1;
     }
   }
+  if (P->advance_flow && P->use_flow_from_files) { /* F:4415-4426 */
+    if (S->time + S->dtime_global >= S->time_of_next_input_flow) {
+      S->dtime_global = S->time_of_next_input_flow - S->time;
+      S->timestep_needs_updating = 1;
+      S->flow_needs_updating = 1;
+      S->timestep_flow_needs_updating = 1;
+      S->time_step_changed = 1;
+    }
+  }
   if (S->time + S->dtime_global >= P->time_end) {
     S->dtime_global = P->time_end - S->time;
     S->timestep_needs_updating = 0;
@@ -1438,6 +1529,10 @@ int orc_run(const orc_params *P, int n1, int n2, const double *s1in, const doubl
       S->atten_i = dalloc(nr);
       for (int i = 0; i < nr; i++)
         S->atten_i[i] = (P->flow_attenuate_values[i] > zero) ? one / P->flow_attenuate_values[i] : DBL_MAX;
+    }
+    if (P->use_flow_from_files) {
+      if (P->n_flows < 2 || !P->flow_jd || !P->flow_vt || !P->flow_vp) return 3;
+      load_flow_from_files(S); /* F:2564 */
     }
   }
   if (P->advance_diffusion) load_diffusion(S);

@@ -31,6 +31,7 @@ DEFAULTS = dict(
     output_map_time_cadence=0.0, output_history_time_cadence=0.0,
     output_single_precision=True, output_map_flux_balance=False, output_map_2d=True,
     output_map_root_filename="hipft_brmap", output_map_directory="output_maps",
+    flow_list_filename="", flow_root_dir=".",
     time_start=0.0, time_end=1.0, dt_min=1.0e-15,
     dt_max=float(np.finfo(np.float64).max),
     strang_splitting=False, pole_flux_lat_limit=30.0,
@@ -165,7 +166,11 @@ class OrcParams(ctypes.Structure):
         "flow_dr_coef_p0_values", "flow_dr_coef_p2_values", "flow_dr_coef_p4_values",
         "flow_mf_coef_p1_values", "flow_mf_coef_p3_values", "flow_mf_coef_p5_values",
         "assimilate_data_lat_limits", "assimilate_data_mu_powers", "assimilate_data_mu_limits")] + [
-        ("output_map_flux_balance", ctypes.c_int)]
+        ("output_map_flux_balance", ctypes.c_int),
+        ("use_flow_from_files", ctypes.c_int), ("n_flows", ctypes.c_int),
+        ("flow_jd", ctypes.POINTER(ctypes.c_double)), ("flow_vt", ctypes.POINTER(ctypes.c_double)),
+        ("flow_vp", ctypes.POINTER(ctypes.c_double))]
+FLOW_FILE_FIELDS = ("n_flows", "flow_jd", "flow_vt", "flow_vp")  # set by run(flows=...)
 
 
 class OrcHist(ctypes.Structure):
@@ -213,6 +218,8 @@ def _params_struct(p: dict):
     keep = []
     c = OrcParams()
     for name, typ in OrcParams._fields_:
+        if name in FLOW_FILE_FIELDS:
+            continue
         if name in RVECS:
             arr = np.ascontiguousarray(np.asarray(p[name], dtype=np.float64))
             keep.append(arr)
@@ -225,7 +232,7 @@ def _params_struct(p: dict):
 
 
 def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
-        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True, map_cap: int = 0):
+        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True, map_cap: int = 0, flows=None):
     """Run the oracle on processed parameters ``p``.
 
     map_pt: (nr, ntm, npm1) C-order array (i.e. Fortran (npm1,ntm,nr)), or None.
@@ -233,10 +240,17 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
     With map_cap > 0 also maps=(n,nr,npm,ntm), map_idx, map_time (the numbered
     map outputs, at most map_cap) and map_initial, map_final (nr,npm,ntm): the
     fields write_map writes, flux-balanced when output_map_flux_balance.
+    flows (use_flow_from_files): dict(jd=(n,), vt=(n, nt, npm1), vp=(n, ntm, np)),
+    the flow list's Julian days and the files' data in C order, m/s.
     """
     L = lib()
     nr = int(p["n_realizations"])
     c, keep = _params_struct(p)
+    if flows is not None:
+        fa = [np.ascontiguousarray(flows[k], dtype=np.float64) for k in ("jd", "vt", "vp")]
+        keep.extend(fa)
+        c.n_flows = len(fa[0])
+        c.flow_jd, c.flow_vt, c.flow_vp = (a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in fa)
     if map_pt is not None:
         map_pt = np.ascontiguousarray(map_pt, dtype=np.float64)
         n2, n1 = map_pt.shape[-2], map_pt.shape[-1]
