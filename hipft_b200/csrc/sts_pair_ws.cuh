@@ -19,8 +19,11 @@
 //    per stage.  The consumers synchronise with named barrier 1 only.
 //
 // Tiles are walked phi tile fastest, so every CTA sees every theta block.
-// Shared memory per CTA: 2 x 48.8 KB buffers + 10.6 KB for Y_k = 108 KB, two
-// CTAs per SM.  Tiles holding rows 2 / ntm-1 publish ring partials of Y_k; the
+// Each buffer also carries a small tile record (realization, tile indices,
+// D and the pole terms of the input's ring sums) that the producer writes
+// before its arrival, so consumers start a tile without global loads or
+// index division.  Shared memory per CTA: 2 x 48.8 KB buffers + 10.6 KB for
+// Y_k = 108 KB, two CTAs per SM.  Tiles holding rows 2 / ntm-1 publish ring partials of Y_k; the
 // pole rows of Y_{k+1} and its ring sums are finished either by the last of
 // those tiles (atomic counter, no waiting; INLINE_POLES) or by k_pair_poles in
 // a launch of its own.
@@ -43,7 +46,8 @@ constexpr int kWU = kWY2 + (kWK + 2) * kWR;    // u0
 constexpr int kWD = kWU + (kWK + 2) * kWR;     // dty0
 constexpr int kWRT = kWD + (kWK + 2) * kWR;    // rows: {st_i, c2, c4, 0} per shared row
 constexpr int kWCT = kWRT + 4 * kWR;           // columns: {P1, P5} per shared column
-constexpr int kWBuf = kWCT + 2 * (kWK + 4);
+constexpr int kWInfo = kWCT + 2 * (kWK + 4);  // tile record: D, pole terms, (kt, rb, i)
+constexpr int kWBuf = kWInfo + 8;
 constexpr int kWYk = kWNB * kWBuf;             // Y_k: kWK+2 columns, consumers only
 constexpr int kWEnd = kWYk + (kWK + 2) * kWR;
 constexpr size_t kWSmem = (size_t)kWEnd * sizeof(double) + 2 * kWNB * sizeof(uint64_t);
@@ -195,8 +199,18 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       const int64_t pbase = (int64_t)(i - 1) * m.plane;
       double *B = wsm + b * kWBuf;
       const int nx = nk + 4, ny = nk + 2, ncp = nx + 3 * ny + 2;
-      if (lane == 0)
+      if (lane == 0) {
+        // the tile record, written before the arrival that releases it
+        double *I = B + kWInfo;
+        I[0] = dfac[i];
+        I[1] = ring_in[2 * (i - 1)] * bcn;
+        I[2] = -ring_in[2 * (i - 1) + 1] * bcs;
+        int *Ii = reinterpret_cast<int *>(I + 3);
+        Ii[0] = kt;
+        Ii[1] = rb;
+        Ii[2] = i;
         mbar_expect_tx(&full[b], (uint32_t)(nx + 3 * ny) * run + (uint32_t)(kWR * 32 + (kWK + 4) * 16));
+      }
       __syncwarp();
       for (int q = lane; q < ncp; q += 32) {
         const double *src;
@@ -244,14 +258,6 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
   int n = 0;
   for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
     const int b = n % kWNB, u = n / kWNB;
-    const int kt = t % pt.nkt, rest = t / pt.nkt;
-    const int rb = rest % pt.nb, i = rest / pt.nb + 1;
-    const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
-    const int nk = min(kWK, npm - 1 - k0 + 1);
-    const int64_t pbase = (int64_t)(i - 1) * m.plane;
-    const double Dr = dfac[i];
-    const double ax_n = ring_in[2 * (i - 1)] * bcn;
-    const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
     const bool landed = mbar_wait_bounded(&full[b], (uint32_t)(u & 1), 1u << 22);
     // one vote: every consumer stops together; also orders the previous
     // tile's reads of sYk before this tile's writes
@@ -260,6 +266,12 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       break;
     }
     const double *B = wsm + b * kWBuf;
+    const double Dr = B[kWInfo], ax_n = B[kWInfo + 1], ax_s = B[kWInfo + 2];
+    const int *Ii = reinterpret_cast<const int *>(B + kWInfo + 3);
+    const int kt = Ii[0], rb = Ii[1], i = Ii[2];
+    const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
+    const int nk = min(kWK, npm - 1 - k0 + 1);
+    const int64_t pbase = (int64_t)(i - 1) * m.plane;
     const double *X1 = B + kWX1, *Y2 = B + kWY2, *U = B + kWU, *D = B + kWD, *RT = B + kWRT;
     const double2 *CT = reinterpret_cast<const double2 *>(B + kWCT);
     const int64_t seam = (int64_t)(npm - 2) * ld;
