@@ -14,6 +14,9 @@
 #include <sys/stat.h>
 
 #include <cfloat>
+#include <ctime>
+#include <cstdint>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -35,6 +38,8 @@ constexpr double c_pi_four = 0.7853981633974483;
 constexpr double c_twopi = 6.2831853071795864;
 constexpr double c_threepi_two = 4.71238898038469;
 constexpr double c_km_s_to_rs_hr = 0.005172413793103448;
+constexpr double c_rsun_cm2 = 4.84416e21;        // src/hipft.f90:119
+constexpr double c_input_flux_fac = 1.0e21;      // src/hipft.f90:132
 
 // Fortran 1PE23.15E3: sign column, one digit, 15 decimals, 3-digit exponent.
 std::string fmt_e(double v) {
@@ -225,9 +230,110 @@ bool read_flow_list(const std::string &path, FlowFiles &L, std::string &err) {
   return true;
 }
 
+// Normal deviates for the random flux emergence source: get_gaussian
+// (src/hipft.f90:8616-8670), the Marsaglia-Bray polar method, with its second
+// deviate kept for the next call.  The uniform numbers come from xoshiro256**
+// (Blackman and Vigna) seeded through splitmix64 from source_rfe_seed; the
+// reference draws them with gfortran's RANDOM_NUMBER, so a seeded run here
+// is reproducible but does not repeat the reference's random field.
+struct Gaussian {
+  uint64_t s[4] = {1, 2, 3, 4};
+  bool second = false;
+  double v = 0.0, sln = 0.0;
+  void seed(uint64_t x) {
+    for (auto &w : s) {
+      x += 0x9e3779b97f4a7c15ULL;
+      uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+      w = z ^ (z >> 31);
+    }
+    second = false;
+  }
+  static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+  uint64_t next() {
+    const uint64_t r = rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotl(s[3], 45);
+    return r;
+  }
+  double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }  // [0, 1)
+  double operator()() {
+    if (second) {
+      second = false;
+      return v * sln;
+    }
+    second = true;
+    double u, q;
+    for (;;) {
+      u = 2.0 * uniform() - 1.0;
+      v = 2.0 * uniform() - 1.0;
+      q = u * u + v * v;
+      if (q < 1.0 && q > 0.0) break;
+    }
+    sln = std::sqrt(-(2.0 * std::log(q)) / q);
+    return u * sln;
+  }
+};
+
+// interp2d with flint's monotonicity check and interp (src/hipft.f90:
+// 7992-8073, 8083-8176, 8178-8210): bilinear from (xi, yi, fi(nxi, nyi)) onto
+// (x, y); points outside the table are 0.  Returns false when a scale is not
+// strictly increasing.
+bool interp2d(const std::vector<double> &xi, const std::vector<double> &yi, const std::vector<double> &fi,
+              const std::vector<double> &x, const std::vector<double> &y, std::vector<double> &f) {
+  const int nxi = (int)xi.size(), nyi = (int)yi.size(), nx = (int)x.size(), ny = (int)y.size();
+  for (int i = 0; i + 1 < nxi; ++i)
+    if (xi[i + 1] <= xi[i]) return false;
+  for (int i = 0; i + 1 < nyi; ++i)
+    if (yi[i + 1] <= yi[i]) return false;
+  auto interp = [](const std::vector<double> &t, double xv, int &i0, int &i1, double &a) {
+    const int n = (int)t.size();
+    if (n == 1 && xv == t[0]) {
+      i0 = i1 = 0;
+      a = 0.0;
+      return true;
+    }
+    for (int i = 0; i < n - 1; ++i)
+      if (xv >= t[i] && xv <= t[i + 1]) {
+        i0 = i;
+        i1 = i + 1;
+        a = (t[i] == t[i + 1]) ? 0.0 : (xv - t[i]) / (t[i + 1] - t[i]);
+        return true;
+      }
+    return false;
+  };
+  f.assign((size_t)nx * ny, 0.0);
+  for (int j = 0; j < ny; ++j) {
+    const double yv = y[j];
+    int jj, jp;
+    double ay;
+    if (yv < yi[0] || yv > yi[nyi - 1] || !interp(yi, yv, jj, jp, ay)) continue;
+    for (int i = 0; i < nx; ++i) {
+      const double xv = x[i];
+      int ii, ip;
+      double ax;
+      if (xv < xi[0] || xv > xi[nxi - 1] || !interp(xi, xv, ii, ip, ax)) continue;
+      auto F = [&](int a, int b) { return fi[(size_t)b * nxi + a]; };
+      f[(size_t)j * nx + i] =
+          (1.0 - ax) * ((1.0 - ay) * F(ii, jj) + ay * F(ii, jp)) + ax * ((1.0 - ay) * F(ip, jj) + ay * F(ip, jp));
+    }
+  }
+  return true;
+}
+
 struct Run {
   Namelist nl;
   FlowFiles ff;
+  // sources (module sources, src/hipft.f90:290-304)
+  Gaussian gauss;
+  int rfe1 = 0, rfe2 = 1;
+  double time_of_next_source_rfe = 0.0, time_of_prev_source_rfe = 0.0;
+  std::vector<double> uf_rvec;
   std::string dir;
   std::string map_dir;             // output_map_directory (relative to the run directory)
   std::vector<double> pscale, tscale;  // the map scales: p(1:npm1), t(1:ntm)
@@ -291,6 +397,88 @@ struct Run {
       std::fclose(fs);
     }
     return HIPFT_OK;
+  }
+
+  // generate_rfe (src/hipft.f90:8809-8921): the random map, then the frame
+  int generate_rfe(int slot) {
+    hipft_info inf;
+    hipft_gpu_info(h, &inf);
+    const int ntm = inf.ntm, npm = inf.npm;
+    const double normfac = c_pi / std::sqrt(c_twopi);
+    std::vector<double> rnd((size_t)ntm * npm, 0.0);
+    for (int k = 2; k <= npm - 1; ++k)
+      for (int j = 1; j <= ntm; ++j) rnd[(size_t)(k - 1) * ntm + (j - 1)] = normfac * gauss();
+    return hipft_gpu_set_rfe_frame(h, slot, nl.source_rfe_model, rnd.data(), uf_rvec.data());
+  }
+
+  // load_source (src/hipft.f90:7050-7213)
+  int load_source() {
+    hipft_info inf;
+    hipft_gpu_info(h, &inf);
+    const int ntm = inf.ntm, npm = inf.npm;
+    if (nl.source_from_file) {
+      int nd = 0;
+      int64_t dims[3];
+      std::string f = path(nl.source_filename);
+      int rc = hipft_h5_read(f.c_str(), &nd, dims, nullptr, nullptr, nullptr, nullptr);
+      if (rc || nd != 2) {
+        err = "cannot read the source file " + f + " as a 2D map";
+        return rc ? rc : HIPFT_EINVAL;
+      }
+      const int nfp = (int)dims[0], nft = (int)dims[1];
+      std::vector<double> sf((size_t)nfp * nft), pf(nfp), tf(nft);
+      rc = hipft_h5_read(f.c_str(), &nd, dims, sf.data(), pf.data(), tf.data(), nullptr);
+      if (rc) return rc;
+      std::vector<double> fi((size_t)nft * nfp);  // TRANSPOSE: (nft, nfp), theta fastest
+      for (int jp = 0; jp < nfp; ++jp)
+        for (int it = 0; it < nft; ++it) fi[(size_t)jp * nft + it] = sf[(size_t)it * nfp + jp];
+      std::vector<double> p(pscale);
+      p.push_back(pscale[1] + c_twopi);  // p(npm) = p(2) + 2 pi (src/hipft.f90:2131)
+      std::vector<double> out;
+      if (!interp2d(tf, pf, fi, tscale, p, out)) {
+        err = "the source file's scales are not monotonically increasing";
+        return HIPFT_EINVAL;
+      }
+      rc = hipft_gpu_set_source_file(h, out.data());
+      if (rc) return rc;
+    }
+    if (nl.source_rfe_model > 0) {
+      if (nl.source_rfe_seed != -9999) gauss.seed((uint64_t)nl.source_rfe_seed);
+      else gauss.seed((uint64_t)std::time(nullptr) ^ ((uint64_t)(uintptr_t)this << 16));
+      const double num_cells = (double)ntm * (npm - 2);
+      uf_rvec.assign(nr, 0.0);
+      for (int i = 0; i < nr; ++i)
+        uf_rvec[i] = (nl.source_rfe_model == 1)
+                         ? nl.source_rfe_total_unsigned_flux_per_hours[i] * c_input_flux_fac / (c_rsun_cm2 * num_cells)
+                         : nl.source_rfe_total_unsigned_flux_per_hours[i] * c_input_flux_fac /
+                               (c_rsun_cm2 * 4.0 * c_pi);
+      rfe1 = 0;
+      rfe2 = 1;
+      int rc = generate_rfe(rfe1);
+      if (rc) return rc;
+      rc = generate_rfe(rfe2);
+      if (rc) return rc;
+      time_of_next_source_rfe = time + nl.source_rfe_lifetime;
+      time_of_prev_source_rfe = time;
+    }
+    return HIPFT_OK;
+  }
+
+  // update_source (src/hipft.f90:3875-3947)
+  int update_source() {
+    const bool rfe = nl.source_rfe_model > 0;
+    double alpha = 0.0;
+    if (rfe) {
+      if (time >= time_of_next_source_rfe) {
+        time_of_prev_source_rfe = time_of_next_source_rfe;
+        time_of_next_source_rfe = time_of_prev_source_rfe + nl.source_rfe_lifetime;
+        std::swap(rfe1, rfe2);
+        int rc = generate_rfe(rfe2);
+        if (rc) return rc;
+      }
+      alpha = (time - time_of_prev_source_rfe) / nl.source_rfe_lifetime;
+    }
+    return hipft_gpu_update_source(h, nl.source_from_file, rfe, rfe1, rfe2, alpha);
   }
 
   // read_2d_file of one flow pair and hand it to the library
@@ -454,6 +642,11 @@ struct Run {
       dtime_global = ff.t_next - time;
       timestep_needs_updating = timestep_flow_needs_updating = time_step_changed = true;
     }
+    if (nl.advance_source && nl.source_rfe_model > 0 &&
+        time + dtime_global >= time_of_next_source_rfe) {  // src/hipft.f90:4431-4442
+      dtime_global = std::min(time_of_next_source_rfe - time, 0.5 * nl.source_rfe_lifetime);
+      timestep_needs_updating = timestep_flow_needs_updating = time_step_changed = true;
+    }
     if (time + dtime_global >= nl.time_end) {
       dtime_global = nl.time_end - time;
       timestep_needs_updating = false;
@@ -513,10 +706,6 @@ struct Run {
   int setup(int device) {
     nr = nl.n_realizations;
     hist.assign((size_t)nr * 14, 0.0);
-    if (nl.advance_source) {
-      err = "sources (advance_source) are not part of this library";
-      return HIPFT_EINVAL;
-    }
     if (!nl.diffusion_coef_filename.empty()) {
       err = "diffusion_coef_filename is not supported yet";
       return HIPFT_EINVAL;
@@ -634,6 +823,7 @@ struct Run {
     P.diffusion_coef_constants = nl.diffusion_coef_constants.data();
     P.pole_flux_lat_limit = nl.pole_flux_lat_limit;
     P.verbose = nl.verbose;
+    P.advance_source = nl.advance_source;
     int rc = hipft_gpu_create(&g, &P, &h);
     if (rc) {
       err = "hipft_gpu_create failed";
@@ -669,11 +859,15 @@ struct Run {
         if (rc) return rc;
       }
     }
+    time = nl.time_start;
+    if (nl.advance_source) {
+      rc = load_source();
+      if (rc) return rc;
+    }
     hipft_info inf;
     hipft_gpu_info(h, &inf);
     dt_euler = inf.dtime_diffusion_euler;
     subcycles = nl.diffusion_subcycles;
-    time = nl.time_start;
     idx_out = nl.output_map_idx_start - 1;
     if (nl.output_map_idx_cadence > 0 || nl.output_map_time_cadence > 0.0) {
       output_current_map = true;
@@ -755,6 +949,10 @@ struct Run {
         rc = hipft_gpu_update_flow(h, &upd);
         if (rc) return rc;
         if (upd) timestep_flow_needs_updating = timestep_needs_updating = true;
+      }
+      if (nl.advance_source) {
+        int rc = update_source();
+        if (rc) return rc;
       }
       int rc = update_timestep();
       if (rc) return rc;

@@ -111,6 +111,9 @@ struct hipft_gpu {
   double vwidth = 0.03, vt_const = 0.0, vp_omega = 0.0, vtime_start = 0.0;
   // assimilation
   double *d_da = nullptr, *d_daopt = nullptr;
+  // sources: file term (one plane), two RFE frames, the blended source
+  double *d_src_file = nullptr, *d_rfe[2] = {}, *d_src = nullptr, *d_rnd = nullptr, *d_rfe_aux = nullptr;
+  bool src_set = false;
   int *d_tidx = nullptr;
   std::string err;
   int64_t launches = 0, cell_updates = 0;
@@ -1345,13 +1348,105 @@ extern "C" int hipft_gpu_flux_transport_step(hipft_gpu *h, double dt, hipft_cycl
   if (!h) return HIPFT_EINVAL;
   if (h->P.strang_splitting) {
     double half = dt * 0.5;
+    if (h->P.advance_source) TRY(hipft_gpu_source_step(h, half));
     if (h->P.advance_flow) TRY(hipft_gpu_advection_step(h, half));
     if (h->P.advance_diffusion) TRY(hipft_gpu_diffusion_step(h, dt, cb, user, info));
     if (h->P.advance_flow) TRY(hipft_gpu_advection_step(h, half));
+    if (h->P.advance_source) TRY(hipft_gpu_source_step(h, half));
   } else {
     if (h->P.advance_flow) TRY(hipft_gpu_advection_step(h, dt));
     if (h->P.advance_diffusion) TRY(hipft_gpu_diffusion_step(h, dt, cb, user, info));
+    if (h->P.advance_source) TRY(hipft_gpu_source_step(h, dt));
   }
+  return HIPFT_OK;
+}
+
+// ----------------------------------------------------------------- sources
+static int ensure_sources(hipft_gpu *h) {
+  if (h->d_src) return HIPFT_OK;
+  TRY(dalloc(h, &h->d_src, h->fieldn));
+  CK(h, cudaMemsetAsync(h->d_src, 0, h->fieldn * sizeof(double), h->stream));
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_set_source_file(hipft_gpu *h, const double *data_tp) {
+  if (!h || !data_tp) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  TRY(ensure_sources(h));
+  if (!h->d_src_file) TRY(dalloc(h, &h->d_src_file, (size_t)h->ldt * h->npm));
+  CK(h, cudaMemcpy2DAsync(h->d_src_file, (size_t)h->ldt * sizeof(double), data_tp, (size_t)h->ntm * sizeof(double),
+                          (size_t)h->ntm * sizeof(double), (size_t)h->npm, cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+static int balance_buffer(hipft_gpu *h, double *a);
+
+extern "C" int hipft_gpu_set_rfe_frame(hipft_gpu *h, int slot, int model, const double *rnd_tp, const double *uf) {
+  if (!h || !rnd_tp || !uf || slot < 0 || slot > 1 || model < 1 || model > 2) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  TRY(ensure_sources(h));
+  const int ntm = h->ntm, npm = h->npm, nr = h->nr;
+  if (!h->d_rfe[slot]) {
+    TRY(dalloc(h, &h->d_rfe[slot], h->fieldn));
+    CK(h, cudaMemsetAsync(h->d_rfe[slot], 0, h->fieldn * sizeof(double), h->stream));
+  }
+  if (!h->d_rnd) {
+    TRY(dalloc(h, &h->d_rnd, (size_t)ntm * npm));
+    TRY(dalloc(h, &h->d_rfe_aux, (size_t)(nr + 1) + (ntm + 1)));
+  }
+  // da_ti per theta row, model 1 (src/hipft.f90:8840-8853)
+  std::vector<double> aux((size_t)(nr + 1) + (ntm + 1), 0.0);
+  for (int i = 1; i <= nr; ++i) aux[i] = uf[i - 1];
+  double *dati = aux.data() + (nr + 1);
+  for (int j = 1; j <= ntm; ++j) {
+    if (j == 1 || j == ntm) {
+      const double tav = (j == 1) ? 0.5 * (h->t[1] + h->t[2]) : 0.5 * (h->t[ntm] + h->t[ntm - 1]);
+      const double sn_t = std::sin(tav), d_t = (j == 1) ? h->dth[2] : h->dth[ntm];
+      dati[j] = 1.0 / (0.25 * sn_t * d_t);
+    } else {
+      dati[j] = h->st_i[j] * h->dt_i[j];
+    }
+  }
+  TRY(upload(h, h->d_rfe_aux, aux));
+  CK(h, cudaMemcpyAsync(h->d_rnd, rnd_tp, (size_t)ntm * npm * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  double *fr = h->d_rfe[slot];
+  dim3 blk(32, 8), grd((unsigned)((ntm + 31) / 32), (unsigned)((npm - 2 + 7) / 8), (unsigned)nr);
+  k_rfe_frame<<<grd, blk, 0, h->stream>>>(h->M, model, h->d_rnd, h->d_rfe_aux, h->d_rfe_aux + (nr + 1), fr);
+  LAUNCHED(h);
+  k_seam<<<dim3((unsigned)((ntm + 127) / 128), (unsigned)nr), 128, 0, h->stream>>>(h->M, ntm, h->ldt, fr);
+  LAUNCHED(h);
+  k_rfe_poles<<<nr, 128, 0, h->stream>>>(h->M, fr);
+  LAUNCHED(h);
+  TRY(balance_buffer(h, fr));
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_update_source(hipft_gpu *h, int use_file, int use_rfe, int slot1, int slot2,
+                                       double alpha) {
+  if (!h || slot1 < 0 || slot1 > 1 || slot2 < 0 || slot2 > 1) return HIPFT_EINVAL;
+  if ((use_file && !h->d_src_file) || (use_rfe && (!h->d_rfe[slot1] || !h->d_rfe[slot2])))
+    return fail(h, HIPFT_ESTATE, "update_source: source file or RFE frame not set");
+  CK(h, cudaSetDevice(h->dev));
+  TRY(ensure_sources(h));
+  dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)h->nr);
+  k_source_blend<<<grd, blk, 0, h->stream>>>(h->M, use_file ? h->d_src_file : nullptr,
+                                             use_rfe ? h->d_rfe[slot1] : nullptr, use_rfe ? h->d_rfe[slot2] : nullptr,
+                                             alpha, h->d_src);
+  LAUNCHED(h);
+  h->src_set = true;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_source_step(hipft_gpu *h, double dt) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "source_step before set_field");
+  if (!h->src_set) return fail(h, HIPFT_ESTATE, "source_step before update_source");
+  CK(h, cudaSetDevice(h->dev));
+  dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)h->nr);
+  k_source_step<<<grd, blk, 0, h->stream>>>(h->M, h->d_src, dt, h->buf[h->cur]);
+  LAUNCHED(h);
+  h->dring_valid = false;
   return HIPFT_OK;
 }
 
@@ -1556,22 +1651,28 @@ extern "C" int hipft_gpu_get_flux(hipft_gpu *h, double *flux_p, double *flux_m) 
   return HIPFT_OK;
 }
 
-extern "C" int hipft_gpu_balance_flux(hipft_gpu *h) {
-  if (!h) return HIPFT_EINVAL;
-  if (!h->field_set) return fail(h, HIPFT_ESTATE, "balance_flux before set_field");
-  CK(h, cudaSetDevice(h->dev));
+// balance_flux (src/hipft.f90:8752-8807) of every realization of `a`
+static int balance_buffer(hipft_gpu *h, double *a) {
   std::vector<double> fp, fm;
-  TRY(flux_of(h, h->buf[h->cur], fp, fm));
+  TRY(flux_of(h, a, fp, fm));
   std::vector<double> r(h->nr + 1, 1.0);
   for (int i = 0; i < h->nr; ++i) r[i + 1] = (fm[i] + fp[i] == 0.0) ? 1.0 : std::sqrt(std::fabs(fp[i] / fm[i]));
   size_t L = (size_t)h->nr * ((h->npm - 1 + 15) / 16) * 2;
   double *dr = h->d_part + L;
   TRY(upload(h, dr, r));
   dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm + 7) / 8), (unsigned)h->nr);
-  k_scale_balance<<<grd, blk, 0, h->stream>>>(h->M, h->buf[h->cur], dr);
+  k_scale_balance<<<grd, blk, 0, h->stream>>>(h->M, a, dr);
   LAUNCHED(h);
-  h->dring_valid = false;
   CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_balance_flux(hipft_gpu *h) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "balance_flux before set_field");
+  CK(h, cudaSetDevice(h->dev));
+  TRY(balance_buffer(h, h->buf[h->cur]));
+  h->dring_valid = false;
   return HIPFT_OK;
 }
 

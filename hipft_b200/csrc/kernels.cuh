@@ -20,6 +20,7 @@ namespace hipft {
 
 constexpr double kHalf = 0.5;
 constexpr double kOne = 1.0;
+constexpr double kTwoPiI = 0.15915494309189535;  // twopi_i, src/hipft.f90:111
 constexpr double kTwo = 2.0;
 constexpr double kFour = 4.0;
 
@@ -580,6 +581,67 @@ __global__ void k_seam(Mesh m, int n1, int ld, double *a) {
   int64_t b = (int64_t)(i - 1) * m.npm * ld + (j - 1);
   a[b] = a[b + (int64_t)(m.npm - 2) * ld];
   a[b + (int64_t)(m.npm - 1) * ld] = a[b + (int64_t)ld];
+}
+
+// ------------------------------------------------------------------ sources
+// generate_rfe (src/hipft.f90:8854-8873) on the interior columns of one
+// frame: rfe = rnd(j,k) * uf(i) * da_ti(j) * dp_i(k) (model 1) or
+// rnd(j,k) * uf(i) (model 2).  rnd is (ntm, npm), theta fastest.
+__global__ void k_rfe_frame(Mesh m, int model, const double *__restrict__ rnd, const double *__restrict__ uf,
+                            const double *__restrict__ dati, double *rfe) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm - 1) return;
+  const double r = rnd[(int64_t)(k - 1) * m.ntm + (j - 1)];
+  rfe[fidx(m, j, k, i)] = (model == 1) ? r * uf[i] * dati[j] * m.dp_i[k] : r * uf[i];
+}
+
+// The frame's pole rows: the mean over phi of rows 1 and ntm, summed in the
+// reference's sequential order (src/hipft.f90:8880-8894).  One block per
+// realization.
+__global__ void k_rfe_poles(Mesh m, double *rfe) {
+  const int i = blockIdx.x + 1;
+  __shared__ double s[2];
+  if (threadIdx.x == 0) {
+    double fn = 0.0, fs = 0.0;
+    for (int k = 1; k <= m.npm - 2; ++k) {
+      fn = fn + rfe[fidx(m, 1, k, i)] * m.dp[k];
+      fs = fs + rfe[fidx(m, m.ntm, k, i)] * m.dp[k];
+    }
+    s[0] = fn * kTwoPiI;
+    s[1] = fs * kTwoPiI;
+  }
+  __syncthreads();
+  for (int k = 1 + threadIdx.x; k <= m.npm; k += blockDim.x) {
+    rfe[fidx(m, 1, k, i)] = s[0];
+    rfe[fidx(m, m.ntm, k, i)] = s[1];
+  }
+}
+
+// update_source (src/hipft.f90:3898-3945): source = 0 [+ file]
+// [+ (1-alpha) frame1 + alpha frame2], in that order.
+__global__ void k_source_blend(Mesh m, const double *__restrict__ file, const double *__restrict__ r1,
+                               const double *__restrict__ r2, double alpha, double *src) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm) return;
+  const int64_t q = fidx(m, j, k, i);
+  double v = 0.0;
+  if (file) v = v + file[(int64_t)(k - 1) * m.ldt + (j - 1)];
+  if (r1) v = v + (kOne - alpha) * r1[q] + alpha * r2[q];
+  src[q] = v;
+}
+
+// source_step (src/hipft.f90:4719-4721): f = f + dt * source.
+__global__ void k_source_step(Mesh m, const double *__restrict__ src, double dt, double *f) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 1;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm) return;
+  const int64_t q = fidx(m, j, k, i);
+  f[q] = f[q] + dt * src[q];
 }
 
 // Local Lax-Friedrichs alpha from 2-D velocities (set_lf_alpha,

@@ -196,6 +196,7 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"assimilate_data_lat_limits", &nl.assimilate_data_lat_limits},
       {"assimilate_data_mu_powers", &nl.assimilate_data_mu_powers},
       {"assimilate_data_mu_limits", &nl.assimilate_data_mu_limits},
+      {"source_rfe_total_unsigned_flux_per_hours", &nl.source_rfe_total_unsigned_flux_per_hours},
   };
   // Sentinels of the reference's DATA statements (src/hipft.f90:593-706).
   for (auto &kv : rvec) {
@@ -207,9 +208,10 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"n_realizations", &nl.n_realizations}, {"validation_run", &nl.validation_run},
       {"flow_dr_model", &nl.flow_dr_model}, {"flow_mf_model", &nl.flow_mf_model},
       {"flow_num_method", &nl.flow_num_method}, {"diffusion_num_method", &nl.diffusion_num_method},
-      {"diffusion_subcycles", &nl.diffusion_subcycles}};
+      {"diffusion_subcycles", &nl.diffusion_subcycles}, {"source_rfe_model", &nl.source_rfe_model}};
   std::map<std::string, long *> longs = {{"output_map_idx_start", &nl.output_map_idx_start},
-                                         {"output_map_idx_cadence", &nl.output_map_idx_cadence}};
+                                         {"output_map_idx_cadence", &nl.output_map_idx_cadence},
+                                         {"source_rfe_seed", &nl.source_rfe_seed}};
   std::map<std::string, double *> dbls = {
       {"validation_run_width", &nl.validation_run_width},
       {"initial_map_mult_fac", &nl.initial_map_mult_fac},
@@ -231,7 +233,8 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"assimilate_data_lat_limit", &nl.assimilate_data_lat_limit},
       {"assimilate_data_mu_power", &nl.assimilate_data_mu_power},
       {"assimilate_data_mu_limit", &nl.assimilate_data_mu_limit},
-      {"source_rfe_total_unsigned_flux_per_hour", nullptr}, {"source_rfe_lifetime", nullptr}};
+      {"source_rfe_total_unsigned_flux_per_hour", &nl.source_rfe_total_unsigned_flux_per_hour},
+      {"source_rfe_lifetime", &nl.source_rfe_lifetime}};
   std::map<std::string, bool *> bools = {
       {"initial_map_flux_balance", &nl.initial_map_flux_balance},
       {"output_map_flux_balance", &nl.output_map_flux_balance}, {"output_map_2d", &nl.output_map_2d},
@@ -243,7 +246,7 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"assimilate_data_balance_flux", &nl.assimilate_data_balance_flux},
       {"assimilate_data_add", &nl.assimilate_data_add},
       {"assimilate_data_custom_from_mu", &nl.assimilate_data_custom_from_mu},
-      {"output_flows", nullptr}, {"source_from_file", nullptr}};
+      {"output_flows", nullptr}, {"source_from_file", &nl.source_from_file}};
   std::map<std::string, std::string *> strs = {
       {"initial_map_filename", &nl.initial_map_filename},
       {"output_map_root_filename", &nl.output_map_root_filename},
@@ -253,8 +256,8 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"assimilate_data_map_root_dir", &nl.assimilate_data_map_root_dir},
       {"output_flows_directory", nullptr}, {"output_flows_root_filename", nullptr},
       {"flow_list_filename", &nl.flow_list_filename}, {"flow_root_dir", &nl.flow_root_dir},
-      {"source_filename", nullptr}};
-  std::map<std::string, int> ignored_ints = {{"source_rfe_model", 0}, {"source_rfe_seed", 0}};
+      {"source_filename", &nl.source_filename}};
+  std::map<std::string, int> ignored_ints = {};
 
   for (const auto &a : assigns) {
     std::vector<std::string> vals = split_values(a.value);
@@ -275,7 +278,6 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       }
       continue;
     }
-    if (a.name == "source_rfe_total_unsigned_flux_per_hours") continue;
     const std::string &v = vals[0];
     bool ok = true;
     if (ints.count(a.name)) {
@@ -346,6 +348,7 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
   fill(nl.flow_mf_coef_p5_values, nl.flow_mf_coef_p5_value, big);
   fill(nl.flow_attenuate_values, nl.flow_attenuate_value, neg);
   fill(nl.diffusion_coef_constants, nl.diffusion_coef_constant, neg);
+  fill(nl.source_rfe_total_unsigned_flux_per_hours, nl.source_rfe_total_unsigned_flux_per_hour, neg);
   return true;
 }
 

@@ -54,6 +54,12 @@ struct Namelist {
   int diffusion_num_method = 3;
   int diffusion_subcycles = 0;
   bool advance_source = false;
+  int source_rfe_model = 0;
+  long source_rfe_seed = -9999;
+  double source_rfe_total_unsigned_flux_per_hour = 0.0, source_rfe_lifetime = 0.3;
+  bool source_from_file = false;
+  std::string source_filename;
+  std::vector<double> source_rfe_total_unsigned_flux_per_hours;
   bool assimilate_data = false, assimilate_data_balance_flux = false;
   double assimilate_data_mult_fac = 1.0;
   std::string assimilate_data_map_list_filename, assimilate_data_map_root_dir = ".";

@@ -40,7 +40,8 @@ class Params(ctypes.Structure):
                 ("advance_diffusion", ctypes.c_int), ("diffusion_num_method", ctypes.c_int),
                 ("diffusion_subcycles", ctypes.c_int), ("diffusion_coef_grid", ctypes.c_int),
                 ("diffusion_coef_factor", ctypes.c_double), ("diffusion_coef_constants", DPTR),
-                ("pole_flux_lat_limit", ctypes.c_double), ("verbose", ctypes.c_int)]
+                ("pole_flux_lat_limit", ctypes.c_double), ("verbose", ctypes.c_int),
+                ("advance_source", ctypes.c_int)]
 
 
 class FlowDef(ctypes.Structure):
@@ -108,6 +109,12 @@ SIGNATURES = [
                                               ctypes.c_size_t]),
     ("hipft_h5_read", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
                                      DPTR, DPTR, DPTR, DPTR]),
+    ("hipft_gpu_set_flow_from_files", ctypes.c_int, [_H, DPTR, DPTR, ctypes.c_int]),
+    ("hipft_gpu_set_source_file", ctypes.c_int, [_H, DPTR]),
+    ("hipft_gpu_set_rfe_frame", ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, DPTR, DPTR]),
+    ("hipft_gpu_update_source", ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_double]),
+    ("hipft_gpu_source_step", ctypes.c_int, [_H, ctypes.c_double]),
     ("hipft_h5_write", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), DPTR, DPTR,
                                       DPTR, DPTR, ctypes.c_int]),
 ]

@@ -69,6 +69,7 @@ typedef struct {
   const double *diffusion_coef_constants; /* [nr], km^2/s; also validation 1   */
   double pole_flux_lat_limit; /* degrees, for the polar-flux diagnostics       */
   int verbose;
+  int advance_source;         /* source steps in flux_transport_step           */
 } hipft_params;
 
 /* Analytic / prescribed flow definition (update_flow, src/hipft.f90:3371-3523;
@@ -158,6 +159,26 @@ int hipft_gpu_set_flow_from_files(hipft_gpu *h, const double *vt_pt, const doubl
 /* get_flow_dtmax (src/hipft.f90:7287-7350): CFL limit over all cells and
  * realizations, x2 for Strang splitting, x2 for SSPRK(4,3). */
 int hipft_gpu_flow_dtmax(hipft_gpu *h, double *dtmax);
+
+/* ---- sources (advance_source) ---------------------------------------------- */
+
+/* The source from a file, already on the main mesh (load_source interpolates
+ * the file with interp2d, src/hipft.f90:7094-7146): data (ntm, npm), theta
+ * fastest, the same for every realization. */
+int hipft_gpu_set_source_file(hipft_gpu *h, const double *data_tp);
+/* generate_rfe (src/hipft.f90:8809-8921) into frame slot 0 or 1, then
+ * balance_flux of each realization (src/hipft.f90:3931-3934, 7199-7202).
+ * model 1: flux per cell, 2: flux per unit area.  rnd_tp (ntm, npm), theta
+ * fastest: the reference's rnd_nums, normal deviates times pi/sqrt(2 pi),
+ * read on columns 2..npm-1 only.  uf [nr]: unsigned flux per hour per cell
+ * (model 1) or per unit area (model 2) in code units. */
+int hipft_gpu_set_rfe_frame(hipft_gpu *h, int slot, int model, const double *rnd_tp, const double *uf);
+/* update_source (src/hipft.f90:3875-3947): source = [file] +
+ * [(1-alpha) frame(slot1) + alpha frame(slot2)]. */
+int hipft_gpu_update_source(hipft_gpu *h, int use_file, int use_rfe, int slot1, int slot2, double alpha);
+/* source_step (src/hipft.f90:4697-4732): f += dt * source.
+ * flux_transport_step calls it when advance_source is set. */
+int hipft_gpu_source_step(hipft_gpu *h, double dt);
 
 /* ---- the time step -------------------------------------------------------- */
 

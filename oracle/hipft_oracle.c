@@ -89,6 +89,15 @@ typedef struct {
    * files' contents in PT order, vt (npm1, nt) and vp (np, ntm) per entry, m/s */
   int use_flow_from_files, n_flows;
   const double *flow_jd, *flow_vt, *flow_vp;
+  /* sources (advance_source): random flux emergence with a seeded generator
+   * (seed -9999: seed 0), per-realization unsigned flux per hour; the source
+   * file's data (nfp, nft) PT and its scales */
+  int advance_source, source_rfe_model;
+  long source_rfe_seed;
+  double source_rfe_lifetime;
+  const double *source_rfe_flux;
+  int source_from_file, source_nfp, source_nft;
+  const double *source_data, *source_pf, *source_tf;
 } orc_params;
 
 /* History rows, one block of nr rows per output event.
@@ -125,6 +134,13 @@ typedef struct {
   double *D_C_CPt, *D_C_MCt, *D_M_Tt, *D_CP_Tt, *D_P_Tt, *D_MC_Tt, *weno_eps_t;
   double *D_C_CPp, *D_C_MCp, *D_M_Tp, *D_CP_Tp, *D_P_Tp, *D_MC_Tp, *weno_eps_p;
   double *atten_i;
+  /* sources (module sources F:290-304) and the generator of get_gaussian */
+  double *source, *source_file, *source_rfe[2], *uf;
+  int rfe1, rfe2;
+  double time_of_next_source_rfe, time_of_prev_source_rfe;
+  uint64_t rng[4];
+  int g_second;
+  double g_v, g_sln;
   /* flows from files: current pair (flow_from_files_current_vt/vp) and times */
   double *fvt, *fvp, *flow_times;
   int flow_idx;
@@ -1216,18 +1232,200 @@ static void diffusion_step(orc *S, double dtl) {
 
 /* --------------------------------------------------- flux_transport_step
  * F:4463-4507 (sources are out of scope) */
+static void source_step(orc *S, double dtl);
+
 static void flux_transport_step(orc *S) {
   const orc_params *P = S->P;
   double dtl = S->dtime_global;
   if (P->strang_splitting) {
     double h = dtl * half;
+    if (P->advance_source) source_step(S, h);
     if (P->advance_flow) advection_step(S, h);
     if (P->advance_diffusion) diffusion_step(S, dtl);
     if (P->advance_flow) advection_step(S, h);
+    if (P->advance_source) source_step(S, h);
   } else {
     if (P->advance_flow) advection_step(S, dtl);
     if (P->advance_diffusion) diffusion_step(S, dtl);
+    if (P->advance_source) source_step(S, dtl);
   }
+}
+
+/* ----------------------------------------------------------------- sources
+ * get_gaussian F:8616-8670 (Marsaglia-Bray polar method, second deviate kept
+ * for the next call) over xoshiro256** uniforms seeded through splitmix64:
+ * the same generator as the library's driver (the reference uses gfortran's
+ * RANDOM_NUMBER, whose stream is not restated here). */
+static void rng_seed(orc *S, uint64_t x) {
+  for (int q = 0; q < 4; q++) {
+    x += 0x9e3779b97f4a7c15ULL;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    S->rng[q] = z ^ (z >> 31);
+  }
+  S->g_second = 0;
+}
+static uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+static double rng_uniform(orc *S) {
+  uint64_t *s = S->rng;
+  const uint64_t r = rotl64(s[1] * 5, 7) * 9, t = s[1] << 17;
+  s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3]; s[2] ^= t; s[3] = rotl64(s[3], 45);
+  return (double)(r >> 11) * 0x1.0p-53;
+}
+static double get_gaussian(orc *S) {
+  if (S->g_second) { S->g_second = 0; return S->g_v * S->g_sln; }
+  S->g_second = 1;
+  double u, q;
+  for (;;) {
+    u = 2.0 * rng_uniform(S) - one;
+    S->g_v = 2.0 * rng_uniform(S) - one;
+    q = u * u + S->g_v * S->g_v;
+    if (q < one && q > 0.) break;
+  }
+  S->g_sln = sqrt(-(2.0 * log(q)) / q);
+  return u * S->g_sln;
+}
+
+/* generate_rfe F:8809-8921 followed by balance_flux of each realization */
+static void generate_rfe(orc *S, double *rfe) {
+  const orc_params *P = S->P;
+  int ntm = S->ntm, npm = S->npm, nr = S->nr;
+  double *rnd = dalloc((size_t)ntm * npm);
+  const double normfac = pi / sqrt(twopi);
+  for (int k = 2; k <= npm - 1; k++)
+    for (int j = 1; j <= ntm; j++) rnd[(size_t)(k - 1) * ntm + (j - 1)] = normfac * get_gaussian(S);
+  for (int k = 2; k <= npm - 1; k++)
+    for (int j = 1; j <= ntm; j++) {
+      double da_ti = 0.;
+      if (P->source_rfe_model == 1) {
+        if (j == 1) {
+          double tav = half * (V1(S->t, 1) + V1(S->t, 2));
+          da_ti = one / (quarter * sin(tav) * V1(S->dth, 2));
+        } else if (j == ntm) {
+          double tav = half * (V1(S->t, ntm) + V1(S->t, ntm - 1));
+          da_ti = one / (quarter * sin(tav) * V1(S->dth, ntm));
+        } else {
+          da_ti = V1(S->st_i, j) * V1(S->dt_i, j);
+        }
+      }
+      for (int i = 1; i <= nr; i++) {
+        double r = rnd[(size_t)(k - 1) * ntm + (j - 1)];
+        A3(rfe, j, k, i, ntm, npm) = (P->source_rfe_model == 1) ? r * S->uf[i - 1] * da_ti * V1(S->dp_i, k)
+                                                                : r * S->uf[i - 1];
+      }
+    }
+  for (int i = 1; i <= nr; i++)
+    for (int j = 1; j <= ntm; j++) {
+      A3(rfe, j, 1, i, ntm, npm) = A3(rfe, j, npm - 1, i, ntm, npm);
+      A3(rfe, j, npm, i, ntm, npm) = A3(rfe, j, 2, i, ntm, npm);
+    }
+  for (int i = 1; i <= nr; i++) {
+    double fn1 = zero, fs1 = zero;
+    for (int k = 1; k <= npm - 2; k++) {
+      fn1 = fn1 + A3(rfe, 1, k, i, ntm, npm) * V1(S->dp, k);
+      fs1 = fs1 + A3(rfe, ntm, k, i, ntm, npm) * V1(S->dp, k);
+    }
+    fn1 = fn1 * twopi_i;
+    fs1 = fs1 * twopi_i;
+    for (int k = 1; k <= npm; k++) {
+      A3(rfe, 1, k, i, ntm, npm) = fn1;
+      A3(rfe, ntm, k, i, ntm, npm) = fs1;
+    }
+  }
+  for (int i = 1; i <= nr; i++) balance_flux(S, rfe + (size_t)(i - 1) * ntm * npm);
+  free(rnd);
+}
+
+/* interp2d F:7992-8073 (flint's check F:8135-8150, interp F:8178-8210) */
+static int interp_1(const double *x, int n, double xv, int *i0, int *i1, double *a) {
+  if (n == 1 && xv == x[0]) { *i0 = *i1 = 0; *a = 0.; return 1; }
+  for (int i = 0; i < n - 1; i++)
+    if (xv >= x[i] && xv <= x[i + 1]) {
+      *i0 = i; *i1 = i + 1;
+      *a = (x[i] == x[i + 1]) ? 0. : (xv - x[i]) / (x[i + 1] - x[i]);
+      return 1;
+    }
+  return 0;
+}
+static int interp2d(int nxi, int nyi, const double *xi, const double *yi, const double *fi, int nx, int ny,
+                    const double *x, const double *y, double *f) {
+  for (int i = 0; i + 1 < nxi; i++) if (xi[i + 1] <= xi[i]) return 1;
+  for (int i = 0; i + 1 < nyi; i++) if (yi[i + 1] <= yi[i]) return 1;
+  for (int j = 0; j < ny; j++) {
+    int jj, jp; double ay;
+    for (int i = 0; i < nx; i++) f[(size_t)j * nx + i] = 0.;
+    if (y[j] < yi[0] || y[j] > yi[nyi - 1] || !interp_1(yi, nyi, y[j], &jj, &jp, &ay)) continue;
+    for (int i = 0; i < nx; i++) {
+      int ii, ip; double ax;
+      if (x[i] < xi[0] || x[i] > xi[nxi - 1] || !interp_1(xi, nxi, x[i], &ii, &ip, &ax)) continue;
+#define FI(a, b) fi[(size_t)(b) * nxi + (a)]
+      f[(size_t)j * nx + i] = (one - ax) * ((one - ay) * FI(ii, jj) + ay * FI(ii, jp)) +
+                              ax * ((one - ay) * FI(ip, jj) + ay * FI(ip, jp));
+#undef FI
+    }
+  }
+  return 0;
+}
+
+/* load_source F:7050-7213 */
+static int load_source(orc *S) {
+  const orc_params *P = S->P;
+  int ntm = S->ntm, npm = S->npm, nr = S->nr;
+  size_t n = (size_t)ntm * npm * nr;
+  S->source = dalloc(n);
+  if (P->source_from_file) {
+    int nfp = P->source_nfp, nft = P->source_nft;
+    double *fi = dalloc((size_t)nft * nfp), *ft = dalloc((size_t)ntm * npm);
+    for (int jp = 0; jp < nfp; jp++)
+      for (int it = 0; it < nft; it++) fi[(size_t)jp * nft + it] = P->source_data[(size_t)it * nfp + jp];
+    if (interp2d(nft, nfp, P->source_tf, P->source_pf, fi, ntm, npm, &V1(S->t, 1), &V1(S->p, 1), ft)) return 4;
+    S->source_file = dalloc(n);
+    for (int i = 1; i <= nr; i++) memcpy(S->source_file + (size_t)(i - 1) * ntm * npm, ft, sizeof(double) * ntm * npm);
+    free(fi); free(ft);
+  }
+  if (P->source_rfe_model > 0) {
+    rng_seed(S, (uint64_t)(P->source_rfe_seed == -9999 ? 0 : P->source_rfe_seed));
+    S->uf = dalloc(nr);
+    double num_cells = (double)ntm * (npm - 2);
+    for (int i = 0; i < nr; i++)
+      S->uf[i] = (P->source_rfe_model == 1) ? P->source_rfe_flux[i] * 1.0e21 / (rsun_cm2 * num_cells)
+                                            : P->source_rfe_flux[i] * 1.0e21 / (rsun_cm2 * four * pi);
+    S->source_rfe[0] = dalloc(n);
+    S->source_rfe[1] = dalloc(n);
+    S->rfe1 = 0; S->rfe2 = 1;
+    generate_rfe(S, S->source_rfe[S->rfe1]);
+    generate_rfe(S, S->source_rfe[S->rfe2]);
+    S->time_of_next_source_rfe = S->time + P->source_rfe_lifetime;
+    S->time_of_prev_source_rfe = S->time;
+  }
+  return 0;
+}
+
+/* update_source F:3875-3947 */
+static void update_source(orc *S) {
+  const orc_params *P = S->P;
+  size_t n = (size_t)S->ntm * S->npm * S->nr;
+  for (size_t q = 0; q < n; q++) S->source[q] = 0.;
+  if (P->source_from_file)
+    for (size_t q = 0; q < n; q++) S->source[q] = S->source[q] + S->source_file[q];
+  if (P->source_rfe_model > 0) {
+    if (S->time >= S->time_of_next_source_rfe) {
+      S->time_of_prev_source_rfe = S->time_of_next_source_rfe;
+      S->time_of_next_source_rfe = S->time_of_prev_source_rfe + P->source_rfe_lifetime;
+      int t = S->rfe1; S->rfe1 = S->rfe2; S->rfe2 = t;
+      generate_rfe(S, S->source_rfe[S->rfe2]);
+    }
+    double alpha = (S->time - S->time_of_prev_source_rfe) / P->source_rfe_lifetime;
+    const double *r1 = S->source_rfe[S->rfe1], *r2 = S->source_rfe[S->rfe2];
+    for (size_t q = 0; q < n; q++) S->source[q] = S->source[q] + (one - alpha) * r1[q] + alpha * r2[q];
+  }
+}
+
+/* source_step F:4697-4732 */
+static void source_step(orc *S, double dtl) {
+  size_t n = (size_t)S->ntm * S->npm * S->nr;
+  for (size_t q = 0; q < n; q++) S->f[q] = S->f[q] + dtl * S->source[q];
 }
 
 /* ------------------------------------------------------ update_timestep
@@ -1270,6 +1468,14 @@ static void update_timestep(orc *S) {
       S->dtime_global = S->time_of_next_input_flow - S->time;
       S->timestep_needs_updating = 1;
       S->flow_needs_updating = 1;
+      S->timestep_flow_needs_updating = 1;
+      S->time_step_changed = 1;
+    }
+  }
+  if (P->advance_source && P->source_rfe_model > 0) { /* F:4431-4442 */
+    if (S->time + S->dtime_global >= S->time_of_next_source_rfe) {
+      S->dtime_global = fmin(S->time_of_next_source_rfe - S->time, half * P->source_rfe_lifetime);
+      S->timestep_needs_updating = 1;
       S->timestep_flow_needs_updating = 1;
       S->time_step_changed = 1;
     }
@@ -1536,6 +1742,10 @@ int orc_run(const orc_params *P, int n1, int n2, const double *s1in, const doubl
     }
   }
   if (P->advance_diffusion) load_diffusion(S);
+  if (P->advance_source) {
+    int rc = load_source(S);
+    if (rc) return rc;
+  }
   if (P->assimilate_data && n_da > 0) {
     S->n_da = n_da; S->da_times = da_times; S->da_maps = da_maps;
     load_data_assimilation(S);
@@ -1547,6 +1757,7 @@ int orc_run(const orc_params *P, int n1, int n2, const double *s1in, const doubl
   for (;;) {
     S->ntime++;
     if (P->advance_flow) update_flow(S);
+    if (P->advance_source) update_source(S);
     update_timestep(S);
     flux_transport_step(S);
     S->time = S->time + S->dtime_global;

@@ -47,7 +47,8 @@ DEFAULTS = dict(
     diffusion_coef_filename="", diffusion_coef_grid=False,
     diffusion_coef_factor=7.43162901307967e-09,
     diffusion_num_method=3, diffusion_subcycles=0,
-    advance_source=False,
+    advance_source=False, source_rfe_model=0, source_rfe_seed=-9999, source_rfe_lifetime=0.3,
+    source_rfe_total_unsigned_flux_per_hour=0.0, source_from_file=False, source_filename="",
     assimilate_data=False, assimilate_data_balance_flux=False,
     assimilate_data_mult_fac=1.0, assimilate_data_map_list_filename="",
     assimilate_data_map_root_dir=".", assimilate_data_add=False,
@@ -69,6 +70,7 @@ RVECS = {
     "assimilate_data_lat_limits": ("assimilate_data_lat_limit", lambda v: v < 0.0),
     "assimilate_data_mu_powers": ("assimilate_data_mu_power", lambda v: v < 0.0),
     "assimilate_data_mu_limits": ("assimilate_data_mu_limit", lambda v: v < 0.0),
+    "source_rfe_total_unsigned_flux_per_hours": ("source_rfe_total_unsigned_flux_per_hour", lambda v: v < 0.0),
 }
 RVEC_SENTINEL = {k: (-1000000.0 if "coef_p" in k else -1.0) for k in RVECS}
 
@@ -169,8 +171,16 @@ class OrcParams(ctypes.Structure):
         ("output_map_flux_balance", ctypes.c_int),
         ("use_flow_from_files", ctypes.c_int), ("n_flows", ctypes.c_int),
         ("flow_jd", ctypes.POINTER(ctypes.c_double)), ("flow_vt", ctypes.POINTER(ctypes.c_double)),
-        ("flow_vp", ctypes.POINTER(ctypes.c_double))]
-FLOW_FILE_FIELDS = ("n_flows", "flow_jd", "flow_vt", "flow_vp")  # set by run(flows=...)
+        ("flow_vp", ctypes.POINTER(ctypes.c_double)),
+        ("advance_source", ctypes.c_int), ("source_rfe_model", ctypes.c_int), ("source_rfe_seed", ctypes.c_long),
+        ("source_rfe_lifetime", ctypes.c_double),
+        ("source_rfe_total_unsigned_flux_per_hours", ctypes.POINTER(ctypes.c_double)),
+        ("source_from_file", ctypes.c_int), ("source_nfp", ctypes.c_int), ("source_nft", ctypes.c_int),
+        ("source_data", ctypes.POINTER(ctypes.c_double)), ("source_pf", ctypes.POINTER(ctypes.c_double)),
+        ("source_tf", ctypes.POINTER(ctypes.c_double))]
+# set by run(flows=..., source=...)
+FLOW_FILE_FIELDS = ("n_flows", "flow_jd", "flow_vt", "flow_vp", "source_nfp", "source_nft", "source_data",
+                    "source_pf", "source_tf")
 
 
 class OrcHist(ctypes.Structure):
@@ -232,7 +242,8 @@ def _params_struct(p: dict):
 
 
 def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
-        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True, map_cap: int = 0, flows=None):
+        max_steps: int = 0, hist_cap: int = 0, want_field: bool = True, map_cap: int = 0, flows=None,
+        source=None):
     """Run the oracle on processed parameters ``p``.
 
     map_pt: (nr, ntm, npm1) C-order array (i.e. Fortran (npm1,ntm,nr)), or None.
@@ -242,6 +253,7 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
     fields write_map writes, flux-balanced when output_map_flux_balance.
     flows (use_flow_from_files): dict(jd=(n,), vt=(n, nt, npm1), vp=(n, ntm, np)),
     the flow list's Julian days and the files' data in C order, m/s.
+    source (source_from_file): dict(data=(nft, nfp) C order, pf=(nfp,), tf=(nft,)).
     """
     L = lib()
     nr = int(p["n_realizations"])
@@ -251,6 +263,11 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
         keep.extend(fa)
         c.n_flows = len(fa[0])
         c.flow_jd, c.flow_vt, c.flow_vp = (a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in fa)
+    if source is not None:
+        sa = [np.ascontiguousarray(source[k], dtype=np.float64) for k in ("data", "pf", "tf")]
+        keep.extend(sa)
+        c.source_nft, c.source_nfp = sa[0].shape
+        c.source_data, c.source_pf, c.source_tf = (a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in sa)
     if map_pt is not None:
         map_pt = np.ascontiguousarray(map_pt, dtype=np.float64)
         n2, n1 = map_pt.shape[-2], map_pt.shape[-1]
