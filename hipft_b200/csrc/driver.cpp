@@ -329,6 +329,10 @@ bool interp2d(const std::vector<double> &xi, const std::vector<double> &yi, cons
 struct Run {
   Namelist nl;
   FlowFiles ff;
+  // realizations of this rank (set_local_number_of_realizations): global
+  // realization roff+i is local i; shard == NULL on a single process
+  const hipft_shard *shard = nullptr;
+  int rank = 0, nranks = 1, roff = 0;
   // sources (module sources, src/hipft.f90:290-304)
   Gaussian gauss;
   int rfe1 = 0, rfe2 = 1;
@@ -360,8 +364,17 @@ struct Run {
   }
   std::string rname(const char *kind, int i) const {
     char b[64];
-    std::snprintf(b, sizeof b, "hipft_history_%s_r%06d.out", kind, i);
+    std::snprintf(b, sizeof b, "hipft_history_%s_r%06d.out", kind, roff + i);
     return path(b);
+  }
+
+  int red(int op, double *v) {
+    if (!shard) return HIPFT_OK;
+    if (shard->allreduce(shard->user, op, v) != 0) {
+      err = "all-reduce callback failed";
+      return HIPFT_ECOMM;
+    }
+    return HIPFT_OK;
   }
 
   bool history_due() const {
@@ -444,7 +457,13 @@ struct Run {
     }
     if (nl.source_rfe_model > 0) {
       if (nl.source_rfe_seed != -9999) gauss.seed((uint64_t)nl.source_rfe_seed);
-      else gauss.seed((uint64_t)std::time(nullptr) ^ ((uint64_t)(uintptr_t)this << 16));
+      else {  // RANDOM_SEED(); every rank takes rank 0's draws (the reference broadcasts them)
+        double sd = (rank == 0) ? (double)((std::time(nullptr) ^ ((uint64_t)(uintptr_t)this >> 4)) & 0xffffffffULL)
+                                : -1.0;
+        int rc = red(HIPFT_RED_MAX, &sd);
+        if (rc) return rc;
+        gauss.seed((uint64_t)sd);
+      }
       const double num_cells = (double)ntm * (npm - 2);
       uf_rvec.assign(nr, 0.0);
       for (int i = 0; i < nr; ++i)
@@ -545,8 +564,23 @@ struct Run {
 
   // write_2d_file / write_3d_file (src/hipft.f90:6353-6493): PT data
   // (n1, n2[, n3]) with scales s1, s2 and realization numbers 1..n3.
+  // (n1, n2[, n3]) with scales s1, s2 and realization numbers 1..n3.  With
+  // `gathered`, f holds this rank's n3 realizations and rank 0 writes all
+  // ranks' (MPI_Gatherv in the reference); otherwise rank 0 writes its own.
   int write_pt(const std::string &fname, int n1, int n2, int n3, const double *f, const double *s1,
-               const double *s2, bool two_d) {
+               const double *s2, bool two_d, bool gathered = true) {
+    std::vector<double> all;
+    if (shard && gathered) {
+      const size_t plane = (size_t)n1 * n2;
+      if (rank == 0) all.resize(plane * nl.n_realizations);
+      if (shard->gather(shard->user, f, (int64_t)(plane * n3), rank == 0 ? all.data() : nullptr) != 0) {
+        err = "gather callback failed";
+        return HIPFT_ECOMM;
+      }
+      f = all.data();
+      n3 = nl.n_realizations;
+    }
+    if (rank != 0) return HIPFT_OK;
     std::vector<double> s3(n3);
     for (int i = 0; i < n3; ++i) s3[i] = (double)(i + 1);
     int64_t dims[3] = {n1, n2, two_d ? 1 : n3};
@@ -600,6 +634,7 @@ struct Run {
       int rc = write_map(map_dir + "/" + base);
       if (rc) return rc;
       output_current_map = false;
+      if (rank != 0) return HIPFT_OK;
       FILE *fl = std::fopen(path("hipft_output_map_list.out").c_str(), "a");
       if (!fl) return HIPFT_EIO;
       std::string ln = fmt_i(idx_out, 10) + "   " + fmt_pe25(time) + "    " + base + "\n";
@@ -705,6 +740,21 @@ struct Run {
 
   int setup(int device) {
     nr = nl.n_realizations;
+    if (shard) {  // set_local_number_of_realizations (src/hipft.f90:1025-1037)
+      const int avg = nl.n_realizations / nranks, rem = nl.n_realizations - avg * nranks;
+      nr = avg + (rank < rem ? 1 : 0);
+      roff = rank * avg + std::min(rank, rem);
+      if (nr < 1) {
+        err = "more ranks than realizations";
+        return HIPFT_EINVAL;
+      }
+      for (auto *v : {&nl.diffusion_coef_constants, &nl.flow_attenuate_values, &nl.flow_dr_coef_p0_values,
+                      &nl.flow_dr_coef_p2_values, &nl.flow_dr_coef_p4_values, &nl.flow_mf_coef_p1_values,
+                      &nl.flow_mf_coef_p3_values, &nl.flow_mf_coef_p5_values, &nl.assimilate_data_lat_limits,
+                      &nl.assimilate_data_mu_powers, &nl.assimilate_data_mu_limits,
+                      &nl.source_rfe_total_unsigned_flux_per_hours})
+        *v = std::vector<double>(v->begin() + roff, v->begin() + roff + nr);
+    }
     hist.assign((size_t)nr * 14, 0.0);
     if (!nl.diffusion_coef_filename.empty()) {
       err = "diffusion_coef_filename is not supported yet";
@@ -741,11 +791,11 @@ struct Run {
       if (nd == 2) {
         for (int i = 0; i < nr; ++i) std::copy(all.begin(), all.begin() + plane, f_local.begin() + plane * i);
       } else {
-        if (dims[2] != nr) {
+        if (dims[2] != nl.n_realizations) {
           err = "number of realizations in the input map differs from n_realizations";
           return HIPFT_EINVAL;
         }
-        f_local = all;
+        std::copy(all.begin() + plane * roff, all.begin() + plane * (roff + nr), f_local.begin());
       }
     }
     double vt_const = nl.flow_vt_const, vp_omega = nl.flow_vp_rigid_omega;
@@ -797,7 +847,7 @@ struct Run {
         }
       // final analytic map of the first realization (src/hipft.f90:2062-2097)
       int rc = write_pt(nl.output_map_root_filename + "_final_analytic.h5", n1, n2, 1, fa.data(), s1.data(),
-                        s2.data(), true);
+                        s2.data(), true, false);
       if (rc) return rc;
     }
     pscale = s1;
@@ -828,6 +878,10 @@ struct Run {
     if (rc) {
       err = "hipft_gpu_create failed";
       return rc;
+    }
+    if (shard) {
+      rc = hipft_gpu_set_allreduce(h, shard->allreduce, shard->user);
+      if (rc) return rc;
     }
     rc = hipft_gpu_load_initial_map(h, f_local.data(), nl.initial_map_flux_balance, nl.initial_map_mult_fac);
     if (rc) return rc;
@@ -873,18 +927,26 @@ struct Run {
       output_current_map = true;
       // output directory and map list (src/hipft.f90:1194-1210, 1654-1664)
       map_dir = nl.output_map_directory;
-      if (!make_dirs(path(map_dir))) {
-        std::printf(" ### Could not make map output subdirectory, using ./\n");
-        map_dir = ".";
+      if (rank == 0) {
+        if (!make_dirs(path(map_dir))) {
+          std::printf(" ### Could not make map output subdirectory, using ./\n");
+          map_dir = ".";
+        }
+        FILE *fl = std::fopen(path("hipft_output_map_list.out").c_str(), "w");
+        if (!fl) {
+          err = "cannot create hipft_output_map_list.out in " + dir;
+          return HIPFT_EIO;
+        }
+        std::string hdr = rjust("IDX", 10) + " " + rjust("TIME", 25) + " FILENAME\n";
+        std::fputs(hdr.c_str(), fl);
+        std::fclose(fl);
       }
-      FILE *fl = std::fopen(path("hipft_output_map_list.out").c_str(), "w");
-      if (!fl) {
-        err = "cannot create hipft_output_map_list.out in " + dir;
-        return HIPFT_EIO;
+      if (shard) {  // the directory rank 0 settled on (an index into two choices)
+        double fallback = (map_dir == ".") ? 1.0 : 0.0;
+        int rc = red(HIPFT_RED_MAX, &fallback);
+        if (rc) return rc;
+        if (fallback > 0.0) map_dir = ".";
       }
-      std::string hdr = rjust("IDX", 10) + " " + rjust("TIME", 25) + " FILENAME\n";
-      std::fputs(hdr.c_str(), fl);
-      std::fclose(fl);
     }
     if (nl.assimilate_data) {
       if (!read_da_list(path(nl.assimilate_data_map_list_filename), da, err)) return HIPFT_EIO;
@@ -979,8 +1041,11 @@ struct Run {
       }
       if (time >= nl.time_end) break;
       FILE *stop = std::fopen(path("STOPRUN").c_str(), "r");
-      if (stop) {
-        std::fclose(stop);
+      double stopped = stop ? 1.0 : 0.0;
+      if (stop) std::fclose(stop);
+      rc = red(HIPFT_RED_MAX, &stopped);  // every rank stops at the same step
+      if (rc) return rc;
+      if (stopped > 0.0) {
         std::printf(" ### NOTE: The run was stopped prematurely via STOPRUN!\n");
         break;
       }
@@ -992,11 +1057,19 @@ struct Run {
 }  // namespace
 }  // namespace hipft
 
-extern "C" int hipft_run_field(const char *namelist_path, const char *run_dir, int device, double *f_out,
-                               size_t f_len) {
+extern "C" int hipft_run_shard(const char *namelist_path, const char *run_dir, int device,
+                               const hipft_shard *shard, double *f_out, size_t f_len) {
   if (!namelist_path || !run_dir) return HIPFT_EINVAL;
+  if (shard && (shard->nranks < 1 || shard->rank < 0 || shard->rank >= shard->nranks || !shard->allreduce ||
+                !shard->gather))
+    return HIPFT_EINVAL;
   hipft::Run r;
   r.dir = run_dir;
+  if (shard) {
+    r.shard = shard;
+    r.rank = shard->rank;
+    r.nranks = shard->nranks;
+  }
   std::string err;
   if (!hipft::read_namelist(namelist_path, r.nl, err)) {
     std::fprintf(stderr, "### ERROR in READ_INPUT_FILE: %s\n", err.c_str());
@@ -1020,6 +1093,11 @@ extern "C" int hipft_run_field(const char *namelist_path, const char *run_dir, i
   return rc;
 }
 
+extern "C" int hipft_run_field(const char *namelist_path, const char *run_dir, int device, double *f_out,
+                               size_t f_len) {
+  return hipft_run_shard(namelist_path, run_dir, device, nullptr, f_out, f_len);
+}
+
 extern "C" int hipft_run(const char *namelist_path, const char *run_dir, int device) {
-  return hipft_run_field(namelist_path, run_dir, device, nullptr, 0);
+  return hipft_run_shard(namelist_path, run_dir, device, nullptr, nullptr, 0);
 }

@@ -94,6 +94,8 @@ struct hipft_gpu {
   unsigned int *d_rcount = nullptr;
   int nkb = 0;
   PairTables ptab{};        // coefficient tables of the warp-specialised two-stage kernel
+  hipft_allreduce_cb red_cb = nullptr;  // scalar all-reduce over ranks (plain-mode sharding)
+  void *red_user = nullptr;
   PoleScratch pole{};       // chunk shares of the ring sums for k_pair_poles
   int pole_nch = 0;
   int *d_err = nullptr;   // set by kernels whose bounded waits gave up
@@ -181,6 +183,13 @@ static int fail(hipft_gpu *h, int code, const char *fmt, ...) {
       return fail((h), HIPFT_ECUDA, "%s:%d kernel launch: %s", __FILE__, __LINE__,          \
                   cudaGetErrorString(e_));                                                  \
   } while (0)
+
+// MIN/MAX of a scalar over the ranks sharing a run; a no-op on one process
+static int allreduce(hipft_gpu *h, int op, double *v) {
+  if (!h->red_cb) return HIPFT_OK;
+  if (h->red_cb(h->red_user, op, v) != 0) return fail(h, HIPFT_ECOMM, "all-reduce callback failed");
+  return HIPFT_OK;
+}
 
 template <typename T>
 static int dalloc(hipft_gpu *h, T **p, size_t n) {
@@ -934,6 +943,14 @@ static void analytic_profiles(const hipft_gpu *h, std::vector<double> &vt1, std:
   }
 }
 
+extern "C" int hipft_gpu_set_allreduce(hipft_gpu *h, hipft_allreduce_cb cb, void *user) {
+  if (!h) return HIPFT_EINVAL;
+  h->red_cb = cb;
+  h->red_user = user;
+  if (h->P.advance_diffusion) TRY(allreduce(h, HIPFT_RED_MIN, &h->dt_euler));  // src/hipft.f90:5036
+  return HIPFT_OK;
+}
+
 extern "C" int hipft_gpu_set_flow_from_files(hipft_gpu *h, const double *vt_pt, const double *vp_pt,
                                              int at_load) {
   if (!h || !vt_pt || !vp_pt) return HIPFT_EINVAL;
@@ -1101,6 +1118,7 @@ extern "C" int hipft_gpu_flow_dtmax(hipft_gpu *h, double *dtmax) {
   d = c_safety * d;
   if (h->P.strang_splitting) d = 2.0 * d;
   if (h->adv_time == 3) d = 2.0 * d;
+  TRY(allreduce(h, HIPFT_RED_MIN, &d));  // src/hipft.f90:7345
   *dtmax = d;
   return HIPFT_OK;
 }
@@ -1272,6 +1290,11 @@ static int ptl_dt(hipft_gpu *h, double *dtl) {
   TRY(sync_read(h, h->d_bits, 8));
   double axabsmax;
   std::memcpy(&axabsmax, h->h_pin, 8);
+  if (h->red_cb) {  // src/hipft.f90:5103: the PTL cells are those at the global maximum
+    TRY(allreduce(h, HIPFT_RED_MAX, &axabsmax));
+    CK(h, cudaMemcpyAsync(h->d_bits, &axabsmax, 8, cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+  }
   double d = DBL_MAX;
   if (axabsmax > 0.0) {
     unsigned long long init = 0x7fefffffffffffffULL;
@@ -1281,6 +1304,7 @@ static int ptl_dt(hipft_gpu *h, double *dtl) {
     LAUNCHED(h);
     TRY(sync_read(h, h->d_bits + 1, 8));
     std::memcpy(&d, h->h_pin, 8);
+    TRY(allreduce(h, HIPFT_RED_MIN, &d));  // src/hipft.f90:5141
     d = 0.95 * d;
     if (d < dtime_in) d = dtime_in;
   }

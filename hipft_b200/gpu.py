@@ -17,8 +17,9 @@ import numpy as np
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libhipft_gpu.so")
 
-HIPFT_OK, HIPFT_EINVAL, HIPFT_ECUDA, HIPFT_ETIMEOUT, HIPFT_ENAN, HIPFT_ESTATE, HIPFT_EIO, HIPFT_ENOMEM = range(8)
-STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ETIMEOUT", 4: "ENAN", 5: "ESTATE", 6: "EIO", 7: "ENOMEM"}
+HIPFT_OK, HIPFT_EINVAL, HIPFT_ECUDA, HIPFT_ETIMEOUT, HIPFT_ENAN, HIPFT_ESTATE, HIPFT_EIO, HIPFT_ENOMEM, HIPFT_ECOMM = \
+    range(9)
+STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ETIMEOUT", 4: "ENAN", 5: "ESTATE", 6: "EIO", 7: "ENOMEM", 8: "ECOMM"}
 
 DPTR = ctypes.POINTER(ctypes.c_double)
 
@@ -42,6 +43,16 @@ class Params(ctypes.Structure):
                 ("diffusion_coef_factor", ctypes.c_double), ("diffusion_coef_constants", DPTR),
                 ("pole_flux_lat_limit", ctypes.c_double), ("verbose", ctypes.c_int),
                 ("advance_source", ctypes.c_int)]
+
+
+ALLREDUCE_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
+GATHER_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int64,
+                             ctypes.POINTER(ctypes.c_double))
+
+
+class Shard(ctypes.Structure):
+    _fields_ = [("rank", ctypes.c_int), ("nranks", ctypes.c_int), ("allreduce", ALLREDUCE_CB),
+                ("gather", GATHER_CB), ("user", ctypes.c_void_p)]
 
 
 class FlowDef(ctypes.Structure):
@@ -110,6 +121,9 @@ SIGNATURES = [
     ("hipft_h5_read", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64),
                                      DPTR, DPTR, DPTR, DPTR]),
     ("hipft_gpu_set_flow_from_files", ctypes.c_int, [_H, DPTR, DPTR, ctypes.c_int]),
+    ("hipft_gpu_set_allreduce", ctypes.c_int, [_H, ALLREDUCE_CB, ctypes.c_void_p]),
+    ("hipft_run_shard", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(Shard), DPTR,
+                                       ctypes.c_size_t]),
     ("hipft_gpu_set_source_file", ctypes.c_int, [_H, DPTR]),
     ("hipft_gpu_set_rfe_frame", ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, DPTR, DPTR]),
     ("hipft_gpu_update_source", ctypes.c_int, [_H, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

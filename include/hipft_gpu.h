@@ -37,7 +37,8 @@ enum {
   HIPFT_ENAN = 4,     /* non-finite value detected                          */
   HIPFT_ESTATE = 5,   /* call out of order (e.g. step before set_field)     */
   HIPFT_EIO = 6,      /* file could not be read/written                     */
-  HIPFT_ENOMEM = 7    /* device allocation failed                           */
+  HIPFT_ENOMEM = 7,   /* device allocation failed                           */
+  HIPFT_ECOMM = 8     /* the all-reduce callback reported an error          */
 };
 
 typedef struct hipft_gpu hipft_gpu;
@@ -137,6 +138,23 @@ int hipft_gpu_get_field(hipft_gpu *h, double *f);
  * fix-up, m=0 poles, optional balance, multiply (src/hipft.f90:2116-2172). */
 int hipft_gpu_load_initial_map(hipft_gpu *h, const double *map_pt, int flux_balance,
                                double mult_fac);
+
+/* ---- several processes (realizations split over ranks) ------------------- */
+
+/* The reference splits the realizations over MPI ranks
+ * (set_local_number_of_realizations, src/hipft.f90:1006-1063) and keeps one
+ * time step for all of them with four scalar all-reduces: the explicit
+ * diffusion limit (MIN, src/hipft.f90:5036), PTL's max |A f| (MAX, 5103) and
+ * time step (MIN, 5141), and the flow CFL limit (MIN, 7345).  A handle that
+ * holds one rank's realizations gets those reductions through this callback:
+ * it replaces *value by the MIN (op 0) or MAX (op 1) over all ranks and
+ * returns 0 (anything else becomes HIPFT_ECOMM).  Every rank calls the
+ * library in the same sequence, so the callbacks happen in the same order on
+ * all ranks.  Setting it reduces the explicit diffusion limit at once, so
+ * all ranks call this right after hipft_gpu_create. */
+enum { HIPFT_RED_MIN = 0, HIPFT_RED_MAX = 1 };
+typedef int (*hipft_allreduce_cb)(void *user, int op, double *value);
+int hipft_gpu_set_allreduce(hipft_gpu *h, hipft_allreduce_cb cb, void *user);
 
 /* ---- flows -------------------------------------------------------------- */
 
@@ -277,6 +295,24 @@ int hipft_run(const char *namelist_path, const char *run_dir, int device);
  * equals ntm*npm*nr (the data of the reference's hipft_brmap_final.h5,
  * wrap_it_up src/hipft.f90:1381-1412, before its PT transpose). */
 int hipft_run_field(const char *namelist_path, const char *run_dir, int device, double *f_out, size_t f_len);
+
+/* One rank of a run whose realizations are split over processes, as the
+ * reference splits them over MPI ranks (src/hipft.f90:1006-1063: rank r takes
+ * the next floor(n/nranks) realizations, the low ranks one more).  allreduce:
+ * the scalar reductions of hipft_gpu_set_allreduce; gather: rank 0's `global`
+ * receives every rank's `local` (n_local doubles) concatenated in rank order,
+ * the other ranks pass global = NULL (write_map's MPI_Gatherv,
+ * src/hipft.f90:2874-2896); both return 0 on success.  Every rank writes the
+ * history files of its own realizations, rank 0 the maps and the map list.
+ * f_out receives this rank's realizations (f_len = ntm*npm*nr_local). */
+typedef struct {
+  int rank, nranks;
+  hipft_allreduce_cb allreduce;
+  int (*gather)(void *user, const double *local, int64_t n_local, double *global);
+  void *user;
+} hipft_shard;
+int hipft_run_shard(const char *namelist_path, const char *run_dir, int device, const hipft_shard *shard,
+                    double *f_out, size_t f_len);
 
 /* ---- map files ------------------------------------------------------------- */
 
