@@ -44,10 +44,10 @@ sys.path.insert(0, ROOT)
 METRIC = "FP64 Gcell-updates/s"
 UNIT = "Gcell-updates/s"
 STS_BYTES_PER_CELL = 40  # RKG2 stage k>=2: read Y_{k-1}, Y_{k-2}, u0, dty0; write Y_k
-# two-stage kernel per HIPFT_STS_PAIR value (the library's default is 4); the
-# timed region of a "launch" is the kernel plus, for 4, its pole-row launch
+# two-stage kernel per HIPFT_STS_PAIR value (the library's default is 5); the
+# timed region of a "launch" is the kernel plus, for 4 and 5, its pole-row launch
 STS_KERNELS = {"1": "k_sts_pair", "2": "k_sts_pair_p", "3": "k_sts_pair_march",
-               "4": "k_sts_pair_ws+k_pair_poles"}
+               "4": "k_sts_pair_ws+k_pair_poles", "5": "k_sts_pair_ws<rows2>+k_pair_poles"}
 
 WORKLOADS = {
     "batched64_1024x2048": dict(ntm=1024, npm1=2049, nr=64, seed=1),
@@ -282,7 +282,7 @@ def run_gpu(args, wl, name):
     sts_avg_ms = sts_ms / max(sts_n, 1)
     achieved = bytes_per_launch / (sts_avg_ms * 1e-3) / 1e9 if sts_n else None
     traffic, traffic_src = None, None
-    sts_kernel = STS_KERNELS.get(os.environ.get("HIPFT_STS_PAIR", "4"), STS_KERNELS["4"]) if stages_per_launch > 1.5 \
+    sts_kernel = STS_KERNELS.get(os.environ.get("HIPFT_STS_PAIR", "5"), STS_KERNELS["5"]) if stages_per_launch > 1.5 \
         else "k_sts_stage_v3"
     tpath = os.path.join(ROOT, "profiles", "sts_stage_traffic.json")
     if os.path.exists(tpath):

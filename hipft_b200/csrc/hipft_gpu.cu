@@ -394,8 +394,10 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
-// Two RKG2 stages per launch: HIPFT_STS_PAIR=4 (default) persistent
-// warp-specialised CTAs (k_sts_pair_ws, then k_pair_poles), 1 one CTA per
+// Two RKG2 stages per launch: HIPFT_STS_PAIR=5 (default) persistent
+// warp-specialised CTAs with two theta rows per consumer thread
+// (k_sts_pair_ws<false, true>, then k_pair_poles), 4 the same with one row
+// per consumer thread, 1 one CTA per
 // tile (k_sts_pair), 2 persistent double-buffered CTAs (k_sts_pair_p), 3 one
 // CTA per tile with row-marching arithmetic (k_sts_pair_march), 0 one stage
 // per launch (A/B timing).
@@ -403,8 +405,8 @@ static int sts_pair_variant() {
   static int v = -1;
   if (v < 0) {
     const char *e = std::getenv("HIPFT_STS_PAIR");
-    v = e ? std::atoi(e) : 4;
-    if (v < 0 || v > 4) v = 4;
+    v = e ? std::atoi(e) : 5;
+    if (v < 0 || v > 5) v = 5;
   }
   return v;
 }
@@ -489,7 +491,7 @@ static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const 
   const int ntj = (h->ntm + tj - 1) / tj;
   {
     ProfScope ps(h, HIPFT_K_STS);
-    if (sts_pair_variant() == 4) {
+    if (sts_pair_variant() >= 4) {
       const int grid = std::min(h->ptab.ntiles, 2 * h->num_sms);
       const PairArgs pa{ca, cb, h->d_err};
       const double *rin = h->d_ringbuf[h->ring_cur];
@@ -498,9 +500,13 @@ static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const 
                                                                     out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
                                                                     h->ptab);
       } else {
-        k_sts_pair_ws<false><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
-                                                                     out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
-                                                                     h->ptab);
+        if (sts_pair_variant() == 5)
+          k_sts_pair_ws<false, true><<<grid, kWThreads, kWSmem, h->stream>>>(
+              h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab);
+        else
+          k_sts_pair_ws<false><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
+                                                                       out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
+                                                                       h->ptab);
         LAUNCHED(h);
         dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
         k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
@@ -654,6 +660,8 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
       cudaFuncSetAttribute(k_sts_pair_ws<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_ws<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess)
     return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernels"));
   if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->num_sms < 1)
@@ -683,7 +691,7 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
     pt.LR = pt.nb * kWJ + 4;
     pt.LC = pt.nkt * kWK + 4;
     double *tab = nullptr;
-    const size_t nrow = (size_t)nr * pt.LR * 4, ncol = (size_t)nr * pt.LC * 2;
+    const size_t nrow = (size_t)nr * pt.LR * 3, ncol = (size_t)nr * pt.LC * 2;
     if ((rc = dalloc(h, &tab, nrow + ncol))) return bail(rc);
     pt.row = tab;
     pt.col = tab + nrow;

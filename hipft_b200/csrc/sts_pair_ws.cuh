@@ -44,8 +44,8 @@ constexpr int kWX1 = 0;                        // Y_{k-1}: kWK+4 columns (shared
 constexpr int kWY2 = kWX1 + (kWK + 4) * kWR;   // Y_{k-2}: kWK+2 columns (shared columns 1..kWK+2)
 constexpr int kWU = kWY2 + (kWK + 2) * kWR;    // u0
 constexpr int kWD = kWU + (kWK + 2) * kWR;     // dty0
-constexpr int kWRT = kWD + (kWK + 2) * kWR;    // rows: {st_i, c2, c4, 0} per shared row
-constexpr int kWCT = kWRT + 4 * kWR;           // columns: {P1, P5} per shared column
+constexpr int kWRT = kWD + (kWK + 2) * kWR;    // rows: st_i, c2, c4, each kWR long
+constexpr int kWCT = kWRT + 3 * kWR;           // columns: {P1, P5} per shared column
 constexpr int kWInfo = kWCT + 2 * (kWK + 4);  // tile record: D, pole terms, (kt, rb, i)
 constexpr int kWBuf = kWInfo + 8;
 constexpr int kWYk = kWNB * kWBuf;             // Y_k: kWK+2 columns, consumers only
@@ -58,9 +58,10 @@ static_assert((kWR * 8) % 16 == 0, "column stride must keep 16-byte alignment");
 
 // Coefficient tables of the two-stage kernels, in load_diffusion_matrix's
 // operation order (src/hipft.f90:6880-6920) for a per-realization constant D:
-//   rows    [nr][LR][4]: entry jj holds theta row j = jj-1:
-//           {st_i(j), Dh dth_i(j) dt_i(j) st_i(j) sth(j), Dh dth_i(j+1) dt_i(j) st_i(j) sth(j+1), 0}
-//           for 2 <= j <= ntm-1, zeros elsewhere;
+//   rows    [nr][3][LR]: entry jj of the three arrays holds theta row j = jj-1:
+//           st_i(j), Dh dth_i(j) dt_i(j) st_i(j) sth(j), Dh dth_i(j+1) dt_i(j) st_i(j) sth(j+1)
+//           for 2 <= j <= ntm-1, zeros elsewhere (separate arrays, so that
+//           consecutive rows are consecutive in shared memory);
 //   columns [nr][LC][2]: entry kk holds phi column kk mapped onto the interior
 //           column kw in 2..npm-1 it duplicates: {Dh dph_i(kw) dp_i(kw), Dh dph_i(kw+1) dp_i(kw)}.
 __global__ void k_pair_tables(Mesh m, const double *__restrict__ dfac, int LR, int LC, double *rowtab,
@@ -78,11 +79,10 @@ __global__ void k_pair_tables(Mesh m, const double *__restrict__ dfac, int LR, i
         c2 = Dh * m.dth_i[j] * m.dt_i[j] * st * m.sth[j];
         c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * st * m.sth[j + 1];
       }
-      double *o = rowtab + e * 4;
+      double *o = rowtab + (int64_t)(i - 1) * 3 * LR + (e % LR);
       o[0] = st;
-      o[1] = c2;
-      o[2] = c4;
-      o[3] = 0.0;
+      o[LR] = c2;
+      o[2 * LR] = c4;
     } else {
       const int64_t f = e - nrow;
       const int i = (int)(f / LC) + 1, kk = (int)(f % LC);
@@ -150,7 +150,56 @@ struct PairTables {
   int nb, nkt, ntiles;      // theta blocks, phi tiles, all tiles
 };
 
-template <bool INLINE_POLES>
+// One stencil-and-combine step for a theta-row pair (a, b = a+1) of one
+// column, in the single-row kernels' operation order: xl, xc, xr the pair in
+// columns c-1, c, c+1 of the stage input; up = row a-1 and dn = row b+1 of
+// column c; st2, c22, c42 the rows' st_i, c2, c4; P the column's {P1, P5};
+// pole rows take ax from the ring sums; o2 the second input (Y_{k-2} for
+// stage k, Y_{k-1} for stage k+1), u = u0, d = dty0.
+__device__ __forceinline__ double2 pair_rows_step(double2 xl, double2 xc, double2 xr, double up, double dn,
+                                                  double2 st2, double2 c22, double2 c42, double2 P, bool pola,
+                                                  bool polb, double axpa, double axpb, double2 o2, double2 u,
+                                                  double2 d, const StageCoef &sc) {
+  double axa, axb;
+  if (pola) {
+    axa = axpa;
+  } else {
+    const double st = st2.x, c2 = c22.x, c4 = c42.x;
+    const double c1 = P.x * st * st;
+    const double c5 = P.y * st * st;
+    const double c3 = -(c1 + c2 + c4 + c5);
+    axa = c1 * xl.x + c2 * up + c3 * xc.x + c4 * xc.y + c5 * xr.x;
+  }
+  if (polb) {
+    axb = axpb;
+  } else {
+    const double st = st2.y, c2 = c22.y, c4 = c42.y;
+    const double c1 = P.x * st * st;
+    const double c5 = P.y * st * st;
+    const double c3 = -(c1 + c2 + c4 + c5);
+    axb = c1 * xl.y + c2 * xc.x + c3 * xc.y + c4 * dn + c5 * xr.y;
+  }
+  return make_double2(sc.a * xc.x + sc.b * o2.x + sc.c * u.x + sc.d * axa + sc.e * d.x,
+                      sc.a * xc.y + sc.b * o2.y + sc.c * u.y + sc.d * axb + sc.e * d.y);
+}
+
+// The pair's value to HBM (16-byte store when both rows are kept) and to the
+// seam column it duplicates.
+__device__ __forceinline__ void store_pair(double *g, double2 y, bool va, bool vb, int64_t seam_off) {
+  if (va && vb) {
+    *reinterpret_cast<double2 *>(g) = y;
+    if (seam_off) *reinterpret_cast<double2 *>(g + seam_off) = y;
+  } else {
+    if (va) g[0] = y.x;
+    if (vb) g[1] = y.y;
+    if (seam_off) {
+      if (va) g[seam_off] = y.x;
+      if (vb) g[seam_off + 1] = y.y;
+    }
+  }
+}
+
+template <bool INLINE_POLES, bool ROWPAIRS = false>
 __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const double *__restrict__ dfac,
                                                              const double *__restrict__ ykm1,
                                                              const double *__restrict__ ykm2,
@@ -198,7 +247,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       const int roff = rs - (j0 - 2);
       const int64_t pbase = (int64_t)(i - 1) * m.plane;
       double *B = wsm + b * kWBuf;
-      const int nx = nk + 4, ny = nk + 2, ncp = nx + 3 * ny + 2;
+      const int nx = nk + 4, ny = nk + 2, ncp = nx + 3 * ny + 4;
       if (lane == 0) {
         // the tile record, written before the arrival that releases it
         double *I = B + kWInfo;
@@ -209,7 +258,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         Ii[0] = kt;
         Ii[1] = rb;
         Ii[2] = i;
-        mbar_expect_tx(&full[b], (uint32_t)(nx + 3 * ny) * run + (uint32_t)(kWR * 32 + (kWK + 4) * 16));
+        mbar_expect_tx(&full[b], (uint32_t)(nx + 3 * ny) * run + (uint32_t)(3 * kWR * 8 + (kWK + 4) * 16));
       }
       __syncwarp();
       for (int q = lane; q < ncp; q += 32) {
@@ -226,10 +275,11 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
           const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
           src = (a == 0 ? ykm2 : (a == 1 ? u0 : dty0)) + g;
           dst = B + (a == 0 ? kWY2 : (a == 1 ? kWU : kWD)) + (c - 1) * kWR + roff;
-        } else if (q == nx + 3 * ny) {
-          src = pt.row + ((int64_t)(i - 1) * pt.LR + (int64_t)rb * kWJ) * 4;
-          dst = B + kWRT;
-          bytes = kWR * 32;
+        } else if (q < nx + 3 * ny + 3) {
+          const int a = q - (nx + 3 * ny);
+          src = pt.row + ((int64_t)(i - 1) * 3 + a) * pt.LR + (int64_t)rb * kWJ;
+          dst = B + kWRT + a * kWR;
+          bytes = kWR * 8;
         } else {
           src = pt.col + ((int64_t)(i - 1) * pt.LC + (int64_t)kt * kWK) * 2;
           dst = B + kWCT;
@@ -277,13 +327,73 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     const int64_t seam = (int64_t)(npm - 2) * ld;
 
     // ---------------------------------------------- stage k: Y_k into sYk
-    if (nk == kWK) {
+    if (ROWPAIRS && nk == kWK) {
+      // thread: theta-row pair (r0, r0+1), r0 = 2(tid % 64), and a group of
+      // columns 1-3, 4-6, 7-8 or 9-10; the pairs of rows 128-131 are units of
+      // their own for 20 threads of the two-column groups
+      auto rowf = [&](int r0, double2 &st2, double2 &c22, double2 &c42) {
+        st2 = *reinterpret_cast<const double2 *>(RT + r0);
+        c22 = *reinterpret_cast<const double2 *>(RT + kWR + r0);
+        c42 = *reinterpret_cast<const double2 *>(RT + 2 * kWR + r0);
+      };
+      auto unit = [&](int r0, int c, double2 xl, double2 xc, double2 xr, double2 st2, double2 c22,
+                      double2 c42) -> double2 {
+        const int ja = j0 - 2 + r0, jb = ja + 1;
+        const double up = X1[c * kWR + r0 - 1], dn = X1[c * kWR + r0 + 2];
+        const double2 o2 = *reinterpret_cast<const double2 *>(Y2 + (c - 1) * kWR + r0);
+        const double2 u = *reinterpret_cast<const double2 *>(U + (c - 1) * kWR + r0);
+        const double2 d = *reinterpret_cast<const double2 *>(D + (c - 1) * kWR + r0);
+        const double2 y = pair_rows_step(xl, xc, xr, up, dn, st2, c22, c42, CT[c],
+                                         ja == 1 || ja == ntm, jb == 1 || jb == ntm, ja == 1 ? ax_n : ax_s,
+                                         jb == 1 ? ax_n : ax_s, o2, u, d, sa);
+        return y;
+      };
+      auto put = [&](int r0, int c, double2 y) {
+        *reinterpret_cast<double2 *>(sYk + (c - 1) * kWR + r0) = y;
+        if (c >= 2 && c <= kWK + 1 && r0 >= 2 && r0 <= kWJ) {
+          const int ja = j0 - 2 + r0, k = k0 - 2 + c;
+          const bool va = (ja >= 1 && ja <= ntm), vb = (ja + 1 >= 1 && ja + 1 <= ntm);
+          const int64_t so = (k == 2) ? seam : ((k == npm - 1) ? -seam : 0);
+          store_pair(out_k + pbase + (int64_t)(k - 1) * ld + (ja - 1), y, va, vb, so);
+        }
+      };
+      const int g = tid >> 6, r0 = 2 * (tid & 63);
+      const int cb = (g == 0) ? 1 : ((g == 1) ? 4 : ((g == 2) ? 7 : 9));
+      const int nc = (g < 2) ? 3 : 2;
+      double2 st2, c22, c42;
+      rowf(r0, st2, c22, c42);
+      double2 xl = *reinterpret_cast<const double2 *>(X1 + (cb - 1) * kWR + r0);
+      double2 xc = *reinterpret_cast<const double2 *>(X1 + cb * kWR + r0);
+      double2 y[3];
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        if (s < nc) {
+          const double2 xr = *reinterpret_cast<const double2 *>(X1 + (cb + s + 1) * kWR + r0);
+          y[s] = unit(r0, cb + s, xl, xc, xr, st2, c22, c42);
+          xl = xc;
+          xc = xr;
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 3; ++s)
+        if (s < nc) put(r0, cb + s, y[s]);
+      const int e = tid - 2 * 64;  // units of the pairs at rows 128 and 130
+      if (e >= 0 && e < 2 * (kWK + 2)) {
+        const int rr = kWJ + 2 * (e & 1), c = 1 + (e >> 1);
+        const double2 a = *reinterpret_cast<const double2 *>(X1 + (c - 1) * kWR + rr);
+        const double2 b = *reinterpret_cast<const double2 *>(X1 + c * kWR + rr);
+        const double2 z = *reinterpret_cast<const double2 *>(X1 + (c + 1) * kWR + rr);
+        double2 sx, cx2, cx4;
+        rowf(rr, sx, cx2, cx4);
+        put(rr, c, unit(rr, c, a, b, z, sx, cx2, cx4));
+      }
+    } else if (nk == kWK) {
       {
         const int r = r2, j = j0 - 2 + r;
         const bool rowst = (j >= 1 && j <= ntm) && r >= 2;
         const bool pole = (j == 1 || j == ntm);
         const double axp = (j == 1) ? ax_n : ax_s;
-        const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+        const double sti = RT[r], c2 = RT[kWR + r], c4 = RT[2 * kWR + r];
         const int cb = 1 + 5 * h;  // columns cb..cb+4
         const double *x = X1 + cb * kWR + r;
         const double *y2 = Y2 + (cb - 1) * kWR + r, *uu = U + (cb - 1) * kWR + r, *dd = D + (cb - 1) * kWR + r;
@@ -337,7 +447,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
           } else if (j == ntm) {
             ax = ax_s;
           } else {
-            const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+            const double sti = RT[r], c2 = RT[kWR + r], c4 = RT[2 * kWR + r];
             const double2 P = CT[c];
             const double c1 = P.x * sti * sti;
             const double c5 = P.y * sti * sti;
@@ -369,7 +479,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         } else if (j == ntm) {
           ax = ax_s;
         } else {
-          const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+          const double sti = RT[r], c2 = RT[kWR + r], c4 = RT[2 * kWR + r];
           const double2 P = CT[c];
           const double c1 = P.x * sti * sti;
           const double c5 = P.y * sti * sti;
@@ -407,10 +517,41 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     }
 
     // -------------------------------------- stage k+1: Y_{k+1} to HBM
-    if (nk == kWK) {
+    if (ROWPAIRS && nk == kWK) {
+      // thread: theta-row pair (r0, r0+1), r0 = 2 + 2(tid % 64), columns
+      // 2 + 2(tid / 64) and the next one
+      const int r0 = 2 + 2 * (tid & 63), cb = 2 + 2 * (tid >> 6);
+      const int ja = j0 - 2 + r0;
+      const double2 st2 = *reinterpret_cast<const double2 *>(RT + r0);
+      const double2 c22 = *reinterpret_cast<const double2 *>(RT + kWR + r0);
+      const double2 c42 = *reinterpret_cast<const double2 *>(RT + 2 * kWR + r0);
+      const bool va = (ja >= 2 && ja <= ntm - 1), vb = (ja + 1 >= 2 && ja + 1 <= ntm - 1);
+      double2 xl = *reinterpret_cast<const double2 *>(sYk + (cb - 2) * kWR + r0);
+      double2 xc = *reinterpret_cast<const double2 *>(sYk + (cb - 1) * kWR + r0);
+      double2 y[2];
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int c = cb + s;
+        const double2 xr = *reinterpret_cast<const double2 *>(sYk + c * kWR + r0);
+        const double up = sYk[(c - 1) * kWR + r0 - 1], dn = sYk[(c - 1) * kWR + r0 + 2];
+        const double2 o2 = *reinterpret_cast<const double2 *>(X1 + c * kWR + r0);
+        const double2 u = *reinterpret_cast<const double2 *>(U + (c - 1) * kWR + r0);
+        const double2 d = *reinterpret_cast<const double2 *>(D + (c - 1) * kWR + r0);
+        y[s] = pair_rows_step(xl, xc, xr, up, dn, st2, c22, c42, CT[c], false, false, 0.0, 0.0, o2,
+                              u, d, sb);
+        xl = xc;
+        xc = xr;
+      }
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        const int k = k0 - 2 + cb + s;
+        const int64_t so = (k == 2) ? seam : ((k == npm - 1) ? -seam : 0);
+        store_pair(out_k1 + pbase + (int64_t)(k - 1) * ld + (ja - 1), y[s], va, vb, so);
+      }
+    } else if (nk == kWK) {
       const int r = r3, j = j0 - 2 + r;
       const bool rowok = (j >= 2 && j <= ntm - 1);
-      const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+      const double sti = RT[r], c2 = RT[kWR + r], c4 = RT[2 * kWR + r];
       const int cb = 2 + 4 * h;  // columns cb..cb+3
       const double *yk = sYk + (cb - 1) * kWR + r;
       const double *x1 = X1 + cb * kWR + r, *uu = U + (cb - 1) * kWR + r, *dd = D + (cb - 1) * kWR + r;
@@ -443,7 +584,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         const int r = 2 + e % kWJ, c = 2 + e / kWJ;
         const int j = j0 - 2 + r;
         if (j < 2 || j > ntm - 1) continue;
-        const double sti = RT[4 * r], c2 = RT[4 * r + 1], c4 = RT[4 * r + 2];
+        const double sti = RT[r], c2 = RT[kWR + r], c4 = RT[2 * kWR + r];
         const double2 P = CT[c];
         const double c1 = P.x * sti * sti;
         const double c5 = P.y * sti * sti;

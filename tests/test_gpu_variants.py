@@ -25,6 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "pair_persistent": {"HIPFT_STS_PAIR": "2"},
             "pair_64x16": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "64x16"}, "pair_march": {"HIPFT_STS_PAIR": "3"},
             "pair_ws": {"HIPFT_STS_PAIR": "4"}, "pair_ws_inline": {"HIPFT_STS_PAIR": "4", "HIPFT_WS_POLES": "1"},
+            "pair_ws_rowpairs": {"HIPFT_STS_PAIR": "5"},
             "pair_256x4": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "256x4"},
             "single_v3": {"HIPFT_STS_PAIR": "0"}, "single_v2": {"HIPFT_STS_PAIR": "0", "HIPFT_STS_KERNEL": "2"}}
 RUNS = ["diffuse_soccer", "rkg2_auto_ntm33", "rkg2_auto_ntm161", "rkg2_ntm129_np65", "rkg2_ntm130_np96",
