@@ -20,6 +20,10 @@ device->host after every step.  Multi-GPU: realizations are split across
 ranks (block split, low ranks take the remainder) and every rank advances its
 own share independently -- weak scaling, no data-path collective.
 
+At N = 1 the line also carries "plain": the same metric for the plain
+configuration (one realization, 1024 x 2048, fixed physics, no assimilation),
+timed step by step with an L2 flush before each step (its fields fit in L2).
+
 `--impl reference` times the CPU oracle (the restatement of the reference's
 solver in oracle/, all host threads) on a bounded sample of the same
 workload: one realization, one flux-transport step per bench step.
@@ -230,7 +234,6 @@ def run_gpu(args, wl, name):
         dist.barrier()
     torch.cuda.synchronize()
     i0 = g.info()
-    g.set_profiling(True)
     clocks = ClockSampler(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -242,14 +245,28 @@ def run_gpu(args, wl, name):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     i1 = g.info()
+    cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
+    launches = int(i1.kernel_launches - i0.kernel_launches)
+    # kernel breakdown in a second pass of the same steps: per-kernel events
+    # sit between launches, which the timed pass above keeps free of them
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ip = g.info()
+    g.set_profiling(True)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(args.steps):
+        step()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    ms_prof = p0.elapsed_time(p1)
     sts_n, sts_ms = g.kernel_time(0)
     adv_n, adv_ms = g.kernel_time(1)
     ring_n, ring_ms = g.kernel_time(2)
     oth_n, oth_ms = g.kernel_time(3)
     g.set_profiling(False)
-    cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
-    launches = int(i1.kernel_launches - i0.kernel_launches)
-    rkg2_stages = int(i1.rkg2_stages - i0.rkg2_stages)
+    rkg2_stages = int(g.info().rkg2_stages - ip.rkg2_stages)
 
     # end to end through the C ABI with host buffers
     f_host = torch.empty((nrl, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
@@ -307,7 +324,8 @@ def run_gpu(args, wl, name):
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "launches": sts_n, "avg_launch_ms": sts_avg_ms,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
-                     "share_of_step": sts_ms / ms if ms > 0 else None,
+                     "share_of_step": sts_ms / ms_prof if ms_prof > 0 else None,
+                     "timing": "per-kernel CUDA events in a second pass of the same steps",
                      "other_kernels_ms": {"advection_stage": adv_ms, "ring_sums": ring_ms, "other": oth_ms},
                      "other_kernels_launches": {"advection_stage": adv_n, "ring_sums": ring_n, "other": oth_n}},
         "e2e": {"value": e2e_cells / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
@@ -315,6 +333,8 @@ def run_gpu(args, wl, name):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and not args.no_plain:
+        out["plain"] = measure_plain(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cells_c, sec_c = oracle_sample(t, p, br, prm, dt, index=0)
         out["cpu_baseline"] = {"value": cells_c / sec_c / 1e9, "unit": UNIT, "cores": host_threads(),
@@ -330,6 +350,98 @@ def run_gpu(args, wl, name):
     return 0
 
 
+def measure_plain(args, local: int):
+    """The plain configuration beside the batched one: one realization on the
+    same 1024 x 2048 refined grid with fixed physics (D 300 km^2/s, v0 15 m/s,
+    B -2.40, C -1.80 deg/day), no assimilation.  Its fields (17 MB) fit in L2,
+    so a 256 MB buffer is written between timed steps and each step is timed
+    alone; e2e adds the host copies of the field."""
+    import torch
+    import hipft_b200 as H
+    from hipft_b200 import synthetic as S
+    wl = WORKLOADS["single_1024x2048"]
+    t = S.refined_theta(wl["ntm"])
+    p = S.uniform_phi(wl["npm1"])
+    br = S.bipole_map(t, p, wl["seed"])
+    prm = S.plain_params()
+    g = H.HipftGPU(t, p, 1, device=local, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                   advance_diffusion=True, diffusion_coef_constants=prm["diffusion_coef_constants"])
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    g.load_initial_map(br[None])
+    g.set_flow(dr_model=1, mf_model=1, dr_p0=prm["dr_p0"], dr_p2=prm["dr_p2"], dr_p4=prm["dr_p4"],
+               mf_p1=prm["mf_p1"], mf_p3=prm["mf_p3"], mf_p5=prm["mf_p5"])
+    g.update_flow()
+    dt = g.flow_dtmax()
+    ntm, npm = g.ntm, g.npm
+    state = {"time": 0.0}
+
+    def step():
+        g.flux_transport_step(dt)
+        state["time"] += dt
+        g.analysis(state["time"])
+
+    flush = torch.empty(32 * 1024 * 1024, dtype=torch.float64, device=f"cuda:{local}")  # 256 MB > L2
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def timed(profile: bool):
+        info0 = g.info()
+        g.set_profiling(profile)
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return info0, g.info(), tot
+
+    i0, i1, ms = timed(False)
+    ip, ip1, ms_prof = timed(True)
+    sts_n, sts_ms = g.kernel_time(0)
+    g.set_profiling(False)
+    cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
+    rkg2 = int(ip1.rkg2_stages - ip.rkg2_stages)
+    f_host = torch.empty((1, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
+    g.get_field(f_host)
+    torch.cuda.synchronize()
+    i2 = g.info()
+    w = 0.0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        g.set_field(f_host)
+        step()
+        g.get_field(f_host)
+        w += time.perf_counter() - w0
+    i3 = g.info()
+    peak, peak_kind = measured_peak()
+    spl = rkg2 / max(sts_n, 1)
+    avg = sts_ms / max(sts_n, 1)
+    achieved = STS_BYTES_PER_CELL * ntm * (npm - 2) * spl / (avg * 1e-3) / 1e9 if sts_n else None
+    out = {"workload": "single_1024x2048", "grid": [ntm, npm - 2], "realizations": 1, "dt_hours": dt,
+           "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": ms / args.steps, "steps": args.steps,
+           "l2": "256 MB buffer written before every timed step, each step timed alone (fields fit in L2)",
+           "e2e": {"value": float(i3.cell_stage_updates - i2.cell_stage_updates) / w / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": ntm * npm * 8, "d2h_bytes_per_step": ntm * npm * 8},
+           "roofline": {"kernel": STS_KERNELS.get(os.environ.get("HIPFT_STS_PAIR", "5"), STS_KERNELS["5"]),
+                        "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                        "avg_launch_ms": avg, "launches": sts_n,
+                        "share_of_step": sts_ms / ms_prof if ms_prof > 0 else None,
+                        "note": "L2-resident after the first stages of a step; a fraction of the HBM copy "
+                                "bandwidth is not a DRAM measurement here"},
+           "gpu_launches": int(i1.kernel_launches - i0.kernel_launches)}
+    g.close()
+    del flush
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -338,6 +450,7 @@ def main():
     ap.add_argument("--impl", default="hipft", choices=["hipft", "reference"])
     ap.add_argument("--workload", default="batched64_1024x2048", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

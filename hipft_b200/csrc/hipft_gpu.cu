@@ -411,6 +411,16 @@ static int sts_pair_variant() {
   return v;
 }
 static bool sts_pairs_enabled() { return sts_pair_variant() != 0; }
+// HIPFT_PDL=0 turns off the programmatic (overlapping) launch of the
+// two-stage kernel after the previous pair's pole-row kernel.
+static bool ws_pdl() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_PDL");
+    v = (e && std::atoi(e) == 0) ? 0 : 1;
+  }
+  return v == 1;
+}
 // HIPFT_WS_POLES=1: k_sts_pair_ws finishes the pole rows itself (last
 // pole-holding tile); default 0: a separate k_pair_poles launch does.
 static bool ws_inline_poles() {
@@ -480,8 +490,11 @@ static const PairShape &pair_shape() {
   return kPairShapes[idx];
 }
 
+// overlap_prev: the launch before this one on the stream is the previous
+// pair's k_pair_poles (so the two-stage kernel may start while it runs;
+// everything else it reads was finished by the kernels before that one).
 static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
-                    double *out_k, double *out_k1, StageCoef ca, StageCoef cb) {
+                    double *out_k, double *out_k1, StageCoef ca, StageCoef cb, bool overlap_prev) {
   const PairShape &ps_ = pair_shape();
   const int tk = (sts_pair_variant() >= 2) ? kPK : ps_.tk;
   const int tj = (sts_pair_variant() >= 2) ? kPJ : ps_.tj;
@@ -500,13 +513,26 @@ static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const 
                                                                     out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
                                                                     h->ptab);
       } else {
+        // programmatic dependent launch: may overlap the previous pair's
+        // k_pair_poles (the kernel's pole tiles wait for it)
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3(kWThreads);
+        cfg.dynamicSmemBytes = kWSmem;
+        cfg.stream = h->stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaError_t le;
         if (sts_pair_variant() == 5)
-          k_sts_pair_ws<false, true><<<grid, kWThreads, kWSmem, h->stream>>>(
-              h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab);
+          le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
+                                  dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab);
         else
-          k_sts_pair_ws<false><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
-                                                                       out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
-                                                                       h->ptab);
+          le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, false>, h->M, (const double *)h->DC.dfac, ykm1, ykm2,
+                                  u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab);
+        if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
         LAUNCHED(h);
         dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
         k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
@@ -1233,7 +1259,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
     if (fused && sts_pairs_enabled() && k + 1 <= h->sts_s) {
       int bk = free_buf(-1), bk1 = free_buf(bk);
       TRY(sts_pair(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[bk], h->buf[bk1], coef(k),
-                   coef(k + 1)));
+                   coef(k + 1), k > 2));
       ykm2 = bk;
       ykm1 = bk1;
       k += 2;

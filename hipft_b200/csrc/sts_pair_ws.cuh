@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     // ------------------------------------------------------------ producer
     const int lane = tid - kWCons;
     int n = 0;
-    bool ok = true;
+    bool ok = true, dep_done = false;
     for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
       const int b = n % kWNB, u = n / kWNB;
       if (u >= 1 && !mbar_wait_bounded(&empty[b], (uint32_t)((u - 1) & 1), 1u << 22)) {
@@ -248,12 +248,22 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       const int64_t pbase = (int64_t)(i - 1) * m.plane;
       double *B = wsm + b * kWBuf;
       const int nx = nk + 4, ny = nk + 2, ncp = nx + 3 * ny + 4;
+      // Launched programmatically after the previous pair's k_pair_poles,
+      // this kernel may start while that one still runs; it reads and writes
+      // the pole rows 1, ntm, the rows 2, ntm-1 next to them and the ring
+      // sums.  Tiles whose rows (with halo) reach those rows wait for it to
+      // finish first; the other tiles touch none of them.  (Without such a
+      // launch the wait returns at once.)
+      if (!dep_done && (j0 - 2 <= 2 || j0 + kWJ + 1 >= ntm - 1)) {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        dep_done = true;
+      }
       if (lane == 0) {
         // the tile record, written before the arrival that releases it
         double *I = B + kWInfo;
         I[0] = dfac[i];
-        I[1] = ring_in[2 * (i - 1)] * bcn;
-        I[2] = -ring_in[2 * (i - 1) + 1] * bcs;
+        I[1] = dep_done ? ring_in[2 * (i - 1)] * bcn : 0.0;  // used by pole tiles only
+        I[2] = dep_done ? -ring_in[2 * (i - 1) + 1] * bcs : 0.0;
         int *Ii = reinterpret_cast<int *>(I + 3);
         Ii[0] = kt;
         Ii[1] = rb;
@@ -678,6 +688,9 @@ __global__ void __launch_bounds__(kPoleThreads) k_pair_poles(Mesh m, const doubl
   __shared__ double sh[2 * (kPoleThreads / 32)];
   __shared__ double s_ring[2];
   __shared__ int s_last;
+  // the next pair's kernel may launch now; its tiles at the poles wait for
+  // this grid to finish (griddepcontrol.wait)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int tid = threadIdx.x, i = blockIdx.x + 1, ch = blockIdx.y, nch = gridDim.y;
   const int ntm = m.ntm, npm = m.npm;
   const int64_t ld = m.ldt, pbase = (int64_t)(i - 1) * m.plane;

@@ -104,6 +104,18 @@ def batched_params(nr: int, seed: int) -> dict:
     )
 
 
+def plain_params() -> dict:
+    """Coefficients of the plain (one realization) configuration: D = 300
+    km^2/s, v0 = 15 m/s, differential rotation B = -2.40, C = -1.80 deg/day."""
+    v0 = 15.0
+    return dict(
+        diffusion_coef_constants=np.array([300.0]),
+        dr_p0=np.zeros(1), dr_p2=np.array([-2.40 * DEG_DAY_TO_M_S]), dr_p4=np.array([-1.80 * DEG_DAY_TO_M_S]),
+        mf_p1=np.array([2.0 * v0]), mf_p3=np.array([-2.0 * v0]), mf_p5=np.zeros(1),
+        mu_power=np.full(1, 4.0), mu_limit=np.full(1, 0.1), lat_limit=np.zeros(1),
+    )
+
+
 def observed_map(t: np.ndarray, p: np.ndarray, time_hr: float, seed: int, noise_g: float = 2.0) -> np.ndarray:
     """(3, ntm, npm1) assimilation map [data, weight, mu] at model time time_hr."""
     rng = np.random.Generator(np.random.PCG64(seed + int(time_hr * 16)))
