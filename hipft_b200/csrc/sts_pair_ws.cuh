@@ -239,7 +239,10 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         break;
       }
       const int kt = t % pt.nkt, rest = t / pt.nkt;
-      const int rb = rest % pt.nb, i = rest / pt.nb + 1;
+      // theta blocks in the order 1..nb-2, 0, nb-1: interior tiles first, so
+      // that the wait for the previous pole kernel comes as late as possible
+      const int q = rest % pt.nb, i = rest / pt.nb + 1;
+      const int rb = (pt.nb <= 2) ? q : ((q < pt.nb - 2) ? q + 1 : ((q == pt.nb - 2) ? 0 : pt.nb - 1));
       const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
       const int nk = min(kWK, npm - 1 - k0 + 1);
       const int rs = max(1, j0 - 2), re = min((int)ld, j0 + kWJ + 1);
