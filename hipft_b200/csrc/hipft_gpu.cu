@@ -1314,6 +1314,18 @@ static int euler_steps(hipft_gpu *h, double dtl) {
 }
 
 // get_dtime_diffusion_ptl (src/hipft.f90:5042-5161).
+// Reads and clears the flag that kernels set when a bounded wait gave up;
+// HIPFT_ETIMEOUT if it was set (the context stays usable).
+static int check_wait_flag(hipft_gpu *h, const char *what) {
+  int ev = 0;
+  CK(h, cudaMemcpyAsync(&ev, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  if (!ev) return HIPFT_OK;
+  CK(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
+  CK(h, cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned int) * h->nr, h->stream));
+  return fail(h, HIPFT_ETIMEOUT, "%s", what);
+}
+
 static int ptl_dt(hipft_gpu *h, double *dtl) {
   double dtime_in = *dtl;
   double *f = h->buf[h->cur], *af = h->buf[scratch(h, 0)];
@@ -1381,16 +1393,7 @@ extern "C" int hipft_gpu_diffusion_step(hipft_gpu *h, double dtl, hipft_cycle_cb
     i = i + 1;
   }
   if (h->auto_sc) h->subcycles_state = i;
-  {
-    int ev = 0;
-    CK(h, cudaMemcpyAsync(&ev, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    CK(h, cudaStreamSynchronize(h->stream));
-    if (ev) {
-      CK(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
-      CK(h, cudaMemsetAsync(h->d_rcount, 0, sizeof(unsigned int) * h->nr, h->stream));
-      return fail(h, HIPFT_ETIMEOUT, "diffusion_step: a bounded wait for staged tiles gave up");
-    }
-  }
+  TRY(check_wait_flag(h, "diffusion_step: a bounded wait for staged tiles gave up"));
   if (info) {
     info->dtime_diffusion_euler = h->dt_euler;
     info->sts_s = (h->P.diffusion_num_method == 1) ? h->n_euler : h->sts_s;
@@ -1760,6 +1763,22 @@ extern "C" int hipft_gpu_set_stream(hipft_gpu *h, void *s) {
     CK(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     h->own_stream = true;
   }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_check_bounded_wait(hipft_gpu *h, unsigned int limit) {
+  if (!h || limit == 0 || limit > (1u << 22)) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  k_wait_selftest<<<1, 32, 0, h->stream>>>(limit, h->d_err);
+  LAUNCHED(h);
+  return check_wait_flag(h, "check_bounded_wait: the wait gave up as intended");
+}
+
+extern "C" int hipft_gpu_field_device_ptr(hipft_gpu *h, double **ptr, int *ldt) {
+  if (!h || !ptr || !ldt) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "field_device_ptr before set_field");
+  *ptr = h->buf[h->cur];
+  *ldt = h->ldt;
   return HIPFT_OK;
 }
 

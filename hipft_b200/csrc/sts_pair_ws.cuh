@@ -96,6 +96,19 @@ __global__ void k_pair_tables(Mesh m, const double *__restrict__ dfac, int LR, i
   }
 }
 
+// Exercises the error path of the bounded waits: waits for phase 0 of an
+// mbarrier that expects one arrival nobody makes, gives up after `limit`
+// polls, sets the error flag and returns (no copy is in flight).
+__global__ void k_wait_selftest(uint32_t limit, int *err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (!mbar_wait_bounded(&bar, 0, limit) && threadIdx.x == 0) atomicExch(err, 1);
+}
+
 __device__ __forceinline__ void cons_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 // true on every consumer thread if p is true on any of them (named barrier 1)

@@ -122,6 +122,8 @@ SIGNATURES = [
                                      DPTR, DPTR, DPTR, DPTR]),
     ("hipft_gpu_set_flow_from_files", ctypes.c_int, [_H, DPTR, DPTR, ctypes.c_int]),
     ("hipft_gpu_set_allreduce", ctypes.c_int, [_H, ALLREDUCE_CB, ctypes.c_void_p]),
+    ("hipft_gpu_field_device_ptr", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int)]),
+    ("hipft_gpu_check_bounded_wait", ctypes.c_int, [_H, ctypes.c_uint]),
     ("hipft_run_shard", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(Shard), DPTR,
                                        ctypes.c_size_t]),
     ("hipft_gpu_set_source_file", ctypes.c_int, [_H, DPTR]),
@@ -282,6 +284,18 @@ class HipftGPU:
             out = np.empty((self.nr, self.npm, self.ntm))
         self._ck(self.L.hipft_gpu_get_field(self.h, _p(out)), "get_field")
         return out
+
+    def field_tensor(self):
+        """Zero-copy torch view (nr, npm, ldt) of the current field on the GPU
+        (theta padded to ldt); valid until the field next changes."""
+        import torch
+        ptr, ldt = ctypes.c_void_p(), ctypes.c_int()
+        self._ck(self.L.hipft_gpu_field_device_ptr(self.h, ctypes.byref(ptr), ctypes.byref(ldt)), "field_device_ptr")
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (self.nr, self.npm, ldt.value), "typestr": "<f8",
+                                        "data": (ptr.value, False), "version": 2}
+        return torch.as_tensor(_View(), device="cuda")
 
     def load_initial_map(self, map_pt: np.ndarray, flux_balance: bool = False, mult_fac: float = 1.0):
         """load_initial_condition's transpose/seam/pole steps (src/hipft.f90:2116-2172); map is (nr, ntm, npm1)."""

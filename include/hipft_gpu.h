@@ -264,6 +264,17 @@ int hipft_gpu_kernel_time(hipft_gpu *h, int kind, int64_t *launches, double *tot
 /* Runs subsequent work on a caller-owned cudaStream_t (NULL: the handle's). */
 int hipft_gpu_set_stream(hipft_gpu *h, void *cuda_stream);
 int hipft_gpu_synchronize(hipft_gpu *h);
+/* Zero-copy view of the current field for the PyTorch binding: the device
+ * address of f(j, k, i) at (*ptr)[(i-1)*npm*ldt + (k-1)*ldt + (j-1)] (theta
+ * padded to *ldt).  Valid until the next call that advances, assimilates or
+ * sets the field (the library rotates its buffers). */
+int hipft_gpu_field_device_ptr(hipft_gpu *h, double **ptr, int *ldt);
+/* No counterpart in the reference: a self-check of the error path that every
+ * bounded device wait of this library takes.  A kernel waits on an mbarrier
+ * that nothing completes, gives up after `limit` polls (1..2^22) and sets the
+ * handle's error flag; the call then returns HIPFT_ETIMEOUT, as a stalled
+ * copy would, and the handle stays usable. */
+int hipft_gpu_check_bounded_wait(hipft_gpu *h, unsigned int limit);
 
 /* ---- allocation-free flux integral ------------------------------------------ */
 
