@@ -247,10 +247,6 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     bool ok = true, dep_done = false;
     for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
       const int b = n % kWNB, u = n / kWNB;
-      if (u >= 1 && !mbar_wait_bounded(&empty[b], (uint32_t)((u - 1) & 1), 1u << 22)) {
-        ok = false;
-        break;
-      }
       const int kt = t % pt.nkt, rest = t / pt.nkt;
       // theta blocks in the order 1..nb-2, 0, nb-1: interior tiles first, so
       // that the wait for the previous pole kernel comes as late as possible
@@ -274,12 +270,26 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         asm volatile("griddepcontrol.wait;" ::: "memory");
         dep_done = true;
       }
+      // the tile record's global loads go out before the wait for the
+      // buffer, so their latency hides behind it
+      double rd = 0.0, rn = 0.0, rsv = 0.0;
+      if (lane == 0) {
+        rd = dfac[i];
+        if (dep_done) {  // used by pole tiles only
+          rn = ring_in[2 * (i - 1)] * bcn;
+          rsv = -ring_in[2 * (i - 1) + 1] * bcs;
+        }
+      }
+      if (u >= 1 && !mbar_wait_bounded(&empty[b], (uint32_t)((u - 1) & 1), 1u << 22)) {
+        ok = false;
+        break;
+      }
       if (lane == 0) {
         // the tile record, written before the arrival that releases it
         double *I = B + kWInfo;
-        I[0] = dfac[i];
-        I[1] = dep_done ? ring_in[2 * (i - 1)] * bcn : 0.0;  // used by pole tiles only
-        I[2] = dep_done ? -ring_in[2 * (i - 1) + 1] * bcs : 0.0;
+        I[0] = rd;
+        I[1] = rn;
+        I[2] = rsv;
         int *Ii = reinterpret_cast<int *>(I + 3);
         Ii[0] = kt;
         Ii[1] = rb;
