@@ -3,6 +3,7 @@
 // sequences the kernels of kernels.cuh the way HipFT's Fortran routines
 // sequence their do-concurrent loops (src/hipft.f90).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include <algorithm>
 #include <cfloat>
@@ -94,6 +95,14 @@ struct hipft_gpu {
   unsigned int *d_rcount = nullptr;
   int nkb = 0;
   PairTables ptab{};        // coefficient tables of the warp-specialised two-stage kernel
+  struct WsMapEntry {
+    const void *p;
+    int cols;
+    CUtensorMap m;
+  };
+  std::vector<WsMapEntry> ws_map_cache;  // tensor maps of the field buffers, by (pointer, box columns)
+  CUtensorMap ws_rt_map{};               // tensor map of ptab.row
+  bool ws_rt_ok = false;
   hipft_allreduce_cb red_cb = nullptr;  // scalar all-reduce over ranks (plain-mode sharding)
   void *red_user = nullptr;
   PoleScratch pole{};       // chunk shares of the ring sums for k_pair_poles
@@ -394,9 +403,10 @@ static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const
   return HIPFT_OK;
 }
 
-// Two RKG2 stages per launch: HIPFT_STS_PAIR=5 (default) persistent
-// warp-specialised CTAs with two theta rows per consumer thread
-// (k_sts_pair_ws<false, true>, then k_pair_poles), 4 the same with one row
+// Two RKG2 stages per launch: HIPFT_STS_PAIR=6 persistent warp-specialised
+// CTAs with two theta rows per consumer thread whose outputs leave by bulk
+// stores (k_sts_pair_ws<false, true, true>, then k_pair_poles), 5 (default)
+// the same with the consumers storing to global memory, 4 the same with one row
 // per consumer thread, 1 one CTA per
 // tile (k_sts_pair), 2 persistent double-buffered CTAs (k_sts_pair_p), 3 one
 // CTA per tile with row-marching arithmetic (k_sts_pair_march), 0 one stage
@@ -406,7 +416,7 @@ static int sts_pair_variant() {
   if (v < 0) {
     const char *e = std::getenv("HIPFT_STS_PAIR");
     v = e ? std::atoi(e) : 5;
-    if (v < 0 || v > 5) v = 5;
+    if (v < 0 || v > 6) v = 5;
   }
   return v;
 }
@@ -430,6 +440,80 @@ static bool ws_inline_poles() {
     v = (e && std::atoi(e) == 1) ? 1 : 0;
   }
   return v == 1;
+}
+
+// HIPFT_WS_TMAP=0 turns off the tensor-map tile loads of k_sts_pair_ws (one
+// bulk copy per column on every tile instead).
+static bool ws_tmap_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_WS_TMAP");
+    v = (e && std::atoi(e) == 0) ? 0 : 1;
+  }
+  return v == 1;
+}
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (no libcuda link)
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3-D f64 tensor map (dims d0 x d1 x d2, byte strides s1, s2 of dims 1, 2),
+// box b0 x b1 x 1, no swizzle, zero fill outside; false if the driver refuses
+// (e.g. a base address or stride that is not a multiple of 16 bytes)
+static bool encode_f64_3d(CUtensorMap *m, const void *base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t s1,
+                          uint64_t s2, uint32_t b0, uint32_t b1) {
+  PFN_cuTensorMapEncodeTiled_v12000 fn = tmap_encoder();
+  if (!fn) return false;
+  cuuint64_t dims[3] = {d0, d1, d2};
+  cuuint64_t strides[2] = {s1, s2};
+  cuuint32_t box[3] = {b0, b1, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// a field buffer's map with a box of kWR rows x cols columns (cached)
+static bool field_map(hipft_gpu *h, const double *p, int cols, CUtensorMap *out) {
+  for (const auto &e : h->ws_map_cache)
+    if (e.p == p && e.cols == cols) {
+      *out = e.m;
+      return true;
+    }
+  hipft_gpu::WsMapEntry e{};
+  e.p = p;
+  e.cols = cols;
+  if (!encode_f64_3d(&e.m, p, (uint64_t)h->ldt, (uint64_t)h->npm, (uint64_t)h->nr, (uint64_t)h->ldt * 8,
+                     (uint64_t)h->plane * 8, kWR, (uint32_t)cols))
+    return false;
+  h->ws_map_cache.push_back(e);
+  *out = e.m;
+  return true;
+}
+
+// the tensor maps of one k_sts_pair_ws launch; on = 0 (bulk copies per
+// column) when they are turned off or cannot be made
+static WsMaps ws_maps(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0) {
+  WsMaps tm;
+  std::memset(&tm, 0, sizeof(tm));
+  if (!ws_tmap_enabled() || !h->ws_rt_ok) return tm;
+  if (!field_map(h, ykm1, kWK + 4, &tm.x1) || !field_map(h, ykm2, kWK + 2, &tm.y2) ||
+      !field_map(h, u0, kWK + 2, &tm.u) || !field_map(h, dty0, kWK + 2, &tm.d))
+    return tm;
+  tm.rt = h->ws_rt_map;
+  tm.on = 1;
+  return tm;
 }
 
 // Tile shape of the two-stage kernel (theta rows x phi columns), picked by
@@ -508,10 +592,11 @@ static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const 
       const int grid = std::min(h->ptab.ntiles, 2 * h->num_sms);
       const PairArgs pa{ca, cb, h->d_err};
       const double *rin = h->d_ringbuf[h->ring_cur];
+      const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
       if (ws_inline_poles()) {
         k_sts_pair_ws<true><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
                                                                     out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
-                                                                    h->ptab);
+                                                                    h->ptab, tmaps);
       } else {
         // programmatic dependent launch: may overlap the previous pair's
         // k_pair_poles (the kernel's pole tiles wait for it)
@@ -526,12 +611,18 @@ static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const 
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         cudaError_t le;
-        if (sts_pair_variant() == 5)
+        // bulk stores need 16-byte aligned output columns (ldt and the
+        // plane are multiples of 16 elements)
+        const bool aligned = ((reinterpret_cast<uintptr_t>(out_k) | reinterpret_cast<uintptr_t>(out_k1)) & 15) == 0;
+        if (sts_pair_variant() == 6 && aligned)
+          le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true, true>, h->M, (const double *)h->DC.dfac, ykm1,
+                                  ykm2, u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+        else if (sts_pair_variant() >= 5)
           le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
-                                  dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab);
+                                  dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
         else
           le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, false>, h->M, (const double *)h->DC.dfac, ykm1, ykm2,
-                                  u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab);
+                                  u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
         if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
         LAUNCHED(h);
         dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
@@ -688,7 +779,9 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
       cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_sts_pair_ws<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
-          cudaSuccess)
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_ws<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kWSmem) != cudaSuccess)
     return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernels"));
   if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->num_sms < 1)
     h->num_sms = 148;
@@ -721,6 +814,8 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
     if ((rc = dalloc(h, &tab, nrow + ncol))) return bail(rc);
     pt.row = tab;
     pt.col = tab + nrow;
+    h->ws_rt_ok = encode_f64_3d(&h->ws_rt_map, pt.row, (uint64_t)pt.LR, 3, (uint64_t)nr, (uint64_t)pt.LR * 8,
+                                (uint64_t)pt.LR * 24, kWR, 3);
     k_pair_tables<<<2 * h->num_sms, 256, 0, h->stream>>>(h->M, d_dfac, pt.LR, pt.LC, tab, tab + nrow);
     h->launches++;
     if (cudaPeekAtLastError() != cudaSuccess) return bail(fail(h, HIPFT_ECUDA, "k_pair_tables launch failed"));

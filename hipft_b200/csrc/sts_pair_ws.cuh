@@ -6,9 +6,14 @@
 // busy while the SMs compute:
 //
 //  * one producer warp walks the CTA's tiles and fills a ring of two tile
-//    buffers with 1-D bulk copies (cp.async.bulk): Y_{k-1} on the tile plus a
-//    halo of 2, Y_{k-2}, u0 and dty0 plus a halo of 1, and the tile's rows and
-//    columns of two coefficient tables precomputed in HBM (k_pair_tables);
+//    buffers: Y_{k-1} on the tile plus a halo of 2, Y_{k-2}, u0 and dty0 plus
+//    a halo of 1, and the tile's rows and columns of two coefficient tables
+//    precomputed in HBM (k_pair_tables).  A tile whose halo columns need no
+//    phi wrap takes five 3-D tensor copies (cp.async.bulk.tensor, one box per
+//    array) and one bulk copy; the seam tiles take one 1-D bulk copy
+//    (cp.async.bulk) per column.  The number of copies per tile, not their
+//    bytes, had bounded the load rate: 46 copies per tile ran 20% slower per
+//    clock than 6;
 //    each buffer has a "full" mbarrier (copies landed) and an "empty" one (all
 //    consumers done reading it); every wait is bounded and reports through the
 //    error flag;
@@ -29,6 +34,8 @@
 // a launch of its own.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include "kernels.cuh"
 
 namespace hipft {
@@ -39,21 +46,34 @@ constexpr int kWR = kWJ + 4;              // shared rows per column (theta halo 
 constexpr int kWNB = 2;                   // tile buffers
 constexpr int kWCons = 256;               // consumer threads
 constexpr int kWThreads = kWCons + 32;    // + the producer warp
-// doubles, offsets within one tile buffer
-constexpr int kWX1 = 0;                        // Y_{k-1}: kWK+4 columns (shared columns 0..kWK+3)
-constexpr int kWY2 = kWX1 + (kWK + 4) * kWR;   // Y_{k-2}: kWK+2 columns (shared columns 1..kWK+2)
-constexpr int kWU = kWY2 + (kWK + 2) * kWR;    // u0
-constexpr int kWD = kWU + (kWK + 2) * kWR;     // dty0
-constexpr int kWRT = kWD + (kWK + 2) * kWR;    // rows: st_i, c2, c4, each kWR long
-constexpr int kWCT = kWRT + 3 * kWR;           // columns: {P1, P5} per shared column
-constexpr int kWInfo = kWCT + 2 * (kWK + 4);  // tile record: D, pole terms, (kt, rb, i)
-constexpr int kWBuf = kWInfo + 8;
-constexpr int kWYk = kWNB * kWBuf;             // Y_k: kWK+2 columns, consumers only
+// doubles, offsets within one tile buffer; the destinations of tensor copies
+// start on 128-byte boundaries
+constexpr int al16(int x) { return (x + 15) / 16 * 16; }
+constexpr int kWX1 = 0;                             // Y_{k-1}: kWK+4 columns (shared columns 0..kWK+3)
+constexpr int kWY2 = al16(kWX1 + (kWK + 4) * kWR);  // Y_{k-2}: kWK+2 columns (shared columns 1..kWK+2)
+constexpr int kWU = al16(kWY2 + (kWK + 2) * kWR);   // u0
+constexpr int kWD = al16(kWU + (kWK + 2) * kWR);    // dty0
+constexpr int kWRT = al16(kWD + (kWK + 2) * kWR);   // rows: st_i, c2, c4, each kWR long
+constexpr int kWCT = kWRT + 3 * kWR;                // columns: {P1, P5} per shared column
+constexpr int kWInfo = kWCT + 2 * (kWK + 4);       // tile record: D, pole terms, (kt, rb, i)
+constexpr int kWBuf = al16(kWInfo + 8);
+constexpr int kWYk = kWNB * kWBuf;                  // Y_k: kWK+2 columns, consumers only
 constexpr int kWEnd = kWYk + (kWK + 2) * kWR;
 constexpr size_t kWSmem = (size_t)kWEnd * sizeof(double) + 2 * kWNB * sizeof(uint64_t);
-static_assert(kWX1 % 2 == 0 && kWY2 % 2 == 0 && kWU % 2 == 0 && kWD % 2 == 0 && kWRT % 2 == 0 &&
-                  kWCT % 2 == 0 && kWBuf % 2 == 0 && kWYk % 2 == 0 && kWEnd % 2 == 0,
-              "every bulk-copy destination must be 16-byte aligned");
+static_assert(kWX1 % 16 == 0 && kWY2 % 16 == 0 && kWU % 16 == 0 && kWD % 16 == 0 && kWRT % 16 == 0 &&
+                  kWCT % 2 == 0 && kWBuf % 16 == 0 && kWYk % 2 == 0 && kWEnd % 2 == 0,
+              "tensor-copy destinations 128-byte aligned, bulk-copy destinations 16-byte aligned");
+static_assert(2 * (kWSmem + 1024 + 256) <= 228 * 1024, "two CTAs per SM");
+
+// Tensor maps of the tile loads (3-D: theta row, phi column, realization;
+// f64, no swizzle, zero fill outside): x1 with a box of kWR x (kWK+4) x 1,
+// y2, u and d with kWR x (kWK+2) x 1, and the row table ([nr][3][LR]) with
+// kWR x 3 x 1.  With `on` set, a tile whose halo columns need no phi wrap
+// takes five tensor copies instead of one bulk copy per column.
+struct WsMaps {
+  CUtensorMap x1, y2, u, d, rt;
+  int on;
+};
 static_assert((kWR * 8) % 16 == 0, "column stride must keep 16-byte alignment");
 
 // Coefficient tables of the two-stage kernels, in load_diffusion_matrix's
@@ -212,7 +232,48 @@ __device__ __forceinline__ void store_pair(double *g, double2 y, bool va, bool v
   }
 }
 
-template <bool INLINE_POLES, bool ROWPAIRS = false>
+// Tile t of a launch: phi tile kt, theta block rb, realization i.  Theta
+// blocks go in the order 1..nb-2, 0, nb-1: interior tiles first, so that the
+// wait for the previous pole kernel comes as late as possible.
+__device__ __forceinline__ void ws_tile(const PairTables &pt, int t, int &kt, int &rb, int &i) {
+  kt = t % pt.nkt;
+  const int rest = t / pt.nkt;
+  const int q = rest % pt.nb;
+  i = rest / pt.nb + 1;
+  rb = (pt.nb <= 2) ? q : ((q < pt.nb - 2) ? q + 1 : ((q == pt.nb - 2) ? 0 : pt.nb - 1));
+}
+
+// Bulk stores of one tile column set: lane q < kWK writes column k0+q (theta
+// rows j0..j0+kWJ-1, kWJ*8 bytes) from src0 + q*kWR; lanes kWK and kWK+1 write
+// the seam columns (npm duplicates column 2, column 1 duplicates npm-1).
+// Each issuing lane commits its own bulk async-group.
+__device__ __forceinline__ void ws_store_cols(double *out, int64_t pbase, int k0, int j0, const double *src0, int lane,
+                                              int npm, int64_t ld) {
+  int c = -1, kg = 0;
+  if (lane < kWK) {
+    c = lane;
+    kg = k0 + lane;
+  } else if (lane == kWK && k0 == 2) {
+    c = 0;
+    kg = npm;
+  } else if (lane == kWK + 1 && k0 + kWK - 1 == npm - 1) {
+    c = kWK - 1;
+    kg = 1;
+  }
+  if (c >= 0) {
+    bulk_store(out + pbase + (int64_t)(kg - 1) * ld + (j0 - 1), src0 + c * kWR, kWJ * 8u);
+    bulk_commit();
+  }
+}
+
+// BULKST (with ROWPAIRS and a separate pole kernel): on tiles of kWK full
+// columns and kWJ rows inside 1..ntm, Y_k goes to HBM by bulk stores from
+// its shared array and Y_{k+1} by bulk stores from the tile buffer's Y_{k-2}
+// region (free after stage k), issued by the producer when the consumers
+// release the buffer; no consumer thread stores to global memory there.
+// Those stores also write the pole rows 1 / ntm of Y_{k+1} with unused
+// values; k_pair_poles, launched after this kernel, overwrites them.
+template <bool INLINE_POLES, bool ROWPAIRS = false, bool BULKST = false>
 __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const double *__restrict__ dfac,
                                                              const double *__restrict__ ykm1,
                                                              const double *__restrict__ ykm2,
@@ -220,13 +281,14 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
                                                              const double *__restrict__ dty0, double *out_k,
                                                              double *out_k1, const double *__restrict__ ring_in,
                                                              double bcn, double bcs, PairArgs pa, RingOut ro,
-                                                             PairTables pt) {
+                                                             PairTables pt, const __grid_constant__ WsMaps tm) {
   extern __shared__ __align__(128) double wsm[];
   uint64_t *full = reinterpret_cast<uint64_t *>(wsm + kWEnd);
   uint64_t *empty = full + kWNB;
   __shared__ double red[16];
   __shared__ double s_ring[2];
   __shared__ int s_last;
+  static_assert(!BULKST || (ROWPAIRS && !INLINE_POLES), "bulk stores need the row-pair consumers and k_pair_poles");
 
   const int tid = threadIdx.x;
   const int ntm = m.ntm, npm = m.npm;
@@ -245,13 +307,18 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     const int lane = tid - kWCons;
     int n = 0;
     bool ok = true, dep_done = false;
+    const bool maps_ok = tm.on && (smem_addr(wsm) & 127u) == 0;
+    auto store_prev_k1 = [&](int tp, const double *Bp) {
+      int ktp, rbp, ip;
+      ws_tile(pt, tp, ktp, rbp, ip);
+      const int j0p = rbp * kWJ + 1, k0p = ktp * kWK + 2;
+      if (k0p + kWK - 1 <= npm - 1 && j0p + kWJ - 1 <= ntm)
+        ws_store_cols(out_k1, (int64_t)(ip - 1) * m.plane, k0p, j0p, Bp + kWY2, lane, npm, ld);
+    };
     for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
       const int b = n % kWNB, u = n / kWNB;
-      const int kt = t % pt.nkt, rest = t / pt.nkt;
-      // theta blocks in the order 1..nb-2, 0, nb-1: interior tiles first, so
-      // that the wait for the previous pole kernel comes as late as possible
-      const int q = rest % pt.nb, i = rest / pt.nb + 1;
-      const int rb = (pt.nb <= 2) ? q : ((q < pt.nb - 2) ? q + 1 : ((q == pt.nb - 2) ? 0 : pt.nb - 1));
+      int kt, rb, i;
+      ws_tile(pt, t, kt, rb, i);
       const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
       const int nk = min(kWK, npm - 1 - k0 + 1);
       const int rs = max(1, j0 - 2), re = min((int)ld, j0 + kWJ + 1);
@@ -260,6 +327,8 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       const int64_t pbase = (int64_t)(i - 1) * m.plane;
       double *B = wsm + b * kWBuf;
       const int nx = nk + 4, ny = nk + 2, ncp = nx + 3 * ny + 4;
+      // tensor copies when every halo column lies in 1..npm (no phi wrap)
+      const bool boxed = maps_ok && nk == kWK && k0 - 2 >= 1 && k0 + kWK + 1 <= npm;
       // Launched programmatically after the previous pair's k_pair_poles,
       // this kernel may start while that one still runs; it reads and writes
       // the pole rows 1, ntm, the rows 2, ntm-1 next to them and the ring
@@ -284,6 +353,13 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         ok = false;
         break;
       }
+      if (BULKST && u >= 1) {
+        // Y_{k+1} of the tile that used this buffer before, from its
+        // Y_{k-2} region; read out before the buffer is refilled
+        store_prev_k1(t - kWNB * (int)gridDim.x, B);
+        bulk_wait_read();
+        __syncwarp();
+      }
       if (lane == 0) {
         // the tile record, written before the arrival that releases it
         double *I = B + kWInfo;
@@ -294,10 +370,24 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         Ii[0] = kt;
         Ii[1] = rb;
         Ii[2] = i;
-        mbar_expect_tx(&full[b], (uint32_t)(nx + 3 * ny) * run + (uint32_t)(3 * kWR * 8 + (kWK + 4) * 16));
+        if (boxed) {
+          // five tensor copies (halo rows outside the field read as zeros;
+          // x = j0-3 keeps the innermost offset a multiple of 16 bytes) and
+          // the column table
+          mbar_expect_tx(&full[b], (uint32_t)((nx + 3 * ny) * kWR * 8 + 3 * kWR * 8 + (kWK + 4) * 16));
+          tma_load_3d(B + kWX1, &tm.x1, j0 - 3, k0 - 3, i - 1, &full[b]);
+          tma_load_3d(B + kWY2, &tm.y2, j0 - 3, k0 - 2, i - 1, &full[b]);
+          tma_load_3d(B + kWU, &tm.u, j0 - 3, k0 - 2, i - 1, &full[b]);
+          tma_load_3d(B + kWD, &tm.d, j0 - 3, k0 - 2, i - 1, &full[b]);
+          tma_load_3d(B + kWRT, &tm.rt, rb * kWJ, 0, i - 1, &full[b]);
+          bulk_load(B + kWCT, pt.col + ((int64_t)(i - 1) * pt.LC + (int64_t)kt * kWK) * 2, (kWK + 4) * 16,
+                    &full[b]);
+        } else {
+          mbar_expect_tx(&full[b], (uint32_t)(nx + 3 * ny) * run + (uint32_t)(3 * kWR * 8 + (kWK + 4) * 16));
+        }
       }
       __syncwarp();
-      for (int q = lane; q < ncp; q += 32) {
+      for (int q = lane; q < (boxed ? 0 : ncp); q += 32) {
         const double *src;
         double *dst;
         uint32_t bytes = run;
@@ -324,6 +414,18 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         bulk_load(dst, src, bytes, &full[b]);
       }
     }
+    if (BULKST && ok) {
+      // Y_{k+1} of the last tile of each buffer, once the consumers are done
+      for (int nn = max(0, n - kWNB); nn < n; ++nn) {
+        const int bb = nn % kWNB;
+        if (!mbar_wait_bounded(&empty[bb], (uint32_t)((nn / kWNB) & 1), 1u << 22)) {
+          ok = false;
+          break;
+        }
+        store_prev_k1(blockIdx.x + nn * (int)gridDim.x, wsm + bb * kWBuf);
+      }
+    }
+    if (BULKST) bulk_wait_all();
     if (!ok && lane == 0) atomicExch(pa.err, 1);
     // every issued copy lands before this warp exits (tiles 0..n-1 were issued)
     for (int b = 0; b < kWNB; ++b) {
@@ -345,13 +447,15 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
   for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
     const int b = n % kWNB, u = n / kWNB;
     const bool landed = mbar_wait_bounded(&full[b], (uint32_t)(u & 1), 1u << 22);
+    if (BULKST && w == 0) bulk_wait_read();  // the previous tile's Y_k stores have read sYk
     // one vote: every consumer stops together; also orders the previous
     // tile's reads of sYk before this tile's writes
     if (cons_any(!landed)) {
       if (tid == 0) atomicExch(pa.err, 1);
       break;
     }
-    const double *B = wsm + b * kWBuf;
+    double *Bw = wsm + b * kWBuf;
+    const double *B = Bw;
     const double Dr = B[kWInfo], ax_n = B[kWInfo + 1], ax_s = B[kWInfo + 2];
     const int *Ii = reinterpret_cast<const int *>(B + kWInfo + 3);
     const int kt = Ii[0], rb = Ii[1], i = Ii[2];
@@ -361,6 +465,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     const double *X1 = B + kWX1, *Y2 = B + kWY2, *U = B + kWU, *D = B + kWD, *RT = B + kWRT;
     const double2 *CT = reinterpret_cast<const double2 *>(B + kWCT);
     const int64_t seam = (int64_t)(npm - 2) * ld;
+    const bool bulk = BULKST && nk == kWK && j0 + kWJ - 1 <= ntm;
 
     // ---------------------------------------------- stage k: Y_k into sYk
     if (ROWPAIRS && nk == kWK) {
@@ -386,7 +491,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       };
       auto put = [&](int r0, int c, double2 y) {
         *reinterpret_cast<double2 *>(sYk + (c - 1) * kWR + r0) = y;
-        if (c >= 2 && c <= kWK + 1 && r0 >= 2 && r0 <= kWJ) {
+        if (!bulk && c >= 2 && c <= kWK + 1 && r0 >= 2 && r0 <= kWJ) {
           const int ja = j0 - 2 + r0, k = k0 - 2 + c;
           const bool va = (ja >= 1 && ja <= ntm), vb = (ja + 1 >= 1 && ja + 1 <= ntm);
           const int64_t so = (k == 2) ? seam : ((k == npm - 1) ? -seam : 0);
@@ -535,7 +640,10 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         }
       }
     }
+    if (bulk) fence_proxy_async_smem();  // sYk, as written, for the bulk stores
     cons_sync();
+    if (bulk && w == 0)  // Y_k rows j0..j0+kWJ-1 are shared rows 2..kWJ+1
+      ws_store_cols(out_k, pbase, k0, j0, sYk + kWR + 2, lane, npm, ld);
 
     // ---- ring partials of Y_k over this tile's columns (fixed tree over columns)
     const bool has_n = (j0 == 1);
@@ -578,11 +686,20 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         xl = xc;
         xc = xr;
       }
+      if (bulk) {
+        // staged in the Y_{k-2} region (column c at (c-2)*kWR, row j at
+        // j-j0) for the producer's bulk stores; fenced before the release
 #pragma unroll
-      for (int s = 0; s < 2; ++s) {
-        const int k = k0 - 2 + cb + s;
-        const int64_t so = (k == 2) ? seam : ((k == npm - 1) ? -seam : 0);
-        store_pair(out_k1 + pbase + (int64_t)(k - 1) * ld + (ja - 1), y[s], va, vb, so);
+        for (int s = 0; s < 2; ++s)
+          *reinterpret_cast<double2 *>(Bw + kWY2 + (cb + s - 2) * kWR + (r0 - 2)) = y[s];
+        fence_proxy_async_smem();
+      } else {
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+          const int k = k0 - 2 + cb + s;
+          const int64_t so = (k == 2) ? seam : ((k == npm - 1) ? -seam : 0);
+          store_pair(out_k1 + pbase + (int64_t)(k - 1) * ld + (ja - 1), y[s], va, vb, so);
+        }
       }
     } else if (nk == kWK) {
       const int r = r3, j = j0 - 2 + r;
@@ -688,6 +805,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       }
     }
   }
+  if (BULKST && w == 0) bulk_wait_all();  // this warp's Y_k stores, before the CTA exits
 }
 
 // Pole rows of Y_{k+1} and the ring sums of Y_{k+1}, after

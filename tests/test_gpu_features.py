@@ -36,6 +36,11 @@ CASES = {
                              validation_run=1),
     "rkg2_ntm130_np96": dict(res_nt=130, res_np=96, advance_diffusion=True, diffusion_coef_constants=[80.0, 700.0],
                              validation_run=1),
+    # three full 128-row blocks (north pole, interior, south pole) and full
+    # phi tiles at both seams: every tile of the two-stage kernel takes its
+    # widest path
+    "rkg2_ntm384_np45": dict(res_nt=384, res_np=45, advance_diffusion=True, diffusion_coef_constants=[150.0, 900.0],
+                             validation_run=1),
     "rkl2_fixed_sc": dict(advance_diffusion=True, diffusion_num_method=2, diffusion_subcycles=3,
                           diffusion_coef_constants=[250.0, 500.0], validation_run=1),
     "euler_fixed_sc": dict(res_nt=20, res_np=37, advance_diffusion=True, diffusion_num_method=1,

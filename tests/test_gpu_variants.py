@@ -3,7 +3,9 @@
 The library picks its RKG2 stage kernel from the environment at first use
 (HIPFT_STS_PAIR=1: two stages per launch with TMA-staged tiles; =2: the same,
 persistent and double-buffered; =3: row-marching arithmetic; =4: persistent
-with a producer warp and a two-buffer pipeline; =0: one stage per launch, two
+with a producer warp and a two-buffer pipeline; =5: the same with two theta
+rows per consumer thread; =6: the same with the outputs leaving by bulk
+stores; =0: one stage per launch, two
 theta rows per thread, or one row per thread with HIPFT_STS_KERNEL=2), so each variant runs the
 standalone driver in a fresh subprocess; final fields must match the oracle
 to FIELD_TOL."""
@@ -25,11 +27,11 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "pair_persistent": {"HIPFT_STS_PAIR": "2"},
             "pair_64x16": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "64x16"}, "pair_march": {"HIPFT_STS_PAIR": "3"},
             "pair_ws": {"HIPFT_STS_PAIR": "4"}, "pair_ws_inline": {"HIPFT_STS_PAIR": "4", "HIPFT_WS_POLES": "1"},
-            "pair_ws_rowpairs": {"HIPFT_STS_PAIR": "5"},
+            "pair_ws_rowpairs": {"HIPFT_STS_PAIR": "5"}, "pair_ws_bulkst": {"HIPFT_STS_PAIR": "6"},
             "pair_256x4": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "256x4"},
             "single_v3": {"HIPFT_STS_PAIR": "0"}, "single_v2": {"HIPFT_STS_PAIR": "0", "HIPFT_STS_KERNEL": "2"}}
 RUNS = ["diffuse_soccer", "rkg2_auto_ntm33", "rkg2_auto_ntm161", "rkg2_ntm129_np65", "rkg2_ntm130_np96",
-        "strang_dr_mf_diff"]
+        "rkg2_ntm384_np45", "strang_dr_mf_diff"]
 
 
 def _setup(name, tmp_path):
