@@ -1,0 +1,312 @@
+// adjoint.cuh -- discrete adjoint (vector-Jacobian products) of the
+// flux-transport step's two operators, for gradients of a map misfit with
+// respect to the initial map, the diffusion coefficient and the analytic flow
+// profiles (no reference counterpart; the forward operators are
+// diffusion_operator_cd, src/hipft.f90:7927-7990, and
+// advection_operator_weno3, src/hipft.f90:7711-7925).
+//
+// Cotangent fields are "folded": their phi seam columns 1 and npm hold zero,
+// and the dependence of a forward field's seam columns (copies of columns
+// npm-1 and 2) is carried by the columns they copy.  Every kernel here reads
+// and writes core columns 2..npm-1 only.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace hipft {
+
+// neighbour of core column k on the periodic core ring 2..npm-1
+__device__ __forceinline__ int core_wrap(const Mesh &m, int k) {
+  if (k < 2) return k + (m.npm - 2);
+  if (k > m.npm - 1) return k - (m.npm - 2);
+  return k;
+}
+
+// Sums of a folded field over the core columns of the pole rows, one block
+// per realization: g[2(i-1)] = sum_k w(1,k), g[2(i-1)+1] = sum_k w(ntm,k).
+__global__ void k_adj_pole_sums(Mesh m, const double *__restrict__ w, double *__restrict__ g) {
+  __shared__ double sh[64];
+  const int i = blockIdx.x + 1;
+  double a = 0.0, b = 0.0;
+  for (int k = 2 + threadIdx.x; k <= m.npm - 1; k += blockDim.x) {
+    a = a + w[fidx(m, 1, k, i)];
+    b = b + w[fidx(m, m.ntm, k, i)];
+  }
+  block_sum2(a, b, sh);
+  if (threadIdx.x == 0) {
+    g[2 * (i - 1)] = a;
+    g[2 * (i - 1) + 1] = b;
+  }
+}
+
+// (A^T w)(j,k) at core cell (j,k) for the diffusion operator with its pole
+// rows and periodic seam; gn, gs are w's pole sums.  Each term is one output
+// of A that reads x(j,k): (j,k) [c3], (j,k+1) [c1], (j,k-1) [c5], (j+1,k)
+// [c2], (j-1,k) [c4], and the pole rows through the ring sums.
+__device__ __forceinline__ double adj_diff_at(const Mesh &m, const DiffCoef &dc, const double *__restrict__ w, int j,
+                                              int k, int i, double gn, double gs, double bcn, double bcs) {
+  const int ntm = m.ntm;
+  double r = 0.0;
+  if (j >= 2 && j <= ntm - 1) {
+    const int kp = core_wrap(m, k + 1), km = core_wrap(m, k - 1);
+    r += coef5(m, dc, j, k, i).c3 * w[fidx(m, j, k, i)];
+    r += coef5(m, dc, j, kp, i).c1 * w[fidx(m, j, kp, i)];
+    r += coef5(m, dc, j, km, i).c5 * w[fidx(m, j, km, i)];
+    if (j + 1 <= ntm - 1) r += coef5(m, dc, j + 1, k, i).c2 * w[fidx(m, j + 1, k, i)];
+    if (j - 1 >= 2) r += coef5(m, dc, j - 1, k, i).c4 * w[fidx(m, j - 1, k, i)];
+    if (j == 2) r += (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
+    if (j == ntm - 1) r += (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
+  } else if (j == 1) {
+    r += coef5(m, dc, 2, k, i).c2 * w[fidx(m, 2, k, i)];
+    r -= (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
+  } else {
+    r += coef5(m, dc, ntm - 1, k, i).c4 * w[fidx(m, ntm - 1, k, i)];
+    r -= (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
+  }
+  return r;
+}
+
+// One reverse RKG2 stage (or a plain A^T application), per core cell:
+//   out = a*w + b*wp + c*(A^T w);   ub += c0*w;   db += g*w;
+// and per block the sum of (A^T w)*y (the diffusion-coefficient term),
+// written to dpart[block] for k_adj_dsum.  wp, y, ub, db may be null.
+// out may alias wp (each cell reads wp before writing out).
+struct AdjDiffCoef {
+  double a, b, c, c0, g;
+};
+
+__global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const double *__restrict__ w, const double *wp,
+                                                  const double *__restrict__ y, double *out, double *ub, double *db,
+                                                  const double *__restrict__ gring, double bcn, double bcs,
+                                                  AdjDiffCoef ac, double *__restrict__ dpart) {
+  __shared__ double sh[64];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  double dsum = 0.0;
+  if (j <= m.ntm && k <= m.npm - 1) {
+    const int64_t q = fidx(m, j, k, i);
+    const double aw = adj_diff_at(m, dc, w, j, k, i, gring[2 * (i - 1)], gring[2 * (i - 1) + 1], bcn, bcs);
+    const double wq = w[q];
+    double o = ac.a * wq + ac.c * aw;
+    if (wp) o += ac.b * wp[q];
+    out[q] = o;
+    if (ub) ub[q] += ac.c0 * wq;
+    if (db) db[q] += ac.g * wq;
+    if (y) dsum = aw * y[q];
+  }
+  if (dpart) {
+    double z = 0.0;
+    block_sum2(dsum, z, sh);
+    if (threadIdx.x == 0 && threadIdx.y == 0)
+      dpart[((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = dsum;
+  }
+}
+
+// dacc[i] += scale * (sum of realization i's block partials), fixed order.
+__global__ void k_adj_dsum(const double *__restrict__ dpart, int nblk, double scale, double *dacc) {
+  __shared__ double sh[64];
+  const int i = blockIdx.x;
+  double a = 0.0, b = 0.0;
+  for (int q = threadIdx.x; q < nblk; q += blockDim.x) a = a + dpart[(int64_t)i * nblk + q];
+  block_sum2(a, b, sh);
+  if (threadIdx.x == 0) dacc[i] += scale * a;
+}
+
+// y += a*x1 + b*x2 on core cells (x2 may be null)
+__global__ void k_adj_axpy2(Mesh m, double *y, double a, const double *__restrict__ x1, double b,
+                            const double *__restrict__ x2) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm - 1) return;
+  const int64_t q = fidx(m, j, k, i);
+  double v = y[q] + a * x1[q];
+  if (x2) v += b * x2[q];
+  y[q] = v;
+}
+
+// Partial derivatives of weno_face (kernels.cuh) with respect to its six
+// inputs LN(j-2), LN(j-1), LN(j), LP(j-1), LP(j), LP(j+1): d[0..5].  The
+// nonlinear weights are differentiated through: with w = D/(eps+4t^2)^2,
+// d(sum OM*p)/dt = -16 OM (p - u) t / (eps + 4t^2) for each candidate.
+__device__ __forceinline__ void weno_face_vjp(double LNm2, double LNm1, double LN0, double LPm1, double LP0,
+                                              double LPp1, double DCMC_m1, double DCMC_0, double DCCP_m1,
+                                              double DCCP_0, double DPT_m1, double DMCT_m1, double DMT_0,
+                                              double DCPT_0, double eps_m1, double eps_0, double d[6]) {
+  // minus side
+  const double p0m = (kOne + DCMC_m1) * LNm1 - DCMC_m1 * LNm2;
+  const double p1m = DCMC_0 * LNm1 + DCCP_m1 * LN0;
+  const double t0 = DCMC_m1 * (LNm1 - LNm2), t1 = DCCP_m1 * (LN0 - LNm1);
+  const double e0 = eps_m1 + kFour * (t0 * t0), e1 = eps_m1 + kFour * (t1 * t1);
+  const double w0m = DPT_m1 / (e0 * e0), w1m = DMCT_m1 / (e1 * e1);
+  const double sm = w0m + w1m;
+  const double O0m = w0m / sm, O1m = w1m / sm;
+  const double um = O0m * p0m + O1m * p1m;
+  const double dt0 = -16.0 * O0m * (p0m - um) * t0 / e0;
+  const double dt1 = -16.0 * O1m * (p1m - um) * t1 / e1;
+  d[0] = -DCMC_m1 * O0m - DCMC_m1 * dt0;
+  d[1] = (kOne + DCMC_m1) * O0m + DCMC_0 * O1m + DCMC_m1 * dt0 - DCCP_m1 * dt1;
+  d[2] = DCCP_m1 * O1m + DCCP_m1 * dt1;
+  // plus side
+  const double p0p = (kOne + DCCP_0) * LP0 - DCCP_0 * LPp1;
+  const double p1p = DCCP_m1 * LP0 + DCMC_0 * LPm1;
+  const double t2 = DCCP_0 * (LPp1 - LP0), t3 = DCMC_0 * (LP0 - LPm1);
+  const double e2 = eps_0 + kFour * (t2 * t2), e3 = eps_0 + kFour * (t3 * t3);
+  const double w0p = DMT_0 / (e2 * e2), w1p = DCPT_0 / (e3 * e3);
+  const double sp = w0p + w1p;
+  const double O0p = w0p / sp, O1p = w1p / sp;
+  const double up = O0p * p0p + O1p * p1p;
+  const double dt2 = -16.0 * O0p * (p0p - up) * t2 / e2;
+  const double dt3 = -16.0 * O1p * (p1p - up) * t3 / e3;
+  d[3] = DCMC_0 * O1p - DCMC_0 * dt3;
+  d[4] = (kOne + DCCP_0) * O0p + DCCP_m1 * O1p - DCCP_0 * dt2 + DCMC_0 * dt3;
+  d[5] = -DCCP_0 * O0p + DCCP_0 * dt2;
+}
+
+// Reverse of one explicit advection stage at core cell (j,k):
+//   out = alpha*w + beta*base + L_x^T(sigma*w)
+// where L is advection_operator_weno3 linearised at x (analytic 1-D flows,
+// WENO3 faces, upwind faces next to the poles, pole rings, periodic seam).
+// gring holds w's pole sums.  The flow cotangents are accumulated per cell:
+//   gln_t += LNbar*x/2 (for vt(j)+at(j)),  glp_t += LPbar*x/2 (vt(j+1)-at(j)),
+//   gup_t += the upwind faces' vt cotangent (face j), and the same for phi
+//   (gln_p, glp_p: vp(j) + ap(j), vp(j) - ap(j)).
+struct AdjAdvArgs {
+  double sigma, alpha, beta, bcfn, bcfs;
+};
+
+__global__ void __launch_bounds__(256) k_adj_adv(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
+                                                 const double *__restrict__ w, const double *__restrict__ base,
+                                                 double *__restrict__ out, const double *__restrict__ gring,
+                                                 AdjAdvArgs a, double *gln_t, double *glp_t, double *gup_t,
+                                                 double *gln_p, double *glp_p) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  const int ntm = m.ntm, npm = m.npm;
+  if (j > ntm || k > npm - 1) return;
+  const double gn = a.sigma * gring[2 * (i - 1)], gs = a.sigma * gring[2 * (i - 1) + 1];
+  auto abar = [&](int jj, int kk) { return a.sigma * w[fidx(m, jj, kk, i)]; };
+  auto X = [&](int jj, int kk) { return x[fidx(m, jj, kk, i)]; };
+
+  // ---- theta faces jf = j-1 .. j+2 of column k
+  // cotangent of flux_t(jf,k): divergence of cells jf-1 and jf, pole rings
+  auto ftbar = [&](int jf) {
+    double v = 0.0;
+    if (jf - 1 >= 2 && jf - 1 <= ntm - 1) v += abar(jf - 1, k) * m.sth[jf] * m.st_i[jf - 1] * m.dt_i[jf - 1];
+    if (jf >= 2 && jf <= ntm - 1) v -= abar(jf, k) * m.sth[jf] * m.st_i[jf] * m.dt_i[jf];
+    if (jf == 2) v += a.bcfn * m.dp[k] * gn;
+    if (jf == ntm) v -= a.bcfs * m.dp[k] * gs;
+    return v;
+  };
+  double lnb = 0.0, lpb = 0.0, xb = 0.0, upv = 0.0;
+  for (int jf = j - 1; jf <= j + 2; ++jf) {
+    if (jf < 2 || jf > ntm) continue;
+    const double Fb = ftbar(jf);
+    if (Fb == 0.0) continue;
+    if (jf == 2 || jf == ntm) {  // upwind face: x(jf) high side, x(jf-1) low side
+      const double v = vt_at(m, fl, jf, k, i), cct = copysign(fl.upwind, v);
+      if (j == jf) {
+        xb += Fb * v * kHalf * (kOne - cct);
+        upv += Fb * kHalf * ((kOne - cct) * X(jf, k) + (kOne + cct) * X(jf - 1, k));
+      }
+      if (j == jf - 1) xb += Fb * v * kHalf * (kOne + cct);
+    } else {
+      double LN[3], LP[3], d[6];
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        const int c = jf - 2 + e;
+        LN[e] = kHalf * X(c, k) * (vt_at(m, fl, c, k, i) + at_at(m, fl, c, k, i));
+      }
+#pragma unroll
+      for (int e = 0; e < 3; ++e) {
+        const int c = jf - 1 + e;
+        LP[e] = kHalf * X(c, k) * (vt_at(m, fl, c + 1, k, i) - at_at(m, fl, c, k, i));
+      }
+      weno_face_vjp(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mct[jf - 1], wn.mct[jf], wn.cpt[jf - 1],
+                    wn.cpt[jf], wn.pt[jf - 1], wn.mctt[jf - 1], wn.mt[jf], wn.cptt[jf], wn.epst[jf - 1],
+                    wn.epst[jf], d);
+      const int pos = j - jf;  // -2, -1, 0, 1
+      if (pos == -2) lnb += Fb * d[0];
+      if (pos == -1) {
+        lnb += Fb * d[1];
+        lpb += Fb * d[3];
+      }
+      if (pos == 0) {
+        lnb += Fb * d[2];
+        lpb += Fb * d[4];
+      }
+      if (pos == 1) lpb += Fb * d[5];
+    }
+  }
+  const double xj = X(j, k);
+  xb += lnb * kHalf * (vt_at(m, fl, j, k, i) + at_at(m, fl, j, k, i)) +
+        lpb * kHalf * (vt_at(m, fl, j + 1, k, i) - at_at(m, fl, j, k, i));
+  const int64_t q = fidx(m, j, k, i);
+  gln_t[q] += lnb * kHalf * xj;
+  glp_t[q] += lpb * kHalf * xj;
+  gup_t[q] += upv;
+
+  // ---- phi faces (interior rows): core faces kf = 2..npm-1, face npm is
+  // the seam copy of face 2; cell index c' of the padded row (0..npm)
+  // aliases core cell k when c' = k, or c' = 0 (k = npm-2), 1 (k = npm-1),
+  // npm (k = 2)
+  if (j >= 2 && j <= ntm - 1) {
+    auto fpbar = [&](int kf) {
+      double v = 0.0;
+      if (kf >= 3) v += abar(j, kf - 1) * m.st_i[j] * m.dp_i[kf - 1];
+      else v += abar(j, npm - 1) * m.st_i[j] * m.dp_i[npm - 1];
+      v -= abar(j, kf) * m.st_i[j] * m.dp_i[kf];
+      return v;
+    };
+    double lnbp = 0.0, lpbp = 0.0;
+    int alias[4], na = 0;
+    alias[na++] = k;
+    if (k == npm - 2) alias[na++] = 0;
+    if (k == npm - 1) alias[na++] = 1;
+    if (k == 2) alias[na++] = npm;
+    for (int ai = 0; ai < na; ++ai) {
+      const int cp = alias[ai];
+      for (int kf = cp - 1; kf <= cp + 2; ++kf) {
+        if (kf < 2 || kf > npm - 1) continue;
+        const double Fb = fpbar(kf);
+        if (Fb == 0.0) continue;
+        double LN[3], LP[3], d[6];
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const int c = wrap_cell(m, kf - 2 + e);
+          LN[e] = kHalf * X(j, c) * (vp_at(m, fl, j, c, i) + ap_at(m, fl, j, c, i));
+        }
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+          const int c = wrap_cell(m, kf - 1 + e);
+          LP[e] = kHalf * X(j, c) * (vp_at(m, fl, j, c + 1, i) - ap_at(m, fl, j, c, i));
+        }
+        weno_face_vjp(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mcp[kf - 1], wn.mcp[kf], wn.cpp[kf - 1],
+                      wn.cpp[kf], wn.pp[kf - 1], wn.mctp[kf - 1], wn.mp[kf], wn.cptp[kf], wn.epsp[kf - 1],
+                      wn.epsp[kf], d);
+        const int pos = cp - kf;
+        if (pos == -2) lnbp += Fb * d[0];
+        if (pos == -1) {
+          lnbp += Fb * d[1];
+          lpbp += Fb * d[3];
+        }
+        if (pos == 0) {
+          lnbp += Fb * d[2];
+          lpbp += Fb * d[4];
+        }
+        if (pos == 1) lpbp += Fb * d[5];
+      }
+    }
+    xb += lnbp * kHalf * (vp_at(m, fl, j, k, i) + ap_at(m, fl, j, k, i)) +
+          lpbp * kHalf * (vp_at(m, fl, j, k + 1, i) - ap_at(m, fl, j, k, i));
+    gln_p[q] += lnbp * kHalf * xj;
+    glp_p[q] += lpbp * kHalf * xj;
+  }
+  double o = a.alpha * w[q] + xb;
+  if (base) o += a.beta * base[q];
+  out[q] = o;
+}
+
+}  // namespace hipft

@@ -18,6 +18,7 @@
 #include "../../include/hipft_gpu.h"
 #include "kernels.cuh"
 #include "sts_pair_ws.cuh"
+#include "adjoint.cuh"
 
 using namespace hipft;
 
@@ -103,6 +104,12 @@ struct hipft_gpu {
   std::vector<WsMapEntry> ws_map_cache;  // tensor maps of the field buffers, by (pointer, box columns)
   CUtensorMap ws_rt_map{};               // tensor map of ptab.row
   bool ws_rt_ok = false;
+  // adjoint: fields of one taped forward step, folded work fields (seam
+  // columns stay zero), per-block partial sums and pole sums
+  std::vector<double *> tape;
+  double *adjw[8] = {};
+  double *d_dpart = nullptr, *d_gring = nullptr;
+  int dpart_per_r = 0;
   hipft_allreduce_cb red_cb = nullptr;  // scalar all-reduce over ranks (plain-mode sharding)
   void *red_user = nullptr;
   PoleScratch pole{};       // chunk shares of the ring sums for k_pair_poles
@@ -2067,5 +2074,246 @@ extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, in
     return na_fail(err, err_len, HIPFT_ECUDA, "copy of the results failed");
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return na_fail(err, err_len, HIPFT_ECUDA, cudaGetErrorString(e));
+  return HIPFT_OK;
+}
+
+// ------------------------------------------------------------------ adjoint
+// Discrete adjoint of one flux_transport_step (no reference counterpart):
+// the step is replayed from its input with every stage input kept (the
+// "tape"), then run backwards through the transposed stages.  The schedule
+// of the replay (PTL subcycle dts, RKG2 stage counts) is the forward's own,
+// computed by the same routines from the same field, and is held fixed:
+// the gradient is that of the discrete map at this schedule.
+
+namespace {
+struct AdjSub {
+  double dtl;
+  int64_t s;
+  std::vector<double> uj, vj, ubj, gj;
+  size_t t0;  // tape slots: t0 = u0, t0+1 = dty0, t0+1+k = Y_k (k = 1..s-1)
+};
+}  // namespace
+
+static int adj_slot(hipft_gpu *h, size_t n, double **p) {
+  while (h->tape.size() <= n) {
+    double *q = nullptr;
+    TRY(dalloc(h, &q, h->fieldn));
+    h->tape.push_back(q);
+  }
+  *p = h->tape[n];
+  return HIPFT_OK;
+}
+
+static int adj_ensure(hipft_gpu *h) {
+  if (h->adjw[0]) return HIPFT_OK;
+  for (auto &w : h->adjw) {
+    TRY(dalloc(h, &w, h->fieldn));
+    CK(h, cudaMemsetAsync(w, 0, h->fieldn * sizeof(double), h->stream));
+  }
+  dim3 g = stage_grid(h, 32, 8);
+  h->dpart_per_r = (int)(g.x * g.y);
+  TRY(dalloc(h, &h->d_dpart, (size_t)h->dpart_per_r * h->nr));
+  TRY(dalloc(h, &h->d_gring, 2 * (size_t)h->nr));
+  return HIPFT_OK;
+}
+
+// SSPRK(4,3) with its four stage inputs kept (src/hipft.f90:7552-7574);
+// the result replaces the current field.
+static int adj_adv_fwd(hipft_gpu *h, double dtl, size_t &nt, size_t t[4]) {
+  double *T[4];
+  for (int q = 0; q < 4; ++q) {
+    t[q] = nt;
+    TRY(adj_slot(h, nt++, &T[q]));
+  }
+  double *f = h->buf[h->cur];
+  CK(h, cudaMemcpyAsync(T[0], f, h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  TRY(advection_stage(h, T[0], nullptr, T[1], AdvCombine{0, 0.0, 0.0, 0.5 * dtl}));
+  TRY(advection_stage(h, T[1], nullptr, T[2], AdvCombine{0, 0.0, 0.0, 0.5 * dtl}));
+  TRY(advection_stage(h, T[2], T[0], T[3], AdvCombine{1, c_two_third, c_third, c_sixth * dtl}));
+  TRY(advection_stage(h, T[3], nullptr, f, AdvCombine{0, 0.0, 0.0, 0.5 * dtl}));
+  h->dring_valid = false;
+  return HIPFT_OK;
+}
+
+// diffusion_step (src/hipft.f90:4551-4695) with RKG2 super-steps whose
+// stage fields are kept; same subcycle logic as hipft_gpu_diffusion_step.
+static int adj_diff_fwd(hipft_gpu *h, double dtl, size_t &nt, std::vector<AdjSub> &subs) {
+  const int max_sc = 60;
+  int i = 1;
+  bool done = false;
+  double time_stepped = 0.0;
+  double dtl2 = h->auto_sc ? 0.0 : dtl / (double)h->P.diffusion_subcycles;
+  for (;;) {
+    if (h->auto_sc) TRY(ptl_dt(h, &dtl2));
+    if (h->auto_sc && time_stepped + dtl2 >= dtl) {
+      dtl2 = dtl - time_stepped;
+      done = true;
+    }
+    if (h->auto_sc && i == max_sc - 1) {
+      dtl2 = dtl - time_stepped;
+      done = true;
+    }
+    load_sts(h, dtl2);
+    AdjSub S;
+    S.dtl = dtl2;
+    S.s = h->sts_s;
+    S.uj = h->sts_uj;
+    S.vj = h->sts_vj;
+    S.ubj = h->sts_ubj;
+    S.gj = h->sts_gj;
+    S.t0 = nt;
+    double *u0, *dty0;
+    TRY(adj_slot(h, nt++, &u0));
+    TRY(adj_slot(h, nt++, &dty0));
+    std::vector<double *> Y((size_t)S.s + 1, nullptr);
+    Y[0] = u0;
+    for (int64_t k = 1; k <= S.s - 1; ++k) TRY(adj_slot(h, nt++, &Y[k]));
+    Y[S.s] = h->buf[h->cur];
+    CK(h, cudaMemcpyAsync(u0, h->buf[h->cur], h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    TRY(ring_diffusion(h, u0, h->d_ring));
+    TRY(diffusion_stage<MODE_STS1>(h, u0, nullptr, nullptr, nullptr, Y[1], dty0, h->d_ring,
+                                   StageCoef{dtl2, S.ubj[1], 0, 0, 0}, nullptr));
+    for (int64_t k = 2; k <= S.s; ++k) {
+      const double uj = S.uj[k], vj = S.vj[k];
+      TRY(ring_diffusion(h, Y[k - 1], h->d_ring));
+      TRY(diffusion_stage<MODE_STSK>(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], nullptr, h->d_ring,
+                                     StageCoef{uj, vj, 1.0 - uj - vj, S.ubj[k] * dtl2, S.gj[k]}, nullptr));
+    }
+    h->dring_valid = false;
+    h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr * S.s;
+    subs.push_back(std::move(S));
+    time_stepped = time_stepped + dtl2;
+    if (!h->auto_sc && i == h->P.diffusion_subcycles) done = true;
+    if (done) break;
+    i = i + 1;
+  }
+  return HIPFT_OK;
+}
+
+// a work field other than those in `busy`
+static double *adj_free(hipft_gpu *h, std::initializer_list<const double *> busy) {
+  for (double *w : h->adjw) {
+    bool used = false;
+    for (const double *b : busy) used = used || (b == w);
+    if (!used) return w;
+  }
+  return nullptr;
+}
+
+static int adj_adv_rev(hipft_gpu *h, double dtl, const size_t t[4], double *&W, double *gflow) {
+  const dim3 blk(32, 8), grd = stage_grid(h, 32, 8);
+  double *g[5];
+  for (int q = 0; q < 5; ++q) g[q] = gflow + (size_t)q * h->fieldn;
+  auto stage = [&](const double *x, const double *w, double sigma, double alpha, const double *base, double beta,
+                   double *out) -> int {
+    k_adj_pole_sums<<<h->nr, 256, 0, h->stream>>>(h->M, w, h->d_gring);
+    LAUNCHED(h);
+    k_adj_adv<<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->W, x, w, base, out, h->d_gring,
+                                          AdjAdvArgs{sigma, alpha, beta, h->bc_flow_n, h->bc_flow_s}, g[0], g[1],
+                                          g[2], g[3], g[4]);
+    LAUNCHED(h);
+    return HIPFT_OK;
+  };
+  double *b3 = adj_free(h, {W});
+  double *b2 = adj_free(h, {W, b3});
+  double *b1 = adj_free(h, {W, b3, b2});
+  const double *T0 = h->tape[t[0]], *T1 = h->tape[t[1]], *T2 = h->tape[t[2]], *T3 = h->tape[t[3]];
+  TRY(stage(T3, W, -0.5 * dtl, 1.0, nullptr, 0.0, b3));
+  TRY(stage(T2, b3, -c_sixth * dtl, c_third, nullptr, 0.0, b2));
+  TRY(stage(T1, b2, -0.5 * dtl, 1.0, nullptr, 0.0, b1));
+  TRY(stage(T0, b1, -0.5 * dtl, 1.0, b3, c_two_third, W));
+  return HIPFT_OK;
+}
+
+// Reverse of one RKG2 super-step: W (cotangent of Y_s) becomes the
+// cotangent of u0; dacc[i] += the diffusion-coefficient terms
+// sum mu~_k dt <A^T Wbar_k, Y_{k-1}> (+ dt <A^T dbar, u0>).
+static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc) {
+  const dim3 blk(32, 8), grd = stage_grid(h, 32, 8);
+  const double dtl = S.dtl;
+  double *ub = adj_free(h, {W});
+  double *db = adj_free(h, {W, ub});
+  CK(h, cudaMemsetAsync(ub, 0, h->fieldn * sizeof(double), h->stream));
+  CK(h, cudaMemsetAsync(db, 0, h->fieldn * sizeof(double), h->stream));
+  auto Yt = [&](int64_t k) -> const double * { return h->tape[S.t0 + (k == 0 ? 0 : 1 + k)]; };
+  auto adj = [&](const double *w, const double *wp, const double *y, double *out, double *u, double *d,
+                 AdjDiffCoef ac, double dscale) -> int {
+    k_adj_pole_sums<<<h->nr, 256, 0, h->stream>>>(h->M, w, h->d_gring);
+    LAUNCHED(h);
+    k_adj_diff<<<grd, blk, 0, h->stream>>>(h->M, h->DC, w, wp, y, out, u, d, h->d_gring, h->bc_diff_n,
+                                           h->bc_diff_s, ac, y ? h->d_dpart : nullptr);
+    LAUNCHED(h);
+    if (y) {
+      k_adj_dsum<<<h->nr, 256, 0, h->stream>>>(h->d_dpart, h->dpart_per_r, dscale, dacc);
+      LAUNCHED(h);
+    }
+    return HIPFT_OK;
+  };
+  double *Wk = W, *Wk1 = nullptr;
+  for (int64_t k = S.s; k >= 2; --k) {
+    double *Wm = adj_free(h, {Wk, Wk1, ub, db});
+    const double uj = S.uj[k], vj = S.vj[k];
+    const double nu1 = (k < S.s) ? S.vj[k + 1] : 0.0;
+    TRY(adj(Wk, Wk1, Yt(k - 1), Wm, ub, db, AdjDiffCoef{uj, nu1, S.ubj[k] * dtl, 1.0 - uj - vj, S.gj[k]},
+            S.ubj[k] * dtl));
+    Wk1 = Wk;
+    Wk = Wm;
+  }
+  // Y_1 = u0 + mu~_1 dty0 and Y_0 = u0 (read by stage 2 with nu_2)
+  k_adj_axpy2<<<grd, blk, 0, h->stream>>>(h->M, ub, 1.0, Wk, S.vj[2], Wk1);
+  LAUNCHED(h);
+  k_adj_axpy2<<<grd, blk, 0, h->stream>>>(h->M, db, S.ubj[1], Wk, 0.0, nullptr);
+  LAUNCHED(h);
+  // dty0 = dt A u0
+  TRY(adj(db, ub, Yt(0), ub, nullptr, nullptr, AdjDiffCoef{0.0, 1.0, dtl, 0.0, 0.0}, dtl));
+  W = ub;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, double *dacc,
+                              double *gflow) {
+  if (!h || !f_in || !fbar || !dacc || !gflow) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "adjoint step before set_field");
+  if (h->P.advance_flow && (h->adv_time != 3 || h->adv_space != 2 || h->FL.flow2d))
+    return fail(h, HIPFT_ESTATE, "adjoint: advection must be WENO3+SSPRK(4,3) with analytic flows");
+  if (h->P.advance_diffusion && (h->P.diffusion_num_method != 3 || h->DC.grid))
+    return fail(h, HIPFT_ESTATE, "adjoint: diffusion must be RKG2 with per-realization constant coefficients");
+  if (h->P.advance_source) return fail(h, HIPFT_ESTATE, "adjoint: sources are not differentiated");
+  CK(h, cudaSetDevice(h->dev));
+  TRY(adj_ensure(h));
+  const size_t bytes = h->fieldn * sizeof(double);
+  CK(h, cudaMemcpyAsync(h->buf[h->cur], f_in, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  h->dring_valid = false;
+  size_t nt = 0, ta1[4] = {}, ta2[4] = {};
+  std::vector<AdjSub> subs;
+  const bool strang = h->P.strang_splitting != 0;
+  const double da = strang ? 0.5 * dt : dt;
+  if (h->P.advance_flow) TRY(adj_adv_fwd(h, da, nt, ta1));
+  if (h->P.advance_diffusion) TRY(adj_diff_fwd(h, dt, nt, subs));
+  if (strang && h->P.advance_flow) TRY(adj_adv_fwd(h, da, nt, ta2));
+  double *W = h->adjw[0];
+  CK(h, cudaMemcpyAsync(W, fbar, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  if (strang && h->P.advance_flow) TRY(adj_adv_rev(h, da, ta2, W, gflow));
+  for (size_t q = subs.size(); q-- > 0;) TRY(adj_diff_rev(h, subs[q], W, dacc));
+  if (h->P.advance_flow) TRY(adj_adv_rev(h, da, ta1, W, gflow));
+  CK(h, cudaMemcpyAsync(fbar, W, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaGetLastError());
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n) {
+  if (!h || !n) return HIPFT_EINVAL;
+  *n = (int64_t)h->tape.size();
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_set_field_device(hipft_gpu *h, const double *f_dev) {
+  if (!h || !f_dev) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "set_field_device before set_field");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaMemcpyAsync(h->buf[h->cur], f_dev, h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  h->dring_valid = false;
+  CK(h, cudaStreamSynchronize(h->stream));
   return HIPFT_OK;
 }

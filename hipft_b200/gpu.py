@@ -124,6 +124,10 @@ SIGNATURES = [
     ("hipft_gpu_set_allreduce", ctypes.c_int, [_H, ALLREDUCE_CB, ctypes.c_void_p]),
     ("hipft_gpu_field_device_ptr", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_int)]),
     ("hipft_gpu_check_bounded_wait", ctypes.c_int, [_H, ctypes.c_uint]),
+    ("hipft_adj_step", ctypes.c_int, [_H, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]),
+    ("hipft_gpu_set_field_device", ctypes.c_int, [_H, ctypes.c_void_p]),
+    ("hipft_adj_tape_fields", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64)]),
     ("hipft_run_shard", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(Shard), DPTR,
                                        ctypes.c_size_t]),
     ("hipft_gpu_set_source_file", ctypes.c_int, [_H, DPTR]),

@@ -325,6 +325,34 @@ typedef struct {
 int hipft_run_shard(const char *namelist_path, const char *run_dir, int device, const hipft_shard *shard,
                     double *f_out, size_t f_len);
 
+/* ---- discrete adjoint (PyTorch binding; no reference counterpart) ---------- */
+
+/* Reverse pass of one flux_transport_step for gradients of a map misfit.
+ * Device pointers, each a field in the handle's layout (nr x npm x ldt,
+ * theta padded to ldt, see hipft_gpu_field_device_ptr):
+ *   f_in  the step's input field (unchanged);
+ *   fbar  in: cotangent of the step's output, out: cotangent of its input,
+ *         both "folded" (phi seam columns 1 and npm carry nothing; their
+ *         dependence is on columns npm-1 and 2);
+ *   dacc  [nr] += sum over RKG2 stages of mu~_k dt <A^T Wbar, Y_{k-1}> (the
+ *         derivative with respect to the diffusion coefficient constant c
+ *         is dacc / c);
+ *   gflow 5 fields += per-cell flow cotangents: theta LN (vt(j)+at(j)),
+ *         theta LP (vt(j+1)-at(j)), theta upwind faces (vt(j)), phi LN
+ *         (vp+ap), phi LP (vp-ap), each already multiplied by x/2.
+ * The step is replayed from f_in with every stage input kept; its schedule
+ * (PTL subcycle dts, RKG2 stage counts) is the forward's and is held fixed.
+ * Requires WENO3+SSPRK(4,3) with analytic flows, RKG2 with per-realization
+ * constant diffusion coefficients and no sources (else HIPFT_ESTATE).  The
+ * current field becomes the step's output. */
+int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, double *dacc, double *gflow);
+/* Replace the current field from device memory in the handle's layout
+ * (nr x npm x ldt), e.g. a checkpoint taken through
+ * hipft_gpu_field_device_ptr; cached pole sums are dropped. */
+int hipft_gpu_set_field_device(hipft_gpu *h, const double *f_dev);
+/* Fields the adjoint's tape holds (device memory, fieldn doubles each). */
+int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n);
+
 /* ---- map files ------------------------------------------------------------- */
 
 /* Minimal reader of the reference's HDF5 maps (rdh5, src/hipft.f90:5678):
