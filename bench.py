@@ -31,6 +31,7 @@ workload: one realization, one flux-transport step per bench step.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import datetime
 import json
 import os
@@ -340,6 +341,8 @@ def run_gpu(args, wl, name):
     }
     if rank == 0 and world == 1 and not args.no_plain:
         out["plain"] = measure_plain(args, local)
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        out["adjoint"] = measure_adjoint(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cells_c, sec_c = oracle_sample(t, p, br, prm, dt, index=0)
         out["cpu_baseline"] = {"value": cells_c / sec_c / 1e9, "unit": UNIT, "cores": host_threads(),
@@ -447,6 +450,76 @@ def measure_plain(args, local: int):
     return out
 
 
+def measure_adjoint(args, local: int, nsteps: int = 16):
+    """Gradient / forward cost of the misfit adjoint on a 512 x 1024 uniform
+    grid with the plain configuration's physics (one realization, PTL
+    subcycling): wall time of hipft_b200.adjoint.MisfitAdjoint.run (forward
+    with checkpoints, misfit, reverse) over `nsteps` steps, against the same
+    steps through the library's forward alone (field copied in and out).  The
+    target map is the same run with D x 1.2 and v0 + 3 m/s."""
+    import torch
+    import hipft_b200 as H
+    from hipft_b200 import synthetic as S
+    from hipft_b200.adjoint import MisfitAdjoint
+    ntm, npm1 = 512, 1025
+    t = np.linspace(0.0, np.pi, ntm)
+    p = np.linspace(0.0, 2.0 * np.pi, npm1)
+    br = S.bipole_map(t, p, 0)
+    prm = S.plain_params()
+    flow = {"p0": prm["dr_p0"], "p2": prm["dr_p2"], "p4": prm["dr_p4"], "p1": prm["mf_p1"], "p3": prm["mf_p3"],
+            "p5": prm["mf_p5"]}
+
+    def handle(D, fl):
+        g = H.HipftGPU(t, p, 1, device=local, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                       advance_diffusion=True, diffusion_coef_constants=D)
+        g.set_flow(dr_model=1, mf_model=1, dr_p0=fl["p0"], dr_p2=fl["p2"], dr_p4=fl["p4"], mf_p1=fl["p1"],
+                   mf_p3=fl["p3"], mf_p5=fl["p5"])
+        return g
+
+    D = prm["diffusion_coef_constants"]
+    g = handle(D, flow)
+    g.load_initial_map(br[None])
+    f0 = g.get_field()
+    g.update_flow()
+    dt = g.flow_dtmax()
+    dts = [dt] * nsteps
+
+    def forward(gg, f):
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        gg.set_field(f)
+        gg.update_flow()
+        for d in dts:
+            gg.flux_transport_step(d)
+        out = gg.get_field()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - w0
+
+    fl_t = dict(flow, p1=flow["p1"] + 6.0, p3=flow["p3"] - 6.0)
+    gt = handle(D * 1.2, fl_t)
+    target, _ = forward(gt, f0)
+    gt.close()
+    forward(g, f0)
+    _, fwd_s = forward(g, f0)
+    A = MisfitAdjoint(g, D, flow, checkpoint_every=64)
+    A.run(f0, target, dts)
+    torch.cuda.synchronize()
+    w0 = time.perf_counter()
+    loss, grads = A.run(f0, target, dts)
+    torch.cuda.synchronize()
+    grad_s = time.perf_counter() - w0
+    tape = ctypes.c_int64(0)
+    g.L.hipft_adj_tape_fields(g.h, ctypes.byref(tape))
+    g.close()
+    return {"workload": "adjoint_512x1024", "grid": [ntm, npm1 - 1], "realizations": 1, "steps": nsteps,
+            "dt_hours": dt, "subcycling": "PTL (automatic)", "checkpoint_every": 64,
+            "forward_ms": fwd_s * 1e3, "gradient_ms": grad_s * 1e3, "gradient_over_forward": grad_s / fwd_s,
+            "loss": loss, "grad_D": float(grads["D"][0]), "grad_f0_norm": float(np.linalg.norm(grads["f0"])),
+            "tape_fields_per_step": int(tape.value),
+            "note": "wall times with host copies of the field; the gradient covers the checkpointed forward, "
+                    "the segment recompute, the per-step replay with its tape and the reverse kernels"}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -456,6 +529,7 @@ def main():
     ap.add_argument("--workload", default="batched64_1024x2048", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

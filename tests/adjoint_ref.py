@@ -231,21 +231,21 @@ class RefScheme:
             ykm2, ykm1 = ykm1, y
         return ykm1
 
-    def step(self, f, dt, D, flows, subcycles, dt_euler, strang=True):
+    def step(self, f, dt, D, flows, subcycles, dt_euler, strang=True, sub_dts=None):
+        """One step; sub_dts, when given, are the diffusion subcycle dts (a
+        PTL schedule recorded from a forward run), else `subcycles` equal ones."""
         f = self.ssprk43(f, 0.5 * dt if strang else dt, flows)
-        dtl2 = dt / subcycles
-        s = self.rkg2_stages(dtl2, dt_euler)
-        for _ in range(subcycles):
-            f = self.rkg2(f, dtl2, D, s)
+        for dtl2 in (sub_dts if sub_dts is not None else [dt / subcycles] * subcycles):
+            f = self.rkg2(f, dtl2, D, self.rkg2_stages(dtl2, dt_euler))
         if strang:
             f = self.ssprk43(f, 0.5 * dt, flows)
         return f
 
-    def run(self, f0, dts, D, coef, subcycles, dt_euler, strang=True):
+    def run(self, f0, dts, D, coef, subcycles, dt_euler, strang=True, sched=None):
         flows = flow_profiles(self.m, coef)
         f = f0
-        for dt in dts:
-            f = self.step(f, float(dt), D, flows, subcycles, dt_euler, strang)
+        for n, dt in enumerate(dts):
+            f = self.step(f, float(dt), D, flows, subcycles, dt_euler, strang, None if sched is None else sched[n])
         return f
 
     def misfit(self, f, target):

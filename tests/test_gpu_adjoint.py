@@ -17,11 +17,11 @@ GRAD_TOL = 1e-9     # relative max-norm, adjoint vs autograd of the restatement
 FD_TOL = 1e-6       # relative, adjoint vs central differences (h = 1e-6 relative)
 
 
-def _handle(D, coef):
+def _handle(D, coef, subcycles=C.CASE["diffusion_subcycles"]):
     t, p = C.mesh_tp()
     g = G.HipftGPU(t, p, C.CASE["n_realizations"], advance_flow=True, flow_num_method=4, strang_splitting=True,
-                   advance_diffusion=True, diffusion_num_method=3,
-                   diffusion_subcycles=C.CASE["diffusion_subcycles"], diffusion_coef_constants=D)
+                   advance_diffusion=True, diffusion_num_method=3, diffusion_subcycles=subcycles,
+                   diffusion_coef_constants=D)
     g.set_flow(dr_model=1, mf_model=1, dr_p0=coef["p0"], dr_p2=coef["p2"], dr_p4=coef["p4"], mf_p1=coef["p1"],
                mf_p3=coef["p3"], mf_p5=coef["p5"])
     return g
@@ -35,13 +35,13 @@ def _inputs():
     return f0, C.target_field(f0), dts, D, coef
 
 
-def _reference_grads(f0, target, dts, D, coef):
+def _reference_grads(f0, target, dts, D, coef, sched=None):
     t, p = C.mesh_tp()
     S = RefScheme(t, p, len(D))
     f0v = torch.tensor(f0, requires_grad=True)
     Dv = torch.tensor(D, requires_grad=True)
     cv = {k: torch.tensor(v, requires_grad=True) for k, v in coef.items()}
-    f = S.run(f0v, dts, Dv, cv, C.CASE["diffusion_subcycles"], S.euler_dt(D))
+    f = S.run(f0v, dts, Dv, cv, C.CASE["diffusion_subcycles"], S.euler_dt(D), sched=sched)
     L = S.misfit(f, torch.tensor(target))
     L.backward()
     g = {"f0": f0v.grad.numpy(), "D": Dv.grad.numpy()}
@@ -53,11 +53,7 @@ def _rel(a, b):
     return np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(b)), 1e-300)
 
 
-def test_adjoint_matches_autograd_of_restatement():
-    f0, target, dts, D, coef = _inputs()
-    with _handle(D, coef) as g:
-        loss, grads = MisfitAdjoint(g, D, coef, checkpoint_every=2).run(f0, target, dts)
-    Lr, gr = _reference_grads(f0, target, dts, D, coef)
+def _check_against_reference(loss, grads, Lr, gr):
     assert abs(loss - Lr) <= 1e-12 * abs(Lr), (loss, Lr)
     # the restatement's f0 gradient carries the seam columns separately; fold them
     fr = gr["f0"].copy()
@@ -70,6 +66,31 @@ def test_adjoint_matches_autograd_of_restatement():
         assert _rel(grads[k], gr[k]) < GRAD_TOL, (k, grads[k], gr[k])
     phys = chain_physical(grads)
     assert all(np.all(np.isfinite(v)) for v in phys.values())
+
+
+def test_adjoint_matches_autograd_of_restatement():
+    f0, target, dts, D, coef = _inputs()
+    with _handle(D, coef) as g:
+        loss, grads = MisfitAdjoint(g, D, coef, checkpoint_every=2).run(f0, target, dts)
+    _check_against_reference(loss, grads, *_reference_grads(f0, target, dts, D, coef))
+
+
+def test_adjoint_with_ptl_subcycles_matches_autograd_of_restatement():
+    """Automatic (PTL) subcycling: the adjoint replays the forward's subcycle
+    dts, which the restatement takes from the step callback."""
+    f0, target, dts, D, coef = _inputs()
+    sched = []
+    with _handle(D, coef, subcycles=0) as g:
+        g.set_field(f0)
+        g.update_flow()
+        for dt in dts:
+            sub = []
+            g.flux_transport_step(float(dt), cb=lambda c, ts, dtl2, s, sc: sub.append(dtl2))
+            sched.append(sub)
+    assert max(len(s) for s in sched) > 1
+    with _handle(D, coef, subcycles=0) as g:
+        loss, grads = MisfitAdjoint(g, D, coef, checkpoint_every=2).run(f0, target, dts)
+    _check_against_reference(loss, grads, *_reference_grads(f0, target, dts, D, coef, sched=sched))
 
 
 def test_checkpoint_spacing_does_not_change_the_gradient():
