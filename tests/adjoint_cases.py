@@ -24,6 +24,21 @@ def oracle_run(case=CASE):
     return p, r, dts
 
 
+def rough_run(case=CASE, seed=7):
+    """Oracle run of the case from a noisy map (10 cos(theta) G plus unit
+    Gaussian noise) with automatic PTL subcycling, which then takes several
+    subcycles per step: parameters, results and step dts."""
+    c = {k: v for k, v in case.items() if k not in ("res_nt", "res_np")}
+    c.update(diffusion_subcycles=0, validation_run=0)
+    p = O.process_parameters(O.parse_namelist(F._namelist(c)))
+    t, ph = mesh_tp(case)
+    rng = np.random.default_rng(seed)
+    nr = case["n_realizations"]
+    m = 10.0 * np.cos(t)[None, :, None] * np.ones((nr, len(t), len(ph))) + rng.standard_normal((nr, len(t), len(ph)))
+    r = O.run(p, map_pt=m, s1=ph, s2=t, map_cap=1)
+    return p, r, r["num"][1:, 0, 2]
+
+
 def mesh_tp(case=CASE):
     nt, np_ = case["res_nt"], case["res_np"]
     return np.linspace(0.0, np.pi, nt), np.linspace(0.0, 2.0 * np.pi, np_)

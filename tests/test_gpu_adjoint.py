@@ -78,7 +78,11 @@ def test_adjoint_matches_autograd_of_restatement():
 def test_adjoint_with_ptl_subcycles_matches_autograd_of_restatement():
     """Automatic (PTL) subcycling: the adjoint replays the forward's subcycle
     dts, which the restatement takes from the step callback."""
-    f0, target, dts, D, coef = _inputs()
+    _, r, dts = C.rough_run()
+    D = np.array(C.CASE["diffusion_coef_constants"])
+    coef = {k: np.array(C.CASE[v]) for k, v in C.FLOW.items()}
+    f0 = r["map_initial"]
+    target = C.target_field(f0)
     sched = []
     with _handle(D, coef, subcycles=0) as g:
         g.set_field(f0)
