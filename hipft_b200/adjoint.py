@@ -12,9 +12,10 @@ no adjoint; the forward operators are diffusion_operator_cd
 
 Method.  The forward run goes through the library's own fused step
 (hipft_gpu_flux_transport_step) and keeps the field every
-`checkpoint_every` steps on the device.  The reverse pass walks the
-checkpoint segments backwards: it recomputes a segment's step inputs from
-its checkpoint, then, step by step from the last, calls hipft_adj_step,
+`checkpoint_every` steps on the device, and every step input of the last
+segment.  The reverse pass walks the checkpoint segments backwards: it
+recomputes a segment's step inputs from its checkpoint (all but the last
+segment), then, step by step from the last, calls hipft_adj_step,
 which replays that one step with every stage input kept and runs the
 hand-written adjoint kernels (csrc/adjoint.cuh: transposed Laplacian with its
 pole rings and seam, WENO3 face derivatives including the nonlinear weights,
@@ -196,9 +197,13 @@ class MisfitAdjoint:
         g.set_field(f0)
         g.update_flow()
         ckpt = {}
+        last0 = ((n - 1) // self.k) * self.k  # the last segment's inputs are kept, not recomputed
+        kept = []
         for s, dt in enumerate(dts):
             if s % self.k == 0:
                 ckpt[s] = self._dev().clone()
+            if s >= last0:
+                kept.append(ckpt[s] if s == last0 else self._dev().clone())
             g.flux_transport_step(dt)
         fN = g.get_field()
         t1 = time.perf_counter()
@@ -211,8 +216,8 @@ class MisfitAdjoint:
         gflow = torch.zeros((5, self.nr, self.npm, ldt), dtype=torch.float64, device=dev)
         for s0 in sorted(ckpt, reverse=True):
             s1 = min(s0 + self.k, n)
-            states = [ckpt[s0]]
-            if s1 - s0 > 1:
+            states = kept if s0 == last0 else [ckpt[s0]]
+            if s0 != last0 and s1 - s0 > 1:
                 self._set(ckpt[s0])
                 for s in range(s0, s1 - 1):
                     g.flux_transport_step(dts[s])

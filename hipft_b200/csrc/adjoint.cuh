@@ -68,38 +68,77 @@ __device__ __forceinline__ double adj_diff_at(const Mesh &m, const DiffCoef &dc,
 
 // One reverse RKG2 stage (or a plain A^T application), per core cell:
 //   out = a*w + b*wp + c*(A^T w);   ub += c0*w;   db += g*w;
-// and per block the sum of (A^T w)*y (the diffusion-coefficient term),
-// written to dpart[block] for k_adj_dsum.  wp, y, ub, db may be null.
-// out may alias wp (each cell reads wp before writing out).
+// dpart[block] += dscale * (block sum of (A^T w)*y) (the diffusion-
+// coefficient term, summed per realization by k_adj_dsum).  wp, y, ub, db
+// may be null; out may alias wp (each cell reads wp before writing out).
+// w's pole sums come as npin partials per realization, gin[(i-1)][q][2]
+// (summed in order by the blocks that need them); the kernel leaves the
+// pole sums of `out` as gridDim.y partials in gout, for the next stage.
 struct AdjDiffCoef {
-  double a, b, c, c0, g;
+  double a, b, c, c0, g, dscale;
 };
 
 __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const double *__restrict__ w, const double *wp,
                                                   const double *__restrict__ y, double *out, double *ub, double *db,
-                                                  const double *__restrict__ gring, double bcn, double bcs,
-                                                  AdjDiffCoef ac, double *__restrict__ dpart) {
+                                                  const double *__restrict__ gin, int npin, double *__restrict__ gout,
+                                                  double bcn, double bcs, AdjDiffCoef ac, double *__restrict__ dpart) {
   __shared__ double sh[64];
+  __shared__ double s_g[2];
+  __shared__ double s_n[8], s_s[8];
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int i = blockIdx.z + 1;
-  double dsum = 0.0;
-  if (j <= m.ntm && k <= m.npm - 1) {
+  const int j0 = blockIdx.x * blockDim.x + 1, j1 = j0 + blockDim.x - 1;
+  const bool need = (j0 <= 2) || (j1 >= m.ntm - 1);  // rows 1, 2, ntm-1, ntm use the pole sums
+  if (need) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      double a = 0.0, b = 0.0;
+      const double *g = gin + (int64_t)(i - 1) * npin * 2;
+      for (int q = 0; q < npin; ++q) {
+        a = a + g[2 * q];
+        b = b + g[2 * q + 1];
+      }
+      s_g[0] = a;
+      s_g[1] = b;
+    }
+    __syncthreads();
+  }
+  double dsum = 0.0, o = 0.0;
+  const bool active = (j <= m.ntm && k <= m.npm - 1);
+  if (active) {
     const int64_t q = fidx(m, j, k, i);
-    const double aw = adj_diff_at(m, dc, w, j, k, i, gring[2 * (i - 1)], gring[2 * (i - 1) + 1], bcn, bcs);
+    const double gn = need ? s_g[0] : 0.0, gs = need ? s_g[1] : 0.0;
+    const double aw = adj_diff_at(m, dc, w, j, k, i, gn, gs, bcn, bcs);
     const double wq = w[q];
-    double o = ac.a * wq + ac.c * aw;
+    o = ac.a * wq + ac.c * aw;
     if (wp) o += ac.b * wp[q];
     out[q] = o;
     if (ub) ub[q] += ac.c0 * wq;
     if (db) db[q] += ac.g * wq;
     if (y) dsum = aw * y[q];
   }
-  if (dpart) {
+  // pole-row partials of out over this block's columns (fixed order)
+  const bool has_n = (j0 == 1), has_s = (j0 <= m.ntm && j1 >= m.ntm);
+  if (has_n || has_s) {
+    if (threadIdx.x == 0) s_n[threadIdx.y] = active ? o : 0.0;
+    if (j == m.ntm) s_s[threadIdx.y] = active ? o : 0.0;
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+      double a = 0.0, b = 0.0;
+      for (int t = 0; t < (int)blockDim.y; ++t) {
+        a = a + s_n[t];
+        b = b + s_s[t];
+      }
+      double *go = gout + ((int64_t)(i - 1) * gridDim.y + blockIdx.y) * 2;
+      if (has_n) go[0] = a;
+      if (has_s) go[1] = b;
+    }
+  }
+  if (dpart && y) {
     double z = 0.0;
     block_sum2(dsum, z, sh);
     if (threadIdx.x == 0 && threadIdx.y == 0)
-      dpart[((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = dsum;
+      dpart[((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] += ac.dscale * dsum;
   }
 }
 

@@ -108,7 +108,7 @@ struct hipft_gpu {
   // columns stay zero), per-block partial sums and pole sums
   std::vector<double *> tape;
   double *adjw[8] = {};
-  double *d_dpart = nullptr, *d_gring = nullptr;
+  double *d_dpart = nullptr, *d_gring = nullptr, *d_gpart[2] = {};
   int dpart_per_r = 0;
   hipft_allreduce_cb red_cb = nullptr;  // scalar all-reduce over ranks (plain-mode sharding)
   void *red_user = nullptr;
@@ -2114,6 +2114,7 @@ static int adj_ensure(hipft_gpu *h) {
   h->dpart_per_r = (int)(g.x * g.y);
   TRY(dalloc(h, &h->d_dpart, (size_t)h->dpart_per_r * h->nr));
   TRY(dalloc(h, &h->d_gring, 2 * (size_t)h->nr));
+  for (auto &gp : h->d_gpart) TRY(dalloc(h, &gp, 2 * (size_t)g.y * h->nr));
   return HIPFT_OK;
 }
 
@@ -2170,16 +2171,26 @@ static int adj_diff_fwd(hipft_gpu *h, double dtl, size_t &nt, std::vector<AdjSub
     for (int64_t k = 1; k <= S.s - 1; ++k) TRY(adj_slot(h, nt++, &Y[k]));
     Y[S.s] = h->buf[h->cur];
     CK(h, cudaMemcpyAsync(u0, h->buf[h->cur], h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    TRY(ring_diffusion(h, u0, h->d_ring));
-    TRY(diffusion_stage<MODE_STS1>(h, u0, nullptr, nullptr, nullptr, Y[1], dty0, h->d_ring,
-                                   StageCoef{dtl2, S.ubj[1], 0, 0, 0}, nullptr));
-    for (int64_t k = 2; k <= S.s; ++k) {
+    // the same kernels, in the same order, as sts_super_step (with its pole
+    // sums of the current field), writing every stage into the tape
+    const double *r0;
+    TRY(current_dring(h, &r0));
+    TRY(sts_stage_v2<MODE_STS1>(h, u0, nullptr, nullptr, nullptr, Y[1], dty0, StageCoef{dtl2, S.ubj[1], 0, 0, 0}));
+    auto coef = [&](int64_t k) {
       const double uj = S.uj[k], vj = S.vj[k];
-      TRY(ring_diffusion(h, Y[k - 1], h->d_ring));
-      TRY(diffusion_stage<MODE_STSK>(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], nullptr, h->d_ring,
-                                     StageCoef{uj, vj, 1.0 - uj - vj, S.ubj[k] * dtl2, S.gj[k]}, nullptr));
+      return StageCoef{uj, vj, 1.0 - uj - vj, S.ubj[k] * dtl2, S.gj[k]};
+    };
+    int64_t k = 2;
+    while (k <= S.s) {
+      if (sts_pairs_enabled() && k + 1 <= S.s) {
+        TRY(sts_pair(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], Y[k + 1], coef(k), coef(k + 1), k > 2));
+        k += 2;
+        continue;
+      }
+      TRY(sts_stage_v2<MODE_STSK>(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], nullptr, coef(k)));
+      k += 1;
     }
-    h->dring_valid = false;
+    h->dring_valid = true;  // the last fused stage left the ring of the output
     h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr * S.s;
     subs.push_back(std::move(S));
     time_stepped = time_stepped + dtl2;
@@ -2227,7 +2238,8 @@ static int adj_adv_rev(hipft_gpu *h, double dtl, const size_t t[4], double *&W, 
 
 // Reverse of one RKG2 super-step: W (cotangent of Y_s) becomes the
 // cotangent of u0; dacc[i] += the diffusion-coefficient terms
-// sum mu~_k dt <A^T Wbar_k, Y_{k-1}> (+ dt <A^T dbar, u0>).
+// sum mu~_k dt <A^T Wbar_k, Y_{k-1}> (+ dt <A^T dbar, u0>).  One launch per
+// stage: each leaves the pole-row partials of its output for the next.
 static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc) {
   const dim3 blk(32, 8), grd = stage_grid(h, 32, 8);
   const double dtl = S.dtl;
@@ -2235,27 +2247,36 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   double *db = adj_free(h, {W, ub});
   CK(h, cudaMemsetAsync(ub, 0, h->fieldn * sizeof(double), h->stream));
   CK(h, cudaMemsetAsync(db, 0, h->fieldn * sizeof(double), h->stream));
+  CK(h, cudaMemsetAsync(h->d_dpart, 0, (size_t)h->dpart_per_r * h->nr * sizeof(double), h->stream));
   auto Yt = [&](int64_t k) -> const double * { return h->tape[S.t0 + (k == 0 ? 0 : 1 + k)]; };
-  auto adj = [&](const double *w, const double *wp, const double *y, double *out, double *u, double *d,
-                 AdjDiffCoef ac, double dscale) -> int {
+  const double *gin = h->d_gring;
+  int npin = 1, pp = 0;
+  auto pole_sums = [&](const double *w) -> int {
     k_adj_pole_sums<<<h->nr, 256, 0, h->stream>>>(h->M, w, h->d_gring);
     LAUNCHED(h);
-    k_adj_diff<<<grd, blk, 0, h->stream>>>(h->M, h->DC, w, wp, y, out, u, d, h->d_gring, h->bc_diff_n,
-                                           h->bc_diff_s, ac, y ? h->d_dpart : nullptr);
-    LAUNCHED(h);
-    if (y) {
-      k_adj_dsum<<<h->nr, 256, 0, h->stream>>>(h->d_dpart, h->dpart_per_r, dscale, dacc);
-      LAUNCHED(h);
-    }
+    gin = h->d_gring;
+    npin = 1;
     return HIPFT_OK;
   };
+  auto stage = [&](const double *w, const double *wp, const double *y, double *out, double *u, double *d,
+                   AdjDiffCoef ac) -> int {
+    double *gout = h->d_gpart[pp];
+    k_adj_diff<<<grd, blk, 0, h->stream>>>(h->M, h->DC, w, wp, y, out, u, d, gin, npin, gout, h->bc_diff_n,
+                                           h->bc_diff_s, ac, h->d_dpart);
+    LAUNCHED(h);
+    gin = gout;
+    npin = (int)grd.y;
+    pp ^= 1;
+    return HIPFT_OK;
+  };
+  TRY(pole_sums(W));
   double *Wk = W, *Wk1 = nullptr;
   for (int64_t k = S.s; k >= 2; --k) {
     double *Wm = adj_free(h, {Wk, Wk1, ub, db});
     const double uj = S.uj[k], vj = S.vj[k];
     const double nu1 = (k < S.s) ? S.vj[k + 1] : 0.0;
-    TRY(adj(Wk, Wk1, Yt(k - 1), Wm, ub, db, AdjDiffCoef{uj, nu1, S.ubj[k] * dtl, 1.0 - uj - vj, S.gj[k]},
-            S.ubj[k] * dtl));
+    TRY(stage(Wk, Wk1, Yt(k - 1), Wm, ub, db,
+              AdjDiffCoef{uj, nu1, S.ubj[k] * dtl, 1.0 - uj - vj, S.gj[k], S.ubj[k] * dtl}));
     Wk1 = Wk;
     Wk = Wm;
   }
@@ -2265,7 +2286,10 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   k_adj_axpy2<<<grd, blk, 0, h->stream>>>(h->M, db, S.ubj[1], Wk, 0.0, nullptr);
   LAUNCHED(h);
   // dty0 = dt A u0
-  TRY(adj(db, ub, Yt(0), ub, nullptr, nullptr, AdjDiffCoef{0.0, 1.0, dtl, 0.0, 0.0}, dtl));
+  TRY(pole_sums(db));
+  TRY(stage(db, ub, Yt(0), ub, nullptr, nullptr, AdjDiffCoef{0.0, 1.0, dtl, 0.0, 0.0, dtl}));
+  k_adj_dsum<<<h->nr, 256, 0, h->stream>>>(h->d_dpart, h->dpart_per_r, 1.0, dacc);
+  LAUNCHED(h);
   W = ub;
   return HIPFT_OK;
 }
