@@ -12,6 +12,7 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "sts_pair_ws.cuh"  // PairTables (coefficient tables of k_pair_tables)
 
 namespace hipft {
 
@@ -66,6 +67,40 @@ __device__ __forceinline__ double adj_diff_at(const Mesh &m, const DiffCoef &dc,
   return r;
 }
 
+// The same, from the coefficient tables of k_pair_tables (per-realization
+// constant D): row j's st_i, c2, c4 and column k's {P1, P5}, with
+// c1 = P1 st_i^2, c5 = P5 st_i^2 and c3 = -(c1+c2+c4+c5) as in the forward
+// two-stage kernel; five table rows and columns instead of five coef5().
+__device__ __forceinline__ double adj_diff_at_tab(const Mesh &m, const DiffCoef &dc, const PairTables &pt,
+                                                  const double *__restrict__ w, int j, int k, int i, double gn,
+                                                  double gs, double bcn, double bcs) {
+  const int ntm = m.ntm;
+  const double *R = pt.row + (int64_t)(i - 1) * 3 * pt.LR;  // entry jj holds row jj-1
+  const double2 *P = reinterpret_cast<const double2 *>(pt.col) + (int64_t)(i - 1) * pt.LC;
+  double r = 0.0;
+  if (j >= 2 && j <= ntm - 1) {
+    const int kp = core_wrap(m, k + 1), km = core_wrap(m, k - 1);
+    const double sj = R[j + 1], c2 = R[pt.LR + j + 1], c4 = R[2 * pt.LR + j + 1];
+    const double2 Pk = P[k];
+    const double c1 = Pk.x * sj * sj, c5 = Pk.y * sj * sj;
+    const double c3 = -(c1 + c2 + c4 + c5);
+    r += c3 * w[fidx(m, j, k, i)];
+    r += (P[kp].x * sj * sj) * w[fidx(m, j, kp, i)];
+    r += (P[km].y * sj * sj) * w[fidx(m, j, km, i)];
+    if (j + 1 <= ntm - 1) r += R[pt.LR + j + 2] * w[fidx(m, j + 1, k, i)];
+    if (j - 1 >= 2) r += R[2 * pt.LR + j] * w[fidx(m, j - 1, k, i)];
+    if (j == 2) r += (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
+    if (j == ntm - 1) r += (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
+  } else if (j == 1) {
+    r += R[pt.LR + 3] * w[fidx(m, 2, k, i)];
+    r -= (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
+  } else {
+    r += R[2 * pt.LR + ntm] * w[fidx(m, ntm - 1, k, i)];
+    r -= (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
+  }
+  return r;
+}
+
 // One reverse RKG2 stage (or a plain A^T application), per core cell:
 //   out = a*w + b*wp + c*(A^T w);   ub += c0*w;   db += g*w;
 // dpart[block] += dscale * (block sum of (A^T w)*y) (the diffusion-
@@ -81,7 +116,8 @@ struct AdjDiffCoef {
 __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const double *__restrict__ w, const double *wp,
                                                   const double *__restrict__ y, double *out, double *ub, double *db,
                                                   const double *__restrict__ gin, int npin, double *__restrict__ gout,
-                                                  double bcn, double bcs, AdjDiffCoef ac, double *__restrict__ dpart) {
+                                                  double bcn, double bcs, AdjDiffCoef ac, double *__restrict__ dpart,
+                                                  PairTables pt) {
   __shared__ double sh[64];
   __shared__ double s_g[2];
   __shared__ double s_n[8], s_s[8];
@@ -91,15 +127,22 @@ __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const dou
   const int j0 = blockIdx.x * blockDim.x + 1, j1 = j0 + blockDim.x - 1;
   const bool need = (j0 <= 2) || (j1 >= m.ntm - 1);  // rows 1, 2, ntm-1, ntm use the pole sums
   if (need) {
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
+    if (threadIdx.y == 0) {  // one warp: lane-strided sums, then a fixed shuffle tree
       double a = 0.0, b = 0.0;
       const double *g = gin + (int64_t)(i - 1) * npin * 2;
-      for (int q = 0; q < npin; ++q) {
+      for (int q = threadIdx.x; q < npin; q += 32) {
         a = a + g[2 * q];
         b = b + g[2 * q + 1];
       }
-      s_g[0] = a;
-      s_g[1] = b;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+      }
+      if (threadIdx.x == 0) {
+        s_g[0] = a;
+        s_g[1] = b;
+      }
     }
     __syncthreads();
   }
@@ -108,7 +151,8 @@ __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const dou
   if (active) {
     const int64_t q = fidx(m, j, k, i);
     const double gn = need ? s_g[0] : 0.0, gs = need ? s_g[1] : 0.0;
-    const double aw = adj_diff_at(m, dc, w, j, k, i, gn, gs, bcn, bcs);
+    const double aw = pt.row ? adj_diff_at_tab(m, dc, pt, w, j, k, i, gn, gs, bcn, bcs)
+                             : adj_diff_at(m, dc, w, j, k, i, gn, gs, bcn, bcs);
     const double wq = w[q];
     o = ac.a * wq + ac.c * aw;
     if (wp) o += ac.b * wp[q];

@@ -2262,7 +2262,7 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
                    AdjDiffCoef ac) -> int {
     double *gout = h->d_gpart[pp];
     k_adj_diff<<<grd, blk, 0, h->stream>>>(h->M, h->DC, w, wp, y, out, u, d, gin, npin, gout, h->bc_diff_n,
-                                           h->bc_diff_s, ac, h->d_dpart);
+                                           h->bc_diff_s, ac, h->d_dpart, h->ptab);
     LAUNCHED(h);
     gin = gout;
     npin = (int)grd.y;
