@@ -2066,7 +2066,14 @@ extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, in
   m.plane = (int64_t)ldt * npm;
   k_flux_partial<<<dim3((unsigned)nb, (unsigned)nr), 256, 0, s>>>(m, dat, dap, f_dev, 0, part, cpb);
   k_na_flux_final<<<(nr + 127) / 128, 128, 0, s>>>(nb, nr, part, out);
-  if (cudaPeekAtLastError() != cudaSuccess) return na_fail(err, err_len, HIPFT_ECUDA, "kernel launch failed");
+  {
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+      char msg[256];
+      std::snprintf(msg, sizeof msg, "kernel launch failed: %s", cudaGetErrorString(le));
+      return na_fail(err, err_len, HIPFT_ECUDA, msg);
+    }
+  }
   if (cudaMemcpy2DAsync(flux_p, sizeof(double), out, 2 * sizeof(double), sizeof(double), (size_t)nr,
                         cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaMemcpy2DAsync(flux_m, sizeof(double), out + 1, 2 * sizeof(double), sizeof(double), (size_t)nr,

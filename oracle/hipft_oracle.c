@@ -1816,3 +1816,24 @@ int orc_da_blend(const orc_params *P, int ntm, int npm1, const double *t, const 
   da_blend(S, map3);
   return 0;
 }
+
+/* get_flux (F:8672-8750) of every realization of f (ntm, npm1+1, nr), theta
+ * fastest, on the mesh of the scales t[ntm], p[npm1] (test entry point).
+ * flux_p, flux_m receive nr values each.  Returns 0 on success. */
+int orc_get_flux(int ntm, int npm1, int nr, const double *t, const double *p, const double *f, double *flux_p,
+                 double *flux_m) {
+  orc Sx;
+  orc *S = &Sx;
+  memset(S, 0, sizeof(*S));
+  S->nr = nr;
+  S->ntm1 = ntm; S->npm1 = npm1;
+  S->ntm = ntm; S->npm = npm1 + 1; S->nt = ntm + 1; S->np = npm1 + 1;
+  S->t = dalloc(ntm); S->p = dalloc(S->npm);
+  for (int j = 1; j <= ntm; j++) V1(S->t, j) = t[j - 1];
+  for (int k = 1; k <= npm1; k++) V1(S->p, k) = p[k - 1];
+  V1(S->p, npm1 + 1) = V1(S->p, 2) + twopi;
+  if (set_mesh(S)) return -1;
+  for (int i = 0; i < nr; i++)
+    get_flux(S, f + (size_t)i * ntm * S->npm, &flux_p[i], &flux_m[i]);
+  return 0;
+}

@@ -338,6 +338,23 @@ def da_blend(p: dict, t, ph, f, map3):
     return f
 
 
+def get_flux(t, ph, f):
+    """get_flux of every realization of f (nr, npm, ntm) on the mesh of the
+    scales t (ntm) and ph (npm1); returns (flux_p, flux_m), nr values each."""
+    L = lib()
+    L.orc_get_flux.restype = ctypes.c_int
+    L.orc_get_flux.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 5
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    ph = np.ascontiguousarray(ph, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    nr = f.shape[0]
+    assert f.shape[1:] == (len(ph) + 1, len(t))
+    fp, fm = np.zeros(nr), np.zeros(nr)
+    if L.orc_get_flux(len(t), len(ph), nr, _ptr(t), _ptr(ph), _ptr(f), _ptr(fp), _ptr(fm)):
+        raise RuntimeError("oracle get_flux failed")
+    return fp, fm
+
+
 def read_history(path: str) -> np.ndarray:
     """Read a hipft_history_{sol,num}_rNNNNNN.out file into an array."""
     rows = []

@@ -1,8 +1,9 @@
 """Testsuite cases, golden histories and comparison helpers for the tests.
 
-Inputs and golden rows come from the reference testsuite when its tree is
-present, otherwise from the fixtures under tests/golden (made by
-tests/golden/make_golden.py).
+Inputs and golden rows come from the fixtures under tests/golden (made by
+tests/golden/make_golden.py from the reference's testsuite).  Setting
+HIPFT_TESTSUITE to the reference's testsuite directory reads the original
+files instead.
 """
 from __future__ import annotations
 
@@ -14,7 +15,7 @@ import numpy as np
 from oracle import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/testsuite"
+REF = os.environ.get("HIPFT_TESTSUITE", "")
 CASES = ["advect_gaussians_phi", "advect_gaussians_theta", "advect_gaussians_phi_theta", "diffuse_soccer",
          "diffuse_advect_soccer", "diffuse_dipole", "diffuse_advect_atten_map_1cr"]
 # Agreement with the golden histories (column max-norm relative error).
@@ -33,8 +34,8 @@ RSUN_CM2 = 4.84416e21
 
 
 def input_dir(case: str) -> str:
-    d = os.path.join(REF, case, "input")
-    return d if os.path.isdir(d) else os.path.join(HERE, "golden", case)
+    d = os.path.join(REF, case, "input") if REF else ""
+    return d if d and os.path.isdir(d) else os.path.join(HERE, "golden", case)
 
 
 def params(case: str) -> dict:
@@ -44,8 +45,8 @@ def params(case: str) -> dict:
 
 def golden(case: str):
     """(row_indices, sol[nr, rows, 16], num[nr, rows, 8], total_rows)."""
-    d = os.path.join(REF, case, "reference")
-    if os.path.isdir(d):
+    d = os.path.join(REF, case, "reference") if REF else ""
+    if d and os.path.isdir(d):
         sol, num = [], []
         r = 1
         while os.path.exists(os.path.join(d, f"hipft_history_sol_r{r:06d}.out")):

@@ -52,6 +52,39 @@ def test_noalloc_flux_matches_handle_twice():
             np.testing.assert_allclose(fm, fm_ref, rtol=RTOL, atol=0)
 
 
+def test_noalloc_flux_matches_oracle_refined_theta():
+    """Independent check on a nonuniform theta scale (spacing halved near the
+    poles): the entry point against the oracle's get_flux, two calls in a row."""
+    import torch
+    from hipft_b200 import gpu
+    from hipft_b200 import synthetic as S
+    from oracle import oracle as O
+
+    L = gpu.lib()
+    ntm, npm1, nr = 200, 257, 4
+    t = S.refined_theta(ntm)
+    p = S.uniform_phi(npm1)
+    npm = npm1 + 1
+    ldt = 208
+    rng = np.random.default_rng(5)
+    stream = torch.cuda.current_stream()
+    for shift in (0.2, -0.7):
+        f = rng.normal(size=(nr, npm, ntm)) + shift
+        f[:, 0, :] = f[:, npm - 2, :]
+        f[:, npm - 1, :] = f[:, 1, :]
+        fp_ref, fm_ref = O.get_flux(t, p, f)
+        dev = torch.zeros((nr, npm, ldt), dtype=torch.float64, device="cuda")
+        dev[:, :, :ntm] = torch.from_numpy(f).cuda()
+        stream.synchronize()
+        fp, fm = np.full(nr, np.nan), np.full(nr, np.nan)
+        err = ctypes.create_string_buffer(256)
+        rc = L.hipft_get_flux_noalloc(ctypes.c_void_p(dev.data_ptr()), ntm, npm1, nr, ldt, _dp(t), _dp(p),
+                                      _dp(fp), _dp(fm), ctypes.c_void_p(stream.cuda_stream), err, 256)
+        assert rc == 0, err.value.decode()
+        np.testing.assert_allclose(fp, fp_ref, rtol=RTOL, atol=0)
+        np.testing.assert_allclose(fm, fm_ref, rtol=RTOL, atol=0)
+
+
 def test_noalloc_rejects_oversize_grid():
     import torch
     from hipft_b200 import gpu
