@@ -110,6 +110,19 @@ struct hipft_gpu {
   double *adjw[8] = {};
   double *d_dpart = nullptr, *d_gring = nullptr, *d_gpart[2] = {};
   int dpart_per_r = 0;
+  // ragged batches: every realization keeps the schedule it would have if run
+  // alone (Euler limit, CFL substeps, PTL subcycles, stage counts)
+  bool ragged = false;
+  std::vector<double> r_dt_euler, r_dtmax;
+  bool r_dtmax_valid = false;
+  int *d_rlist_dif = nullptr, *d_rlist_adv = nullptr;  // [nr] realization lists of the launches
+  StageCoef *d_rcoef = nullptr;                         // [pairs][nr][2] coefficients of a super-step
+  size_t rcoef_pairs = 0;
+  StageCoef *d_r1coef = nullptr;                        // [nr] stage-1 coefficients
+  double *d_rdt = nullptr;                              // [nr] advection substeps
+  unsigned long long *d_rbits = nullptr;                // [2*nr] per-realization reductions
+  std::vector<int64_t> r_s, r_cycles, r_substeps;       // the last step's schedule
+  int64_t rkg2_cell_stages = 0;  // unique cells x stages k >= 2 advanced (both modes)
   hipft_allreduce_cb red_cb = nullptr;  // scalar all-reduce over ranks (plain-mode sharding)
   void *red_user = nullptr;
   PoleScratch pole{};       // chunk shares of the ring sums for k_pair_poles
@@ -788,6 +801,8 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
       cudaFuncSetAttribute(k_sts_pair_ws<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_sts_pair_ws<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kWSmem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_sts_pair_ws<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kWSmem) != cudaSuccess)
     return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernels"));
   if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->num_sms < 1)
@@ -1235,6 +1250,7 @@ extern "C" int hipft_gpu_update_flow(hipft_gpu *h, int *updated) {
     h->FL.vt = h->d_vt; h->FL.vp = h->d_vp; h->FL.at = h->d_at; h->FL.ap = h->d_ap;
     h->FL.flow2d = 1;
   }
+  h->r_dtmax_valid = false;
   if (updated) *updated = 1;
   return HIPFT_OK;
 }
@@ -1260,11 +1276,9 @@ extern "C" int hipft_gpu_flow_dtmax(hipft_gpu *h, double *dtmax) {
 }
 
 // ------------------------------------------------------------- advection
-extern "C" int hipft_gpu_advection_step(hipft_gpu *h, double dt) {
-  if (!h) return HIPFT_EINVAL;
-  if (!h->field_set) return fail(h, HIPFT_ESTATE, "advection_step before set_field");
-  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "advection_step: advance_flow is off");
-  CK(h, cudaSetDevice(h->dev));
+static int ragged_advection_step(hipft_gpu *h, double dt);
+
+static int plain_advection_step(hipft_gpu *h, double dt) {
   h->dring_valid = false;
   double *f = h->buf[h->cur];
   int ia = scratch(h, 0), ib = scratch(h, 1);
@@ -1285,20 +1299,34 @@ extern "C" int hipft_gpu_advection_step(hipft_gpu *h, double dt) {
   return HIPFT_OK;
 }
 
+extern "C" int hipft_gpu_advection_step(hipft_gpu *h, double dt) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "advection_step before set_field");
+  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "advection_step: advance_flow is off");
+  CK(h, cudaSetDevice(h->dev));
+  if (h->ragged) return ragged_advection_step(h, dt);
+  return plain_advection_step(h, dt);
+}
+
 // ------------------------------------------------------------- diffusion
-// load_sts_rkl2 / load_sts_rkg2 (src/hipft.f90:5244-5475).
-static void load_sts(hipft_gpu *h, double dtl) {
+// Stage count and coefficients of one RKL2 (method 2) or RKG2 (method 3)
+// super-step, load_sts_rkl2 / load_sts_rkg2 (src/hipft.f90:5244-5475).
+struct StsTable {
+  int64_t s = 0;
+  std::vector<double> uj, vj, ubj, gj, b;
+};
+static void sts_coefs(int method, double dtl, double dt_euler, StsTable &T) {
   int64_t s;
-  if (h->P.diffusion_num_method == 2)
-    s = (int64_t)std::ceil(0.5 * (std::sqrt(9.0 + 16.0 * (dtl / h->dt_euler)) - 1.0));
+  if (method == 2)
+    s = (int64_t)std::ceil(0.5 * (std::sqrt(9.0 + 16.0 * (dtl / dt_euler)) - 1.0));
   else
-    s = (int64_t)std::ceil(0.5 * (std::sqrt(25.0 + 24.0 * (dtl / h->dt_euler)) - 3.0));
+    s = (int64_t)std::ceil(0.5 * (std::sqrt(25.0 + 24.0 * (dtl / dt_euler)) - 3.0));
   if (s < 3) s = 3;
   if (s % 2 == 0) s = s + 1;
-  h->sts_s = s;
-  auto &b = h->sts_b, &uj = h->sts_uj, &vj = h->sts_vj, &ubj = h->sts_ubj, &gj = h->sts_gj;
+  T.s = s;
+  auto &b = T.b, &uj = T.uj, &vj = T.vj, &ubj = T.ubj, &gj = T.gj;
   b.assign(s + 1, 0); uj.assign(s + 1, 0); vj.assign(s + 1, 0); ubj.assign(s + 1, 0); gj.assign(s + 1, 0);
-  if (h->P.diffusion_num_method == 2) {
+  if (method == 2) {
     double w = 4.0 / (double)(s * s + s - 2);
     b[1] = 1.0 / 3.0; b[2] = 1.0 / 3.0;
     uj[1] = -9999.0; vj[1] = -9999.0; ubj[1] = 4.0 / (3.0 * (double)(s * s + s - 2)); gj[1] = -9999.0;
@@ -1326,6 +1354,24 @@ static void load_sts(hipft_gpu *h, double dtl) {
       gj[j] = (0.5 * (double)j * ((double)j + 1.0) * b[j - 1] - 1.0) * ubj[j];
     }
   }
+}
+
+// The stage-k combine coefficients of a super-step of length dtl
+// (src/hipft.f90:5224-5235).
+static StageCoef sts_stage_coef(const StsTable &T, int64_t k, double dtl) {
+  double uj = T.uj[k], vj = T.vj[k];
+  return StageCoef{uj, vj, 1.0 - uj - vj, T.ubj[k] * dtl, T.gj[k]};
+}
+
+static void load_sts(hipft_gpu *h, double dtl) {
+  StsTable T;
+  sts_coefs(h->P.diffusion_num_method, dtl, h->dt_euler, T);
+  h->sts_s = T.s;
+  h->sts_b = std::move(T.b);
+  h->sts_uj = std::move(T.uj);
+  h->sts_vj = std::move(T.vj);
+  h->sts_ubj = std::move(T.ubj);
+  h->sts_gj = std::move(T.gj);
 }
 
 // diffusion_step_sts_cd (src/hipft.f90:5163-5242): stage 1 then the
@@ -1366,6 +1412,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
       ykm1 = bk1;
       k += 2;
       h->rkg2_stages += 2;
+      h->rkg2_cell_stages += 2 * (int64_t)h->ntm * (h->npm - 2) * h->nr;
       continue;
     }
     int out = (ykm2 == u0) ? free_buf(-1) : ykm2;
@@ -1382,6 +1429,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
     ykm1 = out;
     k += 1;
     h->rkg2_stages += 1;
+    h->rkg2_cell_stages += (int64_t)h->ntm * (h->npm - 2) * h->nr;
   }
   h->cur = ykm1;
   h->dring_valid = fused;  // the last fused stage left the ring of the new field
@@ -1460,12 +1508,439 @@ static int ptl_dt(hipft_gpu *h, double *dtl) {
   return HIPFT_OK;
 }
 
+// ================================================================ ragged
+// Ragged batches (no counterpart in the reference, which keeps one dt, one
+// Euler limit, one stage count and one PTL subcycle sequence for all
+// realizations through global MIN/MAX reductions, src/hipft.f90:5036, 5103,
+// 5141, 7345).  In a ragged batch every realization gets the schedule it would
+// have if it were run alone: its own Gershgorin limit, its own PTL subcycles
+// and RKG2/RKL2 stage counts, and, when the step is longer than its own CFL
+// limit, its own number of advection substeps.  Launches still cover many
+// realizations at once: a launch walks a list of realizations sorted by the
+// work they still need, and the realizations that are done drop off its end.
+
+// per-realization Euler limits, get_dtime_diffusion_euler (src/hipft.f90:
+// 5019-5025) of each realization alone
+static int ragged_gershgorin(hipft_gpu *h) {
+  const int nr = h->nr;
+  CK(h, cudaMemsetAsync(h->d_rbits, 0, sizeof(unsigned long long) * nr, h->stream));
+  dim3 blk(32, 8);
+  dim3 grd((unsigned)((h->ntm - 2 + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)nr);
+  k_gershgorin<<<grd, blk, 0, h->stream>>>(h->M, h->DC, h->d_rbits, 1);
+  LAUNCHED(h);
+  std::vector<unsigned long long> bits(nr);
+  CK(h, cudaMemcpyAsync(bits.data(), h->d_rbits, sizeof(unsigned long long) * nr, cudaMemcpyDeviceToHost,
+                        h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->r_dt_euler.assign(nr, 0.0);
+  for (int i = 0; i < nr; ++i) {
+    double max_eig;
+    std::memcpy(&max_eig, &bits[i], 8);
+    h->r_dt_euler[i] = c_safety * (2.0 / max_eig);
+  }
+  return HIPFT_OK;
+}
+
+// per-realization CFL limits, get_flow_dtmax (src/hipft.f90:7287-7350) of each
+// realization alone
+static int ragged_dtmax(hipft_gpu *h) {
+  if (h->r_dtmax_valid) return HIPFT_OK;
+  const int nr = h->nr;
+  std::vector<unsigned long long> bits(nr, 0x7fefffffffffffffULL);
+  CK(h, cudaMemcpyAsync(h->d_rbits, bits.data(), sizeof(unsigned long long) * nr, cudaMemcpyHostToDevice,
+                        h->stream));
+  dim3 blk(32, 8), grd((unsigned)((h->ntm - 2 + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)nr);
+  k_flow_dtmax<<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->d_rbits, 1);
+  LAUNCHED(h);
+  CK(h, cudaMemcpyAsync(bits.data(), h->d_rbits, sizeof(unsigned long long) * nr, cudaMemcpyDeviceToHost,
+                        h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  h->r_dtmax.assign(nr, 0.0);
+  for (int i = 0; i < nr; ++i) {
+    double d;
+    std::memcpy(&d, &bits[i], 8);
+    d = c_safety * d;
+    if (h->P.strang_splitting) d = 2.0 * d;
+    if (h->adv_time == 3) d = 2.0 * d;
+    h->r_dtmax[i] = d;
+  }
+  h->r_dtmax_valid = true;
+  return HIPFT_OK;
+}
+
+// realizations `act` ordered by decreasing work (ties by index), uploaded
+static int upload_list(hipft_gpu *h, int *dlist, std::vector<int> &act, const std::vector<int64_t> &work) {
+  std::stable_sort(act.begin(), act.end(), [&](int a, int b) { return work[a] > work[b]; });
+  CK(h, cudaMemcpyAsync(dlist, act.data(), sizeof(int) * act.size(), cudaMemcpyHostToDevice, h->stream));
+  return HIPFT_OK;
+}
+
+// PTL time steps (src/hipft.f90:5042-5161) of the realizations in `act`,
+// each from its own max |Af| and its own argmax cells; dtl[i] is the
+// realization's previous subcycle (the floor), replaced by the new one.
+static int ragged_ptl(hipft_gpu *h, std::vector<int> act, std::vector<double> &dtl) {
+  const int nr = h->nr, na = (int)act.size();
+  std::vector<int64_t> none(nr, 0);
+  TRY(upload_list(h, h->d_rlist_dif, act, none));
+  std::vector<unsigned long long> init(2 * (size_t)nr, 0ULL);
+  for (int i = 0; i < nr; ++i) init[nr + i] = 0x7fefffffffffffffULL;
+  CK(h, cudaMemcpyAsync(h->d_rbits, init.data(), sizeof(unsigned long long) * 2 * nr, cudaMemcpyHostToDevice,
+                        h->stream));
+  double *f = h->buf[h->cur], *af = h->buf[scratch(h, 0)];
+  const double *ring;
+  TRY(current_dring(h, &ring));
+  dim3 blk(32, 8);
+  dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)na);
+  {
+    ProfScope ps(h, HIPFT_K_OTHER);
+    k_diffusion_stage<MODE_AX><<<grd, blk, 0, h->stream>>>(h->M, h->DC, f, nullptr, nullptr, nullptr, af, nullptr,
+                                                          ring, h->bc_diff_n, h->bc_diff_s, StageCoef{}, h->d_rbits,
+                                                          h->d_rlist_dif, 1);
+    LAUNCHED(h);
+    k_ptl<<<grd, blk, 0, h->stream>>>(h->M, f, af, h->d_rbits, h->d_rbits + nr, h->d_rlist_dif, 1);
+    LAUNCHED(h);
+  }
+  std::vector<unsigned long long> bits(2 * (size_t)nr);
+  CK(h, cudaMemcpyAsync(bits.data(), h->d_rbits, sizeof(unsigned long long) * 2 * nr, cudaMemcpyDeviceToHost,
+                        h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  for (int i : act) {
+    double axabsmax, ptl;
+    std::memcpy(&axabsmax, &bits[i], 8);
+    std::memcpy(&ptl, &bits[nr + i], 8);
+    double d = DBL_MAX;
+    if (axabsmax > 0.0) {
+      d = 0.95 * ptl;
+      if (d < dtl[i]) d = dtl[i];
+    }
+    dtl[i] = d;
+  }
+  return HIPFT_OK;
+}
+
+// Two-stage launch of a ragged super-step: the first n realizations of the
+// list d_rlist_dif, coefficients rc ([nr][2]).
+static int sts_pair_ragged(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0,
+                           const double *dty0, double *out_k, double *out_k1, int n, const StageCoef *rc,
+                           bool overlap_prev) {
+  const int nkt = (h->npm - 2 + kWK - 1) / kWK;
+  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
+  PairTables pt = h->ptab;
+  pt.ntiles = pt.nb * pt.nkt * n;
+  const int grid = std::min(pt.ntiles, 2 * h->num_sms);
+  PairArgs pa{StageCoef{}, StageCoef{}, h->d_err, h->d_rlist_dif, rc};
+  const double *rin = h->d_ringbuf[h->ring_cur];
+  const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
+  {
+    ProfScope ps(h, HIPFT_K_STS);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kWThreads);
+    cfg.dynamicSmemBytes = kWSmem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true, false, true>, h->M,
+                                        (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, rin,
+                                        h->bc_diff_n, h->bc_diff_s, pa, ro, pt, tmaps);
+    if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws (ragged) launch: %s", cudaGetErrorString(le));
+    LAUNCHED(h);
+    dim3 pg((unsigned)n, (unsigned)h->pole_nch);
+    k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
+                                                     h->bc_diff_n, h->bc_diff_s, pa, ro, h->pole);
+    LAUNCHED(h);
+  }
+  h->ring_cur = 1 - h->ring_cur;
+  return HIPFT_OK;
+}
+
+// One RKG2/RKL2 super-step of every realization in `act`, realization i over
+// dtl[i] with its own stage count s_i (src/hipft.f90:5163-5242 per
+// realization).  The launch of stage pair p covers the realizations with
+// s_i >= 2p + 3; afterwards every realization's field is gathered into one
+// buffer, which becomes the current field.
+static int ragged_super_step(hipft_gpu *h, std::vector<int> act, const std::vector<double> &dtl) {
+  const int nr = h->nr, method = h->P.diffusion_num_method;
+  std::vector<StsTable> T(nr);
+  std::vector<int64_t> s(nr, 0);
+  int64_t smax = 0;
+  for (int i : act) {
+    sts_coefs(method, dtl[i], h->r_dt_euler[i], T[i]);
+    s[i] = T[i].s;
+    h->r_s[i] = T[i].s;
+    smax = std::max(smax, s[i]);
+  }
+  TRY(upload_list(h, h->d_rlist_dif, act, s));
+  const int na = (int)act.size();
+  const int64_t npairs = (smax - 1) / 2;  // s is odd: stages 2..s are (s-1)/2 pairs
+  // stage-1 and pair coefficients, per realization
+  std::vector<StageCoef> c1(nr, StageCoef{});
+  for (int i : act) c1[i] = StageCoef{dtl[i], T[i].ubj[1], 0, 0, 0};
+  CK(h, cudaMemcpyAsync(h->d_r1coef, c1.data(), sizeof(StageCoef) * nr, cudaMemcpyHostToDevice, h->stream));
+  if ((size_t)npairs > h->rcoef_pairs) {
+    if (h->d_rcoef) {
+      CK(h, cudaStreamSynchronize(h->stream));
+      cudaFree(h->d_rcoef);
+      h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)h->d_rcoef), h->allocs.end());
+      h->d_rcoef = nullptr;
+    }
+    const size_t cap = (size_t)npairs + 64;
+    TRY(dalloc(h, &h->d_rcoef, cap * nr * 2));
+    h->rcoef_pairs = cap;
+  }
+  std::vector<StageCoef> pc((size_t)npairs * nr * 2, StageCoef{});
+  for (int i : act)
+    for (int64_t q = 0; q < (s[i] - 1) / 2; ++q) {
+      const int64_t k = 2 + 2 * q;
+      pc[((size_t)q * nr + i) * 2] = sts_stage_coef(T[i], k, dtl[i]);
+      pc[((size_t)q * nr + i) * 2 + 1] = sts_stage_coef(T[i], k + 1, dtl[i]);
+    }
+  CK(h, cudaMemcpyAsync(h->d_rcoef, pc.data(), sizeof(StageCoef) * pc.size(), cudaMemcpyHostToDevice, h->stream));
+
+  const int u0 = h->cur, idty = scratch(h, 0), ia = scratch(h, 1);
+  const double *r0;
+  TRY(current_dring(h, &r0));
+  {
+    // stage 1 (src/hipft.f90:5211-5218) of every realization in the list
+    const int nkb = (h->npm - 2 + kKPT3 - 1) / kKPT3;
+    RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkb};
+    const int jshift = (h->ntm % 2 == 1 && ((h->ntm - 1) / 2) % 32 == 0) ? 1 : 0;
+    const int nthr = (h->ntm + 2 * jshift + 1) / 2;
+    dim3 grd((unsigned)((nthr + 127) / 128), (unsigned)nkb, (unsigned)na);
+    ProfScope ps(h, HIPFT_K_OTHER);
+    k_sts_stage_v3<MODE_STS1, kKPT3><<<grd, 128, 0, h->stream>>>(
+        h->M, h->DC.dfac, h->buf[u0], nullptr, nullptr, nullptr, h->buf[ia], h->buf[idty], h->d_ringbuf[h->ring_cur],
+        h->bc_diff_n, h->bc_diff_s, StageCoef{}, ro, jshift, h->d_rlist_dif, h->d_r1coef);
+    LAUNCHED(h);
+    h->ring_cur = 1 - h->ring_cur;
+  }
+  int ykm1 = ia, ykm2 = u0;
+  auto free_buf = [&](int avoid) {
+    for (int b = 0; b < kNBuf; ++b)
+      if (b != u0 && b != idty && b != ykm1 && b != ykm2 && b != avoid) return b;
+    return -1;
+  };
+  std::vector<int> fin(nr, u0);  // buffer holding each realization's result
+  const int64_t cells = (int64_t)h->ntm * (h->npm - 2);
+  for (int64_t q = 0; q < npairs; ++q) {
+    int n = 0;
+    while (n < na && (s[act[n]] - 1) / 2 > q) ++n;
+    const int bk = free_buf(-1), bk1 = free_buf(bk);
+    TRY(sts_pair_ragged(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[bk], h->buf[bk1], n,
+                        h->d_rcoef + (size_t)q * nr * 2, q > 0));
+    for (int e = 0; e < n; ++e)
+      if ((s[act[e]] - 1) / 2 == q + 1) fin[act[e]] = bk1;
+    ykm2 = bk;
+    ykm1 = bk1;
+    h->rkg2_stages += 2;
+    h->rkg2_cell_stages += 2 * cells * n;
+  }
+  // gather: realizations that finished earlier, and those not in this
+  // super-step at all (still in u0), into the last pair's output
+  const int dst = ykm1;
+  const size_t pbytes = (size_t)h->plane * sizeof(double);
+  for (int i = 0; i < nr; ++i)
+    if (fin[i] != dst)
+      CK(h, cudaMemcpyAsync(h->buf[dst] + (size_t)i * h->plane, h->buf[fin[i]] + (size_t)i * h->plane, pbytes,
+                            cudaMemcpyDeviceToDevice, h->stream));
+  h->cur = dst;
+  h->dring_valid = false;  // the ring sums of the finished realizations sit in either buffer
+  int64_t tot = 0;
+  for (int i : act) tot += s[i];
+  h->cell_updates += cells * tot;
+  return HIPFT_OK;
+}
+
+// diffusion_step (src/hipft.f90:4551-4695) with every realization's own
+// subcycle sequence (PTL) and stage counts.
+static int ragged_diffusion_step(hipft_gpu *h, double dtl, hipft_diffusion_info *info) {
+  const int nr = h->nr, max_sc = 60;
+  const int64_t stages0 = h->cell_updates;
+  std::vector<double> ts(nr, 0.0), d(nr, h->auto_sc ? 0.0 : dtl / (double)h->P.diffusion_subcycles);
+  std::vector<int> act(nr);
+  for (int i = 0; i < nr; ++i) act[i] = i;
+  h->r_s.assign(nr, 0);
+  h->r_cycles.assign(nr, 0);
+  int cyc = 1;
+  int64_t smax = 0;
+  while (!act.empty()) {
+    if (h->auto_sc) TRY(ragged_ptl(h, act, d));
+    std::vector<int> done;
+    for (int i : act) {
+      bool fin = false;
+      if (h->auto_sc && ts[i] + d[i] >= dtl) {
+        d[i] = dtl - ts[i];
+        fin = true;
+      }
+      if (h->auto_sc && cyc == max_sc - 1) {
+        d[i] = dtl - ts[i];
+        fin = true;
+      }
+      if (!h->auto_sc && cyc == h->P.diffusion_subcycles) fin = true;
+      if (fin) done.push_back(i);
+    }
+    TRY(ragged_super_step(h, act, d));
+    for (int i : act) {
+      ts[i] = ts[i] + d[i];
+      h->r_cycles[i] = cyc;
+      smax = std::max(smax, h->r_s[i]);
+    }
+    std::vector<int> next;
+    for (int i : act)
+      if (std::find(done.begin(), done.end(), i) == done.end()) next.push_back(i);
+    act.swap(next);
+    cyc = cyc + 1;
+  }
+  TRY(check_wait_flag(h, "diffusion_step: a bounded wait for staged tiles gave up"));
+  h->sts_s = smax;
+  h->subcycles_state = cyc - 1;
+  if (info) {
+    info->dtime_diffusion_euler = *std::min_element(h->r_dt_euler.begin(), h->r_dt_euler.end());
+    info->sts_s = smax;
+    info->subcycles = cyc - 1;
+    const int64_t cells = (int64_t)h->ntm * (h->npm - 2) * h->nr;
+    info->total_stages = cells ? (h->cell_updates - stages0) / cells : 0;
+  }
+  return HIPFT_OK;
+}
+
+// advection_step (src/hipft.f90:4509-4549) with every realization's own
+// substep count: realization i takes n_i = ceil(dt / its own CFL limit)
+// substeps of dt / n_i (one substep when dt is within its limit, which is
+// the plain step).
+static int advection_stage_ragged(hipft_gpu *h, const double *x, const double *f0, double *out, AdvCombine cb,
+                                  int n) {
+  {
+    ProfScope ps(h, HIPFT_K_RING);
+    k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
+    LAUNCHED(h);
+  }
+  dim3 blk(32, 8);
+  dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)n);
+  ProfScope ps(h, HIPFT_K_ADV);
+  if (h->adv_space == 2)
+    k_advection_stage<32, 8, true><<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
+                                                               h->bc_flow_s, cb, h->d_rlist_adv, h->d_rdt);
+  else
+    k_advection_stage<32, 8, false><<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out, h->d_ring,
+                                                                h->bc_flow_n, h->bc_flow_s, cb, h->d_rlist_adv,
+                                                                h->d_rdt);
+  LAUNCHED(h);
+  h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * n;
+  return HIPFT_OK;
+}
+
+static int plain_advection_step(hipft_gpu *h, double dt);
+
+static int ragged_advection_step(hipft_gpu *h, double dt) {
+  const int nr = h->nr;
+  TRY(ragged_dtmax(h));
+  // the CFL limit bounds a whole split step: a Strang half step may use half of it
+  const double scale = h->P.strang_splitting ? 2.0 : 1.0;
+  std::vector<int64_t> n(nr, 1);
+  int64_t nmax = 1;
+  for (int i = 0; i < nr; ++i) {
+    const double r = dt * scale / h->r_dtmax[i];
+    n[i] = (r > 1.0) ? (int64_t)std::ceil(r) : 1;
+    nmax = std::max(nmax, n[i]);
+  }
+  h->r_substeps = n;
+  if (nmax == 1) return plain_advection_step(h, dt);
+  std::vector<int> act(nr);
+  for (int i = 0; i < nr; ++i) act[i] = i;
+  TRY(upload_list(h, h->d_rlist_adv, act, n));
+  std::vector<double> rdt(nr);
+  for (int i = 0; i < nr; ++i) rdt[i] = dt / (double)n[i];
+  CK(h, cudaMemcpyAsync(h->d_rdt, rdt.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, h->stream));
+  h->dring_valid = false;
+  double *f = h->buf[h->cur];
+  double *A = h->buf[scratch(h, 0)], *B = h->buf[scratch(h, 1)];
+  for (int64_t q = 0; q < nmax; ++q) {
+    int na = 0;
+    while (na < nr && n[act[na]] > q) ++na;
+    if (h->adv_time == 2) {  // SSPRK(3,3) (src/hipft.f90:7486-7505)
+      TRY(advection_stage_ragged(h, f, nullptr, A, AdvCombine{0, 0.0, 0.0, 1.0}, na));
+      TRY(advection_stage_ragged(h, A, f, B, AdvCombine{1, c_three_quarter, c_quarter, c_quarter}, na));
+      TRY(advection_stage_ragged(h, B, f, f, AdvCombine{1, c_third, c_two_third, c_two_third}, na));
+    } else {  // SSPRK(4,3) (src/hipft.f90:7552-7574)
+      TRY(advection_stage_ragged(h, f, nullptr, A, AdvCombine{0, 0.0, 0.0, 0.5}, na));
+      TRY(advection_stage_ragged(h, A, nullptr, B, AdvCombine{0, 0.0, 0.0, 0.5}, na));
+      TRY(advection_stage_ragged(h, B, f, A, AdvCombine{1, c_two_third, c_third, c_sixth}, na));
+      TRY(advection_stage_ragged(h, A, nullptr, f, AdvCombine{0, 0.0, 0.0, 0.5}, na));
+    }
+  }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_set_ragged(hipft_gpu *h, int on) {
+  if (!h) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  if (!on) {
+    h->ragged = false;
+    return HIPFT_OK;
+  }
+  if (h->red_cb) return fail(h, HIPFT_ESTATE, "set_ragged: a ragged batch has no shared schedule to reduce over ranks");
+  if (h->P.advance_diffusion && (h->DC.grid || h->P.diffusion_num_method == 1))
+    return fail(h, HIPFT_EINVAL, "set_ragged: needs RKG2 or RKL2 with per-realization constant diffusion coefficients");
+  if (h->P.advance_flow && h->adv_time == 1)
+    return fail(h, HIPFT_EINVAL, "set_ragged: needs SSPRK(3,3) or SSPRK(4,3) advection");
+  const int nr = h->nr;
+  if (!h->d_rbits) {
+    TRY(dalloc(h, &h->d_rbits, 2 * (size_t)nr));
+    TRY(dalloc(h, &h->d_rlist_dif, (size_t)nr));
+    TRY(dalloc(h, &h->d_rlist_adv, (size_t)nr));
+    TRY(dalloc(h, &h->d_r1coef, (size_t)nr));
+    TRY(dalloc(h, &h->d_rdt, (size_t)nr));
+  }
+  if (h->P.advance_diffusion) TRY(ragged_gershgorin(h));
+  h->r_dtmax_valid = false;
+  h->r_s.assign(nr, 0);
+  h->r_cycles.assign(nr, 0);
+  h->r_substeps.assign(nr, 1);
+  h->ragged = true;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_flow_dtmax_each(hipft_gpu *h, double *dtmax) {
+  if (!h || !dtmax) return HIPFT_EINVAL;
+  if (!h->P.advance_flow) return fail(h, HIPFT_ESTATE, "flow_dtmax_each: advance_flow is off");
+  CK(h, cudaSetDevice(h->dev));
+  if (!h->d_rbits) {
+    TRY(dalloc(h, &h->d_rbits, 2 * (size_t)h->nr));
+    TRY(dalloc(h, &h->d_rlist_dif, (size_t)h->nr));
+    TRY(dalloc(h, &h->d_rlist_adv, (size_t)h->nr));
+    TRY(dalloc(h, &h->d_r1coef, (size_t)h->nr));
+    TRY(dalloc(h, &h->d_rdt, (size_t)h->nr));
+  }
+  h->r_dtmax_valid = false;
+  TRY(ragged_dtmax(h));
+  std::copy(h->r_dtmax.begin(), h->r_dtmax.end(), dtmax);
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_ragged_schedule(hipft_gpu *h, int64_t *sts_s, int64_t *subcycles, int64_t *adv_substeps,
+                                         double *dt_euler) {
+  if (!h) return HIPFT_EINVAL;
+  if (!h->ragged) return fail(h, HIPFT_ESTATE, "ragged_schedule: the handle is not in ragged mode");
+  for (int i = 0; i < h->nr; ++i) {
+    if (sts_s) sts_s[i] = h->r_s.empty() ? 0 : h->r_s[i];
+    if (subcycles) subcycles[i] = h->r_cycles.empty() ? 0 : h->r_cycles[i];
+    if (adv_substeps) adv_substeps[i] = h->r_substeps.empty() ? 1 : h->r_substeps[i];
+    if (dt_euler) dt_euler[i] = h->r_dt_euler.empty() ? 0.0 : h->r_dt_euler[i];
+  }
+  return HIPFT_OK;
+}
+
 extern "C" int hipft_gpu_diffusion_step(hipft_gpu *h, double dtl, hipft_cycle_cb cb, void *user,
                                         hipft_diffusion_info *info) {
   if (!h) return HIPFT_EINVAL;
   if (!h->field_set) return fail(h, HIPFT_ESTATE, "diffusion_step before set_field");
   if (!h->P.advance_diffusion) return fail(h, HIPFT_ESTATE, "diffusion_step: advance_diffusion is off");
   CK(h, cudaSetDevice(h->dev));
+  if (h->ragged) return ragged_diffusion_step(h, dtl, info);
   const int max_sc = 60;
   int64_t stages0 = h->cell_updates;
   int i = 1;
@@ -1851,6 +2326,7 @@ extern "C" int hipft_gpu_info(const hipft_gpu *h, hipft_info *info) {
   info->cell_stage_updates = h->cell_updates;
   info->device_bytes = h->dev_bytes;
   info->rkg2_stages = h->rkg2_stages;
+  info->rkg2_cell_stages = h->rkg2_cell_stages;
   return HIPFT_OK;
 }
 
@@ -2310,6 +2786,7 @@ extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, doubl
   if (h->P.advance_diffusion && (h->P.diffusion_num_method != 3 || h->DC.grid))
     return fail(h, HIPFT_ESTATE, "adjoint: diffusion must be RKG2 with per-realization constant coefficients");
   if (h->P.advance_source) return fail(h, HIPFT_ESTATE, "adjoint: sources are not differentiated");
+  if (h->ragged) return fail(h, HIPFT_ESTATE, "adjoint: replays the shared (plain) schedule only");
   CK(h, cudaSetDevice(h->dev));
   TRY(adj_ensure(h));
   const size_t bytes = h->fieldn * sizeof(double);

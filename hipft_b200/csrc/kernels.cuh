@@ -129,14 +129,17 @@ struct StageCoef {
   double a, b, c, d, e;  // meaning depends on the mode
 };
 
+// rlist (may be null): realization (0-based) of grid slice z, for ragged
+// batches that advance a subset; per_real: one max |Af| per realization.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_diffusion_stage(
     Mesh m, DiffCoef dc, const double *__restrict__ x, const double *ykm2, const double *__restrict__ u0,
     const double *__restrict__ dty0, double *out, double *out2, const double *__restrict__ ring, double bcn,
-    double bcs, StageCoef sc, unsigned long long *absmax_bits) {
+    double bcs, StageCoef sc, unsigned long long *absmax_bits, const int *__restrict__ rlist = nullptr,
+    int per_real = 0) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const int i = blockIdx.z + 1;
+  const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   double ax = 0.0;
   bool active = (j <= m.ntm && k <= m.npm - 1);
   int64_t q = 0;
@@ -178,18 +181,25 @@ __global__ void __launch_bounds__(256) k_diffusion_stage(
       unsigned long long t = __shfl_down_sync(0xffffffffu, b, o);
       b = t > b ? t : b;
     }
-    if ((threadIdx.x & 31) == 0 && b) atomicMax(absmax_bits, b);
+    if ((threadIdx.x & 31) == 0 && b) atomicMax(absmax_bits + (per_real ? i - 1 : 0), b);
   }
 }
 
-// PTL candidates at the argmax cells (src/hipft.f90:5108-5135).
+// PTL candidates at the argmax cells (src/hipft.f90:5108-5135).  With
+// per_real, each realization has its own maximum and its own minimum (ragged
+// batches); rlist as in k_diffusion_stage.
 __global__ void k_ptl(Mesh m, const double *__restrict__ f, const double *__restrict__ af,
-                      const unsigned long long *absmax_bits, unsigned long long *ptl_bits) {
+                      const unsigned long long *absmax_bits, unsigned long long *ptl_bits,
+                      const int *__restrict__ rlist = nullptr, int per_real = 0) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
-  const int i = blockIdx.z + 1;
+  const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   if (j < 2 || j > m.ntm - 1 || k > m.npm - 1) return;
   const double fmin_v = 1e-14;
+  if (per_real) {
+    absmax_bits += i - 1;
+    ptl_bits += i - 1;
+  }
   double axabsmax = __longlong_as_double(*absmax_bits);
   int64_t q = fidx(m, j, k, i);
   if (!(axabsmax == fabs(af[q]) && fabs(f[q]) > fmin_v)) return;
@@ -204,8 +214,9 @@ __global__ void k_ptl(Mesh m, const double *__restrict__ f, const double *__rest
   if (best < 1.7976931348623157e308) atomicMin(ptl_bits, (unsigned long long)__double_as_longlong(best));
 }
 
-// Gershgorin bound, get_dtime_diffusion_euler (src/hipft.f90:5019-5025).
-__global__ void k_gershgorin(Mesh m, DiffCoef dc, unsigned long long *max_bits) {
+// Gershgorin bound, get_dtime_diffusion_euler (src/hipft.f90:5019-5025);
+// per_real: one bound per realization (ragged batches).
+__global__ void k_gershgorin(Mesh m, DiffCoef dc, unsigned long long *max_bits, int per_real = 0) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int i = blockIdx.z + 1;
@@ -225,7 +236,7 @@ __global__ void k_gershgorin(Mesh m, DiffCoef dc, unsigned long long *max_bits) 
     unsigned long long t = __shfl_down_sync(0xffffffffu, b, o);
     b = t > b ? t : b;
   }
-  if ((threadIdx.x & 31) == 0 && b) atomicMax(max_bits, b);
+  if ((threadIdx.x & 31) == 0 && b) atomicMax(max_bits + (per_real ? i - 1 : 0), b);
 }
 
 // ------------------------------------------------------------ advection
@@ -346,18 +357,22 @@ struct AdvSmem {
 
 // One explicit advection stage over a tile: face fluxes (WENO3 or upwind),
 // divergence (src/hipft.f90:7890-7898), pole rows from the ring sums, seam,
-// and the integrator's combine.
+// and the integrator's combine.  Ragged batches: rlist (may be null) maps grid
+// slice z to a realization, and rdt (may be null) holds each realization's
+// substep, which multiplies cb.C.
 template <int TJ, int TK, bool WENO>
 __global__ void __launch_bounds__(TJ *TK) k_advection_stage(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
                                                             const double *__restrict__ f0, double *out,
                                                             const double *__restrict__ ring, double bcn, double bcs,
-                                                            AdvCombine cb) {
+                                                            AdvCombine cb, const int *__restrict__ rlist = nullptr,
+                                                            const double *__restrict__ rdt = nullptr) {
   __shared__ AdvSmem<TJ, TK> s;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + ty * TJ;
   const int j0 = blockIdx.x * TJ + 1;
   const int k0 = blockIdx.y * TK + 2;
-  const int i = blockIdx.z + 1;
+  const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
+  if (rdt) cb.C = cb.C * rdt[i - 1];
   const int ntm = m.ntm, npm = m.npm;
 
   // x tile with halo 2 (theta clipped to 1..ntm, phi wrapped periodically).
@@ -465,7 +480,8 @@ __global__ void __launch_bounds__(TJ *TK) k_advection_stage(Mesh m, Flow fl, Wen
 
 // CFL limit, get_flow_dtmax (src/hipft.f90:7321-7327): min over interior
 // cells of half/max(kdotv, tiny); positive doubles order like their bits.
-__global__ void k_flow_dtmax(Mesh m, Flow fl, unsigned long long *min_bits) {
+// per_real: one limit per realization (ragged batches).
+__global__ void k_flow_dtmax(Mesh m, Flow fl, unsigned long long *min_bits, int per_real = 0) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 2;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
   const int i = blockIdx.z + 1;
@@ -481,7 +497,7 @@ __global__ void k_flow_dtmax(Mesh m, Flow fl, unsigned long long *min_bits) {
     unsigned long long t = __shfl_down_sync(0xffffffffu, b, o);
     b = t < b ? t : b;
   }
-  if ((threadIdx.x & 31) == 0) atomicMin(min_bits, b);
+  if ((threadIdx.x & 31) == 0) atomicMin(min_bits + (per_real ? i - 1 : 0), b);
 }
 
 // 2-D flow build (update_flow, src/hipft.f90:3393-3519): theta/phi profiles
@@ -1084,13 +1100,17 @@ namespace hipft {
 // instructions.  Row pairs start at an odd row (j = 2t+1, 2t+2) so the pole
 // pairs (1,2) and (ntm-1,ntm) stay inside one thread when ntm is even, and
 // inside one warp otherwise (handled with shuffles).  Requires ldt even.
+// Ragged batches: rlist (may be null) maps grid slice z to a realization and
+// rc (may be null) holds each realization's stage coefficients.
 template <int MODE, int KPT>
 __global__ void __launch_bounds__(128, 4) k_sts_stage_v3(Mesh m, const double *__restrict__ dfac,
                                                         const double *__restrict__ x, const double *ykm2,
                                                         const double *__restrict__ u0,
                                                         const double *__restrict__ dty0, double *out, double *out2,
                                                         const double *__restrict__ ring_in, double bcn, double bcs,
-                                                        StageCoef sc, RingOut ro, int jshift) {
+                                                        StageCoef sc, RingOut ro, int jshift,
+                                                        const int *__restrict__ rlist = nullptr,
+                                                        const StageCoef *__restrict__ rc = nullptr) {
   const int lane = threadIdx.x & 31;
   // thread t owns rows ja = 2t+1-2*jshift and ja+1; for odd ntm, jshift moves
   // the thread owning row ntm off lane 0 so row ntm-1 is in the same warp
@@ -1098,7 +1118,8 @@ __global__ void __launch_bounds__(128, 4) k_sts_stage_v3(Mesh m, const double *_
   const int ja = 2 * t + 1 - 2 * jshift;
   const int kb = blockIdx.y;
   const int k0 = kb * KPT + 2;
-  const int i = blockIdx.z + 1;
+  const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
+  if (rc) sc = rc[i - 1];
   const int ntm = m.ntm, npm = m.npm;
   const int nk = min(KPT, npm - 1 - k0 + 1);
   const bool rowa = (ja >= 1 && ja <= ntm), rowb = (ja + 1 >= 1 && ja + 1 <= ntm);
@@ -1339,6 +1360,11 @@ constexpr size_t kPairSmem = pair_smem_bytes<kPJ, kPK>();
 struct PairArgs {
   StageCoef ca, cb;     // stages k and k+1
   int *err;             // set to 1 when a bounded wait gives up
+  // ragged batches (null otherwise): the realizations (0-based) this launch
+  // advances, and per realization the coefficients of its stages k, k+1
+  // ([nr][2])
+  const int *rlist = nullptr;
+  const StageCoef *rc = nullptr;
 };
 
 template <int TJ, int TK, int MINB>

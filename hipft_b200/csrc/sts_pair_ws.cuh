@@ -55,8 +55,9 @@ constexpr int kWU = al16(kWY2 + (kWK + 2) * kWR);   // u0
 constexpr int kWD = al16(kWU + (kWK + 2) * kWR);    // dty0
 constexpr int kWRT = al16(kWD + (kWK + 2) * kWR);   // rows: st_i, c2, c4, each kWR long
 constexpr int kWCT = kWRT + 3 * kWR;                // columns: {P1, P5} per shared column
-constexpr int kWInfo = kWCT + 2 * (kWK + 4);       // tile record: D, pole terms, (kt, rb, i)
-constexpr int kWBuf = al16(kWInfo + 8);
+constexpr int kWInfo = kWCT + 2 * (kWK + 4);       // tile record: D, pole terms, (kt, rb, i), stage coefficients
+constexpr int kWInfoCoef = kWInfo + 5;              // ragged batches: the tile's two StageCoef (10 doubles)
+constexpr int kWBuf = al16(kWInfo + 16);
 constexpr int kWYk = kWNB * kWBuf;                  // Y_k: kWK+2 columns, consumers only
 constexpr int kWEnd = kWYk + (kWK + 2) * kWR;
 constexpr size_t kWSmem = (size_t)kWEnd * sizeof(double) + 2 * kWNB * sizeof(uint64_t);
@@ -234,12 +235,15 @@ __device__ __forceinline__ void store_pair(double *g, double2 y, bool va, bool v
 
 // Tile t of a launch: phi tile kt, theta block rb, realization i.  Theta
 // blocks go in the order 1..nb-2, 0, nb-1: interior tiles first, so that the
-// wait for the previous pole kernel comes as late as possible.
-__device__ __forceinline__ void ws_tile(const PairTables &pt, int t, int &kt, int &rb, int &i) {
+// wait for the previous pole kernel comes as late as possible.  In a ragged
+// batch the launch covers only the realizations in rlist (pt.ntiles counts
+// their tiles).
+__device__ __forceinline__ void ws_tile(const PairTables &pt, int t, int &kt, int &rb, int &i,
+                                        const int *rlist) {
   kt = t % pt.nkt;
   const int rest = t / pt.nkt;
   const int q = rest % pt.nb;
-  i = rest / pt.nb + 1;
+  i = (rlist ? rlist[rest / pt.nb] : rest / pt.nb) + 1;
   rb = (pt.nb <= 2) ? q : ((q < pt.nb - 2) ? q + 1 : ((q == pt.nb - 2) ? 0 : pt.nb - 1));
 }
 
@@ -273,7 +277,11 @@ __device__ __forceinline__ void ws_store_cols(double *out, int64_t pbase, int k0
 // release the buffer; no consumer thread stores to global memory there.
 // Those stores also write the pole rows 1 / ntm of Y_{k+1} with unused
 // values; k_pair_poles, launched after this kernel, overwrites them.
-template <bool INLINE_POLES, bool ROWPAIRS = false, bool BULKST = false>
+//
+// RAGGED: the launch advances the realizations of pa.rlist, each with its
+// own stage coefficients pa.rc[2(i-1)], pa.rc[2(i-1)+1]; the producer copies
+// them into the tile record, so the consumers read them from shared memory.
+template <bool INLINE_POLES, bool ROWPAIRS = false, bool BULKST = false, bool RAGGED = false>
 __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const double *__restrict__ dfac,
                                                              const double *__restrict__ ykm1,
                                                              const double *__restrict__ ykm2,
@@ -310,7 +318,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     const bool maps_ok = tm.on && (smem_addr(wsm) & 127u) == 0;
     auto store_prev_k1 = [&](int tp, const double *Bp) {
       int ktp, rbp, ip;
-      ws_tile(pt, tp, ktp, rbp, ip);
+      ws_tile(pt, tp, ktp, rbp, ip, RAGGED ? pa.rlist : nullptr);
       const int j0p = rbp * kWJ + 1, k0p = ktp * kWK + 2;
       if (k0p + kWK - 1 <= npm - 1 && j0p + kWJ - 1 <= ntm)
         ws_store_cols(out_k1, (int64_t)(ip - 1) * m.plane, k0p, j0p, Bp + kWY2, lane, npm, ld);
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
       const int b = n % kWNB, u = n / kWNB;
       int kt, rb, i;
-      ws_tile(pt, t, kt, rb, i);
+      ws_tile(pt, t, kt, rb, i, RAGGED ? pa.rlist : nullptr);
       const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
       const int nk = min(kWK, npm - 1 - k0 + 1);
       const int rs = max(1, j0 - 2), re = min((int)ld, j0 + kWJ + 1);
@@ -342,6 +350,11 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       // the tile record's global loads go out before the wait for the
       // buffer, so their latency hides behind it
       double rd = 0.0, rn = 0.0, rsv = 0.0;
+      StageCoef rca{}, rcb{};
+      if (RAGGED && lane == 0) {
+        rca = pa.rc[2 * (i - 1)];
+        rcb = pa.rc[2 * (i - 1) + 1];
+      }
       if (lane == 0) {
         rd = dfac[i];
         if (dep_done) {  // used by pole tiles only
@@ -370,6 +383,11 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
         Ii[0] = kt;
         Ii[1] = rb;
         Ii[2] = i;
+        if (RAGGED) {
+          double *C = B + kWInfoCoef;
+          C[0] = rca.a; C[1] = rca.b; C[2] = rca.c; C[3] = rca.d; C[4] = rca.e;
+          C[5] = rcb.a; C[6] = rcb.b; C[7] = rcb.c; C[8] = rcb.d; C[9] = rcb.e;
+        }
         if (boxed) {
           // five tensor copies (halo rows outside the field read as zeros;
           // x = j0-3 keeps the innermost offset a multiple of 16 bytes) and
@@ -441,7 +459,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
   const int h = tid >> 7;            // column half of the tile
   const int r2 = 1 + (tid & 127);    // stage-k shared row (rows 129, 130 by the last 20 threads)
   const int r3 = r2 + 1;             // stage-k+1 shared row
-  const StageCoef sa = pa.ca, sb = pa.cb;
+  StageCoef sa = pa.ca, sb = pa.cb;
   double *sYk = wsm + kWYk;          // column c of the tile at (c-1)*kWR
   int n = 0;
   for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
@@ -459,6 +477,11 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
     const double Dr = B[kWInfo], ax_n = B[kWInfo + 1], ax_s = B[kWInfo + 2];
     const int *Ii = reinterpret_cast<const int *>(B + kWInfo + 3);
     const int kt = Ii[0], rb = Ii[1], i = Ii[2];
+    if (RAGGED) {
+      const double *C = B + kWInfoCoef;
+      sa = StageCoef{C[0], C[1], C[2], C[3], C[4]};
+      sb = StageCoef{C[5], C[6], C[7], C[8], C[9]};
+    }
     const int j0 = rb * kWJ + 1, k0 = kt * kWK + 2;
     const int nk = min(kWK, npm - 1 - k0 + 1);
     const int64_t pbase = (int64_t)(i - 1) * m.plane;
@@ -810,7 +833,8 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
 
 // Pole rows of Y_{k+1} and the ring sums of Y_{k+1}, after
 // k_sts_pair_ws<false>.  Grid (realization, chunk of kPoleThreads phi
-// columns).  Every block sums the ring partials of Y_k that the pole tiles
+// columns); in a ragged batch grid x walks pa.rlist and the coefficients are
+// the realization's own (pa.rc).  Every block sums the ring partials of Y_k that the pole tiles
 // wrote (tile order, the same fixed tree in every block), computes the pole
 // rows of Y_{k+1} for its columns by stage k+1's combine (src/hipft.f90:
 // 5224-5235) with Y_k at the poles recomputed from the inputs, and writes its
@@ -835,10 +859,11 @@ __global__ void __launch_bounds__(kPoleThreads) k_pair_poles(Mesh m, const doubl
   // the next pair's kernel may launch now; its tiles at the poles wait for
   // this grid to finish (griddepcontrol.wait)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  const int tid = threadIdx.x, i = blockIdx.x + 1, ch = blockIdx.y, nch = gridDim.y;
+  const int tid = threadIdx.x, ch = blockIdx.y, nch = gridDim.y;
+  const int i = (pa.rlist ? pa.rlist[blockIdx.x] : (int)blockIdx.x) + 1;
   const int ntm = m.ntm, npm = m.npm;
   const int64_t ld = m.ldt, pbase = (int64_t)(i - 1) * m.plane;
-  const StageCoef sa = pa.ca, sb = pa.cb;
+  const StageCoef sa = pa.rc ? pa.rc[2 * (i - 1)] : pa.ca, sb = pa.rc ? pa.rc[2 * (i - 1) + 1] : pa.cb;
   const double Dr = dfac[i];
   const double ax_n = ring_in[2 * (i - 1)] * bcn;
   const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;

@@ -77,7 +77,8 @@ class Info(ctypes.Structure):
     _fields_ = [("ntm", ctypes.c_int), ("npm", ctypes.c_int), ("nr", ctypes.c_int), ("ldt", ctypes.c_int),
                 ("dtime_diffusion_euler", ctypes.c_double), ("sts_s", ctypes.c_int64),
                 ("kernel_launches", ctypes.c_int64), ("cell_stage_updates", ctypes.c_int64),
-                ("device_bytes", ctypes.c_size_t), ("rkg2_stages", ctypes.c_int64)]
+                ("device_bytes", ctypes.c_size_t), ("rkg2_stages", ctypes.c_int64),
+                ("rkg2_cell_stages", ctypes.c_int64)]
 
 
 CYCLE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
@@ -137,6 +138,10 @@ SIGNATURES = [
     ("hipft_gpu_source_step", ctypes.c_int, [_H, ctypes.c_double]),
     ("hipft_h5_write", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), DPTR, DPTR,
                                       DPTR, DPTR, ctypes.c_int]),
+    ("hipft_gpu_set_ragged", ctypes.c_int, [_H, ctypes.c_int]),
+    ("hipft_gpu_flow_dtmax_each", ctypes.c_int, [_H, DPTR]),
+    ("hipft_gpu_ragged_schedule", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                                 ctypes.POINTER(ctypes.c_int64), DPTR]),
 ]
 
 _lib = None
@@ -328,6 +333,27 @@ class HipftGPU:
         d = ctypes.c_double(0.0)
         self._ck(self.L.hipft_gpu_flow_dtmax(self.h, ctypes.byref(d)), "flow_dtmax")
         return d.value
+
+    def flow_dtmax_each(self) -> np.ndarray:
+        """get_flow_dtmax (src/hipft.f90:7287) of each realization alone."""
+        d = np.zeros(self.nr)
+        self._ck(self.L.hipft_gpu_flow_dtmax_each(self.h, _p(d)), "flow_dtmax_each")
+        return d
+
+    # -- ragged batches
+    def set_ragged(self, on: bool = True):
+        """Ragged batching: each realization keeps the schedule it would have
+        alone (Euler limit, PTL subcycles, stage counts, advection substeps)."""
+        self._ck(self.L.hipft_gpu_set_ragged(self.h, int(on)), "set_ragged")
+
+    def ragged_schedule(self) -> dict:
+        """Per-realization schedule of the last ragged step."""
+        I64 = ctypes.POINTER(ctypes.c_int64)
+        s, c, a = (np.zeros(self.nr, dtype=np.int64) for _ in range(3))
+        e = np.zeros(self.nr)
+        self._ck(self.L.hipft_gpu_ragged_schedule(self.h, s.ctypes.data_as(I64), c.ctypes.data_as(I64),
+                                                  a.ctypes.data_as(I64), _p(e)), "ragged_schedule")
+        return dict(sts_s=s, subcycles=c, adv_substeps=a, dt_euler=e)
 
     # -- steps
     def advection_step(self, dt: float):

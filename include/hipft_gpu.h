@@ -249,6 +249,7 @@ typedef struct {
   int64_t cell_stage_updates;   /* unique cells x stages advanced so far      */
   size_t device_bytes;          /* device memory held by the handle           */
   int64_t rkg2_stages;          /* super-step stages k >= 2 run so far         */
+  int64_t rkg2_cell_stages;     /* unique cells x stages k >= 2 advanced so far */
 } hipft_info;
 int hipft_gpu_info(const hipft_gpu *h, hipft_info *info);
 /* Per-kernel timing with CUDA events on the handle's stream.  Kinds:
@@ -275,6 +276,34 @@ int hipft_gpu_field_device_ptr(hipft_gpu *h, double **ptr, int *ldt);
  * handle's error flag; the call then returns HIPFT_ETIMEOUT, as a stalled
  * copy would, and the handle stays usable. */
 int hipft_gpu_check_bounded_wait(hipft_gpu *h, unsigned int limit);
+
+/* ---- ragged batches (no counterpart in the reference) ---------------------- */
+
+/* The reference advances all realizations with one schedule: one dt, one
+ * explicit-Euler limit, one RKG2/RKL2 stage count and one PTL subcycle
+ * sequence, from global MIN/MAX reductions (src/hipft.f90:5036, 5103, 5141,
+ * 7345); that is this library's default ("plain" mode).  on = 1 switches a
+ * handle to ragged batching: every realization keeps the schedule it would
+ * have if it were run alone -- its own Gershgorin limit (get_dtime_diffusion_
+ * euler, 4985), its own PTL subcycles (get_dtime_diffusion_ptl, 5042) and
+ * stage counts (load_sts_rkg2 5361 / rkl2 5244), and, when a step is longer
+ * than its own CFL limit (get_flow_dtmax, 7287), ceil(dt / limit) advection
+ * substeps -- while each launch still covers every realization that has work
+ * left.  A step of a ragged batch therefore equals, realization by
+ * realization, the reference run with that realization alone at the same
+ * dt.  Needs RKG2 or RKL2 with per-realization constant coefficients,
+ * SSPRK(3,3) or SSPRK(4,3) advection, and no all-reduce callback (else
+ * HIPFT_EINVAL / HIPFT_ESTATE).  The cycle callback of diffusion_step is not
+ * called in ragged mode; hipft_gpu_ragged_schedule reports the schedule. */
+int hipft_gpu_set_ragged(hipft_gpu *h, int on);
+/* get_flow_dtmax (src/hipft.f90:7287-7350) of each realization alone:
+ * dtmax[nr] (x2 for Strang, x2 for SSPRK(4,3), as the reference scales it). */
+int hipft_gpu_flow_dtmax_each(hipft_gpu *h, double *dtmax);
+/* Per-realization schedule of the last ragged step (arrays of nr, each may
+ * be NULL): stage count of the last super-step, diffusion subcycles,
+ * advection substeps per advection call, and the Euler limit. */
+int hipft_gpu_ragged_schedule(hipft_gpu *h, int64_t *sts_s, int64_t *subcycles, int64_t *adv_substeps,
+                              double *dt_euler);
 
 /* ---- allocation-free flux integral ------------------------------------------ */
 

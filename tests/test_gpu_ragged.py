@@ -1,0 +1,151 @@
+"""Ragged batches: every realization advanced with its own schedule.
+
+The reference keeps one schedule for all realizations (global MIN/MAX
+reductions, src/hipft.f90:5036, 5103, 5141, 7345).  A ragged batch gives each
+realization the schedule it would have alone, so its parity oracle is the
+oracle run of that realization alone at the same dt sequence:
+
+* diffusion + advection, per-realization D and flows: every realization's
+  final field within 1e-12 of its own single-realization oracle run, and its
+  stage counts and subcycles equal to that run's history;
+* advection substeps: a step longer than some realizations' CFL limits
+  splits into ceil(dt / limit) substeps for those realizations, which equals
+  the oracle run of that realization alone with dt_max = dt / n_i;
+* identical realizations: ragged and plain mode give the same field bit for
+  bit (the schedules coincide).
+"""
+import numpy as np
+import pytest
+
+import test_gpu_refined as R
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-12
+
+NTM, NPM1 = 96, 129
+D = [80.0, 300.0, 900.0, 150.0]
+P1 = [22.0, 30.0, 12.0, 40.0]
+P2 = [-262.0, -300.0, -200.0, -340.0]
+
+
+def _grid():
+    from hipft_b200 import synthetic as S
+    t = S.refined_theta(NTM)
+    p = S.uniform_phi(NPM1)
+    return t, p, R.smooth_map(t, p, 17)
+
+
+def _handle(t, p, nr, diffusion=True, **kw):
+    import hipft_b200 as H
+    g = H.HipftGPU(t, p, nr, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                   advance_diffusion=diffusion, diffusion_coef_constants=D[:nr] if diffusion else None, **kw)
+    g.set_flow(dr_model=1, mf_model=1, dr_p2=P2[:nr], mf_p1=P1[:nr])
+    return g
+
+
+def _oracle_alone(i, t, p, br, dt_max, time_end, diffusion=True):
+    raw = dict(n_realizations=1, advance_flow=True, flow_num_method=4, strang_splitting=True, flow_dr_model=1,
+               flow_mf_model=1, advance_diffusion=diffusion, time_end=time_end, dt_max=dt_max,
+               flow_dr_coef_p2_values=[P2[i]], flow_mf_coef_p1_values=[P1[i]],
+               diffusion_coef_constants=[D[i]])
+    prm = O.process_parameters(raw)
+    return O.run(prm, map_pt=br[None], s1=p, s2=t)
+
+
+def _dt_sequence(dt, nsteps):
+    """The dt of each step as the oracle's update_timestep picks it when
+    time_end is the sum of nsteps steps of dt and dt_max = dt."""
+    tend = 0.0
+    for _ in range(nsteps):
+        tend += dt
+    seq, time = [], 0.0
+    for _ in range(nsteps):
+        d = tend - time if time + dt >= tend else dt
+        seq.append(d)
+        time += d
+    return seq, tend
+
+
+def test_ragged_matches_each_realization_alone():
+    t, p, br = _grid()
+    nr, nsteps = 4, 3
+    with _handle(t, p, nr) as g:
+        g.load_initial_map(br[None])
+        g.update_flow()
+        g.set_ragged(True)
+        dt = g.flow_dtmax()  # the shared step: every realization within its own CFL limit
+        seq, tend = _dt_sequence(dt, nsteps)
+        for d in seq:
+            g.flux_transport_step(d)
+        sched = g.ragged_schedule()
+        f = g.get_field()
+    assert len(set(sched["sts_s"].tolist())) > 1, "the realizations should need different stage counts"
+    for i in range(nr):
+        r = _oracle_alone(i, t, p, br, dt, tend)
+        assert r["nsteps"] == nsteps
+        err = np.abs(f[i] - r["f"][0]).max() / np.abs(r["f"][0]).max()
+        assert err <= FIELD_TOL, f"realization {i}: field rel max-norm {err:.3e}"
+        last = r["num"][-1, 0, :]
+        assert int(last[6]) == sched["sts_s"][i], f"realization {i}: stage count {sched['sts_s'][i]} vs {last[6]}"
+        assert int(last[7]) == sched["subcycles"][i], f"realization {i}: subcycles"
+        assert np.isclose(last[5], sched["dt_euler"][i], rtol=1e-14, atol=0), f"realization {i}: Euler limit"
+
+
+def test_ragged_advection_substeps():
+    t, p, br = _grid()
+    nr, nsteps = 3, 2
+    with _handle(t, p, nr, diffusion=False) as g:
+        g.load_initial_map(br[None])
+        g.update_flow()
+        g.set_ragged(True)
+        lim = g.flow_dtmax_each()
+        dt = 2.5 * lim.min()
+        for _ in range(nsteps):
+            g.flux_transport_step(dt)
+        sched = g.ragged_schedule()
+        f = g.get_field()
+    n = np.maximum(1, np.ceil(dt / lim)).astype(int)
+    assert np.array_equal(sched["adv_substeps"], n)
+    assert n.max() >= 2 and len(set(n.tolist())) > 1
+    for i in range(nr):
+        dtm = dt / n[i]
+        tend = 0.0
+        for _ in range(nsteps * n[i]):
+            tend += dtm
+        r = _oracle_alone(i, t, p, br, dtm, tend, diffusion=False)
+        assert r["nsteps"] == nsteps * n[i]
+        err = np.abs(f[i] - r["f"][0]).max() / np.abs(r["f"][0]).max()
+        assert err <= FIELD_TOL, f"realization {i} ({n[i]} substeps): field rel max-norm {err:.3e}"
+
+
+def test_ragged_equals_plain_for_identical_realizations():
+    import hipft_b200 as H
+    t, p, br = _grid()
+    nr = 3
+    out = []
+    for ragged in (False, True):
+        g = H.HipftGPU(t, p, nr, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                       advance_diffusion=True, diffusion_coef_constants=[300.0] * nr)
+        g.set_flow(dr_model=1, mf_model=1, dr_p2=-262.0, mf_p1=22.0)
+        g.load_initial_map(br[None])
+        g.update_flow()
+        if ragged:
+            g.set_ragged(True)
+        dt = g.flow_dtmax()
+        for _ in range(3):
+            g.flux_transport_step(dt)
+        out.append(g.get_field())
+        g.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_ragged_rejects_unsupported_methods():
+    import hipft_b200 as H
+    from hipft_b200 import gpu
+    t, p, br = _grid()
+    with H.HipftGPU(t, p, 2, advance_diffusion=True, diffusion_num_method=1, diffusion_coef_constants=100.0) as g:
+        with pytest.raises(gpu.HipftError) as e:
+            g.set_ragged(True)
+        assert e.value.code == gpu.HIPFT_EINVAL
