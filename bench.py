@@ -192,6 +192,88 @@ def run_reference(args, wl, name):
     return 0
 
 
+def make_handle(H, t, p, br, prm, sl, device, ragged):
+    """A handle holding realizations `sl` of the workload with its initial map
+    and flows loaded; ragged: each realization keeps its own schedule."""
+    nrl = len(prm["diffusion_coef_constants"][sl])
+    g = H.HipftGPU(t, p, nrl, device=device, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                   advance_diffusion=True, diffusion_coef_constants=prm["diffusion_coef_constants"][sl])
+    g.load_initial_map(np.broadcast_to(br, (nrl,) + br.shape))
+    g.set_flow(dr_model=1, mf_model=1, dr_p0=prm["dr_p0"][sl], dr_p2=prm["dr_p2"][sl], dr_p4=prm["dr_p4"][sl],
+               mf_p1=prm["mf_p1"][sl], mf_p3=prm["mf_p3"][sl], mf_p5=prm["mf_p5"][sl])
+    g.update_flow()
+    if ragged:
+        g.set_ragged(True)
+    return g
+
+
+def make_step(g, dt, da_times, da_maps, prm, sl, state):
+    """One bench step: a flux-transport step, the assimilation when the step
+    crosses a 24 h boundary, and the diagnostics."""
+    def step():
+        g.flux_transport_step(dt)
+        state["time"] += dt
+        if state["da"] < len(da_times) and state["time"] >= da_times[state["da"]]:
+            g.assimilate(da_maps[da_times[state["da"]]], custom_from_mu=True, mu_power=prm["mu_power"][sl],
+                         mu_limit=prm["mu_limit"][sl], lat_limit=prm["lat_limit"][sl])
+            state["da"] += 1
+        g.analysis(state["time"])
+    return step
+
+
+def measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_maps, ragged_rs_per_s):
+    """Realization-steps per second of the same realizations three ways: the
+    ragged batch (taken from the timed region), one batch with the shared
+    (reference) schedule, and one handle per realization launched one after
+    another ("plain per-realization launches"), all at the shared dt."""
+    import torch
+    import hipft_b200 as H
+    stream = torch.cuda.current_stream()
+    nr = wl["nr"]
+    k = max(2, min(args.steps, 4))
+    out = {"unit": "realization-steps/s", "dt_hours": dt, "ragged_batch": ragged_rs_per_s}
+    # one batch, shared schedule
+    g = make_handle(H, t, p, br, prm, slice(0, nr), local, False)
+    g.set_stream(stream.cuda_stream)
+    state = {"time": 0.0, "da": 0}
+    step = make_step(g, dt, da_times, da_maps, prm, slice(0, nr), state)
+    step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    out["shared_batch"] = nr * k / (e0.elapsed_time(e1) * 1e-3)
+    out["shared_batch_steps"] = k
+    g.close()
+    # one handle per realization, each with its own schedule
+    tot_ms = 0.0
+    for i in range(nr):
+        gi = make_handle(H, t, p, br, prm, slice(i, i + 1), local, False)
+        gi.set_stream(stream.cuda_stream)
+        st = {"time": 0.0, "da": 0}
+        si = make_step(gi, dt, da_times, da_maps, prm, slice(i, i + 1), st)
+        si()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(k):
+            si()
+        b.record(stream)
+        torch.cuda.synchronize()
+        tot_ms += a.elapsed_time(b)
+        gi.close()
+    out["per_realization_handles"] = nr * k / (tot_ms * 1e-3)
+    out["per_realization_steps"] = k
+    out["ragged_over_per_realization"] = ragged_rs_per_s / out["per_realization_handles"]
+    out["ragged_over_shared"] = ragged_rs_per_s / out["shared_batch"]
+    out["note"] = ("the per-realization handles run one after another, each from the 126 MB L2 (17 MB fields); "
+                   "the batches stream 1.07 GB fields from HBM")
+    return out
+
+
 def run_gpu(args, wl, name):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -209,30 +291,18 @@ def run_gpu(args, wl, name):
     t, p, br, prm = make_inputs(wl)
     first, nrl = split_realizations(wl["nr"], world, rank)
     sl = slice(first, first + nrl)
-    g = H.HipftGPU(t, p, nrl, device=local, advance_flow=True, flow_num_method=4, strang_splitting=True,
-                   advance_diffusion=True, diffusion_coef_constants=prm["diffusion_coef_constants"][sl])
+    ragged = args.schedule == "ragged"
+    g = make_handle(H, t, p, br, prm, sl, local, ragged)
     stream = torch.cuda.current_stream()
     g.set_stream(stream.cuda_stream)
-    g.load_initial_map(np.broadcast_to(br, (nrl,) + br.shape))
-    g.set_flow(dr_model=1, mf_model=1, dr_p0=prm["dr_p0"][sl], dr_p2=prm["dr_p2"][sl], dr_p4=prm["dr_p4"][sl],
-               mf_p1=prm["mf_p1"][sl], mf_p3=prm["mf_p3"][sl], mf_p5=prm["mf_p5"][sl])
-    g.update_flow()
     dt = g.flow_dtmax()
     ntm, npm = g.ntm, g.npm
     # assimilation maps for every 24 h boundary the run will cross
-    n_total = args.warmup + 2 * args.steps + 2
+    n_total = args.warmup + 3 * args.steps + 2
     da_times = [24.0 * k for k in range(1, int(n_total * dt / 24.0) + 2)]
     da_maps = {tt: S.observed_map(t, p, tt, wl["seed"]) for tt in da_times}
     state = {"time": 0.0, "da": 0}
-
-    def step():
-        g.flux_transport_step(dt)
-        state["time"] += dt
-        if state["da"] < len(da_times) and state["time"] >= da_times[state["da"]]:
-            g.assimilate(da_maps[da_times[state["da"]]], custom_from_mu=True, mu_power=prm["mu_power"][sl],
-                         mu_limit=prm["mu_limit"][sl], lat_limit=prm["lat_limit"][sl])
-            state["da"] += 1
-        g.analysis(state["time"])
+    step = make_step(g, dt, da_times, da_maps, prm, sl, state)
 
     for _ in range(args.warmup):
         step()
@@ -253,6 +323,7 @@ def run_gpu(args, wl, name):
     i1 = g.info()
     cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
     launches = int(i1.kernel_launches - i0.kernel_launches)
+    real_steps_per_s = nrl * args.steps / (ms * 1e-3)
     # kernel breakdown in a second pass of the same steps: per-kernel events
     # sit between launches, which the timed pass above keeps free of them
     if dist:
@@ -272,7 +343,10 @@ def run_gpu(args, wl, name):
     ring_n, ring_ms = g.kernel_time(2)
     oth_n, oth_ms = g.kernel_time(3)
     g.set_profiling(False)
-    rkg2_stages = int(g.info().rkg2_stages - ip.rkg2_stages)
+    ipe = g.info()
+    rkg2_stages = int(ipe.rkg2_stages - ip.rkg2_stages)
+    rkg2_cell_stages = float(ipe.rkg2_cell_stages - ip.rkg2_cell_stages)
+    sched = g.ragged_schedule() if ragged else None
 
     # end to end through the C ABI with host buffers
     f_host = torch.empty((nrl, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
@@ -299,9 +373,10 @@ def run_gpu(args, wl, name):
 
     peak, peak_kind = measured_peak()
     # Algorithmic bytes: 40 B per unique cell per RKG2 stage (read Y_{k-1},
-    # Y_{k-2}, u0, dty0; write Y_k), times the stages one launch advances.
+    # Y_{k-2}, u0, dty0; write Y_k), times the cell-stages one launch advances
+    # (in a ragged batch a launch covers the realizations with stages left).
     stages_per_launch = rkg2_stages / max(sts_n, 1)
-    bytes_per_launch = STS_BYTES_PER_CELL * ntm * (npm - 2) * nrl * stages_per_launch
+    bytes_per_launch = STS_BYTES_PER_CELL * rkg2_cell_stages / max(sts_n, 1)
     sts_avg_ms = sts_ms / max(sts_n, 1)
     achieved = bytes_per_launch / (sts_avg_ms * 1e-3) / 1e9 if sts_n else None
     traffic, traffic_src = None, None
@@ -320,6 +395,8 @@ def run_gpu(args, wl, name):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": name, "grid": [ntm, npm - 2], "realizations": wl["nr"],
                    "realizations_per_gpu": nrl, "dt_hours": dt, "parallelism": f"realizations/{world}",
+                   "schedule": ("ragged: each realization its own Euler limit, PTL subcycles and RKG2 stage "
+                                "counts" if ragged else "shared (the reference's MIN/MAX schedule)"),
                    "method": "WENO3+SSPRK(4,3) Strang-split with RKG2 (PTL subcycles), DA every 24 h",
                    "l2": "inputs larger than L2 (%.2f GB per field), no flush" % (ntm * npm * nrl * 8 / 1e9)},
         "roofline": {"bound": "hbm",
@@ -338,7 +415,14 @@ def run_gpu(args, wl, name):
                 "h2d_bytes_per_step": ntm * npm * nrl * 8, "d2h_bytes_per_step": ntm * npm * nrl * 8},
         "gpu_launches": launches,
         "clocks": clk,
+        "realization_steps_per_s": real_steps_per_s,
     }
+    if sched is not None:
+        out["config"]["rkg2_stages_per_realization"] = [int(x) for x in sched["sts_s"]]
+        out["config"]["subcycles_per_realization"] = [int(x) for x in sched["subcycles"]]
+    if rank == 0 and world == 1 and not args.no_plain:
+        out["batched_vs_plain"] = measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_maps,
+                                                           real_steps_per_s)
     if rank == 0 and world == 1 and not args.no_plain:
         out["plain"] = measure_plain(args, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
@@ -530,6 +614,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
+    ap.add_argument("--schedule", default="ragged", choices=["ragged", "shared"],
+                    help="ragged: every realization its own schedule (default); shared: the reference's")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

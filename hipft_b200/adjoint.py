@@ -36,6 +36,7 @@ import time
 from typing import Sequence
 
 import numpy as np
+import torch
 
 from .gpu import HipftError, HipftGPU
 
@@ -150,9 +151,20 @@ class MisfitAdjoint:
 
     gpu: a HipftGPU handle configured for the run (flows set with
     gpu.set_flow); D: the diffusion_coef_constants it was built with; flow:
-    dict of (nr,) arrays p0, p2, p4, p1, p3, p5 as given to gpu.set_flow."""
+    dict of (nr,) arrays p0, p2, p4, p1, p3, p5 as given to gpu.set_flow;
+    assim: optional {step index s: (map3, options)}, an assimilation of the
+    (3, ntm, npm1) map with HipftGPU.assimilate's keyword options right after
+    step s (apply_data_assimilation, src/hipft.f90:4148-4306), differentiated
+    by hipft_adj_assimilate (blend and additive forms; not the balanced
+    increment).
 
-    def __init__(self, gpu: HipftGPU, D: Sequence[float], flow: dict, checkpoint_every: int = 64):
+    Device memory: one field per checkpoint (every `checkpoint_every` steps),
+    the inputs of the last segment's steps (at most checkpoint_every - 1 more
+    fields), and the tape of one step inside hipft_adj_step (bounded by
+    hipft_adj_set_tape_limit; freed by release())."""
+
+    def __init__(self, gpu: HipftGPU, D: Sequence[float], flow: dict, checkpoint_every: int = 64,
+                 assim: dict | None = None):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("the adjoint runs on the GPU (libhipft_gpu); no CUDA device is visible")
@@ -162,9 +174,11 @@ class MisfitAdjoint:
         self.flow = {k: np.asarray(flow.get(k, 0.0), dtype=np.float64).reshape(-1) * np.ones(self.nr)
                      for k in FLOW_KEYS}
         self.k = max(1, int(checkpoint_every))
+        self.assim = dict(assim or {})
         self.mesh = mesh_1d(gpu.t, gpu.p)
         self.w = misfit_weights(self.mesh)
         self.timing = {}
+        self._fwd = None
 
     def _dev(self):
         return self.gpu.field_tensor()
@@ -173,21 +187,29 @@ class MisfitAdjoint:
         self.gpu._ck(self.gpu.L.hipft_gpu_set_field_device(self.gpu.h, ctypes.c_void_p(x.data_ptr())),
                      "set_field_device")
 
+    def _da_opts(self, opts: dict):
+        from .gpu import DAOpts, _p, _vec
+        v = [_vec(opts.get(k, dflt), self.nr) for k, dflt in (("mu_power", 4.0), ("mu_limit", 0.1),
+                                                               ("lat_limit", 0.0))]
+        o = DAOpts(int(opts.get("add", False)), int(opts.get("custom_from_mu", False)),
+                   int(opts.get("balance_flux", False)), float(opts.get("mult_fac", 1.0)), *[_p(a) for a in v])
+        return o, v
+
+    def _step(self, s: int, dt: float):
+        self.gpu.flux_transport_step(dt)
+        if s in self.assim:
+            m3, opts = self.assim[s]
+            self.gpu.assimilate(m3, **opts)
+
     def loss_and_cotangent(self, fN: np.ndarray, target: np.ndarray):
         """Misfit and its folded cotangent (nr, npm, ntm)."""
         r = fN - target
         loss = 0.5 * float(np.sum(self.w[None] * r * r))
         g = self.w[None] * r
-        gb = np.zeros_like(g)
-        gb[:, 1:self.npm - 1] = g[:, 1:self.npm - 1]
-        gb[:, self.npm - 2] += g[:, 0]  # column 1 is the seam copy of column npm-1
-        return loss, gb
+        return loss, fold_cotangent(g)
 
-    def run(self, f0: np.ndarray, target: np.ndarray, dts: Sequence[float]) -> tuple:
-        """Forward, misfit, reverse.  Returns (loss, grads) with grads["f0"]
-        (nr, npm, ntm) (folded: seam columns zero, their share in columns
-        npm-1 and 2), grads["D"] (nr,) and grads["p0".."p5"] (nr,).
-        self.timing holds the wall seconds of the forward and reverse parts."""
+    def forward(self, f0: np.ndarray, dts: Sequence[float]) -> np.ndarray:
+        """The forward run with its checkpoints; returns f_N (nr, npm, ntm)."""
         import torch
         g = self.gpu
         dts = [float(d) for d in dts]
@@ -204,14 +226,29 @@ class MisfitAdjoint:
                 ckpt[s] = self._dev().clone()
             if s >= last0:
                 kept.append(ckpt[s] if s == last0 else self._dev().clone())
-            g.flux_transport_step(dt)
+            self._step(s, dt)
         fN = g.get_field()
+        self._fwd = dict(dts=dts, ckpt=ckpt, kept=kept, last0=last0)
+        self.timing = {"forward_s": time.perf_counter() - t0}
+        return fN
+
+    def backward(self, gb) -> dict:
+        """Reverse pass from the folded cotangent gb (nr, npm, ntm) of f_N
+        (numpy or torch; seam columns ignored).  Returns grads["f0"] (nr,
+        npm, ntm) (folded: seam columns zero, their share in columns npm-1
+        and 2), grads["D"] (nr,) and grads["p0".."p5"] (nr,)."""
+        import torch
+        if self._fwd is None:
+            raise RuntimeError("backward() needs a forward() first")
+        g = self.gpu
+        dts, ckpt, kept, last0 = (self._fwd[k] for k in ("dts", "ckpt", "kept", "last0"))
+        n = len(dts)
         t1 = time.perf_counter()
-        loss, gb = self.loss_and_cotangent(fN, np.asarray(target, dtype=np.float64))
         ldt = self._dev().shape[-1]
         dev = torch.device("cuda")
         fbar = torch.zeros((self.nr, self.npm, ldt), dtype=torch.float64, device=dev)
-        fbar[:, :, :self.ntm] = torch.from_numpy(gb).to(dev)
+        gbt = torch.as_tensor(gb, dtype=torch.float64).to(dev)
+        fbar[:, 1:self.npm - 1, :self.ntm] = gbt[:, 1:self.npm - 1]
         dacc = torch.zeros(self.nr, dtype=torch.float64, device=dev)
         gflow = torch.zeros((5, self.nr, self.npm, ldt), dtype=torch.float64, device=dev)
         for s0 in sorted(ckpt, reverse=True):
@@ -220,9 +257,16 @@ class MisfitAdjoint:
             if s0 != last0 and s1 - s0 > 1:
                 self._set(ckpt[s0])
                 for s in range(s0, s1 - 1):
-                    g.flux_transport_step(dts[s])
+                    self._step(s, dts[s])
                     states.append(self._dev().clone())
             for s in range(s1 - 1, s0 - 1, -1):
+                if s in self.assim:
+                    m3, opts = self.assim[s]
+                    o, keep = self._da_opts(opts)
+                    m3 = np.ascontiguousarray(m3, dtype=np.float64)
+                    g._ck(g.L.hipft_adj_assimilate(g.h, m3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                   ctypes.byref(o), ctypes.c_void_p(fbar.data_ptr())),
+                          "hipft_adj_assimilate")
                 rc = g.L.hipft_adj_step(g.h, dts[s], ctypes.c_void_p(states[s - s0].data_ptr()),
                                         ctypes.c_void_p(fbar.data_ptr()), ctypes.c_void_p(dacc.data_ptr()),
                                         ctypes.c_void_p(gflow.data_ptr()))
@@ -233,9 +277,20 @@ class MisfitAdjoint:
         grads["f0"][:, self.npm - 1] = 0.0
         grads["D"] = dacc.cpu().numpy() / self.D
         grads.update(self._flow_grads(gflow))
-        t2 = time.perf_counter()
-        self.timing = {"forward_s": t1 - t0, "reverse_s": t2 - t1}
-        return loss, grads
+        self.timing["reverse_s"] = time.perf_counter() - t1
+        return grads
+
+    def run(self, f0: np.ndarray, target: np.ndarray, dts: Sequence[float]) -> tuple:
+        """Forward, misfit, reverse: (loss, grads) as backward() returns them.
+        self.timing holds the wall seconds of the forward and reverse parts."""
+        fN = self.forward(f0, dts)
+        loss, gb = self.loss_and_cotangent(fN, np.asarray(target, dtype=np.float64))
+        return loss, self.backward(gb)
+
+    def release(self):
+        """Frees the checkpoints and the library's tape."""
+        self._fwd = None
+        self.gpu._ck(self.gpu.L.hipft_adj_release(self.gpu.h), "hipft_adj_release")
 
     def _flow_grads(self, gflow) -> dict:
         import torch
@@ -258,6 +313,83 @@ class MisfitAdjoint:
         return {k: coef[k].grad.numpy().copy() for k in FLOW_KEYS}
 
 
+def fold_cotangent(g):
+    """Folds a cotangent (nr, npm, ntm) of a periodic field: the seam columns
+    1 and npm are copies of columns npm-1 and 2, so their entries move there
+    and the seam entries become zero (numpy or torch)."""
+    gb = g.clone() if hasattr(g, "clone") else np.array(g, dtype=np.float64, copy=True)
+    npm = gb.shape[1]
+    gb[:, npm - 2] += gb[:, 0]
+    gb[:, 1] += gb[:, npm - 1]
+    gb[:, 0] = 0.0
+    gb[:, npm - 1] = 0.0
+    return gb
+
+
+class FluxTransport:
+    """f_N = F(f0; D, p0, p2, p4, p1, p3, p5): N flux-transport steps of the
+    library (flux_transport_step, src/hipft.f90:4463-4507) as a differentiable
+    PyTorch function.
+
+        run = FluxTransport(t, p, dts, assim=..., checkpoint_every=64)
+        fN = run(f0, D, {"p0": ..., "p2": ..., ...})   # torch tensors, FP64
+        loss = ((fN - target) ** 2 * w).sum(); loss.backward()
+
+    The forward runs the CUDA library (WENO3 + SSPRK(4,3) Strang-split with
+    RKG2); backward runs its hand-written adjoint (hipft_adj_step,
+    hipft_adj_assimilate) through MisfitAdjoint.backward.  f0 must be periodic
+    (columns 1, npm copy columns npm-1, 2), as the reference's fields are; its
+    gradient is folded onto the core columns.  Handle options (diffusion
+    subcycles and so on) are HipftGPU keyword arguments."""
+
+    def __init__(self, t, p, dts, *, assim: dict | None = None, checkpoint_every: int = 64, device: int = 0,
+                 **handle_kw):
+        self.t = np.asarray(t, dtype=np.float64)
+        self.p = np.asarray(p, dtype=np.float64)
+        self.dts = [float(d) for d in dts]
+        self.assim = assim
+        self.k = checkpoint_every
+        self.device = device
+        self.kw = dict(advance_flow=True, flow_num_method=4, strang_splitting=True, advance_diffusion=True,
+                       diffusion_num_method=3)
+        self.kw.update(handle_kw)
+
+    def __call__(self, f0, D, coef: dict):
+        return _FluxTransportFn.apply(f0, D, *[torch.as_tensor(coef.get(k, 0.0), dtype=torch.float64)
+                                             .reshape(-1).expand(f0.shape[0]).contiguous() for k in FLOW_KEYS],
+                                      self)
+
+
+class _FluxTransportFn(torch.autograd.Function):
+    """The autograd node of FluxTransport: forward through the library's
+    steps with checkpoints, backward through its adjoint."""
+
+    @staticmethod
+    def forward(ctx, f0, D, p0, p2, p4, p1, p3, p5, run):
+        nr = f0.shape[0]
+        Dn = D.detach().cpu().numpy().astype(np.float64).reshape(nr)
+        flow = {k: v.detach().cpu().numpy().astype(np.float64).reshape(nr)
+                for k, v in zip(FLOW_KEYS, (p0, p2, p4, p1, p3, p5))}
+        g = HipftGPU(run.t, run.p, nr, device=run.device, diffusion_coef_constants=Dn, **run.kw)
+        g.set_flow(dr_model=1, mf_model=1, dr_p0=flow["p0"], dr_p2=flow["p2"], dr_p4=flow["p4"],
+                   mf_p1=flow["p1"], mf_p3=flow["p3"], mf_p5=flow["p5"])
+        A = MisfitAdjoint(g, Dn, flow, checkpoint_every=run.k, assim=run.assim)
+        fN = A.forward(f0.detach().cpu().numpy().astype(np.float64), run.dts)
+        ctx.A = A
+        return torch.as_tensor(fN, dtype=torch.float64, device=f0.device)
+
+    @staticmethod
+    def backward(ctx, gN):
+        A = ctx.A
+        grads = A.backward(fold_cotangent(gN.detach().to(torch.float64).cpu().numpy()))
+        A.gpu.close()
+        ctx.A = None
+        dev = gN.device
+        out = [torch.as_tensor(grads["f0"], device=dev), torch.as_tensor(grads["D"], device=dev)]
+        out += [torch.as_tensor(grads[k], device=dev) for k in FLOW_KEYS]
+        return (*out, None)
+
+
 def chain_physical(grads: dict) -> dict:
     """Gradients with respect to v0 (p1 = 2 v0, p3 = -2 v0) and A, B, C in
     deg/day (p0, p2, p4 = 140.596... x A, B, C)."""
@@ -266,4 +398,5 @@ def chain_physical(grads: dict) -> dict:
             "B": DEG_DAY_TO_M_S * grads["p2"], "C": DEG_DAY_TO_M_S * grads["p4"]}
 
 
-__all__ = ["MisfitAdjoint", "mesh_1d", "misfit_weights", "flow_profiles", "chain_physical", "HipftError"]
+__all__ = ["MisfitAdjoint", "FluxTransport", "fold_cotangent", "mesh_1d", "misfit_weights", "flow_profiles",
+           "chain_physical", "HipftError"]

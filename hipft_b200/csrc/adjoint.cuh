@@ -187,6 +187,20 @@ __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const dou
 }
 
 // dacc[i] += scale * (sum of realization i's block partials), fixed order.
+// Reverse of the assimilation blend f += w (d - f) (src/hipft.f90:4116-4141):
+// on the core columns the blend is f_new = (1 - w) f + w d, so the folded
+// cotangent becomes (1 - w) fbar; the additive form f += w d leaves it
+// unchanged.  One thread per core cell.
+__global__ void k_adj_da(Mesh m, DAArgs a, double *fbar) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm - 1 || a.add) return;
+  const double w = da_weight(m, a, j, k, i);
+  const int64_t q = fidx(m, j, k, i);
+  fbar[q] = (kOne - w) * fbar[q];
+}
+
 __global__ void k_adj_dsum(const double *__restrict__ dpart, int nblk, double scale, double *dacc) {
   __shared__ double sh[64];
   const int i = blockIdx.x;

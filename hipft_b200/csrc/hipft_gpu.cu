@@ -107,6 +107,11 @@ struct hipft_gpu {
   // adjoint: fields of one taped forward step, folded work fields (seam
   // columns stay zero), per-block partial sums and pole sums
   std::vector<double *> tape;
+  std::vector<double *> adj_block;        // stage fields of one recomputed block
+  double *d_adj_rings = nullptr;          // ring sums of the stage checkpoints
+  size_t adj_rings_cap = 0, adj_rings_n = 0;
+  int64_t adj_tape_limit = 0;             // fields the tape may use (0: half the free memory)
+  int64_t adj_force_q = 0;                // stage-checkpoint spacing forced by the caller (0: automatic)
   double *adjw[8] = {};
   double *d_dpart = nullptr, *d_gring = nullptr, *d_gpart[2] = {};
   int dpart_per_r = 0;
@@ -691,7 +696,7 @@ static int advection_stage(hipft_gpu *h, const double *x, const double *f0, doub
     k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
     LAUNCHED(h);
   }
-  dim3 blk(32, 8);
+  dim3 blk(33, 9);  // (TJ+1) x (TK+1) threads for a 32 x 8 tile
   ProfScope ps(h, HIPFT_K_ADV);
   if (h->adv_space == 2)
     k_advection_stage<32, 8, true><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out,
@@ -1818,7 +1823,7 @@ static int advection_stage_ragged(hipft_gpu *h, const double *x, const double *f
     k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
     LAUNCHED(h);
   }
-  dim3 blk(32, 8);
+  dim3 blk(33, 9);  // (TJ+1) x (TK+1) threads for a 32 x 8 tile
   dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)n);
   ProfScope ps(h, HIPFT_K_ADV);
   if (h->adv_space == 2)
@@ -2089,12 +2094,10 @@ extern "C" int hipft_gpu_source_step(hipft_gpu *h, double dt) {
 }
 
 // ------------------------------------------------------------ assimilation
-extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o) {
-  if (!h || !data3_pt || !o) return HIPFT_EINVAL;
-  if (!h->field_set) return fail(h, HIPFT_ESTATE, "assimilate before set_field");
-  if (!o->lat_limit || (o->custom_from_mu && (!o->mu_power || !o->mu_limit)))
-    return fail(h, HIPFT_EINVAL, "assimilate: missing per-realization options");
-  CK(h, cudaSetDevice(h->dev));
+// Uploads one observed map and the per-realization blend options
+// (assimilate_new_data's inputs, src/hipft.f90:4083-4146; lat-limit indices
+// of load_data_assimilation, 4066-4079) and fills the kernels' arguments.
+static int da_args(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o, DAArgs &a) {
   int ntm = h->ntm, npm1 = h->npm1, nr = h->nr;
   size_t nd = (size_t)npm1 * ntm * 3;
   if (!h->d_da) {
@@ -2109,7 +2112,6 @@ extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const 
     opt[i] = o->mu_power ? o->mu_power[i - 1] : 0.0;
     opt[(nr + 1) + i] = o->mu_limit ? o->mu_limit[i - 1] : 0.0;
     opt[2 * (nr + 1) + i] = o->lat_limit[i - 1];
-    // lat-limit indices (load_data_assimilation, src/hipft.f90:4066-4079)
     int t0 = -1, t1 = -1;
     for (int j = 1; j <= ntm; ++j)
       if (h->t[j] >= o->lat_limit[i - 1] * c_d2r && t0 == -1) t0 = j;
@@ -2120,7 +2122,7 @@ extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const 
   }
   TRY(upload(h, h->d_daopt, opt));
   CK(h, cudaMemcpyAsync(h->d_tidx, tidx.data(), tidx.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
-  DAArgs a{};
+  a = DAArgs{};
   a.data = h->d_da;
   a.mu_power = h->d_daopt;
   a.mu_limit = h->d_daopt + (nr + 1);
@@ -2130,6 +2132,18 @@ extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const 
   a.add = o->add;
   a.custom_from_mu = o->custom_from_mu;
   a.mult_fac = o->mult_fac;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o) {
+  if (!h || !data3_pt || !o) return HIPFT_EINVAL;
+  if (!h->field_set) return fail(h, HIPFT_ESTATE, "assimilate before set_field");
+  if (!o->lat_limit || (o->custom_from_mu && (!o->mu_power || !o->mu_limit)))
+    return fail(h, HIPFT_EINVAL, "assimilate: missing per-realization options");
+  CK(h, cudaSetDevice(h->dev));
+  int ntm = h->ntm, npm1 = h->npm1, nr = h->nr;
+  DAArgs a;
+  TRY(da_args(h, data3_pt, o, a));
   double *f = h->buf[h->cur], *delta = h->buf[scratch(h, 0)];
   dim3 blk(32, 8), grd((unsigned)((ntm + 31) / 32), (unsigned)((npm1 + 31) / 32), (unsigned)nr);
   k_da_delta<<<grd, blk, 0, h->stream>>>(h->M, a, f, delta);
@@ -2569,13 +2583,41 @@ extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, in
 // the gradient is that of the discrete map at this schedule.
 
 namespace {
+// One RKG2 super-step of the replay.  With q == 0 the tape holds every stage:
+// slots t0 = u0, t0+1 = dty0, t0+1+k = Y_k (k = 1..s-1).  With stage
+// checkpoints (q > 0, even) it holds u0, dty0 and, for each block start
+// c = 1, 1+q, 1+2q, ... (odd, the output of a stage pair), the pair
+// (Y_{c-1}, Y_c) in slots t0+2+2b, t0+3+2b (b = block index; Y_0 = u0 is
+// not stored twice) and the pole-ring sums of Y_c; the reverse pass
+// recomputes the stages of one block at a time from its pair.
 struct AdjSub {
   double dtl;
   int64_t s;
   std::vector<double> uj, vj, ubj, gj;
-  size_t t0;  // tape slots: t0 = u0, t0+1 = dty0, t0+1+k = Y_k (k = 1..s-1)
+  size_t t0;
+  int64_t q = 0;
+  std::vector<int64_t> cstart;        // block starts c
+  std::vector<size_t> ck_prev, ck_cur;  // tape slots of Y_{c-1} (SIZE_MAX: u0) and Y_c
+  size_t ring0 = 0;                   // first ring-checkpoint slot (2*nr doubles each)
 };
 }  // namespace
+
+// Stage spacing of the stage checkpoints for a super-step of s stages:
+// 0 (keep every stage) when s + 1 fields fit the tape budget, else an even
+// q near sqrt(2 s), which keeps about 2 sqrt(2 s) fields.
+static int64_t adj_stage_spacing(hipft_gpu *h, int64_t s) {
+  int64_t budget = h->adj_tape_limit;
+  if (budget <= 0) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+    budget = (int64_t)(fr / 2 / (h->fieldn * sizeof(double)));
+  }
+  if (h->adj_force_q > 0) return h->adj_force_q;
+  if (s + 1 <= budget) return 0;
+  int64_t q = (int64_t)std::ceil(std::sqrt(2.0 * (double)s));
+  if (q % 2) ++q;
+  return std::max<int64_t>(q, 2);
+}
 
 static int adj_slot(hipft_gpu *h, size_t n, double **p) {
   while (h->tape.size() <= n) {
@@ -2646,12 +2688,57 @@ static int adj_diff_fwd(hipft_gpu *h, double dtl, size_t &nt, std::vector<AdjSub
     S.ubj = h->sts_ubj;
     S.gj = h->sts_gj;
     S.t0 = nt;
+    S.q = adj_stage_spacing(h, S.s);
     double *u0, *dty0;
     TRY(adj_slot(h, nt++, &u0));
     TRY(adj_slot(h, nt++, &dty0));
     std::vector<double *> Y((size_t)S.s + 1, nullptr);
     Y[0] = u0;
-    for (int64_t k = 1; k <= S.s - 1; ++k) TRY(adj_slot(h, nt++, &Y[k]));
+    if (S.q == 0) {
+      for (int64_t k = 1; k <= S.s - 1; ++k) TRY(adj_slot(h, nt++, &Y[k]));
+    } else {
+      // block starts c = 1, 1+q, ... below s; their pairs (Y_{c-1}, Y_c) are
+      // tape slots, the other stages go through a rotating scratch set
+      for (int64_t c = 1; c <= S.s - 1; c += S.q) S.cstart.push_back(c);
+      for (size_t b = 0; b < S.cstart.size(); ++b) {
+        const int64_t c = S.cstart[b];
+        S.ck_prev.push_back(SIZE_MAX);
+        if (c > 1) {
+          S.ck_prev.back() = nt;
+          TRY(adj_slot(h, nt++, &Y[c - 1]));
+        }
+        S.ck_cur.push_back(nt);
+        TRY(adj_slot(h, nt++, &Y[c]));
+      }
+      S.ring0 = h->adj_rings_n;
+      h->adj_rings_n += S.cstart.size();
+      if (h->adj_rings_n > h->adj_rings_cap) {
+        // grown before any ring checkpoint of this step is written
+        double *nr_ = nullptr;
+        const size_t cap = h->adj_rings_n + 64;
+        TRY(dalloc(h, &nr_, cap * 2 * (size_t)h->nr));
+        if (h->d_adj_rings) {
+          CK(h, cudaMemcpyAsync(nr_, h->d_adj_rings, h->adj_rings_cap * 2 * (size_t)h->nr * sizeof(double),
+                                cudaMemcpyDeviceToDevice, h->stream));
+          CK(h, cudaStreamSynchronize(h->stream));
+          cudaFree(h->d_adj_rings);
+          h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)h->d_adj_rings), h->allocs.end());
+        }
+        h->d_adj_rings = nr_;
+        h->adj_rings_cap = cap;
+      }
+      // stages that are not checkpoints rotate through four scratch fields
+      // of the block buffer: a stage pair reads Y_{k-1}, Y_{k-2} and writes
+      // Y_k, Y_{k+1}, four distinct fields
+      while (h->adj_block.size() < 4) {
+        double *q = nullptr;
+        TRY(dalloc(h, &q, h->fieldn));
+        h->adj_block.push_back(q);
+      }
+      int rot = 0;
+      for (int64_t k = 1; k <= S.s - 1; ++k)
+        if (!Y[k]) Y[k] = h->adj_block[(rot++) % 4];
+    }
     Y[S.s] = h->buf[h->cur];
     CK(h, cudaMemcpyAsync(u0, h->buf[h->cur], h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
     // the same kernels, in the same order, as sts_super_step (with its pole
@@ -2663,14 +2750,26 @@ static int adj_diff_fwd(hipft_gpu *h, double dtl, size_t &nt, std::vector<AdjSub
       const double uj = S.uj[k], vj = S.vj[k];
       return StageCoef{uj, vj, 1.0 - uj - vj, S.ubj[k] * dtl2, S.gj[k]};
     };
+    // ring sums of a block start's Y_c (the ring of the launch's output)
+    auto keep_ring = [&](int64_t c) -> int {
+      if (S.q == 0) return HIPFT_OK;
+      for (size_t b = 0; b < S.cstart.size(); ++b)
+        if (S.cstart[b] == c)
+          CK(h, cudaMemcpyAsync(h->d_adj_rings + (S.ring0 + b) * 2 * (size_t)h->nr, h->d_ringbuf[h->ring_cur],
+                                2 * (size_t)h->nr * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+      return HIPFT_OK;
+    };
+    TRY(keep_ring(1));
     int64_t k = 2;
     while (k <= S.s) {
       if (sts_pairs_enabled() && k + 1 <= S.s) {
         TRY(sts_pair(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], Y[k + 1], coef(k), coef(k + 1), k > 2));
+        TRY(keep_ring(k + 1));
         k += 2;
         continue;
       }
       TRY(sts_stage_v2<MODE_STSK>(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], nullptr, coef(k)));
+      TRY(keep_ring(k));
       k += 1;
     }
     h->dring_valid = true;  // the last fused stage left the ring of the output
@@ -2723,6 +2822,43 @@ static int adj_adv_rev(hipft_gpu *h, double dtl, const size_t t[4], double *&W, 
 // cotangent of u0; dacc[i] += the diffusion-coefficient terms
 // sum mu~_k dt <A^T Wbar_k, Y_{k-1}> (+ dt <A^T dbar, u0>).  One launch per
 // stage: each leaves the pole-row partials of its output for the next.
+// Recomputes the stages Y_{c+1}..Y_e of stage-checkpoint block b (e = the
+// block's last stage input, at most s-1) from its pair (Y_{c-1}, Y_c) and the
+// ring sums of Y_c, with the replay's kernels and launch grouping, so the
+// values are bitwise those of the replay.  Y receives the block's fields.
+static int adj_block_recompute(hipft_gpu *h, const AdjSub &S, size_t b, std::vector<const double *> &Y) {
+  const int64_t c = S.cstart[b], e = std::min(c + S.q - 1, S.s - 1);
+  while ((int64_t)h->adj_block.size() < S.q + 1) {
+    double *q = nullptr;
+    TRY(dalloc(h, &q, h->fieldn));
+    h->adj_block.push_back(q);
+  }
+  const double *u0 = h->tape[S.t0], *dty0 = h->tape[S.t0 + 1];
+  std::vector<double *> Yw((size_t)S.s + 2, nullptr);
+  Yw[c - 1] = (S.ck_prev[b] == SIZE_MAX) ? const_cast<double *>(u0) : h->tape[S.ck_prev[b]];
+  Yw[c] = h->tape[S.ck_cur[b]];
+  for (int64_t k = c + 1; k <= std::min(e + 1, S.s); ++k) Yw[k] = h->adj_block[k - c - 1];
+  CK(h, cudaMemcpyAsync(h->d_ringbuf[h->ring_cur], h->d_adj_rings + (S.ring0 + b) * 2 * (size_t)h->nr,
+                        2 * (size_t)h->nr * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  auto coef = [&](int64_t k) {
+    const double uj = S.uj[k], vj = S.vj[k];
+    return StageCoef{uj, vj, 1.0 - uj - vj, S.ubj[k] * S.dtl, S.gj[k]};
+  };
+  int64_t k = c + 1;
+  while (k <= e) {
+    if (sts_pairs_enabled() && k + 1 <= S.s) {
+      TRY(sts_pair(h, Yw[k - 1], Yw[k - 2], u0, dty0, Yw[k], Yw[k + 1], coef(k), coef(k + 1), k > c + 1));
+      k += 2;
+      continue;
+    }
+    TRY(sts_stage_v2<MODE_STSK>(h, Yw[k - 1], Yw[k - 2], u0, dty0, Yw[k], nullptr, coef(k)));
+    k += 1;
+  }
+  for (int64_t q = c - 1; q <= e; ++q) Y[q] = Yw[q];
+  h->dring_valid = false;
+  return HIPFT_OK;
+}
+
 static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc) {
   const dim3 blk(32, 8), grd = stage_grid(h, 32, 8);
   const double dtl = S.dtl;
@@ -2731,7 +2867,13 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   CK(h, cudaMemsetAsync(ub, 0, h->fieldn * sizeof(double), h->stream));
   CK(h, cudaMemsetAsync(db, 0, h->fieldn * sizeof(double), h->stream));
   CK(h, cudaMemsetAsync(h->d_dpart, 0, (size_t)h->dpart_per_r * h->nr * sizeof(double), h->stream));
-  auto Yt = [&](int64_t k) -> const double * { return h->tape[S.t0 + (k == 0 ? 0 : 1 + k)]; };
+  // stage inputs Y_k: all on the tape (q == 0) or one recomputed block at a time
+  std::vector<const double *> Yr((size_t)S.s + 1, nullptr);
+  Yr[0] = h->tape[S.t0];
+  if (S.q == 0)
+    for (int64_t k = 1; k <= S.s - 1; ++k) Yr[k] = h->tape[S.t0 + 1 + k];
+  int64_t curb = -1;
+  auto Yt = [&](int64_t k) -> const double * { return Yr[k]; };
   const double *gin = h->d_gring;
   int npin = 1, pp = 0;
   auto pole_sums = [&](const double *w) -> int {
@@ -2755,6 +2897,10 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   TRY(pole_sums(W));
   double *Wk = W, *Wk1 = nullptr;
   for (int64_t k = S.s; k >= 2; --k) {
+    if (S.q > 0 && (k - 2) / S.q != curb) {
+      curb = (k - 2) / S.q;  // the block holding Y_{k-1}
+      TRY(adj_block_recompute(h, S, (size_t)curb, Yr));
+    }
     double *Wm = adj_free(h, {Wk, Wk1, ub, db});
     const double uj = S.uj[k], vj = S.vj[k];
     const double nu1 = (k < S.s) ? S.vj[k + 1] : 0.0;
@@ -2792,6 +2938,7 @@ extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, doubl
   const size_t bytes = h->fieldn * sizeof(double);
   CK(h, cudaMemcpyAsync(h->buf[h->cur], f_in, bytes, cudaMemcpyDeviceToDevice, h->stream));
   h->dring_valid = false;
+  h->adj_rings_n = 0;
   size_t nt = 0, ta1[4] = {}, ta2[4] = {};
   std::vector<AdjSub> subs;
   const bool strang = h->P.strang_splitting != 0;
@@ -2807,12 +2954,52 @@ extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, doubl
   CK(h, cudaMemcpyAsync(fbar, W, bytes, cudaMemcpyDeviceToDevice, h->stream));
   CK(h, cudaStreamSynchronize(h->stream));
   CK(h, cudaGetLastError());
+  h->dring_valid = false;
   return HIPFT_OK;
 }
 
 extern "C" int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n) {
   if (!h || !n) return HIPFT_EINVAL;
-  *n = (int64_t)h->tape.size();
+  *n = (int64_t)(h->tape.size() + h->adj_block.size());
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_set_tape_limit(hipft_gpu *h, int64_t max_fields, int64_t stage_spacing) {
+  if (!h || max_fields < 0 || stage_spacing < 0 || stage_spacing % 2) return HIPFT_EINVAL;
+  h->adj_tape_limit = max_fields;
+  h->adj_force_q = stage_spacing;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_release(hipft_gpu *h) {
+  if (!h) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaStreamSynchronize(h->stream));
+  auto drop = [&](void *p) {
+    if (!p) return;
+    cudaFree(p);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
+    h->dev_bytes -= h->fieldn * sizeof(double);
+  };
+  for (double *q : h->tape) drop(q);
+  for (double *q : h->adj_block) drop(q);
+  h->tape.clear();
+  h->adj_block.clear();
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o, double *fbar) {
+  if (!h || !data3_pt || !o || !fbar) return HIPFT_EINVAL;
+  if (!o->lat_limit || (o->custom_from_mu && (!o->mu_power || !o->mu_limit)))
+    return fail(h, HIPFT_EINVAL, "adj_assimilate: missing per-realization options");
+  if (o->balance_flux) return fail(h, HIPFT_ESTATE, "adj_assimilate: the balanced increment is not differentiated");
+  CK(h, cudaSetDevice(h->dev));
+  DAArgs a;
+  TRY(da_args(h, data3_pt, o, a));
+  dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)h->nr);
+  k_adj_da<<<grd, blk, 0, h->stream>>>(h->M, a, fbar);
+  LAUNCHED(h);
+  CK(h, cudaStreamSynchronize(h->stream));
   return HIPFT_OK;
 }
 

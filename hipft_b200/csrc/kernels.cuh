@@ -280,6 +280,13 @@ struct Weno {
 
 // WENO3 face flux (src/hipft.f90:7775-7801).  LN*: LN(j-2), LN(j-1), LN(j);
 // LP*: LP(j-1), LP(j), LP(j+1); weights at indices j-1 (m1) and j (0).
+// The reference normalises the nonlinear weights, OM = w / (w0 + w1) with
+// w0m = D_P_T(j-1)/e0^2, w1m = D_MC_T(j-1)/e1^2, and sums OM*p.  Multiplying
+// each side's numerator and denominator by e0^2 e1^2 gives the same value
+// with one division per side instead of four:
+//   um = (a p0m + b p1m) / (a + b),  a = D_P_T(j-1) e1^2,  b = D_MC_T(j-1) e0^2
+// (likewise up).  The result differs from the reference's operation order by
+// rounding only.
 __device__ __forceinline__ double weno_face(double LNm2, double LNm1, double LN0, double LPm1, double LP0,
                                             double LPp1, double DCMC_m1, double DCMC_0, double DCCP_m1,
                                             double DCCP_0, double DPT_m1, double DMCT_m1, double DMT_0,
@@ -290,18 +297,12 @@ __device__ __forceinline__ double weno_face(double LNm2, double LNm1, double LN0
   double p1p = DCCP_m1 * LP0 + DCMC_0 * LPm1;
   double t0 = DCMC_m1 * (LNm1 - LNm2), t1 = DCCP_m1 * (LN0 - LNm1);
   double t2 = DCCP_0 * (LPp1 - LP0), t3 = DCMC_0 * (LP0 - LPm1);
-  double B0m = kFour * (t0 * t0), B1m = kFour * (t1 * t1);
-  double B0p = kFour * (t2 * t2), B1p = kFour * (t3 * t3);
-  double e0 = eps_m1 + B0m, e1 = eps_m1 + B1m, e2 = eps_0 + B0p, e3 = eps_0 + B1p;
-  double w0m = DPT_m1 / (e0 * e0);
-  double w1m = DMCT_m1 / (e1 * e1);
-  double w0p = DMT_0 / (e2 * e2);
-  double w1p = DCPT_0 / (e3 * e3);
-  double wm_sum = w0m + w1m, wp_sum = w0p + w1p;
-  double OM0m = w0m / wm_sum, OM1m = w1m / wm_sum;
-  double OM0p = w0p / wp_sum, OM1p = w1p / wp_sum;
-  double um = OM0m * p0m + OM1m * p1m;
-  double up = OM0p * p0p + OM1p * p1p;
+  double e0 = eps_m1 + kFour * (t0 * t0), e1 = eps_m1 + kFour * (t1 * t1);
+  double e2 = eps_0 + kFour * (t2 * t2), e3 = eps_0 + kFour * (t3 * t3);
+  double am = DPT_m1 * (e1 * e1), bm = DMCT_m1 * (e0 * e0);
+  double ap = DMT_0 * (e3 * e3), bp = DCPT_0 * (e2 * e2);
+  double um = (am * p0m + bm * p1m) / (am + bm);
+  double up = (ap * p0p + bp * p1p) / (ap + bp);
   return up + um;
 }
 
@@ -347,114 +348,166 @@ __device__ __forceinline__ int wrap_cell(const Mesh &m, int c) {
   return c;
 }
 
-// Tile of TJ x TK cells; block is TJ x TK threads.
+// One explicit advection stage over a tile of TJ x TK cells: face fluxes
+// (WENO3 or upwind), divergence (src/hipft.f90:7890-7898), pole rows from the
+// ring sums, seam, and the integrator's combine.  The block is (TJ+1) x
+// (TK+1) threads: thread (a, b) computes the theta face j0+a of column k0+b
+// (b < TK) and the phi face k0+b of row j0+a (a < TJ), then the cell (a, b)
+// (a < TJ, b < TK); no thread computes more than two faces.  The input tile
+// (halo 2, phi wrapped with the reference's periodic pad), the WENO weights of
+// the tile's faces and, for 1-D flows, the per-row flow terms v +/- alpha
+// are staged in shared memory first.
+// Ragged batches: rlist (may be null) maps grid slice z to a realization, and
+// rdt (may be null) holds each realization's substep, which multiplies cb.C.
 template <int TJ, int TK>
 struct AdvSmem {
-  double x[TJ + 4][TK + 4];  // rows j0-2..j0+TJ+1, cols k0-2..k0+TK+1
-  double ft[TJ + 1][TK];     // theta faces j0..j0+TJ
-  double fp[TJ][TK + 1];     // phi faces k0..k0+TK
+  double x[TK + 4][TJ + 4];   // column k0-2+b, row j0-2+a
+  double ft[TK][TJ + 1];      // theta faces j0..j0+TJ of column k0+b
+  double fp[TK + 1][TJ];      // phi faces k0..k0+TK of row j0+a
+  double wt[10][TJ + 1];      // theta weights of face j0+a, in weno_face's argument order
+  double wp[10][TK + 1];      // phi weights of face k0+b
+  double tn[TJ + 4], tp[TJ + 4];  // 1-D flows: vt(c)+at(c), vt(c+1)-at(c) at row c = j0-2+a
+  double pn[TJ], pp[TJ];          // 1-D flows: vp(j)+ap(j), vp(j)-ap(j) at row j = j0+a
 };
 
-// One explicit advection stage over a tile: face fluxes (WENO3 or upwind),
-// divergence (src/hipft.f90:7890-7898), pole rows from the ring sums, seam,
-// and the integrator's combine.  Ragged batches: rlist (may be null) maps grid
-// slice z to a realization, and rdt (may be null) holds each realization's
-// substep, which multiplies cb.C.
 template <int TJ, int TK, bool WENO>
-__global__ void __launch_bounds__(TJ *TK) k_advection_stage(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
-                                                            const double *__restrict__ f0, double *out,
-                                                            const double *__restrict__ ring, double bcn, double bcs,
-                                                            AdvCombine cb, const int *__restrict__ rlist = nullptr,
-                                                            const double *__restrict__ rdt = nullptr) {
+__global__ void __launch_bounds__((TJ + 1) * (TK + 1)) k_advection_stage(
+    Mesh m, Flow fl, Weno wn, const double *__restrict__ x, const double *__restrict__ f0, double *out,
+    const double *__restrict__ ring, double bcn, double bcs, AdvCombine cb, const int *__restrict__ rlist = nullptr,
+    const double *__restrict__ rdt = nullptr) {
   __shared__ AdvSmem<TJ, TK> s;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = tx + ty * TJ;
+  constexpr int NT = (TJ + 1) * (TK + 1);
+  static_assert(TJ + 1 <= 64 && TK + 1 <= 64 && TJ + 4 <= 64 && TJ <= 64 && NT >= 192 + TJ,
+                "staging thread ranges 0.., 64.., 128.., 192..");
+  const int a = threadIdx.x, b = threadIdx.y;
+  const int tid = a + b * (TJ + 1);
   const int j0 = blockIdx.x * TJ + 1;
   const int k0 = blockIdx.y * TK + 2;
   const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   if (rdt) cb.C = cb.C * rdt[i - 1];
   const int ntm = m.ntm, npm = m.npm;
+  const int64_t pbase = (int64_t)(i - 1) * m.plane;
+  const bool oned = !fl.flow2d;
 
-  // x tile with halo 2 (theta clipped to 1..ntm, phi wrapped periodically).
-  for (int e = tid; e < (TJ + 4) * (TK + 4); e += TJ * TK) {
-    int a = e % (TJ + 4), b = e / (TJ + 4);
-    int j = j0 - 2 + a, k = wrap_cell(m, k0 - 2 + b);
-    double v = 0.0;
-    if (j >= 1 && j <= ntm) v = x[fidx(m, j, k, i)];
-    s.x[a][b] = v;
+  // input tile with halo 2 (theta clipped to 1..ntm, phi wrapped periodically)
+  for (int e = tid; e < (TJ + 4) * (TK + 4); e += NT) {
+    const int r = e % (TJ + 4), c = e / (TJ + 4);
+    const int j = j0 - 2 + r, k = wrap_cell(m, k0 - 2 + c);
+    s.x[c][r] = (j >= 1 && j <= ntm) ? x[pbase + (int64_t)(k - 1) * m.ldt + (j - 1)] : 0.0;
+  }
+  if (WENO) {
+    if (tid < TJ + 1) {
+      const int r = tid, jf = min(max(j0 + r, 2), m.nt - 1);
+      s.wt[0][r] = wn.mct[jf - 1];
+      s.wt[1][r] = wn.mct[jf];
+      s.wt[2][r] = wn.cpt[jf - 1];
+      s.wt[3][r] = wn.cpt[jf];
+      s.wt[4][r] = wn.pt[jf - 1];
+      s.wt[5][r] = wn.mctt[jf - 1];
+      s.wt[6][r] = wn.mt[jf];
+      s.wt[7][r] = wn.cptt[jf];
+      s.wt[8][r] = wn.epst[jf - 1];
+      s.wt[9][r] = wn.epst[jf];
+    } else if (tid >= 64 && tid < 64 + TK + 1) {
+      const int c = tid - 64;
+      const int kw = (k0 + c >= npm) ? 2 : k0 + c;  // face npm copies face 2 (src/hipft.f90:7882)
+      s.wp[0][c] = wn.mcp[kw - 1];
+      s.wp[1][c] = wn.mcp[kw];
+      s.wp[2][c] = wn.cpp[kw - 1];
+      s.wp[3][c] = wn.cpp[kw];
+      s.wp[4][c] = wn.pp[kw - 1];
+      s.wp[5][c] = wn.mctp[kw - 1];
+      s.wp[6][c] = wn.mp[kw];
+      s.wp[7][c] = wn.cptp[kw];
+      s.wp[8][c] = wn.epsp[kw - 1];
+      s.wp[9][c] = wn.epsp[kw];
+    }
+  }
+  if (oned) {
+    const double *vt = fl.vt1 + (int64_t)(i - 1) * (m.nt + 1), *at = fl.at1 + (int64_t)(i - 1) * (m.ntm + 1);
+    const double *vp = fl.vp1 + (int64_t)(i - 1) * (m.ntm + 1), *ap = fl.ap1 + (int64_t)(i - 1) * (m.ntm + 1);
+    const int e = tid - 128;  // threads 128.. (the weight loads use 0..63, 64..)
+    if (e >= 0 && e < TJ + 4) {
+      const int c = j0 - 2 + e;
+      const bool ok = (c >= 1 && c <= ntm);
+      s.tn[e] = ok ? vt[c] + at[c] : 0.0;
+      s.tp[e] = ok ? vt[c + 1] - at[c] : 0.0;
+    }
+    const int f = tid - 192;
+    if (f >= 0 && f < TJ) {
+      const int j = j0 + f;
+      const bool ok = (j >= 1 && j <= ntm);
+      s.pn[f] = ok ? vp[j] + ap[j] : 0.0;
+      s.pp[f] = ok ? vp[j] - ap[j] : 0.0;
+    }
   }
   __syncthreads();
 
-  // theta faces j = j0 .. j0+TJ for columns k0..k0+TK-1
-  for (int e = tid; e < (TJ + 1) * TK; e += TJ * TK) {
-    int a = e % (TJ + 1), b = e / (TJ + 1);
-    int jf = j0 + a, k = k0 + b;
+  // theta face jf = j0 + a of column k = k0 + b
+  if (b < TK) {
+    const int jf = j0 + a, k = k0 + b;
     double F = 0.0;
     if (k <= npm - 1 && jf >= 2 && jf <= ntm) {
-      double xa = s.x[a + 2][b + 2], xb = s.x[a + 1][b + 2];  // x(jf), x(jf-1)
+      const double *xc = &s.x[b + 2][0];
+      const double xa = xc[a + 2], xb = xc[a + 1];  // x(jf), x(jf-1)
       if (!WENO || jf == 2 || jf == ntm) {
         F = upwind_flux(vt_at(m, fl, jf, k, i), fl.upwind, xa, xb);
       } else {
-        // LP(c) = half*x(c)*(vt(c+1)-alpha_t(c)), LN(c) = half*x(c)*(vt(c)+alpha_t(c))
+        // LN(c) = half*x(c)*(vt(c)+alpha_t(c)), LP(c) = half*x(c)*(vt(c+1)-alpha_t(c))
         double LN[3], LP[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          int c = jf - 2 + d;  // LN at jf-2, jf-1, jf
-          double xc = s.x[a + d][b + 2];
-          LN[d] = kHalf * xc * (vt_at(m, fl, c, k, i) + at_at(m, fl, c, k, i));
+          const int c = jf - 2 + d;  // LN at jf-2, jf-1, jf (shared row a + d)
+          const double v = oned ? s.tn[a + d] : vt_at(m, fl, c, k, i) + at_at(m, fl, c, k, i);
+          LN[d] = kHalf * xc[a + d] * v;
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          int c = jf - 1 + d;  // LP at jf-1, jf, jf+1
-          double xc = s.x[a + 1 + d][b + 2];
-          LP[d] = kHalf * xc * (vt_at(m, fl, c + 1, k, i) - at_at(m, fl, c, k, i));
+          const int c = jf - 1 + d;  // LP at jf-1, jf, jf+1 (shared row a + 1 + d)
+          const double v = oned ? s.tp[a + 1 + d] : vt_at(m, fl, c + 1, k, i) - at_at(m, fl, c, k, i);
+          LP[d] = kHalf * xc[a + 1 + d] * v;
         }
-        F = weno_face(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mct[jf - 1], wn.mct[jf], wn.cpt[jf - 1],
-                      wn.cpt[jf], wn.pt[jf - 1], wn.mctt[jf - 1], wn.mt[jf], wn.cptt[jf], wn.epst[jf - 1],
-                      wn.epst[jf]);
+        F = weno_face(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], s.wt[0][a], s.wt[1][a], s.wt[2][a], s.wt[3][a],
+                      s.wt[4][a], s.wt[5][a], s.wt[6][a], s.wt[7][a], s.wt[8][a], s.wt[9][a]);
       }
     }
-    s.ft[a][b] = F;
+    s.ft[b][a] = F;
   }
-
-  // phi faces k = k0 .. k0+TK for rows j0..j0+TJ-1 (interior rows only).
-  // Face npm is the seam copy of face 2 (src/hipft.f90:7882): its stencil
-  // cells are the seam copies of face 2's cells, and it takes face 2's
-  // weights (index kw).
-  for (int e = tid; e < TJ * (TK + 1); e += TJ * TK) {
-    int a = e % TJ, b = e / TJ;
-    int j = j0 + a;
-    int kf = k0 + b;
+  // phi face kf = k0 + b of row j = j0 + a (interior rows only).  Face npm is
+  // the seam copy of face 2 (src/hipft.f90:7882): its stencil cells are the
+  // seam copies of face 2's cells, and it takes face 2's weights.
+  if (a < TJ) {
+    const int j = j0 + a, kf = k0 + b;
     double F = 0.0;
     if (j >= 2 && j <= ntm - 1 && kf <= npm) {
-      int kw = (kf == npm) ? 2 : kf;
-      int bb = b + 2;  // smem column of cell kf
+      const int kw = (kf == npm) ? 2 : kf;
+      const int bb = b + 2;  // shared column of cell kf
       if (!WENO) {
-        F = upwind_flux(vp_at(m, fl, j, kw, i), fl.upwind, s.x[a + 2][bb], s.x[a + 2][bb - 1]);
+        F = upwind_flux(vp_at(m, fl, j, kw, i), fl.upwind, s.x[bb][a + 2], s.x[bb - 1][a + 2]);
       } else {
         double LN[3], LP[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          int c = wrap_cell(m, kf - 2 + d);
-          double xc = s.x[a + 2][bb - 2 + d];
-          LN[d] = kHalf * xc * (vp_at(m, fl, j, c, i) + ap_at(m, fl, j, c, i));
+          const int c = wrap_cell(m, kf - 2 + d);
+          const double v = oned ? s.pn[a] : vp_at(m, fl, j, c, i) + ap_at(m, fl, j, c, i);
+          LN[d] = kHalf * s.x[bb - 2 + d][a + 2] * v;
         }
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          int c = wrap_cell(m, kf - 1 + d);
-          double xc = s.x[a + 2][bb - 1 + d];
-          LP[d] = kHalf * xc * (vp_at(m, fl, j, c + 1, i) - ap_at(m, fl, j, c, i));
+          const int c = wrap_cell(m, kf - 1 + d);
+          const double v = oned ? s.pp[a] : vp_at(m, fl, j, c + 1, i) - ap_at(m, fl, j, c, i);
+          LP[d] = kHalf * s.x[bb - 1 + d][a + 2] * v;
         }
-        F = weno_face(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mcp[kw - 1], wn.mcp[kw], wn.cpp[kw - 1],
-                      wn.cpp[kw], wn.pp[kw - 1], wn.mctp[kw - 1], wn.mp[kw], wn.cptp[kw], wn.epsp[kw - 1],
-                      wn.epsp[kw]);
+        F = weno_face(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], s.wp[0][b], s.wp[1][b], s.wp[2][b], s.wp[3][b],
+                      s.wp[4][b], s.wp[5][b], s.wp[6][b], s.wp[7][b], s.wp[8][b], s.wp[9][b]);
       }
     }
-    s.fp[a][b] = F;
+    s.fp[b][a] = F;
   }
   __syncthreads();
 
-  const int j = j0 + tx, k = k0 + ty;
+  if (a >= TJ || b >= TK) return;
+  const int j = j0 + a, k = k0 + b;
   if (j > ntm || k > npm - 1) return;
   double aop;
   if (j == 1) {
@@ -462,11 +515,11 @@ __global__ void __launch_bounds__(TJ *TK) k_advection_stage(Mesh m, Flow fl, Wen
   } else if (j == ntm) {
     aop = -ring[2 * (i - 1) + 1] * bcs;
   } else {
-    aop = ((m.sth[j + 1] * s.ft[tx + 1][ty] - m.sth[j] * s.ft[tx][ty]) * m.st_i[j] * m.dt_i[j] +
-           (s.fp[tx][ty + 1] - s.fp[tx][ty]) * m.st_i[j] * m.dp_i[k]);
+    aop = ((m.sth[j + 1] * s.ft[b][a + 1] - m.sth[j] * s.ft[b][a]) * m.st_i[j] * m.dt_i[j] +
+           (s.fp[b + 1][a] - s.fp[b][a]) * m.st_i[j] * m.dp_i[k]);
   }
-  int64_t q = fidx(m, j, k, i);
-  double xv = s.x[tx + 2][ty + 2];
+  const int64_t q = pbase + (int64_t)(k - 1) * m.ldt + (j - 1);
+  const double xv = s.x[b + 2][a + 2];
   double y;
   if (cb.mode == 0) {
     y = xv - cb.C * aop;
@@ -836,13 +889,30 @@ struct DAArgs {
   double mult_fac;
 };
 
+// Blend weight of PT cell (theta jt, phi kp) for realization i
+// (src/hipft.f90:4242-4271): the map's weight slice, or mu^power where
+// mu > mu_limit; zero inside the latitude caps.
+__device__ __forceinline__ double da_weight(const Mesh &m, const DAArgs &a, int jt, int kp, int i) {
+  const int npm1 = m.npm - 1;
+  const int64_t slice = (int64_t)npm1 * m.ntm;
+  const int64_t q = (int64_t)(jt - 1) * npm1 + (kp - 1);
+  double w;
+  if (a.custom_from_mu) {
+    double mu = a.data[2 * slice + q];
+    w = (mu > a.mu_limit[i]) ? pow(mu, a.mu_power[i]) : 0.0;
+  } else {
+    w = a.data[slice + q];
+  }
+  if (a.lat_limit[i] > 0 && (jt <= a.tidx0[i] || jt >= a.tidx1[i])) w = 0.0;
+  return w;
+}
+
 __global__ void k_da_delta(Mesh m, DAArgs a, const double *__restrict__ f, double *delta) {
   __shared__ double sd[32][33], sw[32][33];
   const int npm1 = m.npm - 1;
   const int i = blockIdx.z + 1;
   const int j0 = blockIdx.x * 32 + 1;   // theta tile start
   const int k0 = blockIdx.y * 32 + 1;   // phi tile start
-  const int64_t slice = (int64_t)npm1 * m.ntm;
   // load: thread (tx,ty) reads phi = k0+tx, theta = j0+ty+8r
   for (int r = 0; r < 4; ++r) {
     int jt = j0 + threadIdx.y + 8 * r, kp = k0 + threadIdx.x;
@@ -850,13 +920,7 @@ __global__ void k_da_delta(Mesh m, DAArgs a, const double *__restrict__ f, doubl
     if (jt <= m.ntm && kp <= npm1) {
       int64_t q = (int64_t)(jt - 1) * npm1 + (kp - 1);
       d = a.data[q];
-      if (a.custom_from_mu) {
-        double mu = a.data[2 * slice + q];
-        w = (mu > a.mu_limit[i]) ? pow(mu, a.mu_power[i]) : 0.0;
-      } else {
-        w = a.data[slice + q];
-      }
-      if (a.lat_limit[i] > 0 && (jt <= a.tidx0[i] || jt >= a.tidx1[i])) w = 0.0;
+      w = da_weight(m, a, jt, kp, i);
       d = a.mult_fac * d;
     }
     sd[threadIdx.y + 8 * r][threadIdx.x] = d;

@@ -138,6 +138,9 @@ SIGNATURES = [
     ("hipft_gpu_source_step", ctypes.c_int, [_H, ctypes.c_double]),
     ("hipft_h5_write", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int64), DPTR, DPTR,
                                       DPTR, DPTR, ctypes.c_int]),
+    ("hipft_adj_set_tape_limit", ctypes.c_int, [_H, ctypes.c_int64, ctypes.c_int64]),
+    ("hipft_adj_release", ctypes.c_int, [_H]),
+    ("hipft_adj_assimilate", ctypes.c_int, [_H, DPTR, ctypes.POINTER(DAOpts), ctypes.c_void_p]),
     ("hipft_gpu_set_ragged", ctypes.c_int, [_H, ctypes.c_int]),
     ("hipft_gpu_flow_dtmax_each", ctypes.c_int, [_H, DPTR]),
     ("hipft_gpu_ragged_schedule", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),

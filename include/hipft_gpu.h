@@ -381,6 +381,24 @@ int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, do
 int hipft_gpu_set_field_device(hipft_gpu *h, const double *f_dev);
 /* Fields the adjoint's tape holds (device memory, fieldn doubles each). */
 int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n);
+/* Tape budget of hipft_adj_step.  A super-step of s RKG2 stages keeps all
+ * s+1 stage fields when they fit max_fields (0: half of the free device
+ * memory at the time); otherwise it keeps stage checkpoints -- the pair
+ * (Y_{c-1}, Y_c) every q stages, q even near sqrt(2 s) -- and the reverse pass
+ * recomputes one block of q stages at a time from its pair (about
+ * 2 sqrt(2 s) fields, one more forward pass of the diffusion).
+ * stage_spacing > 0 (even) forces that q.  Results do not depend on q. */
+int hipft_adj_set_tape_limit(hipft_gpu *h, int64_t max_fields, int64_t stage_spacing);
+/* Frees the tape (it grows to the largest step seen and is otherwise kept
+ * until the handle is destroyed). */
+int hipft_adj_release(hipft_gpu *h);
+/* Reverse of one data-assimilation blend (apply_data_assimilation,
+ * src/hipft.f90:4116-4141, same map and options as the forward call):
+ * fbar (device, the handle's layout, folded) becomes (1 - w) fbar on every
+ * core cell for the blend f += w (d - f), and is unchanged for the additive
+ * form f += w d.  The balanced increment (balance_flux, 8794-8801) is not
+ * differentiated (HIPFT_ESTATE). */
+int hipft_adj_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o, double *fbar);
 
 /* ---- map files ------------------------------------------------------------- */
 

@@ -9,7 +9,7 @@ import torch
 import adjoint_cases as C
 from adjoint_ref import RefScheme
 from hipft_b200 import gpu as G
-from hipft_b200.adjoint import FLOW_KEYS, MisfitAdjoint, chain_physical
+from hipft_b200.adjoint import FLOW_KEYS, FluxTransport, MisfitAdjoint, chain_physical, misfit_weights, mesh_1d
 
 pytestmark = pytest.mark.gpu
 
@@ -123,7 +123,7 @@ def test_adjoint_matches_finite_differences_of_library_forward():
                 g.flux_transport_step(float(dt))
             return A.loss_and_cotangent(g.get_field(), target)[0]
 
-    for name, i in (("D", 0), ("D", 1), ("p2", 0), ("p1", 1), ("p3", 0)):
+    for name, i in (("D", 0), ("D", 1), ("p0", 0), ("p2", 0), ("p4", 1), ("p1", 1), ("p3", 0), ("p5", 1)):
         base = D if name == "D" else coef[name]
         h = 1e-6 * abs(base[i])
         vals = []
@@ -139,3 +139,122 @@ def test_adjoint_matches_finite_differences_of_library_forward():
     h = 1e-6 * np.max(np.abs(f0))
     fd = (loss_at(D, coef, f0 + h * dirn) - loss_at(D, coef, f0 - h * dirn)) / (2 * h)
     assert abs(float(np.sum(grads["f0"] * dirn)) - fd) <= FD_TOL * abs(fd), (np.sum(grads["f0"] * dirn), fd)
+
+
+def test_autograd_function_matches_restatement():
+    """FluxTransport (torch.autograd.Function over the library's forward and
+    adjoint) inside an ordinary torch loss: its gradients equal the
+    restatement's autograd gradients."""
+    f0, target, dts, D, coef = _inputs()
+    t, p = C.mesh_tp()
+    run = FluxTransport(t, p, dts, checkpoint_every=2, diffusion_subcycles=C.CASE["diffusion_subcycles"])
+    f0v = torch.tensor(f0, requires_grad=True)
+    Dv = torch.tensor(D, requires_grad=True)
+    cv = {k: torch.tensor(v, requires_grad=True) for k, v in coef.items()}
+    fN = run(f0v, Dv, cv)
+    w = torch.tensor(misfit_weights(mesh_1d(t, p)))[None]
+    loss = 0.5 * (w * (fN - torch.tensor(target)) ** 2).sum()
+    loss.backward()
+    grads = {"f0": f0v.grad.numpy(), "D": Dv.grad.numpy()}
+    grads.update({k: cv[k].grad.numpy() for k in FLOW_KEYS})
+    _check_against_reference(loss.item(), grads, *_reference_grads(f0, target, dts, D, coef))
+
+
+def _da_map(seed=3):
+    t, p = C.mesh_tp()
+    rng = np.random.default_rng(seed)
+    data = 5.0 * np.cos(t)[:, None] * np.ones((1, len(p))) + rng.standard_normal((len(t), len(p)))
+    mu = np.sin(t)[:, None] * np.cos(p[None, :] - 0.4)
+    data[:, -1] = data[:, 0]
+    mu[:, -1] = mu[:, 0]
+    return np.stack([data, np.zeros_like(mu), mu])
+
+
+def test_adjoint_through_assimilation_matches_restatement():
+    """An assimilation blend (mu^4 weights, mu > 0.1) after the first step:
+    the hand-written reverse of the blend (hipft_adj_assimilate) against
+    autograd of the restatement with the same blend."""
+    f0, target, dts, D, coef = _inputs()
+    t, p = C.mesh_tp()
+    m3 = _da_map()
+    opts = dict(custom_from_mu=True, mu_power=4.0, mu_limit=0.1)
+    with _handle(D, coef) as g:
+        A = MisfitAdjoint(g, D, coef, checkpoint_every=2, assim={0: (m3, opts)})
+        loss, grads = A.run(f0, target, dts)
+    # the restatement, split at the assimilation
+    S = RefScheme(t, p, len(D))
+    f0v = torch.tensor(f0, requires_grad=True)
+    Dv = torch.tensor(D, requires_grad=True)
+    cv = {k: torch.tensor(v, requires_grad=True) for k, v in coef.items()}
+    sc = C.CASE["diffusion_subcycles"]
+    f = S.run(f0v, dts[:1], Dv, cv, sc, S.euler_dt(D))
+    mu = m3[2]
+    w = np.where(mu > 0.1, mu ** 4.0, 0.0)          # (ntm, npm1): map column c is field column c (0-based)
+    Wc = torch.tensor(w[:, 1:].T)[None]             # core field columns 1..npm-2 (0-based)
+    Dd = torch.tensor(m3[0][:, 1:].T)[None]
+    core = f[:, 1:-1] + Wc * (Dd - f[:, 1:-1])
+    f = S._seam(core)
+    f = S.run(f, dts[1:], Dv, cv, sc, S.euler_dt(D))
+    L = S.misfit(f, torch.tensor(target))
+    L.backward()
+    gr = {"f0": f0v.grad.numpy(), "D": Dv.grad.numpy()}
+    gr.update({k: cv[k].grad.numpy() for k in FLOW_KEYS})
+    _check_against_reference(loss, grads, L.item(), gr)
+
+
+def test_stage_checkpoints_do_not_change_the_gradient():
+    """Stage checkpoints inside the RKG2 super-steps (the reverse recomputes
+    each block of q stages from its pair) give bitwise the gradient of the
+    full tape, with fewer tape fields."""
+    _, r, dts = C.rough_run()
+    D = np.array(C.CASE["diffusion_coef_constants"])
+    coef = {k: np.array(C.CASE[v]) for k, v in C.FLOW.items()}
+    f0 = r["map_initial"]
+    target = C.target_field(f0)
+    out, tapes = [], []
+    for q in (0, 2, 4):
+        with _handle(D, coef, subcycles=0) as g:
+            g.L.hipft_adj_set_tape_limit(g.h, 0, q)
+            A = MisfitAdjoint(g, D, coef, checkpoint_every=2)
+            out.append(A.run(f0, target, dts))
+            n = __import__("ctypes").c_int64(0)
+            g.L.hipft_adj_tape_fields(g.h, __import__("ctypes").byref(n))
+            tapes.append(n.value)
+            A.release()
+            g.L.hipft_adj_tape_fields(g.h, __import__("ctypes").byref(n))
+            assert n.value == 0
+    for loss, grads in out[1:]:
+        assert loss == out[0][0]
+        for key in grads:
+            assert np.array_equal(grads[key], out[0][1][key]), key
+    assert tapes[1] < tapes[0], tapes
+
+
+def test_adjoint_matches_restatement_128x256():
+    """The restatement comparison on a 128 x 256 grid (the adjoint
+    configuration's small grid)."""
+    case = dict(C.CASE, res_nt=128, res_np=257, time_end=40.0, dt_max=20.0,
+                diffusion_coef_constants=[600.0, 1500.0])
+    p_, r, dts = C.oracle_run(case)
+    D = np.array(case["diffusion_coef_constants"])
+    coef = {k: np.array(case[v]) for k, v in C.FLOW.items()}
+    f0 = r["map_initial"]
+    target = C.target_field(f0)
+    t, p = C.mesh_tp(case)
+    g = G.HipftGPU(t, p, case["n_realizations"], advance_flow=True, flow_num_method=4, strang_splitting=True,
+                   advance_diffusion=True, diffusion_num_method=3, diffusion_subcycles=case["diffusion_subcycles"],
+                   diffusion_coef_constants=D)
+    g.set_flow(dr_model=1, mf_model=1, dr_p0=coef["p0"], dr_p2=coef["p2"], dr_p4=coef["p4"], mf_p1=coef["p1"],
+               mf_p3=coef["p3"], mf_p5=coef["p5"])
+    with g:
+        loss, grads = MisfitAdjoint(g, D, coef, checkpoint_every=1).run(f0, target, dts)
+    S = RefScheme(t, p, len(D))
+    f0v = torch.tensor(f0, requires_grad=True)
+    Dv = torch.tensor(D, requires_grad=True)
+    cv = {k: torch.tensor(v, requires_grad=True) for k, v in coef.items()}
+    f = S.run(f0v, dts, Dv, cv, case["diffusion_subcycles"], S.euler_dt(D))
+    L = S.misfit(f, torch.tensor(target))
+    L.backward()
+    gr = {"f0": f0v.grad.numpy(), "D": Dv.grad.numpy()}
+    gr.update({k: cv[k].grad.numpy() for k in FLOW_KEYS})
+    _check_against_reference(loss, grads, L.item(), gr)
