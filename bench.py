@@ -417,6 +417,7 @@ def run_gpu(args, wl, name):
         "clocks": clk,
         "realization_steps_per_s": real_steps_per_s,
     }
+    out["config"]["kernels"] = g.describe()
     if sched is not None:
         out["config"]["rkg2_stages_per_realization"] = [int(x) for x in sched["sts_s"]]
         out["config"]["subcycles_per_realization"] = [int(x) for x in sched["subcycles"]]
@@ -534,12 +535,15 @@ def measure_plain(args, local: int):
     return out
 
 
-def measure_adjoint(args, local: int, nsteps: int = 16):
-    """Gradient / forward cost of the misfit adjoint on a 512 x 1024 uniform
-    grid with the plain configuration's physics (one realization, PTL
-    subcycling): wall time of hipft_b200.adjoint.MisfitAdjoint.run (forward
-    with checkpoints, misfit, reverse) over `nsteps` steps, against the same
-    steps through the library's forward alone (field copied in and out).  The
+def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int = 64):
+    """Gradient / forward cost of the misfit adjoint on the adjoint
+    configuration: 512 x 1024 uniform grid, one realization, the plain
+    configuration's physics (D 300 km^2/s, v0 15 m/s, B -2.40, C -1.80
+    deg/day) with PTL subcycling, `days` of model time at the CFL-limited dt,
+    a checkpoint every `checkpoint_every` steps (so the segment recompute is
+    inside the gradient's time).  Wall time of MisfitAdjoint.run (forward with
+    checkpoints, misfit, recompute, replay, reverse) over the same steps
+    through the library's forward alone (field copied in and out).  The
     target map is the same run with D x 1.2 and v0 + 3 m/s."""
     import torch
     import hipft_b200 as H
@@ -566,7 +570,12 @@ def measure_adjoint(args, local: int, nsteps: int = 16):
     f0 = g.get_field()
     g.update_flow()
     dt = g.flow_dtmax()
-    dts = [dt] * nsteps
+    tend = 24.0 * days
+    dts, time_ = [], 0.0
+    while time_ < tend:
+        d = min(dt, tend - time_)
+        dts.append(d)
+        time_ += d
 
     def forward(gg, f):
         torch.cuda.synchronize()
@@ -585,8 +594,8 @@ def measure_adjoint(args, local: int, nsteps: int = 16):
     gt.close()
     forward(g, f0)
     _, fwd_s = forward(g, f0)
-    A = MisfitAdjoint(g, D, flow, checkpoint_every=64)
-    A.run(f0, target, dts)
+    A = MisfitAdjoint(g, D, flow, checkpoint_every=checkpoint_every)
+    A.run(f0, target, dts[:2])  # warm-up (tape allocation, tuner)
     torch.cuda.synchronize()
     w0 = time.perf_counter()
     loss, grads = A.run(f0, target, dts)
@@ -594,9 +603,11 @@ def measure_adjoint(args, local: int, nsteps: int = 16):
     grad_s = time.perf_counter() - w0
     tape = ctypes.c_int64(0)
     g.L.hipft_adj_tape_fields(g.h, ctypes.byref(tape))
+    A.release()
     g.close()
-    return {"workload": "adjoint_512x1024", "grid": [ntm, npm1 - 1], "realizations": 1, "steps": nsteps,
-            "dt_hours": dt, "subcycling": "PTL (automatic)", "checkpoint_every": 64,
+    return {"workload": "adjoint_512x1024", "grid": [ntm, npm1 - 1], "realizations": 1, "steps": len(dts),
+            "model_days": days, "dt_hours": dt, "subcycling": "PTL (automatic)",
+            "checkpoint_every": checkpoint_every, "segments": -(-len(dts) // checkpoint_every),
             "forward_ms": fwd_s * 1e3, "gradient_ms": grad_s * 1e3, "gradient_over_forward": grad_s / fwd_s,
             "loss": loss, "grad_D": float(grads["D"][0]), "grad_f0_norm": float(np.linalg.norm(grads["f0"])),
             "tape_fields_per_step": int(tape.value),

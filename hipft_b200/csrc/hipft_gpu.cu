@@ -6,12 +6,14 @@
 #include <cudaTypedefs.h>  // PFN_cuTensorMapEncodeTiled
 
 #include <algorithm>
+#include <array>
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -44,6 +46,17 @@ constexpr double c_third = 0.33333333333333333;
 constexpr int kNBuf = 6;  // current field + 5 scratch fields (two-stage RKG2 needs two fresh outputs)
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+// Two-stage kernel kinds (see the autotuner) and the plan a handle uses.
+enum { PK_SINGLE = 0, PK_TILE = 1, PK_WS_ROWS1 = 4, PK_WS_ROWS2 = 5, PK_WS_BULK = 6 };
+struct PairPlan {
+  int kind = -1;    // PK_*; -1: not chosen yet
+  int shape = 0;    // kPairShapes index (PK_TILE)
+  int ctas_per_sm = 2;
+  double ms = 0.0;  // timed ms per launch pair (0: not timed)
+  int candidates = 0;
+};
+
 double pow3(double c) { return c * c * c; }
 double pow5(double c) { return c * c * c * c * c; }
 
@@ -96,6 +109,7 @@ struct hipft_gpu {
   unsigned int *d_rcount = nullptr;
   int nkb = 0;
   PairTables ptab{};        // coefficient tables of the warp-specialised two-stage kernel
+  PairPlan plan{};          // two-stage kernel chosen for this grid (autotuner)
   struct WsMapEntry {
     const void *p;
     int cols;
@@ -384,68 +398,30 @@ static int current_dring(hipft_gpu *h, const double **ring) {
   return HIPFT_OK;
 }
 
-constexpr int kKPT = 8;   // phi columns per thread, fused stage kernel v2 (one row per thread)
-constexpr int kKPT3 = 4;  // phi columns per thread, v3 (two rows per thread)
+constexpr int kKPT3 = 4;  // phi columns per thread of the fused single-stage kernel (two rows per thread)
 
-// Fused stage kernel variant: 3 (row pairs, 16-byte accesses; default) or
-// 2 (one row per thread); HIPFT_STS_KERNEL selects it for A/B timing.
-static int sts_kernel_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = std::getenv("HIPFT_STS_KERNEL");
-    v = (e && std::atoi(e) == 2) ? 2 : 3;
-  }
-  return v;
-}
-
+// One fused RKG2/RKL2 (or Euler) stage, k_sts_stage_v3; leaves the ring sums
+// of its output for the next stage.
 template <int MODE>
 static int sts_stage_v2(hipft_gpu *h, const double *x, const double *ykm2, const double *u0, const double *dty0,
                         double *out, double *out2, StageCoef sc) {
-  const int kpt = (sts_kernel_variant() == 2) ? kKPT : kKPT3;
-  const int nkb = (h->npm - 2 + kpt - 1) / kpt;
+  const int nkb = (h->npm - 2 + kKPT3 - 1) / kKPT3;
   RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkb};
   {
     ProfScope ps(h, MODE == MODE_STSK ? HIPFT_K_STS : HIPFT_K_OTHER);
-    if (sts_kernel_variant() == 2) {
-      // shift the theta-to-lane map by one row when row ntm-1 would be a warp's last lane
-      const int jshift = ((h->ntm - 2) % 32 == 31) ? 1 : 0;
-      dim3 grd((unsigned)((h->ntm + jshift + 127) / 128), (unsigned)nkb, (unsigned)h->nr);
-      k_sts_stage_v2<MODE, kKPT><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
-                                                             h->d_ringbuf[h->ring_cur], h->bc_diff_n,
-                                                             h->bc_diff_s, sc, ro, jshift);
-    } else {
-      // odd ntm: keep the thread owning row ntm off lane 0 (row ntm-1 is its left neighbour)
-      const int jshift = (h->ntm % 2 == 1 && ((h->ntm - 1) / 2) % 32 == 0) ? 1 : 0;
-      const int nthr = (h->ntm + 2 * jshift + 1) / 2;
-      dim3 grd((unsigned)((nthr + 127) / 128), (unsigned)nkb, (unsigned)h->nr);
-      k_sts_stage_v3<MODE, kKPT3><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
-                                                             h->d_ringbuf[h->ring_cur], h->bc_diff_n,
-                                                             h->bc_diff_s, sc, ro, jshift);
-    }
+    // odd ntm: keep the thread owning row ntm off lane 0 (row ntm-1 is its left neighbour)
+    const int jshift = (h->ntm % 2 == 1 && ((h->ntm - 1) / 2) % 32 == 0) ? 1 : 0;
+    const int nthr = (h->ntm + 2 * jshift + 1) / 2;
+    dim3 grd((unsigned)((nthr + 127) / 128), (unsigned)nkb, (unsigned)h->nr);
+    k_sts_stage_v3<MODE, kKPT3><<<grd, 128, 0, h->stream>>>(h->M, h->DC.dfac, x, ykm2, u0, dty0, out, out2,
+                                                           h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s, sc,
+                                                           ro, jshift);
     LAUNCHED(h);
   }
   h->ring_cur = 1 - h->ring_cur;  // the output's ring is now current
   return HIPFT_OK;
 }
 
-// Two RKG2 stages per launch: HIPFT_STS_PAIR=6 persistent warp-specialised
-// CTAs with two theta rows per consumer thread whose outputs leave by bulk
-// stores (k_sts_pair_ws<false, true, true>, then k_pair_poles), 5 (default)
-// the same with the consumers storing to global memory, 4 the same with one row
-// per consumer thread, 1 one CTA per
-// tile (k_sts_pair), 2 persistent double-buffered CTAs (k_sts_pair_p), 3 one
-// CTA per tile with row-marching arithmetic (k_sts_pair_march), 0 one stage
-// per launch (A/B timing).
-static int sts_pair_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = std::getenv("HIPFT_STS_PAIR");
-    v = e ? std::atoi(e) : 5;
-    if (v < 0 || v > 6) v = 5;
-  }
-  return v;
-}
-static bool sts_pairs_enabled() { return sts_pair_variant() != 0; }
 // HIPFT_PDL=0 turns off the programmatic (overlapping) launch of the
 // two-stage kernel after the previous pair's pole-row kernel.
 static bool ws_pdl() {
@@ -453,16 +429,6 @@ static bool ws_pdl() {
   if (v < 0) {
     const char *e = std::getenv("HIPFT_PDL");
     v = (e && std::atoi(e) == 0) ? 0 : 1;
-  }
-  return v == 1;
-}
-// HIPFT_WS_POLES=1: k_sts_pair_ws finishes the pole rows itself (last
-// pole-holding tile); default 0: a separate k_pair_poles launch does.
-static bool ws_inline_poles() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = std::getenv("HIPFT_WS_POLES");
-    v = (e && std::atoi(e) == 1) ? 1 : 0;
   }
   return v == 1;
 }
@@ -541,8 +507,8 @@ static WsMaps ws_maps(hipft_gpu *h, const double *ykm1, const double *ykm2, cons
   return tm;
 }
 
-// Tile shape of the two-stage kernel (theta rows x phi columns), picked by
-// HIPFT_PAIR_TILE ("128x8" default) for tuning sweeps.
+// Tile shapes of the one-CTA-per-tile two-stage kernel (theta rows x phi
+// columns).
 struct PairShape {
   const char *name;
   int tj, tk;
@@ -575,6 +541,7 @@ static const PairShape kPairShapes[] = {
     {"256x8", 256, 8, pair_smem_bytes<256, 8>(), launch_pair<256, 8, 2>},
     {"256x4", 256, 4, pair_smem_bytes<256, 4>(), launch_pair<256, 4, 3>},
 };
+constexpr int kNPairShapes = (int)(sizeof(kPairShapes) / sizeof(kPairShapes[0]));
 
 static cudaError_t pair_attrs_all() {
   cudaError_t e;
@@ -587,93 +554,191 @@ static cudaError_t pair_attrs_all() {
   return pair_attr<256, 4, 3>();
 }
 
-static const PairShape &pair_shape() {
-  static int idx = -1;
-  if (idx < 0) {
-    idx = 0;
-    const char *e = std::getenv("HIPFT_PAIR_TILE");
-    if (e)
-      for (int q = 0; q < (int)(sizeof(kPairShapes) / sizeof(kPairShapes[0])); ++q)
-        if (std::strcmp(e, kPairShapes[q].name) == 0) idx = q;
+// ------------------------------------------------------------ autotuner
+// The two-stage launch has several implementations whose speed depends on
+// the grid and the batch.  The persistent warp-specialised family shares one
+// tile (128 theta rows x 8 phi columns), one ring-sum order and the pole
+// kernel, so its members give bitwise the same values: two theta rows per
+// consumer thread (PK_WS_ROWS2) at 2 or 1 CTAs per SM, the same with bulk
+// stores (PK_WS_BULK), one row per thread (PK_WS_ROWS1).  On the first
+// two-stage super-step of a grid size (ntm, npm, nr) on a device the library
+// times each of them over a few launches on the handle's own buffers and
+// keeps the fastest for the process.  The one-CTA-per-tile kernels (PK_TILE,
+// seven tile shapes) sum the pole rings in another order, so they are not
+// candidates -- a run's result must not depend on timing noise -- and are
+// selected explicitly: HIPFT_STS_PAIR (0: one stage per launch, 1: tiles of
+// HIPFT_PAIR_TILE, 4/5/6: the warp-specialised kinds) fixes the choice, and
+// HIPFT_TUNE=0 takes PK_WS_ROWS2 at 2 CTAs per SM without timing.
+
+static const char *pair_kind_name(int k) {
+  switch (k) {
+    case PK_SINGLE: return "single-stage";
+    case PK_TILE: return "tile";
+    case PK_WS_ROWS1: return "ws-rows1";
+    case PK_WS_ROWS2: return "ws-rows2";
+    case PK_WS_BULK: return "ws-bulk";
   }
-  return kPairShapes[idx];
+  return "?";
 }
 
-// overlap_prev: the launch before this one on the stream is the previous
-// pair's k_pair_poles (so the two-stage kernel may start while it runs;
-// everything else it reads was finished by the kernels before that one).
-static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
-                    double *out_k, double *out_k1, StageCoef ca, StageCoef cb, bool overlap_prev) {
-  const PairShape &ps_ = pair_shape();
-  const int tk = (sts_pair_variant() >= 2) ? kPK : ps_.tk;
-  const int tj = (sts_pair_variant() >= 2) ? kPJ : ps_.tj;
-  static_assert(kWK == kPK && kWJ == kPJ, "the two-stage variants share one tile shape");
-  const int nkt = (h->npm - 2 + tk - 1) / tk;
-  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
-  const int ntj = (h->ntm + tj - 1) / tj;
+static std::mutex g_plan_mutex;
+static std::vector<std::pair<std::array<int, 4>, PairPlan>> g_plans;  // (ntm, npm, nr, device) -> plan
+
+static bool env_plan(PairPlan &p) {
+  const char *e = std::getenv("HIPFT_STS_PAIR");
+  if (e) {
+    const int v = std::atoi(e);
+    p.kind = (v == 0 || v == 1 || v == 4 || v == 6) ? v : PK_WS_ROWS2;
+    if (p.kind == PK_TILE) {
+      const char *t = std::getenv("HIPFT_PAIR_TILE");
+      for (int q = 0; t && q < kNPairShapes; ++q)
+        if (std::strcmp(t, kPairShapes[q].name) == 0) p.shape = q;
+    }
+    return true;
+  }
+  const char *t = std::getenv("HIPFT_TUNE");
+  if (t && std::atoi(t) == 0) {
+    p.kind = PK_WS_ROWS2;
+    return true;
+  }
+  return false;
+}
+
+static bool sts_pairs_enabled(const hipft_gpu *h) { return h->plan.kind != PK_SINGLE; }
+
+static int check_wait_flag(hipft_gpu *h, const char *what);
+
+// Two RKG2 stages per launch (stages k, k+1 of diffusion_step_sts_cd,
+// src/hipft.f90:5222-5237) with the handle's plan.  overlap_prev: the launch
+// before this one on the stream is the previous pair's k_pair_poles (so the
+// warp-specialised kernel may start while it runs; everything else it reads
+// was finished by the kernels before that one).
+static int sts_pair_plan(hipft_gpu *h, const PairPlan &pl, const double *ykm1, const double *ykm2, const double *u0,
+                         const double *dty0, double *out_k, double *out_k1, StageCoef ca, StageCoef cb,
+                         bool overlap_prev) {
+  static_assert(kWK == kPK && kWJ == kPJ, "the two-stage kernels share one tile shape");
   {
     ProfScope ps(h, HIPFT_K_STS);
-    if (sts_pair_variant() >= 4) {
-      const int grid = std::min(h->ptab.ntiles, 2 * h->num_sms);
+    if (pl.kind != PK_TILE) {
+      const int nkt = (h->npm - 2 + kWK - 1) / kWK;
+      RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
+      const int grid = std::min(h->ptab.ntiles, pl.ctas_per_sm * h->num_sms);
       const PairArgs pa{ca, cb, h->d_err};
       const double *rin = h->d_ringbuf[h->ring_cur];
       const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
-      if (ws_inline_poles()) {
-        k_sts_pair_ws<true><<<grid, kWThreads, kWSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
-                                                                    out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
-                                                                    h->ptab, tmaps);
-      } else {
-        // programmatic dependent launch: may overlap the previous pair's
-        // k_pair_poles (the kernel's pole tiles wait for it)
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)grid);
-        cfg.blockDim = dim3(kWThreads);
-        cfg.dynamicSmemBytes = kWSmem;
-        cfg.stream = h->stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cudaError_t le;
-        // bulk stores need 16-byte aligned output columns (ldt and the
-        // plane are multiples of 16 elements)
-        const bool aligned = ((reinterpret_cast<uintptr_t>(out_k) | reinterpret_cast<uintptr_t>(out_k1)) & 15) == 0;
-        if (sts_pair_variant() == 6 && aligned)
-          le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true, true>, h->M, (const double *)h->DC.dfac, ykm1,
-                                  ykm2, u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
-        else if (sts_pair_variant() >= 5)
-          le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
-                                  dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
-        else
-          le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, false>, h->M, (const double *)h->DC.dfac, ykm1, ykm2,
-                                  u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
-        if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
-        LAUNCHED(h);
-        dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
-        k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
-                                                         h->bc_diff_n, h->bc_diff_s, pa, ro, h->pole);
-      }
-    } else if (sts_pair_variant() == 3) {
-      dim3 grd((unsigned)ntj, (unsigned)nkt, (unsigned)h->nr);
-      k_sts_pair_march<<<grd, 256, kMarchSmem, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1,
-                                                             h->d_ringbuf[h->ring_cur], h->bc_diff_n, h->bc_diff_s,
-                                                             PairArgs{ca, cb, h->d_err}, ro);
-    } else if (sts_pair_variant() == 2) {
-      const int ntiles = ntj * nkt * h->nr;
-      const int grid = std::min(ntiles, 2 * h->num_sms);
-      k_sts_pair_p<<<grid, kPThreads, kPairSmemP, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k,
-                                                                out_k1, h->d_ringbuf[h->ring_cur], h->bc_diff_n,
-                                                                h->bc_diff_s, PairArgs{ca, cb, h->d_err}, ro,
-                                                                ntiles);
+      // programmatic dependent launch: may overlap the previous pair's
+      // k_pair_poles (the kernel's pole tiles wait for it)
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)grid);
+      cfg.blockDim = dim3(kWThreads);
+      cfg.dynamicSmemBytes = kWSmem;
+      cfg.stream = h->stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      cudaError_t le;
+      // bulk stores need 16-byte aligned output columns (ldt and the plane
+      // are multiples of 16 elements)
+      const bool aligned = ((reinterpret_cast<uintptr_t>(out_k) | reinterpret_cast<uintptr_t>(out_k1)) & 15) == 0;
+      if (pl.kind == PK_WS_BULK && aligned)
+        le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true, true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
+                                dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+      else if (pl.kind == PK_WS_ROWS1)
+        le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0,
+                                out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+      else
+        le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0,
+                                out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+      if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
+      LAUNCHED(h);
+      dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
+      k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
+                                                       h->bc_diff_n, h->bc_diff_s, pa, ro, h->pole);
     } else {
-      dim3 grd((unsigned)ntj, (unsigned)nkt, (unsigned)h->nr);
-      ps_.launch(grd, h->stream, h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, h->d_ringbuf[h->ring_cur],
-                 h->bc_diff_n, h->bc_diff_s, PairArgs{ca, cb, h->d_err}, ro);
+      const PairShape &sh = kPairShapes[pl.shape];
+      const int nkt = (h->npm - 2 + sh.tk - 1) / sh.tk;
+      RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
+      dim3 grd((unsigned)((h->ntm + sh.tj - 1) / sh.tj), (unsigned)nkt, (unsigned)h->nr);
+      sh.launch(grd, h->stream, h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, h->d_ringbuf[h->ring_cur],
+                h->bc_diff_n, h->bc_diff_s, PairArgs{ca, cb, h->d_err}, ro);
     }
     LAUNCHED(h);
   }
   h->ring_cur = 1 - h->ring_cur;
+  return HIPFT_OK;
+}
+
+static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
+                    double *out_k, double *out_k1, StageCoef ca, StageCoef cb, bool overlap_prev) {
+  return sts_pair_plan(h, h->plan, ykm1, ykm2, u0, dty0, out_k, out_k1, ca, cb, overlap_prev);
+}
+
+// Chooses the handle's two-stage plan (see the autotuner above) before the
+// first super-step.  Timing runs on four buffers other than the current
+// field, with the current field as an input, and leaves the field untouched;
+// the ring sums it disturbs are recomputed afterwards.
+static int ensure_pair_plan(hipft_gpu *h) {
+  if (h->plan.kind >= 0) return HIPFT_OK;
+  PairPlan p;
+  if (env_plan(p)) {
+    h->plan = p;
+    return HIPFT_OK;
+  }
+  const std::array<int, 4> key{h->ntm, h->npm, h->nr, h->dev};
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mutex);
+    for (const auto &e : g_plans)
+      if (e.first == key) {
+        h->plan = e.second;
+        return HIPFT_OK;
+      }
+  }
+  std::vector<PairPlan> cands;
+  for (int c : {2, 1}) {
+    PairPlan q;
+    q.kind = PK_WS_ROWS2;
+    q.ctas_per_sm = c;
+    cands.push_back(q);
+  }
+  for (int k : {PK_WS_BULK, PK_WS_ROWS1}) {
+    PairPlan q;
+    q.kind = k;
+    cands.push_back(q);
+  }
+  const bool prof = h->profiling;
+  h->profiling = false;
+  const double *x = h->buf[h->cur];
+  double *bufs[4];
+  for (int q = 0; q < 4; ++q) bufs[q] = h->buf[scratch(h, q)];
+  const StageCoef ca{0.5, -0.1, 0.6, 1e-3, 0.0}, cb{0.5, -0.1, 0.6, 1e-3, 0.0};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(h, cudaEventCreate(&e0));
+  CK(h, cudaEventCreate(&e1));
+  int best = 0;
+  const int reps = 3;
+  for (size_t c = 0; c < cands.size(); ++c) {
+    TRY(sts_pair_plan(h, cands[c], x, bufs[0], x, bufs[1], bufs[2], bufs[3], ca, cb, false));  // warm-up
+    CK(h, cudaEventRecord(e0, h->stream));
+    for (int r = 0; r < reps; ++r)
+      TRY(sts_pair_plan(h, cands[c], x, bufs[0], x, bufs[1], bufs[2], bufs[3], ca, cb, r > 0));
+    CK(h, cudaEventRecord(e1, h->stream));
+    CK(h, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(h, cudaEventElapsedTime(&ms, e0, e1));
+    cands[c].ms = ms / reps;
+    if (cands[c].ms < cands[best].ms) best = (int)c;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->profiling = prof;
+  TRY(check_wait_flag(h, "pair autotuner: a bounded wait for staged tiles gave up"));
+  h->plan = cands[best];
+  h->plan.candidates = (int)cands.size();
+  h->dring_valid = false;
+  std::lock_guard<std::mutex> lk(g_plan_mutex);
+  g_plans.push_back({key, h->plan});
   return HIPFT_OK;
 }
 
@@ -795,19 +860,13 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   if ((rc = dalloc(h, &h->d_err, 1))) return bail(rc);
   if (cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   if (pair_attrs_all() != cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_march, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMarchSmem) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_p, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPairSmemP) !=
+      cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_sts_pair_ws<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
+      cudaFuncSetAttribute(k_sts_pair_ws<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_ws<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_ws<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kWSmem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_ws<false, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_sts_pair_ws<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kWSmem) != cudaSuccess)
     return bail(fail(h, HIPFT_ECUDA, "cannot reserve shared memory for the two-stage kernels"));
   if (cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->dev) != cudaSuccess || h->num_sms < 1)
@@ -1382,6 +1441,7 @@ static void load_sts(hipft_gpu *h, double dtl) {
 // diffusion_step_sts_cd (src/hipft.f90:5163-5242): stage 1 then the
 // s-1 fused stages, rotating three scratch fields.
 static int sts_super_step(hipft_gpu *h, double dtl) {
+  if (!h->DC.grid) TRY(ensure_pair_plan(h));
   load_sts(h, dtl);
   int u0 = h->cur, idty = scratch(h, 0), ia = scratch(h, 1), ib = scratch(h, 2);
   const bool fused = !h->DC.grid;
@@ -1409,7 +1469,7 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
   (void)ib;
   int64_t k = 2;
   while (k <= h->sts_s) {
-    if (fused && sts_pairs_enabled() && k + 1 <= h->sts_s) {
+    if (fused && sts_pairs_enabled(h) && k + 1 <= h->sts_s) {
       int bk = free_buf(-1), bk1 = free_buf(bk);
       TRY(sts_pair(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[bk], h->buf[bk1], coef(k),
                    coef(k + 1), k > 2));
@@ -1632,7 +1692,8 @@ static int sts_pair_ragged(hipft_gpu *h, const double *ykm1, const double *ykm2,
   RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
   PairTables pt = h->ptab;
   pt.ntiles = pt.nb * pt.nkt * n;
-  const int grid = std::min(pt.ntiles, 2 * h->num_sms);
+  const int cps = (h->plan.kind == PK_WS_ROWS2) ? h->plan.ctas_per_sm : 2;
+  const int grid = std::min(pt.ntiles, cps * h->num_sms);
   PairArgs pa{StageCoef{}, StageCoef{}, h->d_err, h->d_rlist_dif, rc};
   const double *rin = h->d_ringbuf[h->ring_cur];
   const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
@@ -1648,7 +1709,7 @@ static int sts_pair_ragged(hipft_gpu *h, const double *ykm1, const double *ykm2,
     attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false, true, false, true>, h->M,
+    cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true, false, true>, h->M,
                                         (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, rin,
                                         h->bc_diff_n, h->bc_diff_s, pa, ro, pt, tmaps);
     if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws (ragged) launch: %s", cudaGetErrorString(le));
@@ -2344,6 +2405,26 @@ extern "C" int hipft_gpu_info(const hipft_gpu *h, hipft_info *info) {
   return HIPFT_OK;
 }
 
+extern "C" int hipft_gpu_describe(hipft_gpu *h, char *buf, size_t len) {
+  if (!h || !buf || !len) return HIPFT_EINVAL;
+  const PairPlan &p = h->plan;
+  char kind[64];
+  if (p.kind < 0)
+    std::snprintf(kind, sizeof kind, "not chosen yet");
+  else if (p.kind == PK_TILE)
+    std::snprintf(kind, sizeof kind, "tile %s", kPairShapes[p.shape].name);
+  else if (p.kind == PK_SINGLE)
+    std::snprintf(kind, sizeof kind, "%s", pair_kind_name(p.kind));
+  else
+    std::snprintf(kind, sizeof kind, "%s, %d CTAs per SM", pair_kind_name(p.kind), p.ctas_per_sm);
+  if (p.candidates > 0)
+    std::snprintf(buf, len, "schedule=%s; two-stage kernel: %s (tuned over %d candidates, %.4f ms per launch pair)",
+                  h->ragged ? "ragged" : "shared", kind, p.candidates, p.ms);
+  else
+    std::snprintf(buf, len, "schedule=%s; two-stage kernel: %s", h->ragged ? "ragged" : "shared", kind);
+  return HIPFT_OK;
+}
+
 extern "C" int hipft_gpu_set_stream(hipft_gpu *h, void *s) {
   if (!h) return HIPFT_EINVAL;
   CK(h, cudaStreamSynchronize(h->stream));
@@ -2665,6 +2746,7 @@ static int adj_adv_fwd(hipft_gpu *h, double dtl, size_t &nt, size_t t[4]) {
 // stage fields are kept; same subcycle logic as hipft_gpu_diffusion_step.
 static int adj_diff_fwd(hipft_gpu *h, double dtl, size_t &nt, std::vector<AdjSub> &subs) {
   const int max_sc = 60;
+  TRY(ensure_pair_plan(h));
   int i = 1;
   bool done = false;
   double time_stepped = 0.0;
@@ -2762,7 +2844,7 @@ static int adj_diff_fwd(hipft_gpu *h, double dtl, size_t &nt, std::vector<AdjSub
     TRY(keep_ring(1));
     int64_t k = 2;
     while (k <= S.s) {
-      if (sts_pairs_enabled() && k + 1 <= S.s) {
+      if (sts_pairs_enabled(h) && k + 1 <= S.s) {
         TRY(sts_pair(h, Y[k - 1], Y[k - 2], u0, dty0, Y[k], Y[k + 1], coef(k), coef(k + 1), k > 2));
         TRY(keep_ring(k + 1));
         k += 2;
@@ -2846,7 +2928,7 @@ static int adj_block_recompute(hipft_gpu *h, const AdjSub &S, size_t b, std::vec
   };
   int64_t k = c + 1;
   while (k <= e) {
-    if (sts_pairs_enabled() && k + 1 <= S.s) {
+    if (sts_pairs_enabled(h) && k + 1 <= S.s) {
       TRY(sts_pair(h, Yw[k - 1], Yw[k - 2], u0, dty0, Yw[k], Yw[k + 1], coef(k), coef(k + 1), k > c + 1));
       k += 2;
       continue;

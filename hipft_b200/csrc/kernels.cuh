@@ -999,15 +999,13 @@ __global__ void k_scale_balance(Mesh m, double *a, const double *ratio) {
 
 namespace hipft {
 
-// ------------------------------------------------------ RKG2 stage, v2
-// Fused RKG2/RKL2 stage for a diffusion coefficient that is constant per
-// realization (the diffusion_coef_constant path of load_diffusion).  Each
-// thread owns one theta row j and marches over KPT consecutive phi columns;
-// all of its loads are issued before any arithmetic so that 5*KPT+2
-// independent requests per thread are in flight.  The 5-point coefficients
-// are assembled from per-row and per-column factors in exactly the operation
-// order of load_diffusion_matrix (src/hipft.f90:4962-4979), so values are
-// bit-identical to the general kernel.
+// ---------------------------------------------- fused RKG2 stage (ring out)
+// The fused single-stage kernel below is for a diffusion coefficient that is
+// constant per realization (the diffusion_coef_constant path of
+// load_diffusion).  Its 5-point coefficients are assembled from per-row and
+// per-column factors in exactly the operation order of load_diffusion_matrix
+// (src/hipft.f90:4962-4979), so values are bit-identical to the general
+// kernel.
 //
 // The pole-ring sums of the *output* (needed by the next stage's pole rows,
 // src/hipft.f90:7969-7979) are fused: the threads owning rows 2 and ntm-1
@@ -1022,146 +1020,16 @@ struct RingOut {
   int nkb;               // phi blocks per realization
 };
 
-template <int MODE, int KPT>
-__global__ void __launch_bounds__(128, 4) k_sts_stage_v2(Mesh m, const double *__restrict__ dfac,
-                                                     const double *__restrict__ x, const double *ykm2,
-                                                     const double *__restrict__ u0, const double *__restrict__ dty0,
-                                                     double *out, double *out2, const double *__restrict__ ring_in,
-                                                     double bcn, double bcs, StageCoef sc, RingOut ro, int jshift) {
-  const int lane = threadIdx.x & 31;
-  // jshift (0 or 1) keeps rows ntm-1 and ntm in one warp; rows 1 and 2 always are.
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1 - jshift;
-  const int kb = blockIdx.y;
-  const int k0 = kb * KPT + 2;
-  const int i = blockIdx.z + 1;
-  const int ntm = m.ntm, npm = m.npm;
-  const int nk = min(KPT, npm - 1 - k0 + 1);  // columns in this block (k0..k0+nk-1 <= npm-1)
-  const bool row = (j >= 1 && j <= ntm);
-  const bool interior = row && j >= 2 && j <= ntm - 1;
-  const int64_t ld = m.ldt;
-  const int64_t q0 = (int64_t)(i - 1) * m.plane + (int64_t)(k0 - 1) * ld + (j - 1);
-  const double Dr = dfac[i];
-  const double Dh = kHalf * (Dr + Dr);  // half*(D(j,k)+D(j+1,k)) of a constant D
-
-  // ---- loads (all independent, issued before any store)
-  double xv[KPT + 2], xe[KPT], y2[KPT], uu[KPT], dd[KPT];
-#pragma unroll
-  for (int c = 0; c < KPT + 2; ++c) {
-    int kc = k0 - 1 + c;
-    xv[c] = (row && kc <= npm) ? x[q0 + (int64_t)(c - 1) * ld] : 0.0;
-  }
-#pragma unroll
-  for (int c = 0; c < KPT; ++c) {
-    bool ok = row && c < nk;
-    int64_t q = q0 + (int64_t)c * ld;
-    // theta neighbours across warp boundaries: lane 0 needs x(j-1), lane 31 x(j+1)
-    double e = 0.0;
-    if (ok && interior && (lane == 0 || lane == 31)) e = (lane == 0) ? x[q - 1] : x[q + 1];
-    xe[c] = e;
-    if (MODE == MODE_STSK) {
-      y2[c] = ok ? ykm2[q] : 0.0;
-      uu[c] = ok ? u0[q] : 0.0;
-      dd[c] = ok ? dty0[q] : 0.0;
-    }
-  }
-  // per-row factors
-  double sti = 0, c2 = 0, c4 = 0;
-  if (interior) {
-    sti = m.st_i[j];
-    c2 = Dh * m.dth_i[j] * m.dt_i[j] * sti * m.sth[j];
-    c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * sti * m.sth[j + 1];
-  }
-  const bool north = (j == 2), south = (j == ntm - 1);
-  double rn_acc = 0.0;  // ring partial (north or south) over this block's columns
-  const double ax_n = ring_in[2 * (i - 1)] * bcn;
-  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
-#pragma unroll
-  for (int c = 0; c < KPT; ++c) {
-    const int k = k0 + c;
-    const bool active = row && c < nk;
-    double xc = xv[c + 1];
-    double up = __shfl_up_sync(0xffffffffu, xc, 1);
-    double dn = __shfl_down_sync(0xffffffffu, xc, 1);
-    double xjm = (lane == 0) ? xe[c] : up;
-    double xjp = (lane == 31) ? xe[c] : dn;
-    double ax;
-    if (j == 1) {
-      ax = ax_n;
-    } else if (j == ntm) {
-      ax = ax_s;
-    } else {
-      double pk = m.dph_i[min(k, npm)], pk1 = m.dph_i[min(k + 1, npm)], dpi = m.dp_i[min(k, npm)];
-      double c1 = Dh * pk * dpi * sti * sti;
-      double c5 = Dh * pk1 * dpi * sti * sti;
-      double c3 = -(c1 + c2 + c4 + c5);
-      ax = c1 * xv[c] + c2 * xjm + c3 * xc + c4 * xjp + c5 * xv[c + 2];
-    }
-    double y, d0 = 0.0;
-    if (MODE == MODE_STS1) {
-      d0 = sc.a * ax;
-      y = xc + sc.b * d0;
-    } else if (MODE == MODE_STSK) {
-      y = sc.a * xc + sc.b * y2[c] + sc.c * uu[c] + sc.d * ax + sc.e * dd[c];
-    } else {  // MODE_EULER
-      y = xc + sc.a * ax;
-    }
-    // ring terms of the output, ((D(1,k)+D(2,k))*(y(2,k)-y(1,k)))*dp(k), with
-    // the pole-row output taken from the neighbouring lane
-    double yup = __shfl_up_sync(0xffffffffu, y, 1);
-    double ydn = __shfl_down_sync(0xffffffffu, y, 1);
-    if (!active) continue;
-    if (north) rn_acc = rn_acc + (Dr + Dr) * (y - yup) * m.dp[k];
-    if (south) rn_acc = rn_acc + (Dr + Dr) * (ydn - y) * m.dp[k];
-    const int64_t q = q0 + (int64_t)c * ld;
-    out[q] = y;
-    if (k == 2) out[q + (int64_t)(npm - 2) * ld] = y;
-    if (k == npm - 1) out[q - (int64_t)(npm - 2) * ld] = y;
-    if (MODE == MODE_STS1) {
-      out2[q] = d0;
-      if (k == 2) out2[q + (int64_t)(npm - 2) * ld] = d0;
-      if (k == npm - 1) out2[q - (int64_t)(npm - 2) * ld] = d0;
-    }
-  }
-  // ---- publish ring partials; the last contributor of realization i reduces
-  const bool contrib = (north || south) && row;
-  unsigned int last = 0;
-  if (contrib) {
-    ro.part[((int64_t)(south ? 1 : 0) * m.nr + (i - 1)) * ro.nkb + kb] = rn_acc;
-    __threadfence();
-    unsigned int old = atomicAdd(&ro.count[i - 1], 1u);
-    last = (old == 2u * (unsigned)ro.nkb - 1u) ? 1u : 0u;
-  }
-  // broadcast "last" to the contributor's warp (all lanes reach this point)
-  unsigned int src_mask = __ballot_sync(0xffffffffu, last != 0);
-  if (src_mask) {
-    __threadfence();
-    double sn = 0.0, ss = 0.0;
-    for (int b = lane; b < ro.nkb; b += 32) {
-      sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + b]);
-      ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      sn += __shfl_down_sync(0xffffffffu, sn, o);
-      ss += __shfl_down_sync(0xffffffffu, ss, o);
-    }
-    if (lane == 0) {
-      ro.ring[2 * (i - 1)] = sn;
-      ro.ring[2 * (i - 1) + 1] = ss;
-      ro.count[i - 1] = 0u;
-    }
-  }
-}
 
 }  // namespace hipft
 
 namespace hipft {
 
 // ------------------------------------------------------ RKG2 stage, v3
-// As k_sts_stage_v2, but every thread owns two adjacent theta rows and moves
-// them with 16-byte loads and stores, so a warp touches 512 contiguous bytes
-// per array and phi column (twice the DRAM burst of v2) with half the load
-// instructions.  Row pairs start at an odd row (j = 2t+1, 2t+2) so the pole
+// Every thread owns two adjacent theta rows and marches over KPT phi
+// columns, moving the rows with 16-byte loads and stores (a warp touches 512
+// contiguous bytes per array and column); all of its loads are issued
+// before any arithmetic.  Row pairs start at an odd row (j = 2t+1, 2t+2) so the pole
 // pairs (1,2) and (ntm-1,ntm) stay inside one thread when ntm is even, and
 // inside one warp otherwise (handled with shuffles).  Requires ldt even.
 // Ragged batches: rlist (may be null) maps grid slice z to a realization and
@@ -1641,540 +1509,6 @@ __global__ void __launch_bounds__(kPThreads, MINB) k_sts_pair(Mesh m, const doub
     const int64_t qs = qn + (ntm - 1);                 // row ntm
     // Y_k at the pole rows, recomputed from the inputs (stage k's pole rows
     // use the input's ring sums), so no other CTA's stores are needed here
-    const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
-    const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
-    const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];
-    const double ys = sb.a * yks + sb.b * ykm1[qs] + sb.c * u0[qs] + sb.d * axs1 + sb.e * dty0[qs];
-    out_k1[qn] = yn;
-    out_k1[qs] = ys;
-    if (k >= 2 && k <= npm - 1) {
-      rn = rn + (Dr + Dr) * (__ldcg(&out_k1[qn + 1]) - yn) * m.dp[k];
-      rsum = rsum + (Dr + Dr) * (ys - __ldcg(&out_k1[qs - 1])) * m.dp[k];
-    }
-  }
-  block_sum2(rn, rsum, &red[0][0]);
-  if (tid == 0) {
-    ro.ring[2 * (i - 1)] = rn;
-    ro.ring[2 * (i - 1) + 1] = rsum;
-    ro.count[i - 1] = 0u;
-  }
-}
-
-}  // namespace hipft
-
-namespace hipft {
-
-// ------------------------------------ two RKG2 stages, persistent, 2 buffers
-// Same arithmetic as k_sts_pair, but each CTA walks a strided list of tiles
-// and double-buffers them: while it computes tile n from one shared buffer,
-// the TMA copies of tile n+1 land in the other, so HBM stays busy during the
-// arithmetic.  Each buffer has its own mbarrier whose phase flips per use;
-// every wait is bounded.  Shared writes of a buffer (Y_k in place) are
-// fenced against the async proxy before the buffer is refilled.
-constexpr size_t kPairBuf = (size_t)4 * kPC * kPR + 3 * kPR + 2 * kPC;  // doubles per buffer
-constexpr size_t kPairSmemP = 2 * kPairBuf * sizeof(double) + 64;
-
-__global__ void __launch_bounds__(kPThreads, 2) k_sts_pair_p(Mesh m, const double *__restrict__ dfac,
-                                                             const double *__restrict__ ykm1,
-                                                             const double *__restrict__ ykm2,
-                                                             const double *__restrict__ u0,
-                                                             const double *__restrict__ dty0, double *out_k,
-                                                             double *out_k1, const double *__restrict__ ring_in,
-                                                             double bcn, double bcs, PairArgs pa, RingOut ro,
-                                                             int ntiles) {
-  extern __shared__ __align__(128) double psm[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(psm + 2 * kPairBuf);
-  __shared__ double red[2][kPThreads / 32];
-  __shared__ double s_ring[2];
-  __shared__ int s_last;
-
-  const int tid = threadIdx.x;
-  const int ntm = m.ntm, npm = m.npm;
-  const int64_t ld = m.ldt;
-  const int ntj = (ntm + kPJ - 1) / kPJ;
-  const int nkt = ro.nkb;
-  auto wrapc = [&](int c) {
-    if (c < 1) return c + (npm - 2);
-    if (c > npm) return c - (npm - 2);
-    return c;
-  };
-#define SIDX(c, r) ((c) * kPR + (r))
-  // issue the copies of tile t into buffer b (thread 0)
-  auto issue = [&](int t, int b) {
-    const int jt = t % ntj, kt = (t / ntj) % nkt, ii = t / (ntj * nkt) + 1;
-    const int j0 = jt * kPJ + 1, k0 = kt * kPK + 2;
-    const int nk = min(kPK, npm - 1 - k0 + 1);
-    const int rs = max(1, j0 - 2), re = min((int)ld, j0 + kPJ + 1);
-    const uint32_t run_bytes = (uint32_t)(re - rs + 1) * 8u;
-    const int roff = rs - (j0 - 2);
-    const int64_t pbase = (int64_t)(ii - 1) * m.plane;
-    double *B = psm + (size_t)b * kPairBuf;
-    double *sX1 = B, *sYk = B + kPC * kPR, *sU = B + 2 * kPC * kPR, *sD = B + 3 * kPC * kPR;
-    const uint32_t ncopy = (uint32_t)(nk + 4) + 3u * (uint32_t)(nk + 2);
-    mbar_expect_tx(&bars[b], ncopy * run_bytes);
-    for (int c = 0; c < nk + 4; ++c) {
-      const int kg = wrapc(k0 - 2 + c);
-      bulk_load(&sX1[SIDX(c, roff)], ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1), run_bytes, &bars[b]);
-    }
-    for (int c = 1; c < nk + 3; ++c) {
-      const int kg = wrapc(k0 - 2 + c);
-      const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
-      bulk_load(&sYk[SIDX(c, roff)], ykm2 + g, run_bytes, &bars[b]);
-      bulk_load(&sU[SIDX(c, roff)], u0 + g, run_bytes, &bars[b]);
-      bulk_load(&sD[SIDX(c, roff)], dty0 + g, run_bytes, &bars[b]);
-    }
-  };
-
-  if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  int t = blockIdx.x;
-  if (t >= ntiles) return;
-  if (tid == 0) issue(t, 0);
-  uint32_t phase[2] = {0u, 0u};
-  int b = 0;
-  for (; t < ntiles; t += gridDim.x, b ^= 1) {
-    const int tn = t + gridDim.x;
-    if (tid == 0 && tn < ntiles) {
-      fence_proxy_async_smem();
-      issue(tn, b ^ 1);
-    }
-    const int jt = t % ntj, kt = (t / ntj) % nkt, i = t / (ntj * nkt) + 1;
-    const int j0 = jt * kPJ + 1, k0 = kt * kPK + 2;
-    const int nk = min(kPK, npm - 1 - k0 + 1);
-    const int64_t pbase = (int64_t)(i - 1) * m.plane;
-    double *B = psm + (size_t)b * kPairBuf;
-    double *sX1 = B, *sYk = B + kPC * kPR, *sU = B + 2 * kPC * kPR, *sD = B + 3 * kPC * kPR;
-    double *tST = B + 4 * kPC * kPR, *tC2 = tST + kPR, *tC4 = tC2 + kPR, *tP1 = tC4 + kPR, *tP5 = tP1 + kPC;
-    const double Dr = dfac[i];
-    const double Dh = kHalf * (Dr + Dr);
-    const double ax_n = ring_in[2 * (i - 1)] * bcn;
-    const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
-    for (int r = tid; r < kPR; r += kPThreads) {
-      const int j = j0 - 2 + r;
-      double st = 0.0, c2 = 0.0, c4 = 0.0;
-      if (j >= 2 && j <= ntm - 1) {
-        st = m.st_i[j];
-        c2 = Dh * m.dth_i[j] * m.dt_i[j] * st * m.sth[j];
-        c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * st * m.sth[j + 1];
-      }
-      tST[r] = st;
-      tC2[r] = c2;
-      tC4[r] = c4;
-    }
-    for (int c = tid; c < kPC; c += kPThreads) {
-      const int kc = wrapc(k0 - 2 + c);
-      const int kw = kc == npm ? 2 : (kc == 1 ? npm - 1 : kc);
-      tP1[c] = Dh * m.dph_i[kw] * m.dp_i[kw];
-      tP5[c] = Dh * m.dph_i[kw + 1] * m.dp_i[kw];
-    }
-    if (!mbar_wait_bounded(&bars[b], phase[b], 1u << 22)) {
-      if (tid == 0) atomicExch(pa.err, 1);
-      mbar_wait_bounded(&bars[b], phase[b], 1u << 22);
-      mbar_wait_bounded(&bars[b ^ 1], phase[b ^ 1], 1u << 22);
-      return;
-    }
-    phase[b] ^= 1u;
-    __syncthreads();
-
-    // phase 2: Y_k on the tile plus a halo of 1, in place of Y_{k-2}
-    const int nr2 = kPJ + 2, nc2 = nk + 2;
-    const StageCoef sa = pa.ca;
-    for (int e = tid; e < nr2 * nc2; e += kPThreads) {
-      const int r = 1 + e % nr2;
-      const int c = 1 + e / nr2;
-      const int j = j0 - 2 + r;
-      if (j < 1 || j > ntm) continue;
-      double ax;
-      if (j == 1) {
-        ax = ax_n;
-      } else if (j == ntm) {
-        ax = ax_s;
-      } else {
-        const double sti = tST[r];
-        const double c1 = tP1[c] * sti * sti;
-        const double c2 = tC2[r];
-        const double c4 = tC4[r];
-        const double c5 = tP5[c] * sti * sti;
-        const double c3 = -(c1 + c2 + c4 + c5);
-        ax = c1 * sX1[SIDX(c - 1, r)] + c2 * sX1[SIDX(c, r - 1)] + c3 * sX1[SIDX(c, r)] +
-             c4 * sX1[SIDX(c, r + 1)] + c5 * sX1[SIDX(c + 1, r)];
-      }
-      const double y = sa.a * sX1[SIDX(c, r)] + sa.b * sYk[SIDX(c, r)] + sa.c * sU[SIDX(c, r)] + sa.d * ax +
-                       sa.e * sD[SIDX(c, r)];
-      sYk[SIDX(c, r)] = y;
-      if (r >= 2 && r < 2 + kPJ && c >= 2 && c < 2 + nk) {
-        const int k = k0 - 2 + c;
-        const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
-        out_k[q] = y;
-        if (k == 2) out_k[q + (int64_t)(npm - 2) * ld] = y;
-        if (k == npm - 1) out_k[q - (int64_t)(npm - 2) * ld] = y;
-      }
-    }
-    __syncthreads();
-
-    const bool has_n = (j0 == 1);
-    const bool has_s = (ntm - 1 >= j0 && ntm - 1 <= j0 + kPJ - 1);
-    if (tid == 0 && (has_n || has_s)) {
-      if (has_n) {
-        double acc = 0.0;
-        for (int c = 2; c < 2 + nk; ++c)
-          acc = acc + (Dr + Dr) * (sYk[SIDX(c, 3)] - sYk[SIDX(c, 2)]) * m.dp[k0 - 2 + c];
-        ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
-      }
-      if (has_s) {
-        const int rS = ntm - (j0 - 2);
-        double acc = 0.0;
-        for (int c = 2; c < 2 + nk; ++c)
-          acc = acc + (Dr + Dr) * (sYk[SIDX(c, rS)] - sYk[SIDX(c, rS - 1)]) * m.dp[k0 - 2 + c];
-        ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
-      }
-    }
-
-    // phase 3: Y_{k+1} on the tile interior
-    const StageCoef sb = pa.cb;
-    for (int e = tid; e < kPJ * nk; e += kPThreads) {
-      const int r = 2 + e % kPJ;
-      const int c = 2 + e / kPJ;
-      const int j = j0 - 2 + r;
-      if (j < 2 || j > ntm - 1) continue;
-      const int k = k0 - 2 + c;
-      const double sti = tST[r];
-      const double c1 = tP1[c] * sti * sti;
-      const double c2 = tC2[r];
-      const double c4 = tC4[r];
-      const double c5 = tP5[c] * sti * sti;
-      const double c3 = -(c1 + c2 + c4 + c5);
-      const double ax = c1 * sYk[SIDX(c - 1, r)] + c2 * sYk[SIDX(c, r - 1)] + c3 * sYk[SIDX(c, r)] +
-                        c4 * sYk[SIDX(c, r + 1)] + c5 * sYk[SIDX(c + 1, r)];
-      const double y = sb.a * sYk[SIDX(c, r)] + sb.b * sX1[SIDX(c, r)] + sb.c * sU[SIDX(c, r)] + sb.d * ax +
-                       sb.e * sD[SIDX(c, r)];
-      const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
-      out_k1[q] = y;
-      if (k == 2) out_k1[q + (int64_t)(npm - 2) * ld] = y;
-      if (k == npm - 1) out_k1[q - (int64_t)(npm - 2) * ld] = y;
-    }
-    // this buffer's shared writes are done before the TMA refills it
-    fence_proxy_async_smem();
-
-    // publish; the last pole-holding CTA of realization i finishes the poles
-    const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
-    if (contrib) {
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) {
-        const unsigned int old = atomicAdd(&ro.count[i - 1], (unsigned)contrib);
-        s_last = (old + (unsigned)contrib == 2u * (unsigned)ro.nkb) ? 1 : 0;
-      }
-      __syncthreads();
-      if (s_last) {
-        __threadfence();
-        double sn = 0.0, ss = 0.0;
-        for (int bb = tid; bb < ro.nkb; bb += kPThreads) {
-          sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + bb]);
-          ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + bb]);
-        }
-        block_sum2(sn, ss, &red[0][0]);
-        if (tid == 0) {
-          s_ring[0] = sn;
-          s_ring[1] = ss;
-        }
-        __syncthreads();
-        const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
-        double rn = 0.0, rsum = 0.0;
-        for (int k = 1 + tid; k <= npm; k += kPThreads) {
-          const int64_t qn = pbase + (int64_t)(k - 1) * ld;
-          const int64_t qs = qn + (ntm - 1);
-          const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
-          const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
-          const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];
-          const double ys = sb.a * yks + sb.b * ykm1[qs] + sb.c * u0[qs] + sb.d * axs1 + sb.e * dty0[qs];
-          out_k1[qn] = yn;
-          out_k1[qs] = ys;
-          if (k >= 2 && k <= npm - 1) {
-            rn = rn + (Dr + Dr) * (__ldcg(&out_k1[qn + 1]) - yn) * m.dp[k];
-            rsum = rsum + (Dr + Dr) * (ys - __ldcg(&out_k1[qs - 1])) * m.dp[k];
-          }
-        }
-        block_sum2(rn, rsum, &red[0][0]);
-        if (tid == 0) {
-          ro.ring[2 * (i - 1)] = rn;
-          ro.ring[2 * (i - 1) + 1] = rsum;
-          ro.count[i - 1] = 0u;
-        }
-      }
-    }
-    __syncthreads();  // everyone is done with buffer b before it is refilled
-  }
-#undef SIDX
-}
-
-}  // namespace hipft
-
-namespace hipft {
-
-// ------------------------------- two RKG2 stages per launch, row marching
-// k_sts_pair's tiles and TMA staging, with the arithmetic reorganised to cut
-// instructions: thread t owns shared row 1 + (t % 128) and one half of the
-// tile's columns, marches along phi with a register window of the row, and
-// takes the theta neighbours from the adjacent lanes by shuffle (shared
-// loads only at the warp's two edge lanes).  Per-row coefficient factors
-// live in registers, per-column ones in shared memory.  Arithmetic is the
-// same expression sequence as k_sts_pair (bit-identical results).
-constexpr int kMJ = 128, kMK = 8, kMR = kMJ + 4, kMC = kMK + 4;
-constexpr size_t kMarchSmem = pair_smem_bytes<kMJ, kMK>();
-
-__global__ void __launch_bounds__(256, 4) k_sts_pair_march(Mesh m, const double *__restrict__ dfac,
-                                                          const double *__restrict__ ykm1,
-                                                          const double *__restrict__ ykm2,
-                                                          const double *__restrict__ u0,
-                                                          const double *__restrict__ dty0, double *out_k,
-                                                          double *out_k1, const double *__restrict__ ring_in,
-                                                          double bcn, double bcs, PairArgs pa, RingOut ro) {
-  extern __shared__ __align__(128) double psm[];
-  double *sX1 = psm;
-  double *sYk = psm + kMC * kMR;
-  double *sU = psm + 2 * kMC * kMR;
-  double *sD = psm + 3 * kMC * kMR;
-  double *tST = psm + 4 * kMC * kMR;
-  double *tC2 = tST + kMR;
-  double *tC4 = tC2 + kMR;
-  double *tP1 = tC4 + kMR;
-  double *tP5 = tP1 + kMC;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tP5 + kMC);
-  __shared__ double red[2][8];
-  __shared__ double s_ring[2];
-  __shared__ int s_last;
-
-  const int tid = threadIdx.x;
-  const int lane = tid & 31;
-  const int ntm = m.ntm, npm = m.npm;
-  const int64_t ld = m.ldt;
-  const int j0 = blockIdx.x * kMJ + 1;
-  const int kt = blockIdx.y;
-  const int k0 = kt * kMK + 2;
-  const int i = blockIdx.z + 1;
-  const int nk = min(kMK, npm - 1 - k0 + 1);
-  const int64_t pbase = (int64_t)(i - 1) * m.plane;
-#define SIDX(c, r) ((c) * kMR + (r))
-  auto wrapc = [&](int c) {
-    if (c < 1) return c + (npm - 2);
-    if (c > npm) return c - (npm - 2);
-    return c;
-  };
-  const int rs = max(1, j0 - 2);
-  const int re = min((int)ld, j0 + kMJ + 1);
-  const uint32_t run_bytes = (uint32_t)(re - rs + 1) * 8u;
-  const int roff = rs - (j0 - 2);
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (tid == 0) {
-    const uint32_t ncopy = (uint32_t)(nk + 4) + 3u * (uint32_t)(nk + 2);
-    mbar_expect_tx(bar, ncopy * run_bytes);
-    for (int c = 0; c < nk + 4; ++c) {
-      const int kg = wrapc(k0 - 2 + c);
-      bulk_load(&sX1[SIDX(c, roff)], ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1), run_bytes, bar);
-    }
-    for (int c = 1; c < nk + 3; ++c) {
-      const int kg = wrapc(k0 - 2 + c);
-      const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
-      bulk_load(&sYk[SIDX(c, roff)], ykm2 + g, run_bytes, bar);
-      bulk_load(&sU[SIDX(c, roff)], u0 + g, run_bytes, bar);
-      bulk_load(&sD[SIDX(c, roff)], dty0 + g, run_bytes, bar);
-    }
-  }
-  const double Dr = dfac[i];
-  const double Dh = kHalf * (Dr + Dr);
-  const double ax_n = ring_in[2 * (i - 1)] * bcn;
-  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
-  for (int r = tid; r < kMR; r += 256) {
-    const int j = j0 - 2 + r;
-    double st = 0.0, c2 = 0.0, c4 = 0.0;
-    if (j >= 2 && j <= ntm - 1) {
-      st = m.st_i[j];
-      c2 = Dh * m.dth_i[j] * m.dt_i[j] * st * m.sth[j];
-      c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * st * m.sth[j + 1];
-    }
-    tST[r] = st;
-    tC2[r] = c2;
-    tC4[r] = c4;
-  }
-  for (int c = tid; c < kMC; c += 256) {
-    const int kc = wrapc(k0 - 2 + c);
-    const int kw = kc == npm ? 2 : (kc == 1 ? npm - 1 : kc);
-    tP1[c] = Dh * m.dph_i[kw] * m.dp_i[kw];
-    tP5[c] = Dh * m.dph_i[kw + 1] * m.dp_i[kw];
-  }
-  if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
-    if (tid == 0) atomicExch(pa.err, 1);
-    mbar_wait_bounded(bar, 0, 1u << 22);
-    return;
-  }
-  __syncthreads();
-
-  const StageCoef sa = pa.ca, sb = pa.cb;
-  const int half = tid >> 7;
-  // ---------- phase 2: Y_k on shared rows 1..130, columns 1..nk+2
-  {
-    const int nc2 = nk + 2;
-    const int cA = (nc2 + 1) / 2;
-    const int cbeg = 1 + (half ? cA : 0), cend = half ? nc2 : cA;  // inclusive range [cbeg, cend]
-    const int r = 1 + (tid & 127);                                  // shared row (rows 1..128 here)
-    const int j = j0 - 2 + r;
-    const bool rowok = (j >= 1 && j <= ntm);
-    const bool pole = (j == 1 || j == ntm);
-    const double axp = (j == 1) ? ax_n : ax_s;
-    const double sti = tST[r], c2 = tC2[r], c4 = tC4[r];
-    double xl = sX1[SIDX(cbeg - 1, r)], xc = sX1[SIDX(cbeg, r)];
-    for (int c = cbeg; c <= cend; ++c) {
-      const double xr = sX1[SIDX(c + 1, r)];
-      double up = __shfl_up_sync(0xffffffffu, xc, 1);
-      double dn = __shfl_down_sync(0xffffffffu, xc, 1);
-      if (lane == 0) up = sX1[SIDX(c, r - 1)];
-      if (lane == 31) dn = sX1[SIDX(c, r + 1)];
-      double ax;
-      if (pole) {
-        ax = axp;
-      } else {
-        const double c1 = tP1[c] * sti * sti;
-        const double c5 = tP5[c] * sti * sti;
-        const double c3 = -(c1 + c2 + c4 + c5);
-        ax = c1 * xl + c2 * up + c3 * xc + c4 * dn + c5 * xr;
-      }
-      if (rowok) {
-        const double y = sa.a * xc + sa.b * sYk[SIDX(c, r)] + sa.c * sU[SIDX(c, r)] + sa.d * ax +
-                         sa.e * sD[SIDX(c, r)];
-        sYk[SIDX(c, r)] = y;
-        if (r >= 2 && c >= 2 && c < 2 + nk) {
-          const int k = k0 - 2 + c;
-          const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
-          out_k[q] = y;
-          if (k == 2) out_k[q + (int64_t)(npm - 2) * ld] = y;
-          if (k == npm - 1) out_k[q - (int64_t)(npm - 2) * ld] = y;
-        }
-      }
-      xl = xc;
-      xc = xr;
-    }
-    // shared rows 129 and 130 (theta j0+127, j0+128): one cell per thread
-    for (int e = tid; e < 2 * nc2; e += 256) {
-      const int rr = 129 + (e & 1);
-      const int c = 1 + (e >> 1);
-      const int jj = j0 - 2 + rr;
-      if (jj < 1 || jj > ntm) continue;
-      double ax;
-      if (jj == 1) {
-        ax = ax_n;
-      } else if (jj == ntm) {
-        ax = ax_s;
-      } else {
-        const double st2 = tST[rr];
-        const double c1 = tP1[c] * st2 * st2;
-        const double c5 = tP5[c] * st2 * st2;
-        const double c3 = -(c1 + tC2[rr] + tC4[rr] + c5);
-        ax = c1 * sX1[SIDX(c - 1, rr)] + tC2[rr] * sX1[SIDX(c, rr - 1)] + c3 * sX1[SIDX(c, rr)] +
-             tC4[rr] * sX1[SIDX(c, rr + 1)] + c5 * sX1[SIDX(c + 1, rr)];
-      }
-      const double y = sa.a * sX1[SIDX(c, rr)] + sa.b * sYk[SIDX(c, rr)] + sa.c * sU[SIDX(c, rr)] + sa.d * ax +
-                       sa.e * sD[SIDX(c, rr)];
-      sYk[SIDX(c, rr)] = y;
-      if (rr < 2 + kMJ && c >= 2 && c < 2 + nk) {
-        const int k = k0 - 2 + c;
-        const int64_t q = pbase + (int64_t)(k - 1) * ld + (jj - 1);
-        out_k[q] = y;
-        if (k == 2) out_k[q + (int64_t)(npm - 2) * ld] = y;
-        if (k == npm - 1) out_k[q - (int64_t)(npm - 2) * ld] = y;
-      }
-    }
-  }
-  __syncthreads();
-
-  const bool has_n = (j0 == 1);
-  const bool has_s = (ntm - 1 >= j0 && ntm - 1 <= j0 + kMJ - 1);
-  if (tid == 0 && (has_n || has_s)) {
-    if (has_n) {
-      double acc = 0.0;
-      for (int c = 2; c < 2 + nk; ++c)
-        acc = acc + (Dr + Dr) * (sYk[SIDX(c, 3)] - sYk[SIDX(c, 2)]) * m.dp[k0 - 2 + c];
-      ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
-    }
-    if (has_s) {
-      const int rS = ntm - (j0 - 2);
-      double acc = 0.0;
-      for (int c = 2; c < 2 + nk; ++c)
-        acc = acc + (Dr + Dr) * (sYk[SIDX(c, rS)] - sYk[SIDX(c, rS - 1)]) * m.dp[k0 - 2 + c];
-      ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
-    }
-  }
-
-  // ---------- phase 3: Y_{k+1} on shared rows 2..129, columns 2..nk+1
-  {
-    const int cA = (nk + 1) / 2;
-    const int cbeg = 2 + (half ? cA : 0), cend = half ? nk + 1 : 1 + cA;
-    const int r = 2 + (tid & 127);
-    const int j = j0 - 2 + r;
-    const bool rowok = (j >= 2 && j <= ntm - 1);
-    const double sti = tST[r], c2 = tC2[r], c4 = tC4[r];
-    double xl = sYk[SIDX(cbeg - 1, r)], xc = sYk[SIDX(cbeg, r)];
-    for (int c = cbeg; c <= cend; ++c) {
-      const double xr = sYk[SIDX(c + 1, r)];
-      double up = __shfl_up_sync(0xffffffffu, xc, 1);
-      double dn = __shfl_down_sync(0xffffffffu, xc, 1);
-      if (lane == 0) up = sYk[SIDX(c, r - 1)];
-      if (lane == 31) dn = sYk[SIDX(c, r + 1)];
-      const double c1 = tP1[c] * sti * sti;
-      const double c5 = tP5[c] * sti * sti;
-      const double c3 = -(c1 + c2 + c4 + c5);
-      const double ax = c1 * xl + c2 * up + c3 * xc + c4 * dn + c5 * xr;
-      if (rowok) {
-        const double y = sb.a * xc + sb.b * sX1[SIDX(c, r)] + sb.c * sU[SIDX(c, r)] + sb.d * ax +
-                         sb.e * sD[SIDX(c, r)];
-        const int k = k0 - 2 + c;
-        const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
-        out_k1[q] = y;
-        if (k == 2) out_k1[q + (int64_t)(npm - 2) * ld] = y;
-        if (k == npm - 1) out_k1[q - (int64_t)(npm - 2) * ld] = y;
-      }
-      xl = xc;
-      xc = xr;
-    }
-  }
-#undef SIDX
-
-  // ---- publish: the last pole-holding CTA of realization i finishes the poles
-  const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
-  if (contrib == 0) return;
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) {
-    const unsigned int old = atomicAdd(&ro.count[i - 1], (unsigned)contrib);
-    s_last = (old + (unsigned)contrib == 2u * (unsigned)ro.nkb) ? 1 : 0;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  double sn = 0.0, ss = 0.0;
-  for (int b = tid; b < ro.nkb; b += 256) {
-    sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + b]);
-    ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
-  }
-  block_sum2(sn, ss, &red[0][0]);
-  if (tid == 0) {
-    s_ring[0] = sn;
-    s_ring[1] = ss;
-  }
-  __syncthreads();
-  const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
-  double rn = 0.0, rsum = 0.0;
-  for (int k = 1 + tid; k <= npm; k += 256) {
-    const int64_t qn = pbase + (int64_t)(k - 1) * ld;
-    const int64_t qs = qn + (ntm - 1);
     const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
     const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
     const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];

@@ -29,9 +29,8 @@
 // before its arrival, so consumers start a tile without global loads or
 // index division.  Shared memory per CTA: 2 x 48.8 KB buffers + 10.6 KB for
 // Y_k = 108 KB, two CTAs per SM.  Tiles holding rows 2 / ntm-1 publish ring partials of Y_k; the
-// pole rows of Y_{k+1} and its ring sums are finished either by the last of
-// those tiles (atomic counter, no waiting; INLINE_POLES) or by k_pair_poles in
-// a launch of its own.
+// pole rows of Y_{k+1} and its ring sums are finished by k_pair_poles in a
+// launch of its own.
 #pragma once
 
 #include <cuda.h>  // CUtensorMap
@@ -147,31 +146,6 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// fixed-tree sum of two values over the 256 consumer threads; result in thread 0
-__device__ __forceinline__ void cons_sum2(double &a, double &b, double *sh) {
-  const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-  }
-  if (l == 0) {
-    sh[2 * w] = a;
-    sh[2 * w + 1] = b;
-  }
-  cons_sync();
-  if (w == 0) {
-    a = (l < kWCons / 32) ? sh[2 * l] : 0.0;
-    b = (l < kWCons / 32) ? sh[2 * l + 1] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_down_sync(0xffffffffu, a, o);
-      b += __shfl_down_sync(0xffffffffu, b, o);
-    }
-  }
-  cons_sync();
-}
-
 __device__ __forceinline__ int wrap_col(int c, int npm) {
   if (c < 1) return c + (npm - 2);
   if (c > npm) return c - (npm - 2);
@@ -281,7 +255,7 @@ __device__ __forceinline__ void ws_store_cols(double *out, int64_t pbase, int k0
 // RAGGED: the launch advances the realizations of pa.rlist, each with its
 // own stage coefficients pa.rc[2(i-1)], pa.rc[2(i-1)+1]; the producer copies
 // them into the tile record, so the consumers read them from shared memory.
-template <bool INLINE_POLES, bool ROWPAIRS = false, bool BULKST = false, bool RAGGED = false>
+template <bool ROWPAIRS, bool BULKST = false, bool RAGGED = false>
 __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const double *__restrict__ dfac,
                                                              const double *__restrict__ ykm1,
                                                              const double *__restrict__ ykm2,
@@ -293,10 +267,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
   extern __shared__ __align__(128) double wsm[];
   uint64_t *full = reinterpret_cast<uint64_t *>(wsm + kWEnd);
   uint64_t *empty = full + kWNB;
-  __shared__ double red[16];
-  __shared__ double s_ring[2];
-  __shared__ int s_last;
-  static_assert(!BULKST || (ROWPAIRS && !INLINE_POLES), "bulk stores need the row-pair consumers and k_pair_poles");
+  static_assert(!BULKST || ROWPAIRS, "bulk stores need the row-pair consumers");
 
   const int tid = threadIdx.x;
   const int ntm = m.ntm, npm = m.npm;
@@ -777,56 +748,6 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       }
     }
     mbar_arrive(&empty[b]);  // this thread is done with buffer b
-
-    // ---- the last pole-holding tile of realization i finishes the poles
-    // (or k_pair_poles does, in a launch of its own)
-    const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
-    if (INLINE_POLES && contrib) {
-      __threadfence();
-      cons_sync();
-      if (tid == 0) {
-        const unsigned int old = atomicAdd(&ro.count[i - 1], (unsigned)contrib);
-        s_last = (old + (unsigned)contrib == 2u * (unsigned)ro.nkb) ? 1 : 0;
-      }
-      cons_sync();
-      if (s_last) {
-        __threadfence();
-        double sn = 0.0, ss = 0.0;
-        for (int q = tid; q < ro.nkb; q += kWCons) {
-          sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + q]);
-          ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + q]);
-        }
-        cons_sum2(sn, ss, red);
-        if (tid == 0) {
-          s_ring[0] = sn;
-          s_ring[1] = ss;
-        }
-        cons_sync();
-        const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
-        double rn = 0.0, rsum = 0.0;
-        for (int k = 1 + tid; k <= npm; k += kWCons) {
-          const int64_t qn = pbase + (int64_t)(k - 1) * ld;  // row 1
-          const int64_t qs = qn + (ntm - 1);                 // row ntm
-          // Y_k at the pole rows, recomputed from the inputs
-          const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
-          const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
-          const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];
-          const double ys = sb.a * yks + sb.b * ykm1[qs] + sb.c * u0[qs] + sb.d * axs1 + sb.e * dty0[qs];
-          out_k1[qn] = yn;
-          out_k1[qs] = ys;
-          if (k >= 2 && k <= npm - 1) {
-            rn = rn + (Dr + Dr) * (__ldcg(&out_k1[qn + 1]) - yn) * m.dp[k];
-            rsum = rsum + (Dr + Dr) * (ys - __ldcg(&out_k1[qs - 1])) * m.dp[k];
-          }
-        }
-        cons_sum2(rn, rsum, red);
-        if (tid == 0) {
-          ro.ring[2 * (i - 1)] = rn;
-          ro.ring[2 * (i - 1) + 1] = rsum;
-          ro.count[i - 1] = 0u;
-        }
-      }
-    }
   }
   if (BULKST && w == 0) bulk_wait_all();  // this warp's Y_k stores, before the CTA exits
 }

@@ -141,6 +141,7 @@ SIGNATURES = [
     ("hipft_adj_set_tape_limit", ctypes.c_int, [_H, ctypes.c_int64, ctypes.c_int64]),
     ("hipft_adj_release", ctypes.c_int, [_H]),
     ("hipft_adj_assimilate", ctypes.c_int, [_H, DPTR, ctypes.POINTER(DAOpts), ctypes.c_void_p]),
+    ("hipft_gpu_describe", ctypes.c_int, [_H, ctypes.c_char_p, ctypes.c_size_t]),
     ("hipft_gpu_set_ragged", ctypes.c_int, [_H, ctypes.c_int]),
     ("hipft_gpu_flow_dtmax_each", ctypes.c_int, [_H, DPTR]),
     ("hipft_gpu_ragged_schedule", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
@@ -425,6 +426,12 @@ class HipftGPU:
         n, ms = ctypes.c_int64(0), ctypes.c_double(0.0)
         self._ck(self.L.hipft_gpu_kernel_time(self.h, int(kind), ctypes.byref(n), ctypes.byref(ms)), "kernel_time")
         return n.value, ms.value
+
+    def describe(self) -> str:
+        """Schedule and the two-stage kernel the autotuner picked."""
+        buf = ctypes.create_string_buffer(256)
+        self._ck(self.L.hipft_gpu_describe(self.h, buf, 256), "describe")
+        return buf.value.decode()
 
     def set_stream(self, stream_ptr: int):
         self._ck(self.L.hipft_gpu_set_stream(self.h, ctypes.c_void_p(stream_ptr)), "set_stream")

@@ -262,6 +262,10 @@ int hipft_gpu_set_profiling(hipft_gpu *h, int on);
 /* Launch count and summed device time (ms) of one kernel kind since
  * profiling was enabled (synchronizes the stream). */
 int hipft_gpu_kernel_time(hipft_gpu *h, int kind, int64_t *launches, double *total_ms);
+/* No counterpart in the reference: a one-line description of how the handle
+ * runs (shared or ragged schedule; the two-stage RKG2 kernel the autotuner
+ * picked for this grid and its timed launch, or the one HIPFT_STS_PAIR fixed). */
+int hipft_gpu_describe(hipft_gpu *h, char *buf, size_t len);
 /* Runs subsequent work on a caller-owned cudaStream_t (NULL: the handle's). */
 int hipft_gpu_set_stream(hipft_gpu *h, void *cuda_stream);
 int hipft_gpu_synchronize(hipft_gpu *h);
