@@ -196,28 +196,45 @@ class OrcHist(ctypes.Structure):
 
 
 _lib = None
+_fast = None
+FAST_PATH = os.path.join(HERE, "liboracle_fast.so")
+FAST_FLAGS = "-O3 -march=x86-64-v3 -fopenmp (contraction allowed)"
 
 
 def build():
-    """Compile liboracle.so from hipft_oracle.c (gcc; no GPU needed)."""
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """Compile liboracle.so (parity build) and liboracle_fast.so (timing
+    build) from hipft_oracle.c (gcc; no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def _load(path, target):
+    src = os.path.join(HERE, "hipft_oracle.c")
+    if not os.path.exists(path) or (os.path.exists(src) and os.path.getmtime(src) > os.path.getmtime(path)):
+        subprocess.run(["make", "-s", "-C", HERE, target], check=True)
+    L = ctypes.CDLL(path)
+    L.orc_run.restype = ctypes.c_int
+    L.orc_run.argtypes = [
+        ctypes.POINTER(OrcParams), ctypes.c_int, ctypes.c_int,
+        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ctypes.POINTER(OrcHist), ctypes.c_long, ctypes.c_void_p]
+    return L
 
 
 def lib():
+    """The parity build (-O2 -ffp-contract=off), the oracle of every test."""
     global _lib
     if _lib is None:
-        src = os.path.join(HERE, "hipft_oracle.c")
-        if not os.path.exists(LIB_PATH) or (
-                os.path.exists(src) and os.path.getmtime(src) > os.path.getmtime(LIB_PATH)):
-            build()
-        _lib = ctypes.CDLL(LIB_PATH)
-        _lib.orc_run.restype = ctypes.c_int
-        _lib.orc_run.argtypes = [
-            ctypes.POINTER(OrcParams), ctypes.c_int, ctypes.c_int,
-            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-            ctypes.POINTER(OrcHist), ctypes.c_long, ctypes.c_void_p]
+        _lib = _load(LIB_PATH, "liboracle.so")
     return _lib
+
+
+def lib_fast():
+    """The timing build of the same source, for the CPU baseline only."""
+    global _fast
+    if _fast is None:
+        _fast = _load(FAST_PATH, "liboracle_fast.so")
+    return _fast
 
 
 def _ptr(a):
@@ -243,7 +260,7 @@ def _params_struct(p: dict):
 
 def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
         max_steps: int = 0, hist_cap: int = 0, want_field: bool = True, map_cap: int = 0, flows=None,
-        source=None):
+        source=None, fast: bool = False):
     """Run the oracle on processed parameters ``p``.
 
     map_pt: (nr, ntm, npm1) C-order array (i.e. Fortran (npm1,ntm,nr)), or None.
@@ -254,8 +271,9 @@ def run(p: dict, map_pt=None, s1=None, s2=None, da_times=None, da_maps=None,
     flows (use_flow_from_files): dict(jd=(n,), vt=(n, nt, npm1), vp=(n, ntm, np)),
     the flow list's Julian days and the files' data in C order, m/s.
     source (source_from_file): dict(data=(nft, nfp) C order, pf=(nfp,), tf=(nft,)).
+    fast: run the timing build (lib_fast) instead of the parity build.
     """
-    L = lib()
+    L = lib_fast() if fast else lib()
     nr = int(p["n_realizations"])
     c, keep = _params_struct(p)
     if flows is not None:
