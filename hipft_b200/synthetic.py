@@ -18,6 +18,13 @@ benchmark configurations.
   the Carrington rate, in the [data, weight, mu] slice order of HipFT's
   assimilation maps.
 
+* ``supergranular_flow``: a random divergent velocity v = grad(psi), psi a
+  sum of Gaussian cells of correlation length 30 Mm with random signs and
+  centres, differenced onto HipFT's staggered faces (vt on theta faces, vp on
+  phi faces), scaled to 300 m/s rms and returned in the layouts of HipFT's
+  flow files (use_flow_from_files, src/hipft.f90:3525-3873).  A new field per
+  day: ``supergranular_flow(..., day=d)`` seeds with (seed, d).
+
 Flow-model conversion (HipFT's analytic models, src/hipft.f90:7219-7285):
 Omega = A + B cos^2 + C cos^4 deg/day becomes vp = st (p0 + p2 ct^2 + p4 ct^4)
 m/s with p = (pi/180)/86400 * 6.96e8 * (A, B, C); v0 sin(2 lat) cos^2(lat)
@@ -124,3 +131,77 @@ def observed_map(t: np.ndarray, p: np.ndarray, time_hr: float, seed: int, noise_
     mu = np.sin(t)[:, None] * np.cos(p[None, :] - lon0)
     weight = np.where(mu > 0.1, mu ** 4, 0.0)
     return np.stack([data, weight, mu])
+
+
+RSUN_MM = 696.0  # solar radius, Mm
+
+
+def supergranular_psi(t: np.ndarray, p: np.ndarray, seed: int, day: int = 0, corr_mm: float = 30.0,
+                      window: float = 5.0) -> np.ndarray:
+    """The random potential of supergranular_flow at the nodes t x p,
+    (ntm, npm1): psi = sum_n a_n exp(-d_n^2 / (2 L^2)), d_n the chord distance
+    to centre n on the unit sphere, L = corr_mm / 696 Mm, a_n = +-1, centres
+    uniform on the sphere with one per L^2 of area, each cell evaluated within
+    `window` L of its centre."""
+    rng = np.random.Generator(np.random.PCG64([seed, day]))
+    L = corr_mm / RSUN_MM
+    n = int(4.0 * np.pi / (L * L))
+    z = rng.uniform(-1.0, 1.0, n)
+    lon = rng.uniform(0.0, 2.0 * np.pi, n)
+    amp = rng.choice([-1.0, 1.0], n)
+    R = window * L
+    psi = np.zeros((len(t), len(p)))
+    for c_z, c_lon, a in zip(z, lon, amp):
+        c_t = np.arccos(c_z)
+        r0, r1 = np.searchsorted(t, c_t - R), np.searchsorted(t, c_t + R)
+        if r1 <= r0:
+            continue
+        st, ct = np.sin(t[r0:r1]), np.cos(t[r0:r1])
+        smin = min(np.sin(c_t - R), np.sin(c_t + R)) if R < c_t < np.pi - R else 0.0
+        if smin > R:
+            dphi = np.abs(((p - c_lon + np.pi) % (2.0 * np.pi)) - np.pi)
+            cols = np.nonzero(dphi <= R / smin)[0]
+        else:
+            cols = np.arange(len(p))
+        s_c = np.sqrt(max(1.0 - c_z * c_z, 0.0))
+        dot = st[:, None] * s_c * np.cos(p[cols][None, :] - c_lon) + ct[:, None] * c_z
+        psi[r0:r1, cols] += a * np.exp(-(2.0 - 2.0 * dot) / (2.0 * L * L))
+    return psi
+
+
+def supergranular_flow(t: np.ndarray, p: np.ndarray, seed: int, day: int = 0, corr_mm: float = 30.0,
+                       rms_m_s: float = 300.0, coarse=None):
+    """Random divergent flow v = grad(psi) for the day `day` (psi of
+    supergranular_psi), scaled to rms_m_s: returns (vt, vp) in m/s in the
+    flow-file layouts, vt (nt, npm1) on theta faces x phi nodes and vp
+    (ntm, np) on theta nodes x phi faces (C order, phi fastest: the files'
+    Fortran (npm1, nt) and (np, ntm)).  vt(j) = (psi(t_j) - psi(t_{j-1})) / (t_j - t_{j-1}) on the
+    interior faces (zero on the faces beyond the poles), vp(k) = (psi(p_k) -
+    psi(p_{k-1})) / (sin t (p_k - p_{k-1})) (zero on the pole rows), phi
+    periodic.  coarse = (ntc, npc): evaluate psi on a uniform ntc x npc grid
+    and interpolate it (cubic) to the nodes, for large grids."""
+    if coarse is None:
+        psi = supergranular_psi(t, p, seed, day, corr_mm)
+    else:
+        from scipy.interpolate import RegularGridInterpolator
+        tc = np.linspace(0.0, np.pi, coarse[0])
+        pc = np.linspace(0.0, 2.0 * np.pi, coarse[1])
+        pc_ext = np.concatenate([pc[-4:-1] - 2.0 * np.pi, pc, pc[1:4] + 2.0 * np.pi])
+        psic = supergranular_psi(tc, pc, seed, day, corr_mm)
+        psic = np.concatenate([psic[:, -4:-1], psic, psic[:, 1:4]], axis=1)
+        f = RegularGridInterpolator((tc, pc_ext), psic, method="cubic")
+        T, P = np.meshgrid(t, p, indexing="ij")
+        psi = f(np.stack([T.ravel(), P.ravel()], axis=1)).reshape(len(t), len(p))
+    ntm, npm1 = psi.shape
+    vt = np.zeros((ntm + 1, npm1))
+    vt[1:ntm] = (psi[1:] - psi[:-1]) / (t[1:] - t[:-1])[:, None]
+    vp = np.zeros((ntm, npm1 + 1))
+    st = np.sin(t)
+    dps = (psi[:, 1:] - psi[:, :-1]) / (p[1:] - p[:-1])[None, :]
+    inner = slice(1, ntm - 1)
+    vp[inner, 1:npm1] = dps[inner] / st[inner, None]
+    vp[:, 0] = vp[:, npm1 - 1]
+    vp[:, npm1] = vp[:, 1]
+    rms = np.sqrt(0.5 * (np.mean(vt ** 2) + np.mean(vp ** 2)))
+    scale = (rms_m_s / rms) if rms > 0 else 0.0
+    return vt * scale, vp * scale
