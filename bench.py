@@ -435,6 +435,8 @@ def run_gpu(args, wl, name):
         out["plain"] = measure_plain(args, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
         out["adjoint"] = measure_adjoint(args, local)
+    if rank == 0 and world == 1 and args.c5:
+        out["c5"] = measure_c5(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         idx = [0, 1, 2, 3]
@@ -625,6 +627,60 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
                     "the segment recompute, the per-step replay with its tape and the reverse kernels"}
 
 
+def measure_c5(args, local: int, steps: int = 2):
+    """The large configuration's forward leg: 16 realizations (seed 2, the
+    64-realization configuration's parameter ranges) on 2048 x 4096 with theta
+    refined near the poles, the random divergent supergranular flow of day 0
+    (30 Mm, 300 m/s rms; shared by the realizations, as HipFT's flow files are)
+    under each realization's analytic differential rotation and meridional
+    flow, ragged schedule, a few steps at the CFL-limited dt."""
+    import torch
+    import hipft_b200 as H
+    from hipft_b200 import synthetic as S
+    ntm, npm1, nr, seed = 2048, 4097, 16, 2
+    t = S.refined_theta(ntm)
+    p = S.uniform_phi(npm1)
+    br = S.bipole_map(t, p, seed)
+    prm = S.batched_params(nr, seed)
+    w0 = time.perf_counter()
+    vt, vp = S.supergranular_flow(t, p, seed, day=0, coarse=(256, 513))
+    gen_s = time.perf_counter() - w0
+    g = H.HipftGPU(t, p, nr, device=local, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                   advance_diffusion=True, diffusion_coef_constants=prm["diffusion_coef_constants"])
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    g.load_initial_map(np.broadcast_to(br, (nr,) + br.shape))
+    g.set_flow_from_files(vt, vp, at_load=True)
+    g.set_flow(dr_model=1, mf_model=1, dr_p0=prm["dr_p0"], dr_p2=prm["dr_p2"], dr_p4=prm["dr_p4"],
+               mf_p1=prm["mf_p1"], mf_p3=prm["mf_p3"], mf_p5=prm["mf_p5"])
+    g.update_flow()
+    g.set_ragged(True)
+    dt = g.flow_dtmax()
+    g.flux_transport_step(dt)
+    torch.cuda.synchronize()
+    i0 = g.info()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        g.update_flow()
+        g.flux_transport_step(dt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    i1 = g.info()
+    sched = g.ragged_schedule()
+    out = {"workload": "batched16_2048x4096", "grid": [ntm, npm1 - 1], "realizations": nr, "steps": steps,
+           "dt_hours": dt, "ms_per_step": ms / steps,
+           "value": float(i1.cell_stage_updates - i0.cell_stage_updates) / (ms * 1e-3) / 1e9, "unit": UNIT,
+           "realization_steps_per_s": nr * steps / (ms * 1e-3),
+           "rkg2_stages_per_realization": [int(x) for x in sched["sts_s"]],
+           "device_bytes": int(i1.device_bytes), "flow_generation_s": gen_s,
+           "note": "flows from the supergranular generator through hipft_gpu_set_flow_from_files, rebuilt at "
+                   "every update_flow as HipFT does while flows come from files"}
+    g.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -635,6 +691,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
+    ap.add_argument("--c5", action="store_true", help="add the 16-realization 2048 x 4096 forward leg")
     ap.add_argument("--schedule", default="ragged", choices=["ragged", "shared"],
                     help="ragged: every realization its own schedule (default); shared: the reference's")
     args = ap.parse_args()

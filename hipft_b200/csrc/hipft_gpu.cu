@@ -20,6 +20,7 @@
 #include "../../include/hipft_gpu.h"
 #include "kernels.cuh"
 #include "sts_pair_ws.cuh"
+#include "sts_quad_ws.cuh"
 #include "adjoint.cuh"
 
 using namespace hipft;
@@ -43,12 +44,12 @@ constexpr double c_sixth = 0.16666666666666666;
 constexpr double c_two_third = 0.66666666666666666;
 constexpr double c_third = 0.33333333333333333;
 
-constexpr int kNBuf = 6;  // current field + 5 scratch fields (two-stage RKG2 needs two fresh outputs)
+constexpr int kNBuf = 8;  // current field + scratch: u0, dty0, two inputs and up to four outputs of a pass
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
 // Two-stage kernel kinds (see the autotuner) and the plan a handle uses.
-enum { PK_SINGLE = 0, PK_TILE = 1, PK_WS_ROWS1 = 4, PK_WS_ROWS2 = 5, PK_WS_BULK = 6 };
+enum { PK_SINGLE = 0, PK_TILE = 1, PK_WS_ROWS1 = 4, PK_WS_ROWS2 = 5, PK_WS_BULK = 6, PK_WS_QUAD = 7 };
 struct PairPlan {
   int kind = -1;    // PK_*; -1: not chosen yet
   int shape = 0;    // kPairShapes index (PK_TILE)
@@ -83,6 +84,7 @@ struct hipft_gpu {
   double bc_flow_n = 0, bc_flow_s = 0, bc_diff_n = 0, bc_diff_s = 0;
   // fields
   double *buf[kNBuf] = {};
+  int nbuf = 6;             // allocated fields (8 once the four-stage path is in use)
   int cur = 0;
   bool field_set = false;
   // flows
@@ -112,12 +114,18 @@ struct hipft_gpu {
   PairPlan plan{};          // two-stage kernel chosen for this grid (autotuner)
   struct WsMapEntry {
     const void *p;
-    int cols;
+    int rows, cols;
     CUtensorMap m;
   };
   std::vector<WsMapEntry> ws_map_cache;  // tensor maps of the field buffers, by (pointer, box columns)
   CUtensorMap ws_rt_map{};               // tensor map of ptab.row
   bool ws_rt_ok = false;
+  // four stages per pass on the interior theta blocks
+  int q_rb_lo = 0, q_rb_hi = -1;         // interior blocks (none when q_rb_hi < q_rb_lo)
+  double *d_qcol = nullptr;              // column table of the quad tiles
+  int q_LC = 0, q_nkt = 0;
+  CUtensorMap q_rt_map{};
+  bool q_rt_ok = false;
   // adjoint: fields of one taped forward step, folded work fields (seam
   // columns stay zero), per-block partial sums and pole sums
   std::vector<double *> tape;
@@ -349,7 +357,7 @@ static void weno_weights(const hipft_gpu *h, std::vector<double> wt[7], std::vec
 // Scratch buffer n (0,1,2) other than the current field.
 static int scratch(const hipft_gpu *h, int n) {
   int c = 0;
-  for (int b = 0; b < kNBuf; ++b) {
+  for (int b = 0; b < h->nbuf; ++b) {
     if (b == h->cur) continue;
     if (c == n) return b;
     ++c;
@@ -475,18 +483,19 @@ static bool encode_f64_3d(CUtensorMap *m, const void *base, uint64_t d0, uint64_
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// a field buffer's map with a box of kWR rows x cols columns (cached)
-static bool field_map(hipft_gpu *h, const double *p, int cols, CUtensorMap *out) {
+// a field buffer's map with a box of rows x cols (cached)
+static bool field_map(hipft_gpu *h, const double *p, int cols, CUtensorMap *out, int rows = kWR) {
   for (const auto &e : h->ws_map_cache)
-    if (e.p == p && e.cols == cols) {
+    if (e.p == p && e.cols == cols && e.rows == rows) {
       *out = e.m;
       return true;
     }
   hipft_gpu::WsMapEntry e{};
   e.p = p;
+  e.rows = rows;
   e.cols = cols;
   if (!encode_f64_3d(&e.m, p, (uint64_t)h->ldt, (uint64_t)h->npm, (uint64_t)h->nr, (uint64_t)h->ldt * 8,
-                     (uint64_t)h->plane * 8, kWR, (uint32_t)cols))
+                     (uint64_t)h->plane * 8, (uint32_t)rows, (uint32_t)cols))
     return false;
   h->ws_map_cache.push_back(e);
   *out = e.m;
@@ -567,8 +576,11 @@ static cudaError_t pair_attrs_all() {
 // seven tile shapes) sum the pole rings in another order, so they are not
 // candidates -- a run's result must not depend on timing noise -- and are
 // selected explicitly: HIPFT_STS_PAIR (0: one stage per launch, 1: tiles of
-// HIPFT_PAIR_TILE, 4/5/6: the warp-specialised kinds) fixes the choice, and
-// HIPFT_TUNE=0 takes PK_WS_ROWS2 at 2 CTAs per SM without timing.
+// HIPFT_PAIR_TILE, 4/5/6: the warp-specialised kinds, 7: four stages per pass
+// on the interior theta blocks) fixes the choice, and HIPFT_TUNE=0 takes
+// PK_WS_ROWS2 at 2 CTAs per SM without timing.  The four-stage path
+// (PK_WS_QUAD, sts_quad_ws.cuh) computes the same cell values and is a
+// candidate whenever the grid has interior blocks.
 
 static const char *pair_kind_name(int k) {
   switch (k) {
@@ -577,6 +589,7 @@ static const char *pair_kind_name(int k) {
     case PK_WS_ROWS1: return "ws-rows1";
     case PK_WS_ROWS2: return "ws-rows2";
     case PK_WS_BULK: return "ws-bulk";
+    case PK_WS_QUAD: return "ws-quad (four stages per pass on interior blocks)";
   }
   return "?";
 }
@@ -588,7 +601,7 @@ static bool env_plan(PairPlan &p) {
   const char *e = std::getenv("HIPFT_STS_PAIR");
   if (e) {
     const int v = std::atoi(e);
-    p.kind = (v == 0 || v == 1 || v == 4 || v == 6) ? v : PK_WS_ROWS2;
+    p.kind = (v == 0 || v == 1 || v == 4 || v == 6 || v == 7) ? v : PK_WS_ROWS2;
     if (p.kind == PK_TILE) {
       const char *t = std::getenv("HIPFT_PAIR_TILE");
       for (int q = 0; t && q < kNPairShapes; ++q)
@@ -672,7 +685,132 @@ static int sts_pair_plan(hipft_gpu *h, const PairPlan &pl, const double *ykm1, c
 
 static int sts_pair(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
                     double *out_k, double *out_k1, StageCoef ca, StageCoef cb, bool overlap_prev) {
-  return sts_pair_plan(h, h->plan, ykm1, ykm2, u0, dty0, out_k, out_k1, ca, cb, overlap_prev);
+  PairPlan pl = h->plan;
+  if (pl.kind == PK_WS_QUAD) pl.kind = PK_WS_ROWS2;  // lone pairs of a four-stage plan
+  return sts_pair_plan(h, pl, ykm1, ykm2, u0, dty0, out_k, out_k1, ca, cb, overlap_prev);
+}
+
+// ------------------------------------------------ four stages per pass
+// The interior theta blocks rb_lo..rb_hi (rows j0-3 .. j0+130 of a block
+// inside 2..ntm-1, see sts_quad_ws.cuh); false when there are none.
+static bool quad_eligible(const hipft_gpu *h) {
+  if (h->DC.grid || !h->ptab.row || h->ntm < kQJ + 132) return false;
+  const int rb_hi = (h->ntm - 132) / kQJ;  // largest rb with 128 rb + 132 <= ntm
+  return h->ptab.nb - rb_hi <= 6;           // pole blocks: 0 and rb_hi+1 .. nb-1
+}
+
+// Tables, tensor map and the two extra fields of the four-stage path.
+static int quad_setup(hipft_gpu *h) {
+  if (h->d_qcol) return HIPFT_OK;
+  h->q_rb_lo = 1;
+  h->q_rb_hi = (h->ntm - 132) / kQJ;
+  while (h->nbuf < kNBuf) {
+    TRY(dalloc(h, &h->buf[h->nbuf], h->fieldn));
+    CK(h, cudaMemsetAsync(h->buf[h->nbuf], 0, h->fieldn * sizeof(double), h->stream));
+    ++h->nbuf;
+  }
+  h->q_nkt = (h->npm - 2 + kQK - 1) / kQK;
+  h->q_LC = h->q_nkt * kQK + 24;
+  TRY(dalloc(h, &h->d_qcol, (size_t)h->nr * h->q_LC * 2));
+  k_quad_coltab<<<2 * h->num_sms, 256, 0, h->stream>>>(h->M, h->DC.dfac, h->q_LC, h->d_qcol);
+  LAUNCHED(h);
+  h->q_rt_ok = encode_f64_3d(&h->q_rt_map, h->ptab.row, (uint64_t)h->ptab.LR, 3, (uint64_t)h->nr,
+                             (uint64_t)h->ptab.LR * 8, (uint64_t)h->ptab.LR * 24, kQR, 3);
+  CK(h, cudaFuncSetAttribute(k_sts_quad_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
+  return HIPFT_OK;
+}
+
+// The pole blocks (every block outside rb_lo..rb_hi) for the two-stage launches
+static PairTables quad_pole_tables(const hipft_gpu *h, int nreal) {
+  PairTables pt = h->ptab;
+  pt.nsel = 0;
+  for (int rb = 0; rb < pt.nb; ++rb)
+    if (rb < h->q_rb_lo || rb > h->q_rb_hi) pt.sel[pt.nsel++] = rb;
+  pt.ntiles = pt.nsel * pt.nkt * nreal;
+  return pt;
+}
+
+// Two-stage launch (k_sts_pair_ws, two rows per consumer) plus k_pair_poles
+// over the tiles of `pt`.
+static int ws_pair_launch(hipft_gpu *h, const PairTables &pt, int cps, const double *ykm1, const double *ykm2,
+                          const double *u0, const double *dty0, double *out_k, double *out_k1, StageCoef ca,
+                          StageCoef cb, bool overlap_prev) {
+  const int nkt = (h->npm - 2 + kWK - 1) / kWK;
+  RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
+  const int grid = std::min(pt.ntiles, cps * h->num_sms);
+  const PairArgs pa{ca, cb, h->d_err};
+  const double *rin = h->d_ringbuf[h->ring_cur];
+  const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kWThreads);
+  cfg.dynamicSmemBytes = kWSmem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
+                                      dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, pt, tmaps);
+  if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
+  LAUNCHED(h);
+  dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
+  k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin, h->bc_diff_n,
+                                                   h->bc_diff_s, pa, ro, h->pole);
+  LAUNCHED(h);
+  h->ring_cur = 1 - h->ring_cur;
+  return HIPFT_OK;
+}
+
+// Stages k..k+3: the pole blocks by two two-stage launches, the interior
+// blocks by one four-stage launch between them (it reads nothing the first
+// pole launch writes, so it may start while that launch's pole kernel runs).
+// Outputs ok..ok3 hold Y_k..Y_{k+3}; Y_k and Y_{k+1} only on the pole blocks
+// and the interior blocks' edge rows.
+static int quad_pass(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
+                     double *ok, double *ok1, double *ok2, double *ok3, const StageCoef c[4], bool overlap_prev) {
+  const int cps = h->plan.ctas_per_sm;
+  const PairTables pp = quad_pole_tables(h, h->nr);
+  ProfScope ps(h, HIPFT_K_STS);
+  TRY(ws_pair_launch(h, pp, cps, ykm1, ykm2, u0, dty0, ok, ok1, c[0], c[1], overlap_prev));
+  {
+    QuadArgs qa{};
+    for (int q = 0; q < 4; ++q) qa.c[q] = c[q];
+    qa.err = h->d_err;
+    qa.rb_lo = h->q_rb_lo;
+    qa.nbi = h->q_rb_hi - h->q_rb_lo + 1;
+    qa.nkt = h->q_nkt;
+    qa.ntiles = qa.nbi * qa.nkt * h->nr;
+    qa.edge_lo = (h->q_rb_lo > 0) ? h->q_rb_lo : -1;
+    qa.edge_hi = (h->q_rb_hi < h->ptab.nb - 1) ? h->q_rb_hi : -1;
+    qa.col = h->d_qcol;
+    qa.LC = h->q_LC;
+    QuadMaps qm;
+    std::memset(&qm, 0, sizeof(qm));
+    if (ws_tmap_enabled() && h->q_rt_ok && field_map(h, ykm1, kQX, &qm.x1, kQR) &&
+        field_map(h, ykm2, kQI, &qm.y2, kQR) && field_map(h, u0, kQI, &qm.u, kQR) &&
+        field_map(h, dty0, kQI, &qm.d, kQR)) {
+      qm.rt = h->q_rt_map;
+      qm.on = 1;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)std::min(qa.ntiles, 2 * h->num_sms));
+    cfg.blockDim = dim3(kQThreads);
+    cfg.dynamicSmemBytes = kQSmem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = ws_pdl() ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    PairTables pt = h->ptab;
+    cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_quad_ws, h->M, ykm1, ykm2, u0, dty0, ok, ok1, ok2, ok3, qa, pt, qm);
+    if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_quad_ws launch: %s", cudaGetErrorString(le));
+    LAUNCHED(h);
+  }
+  TRY(ws_pair_launch(h, pp, cps, ok1, ok, u0, dty0, ok2, ok3, c[2], c[3], false));
+  return HIPFT_OK;
 }
 
 // Chooses the handle's two-stage plan (see the autotuner above) before the
@@ -683,6 +821,10 @@ static int ensure_pair_plan(hipft_gpu *h) {
   if (h->plan.kind >= 0) return HIPFT_OK;
   PairPlan p;
   if (env_plan(p)) {
+    if (p.kind == PK_WS_QUAD) {
+      if (quad_eligible(h)) TRY(quad_setup(h));
+      else p.kind = PK_WS_ROWS2;
+    }
     h->plan = p;
     return HIPFT_OK;
   }
@@ -707,27 +849,43 @@ static int ensure_pair_plan(hipft_gpu *h) {
     q.kind = k;
     cands.push_back(q);
   }
+  if (quad_eligible(h)) {
+    TRY(quad_setup(h));
+    PairPlan q;
+    q.kind = PK_WS_QUAD;
+    cands.push_back(q);
+  }
   const bool prof = h->profiling;
   h->profiling = false;
   const double *x = h->buf[h->cur];
-  double *bufs[4];
-  for (int q = 0; q < 4; ++q) bufs[q] = h->buf[scratch(h, q)];
+  double *bufs[6] = {};
+  for (int q = 0; q < 6 && q < h->nbuf - 1; ++q) bufs[q] = h->buf[scratch(h, q)];
   const StageCoef ca{0.5, -0.1, 0.6, 1e-3, 0.0}, cb{0.5, -0.1, 0.6, 1e-3, 0.0};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   CK(h, cudaEventCreate(&e0));
   CK(h, cudaEventCreate(&e1));
   int best = 0;
   const int reps = 3;
+  const StageCoef cq[4] = {ca, cb, ca, cb};
   for (size_t c = 0; c < cands.size(); ++c) {
-    TRY(sts_pair_plan(h, cands[c], x, bufs[0], x, bufs[1], bufs[2], bufs[3], ca, cb, false));  // warm-up
+    // time per two stages: a four-stage pass counts as two launch pairs
+    const bool quad = cands[c].kind == PK_WS_QUAD;
+    const PairPlan saved = h->plan;
+    h->plan = cands[c];
+    auto once = [&](bool ov) -> int {
+      if (quad) return quad_pass(h, x, bufs[0], x, bufs[1], bufs[2], bufs[3], bufs[4], bufs[5], cq, ov);
+      return sts_pair_plan(h, cands[c], x, bufs[0], x, bufs[1], bufs[2], bufs[3], ca, cb, ov);
+    };
+    int rc = once(false);  // warm-up
     CK(h, cudaEventRecord(e0, h->stream));
-    for (int r = 0; r < reps; ++r)
-      TRY(sts_pair_plan(h, cands[c], x, bufs[0], x, bufs[1], bufs[2], bufs[3], ca, cb, r > 0));
+    for (int r = 0; r < reps && rc == HIPFT_OK; ++r) rc = once(r > 0);
+    h->plan = saved;
+    TRY(rc);
     CK(h, cudaEventRecord(e1, h->stream));
     CK(h, cudaEventSynchronize(e1));
     float ms = 0.f;
     CK(h, cudaEventElapsedTime(&ms, e0, e1));
-    cands[c].ms = ms / reps;
+    cands[c].ms = ms / reps / (quad ? 2.0 : 1.0);
     if (cands[c].ms < cands[best].ms) best = (int)c;
   }
   cudaEventDestroy(e0);
@@ -846,8 +1004,8 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   h->M.st_i = dm + offs[4]; h->M.sth = dm + offs[5]; h->M.dp = dm + offs[6]; h->M.dth = dm + offs[7];
   h->M.dph = dm + offs[8];
 
-  // fields
-  for (int b = 0; b < kNBuf; ++b) {
+  // fields (the four-stage path adds two more when it is first used)
+  for (int b = 0; b < h->nbuf; ++b) {
     if ((rc = dalloc(h, &h->buf[b], h->fieldn))) return bail(rc);
     if (cudaMemsetAsync(h->buf[b], 0, h->fieldn * sizeof(double), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
   }
@@ -1462,13 +1620,27 @@ static int sts_super_step(hipft_gpu *h, double dtl) {
   };
   // a buffer not holding u0, dty0, Y_{k-1}, Y_{k-2} (or `avoid`)
   auto free_buf = [&](int avoid) {
-    for (int b = 0; b < kNBuf; ++b)
+    for (int b = 0; b < h->nbuf; ++b)
       if (b != u0 && b != idty && b != ykm1 && b != ykm2 && b != avoid) return b;
     return -1;
   };
   (void)ib;
   int64_t k = 2;
   while (k <= h->sts_s) {
+    if (fused && h->plan.kind == PK_WS_QUAD && k + 3 <= h->sts_s) {
+      int ob[4], no = 0;
+      for (int b = 0; b < h->nbuf && no < 4; ++b)
+        if (b != u0 && b != idty && b != ykm1 && b != ykm2) ob[no++] = b;
+      const StageCoef cq[4] = {coef(k), coef(k + 1), coef(k + 2), coef(k + 3)};
+      TRY(quad_pass(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[ob[0]], h->buf[ob[1]],
+                    h->buf[ob[2]], h->buf[ob[3]], cq, k > 2));
+      ykm2 = ob[2];
+      ykm1 = ob[3];
+      k += 4;
+      h->rkg2_stages += 4;
+      h->rkg2_cell_stages += 4 * (int64_t)h->ntm * (h->npm - 2) * h->nr;
+      continue;
+    }
     if (fused && sts_pairs_enabled(h) && k + 1 <= h->sts_s) {
       int bk = free_buf(-1), bk1 = free_buf(bk);
       TRY(sts_pair(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[bk], h->buf[bk1], coef(k),
@@ -1785,7 +1957,7 @@ static int ragged_super_step(hipft_gpu *h, std::vector<int> act, const std::vect
   }
   int ykm1 = ia, ykm2 = u0;
   auto free_buf = [&](int avoid) {
-    for (int b = 0; b < kNBuf; ++b)
+    for (int b = 0; b < h->nbuf; ++b)
       if (b != u0 && b != idty && b != ykm1 && b != ykm2 && b != avoid) return b;
     return -1;
   };
@@ -2408,7 +2580,7 @@ extern "C" int hipft_gpu_info(const hipft_gpu *h, hipft_info *info) {
 extern "C" int hipft_gpu_describe(hipft_gpu *h, char *buf, size_t len) {
   if (!h || !buf || !len) return HIPFT_EINVAL;
   const PairPlan &p = h->plan;
-  char kind[64];
+  char kind[128];
   if (p.kind < 0)
     std::snprintf(kind, sizeof kind, "not chosen yet");
   else if (p.kind == PK_TILE)

@@ -156,6 +156,10 @@ struct PairTables {
   const double *row, *col;  // k_pair_tables output
   int LR, LC;               // entries per realization
   int nb, nkt, ntiles;      // theta blocks, phi tiles, all tiles
+  // nsel > 0: the launch covers only theta blocks sel[0..nsel-1] (the pole
+  // blocks, when the interior blocks take four stages per pass)
+  int nsel = 0;
+  int sel[6] = {};
 };
 
 // One stencil-and-combine step for a theta-row pair (a, b = a+1) of one
@@ -216,6 +220,11 @@ __device__ __forceinline__ void ws_tile(const PairTables &pt, int t, int &kt, in
                                         const int *rlist) {
   kt = t % pt.nkt;
   const int rest = t / pt.nkt;
+  if (pt.nsel > 0) {
+    rb = pt.sel[rest % pt.nsel];
+    i = (rlist ? rlist[rest / pt.nsel] : rest / pt.nsel) + 1;
+    return;
+  }
   const int q = rest % pt.nb;
   i = (rlist ? rlist[rest / pt.nb] : rest / pt.nb) + 1;
   rb = (pt.nb <= 2) ? q : ((q < pt.nb - 2) ? q + 1 : ((q == pt.nb - 2) ? 0 : pt.nb - 1));

@@ -1,0 +1,310 @@
+// Four RKG2 stages per HBM pass on the interior theta blocks.
+//
+// Stages k..k+3 of diffusion_step_sts_cd (src/hipft.f90:5222-5237) with the
+// 5-point operator of diffusion_operator_cd (src/hipft.f90:7927-7984).  A
+// theta block is "interior" when the rows that its four stages compute, with
+// their halos, stay clear of the pole rows 1 and ntm: then no stage of the
+// block needs the pole-ring sums, which couple every phi column, and the
+// block can advance four stages from one load of its inputs.  The pole blocks
+// take the two-stage path twice (k_sts_pair_ws + k_pair_poles for stages
+// k, k+1, then for k+2, k+3), which supplies the ring sums.
+//
+// A tile is 128 theta rows x 16 phi columns.  Its inputs are staged once:
+// Y_{k-1} with a halo of 4 (136 rows x 24 columns) and Y_{k-2}, u0, dty0 with
+// a halo of 3 (22 columns), together with the tile's rows of the row table
+// (st_i, c2, c4) and columns of a column table ({P1, P5}).  The consumers then
+// compute, in shared memory and in place,
+//   stage k   on the tile plus 3 (over Y_{k-2}),
+//   stage k+1 on the tile plus 2 (over Y_{k-1}),
+//   stage k+2 on the tile plus 1 (over Y_k),
+//   stage k+3 on the tile,
+// and store Y_{k+2} and Y_{k+3} (the next pass's Y_{k-2}, Y_{k-1}) to HBM:
+// per cell and four stages 4 reads + 2 writes = 48 B instead of 4 x 40 B
+// (2 x 48 B on the two-stage path).  Every cell value is computed by the same
+// expressions, in the same order, as on the two-stage path, so the results
+// are bitwise the same.  The blocks next to a pole block also store the rows
+// of Y_k (one) and Y_{k+1} (two) at their edge, which the pole block's second
+// two-stage launch reads as its halo.
+//
+// Shared row r is theta row j0-4+r (r = 0..135; the stage-k pass also runs
+// the unused rows 0 and 135 so that every row pair starts on a 16-byte
+// boundary); shared column c of Y_{k-1} is phi column k0-4+c (c = 0..23) and
+// column c-1 of the other arrays holds phi column k0-4+c.  One producer warp
+// stages the tiles (five tensor copies and one bulk copy per tile, or one bulk
+// copy per column at the phi seams) and eight consumer warps compute; every
+// wait is bounded and reports through the error flag.
+#pragma once
+
+#include "sts_pair_ws.cuh"
+
+namespace hipft {
+
+constexpr int kQJ = 128;                 // theta rows per tile
+constexpr int kQK = 16;                  // phi columns per tile
+constexpr int kQR = kQJ + 8;             // shared rows per column (halo 4)
+constexpr int kQX = kQK + 8;             // shared columns of Y_{k-1} (halo 4)
+constexpr int kQI = kQK + 6;             // shared columns of Y_{k-2}, u0, dty0 (halo 3)
+constexpr int kQCons = 256;              // consumer threads
+constexpr int kQThreads = kQCons + 32;   // + the producer warp
+constexpr int kQX1 = 0;                              // Y_{k-1}
+constexpr int kQY2 = al16(kQX1 + kQX * kQR);         // Y_{k-2}
+constexpr int kQU = al16(kQY2 + kQI * kQR);          // u0
+constexpr int kQD = al16(kQU + kQI * kQR);           // dty0
+constexpr int kQRT = al16(kQD + kQI * kQR);          // rows: st_i, c2, c4, kQR each
+constexpr int kQCT = kQRT + 3 * kQR;                 // columns: {P1, P5} per shared column of Y_{k-1}
+constexpr int kQInfo = kQCT + 2 * kQX;               // tile record
+constexpr int kQBuf = al16(kQInfo + 8);
+constexpr size_t kQSmem = (size_t)kQBuf * sizeof(double) + 2 * sizeof(uint64_t);
+static_assert(kQX1 % 16 == 0 && kQY2 % 16 == 0 && kQU % 16 == 0 && kQD % 16 == 0 && kQRT % 16 == 0 &&
+                  kQCT % 2 == 0 && kQR % 2 == 0,
+              "tensor-copy destinations 128-byte aligned, row pairs 16-byte aligned");
+static_assert(2 * (kQSmem + 1024 + 256) <= 228 * 1024, "two CTAs per SM");
+
+// Tensor maps of the quad tiles: fields with boxes of kQR rows x kQX (x1) or
+// kQI (y2, u, d) columns, the row table with kQR x 3.
+struct QuadMaps {
+  CUtensorMap x1, y2, u, d, rt;
+  int on;
+};
+
+struct QuadArgs {
+  StageCoef c[4];        // stages k..k+3
+  int *err;              // set to 1 when a bounded wait gives up
+  int rb_lo, nbi;        // interior theta blocks rb_lo .. rb_lo+nbi-1
+  int nkt;               // phi tiles of kQK columns
+  int ntiles;            // nbi * nkt * realizations
+  int edge_lo, edge_hi;  // blocks whose first / last rows of Y_k, Y_{k+1} the pole blocks read
+  const double *col;     // column table: entry kk holds phi column kk-2 (mapped onto 2..npm-1)
+  int LC;                // column-table entries per realization
+};
+
+// Column table of the quad tiles: entry kk (0..LC-1) of realization i holds
+// {Dh dph_i(kw) dp_i(kw), Dh dph_i(kw+1) dp_i(kw)} for the interior column kw
+// that phi column kk-2 duplicates (load_diffusion_matrix's order, src/hipft.f90:
+// 6880-6920, as in k_pair_tables).
+__global__ void k_quad_coltab(Mesh m, const double *__restrict__ dfac, int LC, double *coltab) {
+  const int64_t ncol = (int64_t)m.nr * LC;
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < ncol; f += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(f / LC) + 1, kk = (int)(f % LC);
+    const int n2 = m.npm - 2;
+    const int kw = ((kk - 2 - 2) % n2 + n2) % n2 + 2;
+    const double Dr = dfac[i];
+    const double Dh = kHalf * (Dr + Dr);
+    coltab[2 * f] = Dh * m.dph_i[kw] * m.dp_i[kw];
+    coltab[2 * f + 1] = Dh * m.dph_i[kw + 1] * m.dp_i[kw];
+  }
+}
+
+__device__ __forceinline__ void quad_tile(const QuadArgs &qa, int t, int &kt, int &rb, int &i) {
+  kt = t % qa.nkt;
+  const int rest = t / qa.nkt;
+  rb = qa.rb_lo + rest % qa.nbi;
+  i = rest / qa.nbi + 1;
+}
+
+// One stage over a rectangle of row pairs p in [p0, p0+np) and shared columns
+// c in [c0, c0+nc) (columns of Y_{k-1}'s indexing).  S: the stencil input,
+// O2: the combine's second input, OUT: the output (all in shared memory; an
+// array with soff = 1 holds shared column c at index c-1).  store(r, c, y) is
+// called for every computed pair (r = 2p).
+template <typename Store>
+__device__ __forceinline__ void quad_stage(int tid, int p0, int np, int c0, int nc, const double *S, int soff,
+                                           const double *O2, int ooff, double *OUT, int woff, const double *U,
+                                           const double *D, const double *RT, const double2 *CT,
+                                           const StageCoef &sc, Store store) {
+  const int n = np * nc;
+  for (int e = tid; e < n; e += kQCons) {
+    const int r = 2 * (p0 + e % np), c = c0 + e / np;
+    const double *s = S + (c - soff) * kQR + r;
+    const double2 xl = *reinterpret_cast<const double2 *>(s - kQR);
+    const double2 xc = *reinterpret_cast<const double2 *>(s);
+    const double2 xr = *reinterpret_cast<const double2 *>(s + kQR);
+    const double up = s[-1], dn = s[2];
+    const double2 st2 = *reinterpret_cast<const double2 *>(RT + r);
+    const double2 c22 = *reinterpret_cast<const double2 *>(RT + kQR + r);
+    const double2 c42 = *reinterpret_cast<const double2 *>(RT + 2 * kQR + r);
+    const double2 o2 = *reinterpret_cast<const double2 *>(O2 + (c - ooff) * kQR + r);
+    const double2 u = *reinterpret_cast<const double2 *>(U + (c - 1) * kQR + r);
+    const double2 d = *reinterpret_cast<const double2 *>(D + (c - 1) * kQR + r);
+    const double2 y = pair_rows_step(xl, xc, xr, up, dn, st2, c22, c42, CT[c], false, false, 0.0, 0.0, o2, u, d, sc);
+    *reinterpret_cast<double2 *>(OUT + (c - woff) * kQR + r) = y;
+    store(r, c, y);
+  }
+}
+
+// Four RKG2 stages on the interior blocks (see the file comment).  Outputs:
+// out_k2 = Y_{k+2}, out_k3 = Y_{k+3} on the tiles, and the edge rows of
+// out_k = Y_k, out_k1 = Y_{k+1} on the blocks edge_lo / edge_hi.
+__global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const double *__restrict__ ykm1,
+                                                             const double *__restrict__ ykm2,
+                                                             const double *__restrict__ u0,
+                                                             const double *__restrict__ dty0, double *out_k,
+                                                             double *out_k1, double *out_k2, double *out_k3,
+                                                             QuadArgs qa, PairTables pt,
+                                                             const __grid_constant__ QuadMaps tm) {
+  extern __shared__ __align__(128) double qsm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(qsm + kQBuf);
+  uint64_t *empty = full + 1;
+  const int tid = threadIdx.x;
+  const int npm = m.npm;
+  const int64_t ld = m.ldt;
+  if (tid == 0) {
+    mbar_init(full, 1);
+    mbar_init(empty, kQCons);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (tid >= kQCons) {
+    // ------------------------------------------------------------ producer
+    const int lane = tid - kQCons;
+    const bool maps_ok = tm.on && (smem_addr(qsm) & 127u) == 0;
+    int n = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < qa.ntiles; t += gridDim.x, ++n) {
+      int kt, rb, i;
+      quad_tile(qa, t, kt, rb, i);
+      const int j0 = rb * kQJ + 1, k0 = kt * kQK + 2;
+      const int nk = min(kQK, npm - 1 - k0 + 1);
+      const int64_t pbase = (int64_t)(i - 1) * m.plane;
+      double *B = qsm;
+      // the single buffer is free once the consumers are done with the last tile
+      if (n >= 1 && !mbar_wait_bounded(empty, (uint32_t)((n - 1) & 1), 1u << 22)) {
+        ok = false;
+        break;
+      }
+      const bool boxed = maps_ok && nk == kQK && k0 - 4 >= 1 && k0 + kQK + 3 <= npm;
+      const uint32_t run = kQR * 8u;  // rows j0-4 .. j0+131, all inside 1..ntm for an interior block
+      if (lane == 0) {
+        int *Ii = reinterpret_cast<int *>(B + kQInfo);
+        Ii[0] = kt;
+        Ii[1] = rb;
+        Ii[2] = i;
+        Ii[3] = nk;
+        mbar_expect_tx(full, (uint32_t)((kQX + 3 * kQI) * kQR * 8 + 3 * kQR * 8 + kQX * 16));
+        if (boxed) {
+          tma_load_3d(B + kQX1, &tm.x1, j0 - 5, k0 - 5, i - 1, full);
+          tma_load_3d(B + kQY2, &tm.y2, j0 - 5, k0 - 4, i - 1, full);
+          tma_load_3d(B + kQU, &tm.u, j0 - 5, k0 - 4, i - 1, full);
+          tma_load_3d(B + kQD, &tm.d, j0 - 5, k0 - 4, i - 1, full);
+          tma_load_3d(B + kQRT, &tm.rt, rb * kQJ - 2, 0, i - 1, full);
+          bulk_load(B + kQCT, qa.col + ((int64_t)(i - 1) * qa.LC + (int64_t)kt * kQK) * 2, kQX * 16, full);
+        }
+      }
+      __syncwarp();
+      if (!boxed) {
+        // one bulk copy per column (phi seam tiles, or no tensor maps)
+        const int ncp = kQX + 3 * kQI + 4;
+        for (int q = lane; q < ncp; q += 32) {
+          const double *src;
+          double *dst;
+          uint32_t bytes = run;
+          if (q < kQX) {
+            const int kg = wrap_col(k0 - 4 + q, npm);
+            src = ykm1 + pbase + (int64_t)(kg - 1) * ld + (j0 - 5);
+            dst = B + kQX1 + q * kQR;
+          } else if (q < kQX + 3 * kQI) {
+            const int qq = q - kQX, a = qq / kQI, c = qq % kQI;
+            const int kg = wrap_col(k0 - 3 + c, npm);
+            src = (a == 0 ? ykm2 : (a == 1 ? u0 : dty0)) + pbase + (int64_t)(kg - 1) * ld + (j0 - 5);
+            dst = B + (a == 0 ? kQY2 : (a == 1 ? kQU : kQD)) + c * kQR;
+          } else if (q < kQX + 3 * kQI + 3) {
+            const int a = q - (kQX + 3 * kQI);
+            src = pt.row + ((int64_t)(i - 1) * 3 + a) * pt.LR + (int64_t)(rb * kQJ - 2);
+            dst = B + kQRT + a * kQR;
+          } else {
+            src = qa.col + ((int64_t)(i - 1) * qa.LC + (int64_t)kt * kQK) * 2;
+            dst = B + kQCT;
+            bytes = kQX * 16;
+          }
+          bulk_load(dst, src, bytes, full);
+        }
+      }
+    }
+    if (!ok && lane == 0) atomicExch(qa.err, 1);
+    // the last tile's copies land before this warp exits
+    if (n >= 1) mbar_wait_bounded(full, (uint32_t)((n - 1) & 1), 1u << 22);
+    return;
+  }
+
+  // -------------------------------------------------------------- consumers
+  const StageCoef s0 = qa.c[0], s1 = qa.c[1], s2 = qa.c[2], s3 = qa.c[3];
+  const int64_t seam = (int64_t)(npm - 2) * ld;
+  int n = 0;
+  for (int t = blockIdx.x; t < qa.ntiles; t += gridDim.x, ++n) {
+    const bool landed = mbar_wait_bounded(full, (uint32_t)(n & 1), 1u << 22);
+    if (cons_any(!landed)) {
+      if (tid == 0) atomicExch(qa.err, 1);
+      break;
+    }
+    double *B = qsm;
+    const int *Ii = reinterpret_cast<const int *>(B + kQInfo);
+    const int kt = Ii[0], rb = Ii[1], i = Ii[2], nk = Ii[3];
+    const int j0 = rb * kQJ + 1, k0 = kt * kQK + 2;
+    const int64_t pbase = (int64_t)(i - 1) * m.plane;
+    double *X = B + kQX1, *Y2 = B + kQY2;
+    const double *U = B + kQU, *D = B + kQD, *RT = B + kQRT;
+    const double2 *CT = reinterpret_cast<const double2 *>(B + kQCT);
+    const bool elo = (rb == qa.edge_lo), ehi = (rb == qa.edge_hi);
+    // a value of shared cell (r, c) to HBM (with its seam copy), for the
+    // tile's own columns c = 4 .. 3+nk
+    auto put = [&](double *g, int r, int c, double2 y) {
+      const int k = k0 - 4 + c;
+      double *q = g + pbase + (int64_t)(k - 1) * ld + (j0 - 5 + r);
+      *reinterpret_cast<double2 *>(q) = y;
+      if (k == 2) *reinterpret_cast<double2 *>(q + seam) = y;
+      if (k == npm - 1) *reinterpret_cast<double2 *>(q - seam) = y;
+    };
+    const int cend = 4 + nk;  // one past the tile's last shared column
+    // stage k on rows 0..135 (1..134 valid), columns 1..cend+2, over Y_{k-2}
+    quad_stage(tid, 0, kQR / 2, 1, nk + 6, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s0, [&](int r, int c, double2 y) {
+      // Y_k at the edge row a neighbouring pole block reads (rows j0 or j0+127)
+      if (c >= 4 && c < cend && ((elo && r == 4) || (ehi && r == 130))) {
+        const int k = k0 - 4 + c;
+        double *q = out_k + pbase + (int64_t)(k - 1) * ld + (j0 - 5 + r);
+        const int rr = (r == 4) ? 0 : 1;  // row j0 is the pair's first row, row j0+127 its second
+        const double v = rr ? y.y : y.x;
+        q[rr] = v;
+        if (k == 2) q[rr + seam] = v;
+        if (k == npm - 1) q[rr - seam] = v;
+      }
+    });
+    cons_sync();
+    // stage k+1 on rows 2..133, columns 2..cend+1, stencil Y_k, over Y_{k-1}
+    quad_stage(tid, 1, kQR / 2 - 2, 2, nk + 4, Y2, 1, X, 0, X, 0, U, D, RT, CT, s1, [&](int r, int c, double2 y) {
+      // Y_{k+1} at the two edge rows (j0, j0+1 or j0+126, j0+127)
+      if (c >= 4 && c < cend && ((elo && r == 4) || (ehi && r == 130))) put(out_k1, r, c, y);
+    });
+    cons_sync();
+    // stage k+2 on rows 2..133 (3..132 valid), columns 3..cend, stencil Y_{k+1}, over Y_k
+    quad_stage(tid, 1, kQR / 2 - 2, 3, nk + 2, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s2, [&](int r, int c, double2 y) {
+      if (c >= 4 && c < cend && r >= 4 && r <= 130) put(out_k2, r, c, y);
+    });
+    cons_sync();
+    // stage k+3 on the tile: rows 4..131, columns 4..cend-1, stencil Y_{k+2}, second input Y_{k+1}
+    {
+      const int np = kQJ / 2, nc = nk, ntot = np * nc;
+      for (int e = tid; e < ntot; e += kQCons) {
+        const int r = 4 + 2 * (e % np), c = 4 + e / np;
+        const double *s = Y2 + (c - 1) * kQR + r;
+        const double2 xl = *reinterpret_cast<const double2 *>(s - kQR);
+        const double2 xc = *reinterpret_cast<const double2 *>(s);
+        const double2 xr = *reinterpret_cast<const double2 *>(s + kQR);
+        const double up = s[-1], dn = s[2];
+        const double2 st2 = *reinterpret_cast<const double2 *>(RT + r);
+        const double2 c22 = *reinterpret_cast<const double2 *>(RT + kQR + r);
+        const double2 c42 = *reinterpret_cast<const double2 *>(RT + 2 * kQR + r);
+        const double2 o2 = *reinterpret_cast<const double2 *>(X + c * kQR + r);
+        const double2 u = *reinterpret_cast<const double2 *>(U + (c - 1) * kQR + r);
+        const double2 d = *reinterpret_cast<const double2 *>(D + (c - 1) * kQR + r);
+        const double2 y =
+            pair_rows_step(xl, xc, xr, up, dn, st2, c22, c42, CT[c], false, false, 0.0, 0.0, o2, u, d, s3);
+        put(out_k3, r, c, y);
+      }
+    }
+    cons_sync();               // all reads of the buffer are done
+    mbar_arrive(empty);        // the producer may refill it
+  }
+}
+
+}  // namespace hipft

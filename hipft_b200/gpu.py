@@ -326,6 +326,15 @@ class HipftGPU:
                     float(rigid_omega), int(attenuate), _p(v[6]))
         self._ck(self.L.hipft_gpu_set_flow(self.h, ctypes.byref(d)), "set_flow")
 
+    def set_flow_from_files(self, vt: np.ndarray, vp: np.ndarray, at_load: bool = True):
+        """The 2-D flow of HipFT's flow files (add_flow_from_files / load_flow_from_files,
+        src/hipft.f90:3525-3800), shared by all realizations, in m/s: vt (nt, npm1) and
+        vp (ntm, np) in C order (the files' Fortran (npm1, nt) and (np, ntm))."""
+        a = np.ascontiguousarray(vt, dtype=np.float64)
+        b = np.ascontiguousarray(vp, dtype=np.float64)
+        assert a.shape == (self.ntm + 1, self.npm1) and b.shape == (self.ntm, self.npm1 + 1), (a.shape, b.shape)
+        self._ck(self.L.hipft_gpu_set_flow_from_files(self.h, _p(a), _p(b), int(at_load)), "set_flow_from_files")
+
     def update_flow(self) -> bool:
         """update_flow (src/hipft.f90:3371); True when the flow changed."""
         u = ctypes.c_int(0)

@@ -41,6 +41,11 @@ CASES = {
     # widest path
     "rkg2_ntm384_np45": dict(res_nt=384, res_np=45, advance_diffusion=True, diffusion_coef_constants=[150.0, 900.0],
                              validation_run=1),
+    # five interior 128-row blocks between the pole blocks: the four-stage
+    # path (interior blocks) meets the two-stage path (pole blocks) at both
+    # block edges
+    "rkg2_ntm900_np70": dict(res_nt=900, res_np=70, advance_diffusion=True, diffusion_coef_constants=[200.0, 800.0],
+                             validation_run=1, time_end=3.0),
     "rkl2_fixed_sc": dict(advance_diffusion=True, diffusion_num_method=2, diffusion_subcycles=3,
                           diffusion_coef_constants=[250.0, 500.0], validation_run=1),
     "euler_fixed_sc": dict(res_nt=20, res_np=37, advance_diffusion=True, diffusion_num_method=1,

@@ -4,8 +4,8 @@ stage per launch, against the oracle.
 The library fixes its RKG2 kernel from the environment when asked
 (HIPFT_STS_PAIR=1: one CTA per tile, shape HIPFT_PAIR_TILE; =4: persistent
 warp-specialised CTAs with one theta row per consumer thread; =5: two rows
-per thread; =6: the same with the outputs leaving by bulk stores; =0: one
-stage per launch), so each variant runs the standalone driver in a fresh
+per thread; =6: the same with the outputs leaving by bulk stores; =7: four
+stages per pass on the interior theta blocks; =0: one stage per launch), so each variant runs the standalone driver in a fresh
 subprocess; final fields must match the oracle to FIELD_TOL.  The "tuned"
 variant lets the autotuner choose."""
 import os
@@ -26,9 +26,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "pair_64x16": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "64x16"},
             "pair_256x4": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "256x4"},
             "pair_ws": {"HIPFT_STS_PAIR": "4"}, "pair_ws_rowpairs": {"HIPFT_STS_PAIR": "5"},
-            "pair_ws_bulkst": {"HIPFT_STS_PAIR": "6"}, "single_v3": {"HIPFT_STS_PAIR": "0"}, "tuned": {}}
+            "pair_ws_bulkst": {"HIPFT_STS_PAIR": "6"}, "quad_ws": {"HIPFT_STS_PAIR": "7"},
+            "single_v3": {"HIPFT_STS_PAIR": "0"}, "tuned": {}}
 RUNS = ["diffuse_soccer", "rkg2_auto_ntm33", "rkg2_auto_ntm161", "rkg2_ntm129_np65", "rkg2_ntm130_np96",
-        "rkg2_ntm384_np45", "strang_dr_mf_diff"]
+        "rkg2_ntm384_np45", "rkg2_ntm900_np70", "strang_dr_mf_diff"]
 
 
 def _setup(name, tmp_path):
