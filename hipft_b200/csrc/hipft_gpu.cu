@@ -716,11 +716,13 @@ static int quad_setup(hipft_gpu *h) {
   LAUNCHED(h);
   h->q_rt_ok = encode_f64_3d(&h->q_rt_map, h->ptab.row, (uint64_t)h->ptab.LR, 3, (uint64_t)h->nr,
                              (uint64_t)h->ptab.LR * 8, (uint64_t)h->ptab.LR * 24, kQR, 3);
-  CK(h, cudaFuncSetAttribute(k_sts_quad_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
+  CK(h, cudaFuncSetAttribute(k_sts_quad_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
+  CK(h, cudaFuncSetAttribute(k_sts_quad_ws<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
   return HIPFT_OK;
 }
 
-// The pole blocks (every block outside rb_lo..rb_hi) for the two-stage launches
+// The pole blocks (every block outside rb_lo..rb_hi) of `nreal` realizations
+// for the two-stage launches of the four-stage path.
 static PairTables quad_pole_tables(const hipft_gpu *h, int nreal) {
   PairTables pt = h->ptab;
   pt.nsel = 0;
@@ -731,14 +733,18 @@ static PairTables quad_pole_tables(const hipft_gpu *h, int nreal) {
 }
 
 // Two-stage launch (k_sts_pair_ws, two rows per consumer) plus k_pair_poles
-// over the tiles of `pt`.
+// over the tiles of `pt`; rlist/rc (may be null): the realizations of a
+// ragged batch and their coefficients.  flip: the launch's output ring sums
+// become current (a launch that shares its input ring with a following one
+// leaves that to the last of them).
 static int ws_pair_launch(hipft_gpu *h, const PairTables &pt, int cps, const double *ykm1, const double *ykm2,
                           const double *u0, const double *dty0, double *out_k, double *out_k1, StageCoef ca,
-                          StageCoef cb, bool overlap_prev) {
+                          StageCoef cb, bool overlap_prev, const int *rlist = nullptr, int nreal = 0,
+                          const StageCoef *rc = nullptr, bool flip = true) {
   const int nkt = (h->npm - 2 + kWK - 1) / kWK;
   RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
   const int grid = std::min(pt.ntiles, cps * h->num_sms);
-  const PairArgs pa{ca, cb, h->d_err};
+  PairArgs pa{ca, cb, h->d_err, rlist, rc};
   const double *rin = h->d_ringbuf[h->ring_cur];
   const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
   cudaLaunchConfig_t cfg = {};
@@ -751,64 +757,82 @@ static int ws_pair_launch(hipft_gpu *h, const PairTables &pt, int cps, const dou
   attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
-                                      dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, pt, tmaps);
+  cudaError_t le = rlist ? cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true, false, true>, h->M, (const double *)h->DC.dfac,
+                                              ykm1, ykm2, u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s,
+                                              pa, ro, pt, tmaps)
+                         : cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2,
+                                              u0, dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, pt,
+                                              tmaps);
   if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
   LAUNCHED(h);
-  dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
+  dim3 pg((unsigned)(rlist ? nreal : h->nr), (unsigned)h->pole_nch);
   k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin, h->bc_diff_n,
                                                    h->bc_diff_s, pa, ro, h->pole);
   LAUNCHED(h);
-  h->ring_cur = 1 - h->ring_cur;
+  if (flip) h->ring_cur = 1 - h->ring_cur;
+  return HIPFT_OK;
+}
+
+// The four-stage launch over the interior blocks of all realizations, or of
+// the n realizations of rlist with coefficients rcA (stages k, k+1) and rcB
+// (k+2, k+3).  It reads nothing the pole blocks' first two-stage launch
+// writes, so it may start while that launch's pole kernel runs.
+static int quad_launch(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
+                       double *ok, double *ok1, double *ok2, double *ok3, const StageCoef c[4],
+                       const int *rlist = nullptr, int n = 0, const StageCoef *rcA = nullptr,
+                       const StageCoef *rcB = nullptr) {
+  QuadArgs qa{};
+  for (int q = 0; q < 4; ++q) qa.c[q] = c[q];
+  qa.err = h->d_err;
+  qa.rb_lo = h->q_rb_lo;
+  qa.nbi = h->q_rb_hi - h->q_rb_lo + 1;
+  qa.nkt = h->q_nkt;
+  qa.ntiles = qa.nbi * qa.nkt * (rlist ? n : h->nr);
+  qa.edge_lo = (h->q_rb_lo > 0) ? h->q_rb_lo : -1;
+  qa.edge_hi = (h->q_rb_hi < h->ptab.nb - 1) ? h->q_rb_hi : -1;
+  qa.col = h->d_qcol;
+  qa.LC = h->q_LC;
+  qa.rlist = rlist;
+  qa.rcA = rcA;
+  qa.rcB = rcB;
+  QuadMaps qm;
+  std::memset(&qm, 0, sizeof(qm));
+  if (ws_tmap_enabled() && h->q_rt_ok && field_map(h, ykm1, kQX, &qm.x1, kQR) && field_map(h, ykm2, kQI, &qm.y2, kQR) &&
+      field_map(h, u0, kQI, &qm.u, kQR) && field_map(h, dty0, kQI, &qm.d, kQR)) {
+    qm.rt = h->q_rt_map;
+    qm.on = 1;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)std::min(qa.ntiles, 2 * h->num_sms));
+  cfg.blockDim = dim3(kQThreads);
+  cfg.dynamicSmemBytes = kQSmem;
+  cfg.stream = h->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = ws_pdl() ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  PairTables pt = h->ptab;
+  cudaError_t le = rlist ? cudaLaunchKernelEx(&cfg, k_sts_quad_ws<true>, h->M, ykm1, ykm2, u0, dty0, ok, ok1, ok2,
+                                              ok3, qa, pt, qm)
+                         : cudaLaunchKernelEx(&cfg, k_sts_quad_ws<false>, h->M, ykm1, ykm2, u0, dty0, ok, ok1, ok2,
+                                              ok3, qa, pt, qm);
+  if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_quad_ws launch: %s", cudaGetErrorString(le));
+  LAUNCHED(h);
   return HIPFT_OK;
 }
 
 // Stages k..k+3: the pole blocks by two two-stage launches, the interior
-// blocks by one four-stage launch between them (it reads nothing the first
-// pole launch writes, so it may start while that launch's pole kernel runs).
-// Outputs ok..ok3 hold Y_k..Y_{k+3}; Y_k and Y_{k+1} only on the pole blocks
-// and the interior blocks' edge rows.
+// blocks by one four-stage launch between them.  Outputs ok..ok3 hold
+// Y_k..Y_{k+3}; Y_k and Y_{k+1} only on the pole blocks and the interior
+// blocks' edge rows.
 static int quad_pass(hipft_gpu *h, const double *ykm1, const double *ykm2, const double *u0, const double *dty0,
                      double *ok, double *ok1, double *ok2, double *ok3, const StageCoef c[4], bool overlap_prev) {
   const int cps = h->plan.ctas_per_sm;
   const PairTables pp = quad_pole_tables(h, h->nr);
   ProfScope ps(h, HIPFT_K_STS);
   TRY(ws_pair_launch(h, pp, cps, ykm1, ykm2, u0, dty0, ok, ok1, c[0], c[1], overlap_prev));
-  {
-    QuadArgs qa{};
-    for (int q = 0; q < 4; ++q) qa.c[q] = c[q];
-    qa.err = h->d_err;
-    qa.rb_lo = h->q_rb_lo;
-    qa.nbi = h->q_rb_hi - h->q_rb_lo + 1;
-    qa.nkt = h->q_nkt;
-    qa.ntiles = qa.nbi * qa.nkt * h->nr;
-    qa.edge_lo = (h->q_rb_lo > 0) ? h->q_rb_lo : -1;
-    qa.edge_hi = (h->q_rb_hi < h->ptab.nb - 1) ? h->q_rb_hi : -1;
-    qa.col = h->d_qcol;
-    qa.LC = h->q_LC;
-    QuadMaps qm;
-    std::memset(&qm, 0, sizeof(qm));
-    if (ws_tmap_enabled() && h->q_rt_ok && field_map(h, ykm1, kQX, &qm.x1, kQR) &&
-        field_map(h, ykm2, kQI, &qm.y2, kQR) && field_map(h, u0, kQI, &qm.u, kQR) &&
-        field_map(h, dty0, kQI, &qm.d, kQR)) {
-      qm.rt = h->q_rt_map;
-      qm.on = 1;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)std::min(qa.ntiles, 2 * h->num_sms));
-    cfg.blockDim = dim3(kQThreads);
-    cfg.dynamicSmemBytes = kQSmem;
-    cfg.stream = h->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = ws_pdl() ? 1 : 0;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    PairTables pt = h->ptab;
-    cudaError_t le = cudaLaunchKernelEx(&cfg, k_sts_quad_ws, h->M, ykm1, ykm2, u0, dty0, ok, ok1, ok2, ok3, qa, pt, qm);
-    if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_quad_ws launch: %s", cudaGetErrorString(le));
-    LAUNCHED(h);
-  }
+  TRY(quad_launch(h, ykm1, ykm2, u0, dty0, ok, ok1, ok2, ok3, c));
   TRY(ws_pair_launch(h, pp, cps, ok1, ok, u0, dty0, ok2, ok3, c[2], c[3], false));
   return HIPFT_OK;
 }
@@ -1902,6 +1926,7 @@ static int sts_pair_ragged(hipft_gpu *h, const double *ykm1, const double *ykm2,
 // buffer, which becomes the current field.
 static int ragged_super_step(hipft_gpu *h, std::vector<int> act, const std::vector<double> &dtl) {
   const int nr = h->nr, method = h->P.diffusion_num_method;
+  TRY(ensure_pair_plan(h));
   std::vector<StsTable> T(nr);
   std::vector<int64_t> s(nr, 0);
   int64_t smax = 0;
@@ -1963,9 +1988,47 @@ static int ragged_super_step(hipft_gpu *h, std::vector<int> act, const std::vect
   };
   std::vector<int> fin(nr, u0);  // buffer holding each realization's result
   const int64_t cells = (int64_t)h->ntm * (h->npm - 2);
-  for (int64_t q = 0; q < npairs; ++q) {
-    int n = 0;
+  const bool quad = h->plan.kind == PK_WS_QUAD && h->d_qcol;
+  for (int64_t q = 0; q < npairs;) {
+    int n = 0;   // realizations with pair q
     while (n < na && (s[act[n]] - 1) / 2 > q) ++n;
+    int nq = 0;  // realizations with pairs q and q+1: four stages in one pass
+    while (quad && nq < na && (s[act[nq]] - 1) / 2 >= q + 2) ++nq;
+    if (nq > 0) {
+      int ob[4], no = 0;
+      for (int b = 0; b < h->nbuf && no < 4; ++b)
+        if (b != u0 && b != idty && b != ykm1 && b != ykm2) ob[no++] = b;
+      const StageCoef *rcA = h->d_rcoef + (size_t)q * nr * 2, *rcB = h->d_rcoef + (size_t)(q + 1) * nr * 2;
+      const StageCoef none[4] = {};
+      const PairTables pp = quad_pole_tables(h, nq);
+      const int cps = h->plan.ctas_per_sm;
+      ProfScope ps(h, HIPFT_K_STS);
+      // stages k, k+1: the pole blocks of the four-stage realizations and, for
+      // the realizations whose last pair this is, every block
+      TRY(ws_pair_launch(h, pp, cps, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[ob[0]],
+                         h->buf[ob[1]], StageCoef{}, StageCoef{}, q > 0, h->d_rlist_dif, nq, rcA, n == nq));
+      if (n > nq) {
+        PairTables pt = h->ptab;
+        pt.ntiles = pt.nb * pt.nkt * (n - nq);
+        TRY(ws_pair_launch(h, pt, cps, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[ob[0]],
+                           h->buf[ob[1]], StageCoef{}, StageCoef{}, true, h->d_rlist_dif + nq, n - nq, rcA, true));
+      }
+      TRY(quad_launch(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[ob[0]], h->buf[ob[1]],
+                      h->buf[ob[2]], h->buf[ob[3]], none, h->d_rlist_dif, nq, rcA, rcB));
+      TRY(ws_pair_launch(h, pp, cps, h->buf[ob[1]], h->buf[ob[0]], h->buf[u0], h->buf[idty], h->buf[ob[2]],
+                         h->buf[ob[3]], StageCoef{}, StageCoef{}, false, h->d_rlist_dif, nq, rcB, true));
+      for (int e = 0; e < n; ++e) {
+        const int64_t P = (s[act[e]] - 1) / 2;
+        if (e >= nq && P == q + 1) fin[act[e]] = ob[1];
+        if (e < nq && P == q + 2) fin[act[e]] = ob[3];
+      }
+      ykm2 = ob[2];
+      ykm1 = ob[3];
+      h->rkg2_stages += 4;
+      h->rkg2_cell_stages += 4 * cells * nq + 2 * cells * (n - nq);
+      q += 2;
+      continue;
+    }
     const int bk = free_buf(-1), bk1 = free_buf(bk);
     TRY(sts_pair_ragged(h, h->buf[ykm1], h->buf[ykm2], h->buf[u0], h->buf[idty], h->buf[bk], h->buf[bk1], n,
                         h->d_rcoef + (size_t)q * nr * 2, q > 0));
@@ -1975,6 +2038,7 @@ static int ragged_super_step(hipft_gpu *h, std::vector<int> act, const std::vect
     ykm1 = bk1;
     h->rkg2_stages += 2;
     h->rkg2_cell_stages += 2 * cells * n;
+    q += 1;
   }
   // gather: realizations that finished earlier, and those not in this
   // super-step at all (still in u0), into the last pair's output

@@ -52,8 +52,9 @@ constexpr int kQU = al16(kQY2 + kQI * kQR);          // u0
 constexpr int kQD = al16(kQU + kQI * kQR);           // dty0
 constexpr int kQRT = al16(kQD + kQI * kQR);          // rows: st_i, c2, c4, kQR each
 constexpr int kQCT = kQRT + 3 * kQR;                 // columns: {P1, P5} per shared column of Y_{k-1}
-constexpr int kQInfo = kQCT + 2 * kQX;               // tile record
-constexpr int kQBuf = al16(kQInfo + 8);
+constexpr int kQInfo = kQCT + 2 * kQX;               // tile record: (kt, rb, i, nk)
+constexpr int kQInfoCoef = kQInfo + 4;               // ragged batches: the tile's four StageCoef (20 doubles)
+constexpr int kQBuf = al16(kQInfoCoef + 20);
 constexpr size_t kQSmem = (size_t)kQBuf * sizeof(double) + 2 * sizeof(uint64_t);
 static_assert(kQX1 % 16 == 0 && kQY2 % 16 == 0 && kQU % 16 == 0 && kQD % 16 == 0 && kQRT % 16 == 0 &&
                   kQCT % 2 == 0 && kQR % 2 == 0,
@@ -76,6 +77,11 @@ struct QuadArgs {
   int edge_lo, edge_hi;  // blocks whose first / last rows of Y_k, Y_{k+1} the pole blocks read
   const double *col;     // column table: entry kk holds phi column kk-2 (mapped onto 2..npm-1)
   int LC;                // column-table entries per realization
+  // ragged batches: realizations (0-based) of the launch, and per
+  // realization the coefficients of stages k, k+1 (rcA[2(i-1)], rcA[2(i-1)+1])
+  // and k+2, k+3 (rcB)
+  const int *rlist;
+  const StageCoef *rcA, *rcB;
 };
 
 // Column table of the quad tiles: entry kk (0..LC-1) of realization i holds
@@ -95,11 +101,11 @@ __global__ void k_quad_coltab(Mesh m, const double *__restrict__ dfac, int LC, d
   }
 }
 
-__device__ __forceinline__ void quad_tile(const QuadArgs &qa, int t, int &kt, int &rb, int &i) {
+__device__ __forceinline__ void quad_tile(const QuadArgs &qa, int t, int &kt, int &rb, int &i, bool ragged) {
   kt = t % qa.nkt;
   const int rest = t / qa.nkt;
   rb = qa.rb_lo + rest % qa.nbi;
-  i = rest / qa.nbi + 1;
+  i = (ragged ? qa.rlist[rest / qa.nbi] : rest / qa.nbi) + 1;
 }
 
 // One stage over a rectangle of row pairs p in [p0, p0+np) and shared columns
@@ -134,7 +140,10 @@ __device__ __forceinline__ void quad_stage(int tid, int p0, int np, int c0, int 
 
 // Four RKG2 stages on the interior blocks (see the file comment).  Outputs:
 // out_k2 = Y_{k+2}, out_k3 = Y_{k+3} on the tiles, and the edge rows of
-// out_k = Y_k, out_k1 = Y_{k+1} on the blocks edge_lo / edge_hi.
+// out_k = Y_k, out_k1 = Y_{k+1} on the blocks edge_lo / edge_hi.  RAGGED:
+// the tiles of the realizations in qa.rlist, each with its own coefficients,
+// which the producer copies into the tile record.
+template <bool RAGGED>
 __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const double *__restrict__ ykm1,
                                                              const double *__restrict__ ykm2,
                                                              const double *__restrict__ u0,
@@ -163,7 +172,14 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
     bool ok = true;
     for (int t = blockIdx.x; t < qa.ntiles; t += gridDim.x, ++n) {
       int kt, rb, i;
-      quad_tile(qa, t, kt, rb, i);
+      quad_tile(qa, t, kt, rb, i, RAGGED);
+      StageCoef rc[4] = {};
+      if (RAGGED && lane == 0) {
+        rc[0] = qa.rcA[2 * (i - 1)];
+        rc[1] = qa.rcA[2 * (i - 1) + 1];
+        rc[2] = qa.rcB[2 * (i - 1)];
+        rc[3] = qa.rcB[2 * (i - 1) + 1];
+      }
       const int j0 = rb * kQJ + 1, k0 = kt * kQK + 2;
       const int nk = min(kQK, npm - 1 - k0 + 1);
       const int64_t pbase = (int64_t)(i - 1) * m.plane;
@@ -181,6 +197,16 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
         Ii[1] = rb;
         Ii[2] = i;
         Ii[3] = nk;
+        if (RAGGED) {
+          double *C = B + kQInfoCoef;
+          for (int q = 0; q < 4; ++q) {
+            C[5 * q] = rc[q].a;
+            C[5 * q + 1] = rc[q].b;
+            C[5 * q + 2] = rc[q].c;
+            C[5 * q + 3] = rc[q].d;
+            C[5 * q + 4] = rc[q].e;
+          }
+        }
         mbar_expect_tx(full, (uint32_t)((kQX + 3 * kQI) * kQR * 8 + 3 * kQR * 8 + kQX * 16));
         if (boxed) {
           tma_load_3d(B + kQX1, &tm.x1, j0 - 5, k0 - 5, i - 1, full);
@@ -228,7 +254,7 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
   }
 
   // -------------------------------------------------------------- consumers
-  const StageCoef s0 = qa.c[0], s1 = qa.c[1], s2 = qa.c[2], s3 = qa.c[3];
+  StageCoef s0 = qa.c[0], s1 = qa.c[1], s2 = qa.c[2], s3 = qa.c[3];
   const int64_t seam = (int64_t)(npm - 2) * ld;
   int n = 0;
   for (int t = blockIdx.x; t < qa.ntiles; t += gridDim.x, ++n) {
@@ -240,6 +266,13 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
     double *B = qsm;
     const int *Ii = reinterpret_cast<const int *>(B + kQInfo);
     const int kt = Ii[0], rb = Ii[1], i = Ii[2], nk = Ii[3];
+    if (RAGGED) {
+      const double *C = B + kQInfoCoef;
+      s0 = StageCoef{C[0], C[1], C[2], C[3], C[4]};
+      s1 = StageCoef{C[5], C[6], C[7], C[8], C[9]};
+      s2 = StageCoef{C[10], C[11], C[12], C[13], C[14]};
+      s3 = StageCoef{C[15], C[16], C[17], C[18], C[19]};
+    }
     const int j0 = rb * kQJ + 1, k0 = kt * kQK + 2;
     const int64_t pbase = (int64_t)(i - 1) * m.plane;
     double *X = B + kQX1, *Y2 = B + kQY2;
