@@ -186,7 +186,6 @@ __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const dou
   }
 }
 
-// dacc[i] += scale * (sum of realization i's block partials), fixed order.
 // Reverse of the assimilation blend f += w (d - f) (src/hipft.f90:4116-4141):
 // on the core columns the blend is f_new = (1 - w) f + w d, so the folded
 // cotangent becomes (1 - w) fbar; the additive form f += w d leaves it
@@ -201,6 +200,7 @@ __global__ void k_adj_da(Mesh m, DAArgs a, double *fbar) {
   fbar[q] = (kOne - w) * fbar[q];
 }
 
+// dacc[i] += scale * (sum of realization i's block partials), fixed order.
 __global__ void k_adj_dsum(const double *__restrict__ dpart, int nblk, double scale, double *dacc) {
   __shared__ double sh[64];
   const int i = blockIdx.x;
