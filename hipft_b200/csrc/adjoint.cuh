@@ -186,6 +186,223 @@ __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const dou
   }
 }
 
+// ---------------------------------------------- two reverse stages per launch
+// Stages k and k-1 of the reverse RKG2 recurrence in one pass over the field:
+//   W_{k-1} = a1 W_k + b1 W_{k+1} + c1 A^T W_k,
+//   W_{k-2} = a2 W_{k-1} + b2 W_k + c2 A^T W_{k-1},
+//   ub += c01 W_k + c02 W_{k-1},  db += g1 W_k + g2 W_{k-1},
+//   dpart += ds1 <A^T W_k, Y_{k-1}> + ds2 <A^T W_{k-1}, Y_{k-2}> (block partials).
+// A tile of 32 theta rows x 8 core columns stages W_k with a halo of 2 in
+// shared memory, computes W_{k-1} on the tile plus a halo of 1 there, then
+// W_{k-2} on the tile: per cell and two stages W_k, W_{k+1}, Y_{k-1}, Y_{k-2},
+// ub, db are read and W_{k-1}, W_{k-2}, ub, db written (80 B) where two
+// one-stage launches move 128 B.  A^T at rows 1, 2, ntm-1, ntm needs the pole
+// sums of its input over every column, which for W_{k-1} exist only after the
+// whole grid; k_adj_pole2 finishes W_{k-2} (and its D partials) there and
+// leaves the pole sums of W_{k-2} for the next launch.  Tiles holding rows 1 /
+// ntm write per-tile partials of W_{k-1}'s pole sums.  Operation order per
+// cell as adj_diff_at_tab.
+struct AdjDiff2Coef {
+  double a1, b1, c1, c01, g1, ds1;  // stage k
+  double a2, b2, c2, c02, g2, ds2;  // stage k-1
+};
+
+constexpr int kA2J = 32, kA2K = 8;  // tile: theta rows x core columns (block 32 x 8 threads)
+
+// A^T w at (j, k) from a shared tile ws (column stride ld) at shared (r, c);
+// gn, gs: w's pole sums.  Same expression order as adj_diff_at_tab.
+__device__ __forceinline__ double adj_at_tile(const Mesh &m, const DiffCoef &dc, const PairTables &pt, int i, int j,
+                                              int k, int kp, int km, const double *ws, int ld, int r, int c,
+                                              double gn, double gs, double bcn, double bcs) {
+  const int ntm = m.ntm;
+  const double *R = pt.row + (int64_t)(i - 1) * 3 * pt.LR;
+  const double2 *P = reinterpret_cast<const double2 *>(pt.col) + (int64_t)(i - 1) * pt.LC;
+  auto W = [&](int dr, int dcl) { return ws[(c + dcl) * ld + (r + dr)]; };
+  double res = 0.0;
+  if (j >= 2 && j <= ntm - 1) {
+    const double sj = R[j + 1], c2 = R[pt.LR + j + 1], c4 = R[2 * pt.LR + j + 1];
+    const double2 Pk = P[k];
+    const double c1 = Pk.x * sj * sj, c5 = Pk.y * sj * sj;
+    const double c3 = -(c1 + c2 + c4 + c5);
+    res += c3 * W(0, 0);
+    res += (P[kp].x * sj * sj) * W(0, 1);
+    res += (P[km].y * sj * sj) * W(0, -1);
+    if (j + 1 <= ntm - 1) res += R[pt.LR + j + 2] * W(1, 0);
+    if (j - 1 >= 2) res += R[2 * pt.LR + j] * W(-1, 0);
+    if (j == 2) res += (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
+    if (j == ntm - 1) res += (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
+  } else if (j == 1) {
+    res += R[pt.LR + 3] * W(1, 0);
+    res -= (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
+  } else {
+    res += R[2 * pt.LR + ntm] * W(-1, 0);
+    res -= (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
+  }
+  return res;
+}
+
+__global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const double *__restrict__ w,
+                                                   const double *__restrict__ wp, const double *__restrict__ y1,
+                                                   const double *__restrict__ y2, double *out1, double *out2,
+                                                   double *ub, double *db, const double *__restrict__ gin, int npin,
+                                                   double *__restrict__ gpart, double bcn, double bcs,
+                                                   AdjDiff2Coef ac, double *__restrict__ dpart, PairTables pt) {
+  constexpr int LW = kA2J + 4, LM = kA2J + 2;
+  __shared__ double sw[(kA2K + 4) * LW];  // W_k, halo 2: sw(r, c) = row j0-2+r, core column k0-2+c
+  __shared__ double sm[(kA2K + 2) * LM];  // W_{k-1}, halo 1: sm(r, c) = row j0-1+r, core column k0-1+c
+  __shared__ double sh[64];
+  __shared__ double s_g[2];
+  __shared__ double s_n[kA2K], s_s[kA2K];
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * kA2J;
+  const int j0 = blockIdx.x * kA2J + 1, k0 = blockIdx.y * kA2K + 2;
+  const int i = blockIdx.z + 1;
+  const int ntm = m.ntm, npm = m.npm;
+  // pole sums of W_k, summed in order by every block (a fixed tree)
+  if (ty == 0) {
+    double a = 0.0, b = 0.0;
+    const double *g = gin + (int64_t)(i - 1) * npin * 2;
+    for (int q = tx; q < npin; q += 32) {
+      a = a + g[2 * q];
+      b = b + g[2 * q + 1];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (tx == 0) {
+      s_g[0] = a;
+      s_g[1] = b;
+    }
+  }
+  for (int e = tid; e < (kA2K + 4) * LW; e += 256) {
+    const int r = e % LW, c = e / LW;
+    const int j = j0 - 2 + r, k = core_wrap(m, k0 - 2 + c);
+    sw[e] = (j >= 1 && j <= ntm) ? w[fidx(m, j, k, i)] : 0.0;
+  }
+  __syncthreads();
+  const double gn = s_g[0], gs = s_g[1];
+  double dsum = 0.0;
+  // stage k on the tile plus a halo of 1: W_{k-1} into shared memory
+  for (int e = tid; e < (kA2K + 2) * LM; e += 256) {
+    const int r = e % LM, c = e / LM;
+    const int j = j0 - 1 + r, k = core_wrap(m, k0 - 1 + c);
+    double o = 0.0;
+    if (j >= 1 && j <= ntm) {
+      const int kp = core_wrap(m, k + 1), km = core_wrap(m, k - 1);
+      const double aw = adj_at_tile(m, dc, pt, i, j, k, kp, km, sw, LW, r + 1, c + 1, gn, gs, bcn, bcs);
+      const int64_t q = fidx(m, j, k, i);
+      const double wq = sw[(c + 1) * LW + r + 1];
+      o = ac.a1 * wq + ac.c1 * aw;
+      if (wp) o += ac.b1 * wp[q];
+      const bool own = (r >= 1 && r <= kA2J && c >= 1 && c <= kA2K && k0 - 1 + c <= npm - 1);
+      if (own) {
+        out1[q] = o;
+        if (y1) dsum += ac.ds1 * (aw * y1[q]);
+      }
+    }
+    sm[e] = o;
+  }
+  __syncthreads();
+  // stage k-1 on the tile, except the rows that need W_{k-1}'s pole sums
+  const int j = j0 + tx, k = k0 + ty;
+  double wm = 0.0;
+  const bool active = (j <= ntm && k <= npm - 1);
+  if (active) {
+    const int64_t q = fidx(m, j, k, i);
+    const double wk = sw[(ty + 2) * LW + tx + 2];
+    wm = sm[(ty + 1) * LM + tx + 1];
+    if (ub) ub[q] = ub[q] + ac.c01 * wk + ac.c02 * wm;
+    if (db) db[q] = db[q] + ac.g1 * wk + ac.g2 * wm;
+    if (j >= 3 && j <= ntm - 2) {
+      const int kp = core_wrap(m, k + 1), km = core_wrap(m, k - 1);
+      const double aw = adj_at_tile(m, dc, pt, i, j, k, kp, km, sm, LM, tx + 1, ty + 1, 0.0, 0.0, bcn, bcs);
+      out2[q] = ac.a2 * wm + ac.b2 * wk + ac.c2 * aw;
+      if (y2) dsum += ac.ds2 * (aw * y2[q]);
+    }
+  }
+  // per-tile partials of W_{k-1}'s pole sums (fixed order over the tile's columns)
+  const bool has_n = (j0 == 1), has_s = (j0 <= ntm && j0 + kA2J - 1 >= ntm);
+  if (has_n || has_s) {
+    if (tx == 0) s_n[ty] = active ? wm : 0.0;
+    if (j == ntm) s_s[ty] = active ? wm : 0.0;
+    __syncthreads();
+    if (tid == 0) {
+      double a = 0.0, b = 0.0;
+      for (int t = 0; t < kA2K; ++t) {
+        a = a + s_n[t];
+        b = b + s_s[t];
+      }
+      double *go = gpart + ((int64_t)(i - 1) * gridDim.y + blockIdx.y) * 2;
+      if (has_n) go[0] = a;
+      if (has_s) go[1] = b;
+    }
+  }
+  if (dpart) {
+    double z = 0.0;
+    block_sum2(dsum, z, sh);
+    if (tid == 0) dpart[((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] += dsum;
+  }
+}
+
+// Stage k-1 at rows 1, 2, ntm-1, ntm (after k_adj_diff2), one block per
+// realization: W_{k-1}'s pole sums from the tiles' partials (fixed order),
+// W_{k-2} = a2 W_{k-1} + b2 W_k + c2 A^T W_{k-1} there, the D partials of
+// those rows (added to the realization's first block slot), and the pole sums
+// of W_{k-2} for the next launch (gout[(i-1)][0..1], one partial).
+__global__ void __launch_bounds__(256) k_adj_pole2(Mesh m, DiffCoef dc, const double *__restrict__ w,
+                                                   const double *__restrict__ wm1, const double *__restrict__ y2,
+                                                   double *out2, const double *__restrict__ gpart, int npart,
+                                                   double *__restrict__ gout, double bcn, double bcs,
+                                                   AdjDiff2Coef ac, double *__restrict__ dpart, int dpart_per_r,
+                                                   PairTables pt) {
+  __shared__ double sh[64];
+  __shared__ double s_g[2];
+  const int i = blockIdx.x + 1, tid = threadIdx.x, ntm = m.ntm;
+  if (tid < 32) {
+    double a = 0.0, b = 0.0;
+    const double *g = gpart + (int64_t)(i - 1) * npart * 2;
+    for (int q = tid; q < npart; q += 32) {
+      a = a + g[2 * q];
+      b = b + g[2 * q + 1];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (tid == 0) {
+      s_g[0] = a;
+      s_g[1] = b;
+    }
+  }
+  __syncthreads();
+  const double gn = s_g[0], gs = s_g[1];
+  double dsum = 0.0, pn = 0.0, ps = 0.0;
+  for (int k = 2 + tid; k <= m.npm - 1; k += blockDim.x) {
+    for (int q = 0; q < 4; ++q) {
+      const int j = (q == 0) ? 1 : ((q == 1) ? 2 : ((q == 2) ? ntm - 1 : ntm));
+      const double aw = adj_diff_at_tab(m, dc, pt, wm1, j, k, i, gn, gs, bcn, bcs);
+      const int64_t x = fidx(m, j, k, i);
+      const double v = ac.a2 * wm1[x] + ac.b2 * w[x] + ac.c2 * aw;
+      out2[x] = v;
+      if (y2) dsum += ac.ds2 * (aw * y2[x]);
+      if (j == 1) pn = pn + v;
+      if (j == ntm) ps = ps + v;
+    }
+  }
+  block_sum2(pn, ps, sh);
+  if (tid == 0) {
+    gout[2 * (i - 1)] = pn;
+    gout[2 * (i - 1) + 1] = ps;
+  }
+  if (dpart) {
+    double z = 0.0;
+    block_sum2(dsum, z, sh);
+    if (tid == 0) dpart[(int64_t)(i - 1) * dpart_per_r] += dsum;
+  }
+}
+
 // Reverse of the assimilation blend f += w (d - f) (src/hipft.f90:4116-4141):
 // on the core columns the blend is f_new = (1 - w) f + w d, so the folded
 // cotangent becomes (1 - w) fbar; the additive form f += w d leaves it

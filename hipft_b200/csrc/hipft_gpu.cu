@@ -3177,6 +3177,16 @@ static int adj_block_recompute(hipft_gpu *h, const AdjSub &S, size_t b, std::vec
   return HIPFT_OK;
 }
 
+// HIPFT_ADJ_PAIR=0 runs the reverse RKG2 stages one per launch (A/B timing).
+static bool adj_pairs_enabled() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_ADJ_PAIR");
+    v = (e && std::atoi(e) == 0) ? 0 : 1;
+  }
+  return v == 1;
+}
+
 static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc) {
   const dim3 blk(32, 8), grd = stage_grid(h, 32, 8);
   const double dtl = S.dtl;
@@ -3214,7 +3224,35 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   };
   TRY(pole_sums(W));
   double *Wk = W, *Wk1 = nullptr;
-  for (int64_t k = S.s; k >= 2; --k) {
+  int64_t k = S.s;
+  // two reverse stages per launch (k_adj_diff2 + k_adj_pole2) while both of
+  // their stage inputs Y_{k-1}, Y_{k-2} lie in one stage-checkpoint block
+  while (adj_pairs_enabled() && k >= 3 && (S.q == 0 || (k - 2) / S.q == (k - 3) / S.q)) {
+    if (S.q > 0 && (k - 3) / S.q != curb) {
+      curb = (k - 3) / S.q;
+      TRY(adj_block_recompute(h, S, (size_t)curb, Yr));
+    }
+    double *Wm1 = adj_free(h, {Wk, Wk1, ub, db});
+    double *Wm2 = adj_free(h, {Wk, Wk1, ub, db, Wm1});
+    const double u1 = S.uj[k], v1 = S.vj[k], u2 = S.uj[k - 1], v2 = S.vj[k - 1];
+    const double nu1 = (k < S.s) ? S.vj[k + 1] : 0.0;
+    const AdjDiff2Coef ac{u1, nu1, S.ubj[k] * dtl, 1.0 - u1 - v1, S.gj[k], S.ubj[k] * dtl,
+                          u2, v1, S.ubj[k - 1] * dtl, 1.0 - u2 - v2, S.gj[k - 1], S.ubj[k - 1] * dtl};
+    double *gpart = h->d_gpart[pp];
+    k_adj_diff2<<<grd, blk, 0, h->stream>>>(h->M, h->DC, Wk, Wk1, Yt(k - 1), Yt(k - 2), Wm1, Wm2, ub, db, gin, npin,
+                                            gpart, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpart, h->ptab);
+    LAUNCHED(h);
+    k_adj_pole2<<<h->nr, 256, 0, h->stream>>>(h->M, h->DC, Wk, Wm1, Yt(k - 2), Wm2, gpart, (int)grd.y, h->d_gring,
+                                              h->bc_diff_n, h->bc_diff_s, ac, h->d_dpart, h->dpart_per_r, h->ptab);
+    LAUNCHED(h);
+    gin = h->d_gring;
+    npin = 1;
+    pp ^= 1;
+    Wk1 = Wm1;
+    Wk = Wm2;
+    k -= 2;
+  }
+  for (; k >= 2; --k) {
     if (S.q > 0 && (k - 2) / S.q != curb) {
       curb = (k - 2) / S.q;  // the block holding Y_{k-1}
       TRY(adj_block_recompute(h, S, (size_t)curb, Yr));
