@@ -8,9 +8,12 @@ v0 U(10, 20) m/s and differential rotation B, C x U(0.9, 1.1) (seed 1);
 WENO3-CS(h) + SSPRK(4,3) advection Strang-split with RKG2 super-time-stepped
 diffusion (automatic PTL subcycling), assimilation of a synthetic observed
 map every 24 model hours (mu^4 weights, mu > 0.1), diagnostics every step.
-A step is one flux-transport time step at the CFL-limited dt over all
-realizations.  Unit of work: one unique grid point of one realization
-advanced through one stage (one RKG2 stage or one SSPRK stage).
+The configuration is a batch of ragged realizations, so by default every
+realization keeps its own schedule (Euler limit, PTL subcycles, RKG2 stage
+counts; `--schedule shared` runs the reference's one schedule for all).
+A step is one flux-transport time step at the CFL-limited dt of the batch.
+Unit of work: one unique grid point of one realization advanced through one
+stage (one RKG2 stage or one SSPRK stage).
 
 Timing: W untimed warm-up steps, then K steps between CUDA events on the
 library's stream (inputs resident in HBM; each field is 1.07 GB, far above
@@ -20,13 +23,21 @@ device->host after every step.  Multi-GPU: realizations are split across
 ranks (block split, low ranks take the remainder) and every rank advances its
 own share independently -- weak scaling, no data-path collective.
 
-At N = 1 the line also carries "plain": the same metric for the plain
-configuration (one realization, 1024 x 2048, fixed physics, no assimilation),
-timed step by step with an L2 flush before each step (its fields fit in L2).
+At N = 1 the line also carries:
+  "batched_vs_plain": realization-steps/s of the ragged batch, of one batch
+      on the shared schedule, and of one handle per realization run one
+      after another, all at the batch's dt;
+  "plain": the same metric for the plain configuration (one realization,
+      1024 x 2048, fixed physics, no assimilation), timed step by step with
+      an L2 flush before each step (its fields fit in L2);
+  "adjoint": gradient / forward cost on the adjoint configuration;
+  "cpu_baseline": the CPU oracle's timing build on several realizations.
+`--c5` adds the 16-realization 2048 x 4096 forward leg.
 
 `--impl reference` times the CPU oracle (the restatement of the reference's
-solver in oracle/, all host threads) on a bounded sample of the same
-workload: one realization, one flux-transport step per bench step.
+solver in oracle/, its timing build, all host threads) on a bounded sample
+of the same workload: two realizations, one flux-transport step per bench
+step.
 """
 from __future__ import annotations
 
