@@ -427,6 +427,7 @@ def run_gpu(args, wl, name):
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "share_of_step": sts_ms / ms_prof if ms_prof > 0 else None,
                      "timing": "per-kernel CUDA events in a second pass of the same steps",
+                     "kernels_over_step": ((sts_ms + adv_ms + ring_ms + oth_ms) / ms_prof) if ms_prof > 0 else None,
                      "other_kernels_ms": {"advection_stage": adv_ms, "ring_sums": ring_ms, "other": oth_ms},
                      "other_kernels_launches": {"advection_stage": adv_n, "ring_sums": ring_n, "other": oth_n}},
         "e2e": {"value": e2e_cells / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
