@@ -30,10 +30,10 @@ P1 = [22.0, 30.0, 12.0, 40.0]
 P2 = [-262.0, -300.0, -200.0, -340.0]
 
 
-def _grid():
+def _grid(ntm=NTM, npm1=NPM1):
     from hipft_b200 import synthetic as S
-    t = S.refined_theta(NTM)
-    p = S.uniform_phi(NPM1)
+    t = S.refined_theta(ntm)
+    p = S.uniform_phi(npm1)
     return t, p, R.smooth_map(t, p, 17)
 
 
@@ -149,3 +149,51 @@ def test_ragged_rejects_unsupported_methods():
         with pytest.raises(gpu.HipftError) as e:
             g.set_ragged(True)
         assert e.value.code == gpu.HIPFT_EINVAL
+
+
+_CHILD = r"""
+import sys, numpy as np
+sys.path.insert(0, %(root)r); sys.path.insert(0, %(tests)r)
+import test_gpu_ragged as T
+t, p, br = T._grid(%(ntm)d, %(npm1)d)
+g = T._handle(t, p, %(nr)d)
+g.load_initial_map(br[None]); g.update_flow(); g.set_ragged(True)
+dt = g.flow_dtmax()
+seq, tend = T._dt_sequence(dt, %(nsteps)d)
+for d in seq:
+    g.flux_transport_step(d)
+sched = g.ragged_schedule()
+np.savez(%(out)r, f=g.get_field(), s=sched["sts_s"], c=sched["subcycles"], dt=dt, tend=tend, desc=g.describe())
+g.close()
+"""
+
+
+@pytest.mark.parametrize("kind", ["7", "5"])
+def test_ragged_four_stage_path(tmp_path, kind):
+    """A grid with interior theta blocks (ntm = 300), so that ragged
+    super-steps take four-stage passes for the realizations with two stage
+    pairs left and two-stage launches for the rest (HIPFT_STS_PAIR=7), and
+    the same with two-stage launches only (=5): every realization against the
+    oracle run of that realization alone."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = str(tmp_path / "r.npz")
+    nr, nsteps, ntm, npm1 = 4, 2, 300, 65
+    code = _CHILD % dict(root=root, tests=os.path.join(root, "tests"), ntm=ntm, npm1=npm1, nr=nr, nsteps=nsteps,
+                         out=out)
+    env = {k: v for k, v in os.environ.items() if k not in ("HIPFT_STS_PAIR", "HIPFT_TUNE")}
+    env["HIPFT_STS_PAIR"] = kind
+    res = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    z = np.load(out)
+    if kind == "7":
+        assert "ws-quad" in str(z["desc"]), str(z["desc"])
+    t, p, br = _grid(ntm, npm1)
+    assert len(set(z["s"].tolist())) > 1
+    for i in range(nr):
+        r = _oracle_alone(i, t, p, br, float(z["dt"]), float(z["tend"]))
+        err = np.abs(z["f"][i] - r["f"][0]).max() / np.abs(r["f"][0]).max()
+        assert err <= FIELD_TOL, f"realization {i}: field rel max-norm {err:.3e}"
+        assert int(r["num"][-1, 0, 6]) == z["s"][i]
