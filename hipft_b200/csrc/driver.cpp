@@ -350,6 +350,9 @@ struct Run {
   bool output_current_map = false;
   double dt_euler = 0.0;
   int64_t niters = 0, subcycles = 0;
+  // ragged batches: each realization's own Euler limit, stage count and subcycles
+  std::vector<double> r_dt_euler, r_dtmax_flow;
+  std::vector<int64_t> r_niters, r_subcycles, r_substeps;
   // DA
   DAList da;
   bool da_active = false;
@@ -397,9 +400,12 @@ struct Run {
         if (fs) std::fclose(fs);
         return HIPFT_EIO;
       }
-      std::string ln = fmt_i(ntime, 10) + " " + fmt_e(time) + " " + fmt_e(dtime_global) + " " + fmt_e(dtmax_flow) +
-                       " " + fmt_e(dtime_advection_used) + " " + fmt_e(dt_euler) + " " + fmt_i((long)niters, 15) +
-                       " " + fmt_i((long)subcycles, 15) + "\n";
+      const bool rg = nl.ragged_realizations && !r_dt_euler.empty();
+      const double dfl = (rg && !r_dtmax_flow.empty()) ? r_dtmax_flow[i - 1] : dtmax_flow;
+      std::string ln = fmt_i(ntime, 10) + " " + fmt_e(time) + " " + fmt_e(dtime_global) + " " + fmt_e(dfl) +
+                       " " + fmt_e(dtime_advection_used) + " " + fmt_e(rg ? r_dt_euler[i - 1] : dt_euler) + " " +
+                       fmt_i((long)(rg ? r_niters[i - 1] : niters), 15) + " " +
+                       fmt_i((long)(rg ? r_subcycles[i - 1] : subcycles), 15) + "\n";
       std::fputs(ln.c_str(), fn);
       std::string ls = fmt_i(ntime, 10) + " " + fmt_e(time) + " ";
       const double *v = &hist[(size_t)(i - 1) * 14];
@@ -651,9 +657,12 @@ struct Run {
       time_step_changed = true;
       if (nl.advance_flow) {
         dtmax_flow = DBL_MAX;
+        if (nl.ragged_realizations) r_dtmax_flow.assign(nr, DBL_MAX);
         if (timestep_flow_needs_updating) {
           int rc = hipft_gpu_flow_dtmax(h, &dtmax_flow);
           if (rc) return rc;
+          // each realization's own limit, for its history (the step takes the smallest)
+          if (nl.ragged_realizations && (rc = hipft_gpu_flow_dtmax_each(h, r_dtmax_flow.data()))) return rc;
           timestep_flow_needs_updating = false;
         }
         if (dtmax_flow < dtime_global) dtime_global = dtmax_flow;
@@ -885,6 +894,19 @@ struct Run {
     }
     rc = hipft_gpu_load_initial_map(h, f_local.data(), nl.initial_map_flux_balance, nl.initial_map_mult_fac);
     if (rc) return rc;
+    if (nl.ragged_realizations) {
+      rc = hipft_gpu_set_ragged(h, 1);
+      if (rc) {
+        err = "ragged_realizations: the method switches do not allow a ragged batch";
+        return rc;
+      }
+      r_dt_euler.assign(nr, 0.0);
+      r_niters.assign(nr, 0);
+      r_subcycles.assign(nr, nl.diffusion_subcycles);
+      r_substeps.assign(nr, 1);
+      rc = hipft_gpu_ragged_schedule(h, nullptr, nullptr, nullptr, r_dt_euler.data());
+      if (rc) return rc;
+    }
     rc = write_map(nl.output_map_root_filename + "_initial.h5");  // src/hipft.f90:2185
     if (rc) return rc;
     if (nl.validation_run == 1) rc = hipft_gpu_set_validation(h, 1, fval_u0.data(), 0, 0, 0, nl.time_start);
@@ -1027,6 +1049,10 @@ struct Run {
       if (nl.advance_diffusion) {
         niters = di.sts_s;
         subcycles = di.subcycles;
+        if (nl.ragged_realizations) {
+          rc = hipft_gpu_ragged_schedule(h, r_niters.data(), r_subcycles.data(), r_substeps.data(), r_dt_euler.data());
+          if (rc) return rc;
+        }
       }
       time = time + dtime_global;
       rc = apply_data_assimilation();

@@ -240,6 +240,7 @@ bool parse_namelist(const std::string &text, Namelist &nl, std::string &err) {
       {"output_map_flux_balance", &nl.output_map_flux_balance}, {"output_map_2d", &nl.output_map_2d},
       {"output_single_precision", &nl.output_single_precision},
       {"strang_splitting", &nl.strang_splitting}, {"advance_flow", &nl.advance_flow},
+      {"ragged_realizations", &nl.ragged_realizations},
       {"flow_attenuate", &nl.flow_attenuate}, {"use_flow_from_files", &nl.use_flow_from_files},
       {"advance_diffusion", &nl.advance_diffusion}, {"diffusion_coef_grid", &nl.diffusion_coef_grid},
       {"advance_source", &nl.advance_source}, {"assimilate_data", &nl.assimilate_data},

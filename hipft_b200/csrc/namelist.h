@@ -32,6 +32,9 @@ struct Namelist {
   double time_start = 0.0, time_end = 1.0;
   double dt_min = 1.0e-15, dt_max = 1.7976931348623157e308;
   bool strang_splitting = false;
+  // not a reference key: every realization keeps its own diffusion schedule
+  // (hipft_gpu_set_ragged); the histories then report each one's own
+  bool ragged_realizations = false;
   double pole_flux_lat_limit = 30.0;
   bool advance_flow = false;
   double flow_vp_rigid_omega = 0.0, flow_rigid_omega = 0.0, flow_vt_const = 0.0;

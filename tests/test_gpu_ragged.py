@@ -197,3 +197,40 @@ def test_ragged_four_stage_path(tmp_path, kind):
         err = np.abs(z["f"][i] - r["f"][0]).max() / np.abs(r["f"][0]).max()
         assert err <= FIELD_TOL, f"realization {i}: field rel max-norm {err:.3e}"
         assert int(r["num"][-1, 0, 6]) == z["s"][i]
+
+
+def test_driver_ragged_namelist(tmp_path):
+    """The standalone driver with ragged_realizations = .true.: each
+    realization's final field and its history rows, including its own Euler
+    limit, stage count and subcycle columns, against the oracle run of that
+    realization alone (dt_max below every realization's CFL limit, so the
+    step sequence is the same)."""
+    import cases
+    import hipft_b200 as H
+    import test_gpu_features as F
+    Ds, p1s, p2s = [80.0, 300.0, 900.0], [20.0, 30.0, 12.0], [-262.0, -300.0, -200.0]
+    base = dict(F.BASE, advance_flow=True, flow_dr_model=1, flow_mf_model=1, advance_diffusion=True,
+                strang_splitting=True, validation_run=1, time_end=24.0, dt_max=6.0)
+    d = dict(base, n_realizations=3, diffusion_coef_constants=Ds, flow_mf_coef_p1_values=p1s,
+             flow_dr_coef_p2_values=p2s, ragged_realizations=True)
+    text = F._namelist(d)
+    (tmp_path / "hipft.in").write_text(text)
+    prm = O.process_parameters(O.parse_namelist(text))
+    shape = (3, prm["res_np"] + 1, prm["res_nt"])
+    f = H.run_field(str(tmp_path / "hipft.in"), str(tmp_path), shape)
+    sol, num = cases.read_run_histories(str(tmp_path), 3)
+    assert len(set(num[:, -1, 6].tolist())) > 1, "the realizations should run different stage counts"
+    for i in range(3):
+        di = dict(base, n_realizations=1, diffusion_coef_constants=[Ds[i]], flow_mf_coef_p1_values=[p1s[i]],
+                  flow_dr_coef_p2_values=[p2s[i]])
+        r = O.run(O.process_parameters(O.parse_namelist(F._namelist(di))))
+        err = np.abs(f[i] - r["f"][0]).max() / np.abs(r["f"][0]).max()
+        assert err <= FIELD_TOL, f"realization {i}: field rel max-norm {err:.3e}"
+        e = cases.col_errors(sol[i], r["sol"][:, 0, :])
+        bad = {cases.COLS[c - 2]: float(e[c]) for c in range(2, 16)
+               if e[c] > (1e-10 if c < 15 else max(1e-10, cases.VALERR_TOL))}
+        assert not bad, f"realization {i}: {bad}"
+        o = r["num"][:, 0, :]
+        rel = np.abs(num[i][:, :6] - o[:, :6]) / np.maximum(np.abs(o[:, :6]), 1e-300)
+        assert rel.max() <= 1e-10, f"realization {i} num columns: {rel.max(0)}"
+        assert np.array_equal(num[i][:, 6:], o[:, 6:]), f"realization {i}: stage/cycle counts differ"
