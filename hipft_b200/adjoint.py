@@ -307,9 +307,12 @@ class MisfitAdjoint:
         vp_bar[:, 1:] = gln_p + glp_p
         ap_bar = torch.zeros((self.nr, ntm + 1), dtype=torch.float64)
         ap_bar[:, 1:] = gln_p - glp_p
-        coef = {k: torch.tensor(self.flow[k], dtype=torch.float64, requires_grad=True) for k in FLOW_KEYS}
-        vt, at, vp, ap = flow_profiles(self.mesh, coef)
-        torch.autograd.backward([vt, at, vp, ap], [vt_bar, at_bar, vp_bar, ap_bar])
+        # the profile chain needs autograd even inside a Function's backward,
+        # where grad mode is off
+        with torch.enable_grad():
+            coef = {k: torch.tensor(self.flow[k], dtype=torch.float64, requires_grad=True) for k in FLOW_KEYS}
+            vt, at, vp, ap = flow_profiles(self.mesh, coef)
+            torch.autograd.backward([vt, at, vp, ap], [vt_bar, at_bar, vp_bar, ap_bar])
         return {k: coef[k].grad.numpy().copy() for k in FLOW_KEYS}
 
 

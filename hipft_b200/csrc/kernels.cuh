@@ -280,13 +280,12 @@ struct Weno {
 
 // WENO3 face flux (src/hipft.f90:7775-7801).  LN*: LN(j-2), LN(j-1), LN(j);
 // LP*: LP(j-1), LP(j), LP(j+1); weights at indices j-1 (m1) and j (0).
-// The reference normalises the nonlinear weights, OM = w / (w0 + w1) with
-// w0m = D_P_T(j-1)/e0^2, w1m = D_MC_T(j-1)/e1^2, and sums OM*p.  Multiplying
-// each side's numerator and denominator by e0^2 e1^2 gives the same value
-// with one division per side instead of four:
-//   um = (a p0m + b p1m) / (a + b),  a = D_P_T(j-1) e1^2,  b = D_MC_T(j-1) e0^2
-// (likewise up).  The result differs from the reference's operation order by
-// rounding only.
+// The nonlinear weights are normalised in the reference's order,
+// OM = w / (w0 + w1) with w0m = D_P_T(j-1)/e0^2, w1m = D_MC_T(j-1)/e1^2, and
+// the face value is sum(OM*p): six divisions per face.  A form with one
+// division per side (numerator and denominator multiplied by e0^2 e1^2) is
+// the same value in exact arithmetic, but its rounding drifts the 24-hour
+// 1024x2048 field by 1.5e-12 relative, above the 1e-12 parity bar.
 __device__ __forceinline__ double weno_face(double LNm2, double LNm1, double LN0, double LPm1, double LP0,
                                             double LPp1, double DCMC_m1, double DCMC_0, double DCCP_m1,
                                             double DCCP_0, double DPT_m1, double DMCT_m1, double DMT_0,
@@ -299,10 +298,11 @@ __device__ __forceinline__ double weno_face(double LNm2, double LNm1, double LN0
   double t2 = DCCP_0 * (LPp1 - LP0), t3 = DCMC_0 * (LP0 - LPm1);
   double e0 = eps_m1 + kFour * (t0 * t0), e1 = eps_m1 + kFour * (t1 * t1);
   double e2 = eps_0 + kFour * (t2 * t2), e3 = eps_0 + kFour * (t3 * t3);
-  double am = DPT_m1 * (e1 * e1), bm = DMCT_m1 * (e0 * e0);
-  double ap = DMT_0 * (e3 * e3), bp = DCPT_0 * (e2 * e2);
-  double um = (am * p0m + bm * p1m) / (am + bm);
-  double up = (ap * p0p + bp * p1p) / (ap + bp);
+  double w0m = DPT_m1 / (e0 * e0), w1m = DMCT_m1 / (e1 * e1);
+  double w0p = DMT_0 / (e2 * e2), w1p = DCPT_0 / (e3 * e3);
+  double sm = w0m + w1m, sp = w0p + w1p;
+  double um = (w0m / sm) * p0m + (w1m / sm) * p1m;
+  double up = (w0p / sp) * p0p + (w1p / sp) * p1p;
   return up + um;
 }
 

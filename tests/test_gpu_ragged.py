@@ -49,6 +49,9 @@ def _oracle_alone(i, t, p, br, dt_max, time_end, diffusion=True):
     raw = dict(n_realizations=1, advance_flow=True, flow_num_method=4, strang_splitting=True, flow_dr_model=1,
                flow_mf_model=1, advance_diffusion=diffusion, time_end=time_end, dt_max=dt_max,
                flow_dr_coef_p2_values=[P2[i]], flow_mf_coef_p1_values=[P1[i]],
+               # the handle's set_flow leaves the other coefficients at zero
+               flow_dr_coef_p0_values=[0.0], flow_dr_coef_p4_values=[0.0],
+               flow_mf_coef_p3_values=[0.0], flow_mf_coef_p5_values=[0.0],
                diffusion_coef_constants=[D[i]])
     prm = O.process_parameters(raw)
     return O.run(prm, map_pt=br[None], s1=p, s2=t)

@@ -184,9 +184,12 @@ def _cfl_rank(prm, t):
 
 @pytest.mark.slow
 def test_config_batched64_two_steps_across_assimilation(tmp_path):
-    """64 realizations (seed 1) on 1024 x 2048 refined: two steps with an
-    assimilation of a synthetic observed map (mu^4 weights, mu > 0.1) between
-    them.  The oracle runs the schedule-setting realizations and two others."""
+    """64 realizations (seed 1) on 1024 x 2048 refined with synthetic observed
+    maps (mu^4 weights, mu > 0.1) at 0 h and 1 h, to 2.5 h.  As in the
+    reference (load_data_assimilation, src/hipft.f90:4010-4042), a map at the
+    start time makes the first step zero-length, so the run takes three steps:
+    0 h (assimilate map 0), 0 -> 1 h (assimilate map 1), 1 -> 2.5 h.  The
+    oracle runs the schedule-setting realizations and two others."""
     import hipft_b200 as H
     from hipft_b200 import synthetic as S
     nr = 64
@@ -221,7 +224,7 @@ def test_config_batched64_two_steps_across_assimilation(tmp_path):
     times = [24.0 * (jd - jd0) for jd in jds]
     r = O.run(sub, map_pt=np.broadcast_to(br, (len(subset),) + br.shape), s1=p, s2=t, da_times=times,
               da_maps=np.stack(maps))
-    assert r["nsteps"] == 2, f"expected two steps, the oracle took {r['nsteps']}"
+    assert r["nsteps"] == 3, f"expected three steps, the oracle took {r['nsteps']}"
     shape = (nr,) + r["f"].shape[1:]
     f = H.run_field(str(tmp_path / "hipft.in"), str(tmp_path), shape)
     sol, num = cases.read_run_histories(str(tmp_path), nr)
