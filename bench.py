@@ -210,9 +210,10 @@ def run_reference(args, wl, name):
     return 0
 
 
-def make_handle(H, t, p, br, prm, sl, device, ragged):
+def make_handle(H, t, p, br, prm, sl, device, ragged, graph=False):
     """A handle holding realizations `sl` of the workload with its initial map
-    and flows loaded; ragged: each realization keeps its own schedule."""
+    and flows loaded; ragged: each realization keeps its own schedule; graph:
+    every step runs as one CUDA-graph launch."""
     nrl = len(prm["diffusion_coef_constants"][sl])
     g = H.HipftGPU(t, p, nrl, device=device, advance_flow=True, flow_num_method=4, strang_splitting=True,
                    advance_diffusion=True, diffusion_coef_constants=prm["diffusion_coef_constants"][sl])
@@ -222,6 +223,8 @@ def make_handle(H, t, p, br, prm, sl, device, ragged):
     g.update_flow()
     if ragged:
         g.set_ragged(True)
+    if graph:
+        g.set_graph(True)
     return g
 
 
@@ -310,7 +313,7 @@ def run_gpu(args, wl, name):
     first, nrl = split_realizations(wl["nr"], world, rank)
     sl = slice(first, first + nrl)
     ragged = args.schedule == "ragged"
-    g = make_handle(H, t, p, br, prm, sl, local, ragged)
+    g = make_handle(H, t, p, br, prm, sl, local, ragged, graph=args.step == "graph")
     stream = torch.cuda.current_stream()
     g.set_stream(stream.cuda_stream)
     dt = g.flow_dtmax()
@@ -348,6 +351,8 @@ def run_gpu(args, wl, name):
         dist.barrier()
     torch.cuda.synchronize()
     ip = g.info()
+    if args.step == "graph":
+        g.set_graph(False)  # per-kernel events need host-driven launches (the same kernels)
     g.set_profiling(True)
     p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     p0.record(stream)
@@ -361,6 +366,8 @@ def run_gpu(args, wl, name):
     ring_n, ring_ms = g.kernel_time(2)
     oth_n, oth_ms = g.kernel_time(3)
     g.set_profiling(False)
+    if args.step == "graph":
+        g.set_graph(True)
     ipe = g.info()
     rkg2_stages = int(ipe.rkg2_stages - ip.rkg2_stages)
     rkg2_cell_stages = float(ipe.rkg2_cell_stages - ip.rkg2_cell_stages)
@@ -416,6 +423,8 @@ def run_gpu(args, wl, name):
                    "schedule": ("ragged: each realization its own Euler limit, PTL subcycles and RKG2 stage "
                                 "counts" if ragged else "shared (the reference's MIN/MAX schedule)"),
                    "method": "WENO3+SSPRK(4,3) Strang-split with RKG2 (PTL subcycles), DA every 24 h",
+                   "step": ("one CUDA-graph launch per split step (PTL subcycles, stage counts and substeps "
+                            "decided on the device)" if args.step == "graph" else "host-driven launches"),
                    "l2": "inputs larger than L2 (%.2f GB per field), no flush" % (ntm * npm * nrl * 8 / 1e9)},
         "roofline": {"bound": "hbm",
                      "kernel": sts_kernel, "kernel_role": ("two fused RKG2 stages per launch"
@@ -704,6 +713,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
     ap.add_argument("--c5", action="store_true", help="add the 16-realization 2048 x 4096 forward leg")
+    ap.add_argument("--step", default="graph", choices=["graph", "host"],
+                    help="graph: each split step is one CUDA-graph launch; host: host-driven launches")
     ap.add_argument("--schedule", default="ragged", choices=["ragged", "shared"],
                     help="ragged: every realization its own schedule (default); shared: the reference's")
     args = ap.parse_args()

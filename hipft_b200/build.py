@@ -19,7 +19,7 @@ EXE = os.path.join(PKG, "bin", "hipft")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["hipft_gpu.cu"]
 CXX_SOURCES = ["namelist.cpp", "h5lite.cpp", "h5write.cpp", "driver.cpp"]
-HEADERS = ["kernels.cuh", "sts_pair_ws.cuh", "namelist.h"]
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 
 
 def _nvcc() -> str:

@@ -22,6 +22,7 @@
 #include "sts_pair_ws.cuh"
 #include "sts_quad_ws.cuh"
 #include "adjoint.cuh"
+#include "graph_step.cuh"
 
 using namespace hipft;
 
@@ -150,6 +151,18 @@ struct hipft_gpu {
   unsigned long long *d_rbits = nullptr;                // [2*nr] per-realization reductions
   std::vector<int64_t> r_s, r_cycles, r_substeps;       // the last step's schedule
   int64_t rkg2_cell_stages = 0;  // unique cells x stages k >= 2 advanced (both modes)
+  // steps run as one CUDA graph each (hipft_gpu_set_graph)
+  bool graph_on = false;
+  cudaGraph_t g_graph = nullptr;
+  cudaGraphExec_t g_exec = nullptr;
+  cudaStream_t g_side[3] = {};      // streams the step (and its loop bodies) are captured on
+  GArrays GA{};                     // device schedule arrays
+  int g_cur = -1;                   // buffer the capture used as the field
+  int g_paircap = 0;                // stage pairs the coefficient tables hold
+  bool g_pdl = true;                // programmatic launches inside the captured pair loop
+  std::vector<unsigned char> g_key; // launch parameters the capture baked in
+  GState g_last{};                  // statistics of the last graph-run step
+  bool g_stats_valid = true;        // g_last read back since the last launch
   hipft_allreduce_cb red_cb = nullptr;  // scalar all-reduce over ranks (plain-mode sharding)
   void *red_user = nullptr;
   PoleScratch pole{};       // chunk shares of the ring sums for k_pair_poles
@@ -169,6 +182,10 @@ struct hipft_gpu {
   double vwidth = 0.03, vt_const = 0.0, vp_omega = 0.0, vtime_start = 0.0;
   // assimilation
   double *d_da = nullptr, *d_daopt = nullptr;
+  double *d_daw = nullptr;                   // mu^power weight planes
+  int *d_dawidx = nullptr;                   // [nr+1] plane of each realization
+  size_t daw_cap = 0;
+  std::vector<double> h_daw;
   // sources: file term (one plane), two RFE frames, the blended source
   double *d_src_file = nullptr, *d_rfe[2] = {}, *d_src = nullptr, *d_rnd = nullptr, *d_rfe_aux = nullptr;
   bool src_set = false;
@@ -183,6 +200,8 @@ struct hipft_gpu {
   double prof_ms[HIPFT_K_NKINDS] = {};
   int64_t prof_n[HIPFT_K_NKINDS] = {};
 };
+
+static void graph_release(hipft_gpu *h);
 
 // Event pair around one launch when profiling (returns the stop event).
 struct ProfScope {
@@ -1201,6 +1220,9 @@ extern "C" int hipft_gpu_destroy(hipft_gpu *h) {
       cudaEventDestroy(pr.second);
     }
   for (auto e : h->ev_pool) cudaEventDestroy(e);
+  graph_release(h);
+  for (auto s : h->g_side)
+    if (s) cudaStreamDestroy(s);
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1562,43 +1584,12 @@ struct StsTable {
   std::vector<double> uj, vj, ubj, gj, b;
 };
 static void sts_coefs(int method, double dtl, double dt_euler, StsTable &T) {
-  int64_t s;
-  if (method == 2)
-    s = (int64_t)std::ceil(0.5 * (std::sqrt(9.0 + 16.0 * (dtl / dt_euler)) - 1.0));
-  else
-    s = (int64_t)std::ceil(0.5 * (std::sqrt(25.0 + 24.0 * (dtl / dt_euler)) - 3.0));
-  if (s < 3) s = 3;
-  if (s % 2 == 0) s = s + 1;
+  const int64_t s = sts_count(method, dtl, dt_euler);
   T.s = s;
-  auto &b = T.b, &uj = T.uj, &vj = T.vj, &ubj = T.ubj, &gj = T.gj;
-  b.assign(s + 1, 0); uj.assign(s + 1, 0); vj.assign(s + 1, 0); ubj.assign(s + 1, 0); gj.assign(s + 1, 0);
-  if (method == 2) {
-    double w = 4.0 / (double)(s * s + s - 2);
-    b[1] = 1.0 / 3.0; b[2] = 1.0 / 3.0;
-    uj[1] = -9999.0; vj[1] = -9999.0; ubj[1] = 4.0 / (3.0 * (double)(s * s + s - 2)); gj[1] = -9999.0;
-    uj[2] = 3.0 / 2.0; vj[2] = -0.5; ubj[2] = uj[2] * w; gj[2] = -w;
-    for (int64_t j = 3; j <= s; ++j) {
-      b[j] = ((double)(j * j + j) - 2.0) / (2.0 * (double)j * (double)(j + 1));
-      double r1 = b[j] / b[j - 1], r2 = b[j] / b[j - 2];
-      uj[j] = r1 * (2.0 - 1.0 / (double)j);
-      vj[j] = r2 * (1.0 / (double)j - 1.0);
-      ubj[j] = uj[j] * w;
-      gj[j] = (b[j - 1] - 1.0) * ubj[j];
-    }
-  } else {
-    double w = 6.0 / (double)((s + 4) * (s - 1));
-    b[1] = 1.0 / 3.0; b[2] = 1.0 / 15.0;
-    uj[1] = 1.0; vj[1] = -9999.0; ubj[1] = w; gj[1] = -9999.0;
-    uj[2] = 1.0 / 2.0; vj[2] = -1.0 / 10.0; ubj[2] = uj[2] * w; gj[2] = 0.0;
-    for (int64_t j = 3; j <= s; ++j) {
-      b[j] = (4.0 * (double)(j - 1) * (double)(j + 4)) /
-             (3.0 * (double)j * (double)(j + 1) * (double)(j + 2) * (double)(j + 3));
-      double r1 = b[j] / b[j - 1], r2 = b[j] / b[j - 2];
-      uj[j] = r1 * (2.0 + 1.0 / (double)j);
-      vj[j] = -r2 * (1.0 / (double)j + 1.0);
-      ubj[j] = uj[j] * w;
-      gj[j] = (0.5 * (double)j * ((double)j + 1.0) * b[j - 1] - 1.0) * ubj[j];
-    }
+  T.b.assign(s + 1, 0); T.uj.assign(s + 1, 0); T.vj.assign(s + 1, 0); T.ubj.assign(s + 1, 0); T.gj.assign(s + 1, 0);
+  for (int64_t j = 1; j <= s; ++j) {
+    T.b[j] = sts_b(method, j);
+    sts_stage(method, s, j, T.uj[j], T.vj[j], T.ubj[j], T.gj[j]);
   }
 }
 
@@ -2227,6 +2218,21 @@ extern "C" int hipft_gpu_ragged_schedule(hipft_gpu *h, int64_t *sts_s, int64_t *
                                          double *dt_euler) {
   if (!h) return HIPFT_EINVAL;
   if (!h->ragged) return fail(h, HIPFT_ESTATE, "ragged_schedule: the handle is not in ragged mode");
+  if (h->graph_on && h->GA.st) {
+    // the device's record of the last graph-run step
+    const int nr = h->nr;
+    std::vector<long long> s(nr);
+    std::vector<int> c(nr), q(nr);
+    CK(h, cudaMemcpyAsync(s.data(), h->GA.s_last, sizeof(long long) * nr, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(c.data(), h->GA.cycles_i, sizeof(int) * nr, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(q.data(), h->GA.nsub_i, sizeof(int) * nr, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < nr; ++i) {
+      h->r_s[i] = s[i];
+      h->r_cycles[i] = c[i];
+      h->r_substeps[i] = q[i] > 0 ? q[i] : 1;
+    }
+  }
   for (int i = 0; i < h->nr; ++i) {
     if (sts_s) sts_s[i] = h->r_s.empty() ? 0 : h->r_s[i];
     if (subcycles) subcycles[i] = h->r_cycles.empty() ? 0 : h->r_cycles[i];
@@ -2243,6 +2249,10 @@ extern "C" int hipft_gpu_diffusion_step(hipft_gpu *h, double dtl, hipft_cycle_cb
   if (!h->P.advance_diffusion) return fail(h, HIPFT_ESTATE, "diffusion_step: advance_diffusion is off");
   CK(h, cudaSetDevice(h->dev));
   if (h->ragged) return ragged_diffusion_step(h, dtl, info);
+  // the ring sums of the step's input are summed afresh (as in ragged
+  // batches and in a graph-run step), also when the previous step left the
+  // fused kernels' ring sums of the same field
+  h->dring_valid = false;
   const int max_sc = 60;
   int64_t stages0 = h->cell_updates;
   int i = 1;
@@ -2283,9 +2293,463 @@ extern "C" int hipft_gpu_diffusion_step(hipft_gpu *h, double dtl, hipft_cycle_cb
   return HIPFT_OK;
 }
 
+// ================================================================ graph mode
+// hipft_gpu_set_graph: every flux_transport_step runs as one launch of a
+// captured CUDA graph.  The schedule decisions that the host-driven step
+// makes between launches (PTL subcycles, stage counts, advection substeps)
+// are made on the device by the schedule kernels of graph_step.cuh, and the
+// loops they size are WHILE nodes.  The capture fixes the buffers: the field
+// stays in buffer g_cur; stage outputs rotate through four others with fixed
+// roles (an even stage pair reads (R0, R3) and writes (R1, R2), an odd one
+// reads (R2, R1) and writes (R3, R0)); each realization's result is gathered
+// back into the field buffer after its super-step.
+
+static void graph_release(hipft_gpu *h) {
+  if (h->g_exec) cudaGraphExecDestroy(h->g_exec);
+  if (h->g_graph) cudaGraphDestroy(h->g_graph);
+  h->g_exec = nullptr;
+  h->g_graph = nullptr;
+}
+
+template <typename T>
+static void dfree(hipft_gpu *h, T *&p) {
+  if (p) {
+    cudaFree((void *)p);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)p), h->allocs.end());
+  }
+  p = nullptr;
+}
+
+// Schedule arrays for the handle's realizations and `paircap` stage pairs.
+static int graph_alloc(hipft_gpu *h, int paircap) {
+  GArrays &g = h->GA;
+  const size_t nr = (size_t)h->nr;
+  if (!g.st) {
+    double *de = nullptr, *dm = nullptr;
+    TRY(dalloc(h, &g.st, 1));
+    TRY(dalloc(h, &g.ts, nr));
+    TRY(dalloc(h, &g.d, nr));
+    TRY(dalloc(h, &de, nr));
+    TRY(dalloc(h, &dm, nr));
+    TRY(dalloc(h, &g.rdt, nr));
+    TRY(dalloc(h, &g.act, nr));
+    TRY(dalloc(h, &g.fin, nr));
+    TRY(dalloc(h, &g.rl_ptl, nr));
+    TRY(dalloc(h, &g.rl_dif, nr));
+    TRY(dalloc(h, &g.rl_adv, nr));
+    TRY(dalloc(h, &g.rl_adv_all, nr));
+    TRY(dalloc(h, &g.nsub_i, nr));
+    TRY(dalloc(h, &g.cycles_i, nr));
+    TRY(dalloc(h, &g.s_i, nr));
+    TRY(dalloc(h, &g.s_last, nr));
+    TRY(dalloc(h, &g.c1, nr));
+    TRY(dalloc(h, &g.bits, 2 * nr));
+    g.dt_euler = de;
+    g.dtmax = dm;
+    CK(h, cudaMemsetAsync(g.st, 0, sizeof(GState), h->stream));
+    CK(h, cudaMemsetAsync(g.s_last, 0, nr * sizeof(long long), h->stream));
+    CK(h, cudaMemsetAsync(g.cycles_i, 0, nr * sizeof(int), h->stream));
+    CK(h, cudaMemsetAsync(g.nsub_i, 0, nr * sizeof(int), h->stream));
+    g.nr = h->nr;
+  }
+  if (paircap > g.paircap) {
+    dfree(h, g.nactp);
+    dfree(h, g.rc);
+    TRY(dalloc(h, &g.nactp, (size_t)paircap));
+    TRY(dalloc(h, &g.rc, (size_t)paircap * nr * 2));
+    g.paircap = paircap;
+  }
+  return HIPFT_OK;
+}
+
+// Stage pairs (with the pair loop's slack) a step of length dt can need: one
+// subcycle over the whole step at the smallest Euler limit bounds every
+// realization's stage count.
+static int graph_pairs_needed(const hipft_gpu *h, double dt) {
+  if (!h->P.advance_diffusion) return kGUnroll;
+  double dte = h->dt_euler;
+  if (h->ragged)
+    for (double v : h->r_dt_euler) dte = std::min(dte, v);
+  const int64_t s = sts_count(h->P.diffusion_num_method, dt, dte);
+  return (int)((s - 1) / 2) + kGUnroll;
+}
+
+// Launch parameters a capture bakes in besides the buffers; any change (new
+// flows, ragged mode, larger tables) means a new capture.
+static std::vector<unsigned char> graph_key(const hipft_gpu *h) {
+  std::vector<unsigned char> k;
+  auto add = [&](const void *p, size_t n) {
+    const unsigned char *c = static_cast<const unsigned char *>(p);
+    k.insert(k.end(), c, c + n);
+  };
+  add(&h->FL, sizeof(h->FL));
+  add(&h->DC, sizeof(h->DC));
+  add(&h->ptab, sizeof(h->ptab));
+  const double bc[4] = {h->bc_flow_n, h->bc_flow_s, h->bc_diff_n, h->bc_diff_s};
+  add(bc, sizeof(bc));
+  const int flags[6] = {h->ragged ? 1 : 0, h->cur, h->GA.paircap, h->g_pdl ? 1 : 0, h->auto_sc ? 1 : 0,
+                        (int)h->P.diffusion_subcycles};
+  add(flags, sizeof(flags));
+  return k;
+}
+
+// A conditional handle on the graph that stream s is capturing into.
+static cudaError_t g_handle(cudaStream_t s, cudaGraphConditionalHandle *hc) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, nullptr, nullptr);
+  if (e != cudaSuccess) return e;
+  if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+  return cudaGraphConditionalHandleCreate(hc, cg, 0, 0);
+}
+
+// A WHILE node on handle hc at stream s's capture point; returns its body.
+static cudaError_t g_while(cudaStream_t s, cudaGraphConditionalHandle hc, cudaGraph_t *body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd);
+  if (e != cudaSuccess) return e;
+  if (cs != cudaStreamCaptureStatusActive) return cudaErrorStreamCaptureInvalidated;
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = hc;
+  p.conditional.type = cudaGraphCondTypeWhile;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  e = cudaGraphAddNode(&node, cg, deps, nd, &p);
+  if (e != cudaSuccess) return e;
+  *body = p.conditional.phGraph_out[0];
+  return cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+}
+
+// Captures the split step: the host-driven step's kernels, grids and
+// argument values (ragged or plain), with realization lists, coefficients
+// and substep lengths read from the schedule arrays.
+static int graph_capture(hipft_gpu *h) {
+  graph_release(h);
+  for (auto &s : h->g_side)
+    if (!s) CK(h, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const int nr = h->nr;
+  GArrays &G = h->GA;
+  G.method = h->P.diffusion_num_method;
+  G.auto_sc = h->auto_sc ? 1 : 0;
+  G.subcycles = (int)h->P.diffusion_subcycles;
+  G.ragged = h->ragged ? 1 : 0;
+  G.strang = h->P.strang_splitting ? 1 : 0;
+  G.nadv = (h->adv_time == 1) ? 1 : ((h->adv_time == 2) ? 3 : 4);
+  G.ring0 = h->d_ringbuf[0];
+  G.ring1 = h->d_ringbuf[1];
+  const GArrays g = G;
+  h->g_cur = h->cur;
+  double *F = h->buf[h->cur];
+  double *Bd = h->buf[scratch(h, 0)];  // dty0
+  double *R[4] = {h->buf[scratch(h, 1)], h->buf[scratch(h, 2)], h->buf[scratch(h, 3)], h->buf[scratch(h, 4)]};
+  const Mesh M = h->M;
+  const int64_t nfield = (int64_t)h->fieldn;
+  const int cblocks = 4 * h->num_sms;
+  cudaError_t first = cudaSuccess;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  };
+  auto peek = [&]() { ok(cudaPeekAtLastError()); };
+  // captured on a stream of its own (the handle's stream may be the legacy
+  // default stream, which cannot capture); launched on the handle's stream
+  cudaStream_t s0 = h->g_side[2], s1 = h->g_side[0], s2 = h->g_side[1];
+  // the body of a WHILE node at stream s's capture point, captured on stream b
+  auto begin_body = [&](cudaStream_t s, cudaGraphConditionalHandle hc, cudaStream_t b) {
+    cudaGraph_t body = nullptr;
+    ok(g_while(s, hc, &body));
+    if (first == cudaSuccess)
+      ok(cudaStreamBeginCaptureToGraph(b, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  };
+  auto end_body = [&](cudaStream_t b) {
+    cudaGraph_t gdone = nullptr;
+    ok(cudaStreamEndCapture(b, &gdone));
+  };
+
+  // ---- advection_step over frac * dt (src/hipft.f90:4509-4549)
+  auto adv_stage = [&](cudaStream_t s, const double *x, const double *f0, double *out, AdvCombine cb) {
+    k_ring_advection<<<nr, 256, 0, s>>>(M, h->FL, x, h->d_ring);
+    peek();
+    const dim3 blk(33, 9);
+    const dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)nr);
+    if (h->adv_space == 2)
+      k_advection_stage<32, 8, true><<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
+                                                          h->bc_flow_s, cb, g.rl_adv, g.rdt);
+    else
+      k_advection_stage<32, 8, false><<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
+                                                           h->bc_flow_s, cb, g.rl_adv, g.rdt);
+    peek();
+  };
+  auto advection = [&](double frac) {
+    cudaGraphConditionalHandle hc{};
+    ok(g_handle(s0, &hc));
+    if (first != cudaSuccess) return;
+    k_g_adv_plan<<<1, 256, 0, s0>>>(g, frac, hc);
+    peek();
+    begin_body(s0, hc, s1);
+    if (first != cudaSuccess) return;
+    double *A = R[0], *B = R[1];
+    if (h->adv_time == 1) {  // FE (src/hipft.f90:7440-7444), then back into the field
+      adv_stage(s1, F, nullptr, A, AdvCombine{0, 0.0, 0.0, 1.0});
+      k_g_copy<<<cblocks, 256, 0, s1>>>(F, A, nfield);
+      peek();
+    } else if (h->adv_time == 2) {  // SSPRK(3,3) (src/hipft.f90:7486-7505)
+      adv_stage(s1, F, nullptr, A, AdvCombine{0, 0.0, 0.0, 1.0});
+      adv_stage(s1, A, F, B, AdvCombine{1, c_three_quarter, c_quarter, c_quarter});
+      adv_stage(s1, B, F, F, AdvCombine{1, c_third, c_two_third, c_two_third});
+    } else {  // SSPRK(4,3) (src/hipft.f90:7552-7574)
+      adv_stage(s1, F, nullptr, A, AdvCombine{0, 0.0, 0.0, 0.5});
+      adv_stage(s1, A, nullptr, B, AdvCombine{0, 0.0, 0.0, 0.5});
+      adv_stage(s1, B, F, A, AdvCombine{1, c_two_third, c_third, c_sixth});
+      adv_stage(s1, A, nullptr, F, AdvCombine{0, 0.0, 0.0, 0.5});
+    }
+    k_g_adv_tick<<<1, 256, 0, s1>>>(g, (h->adv_time == 1) ? 4 : 2 * g.nadv + 1, hc);
+    peek();
+    end_body(s1);
+  };
+
+  // ---- one stage pair of the loop body: pair q of the iteration (q = 0..3)
+  const int nkt = (h->npm - 2 + kWK - 1) / kWK;
+  auto pair = [&](cudaStream_t s, int q, bool overlap) {
+    const bool even = (q % 2) == 0;
+    const double *ykm1 = even ? R[0] : R[2], *ykm2 = even ? R[3] : R[1];
+    double *ok_ = even ? R[1] : R[3], *ok1 = even ? R[2] : R[0];
+    const double *rin = even ? g.ring1 : g.ring0;
+    double *rout = even ? g.ring0 : g.ring1;
+    RingOut ro{rout, h->d_rpart, h->d_rcount, nkt};
+    PairArgs pa{StageCoef{}, StageCoef{}, h->d_err, g.rl_dif, g.rc};
+    pa.dctr = &g.st->pctr;
+    pa.doff = q;
+    pa.dnact = g.nactp;
+    pa.dstride = 2 * nr;
+    PairTables pt = h->ptab;
+    pt.ntiles = pt.nb * pt.nkt * nr;
+    const int grid = std::min(pt.ntiles, 2 * h->num_sms);
+    const WsMaps tmaps = ws_maps(h, ykm1, ykm2, F, Bd);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kWThreads);
+    cfg.dynamicSmemBytes = kWSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = (h->g_pdl && overlap) ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    ok(cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true, false, true>, M, (const double *)h->DC.dfac, ykm1, ykm2,
+                          (const double *)F, (const double *)Bd, ok_, ok1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro,
+                          pt, tmaps));
+    const dim3 pg((unsigned)nr, (unsigned)h->pole_nch);
+    k_pair_poles<<<pg, kPoleThreads, 0, s>>>(M, h->DC.dfac, ykm1, ykm2, F, Bd, ok1, rin, h->bc_diff_n,
+                                             h->bc_diff_s, pa, ro, h->pole);
+    peek();
+  };
+
+  // ---- diffusion_step over dt (src/hipft.f90:4551-4695)
+  auto diffusion = [&]() {
+    cudaGraphConditionalHandle hsub{};
+    ok(g_handle(s0, &hsub));
+    if (first != cudaSuccess) return;
+    k_g_dif_begin<<<1, 256, 0, s0>>>(g, h->ragged ? 0 : 1, hsub);
+    peek();
+    // plain mode: the ring of the field once; later subcycles reuse the ring
+    // sums the last stage pair left (the gather moves them to ring0)
+    if (!h->ragged) {
+      k_ring_diffusion<<<nr, 256, 0, s0>>>(M, h->DC, F, g.ring0);
+      peek();
+    }
+    begin_body(s0, hsub, s1);
+    if (first != cudaSuccess) return;
+    int body_kernels = 1;  // the subcycle tick itself
+    if (h->ragged) {
+      k_ring_diffusion<<<nr, 256, 0, s1>>>(M, h->DC, F, g.ring0);
+      peek();
+      ++body_kernels;
+    }
+    const dim3 blk(32, 8);
+    const dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)nr);
+    if (h->auto_sc) {  // PTL (src/hipft.f90:5042-5161) of the active realizations
+      k_g_ptl_reset<<<1, 256, 0, s1>>>(g);
+      peek();
+      const int pr = h->ragged ? 1 : 0;
+      unsigned long long *bmax = g.bits, *bmin = g.bits + (h->ragged ? nr : 1);
+      k_diffusion_stage<MODE_AX><<<grd, blk, 0, s1>>>(M, h->DC, F, nullptr, nullptr, nullptr, R[0], nullptr, g.ring0,
+                                                      h->bc_diff_n, h->bc_diff_s, StageCoef{}, bmax, g.rl_ptl, pr);
+      peek();
+      k_ptl<<<grd, blk, 0, s1>>>(M, F, R[0], bmax, bmin, g.rl_ptl, pr);
+      peek();
+      body_kernels += 2;
+    }
+    cudaGraphConditionalHandle hpair{};
+    ok(g_handle(s1, &hpair));
+    if (first != cudaSuccess) return;
+    k_g_plan<<<1, 256, 0, s1>>>(g, hpair);
+    peek();
+    const int64_t ncoef = (int64_t)g.paircap * nr;
+    k_g_coefs<<<(unsigned)((ncoef + 255) / 256), 256, 0, s1>>>(g);
+    peek();
+    // stage 1 (src/hipft.f90:5211-5218): Y_1 into R0, dty0; Y_0 = u0 into R3
+    {
+      const int nkb = (h->npm - 2 + kKPT3 - 1) / kKPT3;
+      RingOut ro{g.ring1, h->d_rpart, h->d_rcount, nkb};
+      const int jshift = (h->ntm % 2 == 1 && ((h->ntm - 1) / 2) % 32 == 0) ? 1 : 0;
+      const int nthr = (h->ntm + 2 * jshift + 1) / 2;
+      const dim3 g1((unsigned)((nthr + 127) / 128), (unsigned)nkb, (unsigned)nr);
+      k_sts_stage_v3<MODE_STS1, kKPT3><<<g1, 128, 0, s1>>>(M, h->DC.dfac, F, nullptr, nullptr, nullptr, R[0], Bd,
+                                                           g.ring0, h->bc_diff_n, h->bc_diff_s, StageCoef{}, ro,
+                                                           jshift, g.rl_dif, g.c1);
+      peek();
+      k_g_copy<<<cblocks, 256, 0, s1>>>(R[3], F, nfield);
+      peek();
+      body_kernels += 2;
+    }
+    begin_body(s1, hpair, s2);
+    if (first != cudaSuccess) return;
+    for (int q = 0; q < kGUnroll; ++q) pair(s2, q, q > 0);
+    k_g_pair_tick<<<1, 1, 0, s2>>>(g, hpair);
+    peek();
+    end_body(s2);
+    // the result of each realization back into the field: Y_s is in R2 after
+    // an even last pair, in R0 after an odd one
+    k_g_gather<<<dim3((unsigned)nr, 64u), 256, 0, s1>>>(g, M, F, R[2], R[0]);
+    peek();
+    k_g_sub_tick<<<1, 256, 0, s1>>>(g, body_kernels, hsub);
+    peek();
+    end_body(s1);
+  };
+
+  ok(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  if (first == cudaSuccess) {
+    k_g_step_begin<<<1, 32, 0, s0>>>(g);
+    peek();
+    const double fa = h->P.strang_splitting ? 0.5 : 1.0;
+    if (h->P.advance_flow) advection(fa);
+    if (h->P.advance_diffusion && first == cudaSuccess) diffusion();
+    if (h->P.strang_splitting && h->P.advance_flow && first == cudaSuccess) advection(0.5);
+  }
+  // a failed body capture may leave a side stream capturing
+  for (cudaStream_t s : {s1, s2}) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t gd = nullptr;
+      cudaStreamEndCapture(s, &gd);
+      if (first == cudaSuccess) first = cudaErrorStreamCaptureInvalidated;
+    }
+  }
+  cudaGraph_t graph = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(s0, &graph);
+  if (first == cudaSuccess) first = ee;
+  if (first == cudaSuccess) first = cudaGraphInstantiate(&h->g_exec, graph, 0);
+  if (first != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    h->g_exec = nullptr;
+    cudaGetLastError();
+    return fail(h, HIPFT_ECUDA, "graph capture of the step: %s", cudaGetErrorString(first));
+  }
+  h->g_graph = graph;
+  h->g_key = graph_key(h);
+  return HIPFT_OK;
+}
+
+// Statistics of the last graph-run step into the handle's counters.
+static int graph_collect(hipft_gpu *h) {
+  if (h->g_stats_valid) return HIPFT_OK;
+  CK(h, cudaMemcpyAsync(h->h_pin, h->GA.st, sizeof(GState), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(&h->g_last, h->h_pin, sizeof(GState));
+  h->g_stats_valid = true;
+  const GState &st = h->g_last;
+  const int64_t cells = (int64_t)h->ntm * (h->npm - 2);
+  h->cell_updates += cells * (st.stage_sum + st.adv_slices);
+  h->rkg2_cell_stages += cells * st.rkg2_sum;
+  h->launches += st.kernels;
+  if (h->P.advance_diffusion) {
+    h->sts_s = st.smax;
+    h->subcycles_state = st.cycles;
+  }
+  if (st.err == 1) return fail(h, HIPFT_ECUDA, "graph-run step: the stage tables were too small");
+  if (st.err == 2) return fail(h, HIPFT_ECUDA, "graph-run step: a loop ran past its iteration limit");
+  return HIPFT_OK;
+}
+
+// One split step as one graph launch.
+static int graph_step(hipft_gpu *h, double dt, hipft_diffusion_info *info) {
+  TRY(graph_collect(h));
+  if (h->P.advance_diffusion) TRY(ensure_pair_plan(h));
+  const int need = graph_pairs_needed(h, dt);
+  const bool grow = need > h->GA.paircap;
+  TRY(graph_alloc(h, grow ? need + need / 4 : need));
+  if (h->cur != h->g_cur && h->g_cur >= 0) {
+    // another entry point left the field elsewhere: back into the captured buffer
+    CK(h, cudaMemcpyAsync(h->buf[h->g_cur], h->buf[h->cur], h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice,
+                          h->stream));
+    h->cur = h->g_cur;
+  }
+  // per-realization limits (ragged: each its own; plain: the shared ones)
+  const int nr = h->nr;
+  std::vector<double> de(nr, h->dt_euler), dm(nr, 0.0);
+  if (h->ragged) {
+    if (h->P.advance_diffusion) de = h->r_dt_euler;
+    if (h->P.advance_flow) {
+      TRY(ragged_dtmax(h));
+      dm = h->r_dtmax;
+    }
+  }
+  CK(h, cudaMemcpyAsync(const_cast<double *>(h->GA.dt_euler), de.data(), sizeof(double) * nr,
+                        cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaMemcpyAsync(const_cast<double *>(h->GA.dtmax), dm.data(), sizeof(double) * nr, cudaMemcpyHostToDevice,
+                        h->stream));
+  if (!h->g_exec || graph_key(h) != h->g_key) TRY(graph_capture(h));
+  CK(h, cudaMemcpyAsync(&h->GA.st->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(h, cudaGraphLaunch(h->g_exec, h->stream));
+  h->g_stats_valid = false;
+  h->dring_valid = false;
+  h->ring_cur = 0;
+  if (info) {
+    TRY(graph_collect(h));
+    TRY(check_wait_flag(h, "graph-run step: a bounded wait for staged tiles gave up"));
+    info->dtime_diffusion_euler = h->dt_euler;
+    if (h->ragged && !h->r_dt_euler.empty())
+      info->dtime_diffusion_euler = *std::min_element(h->r_dt_euler.begin(), h->r_dt_euler.end());
+    info->sts_s = h->g_last.smax;
+    info->subcycles = h->g_last.cycles;
+    info->total_stages = nr ? h->g_last.stage_sum / nr : 0;
+  }
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_gpu_set_graph(hipft_gpu *h, int on) {
+  if (!h) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  if (!on) {
+    TRY(graph_collect(h));
+    h->graph_on = false;
+    graph_release(h);
+    return HIPFT_OK;
+  }
+  if (h->red_cb) return fail(h, HIPFT_ESTATE, "set_graph: a step shared over ranks reduces on the host");
+  if (h->P.advance_source) return fail(h, HIPFT_EINVAL, "set_graph: sources are not part of a graph-run step");
+  if (h->P.advance_diffusion && (h->DC.grid || h->P.diffusion_num_method == 1))
+    return fail(h, HIPFT_EINVAL, "set_graph: needs RKG2 or RKL2 with per-realization constant diffusion coefficients");
+  if (h->nbuf < 6) return fail(h, HIPFT_ESTATE, "set_graph: needs six field buffers");
+  const char *e = std::getenv("HIPFT_GRAPH_PDL");
+  h->g_pdl = ws_pdl() && !(e && std::atoi(e) == 0);
+  h->graph_on = true;
+  return HIPFT_OK;
+}
+
 extern "C" int hipft_gpu_flux_transport_step(hipft_gpu *h, double dt, hipft_cycle_cb cb, void *user,
                                              hipft_diffusion_info *info) {
   if (!h) return HIPFT_EINVAL;
+  if (h->graph_on) {
+    if (cb) return fail(h, HIPFT_ESTATE, "flux_transport_step: subcycle callbacks need the host-driven step");
+    if (!h->field_set) return fail(h, HIPFT_ESTATE, "flux_transport_step before set_field");
+    CK(h, cudaSetDevice(h->dev));
+    return graph_step(h, dt, info);
+  }
   if (h->P.strang_splitting) {
     double half = dt * 0.5;
     if (h->P.advance_source) TRY(hipft_gpu_source_step(h, half));
@@ -2419,6 +2883,47 @@ static int da_args(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o,
   }
   TRY(upload(h, h->d_daopt, opt));
   CK(h, cudaMemcpyAsync(h->d_tidx, tidx.data(), tidx.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if (o->custom_from_mu && (!o->mu_power || !o->mu_limit))
+    return fail(h, HIPFT_EINVAL, "assimilate: custom_from_mu needs mu_power and mu_limit");
+  if (o->custom_from_mu) {
+    // mu^power weights (src/hipft.f90:4246-4252) on the host, with the C
+    // library's pow: the weights then carry the reference's bits, which the
+    // 1e-12 field bar needs (a 2-ulp change of every weight moves the
+    // assimilated 1024x2048 fields by 1.8e-12 after 2.5 hours).  One plane
+    // per distinct (power, limit).
+    const size_t slice = (size_t)npm1 * ntm;
+    std::vector<std::pair<double, double>> keys;
+    std::vector<int> widx((size_t)nr + 1, 0);
+    for (int i = 1; i <= nr; ++i) {
+      const std::pair<double, double> key(o->mu_power[i - 1], o->mu_limit[i - 1]);
+      size_t u = 0;
+      while (u < keys.size() && keys[u] != key) ++u;
+      if (u == keys.size()) keys.push_back(key);
+      widx[i] = (int)u;
+    }
+    if (keys.size() * slice > h->daw_cap) {
+      if (h->d_daw) {
+        CK(h, cudaStreamSynchronize(h->stream));
+        cudaFree(h->d_daw);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void *)h->d_daw), h->allocs.end());
+        h->d_daw = nullptr;
+      }
+      TRY(dalloc(h, &h->d_daw, keys.size() * slice));
+      TRY(dalloc(h, &h->d_dawidx, (size_t)nr + 1));
+      h->daw_cap = keys.size() * slice;
+    }
+    h->h_daw.resize(keys.size() * slice);
+    const double *mu = data3_pt + 2 * slice;
+    for (size_t u = 0; u < keys.size(); ++u) {
+      double *w = h->h_daw.data() + u * slice;
+      const double pw = keys[u].first, lim = keys[u].second;
+      for (size_t q = 0; q < slice; ++q) w[q] = (mu[q] > lim) ? std::pow(mu[q], pw) : 0.0;
+    }
+    CK(h, cudaMemcpyAsync(h->d_daw, h->h_daw.data(), keys.size() * slice * sizeof(double), cudaMemcpyHostToDevice,
+                          h->stream));
+    CK(h, cudaMemcpyAsync(h->d_dawidx, widx.data(), widx.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));  // h_daw and widx are reused by the next call
+  }
   a = DAArgs{};
   a.data = h->d_da;
   a.mu_power = h->d_daopt;
@@ -2429,6 +2934,8 @@ static int da_args(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o,
   a.add = o->add;
   a.custom_from_mu = o->custom_from_mu;
   a.mult_fac = o->mult_fac;
+  a.wmap = h->d_daw;
+  a.widx = h->d_dawidx;
   return HIPFT_OK;
 }
 

@@ -129,8 +129,75 @@ struct StageCoef {
   double a, b, c, d, e;  // meaning depends on the mode
 };
 
+// RKL2 (method 2) / RKG2 (method 3) super-step recurrences, load_sts_rkl2 /
+// load_sts_rkg2 (src/hipft.f90:5244-5475).  Host and device evaluate the same
+// expressions (no contraction), so a schedule built on either side has the
+// same bits.
+__host__ __device__ inline int64_t sts_count(int method, double dtl, double dt_euler) {
+  int64_t s;
+  if (method == 2)
+    s = (int64_t)ceil(0.5 * (sqrt(9.0 + 16.0 * (dtl / dt_euler)) - 1.0));
+  else
+    s = (int64_t)ceil(0.5 * (sqrt(25.0 + 24.0 * (dtl / dt_euler)) - 3.0));
+  if (s < 3) s = 3;
+  if (s % 2 == 0) s = s + 1;
+  return s;
+}
+
+__host__ __device__ inline double sts_b(int method, int64_t j) {
+  if (method == 2) {
+    if (j <= 2) return 1.0 / 3.0;
+    return ((double)(j * j + j) - 2.0) / (2.0 * (double)j * (double)(j + 1));
+  }
+  if (j <= 1) return 1.0 / 3.0;
+  if (j == 2) return 1.0 / 15.0;
+  return (4.0 * (double)(j - 1) * (double)(j + 4)) /
+         (3.0 * (double)j * (double)(j + 1) * (double)(j + 2) * (double)(j + 3));
+}
+
+// mu_j, nu_j, mu~_j, gamma~_j of stage j of an s-stage super-step; j = 1
+// gives mu~_1 (the others are unused there).
+__host__ __device__ inline void sts_stage(int method, int64_t s, int64_t j, double &uj, double &vj, double &ubj,
+                                          double &gj) {
+  if (method == 2) {
+    const double w = 4.0 / (double)(s * s + s - 2);
+    if (j == 1) {
+      uj = -9999.0; vj = -9999.0; ubj = 4.0 / (3.0 * (double)(s * s + s - 2)); gj = -9999.0;
+    } else if (j == 2) {
+      uj = 3.0 / 2.0; vj = -0.5; ubj = uj * w; gj = -w;
+    } else {
+      const double b = sts_b(2, j), r1 = b / sts_b(2, j - 1), r2 = b / sts_b(2, j - 2);
+      uj = r1 * (2.0 - 1.0 / (double)j);
+      vj = r2 * (1.0 / (double)j - 1.0);
+      ubj = uj * w;
+      gj = (sts_b(2, j - 1) - 1.0) * ubj;
+    }
+    return;
+  }
+  const double w = 6.0 / (double)((s + 4) * (s - 1));
+  if (j == 1) {
+    uj = 1.0; vj = -9999.0; ubj = w; gj = -9999.0;
+  } else if (j == 2) {
+    uj = 1.0 / 2.0; vj = -1.0 / 10.0; ubj = uj * w; gj = 0.0;
+  } else {
+    const double b = sts_b(3, j), r1 = b / sts_b(3, j - 1), r2 = b / sts_b(3, j - 2);
+    uj = r1 * (2.0 + 1.0 / (double)j);
+    vj = -r2 * (1.0 / (double)j + 1.0);
+    ubj = uj * w;
+    gj = (0.5 * (double)j * ((double)j + 1.0) * sts_b(3, j - 1) - 1.0) * ubj;
+  }
+}
+
+// The stage-k combine of a super-step of length dtl (src/hipft.f90:5224-5235).
+__host__ __device__ inline StageCoef sts_combine(int method, int64_t s, int64_t k, double dtl) {
+  double uj, vj, ubj, gj;
+  sts_stage(method, s, k, uj, vj, ubj, gj);
+  return StageCoef{uj, vj, 1.0 - uj - vj, ubj * dtl, gj};
+}
+
 // rlist (may be null): realization (0-based) of grid slice z, for ragged
-// batches that advance a subset; per_real: one max |Af| per realization.
+// batches that advance a subset (a negative entry: the slice does nothing);
+// per_real: one max |Af| per realization.
 template <int MODE>
 __global__ void __launch_bounds__(256) k_diffusion_stage(
     Mesh m, DiffCoef dc, const double *__restrict__ x, const double *ykm2, const double *__restrict__ u0,
@@ -139,6 +206,7 @@ __global__ void __launch_bounds__(256) k_diffusion_stage(
     int per_real = 0) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (rlist && rlist[blockIdx.z] < 0) return;  // slot past the list's end
   const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   double ax = 0.0;
   bool active = (j <= m.ntm && k <= m.npm - 1);
@@ -193,6 +261,7 @@ __global__ void k_ptl(Mesh m, const double *__restrict__ f, const double *__rest
                       const int *__restrict__ rlist = nullptr, int per_real = 0) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
   const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  if (rlist && rlist[blockIdx.z] < 0) return;  // slot past the list's end
   const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   if (j < 2 || j > m.ntm - 1 || k > m.npm - 1) return;
   const double fmin_v = 1e-14;
@@ -383,6 +452,7 @@ __global__ void __launch_bounds__((TJ + 1) * (TK + 1)) k_advection_stage(
   const int tid = a + b * (TJ + 1);
   const int j0 = blockIdx.x * TJ + 1;
   const int k0 = blockIdx.y * TK + 2;
+  if (rlist && rlist[blockIdx.z] < 0) return;  // slot past the list's end
   const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   if (rdt) cb.C = cb.C * rdt[i - 1];
   const int ntm = m.ntm, npm = m.npm;
@@ -887,19 +957,24 @@ struct DAArgs {
   const int *tidx0, *tidx1;                        // [nr+1]
   int add, custom_from_mu;
   double mult_fac;
+  // custom_from_mu: weight planes (npm1, ntm) PT, mu^power where mu >
+  // mu_limit, one per distinct (power, limit), and realization i's plane
+  const double *wmap;
+  const int *widx;                                 // [nr+1]
 };
 
 // Blend weight of PT cell (theta jt, phi kp) for realization i
-// (src/hipft.f90:4242-4271): the map's weight slice, or mu^power where
-// mu > mu_limit; zero inside the latitude caps.
+// (src/hipft.f90:4242-4271): the map's weight slice, or the mu^power plane
+// (evaluated on the host with the C library's pow, the function the
+// reference's real-exponent ** calls, so the weights carry its bits); zero
+// inside the latitude caps.
 __device__ __forceinline__ double da_weight(const Mesh &m, const DAArgs &a, int jt, int kp, int i) {
   const int npm1 = m.npm - 1;
   const int64_t slice = (int64_t)npm1 * m.ntm;
   const int64_t q = (int64_t)(jt - 1) * npm1 + (kp - 1);
   double w;
   if (a.custom_from_mu) {
-    double mu = a.data[2 * slice + q];
-    w = (mu > a.mu_limit[i]) ? pow(mu, a.mu_power[i]) : 0.0;
+    w = a.wmap[(int64_t)a.widx[i] * slice + q];
   } else {
     w = a.data[slice + q];
   }
@@ -1050,6 +1125,7 @@ __global__ void __launch_bounds__(128, 4) k_sts_stage_v3(Mesh m, const double *_
   const int ja = 2 * t + 1 - 2 * jshift;
   const int kb = blockIdx.y;
   const int k0 = kb * KPT + 2;
+  if (rlist && rlist[blockIdx.z] < 0) return;  // slot past the list's end
   const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   if (rc) sc = rc[i - 1];
   const int ntm = m.ntm, npm = m.npm;
@@ -1297,6 +1373,13 @@ struct PairArgs {
   // ([nr][2])
   const int *rlist = nullptr;
   const StageCoef *rc = nullptr;
+  // steps run as a CUDA graph (with rlist and rc): the launch's stage pair is
+  // *dctr + doff, read on the device; dnact[pair] realizations of rlist take
+  // part and rc holds dstride coefficients per pair
+  const int *dctr = nullptr;
+  int doff = 0;
+  const int *dnact = nullptr;
+  int dstride = 0;
 };
 
 template <int TJ, int TK, int MINB>

@@ -281,6 +281,15 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
   const int tid = threadIdx.x;
   const int ntm = m.ntm, npm = m.npm;
   const int64_t ld = m.ldt;
+  // tiles and coefficients of this launch: from the launch arguments, or in a
+  // graph-run step from the device's pair counter
+  int ntiles = pt.ntiles;
+  const StageCoef *rcp = pa.rc;
+  if (RAGGED && pa.dctr) {
+    const int pq = *pa.dctr + pa.doff;
+    ntiles = (pt.nsel > 0 ? pt.nsel : pt.nb) * pt.nkt * pa.dnact[pq];
+    rcp = pa.rc + (int64_t)pq * pa.dstride;
+  }
   if (tid == 0) {
     for (int b = 0; b < kWNB; ++b) {
       mbar_init(&full[b], 1);
@@ -303,7 +312,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       if (k0p + kWK - 1 <= npm - 1 && j0p + kWJ - 1 <= ntm)
         ws_store_cols(out_k1, (int64_t)(ip - 1) * m.plane, k0p, j0p, Bp + kWY2, lane, npm, ld);
     };
-    for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
       const int b = n % kWNB, u = n / kWNB;
       int kt, rb, i;
       ws_tile(pt, t, kt, rb, i, RAGGED ? pa.rlist : nullptr);
@@ -332,8 +341,8 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
       double rd = 0.0, rn = 0.0, rsv = 0.0;
       StageCoef rca{}, rcb{};
       if (RAGGED && lane == 0) {
-        rca = pa.rc[2 * (i - 1)];
-        rcb = pa.rc[2 * (i - 1) + 1];
+        rca = rcp[2 * (i - 1)];
+        rcb = rcp[2 * (i - 1) + 1];
       }
       if (lane == 0) {
         rd = dfac[i];
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(kWThreads, 2) k_sts_pair_ws(Mesh m, const doub
   StageCoef sa = pa.ca, sb = pa.cb;
   double *sYk = wsm + kWYk;          // column c of the tile at (c-1)*kWR
   int n = 0;
-  for (int t = blockIdx.x; t < pt.ntiles; t += gridDim.x, ++n) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++n) {
     const int b = n % kWNB, u = n / kWNB;
     const bool landed = mbar_wait_bounded(&full[b], (uint32_t)(u & 1), 1u << 22);
     if (BULKST && w == 0) bulk_wait_read();  // the previous tile's Y_k stores have read sYk
@@ -790,10 +799,16 @@ __global__ void __launch_bounds__(kPoleThreads) k_pair_poles(Mesh m, const doubl
   // this grid to finish (griddepcontrol.wait)
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int tid = threadIdx.x, ch = blockIdx.y, nch = gridDim.y;
+  const StageCoef *rcp = pa.rc;
+  if (pa.dctr) {  // graph-run step: the grid covers every realization
+    const int pq = *pa.dctr + pa.doff;
+    if ((int)blockIdx.x >= pa.dnact[pq]) return;
+    rcp = pa.rc + (int64_t)pq * pa.dstride;
+  }
   const int i = (pa.rlist ? pa.rlist[blockIdx.x] : (int)blockIdx.x) + 1;
   const int ntm = m.ntm, npm = m.npm;
   const int64_t ld = m.ldt, pbase = (int64_t)(i - 1) * m.plane;
-  const StageCoef sa = pa.rc ? pa.rc[2 * (i - 1)] : pa.ca, sb = pa.rc ? pa.rc[2 * (i - 1) + 1] : pa.cb;
+  const StageCoef sa = rcp ? rcp[2 * (i - 1)] : pa.ca, sb = rcp ? rcp[2 * (i - 1) + 1] : pa.cb;
   const double Dr = dfac[i];
   const double ax_n = ring_in[2 * (i - 1)] * bcn;
   const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;

@@ -138,6 +138,43 @@ __device__ __forceinline__ void quad_stage(int tid, int p0, int np, int c0, int 
   }
 }
 
+// The same stage over row pairs 2..65 (rows 4..131) and shared columns
+// c0 .. c0+nc-1, by column marching: consumer thread t owns row pair
+// 2 + (t % 64) and a quarter of the columns (t / 64), keeps the pair's row
+// table (st2, c22, c42) and its stencil window (columns c-1, c, c+1) in
+// registers, and takes the rows above and below from its warp neighbours
+// (lanes 0 and 31 read theirs from shared memory).  Per cell pair it loads
+// the next window column, the combine inputs and the column table: half the
+// shared-memory reads of quad_stage.  O2 is read through OUT (the same array
+// when the stage works in place; each unit reads only its own cell there).
+template <typename Store>
+__device__ __forceinline__ void quad_march(int tid, int c0, int nc, const double *__restrict__ S, int soff,
+                                           double *OUT, int ooff, int woff, const double *__restrict__ U,
+                                           const double *__restrict__ D, const double2 *__restrict__ CT,
+                                           double2 st2, double2 c22, double2 c42, const StageCoef &sc, Store store) {
+  const int lane = tid & 31, g = tid >> 6;
+  const int r = 4 + 2 * (tid & 63);
+  const int cs = c0 + (g * nc) / 4, ce = c0 + ((g + 1) * nc) / 4;  // columns cs .. ce-1 (warp-uniform)
+  if (cs >= ce) return;
+  double2 xl = *reinterpret_cast<const double2 *>(S + (cs - 1 - soff) * kQR + r);
+  double2 xc = *reinterpret_cast<const double2 *>(S + (cs - soff) * kQR + r);
+  for (int c = cs; c < ce; ++c) {
+    const double2 xr = *reinterpret_cast<const double2 *>(S + (c + 1 - soff) * kQR + r);
+    double up = __shfl_up_sync(0xffffffffu, xc.y, 1);
+    double dn = __shfl_down_sync(0xffffffffu, xc.x, 1);
+    if (lane == 0) up = S[(c - soff) * kQR + r - 1];
+    if (lane == 31) dn = S[(c - soff) * kQR + r + 2];
+    const double2 o2 = *reinterpret_cast<const double2 *>(OUT + (c - ooff) * kQR + r);
+    const double2 u = *reinterpret_cast<const double2 *>(U + (c - 1) * kQR + r);
+    const double2 d = *reinterpret_cast<const double2 *>(D + (c - 1) * kQR + r);
+    const double2 y = pair_rows_step(xl, xc, xr, up, dn, st2, c22, c42, CT[c], false, false, 0.0, 0.0, o2, u, d, sc);
+    *reinterpret_cast<double2 *>(OUT + (c - woff) * kQR + r) = y;
+    store(r, c, y);
+    xl = xc;
+    xc = xr;
+  }
+}
+
 // Four RKG2 stages on the interior blocks (see the file comment).  Outputs:
 // out_k2 = Y_{k+2}, out_k3 = Y_{k+3} on the tiles, and the edge rows of
 // out_k = Y_k, out_k1 = Y_{k+1} on the blocks edge_lo / edge_hi.  RAGGED:
@@ -289,8 +326,13 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
       if (k == npm - 1) *reinterpret_cast<double2 *>(q - seam) = y;
     };
     const int cend = 4 + nk;  // one past the tile's last shared column
+    // the row pair of this thread's column march (rows 4..131), for all four stages
+    const int rm = 4 + 2 * (tid & 63);
+    const double2 st2 = *reinterpret_cast<const double2 *>(RT + rm);
+    const double2 c22 = *reinterpret_cast<const double2 *>(RT + kQR + rm);
+    const double2 c42 = *reinterpret_cast<const double2 *>(RT + 2 * kQR + rm);
     // stage k on rows 0..135 (1..134 valid), columns 1..cend+2, over Y_{k-2}
-    quad_stage(tid, 0, kQR / 2, 1, nk + 6, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s0, [&](int r, int c, double2 y) {
+    auto st_k = [&](int r, int c, double2 y) {
       // Y_k at the edge row a neighbouring pole block reads (rows j0 or j0+127)
       if (c >= 4 && c < cend && ((elo && r == 4) || (ehi && r == 130))) {
         const int k = k0 - 4 + c;
@@ -301,40 +343,32 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
         if (k == 2) q[rr + seam] = v;
         if (k == npm - 1) q[rr - seam] = v;
       }
-    });
+    };
+    quad_march(tid, 1, nk + 6, X, 0, Y2, 1, 1, U, D, CT, st2, c22, c42, s0, st_k);
+    quad_stage(tid, 0, 2, 1, nk + 6, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s0, st_k);
+    quad_stage(tid, 66, 2, 1, nk + 6, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s0, st_k);
     cons_sync();
     // stage k+1 on rows 2..133, columns 2..cend+1, stencil Y_k, over Y_{k-1}
-    quad_stage(tid, 1, kQR / 2 - 2, 2, nk + 4, Y2, 1, X, 0, X, 0, U, D, RT, CT, s1, [&](int r, int c, double2 y) {
+    auto st_k1 = [&](int r, int c, double2 y) {
       // Y_{k+1} at the two edge rows (j0, j0+1 or j0+126, j0+127)
       if (c >= 4 && c < cend && ((elo && r == 4) || (ehi && r == 130))) put(out_k1, r, c, y);
-    });
+    };
+    quad_march(tid, 2, nk + 4, Y2, 1, X, 0, 0, U, D, CT, st2, c22, c42, s1, st_k1);
+    quad_stage(tid, 1, 1, 2, nk + 4, Y2, 1, X, 0, X, 0, U, D, RT, CT, s1, st_k1);
+    quad_stage(tid, 66, 1, 2, nk + 4, Y2, 1, X, 0, X, 0, U, D, RT, CT, s1, st_k1);
     cons_sync();
     // stage k+2 on rows 2..133 (3..132 valid), columns 3..cend, stencil Y_{k+1}, over Y_k
-    quad_stage(tid, 1, kQR / 2 - 2, 3, nk + 2, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s2, [&](int r, int c, double2 y) {
+    auto st_k2 = [&](int r, int c, double2 y) {
       if (c >= 4 && c < cend && r >= 4 && r <= 130) put(out_k2, r, c, y);
-    });
+    };
+    quad_march(tid, 3, nk + 2, X, 0, Y2, 1, 1, U, D, CT, st2, c22, c42, s2, st_k2);
+    quad_stage(tid, 1, 1, 3, nk + 2, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s2, st_k2);
+    quad_stage(tid, 66, 1, 3, nk + 2, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s2, st_k2);
     cons_sync();
-    // stage k+3 on the tile: rows 4..131, columns 4..cend-1, stencil Y_{k+2}, second input Y_{k+1}
-    {
-      const int np = kQJ / 2, nc = nk, ntot = np * nc;
-      for (int e = tid; e < ntot; e += kQCons) {
-        const int r = 4 + 2 * (e % np), c = 4 + e / np;
-        const double *s = Y2 + (c - 1) * kQR + r;
-        const double2 xl = *reinterpret_cast<const double2 *>(s - kQR);
-        const double2 xc = *reinterpret_cast<const double2 *>(s);
-        const double2 xr = *reinterpret_cast<const double2 *>(s + kQR);
-        const double up = s[-1], dn = s[2];
-        const double2 st2 = *reinterpret_cast<const double2 *>(RT + r);
-        const double2 c22 = *reinterpret_cast<const double2 *>(RT + kQR + r);
-        const double2 c42 = *reinterpret_cast<const double2 *>(RT + 2 * kQR + r);
-        const double2 o2 = *reinterpret_cast<const double2 *>(X + c * kQR + r);
-        const double2 u = *reinterpret_cast<const double2 *>(U + (c - 1) * kQR + r);
-        const double2 d = *reinterpret_cast<const double2 *>(D + (c - 1) * kQR + r);
-        const double2 y =
-            pair_rows_step(xl, xc, xr, up, dn, st2, c22, c42, CT[c], false, false, 0.0, 0.0, o2, u, d, s3);
-        put(out_k3, r, c, y);
-      }
-    }
+    // stage k+3 on the tile: rows 4..131, columns 4..cend-1, stencil Y_{k+2},
+    // second input Y_{k+1} (the shared copy of Y_{k+3} is not read again)
+    quad_march(tid, 4, nk, Y2, 1, X, 0, 0, U, D, CT, st2, c22, c42, s3,
+               [&](int r, int c, double2 y) { put(out_k3, r, c, y); });
     cons_sync();               // all reads of the buffer are done
     mbar_arrive(empty);        // the producer may refill it
   }

@@ -143,6 +143,7 @@ SIGNATURES = [
     ("hipft_adj_assimilate", ctypes.c_int, [_H, DPTR, ctypes.POINTER(DAOpts), ctypes.c_void_p]),
     ("hipft_gpu_describe", ctypes.c_int, [_H, ctypes.c_char_p, ctypes.c_size_t]),
     ("hipft_gpu_set_ragged", ctypes.c_int, [_H, ctypes.c_int]),
+    ("hipft_gpu_set_graph", ctypes.c_int, [_H, ctypes.c_int]),
     ("hipft_gpu_flow_dtmax_each", ctypes.c_int, [_H, DPTR]),
     ("hipft_gpu_ragged_schedule", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                                  ctypes.POINTER(ctypes.c_int64), DPTR]),
@@ -358,6 +359,12 @@ class HipftGPU:
         """Ragged batching: each realization keeps the schedule it would have
         alone (Euler limit, PTL subcycles, stage counts, advection substeps)."""
         self._ck(self.L.hipft_gpu_set_ragged(self.h, int(on)), "set_ragged")
+
+    def set_graph(self, on: bool = True):
+        """Run every flux_transport_step as one launch of a captured CUDA graph
+        whose loops (subcycles, stage pairs, advection substeps) are sized on
+        the device; same field, bit for bit, as the host-driven step."""
+        self._ck(self.L.hipft_gpu_set_graph(self.h, int(on)), "set_graph")
 
     def ragged_schedule(self) -> dict:
         """Per-realization schedule of the last ragged step."""

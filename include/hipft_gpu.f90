@@ -245,6 +245,12 @@ module hipft_gpu_c
       type(c_ptr), value :: h
       integer(c_int), value :: on
     end function
+    ! ---- each step as one CUDA-graph launch (no reference counterpart)
+    integer(c_int) function hipft_gpu_set_graph(h, on) bind(c, name="hipft_gpu_set_graph")
+      import :: c_int, c_ptr
+      type(c_ptr), value :: h
+      integer(c_int), value :: on
+    end function
     integer(c_int) function hipft_gpu_flow_dtmax_each(h, dtmax) bind(c, name="hipft_gpu_flow_dtmax_each")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: h

@@ -309,6 +309,22 @@ int hipft_gpu_flow_dtmax_each(hipft_gpu *h, double *dtmax);
 int hipft_gpu_ragged_schedule(hipft_gpu *h, int64_t *sts_s, int64_t *subcycles, int64_t *adv_substeps,
                               double *dt_euler);
 
+/* on = 1: every hipft_gpu_flux_transport_step runs as ONE launch of a CUDA
+ * graph captured on the first such step (and again when flows, tables or
+ * modes it baked in change).  No counterpart in the reference, whose step
+ * (flux_transport_step, src/hipft.f90:4463-4507) is a host loop over kernels.
+ * The decisions the host-driven step takes between launches -- PTL subcycle
+ * lengths (get_dtime_diffusion_ptl, 5042-5161), RKG2/RKL2 stage counts and
+ * coefficients (5244-5475), advection substeps of ragged batches -- are taken
+ * by device kernels with the same arithmetic, and the loops they size are
+ * conditional WHILE nodes, so a graph-run step gives the same field, bit for
+ * bit, as the host-driven step, in plain and in ragged mode.  The step then
+ * needs no host synchronization (unless an info struct is passed).  Needs
+ * RKG2 or RKL2 with per-realization constant coefficients (or no diffusion),
+ * no sources and no all-reduce callback (else HIPFT_EINVAL / HIPFT_ESTATE);
+ * flux_transport_step with a cycle callback returns HIPFT_ESTATE. */
+int hipft_gpu_set_graph(hipft_gpu *h, int on);
+
 /* ---- allocation-free flux integral ------------------------------------------ */
 
 /* No counterpart in the reference: get_flux (src/hipft.f90:8672) for callers

@@ -185,11 +185,13 @@ def _cfl_rank(prm, t):
 @pytest.mark.slow
 def test_config_batched64_two_steps_across_assimilation(tmp_path):
     """64 realizations (seed 1) on 1024 x 2048 refined with synthetic observed
-    maps (mu^4 weights, mu > 0.1) at 0 h and 1 h, to 2.5 h.  As in the
+    maps (mu^4 weights, mu > 0.1) at 0 h and 1.5 h, to 2.5 h.  As in the
     reference (load_data_assimilation, src/hipft.f90:4010-4042), a map at the
     start time makes the first step zero-length, so the run takes three steps:
-    0 h (assimilate map 0), 0 -> 1 h (assimilate map 1), 1 -> 2.5 h.  The
-    oracle runs the schedule-setting realizations and two others."""
+    0 h (assimilate map 0), 0 -> 1.5 h (assimilate map 1), 1.5 -> 2.5 h.  The
+    map list holds Julian dates to five decimals; 1.5 h (1/16 day) is exact
+    there, so the oracle's map times equal the driver's.  The oracle runs the
+    schedule-setting realizations and two others."""
     import hipft_b200 as H
     from hipft_b200 import synthetic as S
     nr = 64
@@ -200,7 +202,8 @@ def test_config_batched64_two_steps_across_assimilation(tmp_path):
     write_map(tmp_path / "map.h5", t, p, br)
     (tmp_path / "da").mkdir()
     jd0 = 2459580.5
-    jds = [jd0, jd0 + 1.0 / 24.0]
+    jds = [jd0, jd0 + 0.0625]
+    dates = ["2022-01-01T00:00:00", "2022-01-01T01:30:00"]
     maps = []
     rows = ["target_datetime_utc,obs_datetime_utc,obs_jd,path"]
     for q, jd in enumerate(jds):
@@ -208,8 +211,7 @@ def test_config_batched64_two_steps_across_assimilation(tmp_path):
         name = f"obs_{q:03d}.h5"
         H.h5_write(str(tmp_path / "da" / name), slab, [p, t, np.arange(1.0, 4.0)], single_precision=False)
         maps.append(slab)
-        date = f"2022-01-01T{q:02d}:00:00"
-        rows.append(f"{date} {date} {jd:13.5f} {name}")
+        rows.append(f"{dates[q]} {dates[q]} {jd:13.5f} {name}")
     (tmp_path / "da" / "map_list.csv").write_text("\n".join(rows) + "\n")
     da = dict(assimilate_data=True, assimilate_data_map_list_filename="da/map_list.csv",
               assimilate_data_map_root_dir="da", assimilate_data_custom_from_mu=True,
