@@ -10,18 +10,20 @@ no adjoint; the forward operators are diffusion_operator_cd
 (src/hipft.f90:7927-7990) and advection_operator_weno3 (src/hipft.f90:
 7711-7925) inside flux_transport_step (src/hipft.f90:4463-4507).
 
-Method.  The forward run goes through the library's own fused step
-(hipft_gpu_flux_transport_step) and keeps the field every
-`checkpoint_every` steps on the device, and every step input of the last
-segment.  The reverse pass walks the checkpoint segments backwards: it
-recomputes a segment's step inputs from its checkpoint (all but the last
-segment), then, step by step from the last, calls hipft_adj_step,
-which replays that one step with every stage input kept and runs the
-hand-written adjoint kernels (csrc/adjoint.cuh: transposed Laplacian with its
-pole rings and seam, WENO3 face derivatives including the nonlinear weights,
-the SSPRK(4,3) and RKG2 stage recurrences run backwards).  The schedule
-(step dts, PTL subcycle dts, RKG2 stage counts) is the forward's and is held
-fixed: the result is the gradient of the discrete map at that schedule.
+Method.  The forward run keeps the field every `checkpoint_every` steps on
+the device and tapes the steps of the last segment as it runs them
+(hipft_adj_record: the library's own step, the same bits as
+hipft_gpu_flux_transport_step, with every stage input kept on a tape stack).
+The reverse pass walks the segments backwards: a segment other than the last
+is recomputed once from its checkpoint, taped; then its steps are reversed
+from the last (hipft_adj_reverse: the hand-written adjoint kernels of
+csrc/adjoint.cuh -- transposed Laplacian with its pole rings and seam, WENO3
+face derivatives including the nonlinear weights, the SSPRK(4,3) and RKG2
+stage recurrences run backwards).  Steps for which the device has no room
+left keep their input field instead and are taped one at a time in the
+reverse pass.  The schedule (step dts, PTL subcycle dts, RKG2 stage counts)
+is the forward's and is held fixed: the result is the gradient of the
+discrete map at that schedule.
 
 Flow cotangents come back per cell from the kernels; the reduction to the
 1-D profiles and the chain through the LLF alpha (max of |v| over the
@@ -158,13 +160,14 @@ class MisfitAdjoint:
     by hipft_adj_assimilate (blend and additive forms; not the balanced
     increment).
 
-    Device memory: one field per checkpoint (every `checkpoint_every` steps),
-    the inputs of the last segment's steps (at most checkpoint_every - 1 more
-    fields), and the tape of one step inside hipft_adj_step (bounded by
-    hipft_adj_set_tape_limit; freed by release())."""
+    Device memory: one field per checkpoint (every `checkpoint_every` steps)
+    and the tapes of one segment's steps, as many as fit while
+    `reserve_frac` of the device memory stays free (the other steps of the
+    segment keep one input field each); each step's tape is bounded by
+    hipft_adj_set_tape_limit; release() frees the tape."""
 
     def __init__(self, gpu: HipftGPU, D: Sequence[float], flow: dict, checkpoint_every: int = 64,
-                 assim: dict | None = None):
+                 assim: dict | None = None, reserve_frac: float = 0.15):
         import torch
         if not torch.cuda.is_available():
             raise RuntimeError("the adjoint runs on the GPU (libhipft_gpu); no CUDA device is visible")
@@ -179,6 +182,9 @@ class MisfitAdjoint:
         self.w = misfit_weights(self.mesh)
         self.timing = {}
         self._fwd = None
+        self.reserve_frac = float(reserve_frac)
+        self._fbytes = 0
+        self._est_fields = 16
 
     def _dev(self):
         return self.gpu.field_tensor()
@@ -208,27 +214,68 @@ class MisfitAdjoint:
         g = self.w[None] * r
         return loss, fold_cotangent(g)
 
+    # -- taping: a recorded step is a forward step whose tape stays on the
+    # library's stack until its reverse; a segment is recorded while the
+    # device has room for it (beyond `reserve_frac` of its memory) and its
+    # remaining steps keep their input fields instead, to be recorded one at a
+    # time in the reverse pass.
+    def _recorded(self):
+        n, used = ctypes.c_int64(0), ctypes.c_int64(0)
+        self.gpu._ck(self.gpu.L.hipft_adj_recorded(self.gpu.h, ctypes.byref(n), ctypes.byref(used)),
+                     "hipft_adj_recorded")
+        return n.value, used.value
+
+    def _tape_fields(self):
+        n = ctypes.c_int64(0)
+        self.gpu._ck(self.gpu.L.hipft_adj_tape_fields(self.gpu.h, ctypes.byref(n)), "hipft_adj_tape_fields")
+        return n.value
+
+    def _room_to_record(self) -> bool:
+        import torch
+        free, total = torch.cuda.mem_get_info()
+        _, used = self._recorded()
+        spare = max(0, self._tape_fields() - used) * self._fbytes  # allocated, unused tape slots
+        return free + spare - self._est_fields * self._fbytes > self.reserve_frac * total
+
+    def _record(self, s: int, dt: float):
+        _, u0 = self._recorded()
+        self.gpu._ck(self.gpu.L.hipft_adj_record(self.gpu.h, float(dt)), "hipft_adj_record")
+        _, u1 = self._recorded()
+        self._est_fields = max(self._est_fields, u1 - u0)
+        if s in self.assim:
+            m3, opts = self.assim[s]
+            self.gpu.assimilate(m3, **opts)
+
     def forward(self, f0: np.ndarray, dts: Sequence[float]) -> np.ndarray:
-        """The forward run with its checkpoints; returns f_N (nr, npm, ntm)."""
+        """The forward run with its checkpoints, the last segment taped;
+        returns f_N (nr, npm, ntm)."""
         import torch
         g = self.gpu
         dts = [float(d) for d in dts]
         n = len(dts)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        g._ck(g.L.hipft_adj_clear(g.h), "hipft_adj_clear")  # steps left by an earlier run; the tape memory stays
         g.set_field(f0)
         g.update_flow()
-        ckpt = {}
-        last0 = ((n - 1) // self.k) * self.k  # the last segment's inputs are kept, not recomputed
-        kept = []
+        self._fbytes = self._dev().numel() * 8
+        self._est_fields = 16
+        ckpt, recorded, states = {}, set(), {}
+        last0 = ((n - 1) // self.k) * self.k
+        taping = True
         for s, dt in enumerate(dts):
             if s % self.k == 0:
                 ckpt[s] = self._dev().clone()
+            if s >= last0 and taping and self._room_to_record():
+                self._record(s, dt)
+                recorded.add(s)
+                continue
             if s >= last0:
-                kept.append(ckpt[s] if s == last0 else self._dev().clone())
+                taping = False
+                states[s] = self._dev().clone()
             self._step(s, dt)
         fN = g.get_field()
-        self._fwd = dict(dts=dts, ckpt=ckpt, kept=kept, last0=last0)
+        self._fwd = dict(dts=dts, ckpt=ckpt, recorded=recorded, states=states, last0=last0)
         self.timing = {"forward_s": time.perf_counter() - t0}
         return fN
 
@@ -241,7 +288,7 @@ class MisfitAdjoint:
         if self._fwd is None:
             raise RuntimeError("backward() needs a forward() first")
         g = self.gpu
-        dts, ckpt, kept, last0 = (self._fwd[k] for k in ("dts", "ckpt", "kept", "last0"))
+        dts, ckpt, last0 = (self._fwd[k] for k in ("dts", "ckpt", "last0"))
         n = len(dts)
         t1 = time.perf_counter()
         ldt = self._dev().shape[-1]
@@ -251,33 +298,47 @@ class MisfitAdjoint:
         fbar[:, 1:self.npm - 1, :self.ntm] = gbt[:, 1:self.npm - 1]
         dacc = torch.zeros(self.nr, dtype=torch.float64, device=dev)
         gflow = torch.zeros((5, self.nr, self.npm, ldt), dtype=torch.float64, device=dev)
+        ptr = lambda x: ctypes.c_void_p(x.data_ptr())
         for s0 in sorted(ckpt, reverse=True):
             s1 = min(s0 + self.k, n)
-            states = kept if s0 == last0 else [ckpt[s0]]
-            if s0 != last0 and s1 - s0 > 1:
+            if s0 == last0:
+                recorded, states = self._fwd["recorded"], self._fwd["states"]
+            else:
+                # recompute the segment from its checkpoint, taped while there is room
+                recorded, states = set(), {}
                 self._set(ckpt[s0])
-                for s in range(s0, s1 - 1):
-                    self._step(s, dts[s])
-                    states.append(self._dev().clone())
+                taping = True
+                for s in range(s0, s1):
+                    if taping and self._room_to_record():
+                        self._record(s, dts[s])
+                        recorded.add(s)
+                        continue
+                    taping = False
+                    states[s] = self._dev().clone()
+                    if s < s1 - 1:
+                        self._step(s, dts[s])
             for s in range(s1 - 1, s0 - 1, -1):
                 if s in self.assim:
                     m3, opts = self.assim[s]
                     o, keep = self._da_opts(opts)
                     m3 = np.ascontiguousarray(m3, dtype=np.float64)
                     g._ck(g.L.hipft_adj_assimilate(g.h, m3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                                   ctypes.byref(o), ctypes.c_void_p(fbar.data_ptr())),
-                          "hipft_adj_assimilate")
-                rc = g.L.hipft_adj_step(g.h, dts[s], ctypes.c_void_p(states[s - s0].data_ptr()),
-                                        ctypes.c_void_p(fbar.data_ptr()), ctypes.c_void_p(dacc.data_ptr()),
-                                        ctypes.c_void_p(gflow.data_ptr()))
-                g._ck(rc, "hipft_adj_step")
+                                                   ctypes.byref(o), ptr(fbar)), "hipft_adj_assimilate")
+                if s not in recorded:
+                    self._set(states.pop(s))
+                    g._ck(g.L.hipft_adj_record(g.h, float(dts[s])), "hipft_adj_record")
+                g._ck(g.L.hipft_adj_reverse(g.h, ptr(fbar), ptr(dacc), ptr(gflow)), "hipft_adj_reverse")
         torch.cuda.synchronize()
+        nrec, _ = self._recorded()
+        if nrec:
+            raise RuntimeError(f"adjoint: {nrec} recorded steps left after the reverse pass")
         grads = {"f0": fbar[:, :, :self.ntm].cpu().numpy().copy()}
         grads["f0"][:, 0] = 0.0
         grads["f0"][:, self.npm - 1] = 0.0
         grads["D"] = dacc.cpu().numpy() / self.D
         grads.update(self._flow_grads(gflow))
         self.timing["reverse_s"] = time.perf_counter() - t1
+        self._fwd = None
         return grads
 
     def run(self, f0: np.ndarray, target: np.ndarray, dts: Sequence[float]) -> tuple:
@@ -339,7 +400,7 @@ class FluxTransport:
         loss = ((fN - target) ** 2 * w).sum(); loss.backward()
 
     The forward runs the CUDA library (WENO3 + SSPRK(4,3) Strang-split with
-    RKG2); backward runs its hand-written adjoint (hipft_adj_step,
+    RKG2); backward runs its hand-written adjoint (hipft_adj_reverse,
     hipft_adj_assimilate) through MisfitAdjoint.backward.  f0 must be periodic
     (columns 1, npm copy columns npm-1, 2), as the reference's fields are; its
     gradient is folded onto the core columns.  Handle options (diffusion

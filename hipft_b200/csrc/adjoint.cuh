@@ -345,20 +345,21 @@ __global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const do
   }
 }
 
-// Stage k-1 at rows 1, 2, ntm-1, ntm (after k_adj_diff2), one block per
-// realization: W_{k-1}'s pole sums from the tiles' partials (fixed order),
-// W_{k-2} = a2 W_{k-1} + b2 W_k + c2 A^T W_{k-1} there, the D partials of
-// those rows (added to the realization's first block slot), and the pole sums
-// of W_{k-2} for the next launch (gout[(i-1)][0..1], one partial).
+// Stage k-1 at rows 1, 2, ntm-1, ntm (after k_adj_diff2); grid (realization,
+// chunk of blockDim.x phi columns): W_{k-1}'s pole sums from the tiles'
+// partials (fixed order, the same in every block), W_{k-2} = a2 W_{k-1} +
+// b2 W_k + c2 A^T W_{k-1} there, the chunk's D partials of those rows (added
+// to its own slot of dpole), and the chunk's partial pole sums of W_{k-2} for
+// the next launch (gout[(i-1)][chunk][0..1]; the consumer sums the chunks in
+// order).
 __global__ void __launch_bounds__(256) k_adj_pole2(Mesh m, DiffCoef dc, const double *__restrict__ w,
                                                    const double *__restrict__ wm1, const double *__restrict__ y2,
                                                    double *out2, const double *__restrict__ gpart, int npart,
                                                    double *__restrict__ gout, double bcn, double bcs,
-                                                   AdjDiff2Coef ac, double *__restrict__ dpart, int dpart_per_r,
-                                                   PairTables pt) {
+                                                   AdjDiff2Coef ac, double *__restrict__ dpole, PairTables pt) {
   __shared__ double sh[64];
   __shared__ double s_g[2];
-  const int i = blockIdx.x + 1, tid = threadIdx.x, ntm = m.ntm;
+  const int i = blockIdx.x + 1, ch = blockIdx.y, nch = gridDim.y, tid = threadIdx.x, ntm = m.ntm;
   if (tid < 32) {
     double a = 0.0, b = 0.0;
     const double *g = gpart + (int64_t)(i - 1) * npart * 2;
@@ -379,7 +380,7 @@ __global__ void __launch_bounds__(256) k_adj_pole2(Mesh m, DiffCoef dc, const do
   __syncthreads();
   const double gn = s_g[0], gs = s_g[1];
   double dsum = 0.0, pn = 0.0, ps = 0.0;
-  for (int k = 2 + tid; k <= m.npm - 1; k += blockDim.x) {
+  for (int k = 2 + ch * blockDim.x + tid; k <= m.npm - 1; k += nch * blockDim.x) {
     for (int q = 0; q < 4; ++q) {
       const int j = (q == 0) ? 1 : ((q == 1) ? 2 : ((q == 2) ? ntm - 1 : ntm));
       const double aw = adj_diff_at_tab(m, dc, pt, wm1, j, k, i, gn, gs, bcn, bcs);
@@ -393,13 +394,13 @@ __global__ void __launch_bounds__(256) k_adj_pole2(Mesh m, DiffCoef dc, const do
   }
   block_sum2(pn, ps, sh);
   if (tid == 0) {
-    gout[2 * (i - 1)] = pn;
-    gout[2 * (i - 1) + 1] = ps;
+    gout[((int64_t)(i - 1) * nch + ch) * 2] = pn;
+    gout[((int64_t)(i - 1) * nch + ch) * 2 + 1] = ps;
   }
-  if (dpart) {
+  if (dpole) {
     double z = 0.0;
     block_sum2(dsum, z, sh);
-    if (tid == 0) dpart[(int64_t)(i - 1) * dpart_per_r] += dsum;
+    if (tid == 0) dpole[(int64_t)(i - 1) * nch + ch] += dsum;
   }
 }
 
@@ -417,13 +418,17 @@ __global__ void k_adj_da(Mesh m, DAArgs a, double *fbar) {
   fbar[q] = (kOne - w) * fbar[q];
 }
 
-// dacc[i] += scale * (sum of realization i's block partials), fixed order.
-__global__ void k_adj_dsum(const double *__restrict__ dpart, int nblk, double scale, double *dacc) {
+// dacc[i] += scale * (sum of realization i's block partials and pole-row
+// chunk partials), fixed order.
+__global__ void k_adj_dsum(const double *__restrict__ dpart, int nblk, const double *__restrict__ dpole, int nch,
+                           double scale, double *dacc) {
   __shared__ double sh[64];
   const int i = blockIdx.x;
   double a = 0.0, b = 0.0;
   for (int q = threadIdx.x; q < nblk; q += blockDim.x) a = a + dpart[(int64_t)i * nblk + q];
+  for (int q = threadIdx.x; q < nch; q += blockDim.x) b = b + dpole[(int64_t)i * nch + q];
   block_sum2(a, b, sh);
+  a = a + b;
   if (threadIdx.x == 0) dacc[i] += scale * a;
 }
 

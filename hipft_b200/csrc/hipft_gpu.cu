@@ -64,6 +64,36 @@ double pow5(double c) { return c * c * c * c * c; }
 
 }  // namespace
 
+// ------------------------------------------------------------- adjoint tape
+namespace {
+// One RKG2 super-step of the replay.  With q == 0 the tape holds every stage:
+// slots t0 = u0, t0+1 = dty0, t0+1+k = Y_k (k = 1..s-1).  With stage
+// checkpoints (q > 0, even) it holds u0, dty0 and, for each block start
+// c = 1, 1+q, 1+2q, ... (odd, the output of a stage pair), the pair
+// (Y_{c-1}, Y_c) in slots t0+2+2b, t0+3+2b (b = block index; Y_0 = u0 is
+// not stored twice) and the pole-ring sums of Y_c; the reverse pass
+// recomputes the stages of one block at a time from its pair.
+struct AdjSub {
+  double dtl;
+  int64_t s;
+  std::vector<double> uj, vj, ubj, gj;
+  size_t t0;
+  int64_t q = 0;
+  std::vector<int64_t> cstart;        // block starts c
+  std::vector<size_t> ck_prev, ck_cur;  // tape slots of Y_{c-1} (SIZE_MAX: u0) and Y_c
+  size_t ring0 = 0;                   // first ring-checkpoint slot (2*nr doubles each)
+};
+
+// One taped (recorded) flux_transport_step: its tape slots sit on the tape's
+// stack from `first`, its ring checkpoints from `ring_first`.
+struct AdjRec {
+  double dt = 0.0;
+  size_t first = 0, ring_first = 0;
+  size_t ta1[4] = {}, ta2[4] = {};  // SSPRK(4,3) stage inputs of the advection calls
+  std::vector<AdjSub> subs;         // RKG2 super-steps
+};
+}  // namespace
+
 struct hipft_gpu {
   int dev = 0;
   cudaStream_t stream = nullptr;
@@ -129,7 +159,11 @@ struct hipft_gpu {
   bool q_rt_ok = false;
   // adjoint: fields of one taped forward step, folded work fields (seam
   // columns stay zero), per-block partial sums and pole sums
-  std::vector<double *> tape;
+  std::vector<double *> tape;             // tape slots (allocated in chunks, see adj_slot)
+  std::vector<void *> tape_chunks;
+  size_t adj_top = 0;                     // first free tape slot (recorded steps sit below, a stack)
+  size_t adj_top_max = 0;                 // most tape slots in use at once since the last release
+  std::vector<AdjRec> adj_recs;           // recorded steps, oldest first
   std::vector<double *> adj_block;        // stage fields of one recomputed block
   double *d_adj_rings = nullptr;          // ring sums of the stage checkpoints
   size_t adj_rings_cap = 0, adj_rings_n = 0;
@@ -137,6 +171,8 @@ struct hipft_gpu {
   int64_t adj_force_q = 0;                // stage-checkpoint spacing forced by the caller (0: automatic)
   double *adjw[8] = {};
   double *d_dpart = nullptr, *d_gring = nullptr, *d_gpart[2] = {};
+  double *d_dpole = nullptr;  // [nr][adj_nch] D partials of the pole-row chunks
+  int adj_nch = 1;            // phi-column chunks of k_adj_pole2
   int dpart_per_r = 0;
   // ragged batches: every realization keeps the schedule it would have if run
   // alone (Euler limit, CFL substeps, PTL subcycles, stage counts)
@@ -822,7 +858,7 @@ static int quad_launch(hipft_gpu *h, const double *ykm1, const double *ykm2, con
     qm.on = 1;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)std::min(qa.ntiles, 2 * h->num_sms));
+  cfg.gridDim = dim3((unsigned)std::min(qa.ntiles, h->num_sms));  // one CTA (two tile buffers) per SM
   cfg.blockDim = dim3(kQThreads);
   cfg.dynamicSmemBytes = kQSmem;
   cfg.stream = h->stream;
@@ -3406,25 +3442,7 @@ extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, in
 // computed by the same routines from the same field, and is held fixed:
 // the gradient is that of the discrete map at this schedule.
 
-namespace {
-// One RKG2 super-step of the replay.  With q == 0 the tape holds every stage:
-// slots t0 = u0, t0+1 = dty0, t0+1+k = Y_k (k = 1..s-1).  With stage
-// checkpoints (q > 0, even) it holds u0, dty0 and, for each block start
-// c = 1, 1+q, 1+2q, ... (odd, the output of a stage pair), the pair
-// (Y_{c-1}, Y_c) in slots t0+2+2b, t0+3+2b (b = block index; Y_0 = u0 is
-// not stored twice) and the pole-ring sums of Y_c; the reverse pass
-// recomputes the stages of one block at a time from its pair.
-struct AdjSub {
-  double dtl;
-  int64_t s;
-  std::vector<double> uj, vj, ubj, gj;
-  size_t t0;
-  int64_t q = 0;
-  std::vector<int64_t> cstart;        // block starts c
-  std::vector<size_t> ck_prev, ck_cur;  // tape slots of Y_{c-1} (SIZE_MAX: u0) and Y_c
-  size_t ring0 = 0;                   // first ring-checkpoint slot (2*nr doubles each)
-};
-}  // namespace
+
 
 // Stage spacing of the stage checkpoints for a super-step of s stages:
 // 0 (keep every stage) when s + 1 fields fit the tape budget, else an even
@@ -3443,11 +3461,16 @@ static int64_t adj_stage_spacing(hipft_gpu *h, int64_t s) {
   return std::max<int64_t>(q, 2);
 }
 
+// Tape slot n; slots are allocated in chunks of up to 32 fields (at most
+// 256 MB per chunk), so that taping many steps needs few allocations.
 static int adj_slot(hipft_gpu *h, size_t n, double **p) {
   while (h->tape.size() <= n) {
+    const size_t fb = h->fieldn * sizeof(double);
+    const size_t per = std::max<size_t>(1, std::min<size_t>(32, (size_t)(256u << 20) / fb));
     double *q = nullptr;
-    TRY(dalloc(h, &q, h->fieldn));
-    h->tape.push_back(q);
+    TRY(dalloc(h, &q, h->fieldn * per));
+    h->tape_chunks.push_back(q);
+    for (size_t e = 0; e < per; ++e) h->tape.push_back(q + e * h->fieldn);
   }
   *p = h->tape[n];
   return HIPFT_OK;
@@ -3462,7 +3485,9 @@ static int adj_ensure(hipft_gpu *h) {
   dim3 g = stage_grid(h, 32, 8);
   h->dpart_per_r = (int)(g.x * g.y);
   TRY(dalloc(h, &h->d_dpart, (size_t)h->dpart_per_r * h->nr));
-  TRY(dalloc(h, &h->d_gring, 2 * (size_t)h->nr));
+  h->adj_nch = (h->npm - 2 + 255) / 256;
+  TRY(dalloc(h, &h->d_gring, 2 * (size_t)h->nr * h->adj_nch));
+  TRY(dalloc(h, &h->d_dpole, (size_t)h->nr * h->adj_nch));
   for (auto &gp : h->d_gpart) TRY(dalloc(h, &gp, 2 * (size_t)g.y * h->nr));
   return HIPFT_OK;
 }
@@ -3702,6 +3727,7 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   CK(h, cudaMemsetAsync(ub, 0, h->fieldn * sizeof(double), h->stream));
   CK(h, cudaMemsetAsync(db, 0, h->fieldn * sizeof(double), h->stream));
   CK(h, cudaMemsetAsync(h->d_dpart, 0, (size_t)h->dpart_per_r * h->nr * sizeof(double), h->stream));
+  CK(h, cudaMemsetAsync(h->d_dpole, 0, (size_t)h->adj_nch * h->nr * sizeof(double), h->stream));
   // stage inputs Y_k: all on the tape (q == 0) or one recomputed block at a time
   std::vector<const double *> Yr((size_t)S.s + 1, nullptr);
   Yr[0] = h->tape[S.t0];
@@ -3749,11 +3775,12 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
     k_adj_diff2<<<grd, blk, 0, h->stream>>>(h->M, h->DC, Wk, Wk1, Yt(k - 1), Yt(k - 2), Wm1, Wm2, ub, db, gin, npin,
                                             gpart, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpart, h->ptab);
     LAUNCHED(h);
-    k_adj_pole2<<<h->nr, 256, 0, h->stream>>>(h->M, h->DC, Wk, Wm1, Yt(k - 2), Wm2, gpart, (int)grd.y, h->d_gring,
-                                              h->bc_diff_n, h->bc_diff_s, ac, h->d_dpart, h->dpart_per_r, h->ptab);
+    k_adj_pole2<<<dim3((unsigned)h->nr, (unsigned)h->adj_nch), 256, 0, h->stream>>>(
+        h->M, h->DC, Wk, Wm1, Yt(k - 2), Wm2, gpart, (int)grd.y, h->d_gring, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpole,
+        h->ptab);
     LAUNCHED(h);
     gin = h->d_gring;
-    npin = 1;
+    npin = h->adj_nch;
     pp ^= 1;
     Wk1 = Wm1;
     Wk = Wm2;
@@ -3780,15 +3807,13 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   // dty0 = dt A u0
   TRY(pole_sums(db));
   TRY(stage(db, ub, Yt(0), ub, nullptr, nullptr, AdjDiffCoef{0.0, 1.0, dtl, 0.0, 0.0, dtl}));
-  k_adj_dsum<<<h->nr, 256, 0, h->stream>>>(h->d_dpart, h->dpart_per_r, 1.0, dacc);
+  k_adj_dsum<<<h->nr, 256, 0, h->stream>>>(h->d_dpart, h->dpart_per_r, h->d_dpole, h->adj_nch, 1.0, dacc);
   LAUNCHED(h);
   W = ub;
   return HIPFT_OK;
 }
 
-extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, double *dacc,
-                              double *gflow) {
-  if (!h || !f_in || !fbar || !dacc || !gflow) return HIPFT_EINVAL;
+static int adj_check(hipft_gpu *h) {
   if (!h->field_set) return fail(h, HIPFT_ESTATE, "adjoint step before set_field");
   if (h->P.advance_flow && (h->adv_time != 3 || h->adv_space != 2 || h->FL.flow2d))
     return fail(h, HIPFT_ESTATE, "adjoint: advection must be WENO3+SSPRK(4,3) with analytic flows");
@@ -3796,34 +3821,99 @@ extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, doubl
     return fail(h, HIPFT_ESTATE, "adjoint: diffusion must be RKG2 with per-realization constant coefficients");
   if (h->P.advance_source) return fail(h, HIPFT_ESTATE, "adjoint: sources are not differentiated");
   if (h->ragged) return fail(h, HIPFT_ESTATE, "adjoint: replays the shared (plain) schedule only");
-  CK(h, cudaSetDevice(h->dev));
+  return HIPFT_OK;
+}
+
+// One flux_transport_step of the current field with its tape pushed on the
+// tape stack (the field becomes the step's output).
+static int adj_record(hipft_gpu *h, double dt) {
   TRY(adj_ensure(h));
-  const size_t bytes = h->fieldn * sizeof(double);
-  CK(h, cudaMemcpyAsync(h->buf[h->cur], f_in, bytes, cudaMemcpyDeviceToDevice, h->stream));
   h->dring_valid = false;
-  h->adj_rings_n = 0;
-  size_t nt = 0, ta1[4] = {}, ta2[4] = {};
-  std::vector<AdjSub> subs;
+  AdjRec R;
+  R.dt = dt;
+  R.first = h->adj_top;
+  R.ring_first = h->adj_rings_n;
+  size_t nt = h->adj_top;
   const bool strang = h->P.strang_splitting != 0;
   const double da = strang ? 0.5 * dt : dt;
-  if (h->P.advance_flow) TRY(adj_adv_fwd(h, da, nt, ta1));
-  if (h->P.advance_diffusion) TRY(adj_diff_fwd(h, dt, nt, subs));
-  if (strang && h->P.advance_flow) TRY(adj_adv_fwd(h, da, nt, ta2));
+  if (h->P.advance_flow) TRY(adj_adv_fwd(h, da, nt, R.ta1));
+  if (h->P.advance_diffusion) TRY(adj_diff_fwd(h, dt, nt, R.subs));
+  if (strang && h->P.advance_flow) TRY(adj_adv_fwd(h, da, nt, R.ta2));
+  h->adj_top = nt;
+  h->adj_top_max = std::max(h->adj_top_max, nt);
+  h->adj_recs.push_back(std::move(R));
+  return HIPFT_OK;
+}
+
+// Reverse of the most recently recorded step (popped from the stack).
+static int adj_reverse(hipft_gpu *h, double *fbar, double *dacc, double *gflow) {
+  if (h->adj_recs.empty()) return fail(h, HIPFT_ESTATE, "adjoint reverse: no recorded step");
+  const AdjRec &R = h->adj_recs.back();
+  const size_t bytes = h->fieldn * sizeof(double);
+  const bool strang = h->P.strang_splitting != 0;
+  const double da = strang ? 0.5 * R.dt : R.dt;
   double *W = h->adjw[0];
   CK(h, cudaMemcpyAsync(W, fbar, bytes, cudaMemcpyDeviceToDevice, h->stream));
-  if (strang && h->P.advance_flow) TRY(adj_adv_rev(h, da, ta2, W, gflow));
-  for (size_t q = subs.size(); q-- > 0;) TRY(adj_diff_rev(h, subs[q], W, dacc));
-  if (h->P.advance_flow) TRY(adj_adv_rev(h, da, ta1, W, gflow));
+  if (strang && h->P.advance_flow) TRY(adj_adv_rev(h, da, R.ta2, W, gflow));
+  for (size_t q = R.subs.size(); q-- > 0;) TRY(adj_diff_rev(h, R.subs[q], W, dacc));
+  if (h->P.advance_flow) TRY(adj_adv_rev(h, da, R.ta1, W, gflow));
   CK(h, cudaMemcpyAsync(fbar, W, bytes, cudaMemcpyDeviceToDevice, h->stream));
+  h->adj_top = R.first;
+  h->adj_rings_n = R.ring_first;
+  h->adj_recs.pop_back();
+  h->dring_valid = false;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, double *dacc,
+                              double *gflow) {
+  if (!h || !f_in || !fbar || !dacc || !gflow) return HIPFT_EINVAL;
+  TRY(adj_check(h));
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaMemcpyAsync(h->buf[h->cur], f_in, h->fieldn * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  TRY(adj_record(h, dt));
+  TRY(adj_reverse(h, fbar, dacc, gflow));
   CK(h, cudaStreamSynchronize(h->stream));
   CK(h, cudaGetLastError());
-  h->dring_valid = false;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_record(hipft_gpu *h, double dt) {
+  if (!h) return HIPFT_EINVAL;
+  TRY(adj_check(h));
+  CK(h, cudaSetDevice(h->dev));
+  TRY(adj_record(h, dt));
+  CK(h, cudaGetLastError());
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_reverse(hipft_gpu *h, double *fbar, double *dacc, double *gflow) {
+  if (!h || !fbar || !dacc || !gflow) return HIPFT_EINVAL;
+  CK(h, cudaSetDevice(h->dev));
+  TRY(adj_reverse(h, fbar, dacc, gflow));
+  CK(h, cudaStreamSynchronize(h->stream));
+  CK(h, cudaGetLastError());
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_clear(hipft_gpu *h) {
+  if (!h) return HIPFT_EINVAL;
+  h->adj_recs.clear();
+  h->adj_top = 0;
+  h->adj_rings_n = 0;
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_recorded(hipft_gpu *h, int64_t *n, int64_t *slots_used) {
+  if (!h || !n) return HIPFT_EINVAL;
+  *n = (int64_t)h->adj_recs.size();
+  if (slots_used) *slots_used = (int64_t)h->adj_top;
   return HIPFT_OK;
 }
 
 extern "C" int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n) {
   if (!h || !n) return HIPFT_EINVAL;
-  *n = (int64_t)(h->tape.size() + h->adj_block.size());
+  *n = (int64_t)(h->adj_top_max + h->adj_block.size());
   return HIPFT_OK;
 }
 
@@ -3844,10 +3934,24 @@ extern "C" int hipft_adj_release(hipft_gpu *h) {
     h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
     h->dev_bytes -= h->fieldn * sizeof(double);
   };
-  for (double *q : h->tape) drop(q);
+  {
+    const size_t fb = h->fieldn * sizeof(double);
+    const size_t per = std::max<size_t>(1, std::min<size_t>(32, (size_t)(256u << 20) / fb));
+    for (void *q : h->tape_chunks) {
+      if (!q) continue;
+      cudaFree(q);
+      h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), q), h->allocs.end());
+      h->dev_bytes -= per * fb;
+    }
+  }
   for (double *q : h->adj_block) drop(q);
   h->tape.clear();
+  h->tape_chunks.clear();
   h->adj_block.clear();
+  h->adj_recs.clear();
+  h->adj_top = 0;
+  h->adj_top_max = 0;
+  h->adj_rings_n = 0;
   return HIPFT_OK;
 }
 

@@ -29,10 +29,11 @@
 // Shared row r is theta row j0-4+r (r = 0..135; the stage-k pass also runs
 // the unused rows 0 and 135 so that every row pair starts on a 16-byte
 // boundary); shared column c of Y_{k-1} is phi column k0-4+c (c = 0..23) and
-// column c-1 of the other arrays holds phi column k0-4+c.  One producer warp
-// stages the tiles (five tensor copies and one bulk copy per tile, or one bulk
-// copy per column at the phi seams) and eight consumer warps compute; every
-// wait is bounded and reports through the error flag.
+// column c-1 of the other arrays holds phi column k0-4+c.  One CTA per SM
+// holds two tile buffers: one producer warp stages the next tile (five tensor
+// copies and one bulk copy per tile, or one bulk copy per column at the phi
+// seams) while sixteen consumer warps compute the current one; every wait is
+// bounded and reports through the error flag.
 #pragma once
 
 #include "sts_pair_ws.cuh"
@@ -44,8 +45,9 @@ constexpr int kQK = 16;                  // phi columns per tile
 constexpr int kQR = kQJ + 8;             // shared rows per column (halo 4)
 constexpr int kQX = kQK + 8;             // shared columns of Y_{k-1} (halo 4)
 constexpr int kQI = kQK + 6;             // shared columns of Y_{k-2}, u0, dty0 (halo 3)
-constexpr int kQCons = 256;              // consumer threads
+constexpr int kQCons = 512;              // consumer threads (64 row pairs x 8 column groups)
 constexpr int kQThreads = kQCons + 32;   // + the producer warp
+constexpr int kQNB = 2;                  // tile buffers: the next tile loads while one is computed
 constexpr int kQX1 = 0;                              // Y_{k-1}
 constexpr int kQY2 = al16(kQX1 + kQX * kQR);         // Y_{k-2}
 constexpr int kQU = al16(kQY2 + kQI * kQR);          // u0
@@ -55,11 +57,23 @@ constexpr int kQCT = kQRT + 3 * kQR;                 // columns: {P1, P5} per sh
 constexpr int kQInfo = kQCT + 2 * kQX;               // tile record: (kt, rb, i, nk)
 constexpr int kQInfoCoef = kQInfo + 4;               // ragged batches: the tile's four StageCoef (20 doubles)
 constexpr int kQBuf = al16(kQInfoCoef + 20);
-constexpr size_t kQSmem = (size_t)kQBuf * sizeof(double) + 2 * sizeof(uint64_t);
+constexpr size_t kQSmem = (size_t)kQNB * kQBuf * sizeof(double) + 2 * kQNB * sizeof(uint64_t);
 static_assert(kQX1 % 16 == 0 && kQY2 % 16 == 0 && kQU % 16 == 0 && kQD % 16 == 0 && kQRT % 16 == 0 &&
                   kQCT % 2 == 0 && kQR % 2 == 0,
               "tensor-copy destinations 128-byte aligned, row pairs 16-byte aligned");
-static_assert(2 * (kQSmem + 1024 + 256) <= 228 * 1024, "two CTAs per SM");
+static_assert(kQSmem + 1024 <= 227 * 1024, "two tile buffers in one CTA per SM");
+
+// Barriers of the quad kernel's consumer threads (named barrier 1).
+__device__ __forceinline__ void qcons_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+__device__ __forceinline__ bool qcons_any(bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred q, o;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred o, 1, 512, q;\n selp.u32 %0, 1, 0, o;\n}"
+      : "=r"(r)
+      : "r"((uint32_t)p)
+      : "memory");
+  return r != 0;
+}
 
 // Tensor maps of the quad tiles: fields with boxes of kQR rows x kQX (x1) or
 // kQI (y2, u, d) columns, the row table with kQR x 3.
@@ -152,9 +166,10 @@ __device__ __forceinline__ void quad_march(int tid, int c0, int nc, const double
                                            double *OUT, int ooff, int woff, const double *__restrict__ U,
                                            const double *__restrict__ D, const double2 *__restrict__ CT,
                                            double2 st2, double2 c22, double2 c42, const StageCoef &sc, Store store) {
+  constexpr int NG = kQCons / 64;  // column groups
   const int lane = tid & 31, g = tid >> 6;
   const int r = 4 + 2 * (tid & 63);
-  const int cs = c0 + (g * nc) / 4, ce = c0 + ((g + 1) * nc) / 4;  // columns cs .. ce-1 (warp-uniform)
+  const int cs = c0 + (g * nc) / NG, ce = c0 + ((g + 1) * nc) / NG;  // columns cs .. ce-1 (warp-uniform)
   if (cs >= ce) return;
   double2 xl = *reinterpret_cast<const double2 *>(S + (cs - 1 - soff) * kQR + r);
   double2 xc = *reinterpret_cast<const double2 *>(S + (cs - soff) * kQR + r);
@@ -181,7 +196,7 @@ __device__ __forceinline__ void quad_march(int tid, int c0, int nc, const double
 // the tiles of the realizations in qa.rlist, each with its own coefficients,
 // which the producer copies into the tile record.
 template <bool RAGGED>
-__global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const double *__restrict__ ykm1,
+__global__ void __launch_bounds__(kQThreads, 1) k_sts_quad_ws(Mesh m, const double *__restrict__ ykm1,
                                                              const double *__restrict__ ykm2,
                                                              const double *__restrict__ u0,
                                                              const double *__restrict__ dty0, double *out_k,
@@ -189,14 +204,16 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
                                                              QuadArgs qa, PairTables pt,
                                                              const __grid_constant__ QuadMaps tm) {
   extern __shared__ __align__(128) double qsm[];
-  uint64_t *full = reinterpret_cast<uint64_t *>(qsm + kQBuf);
-  uint64_t *empty = full + 1;
+  uint64_t *full = reinterpret_cast<uint64_t *>(qsm + kQNB * kQBuf);
+  uint64_t *empty = full + kQNB;
   const int tid = threadIdx.x;
   const int npm = m.npm;
   const int64_t ld = m.ldt;
   if (tid == 0) {
-    mbar_init(full, 1);
-    mbar_init(empty, kQCons);
+    for (int b = 0; b < kQNB; ++b) {
+      mbar_init(&full[b], 1);
+      mbar_init(&empty[b], kQCons);
+    }
     fence_mbar_init();
   }
   __syncthreads();
@@ -220,9 +237,11 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
       const int j0 = rb * kQJ + 1, k0 = kt * kQK + 2;
       const int nk = min(kQK, npm - 1 - k0 + 1);
       const int64_t pbase = (int64_t)(i - 1) * m.plane;
-      double *B = qsm;
-      // the single buffer is free once the consumers are done with the last tile
-      if (n >= 1 && !mbar_wait_bounded(empty, (uint32_t)((n - 1) & 1), 1u << 22)) {
+      const int b = n % kQNB, u = n / kQNB;
+      double *B = qsm + b * kQBuf;
+      uint64_t *fb = &full[b];
+      // buffer b is free once the consumers are done with its previous tile
+      if (u >= 1 && !mbar_wait_bounded(&empty[b], (uint32_t)((u - 1) & 1), 1u << 22)) {
         ok = false;
         break;
       }
@@ -244,14 +263,14 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
             C[5 * q + 4] = rc[q].e;
           }
         }
-        mbar_expect_tx(full, (uint32_t)((kQX + 3 * kQI) * kQR * 8 + 3 * kQR * 8 + kQX * 16));
+        mbar_expect_tx(fb, (uint32_t)((kQX + 3 * kQI) * kQR * 8 + 3 * kQR * 8 + kQX * 16));
         if (boxed) {
-          tma_load_3d(B + kQX1, &tm.x1, j0 - 5, k0 - 5, i - 1, full);
-          tma_load_3d(B + kQY2, &tm.y2, j0 - 5, k0 - 4, i - 1, full);
-          tma_load_3d(B + kQU, &tm.u, j0 - 5, k0 - 4, i - 1, full);
-          tma_load_3d(B + kQD, &tm.d, j0 - 5, k0 - 4, i - 1, full);
-          tma_load_3d(B + kQRT, &tm.rt, rb * kQJ - 2, 0, i - 1, full);
-          bulk_load(B + kQCT, qa.col + ((int64_t)(i - 1) * qa.LC + (int64_t)kt * kQK) * 2, kQX * 16, full);
+          tma_load_3d(B + kQX1, &tm.x1, j0 - 5, k0 - 5, i - 1, fb);
+          tma_load_3d(B + kQY2, &tm.y2, j0 - 5, k0 - 4, i - 1, fb);
+          tma_load_3d(B + kQU, &tm.u, j0 - 5, k0 - 4, i - 1, fb);
+          tma_load_3d(B + kQD, &tm.d, j0 - 5, k0 - 4, i - 1, fb);
+          tma_load_3d(B + kQRT, &tm.rt, rb * kQJ - 2, 0, i - 1, fb);
+          bulk_load(B + kQCT, qa.col + ((int64_t)(i - 1) * qa.LC + (int64_t)kt * kQK) * 2, kQX * 16, fb);
         }
       }
       __syncwarp();
@@ -280,13 +299,17 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
             dst = B + kQCT;
             bytes = kQX * 16;
           }
-          bulk_load(dst, src, bytes, full);
+          bulk_load(dst, src, bytes, fb);
         }
       }
     }
     if (!ok && lane == 0) atomicExch(qa.err, 1);
-    // the last tile's copies land before this warp exits
-    if (n >= 1) mbar_wait_bounded(full, (uint32_t)((n - 1) & 1), 1u << 22);
+    // every issued copy lands before this warp exits (tiles 0..n-1 were issued)
+    for (int b = 0; b < kQNB; ++b) {
+      int last = n - 1;
+      while (last >= 0 && last % kQNB != b) --last;
+      if (last >= 0) mbar_wait_bounded(&full[b], (uint32_t)((last / kQNB) & 1), 1u << 22);
+    }
     return;
   }
 
@@ -295,12 +318,13 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
   const int64_t seam = (int64_t)(npm - 2) * ld;
   int n = 0;
   for (int t = blockIdx.x; t < qa.ntiles; t += gridDim.x, ++n) {
-    const bool landed = mbar_wait_bounded(full, (uint32_t)(n & 1), 1u << 22);
-    if (cons_any(!landed)) {
+    const int bq = n % kQNB, uq = n / kQNB;
+    const bool landed = mbar_wait_bounded(&full[bq], (uint32_t)(uq & 1), 1u << 22);
+    if (qcons_any(!landed)) {
       if (tid == 0) atomicExch(qa.err, 1);
       break;
     }
-    double *B = qsm;
+    double *B = qsm + bq * kQBuf;
     const int *Ii = reinterpret_cast<const int *>(B + kQInfo);
     const int kt = Ii[0], rb = Ii[1], i = Ii[2], nk = Ii[3];
     if (RAGGED) {
@@ -347,7 +371,7 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
     quad_march(tid, 1, nk + 6, X, 0, Y2, 1, 1, U, D, CT, st2, c22, c42, s0, st_k);
     quad_stage(tid, 0, 2, 1, nk + 6, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s0, st_k);
     quad_stage(tid, 66, 2, 1, nk + 6, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s0, st_k);
-    cons_sync();
+    qcons_sync();
     // stage k+1 on rows 2..133, columns 2..cend+1, stencil Y_k, over Y_{k-1}
     auto st_k1 = [&](int r, int c, double2 y) {
       // Y_{k+1} at the two edge rows (j0, j0+1 or j0+126, j0+127)
@@ -356,7 +380,7 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
     quad_march(tid, 2, nk + 4, Y2, 1, X, 0, 0, U, D, CT, st2, c22, c42, s1, st_k1);
     quad_stage(tid, 1, 1, 2, nk + 4, Y2, 1, X, 0, X, 0, U, D, RT, CT, s1, st_k1);
     quad_stage(tid, 66, 1, 2, nk + 4, Y2, 1, X, 0, X, 0, U, D, RT, CT, s1, st_k1);
-    cons_sync();
+    qcons_sync();
     // stage k+2 on rows 2..133 (3..132 valid), columns 3..cend, stencil Y_{k+1}, over Y_k
     auto st_k2 = [&](int r, int c, double2 y) {
       if (c >= 4 && c < cend && r >= 4 && r <= 130) put(out_k2, r, c, y);
@@ -364,13 +388,13 @@ __global__ void __launch_bounds__(kQThreads, 2) k_sts_quad_ws(Mesh m, const doub
     quad_march(tid, 3, nk + 2, X, 0, Y2, 1, 1, U, D, CT, st2, c22, c42, s2, st_k2);
     quad_stage(tid, 1, 1, 3, nk + 2, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s2, st_k2);
     quad_stage(tid, 66, 1, 3, nk + 2, X, 0, Y2, 1, Y2, 1, U, D, RT, CT, s2, st_k2);
-    cons_sync();
+    qcons_sync();
     // stage k+3 on the tile: rows 4..131, columns 4..cend-1, stencil Y_{k+2},
     // second input Y_{k+1} (the shared copy of Y_{k+3} is not read again)
     quad_march(tid, 4, nk, Y2, 1, X, 0, 0, U, D, CT, st2, c22, c42, s3,
                [&](int r, int c, double2 y) { put(out_k3, r, c, y); });
-    cons_sync();               // all reads of the buffer are done
-    mbar_arrive(empty);        // the producer may refill it
+    qcons_sync();              // all reads of the buffer are done
+    mbar_arrive(&empty[bq]);   // the producer may refill it
   }
 }
 

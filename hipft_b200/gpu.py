@@ -129,6 +129,10 @@ SIGNATURES = [
                                       ctypes.c_void_p]),
     ("hipft_gpu_set_field_device", ctypes.c_int, [_H, ctypes.c_void_p]),
     ("hipft_adj_tape_fields", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64)]),
+    ("hipft_adj_record", ctypes.c_int, [_H, ctypes.c_double]),
+    ("hipft_adj_reverse", ctypes.c_int, [_H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    ("hipft_adj_recorded", ctypes.c_int, [_H, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+    ("hipft_adj_clear", ctypes.c_int, [_H]),
     ("hipft_run_shard", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(Shard), DPTR,
                                        ctypes.c_size_t]),
     ("hipft_gpu_set_source_file", ctypes.c_int, [_H, DPTR]),

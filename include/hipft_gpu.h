@@ -395,13 +395,29 @@ int hipft_run_shard(const char *namelist_path, const char *run_dir, int device, 
  * constant diffusion coefficients and no sources (else HIPFT_ESTATE).  The
  * current field becomes the step's output. */
 int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, double *dacc, double *gflow);
+/* hipft_adj_step in two halves, for checkpoint segments that are taped once:
+ * hipft_adj_record runs one flux_transport_step of the current field (the
+ * field becomes its output, as with hipft_gpu_flux_transport_step, bit for
+ * bit) and pushes the step's tape onto a stack; hipft_adj_reverse runs the
+ * reverse pass of the most recently recorded step (same fbar, dacc, gflow
+ * arguments as hipft_adj_step) and pops its tape.  A segment of n steps is
+ * recorded in order and reversed in the opposite order; hipft_adj_recorded
+ * gives the number of steps on the stack and (slots_used may be NULL) the
+ * tape fields they hold. */
+int hipft_adj_record(hipft_gpu *h, double dt);
+int hipft_adj_reverse(hipft_gpu *h, double *fbar, double *dacc, double *gflow);
+int hipft_adj_recorded(hipft_gpu *h, int64_t *n, int64_t *slots_used);
+/* Drops every recorded step and keeps the tape memory for the next ones. */
+int hipft_adj_clear(hipft_gpu *h);
 /* Replace the current field from device memory in the handle's layout
  * (nr x npm x ldt), e.g. a checkpoint taken through
  * hipft_gpu_field_device_ptr; cached pole sums are dropped. */
 int hipft_gpu_set_field_device(hipft_gpu *h, const double *f_dev);
-/* Fields the adjoint's tape holds (device memory, fieldn doubles each). */
+/* Most fields the adjoint's tape has held at once since the last release
+ * (tape slots of the recorded steps plus the block-recompute fields; device
+ * memory, fieldn doubles each). */
 int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n);
-/* Tape budget of hipft_adj_step.  A super-step of s RKG2 stages keeps all
+/* Tape budget of one recorded step.  A super-step of s RKG2 stages keeps all
  * s+1 stage fields when they fit max_fields (0: half of the free device
  * memory at the time); otherwise it keeps stage checkpoints -- the pair
  * (Y_{c-1}, Y_c) every q stages, q even near sqrt(2 s) -- and the reverse pass
@@ -409,8 +425,9 @@ int hipft_adj_tape_fields(hipft_gpu *h, int64_t *n);
  * 2 sqrt(2 s) fields, one more forward pass of the diffusion).
  * stage_spacing > 0 (even) forces that q.  Results do not depend on q. */
 int hipft_adj_set_tape_limit(hipft_gpu *h, int64_t max_fields, int64_t stage_spacing);
-/* Frees the tape (it grows to the largest step seen and is otherwise kept
- * until the handle is destroyed). */
+/* Frees the tape and drops recorded steps (the tape grows to the largest
+ * set of recorded steps seen and is otherwise kept until the handle is
+ * destroyed). */
 int hipft_adj_release(hipft_gpu *h);
 /* Reverse of one data-assimilation blend (apply_data_assimilation,
  * src/hipft.f90:4116-4141, same map and options as the forward call):
