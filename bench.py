@@ -626,22 +626,40 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
     target, _ = forward(gt, f0)
     gt.close()
     forward(g, f0)
-    _, fwd_s = forward(g, f0)
+    fwd_runs = [forward(g, f0)[1] for _ in range(3)]
     A = MisfitAdjoint(g, D, flow, checkpoint_every=checkpoint_every)
     A.run(f0, target, dts)  # warm-up: tuner, tape allocation (kept by the handle)
-    torch.cuda.synchronize()
-    w0 = time.perf_counter()
-    loss, grads = A.run(f0, target, dts)
-    torch.cuda.synchronize()
-    grad_s = time.perf_counter() - w0
+    grad_runs = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        loss, grads = A.run(f0, target, dts)
+        torch.cuda.synchronize()
+        grad_runs.append(time.perf_counter() - w0)
+    fwd_s, grad_s = statistics.median(fwd_runs), statistics.median(grad_runs)
     tape = ctypes.c_int64(0)
     g.L.hipft_adj_tape_fields(g.h, ctypes.byref(tape))
+    if args.adjoint_kernels:
+        # per-kernel device times of one more gradient, through CUPTI (torch.profiler), to stderr
+        from torch.profiler import profile, ProfilerActivity
+        with profile(activities=[ProfilerActivity.CUDA]) as pr:
+            A.run(f0, target, dts)
+            torch.cuda.synchronize()
+        rows = sorted([(e.key, e.count, e.device_time_total) for e in pr.key_averages() if e.device_time_total > 0],
+                      key=lambda r: -r[2])
+        tot = sum(r[2] for r in rows)
+        print(f"adjoint gradient: device total {tot / 1e3:.1f} ms (kernels may overlap)", file=sys.stderr)
+        for key, cnt, tt in rows[:12]:
+            print(f"  {tt / 1e3:9.2f} ms {100 * tt / tot:5.1f}% {cnt:7d}x {tt / max(cnt, 1):8.2f} us  {key[:80]}",
+                  file=sys.stderr)
     A.release()
     g.close()
     return {"workload": "adjoint_512x1024", "grid": [ntm, npm1 - 1], "realizations": 1, "steps": len(dts),
             "model_days": days, "dt_hours": dt, "subcycling": "PTL (automatic)",
             "checkpoint_every": checkpoint_every, "segments": -(-len(dts) // checkpoint_every),
             "forward_ms": fwd_s * 1e3, "gradient_ms": grad_s * 1e3, "gradient_over_forward": grad_s / fwd_s,
+            "runs": "median of 3 timed runs each", "forward_runs_ms": [x * 1e3 for x in fwd_runs],
+            "gradient_runs_ms": [x * 1e3 for x in grad_runs],
             "loss": loss, "grad_D": float(grads["D"][0]), "grad_f0_norm": float(np.linalg.norm(grads["f0"])),
             "tape_fields_peak": int(tape.value),
             "tape_gb_peak": int(tape.value) * ntm * (npm1 + 1) * 8 / 1e9,
@@ -715,6 +733,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
     ap.add_argument("--c5", action="store_true", help="add the 16-realization 2048 x 4096 forward leg")
+    ap.add_argument("--adjoint-kernels", action="store_true",
+                    help="print the adjoint gradient's per-kernel device times (CUPTI) to stderr")
     ap.add_argument("--step", default="graph", choices=["graph", "host"],
                     help="graph: each split step is one CUDA-graph launch; host: host-driven launches")
     ap.add_argument("--schedule", default="ragged", choices=["ragged", "shared"],

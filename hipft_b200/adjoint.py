@@ -185,6 +185,7 @@ class MisfitAdjoint:
         self.reserve_frac = float(reserve_frac)
         self._fbytes = 0
         self._est_fields = 16
+        self._budget = 0.0
 
     def _dev(self):
         return self.gpu.field_tensor()
@@ -230,18 +231,25 @@ class MisfitAdjoint:
         self.gpu._ck(self.gpu.L.hipft_adj_tape_fields(self.gpu.h, ctypes.byref(n)), "hipft_adj_tape_fields")
         return n.value
 
-    def _room_to_record(self) -> bool:
+    def _segment_budget(self):
+        """Bytes a segment's tapes may take: free device memory plus the
+        allocated, unused tape slots, less the reserve (one query per segment;
+        each recorded step then draws on it)."""
         import torch
         free, total = torch.cuda.mem_get_info()
         _, used = self._recorded()
-        spare = max(0, self._tape_fields() - used) * self._fbytes  # allocated, unused tape slots
-        return free + spare - self._est_fields * self._fbytes > self.reserve_frac * total
+        spare = max(0, self._tape_fields() - used) * self._fbytes
+        self._budget = free + spare - self.reserve_frac * total
+
+    def _room_to_record(self) -> bool:
+        return self._budget >= self._est_fields * self._fbytes
 
     def _record(self, s: int, dt: float):
         _, u0 = self._recorded()
         self.gpu._ck(self.gpu.L.hipft_adj_record(self.gpu.h, float(dt)), "hipft_adj_record")
         _, u1 = self._recorded()
         self._est_fields = max(self._est_fields, u1 - u0)
+        self._budget -= (u1 - u0) * self._fbytes
         if s in self.assim:
             m3, opts = self.assim[s]
             self.gpu.assimilate(m3, **opts)
@@ -263,9 +271,12 @@ class MisfitAdjoint:
         ckpt, recorded, states = {}, set(), {}
         last0 = ((n - 1) // self.k) * self.k
         taping = True
+        self._budget = 0.0
         for s, dt in enumerate(dts):
             if s % self.k == 0:
                 ckpt[s] = self._dev().clone()
+            if s == last0:
+                self._segment_budget()
             if s >= last0 and taping and self._room_to_record():
                 self._record(s, dt)
                 recorded.add(s)
@@ -298,6 +309,7 @@ class MisfitAdjoint:
         fbar[:, 1:self.npm - 1, :self.ntm] = gbt[:, 1:self.npm - 1]
         dacc = torch.zeros(self.nr, dtype=torch.float64, device=dev)
         gflow = torch.zeros((5, self.nr, self.npm, ldt), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()  # the library's stream reads these next
         ptr = lambda x: ctypes.c_void_p(x.data_ptr())
         for s0 in sorted(ckpt, reverse=True):
             s1 = min(s0 + self.k, n)
@@ -307,6 +319,7 @@ class MisfitAdjoint:
                 # recompute the segment from its checkpoint, taped while there is room
                 recorded, states = set(), {}
                 self._set(ckpt[s0])
+                self._segment_budget()
                 taping = True
                 for s in range(s0, s1):
                     if taping and self._room_to_record():

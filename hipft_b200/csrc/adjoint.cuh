@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(256) k_adj_diff(Mesh m, DiffCoef dc, const dou
 //   W_{k-2} = a2 W_{k-1} + b2 W_k + c2 A^T W_{k-1},
 //   ub += c01 W_k + c02 W_{k-1},  db += g1 W_k + g2 W_{k-1},
 //   dpart += ds1 <A^T W_k, Y_{k-1}> + ds2 <A^T W_{k-1}, Y_{k-2}> (block partials).
-// A tile of 32 theta rows x 8 core columns stages W_k with a halo of 2 in
+// A tile of 32 theta rows x 16 core columns stages W_k with a halo of 2 in
 // shared memory, computes W_{k-1} on the tile plus a halo of 1 there, then
 // W_{k-2} on the tile: per cell and two stages W_k, W_{k+1}, Y_{k-1}, Y_{k-2},
 // ub, db are read and W_{k-1}, W_{k-2}, ub, db written (80 B) where two
@@ -207,58 +207,86 @@ struct AdjDiff2Coef {
   double a2, b2, c2, c02, g2, ds2;  // stage k-1
 };
 
-constexpr int kA2J = 32, kA2K = 8;  // tile: theta rows x core columns (block 32 x 8 threads)
+constexpr int kA2J = 32, kA2K = 16;  // tile: theta rows x core columns (block 32 x 16 threads)
 
-// A^T w at (j, k) from a shared tile ws (column stride ld) at shared (r, c);
-// gn, gs: w's pole sums.  Same expression order as adj_diff_at_tab.
-__device__ __forceinline__ double adj_at_tile(const Mesh &m, const DiffCoef &dc, const PairTables &pt, int i, int j,
-                                              int k, int kp, int km, const double *ws, int ld, int r, int c,
-                                              double gn, double gs, double bcn, double bcs) {
+// A^T w at (j, k) from a shared tile ws (column stride ld) at shared (r, c),
+// gn, gs: w's pole sums, with the tile's coefficient tables in shared memory
+// (same expression order as adj_diff_at_tab): sR[a*36 +
+// (jj - jbase)] holds table row jj of array a (st_i, c2, c4; jj = row + 1) for
+// jj in jbase .. jbase+35, and sP[pc] the column entry of the cell's column k
+// (sP[pc+1] of k+1, sP[pc-1] of k-1).  Same expressions, same order.
+constexpr int kA2R = kA2J + 4;  // table rows of a k_adj_diff2 tile
+__device__ __forceinline__ double adj_at_tile_s(const Mesh &m, const DiffCoef &dc, int i, int j, int k,
+                                                const double *ws, int ld, int r, int c, const double *sR, int jbase,
+                                                const double2 *sP, int pc, double gn, double gs, double bcn,
+                                                double bcs) {
   const int ntm = m.ntm;
-  const double *R = pt.row + (int64_t)(i - 1) * 3 * pt.LR;
-  const double2 *P = reinterpret_cast<const double2 *>(pt.col) + (int64_t)(i - 1) * pt.LC;
+  auto R = [&](int a, int jj) { return sR[a * kA2R + (jj - jbase)]; };
   auto W = [&](int dr, int dcl) { return ws[(c + dcl) * ld + (r + dr)]; };
   double res = 0.0;
   if (j >= 2 && j <= ntm - 1) {
-    const double sj = R[j + 1], c2 = R[pt.LR + j + 1], c4 = R[2 * pt.LR + j + 1];
-    const double2 Pk = P[k];
+    const double sj = R(0, j + 1), c2 = R(1, j + 1), c4 = R(2, j + 1);
+    const double2 Pk = sP[pc];
     const double c1 = Pk.x * sj * sj, c5 = Pk.y * sj * sj;
     const double c3 = -(c1 + c2 + c4 + c5);
     res += c3 * W(0, 0);
-    res += (P[kp].x * sj * sj) * W(0, 1);
-    res += (P[km].y * sj * sj) * W(0, -1);
-    if (j + 1 <= ntm - 1) res += R[pt.LR + j + 2] * W(1, 0);
-    if (j - 1 >= 2) res += R[2 * pt.LR + j] * W(-1, 0);
+    res += (sP[pc + 1].x * sj * sj) * W(0, 1);
+    res += (sP[pc - 1].y * sj * sj) * W(0, -1);
+    if (j + 1 <= ntm - 1) res += R(1, j + 2) * W(1, 0);
+    if (j - 1 >= 2) res += R(2, j) * W(-1, 0);
     if (j == 2) res += (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
     if (j == ntm - 1) res += (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
   } else if (j == 1) {
-    res += R[pt.LR + 3] * W(1, 0);
+    res += R(1, 3) * W(1, 0);
     res -= (dcoef(m, dc, 1, k, i) + dcoef(m, dc, 2, k, i)) * m.dp[k] * bcn * gn;
   } else {
-    res += R[2 * pt.LR + ntm] * W(-1, 0);
+    res += R(2, ntm) * W(-1, 0);
     res -= (dcoef(m, dc, m.nt - 1, k, i) + dcoef(m, dc, m.nt, k, i)) * m.dp[k] * bcs * gs;
   }
   return res;
 }
 
-__global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const double *__restrict__ w,
+__global__ void __launch_bounds__(kA2J * kA2K) k_adj_diff2(Mesh m, DiffCoef dc, const double *__restrict__ w,
                                                    const double *__restrict__ wp, const double *__restrict__ y1,
                                                    const double *__restrict__ y2, double *out1, double *out2,
                                                    double *ub, double *db, const double *__restrict__ gin, int npin,
                                                    double *__restrict__ gpart, double bcn, double bcs,
-                                                   AdjDiff2Coef ac, double *__restrict__ dpart, PairTables pt) {
+                                                   AdjDiff2Coef ac, double *__restrict__ dpart, int dstride,
+                                                   PairTables pt) {
   constexpr int LW = kA2J + 4, LM = kA2J + 2;
   __shared__ double sw[(kA2K + 4) * LW];  // W_k, halo 2: sw(r, c) = row j0-2+r, core column k0-2+c
   __shared__ double sm[(kA2K + 2) * LM];  // W_{k-1}, halo 1: sm(r, c) = row j0-1+r, core column k0-1+c
   __shared__ double sh[64];
   __shared__ double s_g[2];
   __shared__ double s_n[kA2K], s_s[kA2K];
+  __shared__ double sR[3 * kA2R];      // row tables, rows j0-2 .. j0+33 (entries jj = j0-1 .. j0+34)
+  __shared__ double2 sP[kA2K + 4];     // column table, core columns k0-2 .. k0+9
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * kA2J;
   const int j0 = blockIdx.x * kA2J + 1, k0 = blockIdx.y * kA2K + 2;
   const int i = blockIdx.z + 1;
   const int ntm = m.ntm, npm = m.npm;
-  // pole sums of W_k, summed in order by every block (a fixed tree)
-  if (ty == 0) {
+  const int jbase = j0 - 1;
+  if (tid < 3 * kA2R) {
+    const int a = tid / kA2R, jj = jbase + tid % kA2R;
+    sR[tid] = (jj < pt.LR) ? pt.row[((int64_t)(i - 1) * 3 + a) * pt.LR + jj] : 0.0;
+  } else if (tid >= 128 && tid < 128 + kA2K + 4) {
+    const int q = tid - 128;
+    sP[q] = reinterpret_cast<const double2 *>(pt.col)[(int64_t)(i - 1) * pt.LC + core_wrap(m, k0 - 2 + q)];
+  }
+  // Launched programmatically after the previous pair's k_adj_pole2, this
+  // kernel may start while that one still writes W_k's pole rows (1, 2,
+  // ntm-1, ntm) and pole sums: the tiles whose rows (with halo) reach them
+  // wait for it; the others read neither.  (Without such a launch the wait
+  // returns at once.)
+  const bool edge = (j0 - 2 <= 2) || (j0 + kA2J + 1 >= ntm - 1);
+  if (edge) asm volatile("griddepcontrol.wait;" ::: "memory");
+  if (tid == 0) {
+    s_g[0] = 0.0;
+    s_g[1] = 0.0;
+  }
+  __syncthreads();
+  // pole sums of W_k, summed in order by every block that uses them (a fixed tree)
+  if (ty == 0 && edge) {
     double a = 0.0, b = 0.0;
     const double *g = gin + (int64_t)(i - 1) * npin * 2;
     for (int q = tx; q < npin; q += 32) {
@@ -275,7 +303,7 @@ __global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const do
       s_g[1] = b;
     }
   }
-  for (int e = tid; e < (kA2K + 4) * LW; e += 256) {
+  for (int e = tid; e < (kA2K + 4) * LW; e += kA2J * kA2K) {
     const int r = e % LW, c = e / LW;
     const int j = j0 - 2 + r, k = core_wrap(m, k0 - 2 + c);
     sw[e] = (j >= 1 && j <= ntm) ? w[fidx(m, j, k, i)] : 0.0;
@@ -284,13 +312,12 @@ __global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const do
   const double gn = s_g[0], gs = s_g[1];
   double dsum = 0.0;
   // stage k on the tile plus a halo of 1: W_{k-1} into shared memory
-  for (int e = tid; e < (kA2K + 2) * LM; e += 256) {
+  for (int e = tid; e < (kA2K + 2) * LM; e += kA2J * kA2K) {
     const int r = e % LM, c = e / LM;
     const int j = j0 - 1 + r, k = core_wrap(m, k0 - 1 + c);
     double o = 0.0;
     if (j >= 1 && j <= ntm) {
-      const int kp = core_wrap(m, k + 1), km = core_wrap(m, k - 1);
-      const double aw = adj_at_tile(m, dc, pt, i, j, k, kp, km, sw, LW, r + 1, c + 1, gn, gs, bcn, bcs);
+      const double aw = adj_at_tile_s(m, dc, i, j, k, sw, LW, r + 1, c + 1, sR, jbase, sP, c + 1, gn, gs, bcn, bcs);
       const int64_t q = fidx(m, j, k, i);
       const double wq = sw[(c + 1) * LW + r + 1];
       o = ac.a1 * wq + ac.c1 * aw;
@@ -315,8 +342,8 @@ __global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const do
     if (ub) ub[q] = ub[q] + ac.c01 * wk + ac.c02 * wm;
     if (db) db[q] = db[q] + ac.g1 * wk + ac.g2 * wm;
     if (j >= 3 && j <= ntm - 2) {
-      const int kp = core_wrap(m, k + 1), km = core_wrap(m, k - 1);
-      const double aw = adj_at_tile(m, dc, pt, i, j, k, kp, km, sm, LM, tx + 1, ty + 1, 0.0, 0.0, bcn, bcs);
+      const double aw =
+          adj_at_tile_s(m, dc, i, j, k, sm, LM, tx + 1, ty + 1, sR, jbase, sP, ty + 2, 0.0, 0.0, bcn, bcs);
       out2[q] = ac.a2 * wm + ac.b2 * wk + ac.c2 * aw;
       if (y2) dsum += ac.ds2 * (aw * y2[q]);
     }
@@ -341,7 +368,7 @@ __global__ void __launch_bounds__(256) k_adj_diff2(Mesh m, DiffCoef dc, const do
   if (dpart) {
     double z = 0.0;
     block_sum2(dsum, z, sh);
-    if (tid == 0) dpart[((int64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] += dsum;
+    if (tid == 0) dpart[(int64_t)blockIdx.z * dstride + blockIdx.y * gridDim.x + blockIdx.x] += dsum;
   }
 }
 
@@ -359,6 +386,8 @@ __global__ void __launch_bounds__(256) k_adj_pole2(Mesh m, DiffCoef dc, const do
                                                    AdjDiff2Coef ac, double *__restrict__ dpole, PairTables pt) {
   __shared__ double sh[64];
   __shared__ double s_g[2];
+  // the next pair's k_adj_diff2 may launch now; its pole tiles wait for this grid
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int i = blockIdx.x + 1, ch = blockIdx.y, nch = gridDim.y, tid = threadIdx.x, ntm = m.ntm;
   if (tid < 32) {
     double a = 0.0, b = 0.0;
@@ -495,23 +524,33 @@ struct AdjAdvArgs {
   double sigma, alpha, beta, bcfn, bcfs;
 };
 
+constexpr int kAAJ = 32, kAAK = 8;  // tile of k_adj_adv: theta rows x core columns (block 32 x 8)
+
+// The reverse of one SSPRK stage on a tile of kAAJ x kAAK cells.  Each WENO3
+// face's cotangent-weighted derivatives (Fb * d[0..5]) are computed once per
+// tile into shared memory -- theta faces j0-1 .. j0+kAAJ+1 of the tile's
+// columns, phi faces k0-1 .. k0+kAAK+1 of its interior rows -- and every cell
+// then gathers the four faces on each axis that read it, in the order
+// jf = j-1 .. j+2 (kf = k-1 .. k+2), so each sum has the operation order of
+// one cell computing its faces itself.  Upwind pole faces and the phi faces
+// that reach a cell through the periodic seam aliases are computed by the
+// cell.
 __global__ void __launch_bounds__(256) k_adj_adv(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
                                                  const double *__restrict__ w, const double *__restrict__ base,
                                                  double *__restrict__ out, const double *__restrict__ gring,
                                                  AdjAdvArgs a, double *gln_t, double *glp_t, double *gup_t,
                                                  double *gln_p, double *glp_p) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  __shared__ double tf[kAAK][kAAJ + 3][6];  // theta face jf = j0-1+e of column k0+c
+  __shared__ double pf[kAAJ][kAAK + 3][6];  // phi face kf = k0-1+e of row j0+r
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + ty * kAAJ;
+  const int j0 = blockIdx.x * kAAJ + 1, k0 = blockIdx.y * kAAK + 2;
   const int i = blockIdx.z + 1;
   const int ntm = m.ntm, npm = m.npm;
-  if (j > ntm || k > npm - 1) return;
   const double gn = a.sigma * gring[2 * (i - 1)], gs = a.sigma * gring[2 * (i - 1) + 1];
   auto abar = [&](int jj, int kk) { return a.sigma * w[fidx(m, jj, kk, i)]; };
   auto X = [&](int jj, int kk) { return x[fidx(m, jj, kk, i)]; };
-
-  // ---- theta faces jf = j-1 .. j+2 of column k
   // cotangent of flux_t(jf,k): divergence of cells jf-1 and jf, pole rings
-  auto ftbar = [&](int jf) {
+  auto ftbar = [&](int jf, int k) {
     double v = 0.0;
     if (jf - 1 >= 2 && jf - 1 <= ntm - 1) v += abar(jf - 1, k) * m.sth[jf] * m.st_i[jf - 1] * m.dt_i[jf - 1];
     if (jf >= 2 && jf <= ntm - 1) v -= abar(jf, k) * m.sth[jf] * m.st_i[jf] * m.dt_i[jf];
@@ -519,12 +558,83 @@ __global__ void __launch_bounds__(256) k_adj_adv(Mesh m, Flow fl, Weno wn, const
     if (jf == ntm) v -= a.bcfs * m.dp[k] * gs;
     return v;
   };
+  // cotangent of flux_p(j,kf): divergence of cells kf-1 (npm-1 for kf = 2) and kf
+  auto fpbar = [&](int j, int kf) {
+    double v = 0.0;
+    if (kf >= 3) v += abar(j, kf - 1) * m.st_i[j] * m.dp_i[kf - 1];
+    else v += abar(j, npm - 1) * m.st_i[j] * m.dp_i[npm - 1];
+    v -= abar(j, kf) * m.st_i[j] * m.dp_i[kf];
+    return v;
+  };
+  // Fb * d of the WENO theta face jf of column k (zeros where Fb is zero)
+  auto theta_face = [&](int jf, int k, double *o) {
+    const double Fb = ftbar(jf, k);
+    if (Fb == 0.0) return;
+    double LN[3], LP[3], d[6];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const int c = jf - 2 + e;
+      LN[e] = kHalf * X(c, k) * (vt_at(m, fl, c, k, i) + at_at(m, fl, c, k, i));
+    }
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const int c = jf - 1 + e;
+      LP[e] = kHalf * X(c, k) * (vt_at(m, fl, c + 1, k, i) - at_at(m, fl, c, k, i));
+    }
+    weno_face_vjp(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mct[jf - 1], wn.mct[jf], wn.cpt[jf - 1],
+                  wn.cpt[jf], wn.pt[jf - 1], wn.mctt[jf - 1], wn.mt[jf], wn.cptt[jf], wn.epst[jf - 1],
+                  wn.epst[jf], d);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = Fb * d[q];
+  };
+  // Fb * d of the phi face kf of row j
+  auto phi_face = [&](int j, int kf, double *o) {
+    const double Fb = fpbar(j, kf);
+    if (Fb == 0.0) return;
+    double LN[3], LP[3], d[6];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const int c = wrap_cell(m, kf - 2 + e);
+      LN[e] = kHalf * X(j, c) * (vp_at(m, fl, j, c, i) + ap_at(m, fl, j, c, i));
+    }
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const int c = wrap_cell(m, kf - 1 + e);
+      LP[e] = kHalf * X(j, c) * (vp_at(m, fl, j, c + 1, i) - ap_at(m, fl, j, c, i));
+    }
+    weno_face_vjp(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mcp[kf - 1], wn.mcp[kf], wn.cpp[kf - 1],
+                  wn.cpp[kf], wn.pp[kf - 1], wn.mctp[kf - 1], wn.mp[kf], wn.cptp[kf], wn.epsp[kf - 1],
+                  wn.epsp[kf], d);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = Fb * d[q];
+  };
+  for (int e = tid; e < kAAK * (kAAJ + 3); e += kAAJ * kAAK) {
+    const int c = e / (kAAJ + 3), f = e % (kAAJ + 3);
+    const int k = k0 + c, jf = j0 - 1 + f;
+    double *o = tf[c][f];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = 0.0;
+    if (k <= npm - 1 && jf >= 3 && jf <= ntm - 1) theta_face(jf, k, o);
+  }
+  for (int e = tid; e < kAAJ * (kAAK + 3); e += kAAJ * kAAK) {
+    const int r = e / (kAAK + 3), f = e % (kAAK + 3);
+    const int j = j0 + r, kf = k0 - 1 + f;
+    double *o = pf[r][f];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = 0.0;
+    if (j >= 2 && j <= ntm - 1 && kf >= 2 && kf <= npm - 1) phi_face(j, kf, o);
+  }
+  __syncthreads();
+  const int j = j0 + tx, k = k0 + ty;
+  if (j > ntm || k > npm - 1) return;
+
+  // ---- theta faces jf = j-1 .. j+2 of column k
   double lnb = 0.0, lpb = 0.0, xb = 0.0, upv = 0.0;
   for (int jf = j - 1; jf <= j + 2; ++jf) {
     if (jf < 2 || jf > ntm) continue;
-    const double Fb = ftbar(jf);
-    if (Fb == 0.0) continue;
     if (jf == 2 || jf == ntm) {  // upwind face: x(jf) high side, x(jf-1) low side
+      const double Fb = ftbar(jf, k);
+      if (Fb == 0.0) continue;
       const double v = vt_at(m, fl, jf, k, i), cct = copysign(fl.upwind, v);
       if (j == jf) {
         xb += Fb * v * kHalf * (kOne - cct);
@@ -532,31 +642,18 @@ __global__ void __launch_bounds__(256) k_adj_adv(Mesh m, Flow fl, Weno wn, const
       }
       if (j == jf - 1) xb += Fb * v * kHalf * (kOne + cct);
     } else {
-      double LN[3], LP[3], d[6];
-#pragma unroll
-      for (int e = 0; e < 3; ++e) {
-        const int c = jf - 2 + e;
-        LN[e] = kHalf * X(c, k) * (vt_at(m, fl, c, k, i) + at_at(m, fl, c, k, i));
-      }
-#pragma unroll
-      for (int e = 0; e < 3; ++e) {
-        const int c = jf - 1 + e;
-        LP[e] = kHalf * X(c, k) * (vt_at(m, fl, c + 1, k, i) - at_at(m, fl, c, k, i));
-      }
-      weno_face_vjp(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mct[jf - 1], wn.mct[jf], wn.cpt[jf - 1],
-                    wn.cpt[jf], wn.pt[jf - 1], wn.mctt[jf - 1], wn.mt[jf], wn.cptt[jf], wn.epst[jf - 1],
-                    wn.epst[jf], d);
+      const double *o = tf[ty][jf - (j0 - 1)];
       const int pos = j - jf;  // -2, -1, 0, 1
-      if (pos == -2) lnb += Fb * d[0];
+      if (pos == -2) lnb += o[0];
       if (pos == -1) {
-        lnb += Fb * d[1];
-        lpb += Fb * d[3];
+        lnb += o[1];
+        lpb += o[3];
       }
       if (pos == 0) {
-        lnb += Fb * d[2];
-        lpb += Fb * d[4];
+        lnb += o[2];
+        lpb += o[4];
       }
-      if (pos == 1) lpb += Fb * d[5];
+      if (pos == 1) lpb += o[5];
     }
   }
   const double xj = X(j, k);
@@ -569,53 +666,34 @@ __global__ void __launch_bounds__(256) k_adj_adv(Mesh m, Flow fl, Weno wn, const
 
   // ---- phi faces (interior rows): core faces kf = 2..npm-1, face npm is
   // the seam copy of face 2; cell index c' of the padded row (0..npm)
-  // aliases core cell k when c' = k, or c' = 0 (k = npm-2), 1 (k = npm-1),
-  // npm (k = 2)
+  // aliases core cell k when c' = k (faces from the tile), or c' = 0
+  // (k = npm-2), 1 (k = npm-1), npm (k = 2) (faces computed here)
   if (j >= 2 && j <= ntm - 1) {
-    auto fpbar = [&](int kf) {
-      double v = 0.0;
-      if (kf >= 3) v += abar(j, kf - 1) * m.st_i[j] * m.dp_i[kf - 1];
-      else v += abar(j, npm - 1) * m.st_i[j] * m.dp_i[npm - 1];
-      v -= abar(j, kf) * m.st_i[j] * m.dp_i[kf];
-      return v;
-    };
     double lnbp = 0.0, lpbp = 0.0;
-    int alias[4], na = 0;
-    alias[na++] = k;
-    if (k == npm - 2) alias[na++] = 0;
-    if (k == npm - 1) alias[na++] = 1;
-    if (k == 2) alias[na++] = npm;
-    for (int ai = 0; ai < na; ++ai) {
-      const int cp = alias[ai];
+    auto add = [&](const double *o, int pos) {
+      if (pos == -2) lnbp += o[0];
+      if (pos == -1) {
+        lnbp += o[1];
+        lpbp += o[3];
+      }
+      if (pos == 0) {
+        lnbp += o[2];
+        lpbp += o[4];
+      }
+      if (pos == 1) lpbp += o[5];
+    };
+    for (int kf = k - 1; kf <= k + 2; ++kf)
+      if (kf >= 2 && kf <= npm - 1) add(pf[tx][kf - (k0 - 1)], k - kf);
+    int cp = -1;
+    if (k == npm - 2) cp = 0;
+    if (k == npm - 1) cp = 1;
+    if (k == 2) cp = npm;
+    if (cp >= 0) {
       for (int kf = cp - 1; kf <= cp + 2; ++kf) {
         if (kf < 2 || kf > npm - 1) continue;
-        const double Fb = fpbar(kf);
-        if (Fb == 0.0) continue;
-        double LN[3], LP[3], d[6];
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-          const int c = wrap_cell(m, kf - 2 + e);
-          LN[e] = kHalf * X(j, c) * (vp_at(m, fl, j, c, i) + ap_at(m, fl, j, c, i));
-        }
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-          const int c = wrap_cell(m, kf - 1 + e);
-          LP[e] = kHalf * X(j, c) * (vp_at(m, fl, j, c + 1, i) - ap_at(m, fl, j, c, i));
-        }
-        weno_face_vjp(LN[0], LN[1], LN[2], LP[0], LP[1], LP[2], wn.mcp[kf - 1], wn.mcp[kf], wn.cpp[kf - 1],
-                      wn.cpp[kf], wn.pp[kf - 1], wn.mctp[kf - 1], wn.mp[kf], wn.cptp[kf], wn.epsp[kf - 1],
-                      wn.epsp[kf], d);
-        const int pos = cp - kf;
-        if (pos == -2) lnbp += Fb * d[0];
-        if (pos == -1) {
-          lnbp += Fb * d[1];
-          lpbp += Fb * d[3];
-        }
-        if (pos == 0) {
-          lnbp += Fb * d[2];
-          lpbp += Fb * d[4];
-        }
-        if (pos == 1) lpbp += Fb * d[5];
+        double o[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        phi_face(j, kf, o);
+        add(o, cp - kf);
       }
     }
     xb += lnbp * kHalf * (vp_at(m, fl, j, k, i) + ap_at(m, fl, j, k, i)) +

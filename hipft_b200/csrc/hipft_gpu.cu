@@ -3229,6 +3229,8 @@ extern "C" int hipft_gpu_check_bounded_wait(hipft_gpu *h, unsigned int limit) {
 extern "C" int hipft_gpu_field_device_ptr(hipft_gpu *h, double **ptr, int *ldt) {
   if (!h || !ptr || !ldt) return HIPFT_EINVAL;
   if (!h->field_set) return fail(h, HIPFT_ESTATE, "field_device_ptr before set_field");
+  CK(h, cudaSetDevice(h->dev));
+  CK(h, cudaStreamSynchronize(h->stream));  // the field is complete when the pointer is handed out
   *ptr = h->buf[h->cur];
   *ldt = h->ldt;
   return HIPFT_OK;
@@ -3760,28 +3762,50 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
   int64_t k = S.s;
   // two reverse stages per launch (k_adj_diff2 + k_adj_pole2) while both of
   // their stage inputs Y_{k-1}, Y_{k-2} lie in one stage-checkpoint block
+  // A pair launch follows the previous pair's k_adj_pole2 programmatically
+  // (its interior tiles start while that kernel runs); its outputs then avoid
+  // the previous pair's W_k as well, which that kernel still reads.
+  double *Wprev = nullptr;
+  bool after_pole2 = false;
+  const dim3 grd2((unsigned)((h->ntm + kA2J - 1) / kA2J), (unsigned)((h->npm - 2 + kA2K - 1) / kA2K), (unsigned)h->nr);
   while (adj_pairs_enabled() && k >= 3 && (S.q == 0 || (k - 2) / S.q == (k - 3) / S.q)) {
     if (S.q > 0 && (k - 3) / S.q != curb) {
       curb = (k - 3) / S.q;
       TRY(adj_block_recompute(h, S, (size_t)curb, Yr));
+      after_pole2 = false;
     }
-    double *Wm1 = adj_free(h, {Wk, Wk1, ub, db});
-    double *Wm2 = adj_free(h, {Wk, Wk1, ub, db, Wm1});
+    double *Wm1 = adj_free(h, {Wk, Wk1, ub, db, Wprev});
+    double *Wm2 = adj_free(h, {Wk, Wk1, ub, db, Wprev, Wm1});
     const double u1 = S.uj[k], v1 = S.vj[k], u2 = S.uj[k - 1], v2 = S.vj[k - 1];
     const double nu1 = (k < S.s) ? S.vj[k + 1] : 0.0;
     const AdjDiff2Coef ac{u1, nu1, S.ubj[k] * dtl, 1.0 - u1 - v1, S.gj[k], S.ubj[k] * dtl,
                           u2, v1, S.ubj[k - 1] * dtl, 1.0 - u2 - v2, S.gj[k - 1], S.ubj[k - 1] * dtl};
     double *gpart = h->d_gpart[pp];
-    k_adj_diff2<<<grd, blk, 0, h->stream>>>(h->M, h->DC, Wk, Wk1, Yt(k - 1), Yt(k - 2), Wm1, Wm2, ub, db, gin, npin,
-                                            gpart, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpart, h->ptab);
-    LAUNCHED(h);
+    {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = grd2;
+      cfg.blockDim = dim3(kA2J, kA2K);
+      cfg.stream = h->stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && after_pole2) ? 1 : 0;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      const double *y1 = Yt(k - 1), *y2 = Yt(k - 2);
+      CK(h, cudaLaunchKernelEx(&cfg, k_adj_diff2, h->M, h->DC, (const double *)Wk, (const double *)Wk1, y1, y2, Wm1,
+                               Wm2, ub, db, gin, npin, gpart, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpart,
+                               h->dpart_per_r, h->ptab));
+      LAUNCHED(h);
+    }
     k_adj_pole2<<<dim3((unsigned)h->nr, (unsigned)h->adj_nch), 256, 0, h->stream>>>(
-        h->M, h->DC, Wk, Wm1, Yt(k - 2), Wm2, gpart, (int)grd.y, h->d_gring, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpole,
+        h->M, h->DC, Wk, Wm1, Yt(k - 2), Wm2, gpart, (int)grd2.y, h->d_gring, h->bc_diff_n, h->bc_diff_s, ac, h->d_dpole,
         h->ptab);
     LAUNCHED(h);
+    after_pole2 = true;
     gin = h->d_gring;
     npin = h->adj_nch;
     pp ^= 1;
+    Wprev = Wk;
     Wk1 = Wm1;
     Wk = Wm2;
     k -= 2;
@@ -3890,8 +3914,7 @@ extern "C" int hipft_adj_record(hipft_gpu *h, double dt) {
 extern "C" int hipft_adj_reverse(hipft_gpu *h, double *fbar, double *dacc, double *gflow) {
   if (!h || !fbar || !dacc || !gflow) return HIPFT_EINVAL;
   CK(h, cudaSetDevice(h->dev));
-  TRY(adj_reverse(h, fbar, dacc, gflow));
-  CK(h, cudaStreamSynchronize(h->stream));
+  TRY(adj_reverse(h, fbar, dacc, gflow));  // asynchronous on the handle's stream
   CK(h, cudaGetLastError());
   return HIPFT_OK;
 }

@@ -271,8 +271,9 @@ int hipft_gpu_set_stream(hipft_gpu *h, void *cuda_stream);
 int hipft_gpu_synchronize(hipft_gpu *h);
 /* Zero-copy view of the current field for the PyTorch binding: the device
  * address of f(j, k, i) at (*ptr)[(i-1)*npm*ldt + (k-1)*ldt + (j-1)] (theta
- * padded to *ldt).  Valid until the next call that advances, assimilates or
- * sets the field (the library rotates its buffers). */
+ * padded to *ldt).  Returns after the handle's stream has finished, so the
+ * field may be read on any stream.  Valid until the next call that advances,
+ * assimilates or sets the field (the library rotates its buffers). */
 int hipft_gpu_field_device_ptr(hipft_gpu *h, double **ptr, int *ldt);
 /* No counterpart in the reference: a self-check of the error path that every
  * bounded device wait of this library takes.  A kernel waits on an mbarrier
