@@ -254,7 +254,7 @@ def measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_ma
     k = max(2, min(args.steps, 4))
     out = {"unit": "realization-steps/s", "dt_hours": dt, "ragged_batch": ragged_rs_per_s}
     # one batch, shared schedule
-    g = make_handle(H, t, p, br, prm, slice(0, nr), local, False)
+    g = make_handle(H, t, p, br, prm, slice(0, nr), local, False, graph=args.step == "graph")
     g.set_stream(stream.cuda_stream)
     state = {"time": 0.0, "da": 0}
     step = make_step(g, dt, da_times, da_maps, prm, slice(0, nr), state)
@@ -272,7 +272,7 @@ def measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_ma
     # one handle per realization, each with its own schedule
     tot_ms = 0.0
     for i in range(nr):
-        gi = make_handle(H, t, p, br, prm, slice(i, i + 1), local, False)
+        gi = make_handle(H, t, p, br, prm, slice(i, i + 1), local, False, graph=args.step == "graph")
         gi.set_stream(stream.cuda_stream)
         st = {"time": 0.0, "da": 0}
         si = make_step(gi, dt, da_times, da_maps, prm, slice(i, i + 1), st)
@@ -455,7 +455,7 @@ def run_gpu(args, wl, name):
     if rank == 0 and world == 1 and not args.no_plain:
         out["plain"] = measure_plain(args, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
-        out["adjoint"] = measure_adjoint(args, local)
+        out["adjoint"] = measure_adjoint(args, local, days=args.adjoint_days)
     if rank == 0 and world == 1 and args.c5:
         out["c5"] = measure_c5(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -526,10 +526,18 @@ def measure_plain(args, local: int):
             tot += e0.elapsed_time(e1)
         return info0, g.info(), tot
 
+    graph = args.step == "graph"
+    if graph:
+        g.set_graph(True)
+        step()  # capture
     i0, i1, ms = timed(False)
+    if graph:
+        g.set_graph(False)  # per-kernel events need host-driven launches (the same kernels)
     ip, ip1, ms_prof = timed(True)
     sts_n, sts_ms = g.kernel_time(0)
     g.set_profiling(False)
+    if graph:
+        g.set_graph(True)
     cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
     rkg2 = int(ip1.rkg2_stages - ip.rkg2_stages)
     f_host = torch.empty((1, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
@@ -733,6 +741,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
     ap.add_argument("--c5", action="store_true", help="add the 16-realization 2048 x 4096 forward leg")
+    ap.add_argument("--adjoint-days", type=float, default=27.27,
+                    help="model days of the adjoint leg (27.27: the adjoint configuration)")
     ap.add_argument("--adjoint-kernels", action="store_true",
                     help="print the adjoint gradient's per-kernel device times (CUPTI) to stderr")
     ap.add_argument("--step", default="graph", choices=["graph", "host"],

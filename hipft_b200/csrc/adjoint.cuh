@@ -246,7 +246,7 @@ __device__ __forceinline__ double adj_at_tile_s(const Mesh &m, const DiffCoef &d
   return res;
 }
 
-__global__ void __launch_bounds__(kA2J * kA2K) k_adj_diff2(Mesh m, DiffCoef dc, const double *__restrict__ w,
+__global__ void __launch_bounds__(kA2J * kA2K, 3) k_adj_diff2(Mesh m, DiffCoef dc, const double *__restrict__ w,
                                                    const double *__restrict__ wp, const double *__restrict__ y1,
                                                    const double *__restrict__ y2, double *out1, double *out2,
                                                    double *ub, double *db, const double *__restrict__ gin, int npin,
@@ -280,16 +280,11 @@ __global__ void __launch_bounds__(kA2J * kA2K) k_adj_diff2(Mesh m, DiffCoef dc, 
   // returns at once.)
   const bool edge = (j0 - 2 <= 2) || (j0 + kA2J + 1 >= ntm - 1);
   if (edge) asm volatile("griddepcontrol.wait;" ::: "memory");
-  if (tid == 0) {
-    s_g[0] = 0.0;
-    s_g[1] = 0.0;
-  }
-  __syncthreads();
   // pole sums of W_k, summed in order by every block that uses them (a fixed tree)
-  if (ty == 0 && edge) {
+  if (ty == 0) {
     double a = 0.0, b = 0.0;
     const double *g = gin + (int64_t)(i - 1) * npin * 2;
-    for (int q = tx; q < npin; q += 32) {
+    for (int q = tx; edge && q < npin; q += 32) {
       a = a + g[2 * q];
       b = b + g[2 * q + 1];
     }
@@ -303,49 +298,72 @@ __global__ void __launch_bounds__(kA2J * kA2K) k_adj_diff2(Mesh m, DiffCoef dc, 
       s_g[1] = b;
     }
   }
-  for (int e = tid; e < (kA2K + 4) * LW; e += kA2J * kA2K) {
+  // Every global operand of the thread's cells is requested here, before
+  // the first barrier, so that the loads' latencies overlap: W_{k+1} of its
+  // (at most two) stage-k cells, Y_{k-1} of those it owns, and ub, db,
+  // Y_{k-2} of its stage-(k-1) cell.
+  constexpr int NT = kA2J * kA2K, NE = (kA2K + 2) * LM, NPER = (NE + NT - 1) / NT;
+  double wpv[NPER], y1v[NPER];
+#pragma unroll
+  for (int n = 0; n < NPER; ++n) {
+    const int e = tid + n * NT, r = e % LM, c = e / LM;
+    const int jj = j0 - 1 + r, kk = core_wrap(m, k0 - 1 + c);
+    const bool in = e < NE && jj >= 1 && jj <= ntm;
+    const bool own = (r >= 1 && r <= kA2J && c >= 1 && c <= kA2K && k0 - 1 + c <= npm - 1);
+    const int64_t q = in ? fidx(m, jj, kk, i) : 0;
+    wpv[n] = (in && wp) ? wp[q] : 0.0;
+    y1v[n] = (in && own && y1) ? y1[q] : 0.0;
+  }
+  const int j = j0 + tx, k = k0 + ty;
+  const bool active = (j <= ntm && k <= npm - 1);
+  const int64_t qa = active ? fidx(m, j, k, i) : 0;
+  const double ubv = (active && ub) ? ub[qa] : 0.0, dbv = (active && db) ? db[qa] : 0.0;
+  const double y2v = (active && y2 && j >= 3 && j <= ntm - 2) ? y2[qa] : 0.0;
+  for (int e = tid; e < (kA2K + 4) * LW; e += NT) {
     const int r = e % LW, c = e / LW;
-    const int j = j0 - 2 + r, k = core_wrap(m, k0 - 2 + c);
-    sw[e] = (j >= 1 && j <= ntm) ? w[fidx(m, j, k, i)] : 0.0;
+    const int jj = j0 - 2 + r, kk = core_wrap(m, k0 - 2 + c);
+    sw[e] = (jj >= 1 && jj <= ntm) ? w[fidx(m, jj, kk, i)] : 0.0;
   }
   __syncthreads();
   const double gn = s_g[0], gs = s_g[1];
   double dsum = 0.0;
   // stage k on the tile plus a halo of 1: W_{k-1} into shared memory
-  for (int e = tid; e < (kA2K + 2) * LM; e += kA2J * kA2K) {
+#pragma unroll
+  for (int n = 0; n < NPER; ++n) {
+    const int e = tid + n * NT;
+    if (e >= NE) break;
     const int r = e % LM, c = e / LM;
-    const int j = j0 - 1 + r, k = core_wrap(m, k0 - 1 + c);
+    const int jj = j0 - 1 + r, kk = core_wrap(m, k0 - 1 + c);
     double o = 0.0;
-    if (j >= 1 && j <= ntm) {
-      const double aw = adj_at_tile_s(m, dc, i, j, k, sw, LW, r + 1, c + 1, sR, jbase, sP, c + 1, gn, gs, bcn, bcs);
-      const int64_t q = fidx(m, j, k, i);
+    if (jj >= 1 && jj <= ntm) {
+      const double aw =
+          adj_at_tile_s(m, dc, i, jj, kk, sw, LW, r + 1, c + 1, sR, jbase, sP, c + 1, gn, gs, bcn, bcs);
+      const int64_t q = fidx(m, jj, kk, i);
       const double wq = sw[(c + 1) * LW + r + 1];
       o = ac.a1 * wq + ac.c1 * aw;
-      if (wp) o += ac.b1 * wp[q];
+      if (wp) o += ac.b1 * wpv[n];
       const bool own = (r >= 1 && r <= kA2J && c >= 1 && c <= kA2K && k0 - 1 + c <= npm - 1);
       if (own) {
         out1[q] = o;
-        if (y1) dsum += ac.ds1 * (aw * y1[q]);
+        if (y1) dsum += ac.ds1 * (aw * y1v[n]);
       }
     }
     sm[e] = o;
   }
   __syncthreads();
   // stage k-1 on the tile, except the rows that need W_{k-1}'s pole sums
-  const int j = j0 + tx, k = k0 + ty;
   double wm = 0.0;
-  const bool active = (j <= ntm && k <= npm - 1);
   if (active) {
-    const int64_t q = fidx(m, j, k, i);
+    const int64_t q = qa;
     const double wk = sw[(ty + 2) * LW + tx + 2];
     wm = sm[(ty + 1) * LM + tx + 1];
-    if (ub) ub[q] = ub[q] + ac.c01 * wk + ac.c02 * wm;
-    if (db) db[q] = db[q] + ac.g1 * wk + ac.g2 * wm;
+    if (ub) ub[q] = ubv + ac.c01 * wk + ac.c02 * wm;
+    if (db) db[q] = dbv + ac.g1 * wk + ac.g2 * wm;
     if (j >= 3 && j <= ntm - 2) {
       const double aw =
           adj_at_tile_s(m, dc, i, j, k, sm, LM, tx + 1, ty + 1, sR, jbase, sP, ty + 2, 0.0, 0.0, bcn, bcs);
       out2[q] = ac.a2 * wm + ac.b2 * wk + ac.c2 * aw;
-      if (y2) dsum += ac.ds2 * (aw * y2[q]);
+      if (y2) dsum += ac.ds2 * (aw * y2v);
     }
   }
   // per-tile partials of W_{k-1}'s pole sums (fixed order over the tile's columns)
@@ -535,7 +553,7 @@ constexpr int kAAJ = 32, kAAK = 8;  // tile of k_adj_adv: theta rows x core colu
 // one cell computing its faces itself.  Upwind pole faces and the phi faces
 // that reach a cell through the periodic seam aliases are computed by the
 // cell.
-__global__ void __launch_bounds__(256) k_adj_adv(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
+__global__ void __launch_bounds__(256, 3) k_adj_adv(Mesh m, Flow fl, Weno wn, const double *__restrict__ x,
                                                  const double *__restrict__ w, const double *__restrict__ base,
                                                  double *__restrict__ out, const double *__restrict__ gring,
                                                  AdjAdvArgs a, double *gln_t, double *glp_t, double *gup_t,

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/hipft_gpu.h"
@@ -143,12 +144,7 @@ struct hipft_gpu {
   int nkb = 0;
   PairTables ptab{};        // coefficient tables of the warp-specialised two-stage kernel
   PairPlan plan{};          // two-stage kernel chosen for this grid (autotuner)
-  struct WsMapEntry {
-    const void *p;
-    int rows, cols;
-    CUtensorMap m;
-  };
-  std::vector<WsMapEntry> ws_map_cache;  // tensor maps of the field buffers, by (pointer, box columns)
+  std::unordered_map<uint64_t, CUtensorMap> ws_map_cache;  // tensor maps of field buffers, by (pointer, box)
   CUtensorMap ws_rt_map{};               // tensor map of ptab.row
   bool ws_rt_ok = false;
   // four stages per pass on the interior theta blocks
@@ -540,20 +536,19 @@ static bool encode_f64_3d(CUtensorMap *m, const void *base, uint64_t d0, uint64_
 
 // a field buffer's map with a box of rows x cols (cached)
 static bool field_map(hipft_gpu *h, const double *p, int cols, CUtensorMap *out, int rows = kWR) {
-  for (const auto &e : h->ws_map_cache)
-    if (e.p == p && e.cols == cols && e.rows == rows) {
-      *out = e.m;
-      return true;
-    }
-  hipft_gpu::WsMapEntry e{};
-  e.p = p;
-  e.rows = rows;
-  e.cols = cols;
-  if (!encode_f64_3d(&e.m, p, (uint64_t)h->ldt, (uint64_t)h->npm, (uint64_t)h->nr, (uint64_t)h->ldt * 8,
+  // key: the address (user-space pointers fit 48 bits) with the box shape above it
+  const uint64_t key = (uint64_t)(uintptr_t)p | ((uint64_t)(cols & 0xff) << 48) | ((uint64_t)(rows & 0xff) << 56);
+  const auto it = h->ws_map_cache.find(key);
+  if (it != h->ws_map_cache.end()) {
+    *out = it->second;
+    return true;
+  }
+  CUtensorMap mp;
+  if (!encode_f64_3d(&mp, p, (uint64_t)h->ldt, (uint64_t)h->npm, (uint64_t)h->nr, (uint64_t)h->ldt * 8,
                      (uint64_t)h->plane * 8, (uint32_t)rows, (uint32_t)cols))
     return false;
-  h->ws_map_cache.push_back(e);
-  *out = e.m;
+  h->ws_map_cache.emplace(key, mp);
+  *out = mp;
   return true;
 }
 
