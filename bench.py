@@ -634,11 +634,11 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
     target, _ = forward(gt, f0)
     gt.close()
     forward(g, f0)
-    fwd_runs = [forward(g, f0)[1] for _ in range(3)]
+    fwd_runs = [forward(g, f0)[1] for _ in range(5)]
     A = MisfitAdjoint(g, D, flow, checkpoint_every=checkpoint_every)
     A.run(f0, target, dts)  # warm-up: tuner, tape allocation (kept by the handle)
     grad_runs = []
-    for _ in range(3):
+    for _ in range(5):
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         loss, grads = A.run(f0, target, dts)
@@ -666,7 +666,7 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
             "model_days": days, "dt_hours": dt, "subcycling": "PTL (automatic)",
             "checkpoint_every": checkpoint_every, "segments": -(-len(dts) // checkpoint_every),
             "forward_ms": fwd_s * 1e3, "gradient_ms": grad_s * 1e3, "gradient_over_forward": grad_s / fwd_s,
-            "runs": "median of 3 timed runs each", "forward_runs_ms": [x * 1e3 for x in fwd_runs],
+            "runs": "median of 5 timed runs each", "forward_runs_ms": [x * 1e3 for x in fwd_runs],
             "gradient_runs_ms": [x * 1e3 for x in grad_runs],
             "loss": loss, "grad_D": float(grads["D"][0]), "grad_f0_norm": float(np.linalg.norm(grads["f0"])),
             "tape_fields_peak": int(tape.value),
