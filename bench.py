@@ -254,7 +254,7 @@ def measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_ma
     k = max(2, min(args.steps, 4))
     out = {"unit": "realization-steps/s", "dt_hours": dt, "ragged_batch": ragged_rs_per_s}
     # one batch, shared schedule
-    g = make_handle(H, t, p, br, prm, slice(0, nr), local, False, graph=args.step == "graph")
+    g = make_handle(H, t, p, br, prm, slice(0, nr), local, False)
     g.set_stream(stream.cuda_stream)
     state = {"time": 0.0, "da": 0}
     step = make_step(g, dt, da_times, da_maps, prm, slice(0, nr), state)
@@ -272,7 +272,7 @@ def measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_ma
     # one handle per realization, each with its own schedule
     tot_ms = 0.0
     for i in range(nr):
-        gi = make_handle(H, t, p, br, prm, slice(i, i + 1), local, False, graph=args.step == "graph")
+        gi = make_handle(H, t, p, br, prm, slice(i, i + 1), local, False)
         gi.set_stream(stream.cuda_stream)
         st = {"time": 0.0, "da": 0}
         si = make_step(gi, dt, da_times, da_maps, prm, slice(i, i + 1), st)
@@ -291,7 +291,8 @@ def measure_batched_vs_plain(args, wl, local, t, p, br, prm, dt, da_times, da_ma
     out["ragged_over_per_realization"] = ragged_rs_per_s / out["per_realization_handles"]
     out["ragged_over_shared"] = ragged_rs_per_s / out["shared_batch"]
     out["note"] = ("the per-realization handles run one after another, each from the 126 MB L2 (17 MB fields); "
-                   "the batches stream 1.07 GB fields from HBM")
+                   "the batches stream 1.07 GB fields from HBM; the shared batch and the per-realization handles run "
+                   "host-driven, their faster mode (a one-realization graph-run step is about 8% slower)")
     return out
 
 
@@ -526,18 +527,10 @@ def measure_plain(args, local: int):
             tot += e0.elapsed_time(e1)
         return info0, g.info(), tot
 
-    graph = args.step == "graph"
-    if graph:
-        g.set_graph(True)
-        step()  # capture
     i0, i1, ms = timed(False)
-    if graph:
-        g.set_graph(False)  # per-kernel events need host-driven launches (the same kernels)
     ip, ip1, ms_prof = timed(True)
     sts_n, sts_ms = g.kernel_time(0)
     g.set_profiling(False)
-    if graph:
-        g.set_graph(True)
     cells = float(i1.cell_stage_updates - i0.cell_stage_updates)
     rkg2 = int(ip1.rkg2_stages - ip.rkg2_stages)
     f_host = torch.empty((1, npm, ntm), dtype=torch.float64, pin_memory=True).numpy()
@@ -634,16 +627,24 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
     target, _ = forward(gt, f0)
     gt.close()
     forward(g, f0)
+    import gc
+    gc.collect()
+    gc.disable()
     fwd_runs = [forward(g, f0)[1] for _ in range(5)]
+    gc.enable()
     A = MisfitAdjoint(g, D, flow, checkpoint_every=checkpoint_every)
     A.run(f0, target, dts)  # warm-up: tuner, tape allocation (kept by the handle)
     grad_runs = []
+    import gc
     for _ in range(5):
+        gc.collect()
+        gc.disable()  # no collector pauses inside a timed run
         torch.cuda.synchronize()
         w0 = time.perf_counter()
         loss, grads = A.run(f0, target, dts)
         torch.cuda.synchronize()
         grad_runs.append(time.perf_counter() - w0)
+        gc.enable()
     fwd_s, grad_s = statistics.median(fwd_runs), statistics.median(grad_runs)
     tape = ctypes.c_int64(0)
     g.L.hipft_adj_tape_fields(g.h, ctypes.byref(tape))

@@ -186,6 +186,7 @@ class MisfitAdjoint:
         self._fbytes = 0
         self._est_fields = 16
         self._budget = 0.0
+        self._free = self._total = self._tape0 = 0
 
     def _dev(self):
         return self.gpu.field_tensor()
@@ -232,14 +233,13 @@ class MisfitAdjoint:
         return n.value
 
     def _segment_budget(self):
-        """Bytes a segment's tapes may take: free device memory plus the
-        allocated, unused tape slots, less the reserve (one query per segment;
-        each recorded step then draws on it)."""
-        import torch
-        free, total = torch.cuda.mem_get_info()
+        """Bytes a segment's tapes may take: the device memory free at the
+        start of the run (queried once, in forward()) plus the allocated,
+        unused tape slots, less the reserve; each recorded step then draws on
+        it."""
         _, used = self._recorded()
-        spare = max(0, self._tape_fields() - used) * self._fbytes
-        self._budget = free + spare - self.reserve_frac * total
+        # free now = free at the start - tape grown since; spare = tape - used
+        self._budget = self._free + (self._tape0 - used) * self._fbytes - self.reserve_frac * self._total
 
     def _room_to_record(self) -> bool:
         return self._budget >= self._est_fields * self._fbytes
@@ -268,6 +268,8 @@ class MisfitAdjoint:
         g.update_flow()
         self._fbytes = self._dev().numel() * 8
         self._est_fields = 16
+        self._free, self._total = torch.cuda.mem_get_info()
+        self._tape0 = self._tape_fields()
         ckpt, recorded, states = {}, set(), {}
         last0 = ((n - 1) // self.k) * self.k
         taping = True
@@ -311,8 +313,10 @@ class MisfitAdjoint:
         gflow = torch.zeros((5, self.nr, self.npm, ldt), dtype=torch.float64, device=dev)
         torch.cuda.synchronize()  # the library's stream reads these next
         ptr = lambda x: ctypes.c_void_p(x.data_ptr())
+        seg_times = []
         for s0 in sorted(ckpt, reverse=True):
             s1 = min(s0 + self.k, n)
+            ta = time.perf_counter()
             if s0 == last0:
                 recorded, states = self._fwd["recorded"], self._fwd["states"]
             else:
@@ -330,6 +334,8 @@ class MisfitAdjoint:
                     states[s] = self._dev().clone()
                     if s < s1 - 1:
                         self._step(s, dts[s])
+            torch.cuda.synchronize()
+            tb = time.perf_counter()
             for s in range(s1 - 1, s0 - 1, -1):
                 if s in self.assim:
                     m3, opts = self.assim[s]
@@ -341,6 +347,8 @@ class MisfitAdjoint:
                     self._set(states.pop(s))
                     g._ck(g.L.hipft_adj_record(g.h, float(dts[s])), "hipft_adj_record")
                 g._ck(g.L.hipft_adj_reverse(g.h, ptr(fbar), ptr(dacc), ptr(gflow)), "hipft_adj_reverse")
+            torch.cuda.synchronize()
+            seg_times.append((s0, tb - ta, time.perf_counter() - tb))
         torch.cuda.synchronize()
         nrec, _ = self._recorded()
         if nrec:
@@ -351,6 +359,8 @@ class MisfitAdjoint:
         grads["D"] = dacc.cpu().numpy() / self.D
         grads.update(self._flow_grads(gflow))
         self.timing["reverse_s"] = time.perf_counter() - t1
+        # per segment: (first step, recompute seconds, reverse seconds)
+        self.timing["segments"] = seg_times
         self._fwd = None
         return grads
 

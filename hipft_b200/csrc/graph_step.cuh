@@ -18,7 +18,7 @@
 
 namespace hipft {
 
-constexpr int kGUnroll = 4;          // stage pairs per iteration of the pair loop (even: buffer roles repeat)
+constexpr int kGUnrollMax = 16;      // most stage pairs per iteration of the pair loop (an even number: buffer roles repeat)
 constexpr int kGMaxCycles = 60;      // max_sc of diffusion_step (src/hipft.f90:4565)
 constexpr int kGAdvLimit = 100000;   // advection substeps after which the loop stops and reports an error
 constexpr int kGSubLimit = 1000;     // subcycles likewise (PTL forces the last one at kGMaxCycles - 1)
@@ -62,6 +62,7 @@ struct GArrays {
   double *ring0, *ring1;          // diffusion ring sums of stage inputs / outputs
   int nr, paircap;
   int method, auto_sc, subcycles, ragged, strang, nadv;  // nadv: advection stages per substep
+  int unroll;                     // stage pairs per pair-loop iteration (even)
 };
 
 __device__ __forceinline__ double bits_to_double(unsigned long long b) { return __longlong_as_double((long long)b); }
@@ -252,9 +253,9 @@ __global__ void __launch_bounds__(256) k_g_plan(GArrays g, cudaGraphConditionalH
   const int na = s_na;
   for (int e = na + tid; e < nr; e += blockDim.x) g.rl_dif[e] = -1;
   int np = s_pmax;
-  const bool fits = np + kGUnroll <= g.paircap;
+  const bool fits = np + g.unroll <= g.paircap;
   if (!fits) np = 0;
-  for (int p = tid; p < np + kGUnroll; p += blockDim.x) {
+  for (int p = tid; p < np + g.unroll; p += blockDim.x) {
     int c = 0;
     for (int e = 0; e < na; ++e) c += ((g.s_i[g.rl_dif[e]] - 1) / 2 > p) ? 1 : 0;
     g.nactp[p] = c;
@@ -290,10 +291,10 @@ __global__ void k_g_coefs(GArrays g) {
 // End of a pair-loop iteration (one thread).
 __global__ void k_g_pair_tick(GArrays g, cudaGraphConditionalHandle hc) {
   GState &st = *g.st;
-  const int p = st.pctr + kGUnroll;
+  const int p = st.pctr + g.unroll;
   st.pctr = p;
-  st.kernels += 2 * kGUnroll + 1;
-  // npairs fits the tables (k_g_plan), so the loop ends within paircap / kGUnroll iterations
+  st.kernels += 2 * g.unroll + 1;
+  // npairs fits the tables (k_g_plan), so the loop ends within paircap / unroll iterations
   cudaGraphSetConditional(hc, p < st.npairs ? 1u : 0u);
 }
 

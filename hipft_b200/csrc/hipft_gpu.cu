@@ -165,6 +165,7 @@ struct hipft_gpu {
   size_t adj_rings_cap = 0, adj_rings_n = 0;
   int64_t adj_tape_limit = 0;             // fields the tape may use (0: half the free memory)
   int64_t adj_force_q = 0;                // stage-checkpoint spacing forced by the caller (0: automatic)
+  size_t adj_free_seen = 0;               // free device memory + 1 as seen by the current record (0: not yet)
   double *adjw[8] = {};
   double *d_dpart = nullptr, *d_gring = nullptr, *d_gpart[2] = {};
   double *d_dpole = nullptr;  // [nr][adj_nch] D partials of the pole-row chunks
@@ -2397,12 +2398,12 @@ static int graph_alloc(hipft_gpu *h, int paircap) {
 // subcycle over the whole step at the smallest Euler limit bounds every
 // realization's stage count.
 static int graph_pairs_needed(const hipft_gpu *h, double dt) {
-  if (!h->P.advance_diffusion) return kGUnroll;
+  if (!h->P.advance_diffusion) return kGUnrollMax;
   double dte = h->dt_euler;
   if (h->ragged)
     for (double v : h->r_dt_euler) dte = std::min(dte, v);
   const int64_t s = sts_count(h->P.diffusion_num_method, dt, dte);
-  return (int)((s - 1) / 2) + kGUnroll;
+  return (int)((s - 1) / 2) + kGUnrollMax;
 }
 
 // Launch parameters a capture bakes in besides the buffers; any change (new
@@ -2470,6 +2471,11 @@ static int graph_capture(hipft_gpu *h) {
   G.ragged = h->ragged ? 1 : 0;
   G.strang = h->P.strang_splitting ? 1 : 0;
   G.nadv = (h->adv_time == 1) ? 1 : ((h->adv_time == 2) ? 3 : 4);
+  {
+    const char *e = std::getenv("HIPFT_GRAPH_UNROLL");
+    const int u = e ? std::atoi(e) : kGUnrollMax;  // each iteration boundary costs ~11 us (tick, node relaunch)
+    G.unroll = std::max(2, std::min(kGUnrollMax, u - u % 2));
+  }
   G.ring0 = h->d_ringbuf[0];
   G.ring1 = h->d_ringbuf[1];
   const GArrays g = G;
@@ -2639,7 +2645,7 @@ static int graph_capture(hipft_gpu *h) {
     }
     begin_body(s1, hpair, s2);
     if (first != cudaSuccess) return;
-    for (int q = 0; q < kGUnroll; ++q) pair(s2, q, q > 0);
+    for (int q = 0; q < g.unroll; ++q) pair(s2, q, q > 0);
     k_g_pair_tick<<<1, 1, 0, s2>>>(g, hpair);
     peek();
     end_body(s2);
@@ -3447,9 +3453,12 @@ extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, in
 static int64_t adj_stage_spacing(hipft_gpu *h, int64_t s) {
   int64_t budget = h->adj_tape_limit;
   if (budget <= 0) {
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
-    budget = (int64_t)(fr / 2 / (h->fieldn * sizeof(double)));
+    if (h->adj_free_seen == 0) {  // once per recorded step
+      size_t fr = 0, tot = 0;
+      if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+      h->adj_free_seen = fr + 1;
+    }
+    budget = (int64_t)((h->adj_free_seen - 1) / 2 / (h->fieldn * sizeof(double)));
   }
   if (h->adj_force_q > 0) return h->adj_force_q;
   if (s + 1 <= budget) return 0;
@@ -3848,6 +3857,7 @@ static int adj_check(hipft_gpu *h) {
 static int adj_record(hipft_gpu *h, double dt) {
   TRY(adj_ensure(h));
   h->dring_valid = false;
+  h->adj_free_seen = 0;
   AdjRec R;
   R.dt = dt;
   R.first = h->adj_top;
