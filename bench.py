@@ -19,9 +19,10 @@ Timing: W untimed warm-up steps, then K steps between CUDA events on the
 library's stream (inputs resident in HBM; each field is 1.07 GB, far above
 the 126 MB L2, so no flush is needed), max over ranks.  `e2e` repeats K steps
 through the C ABI with the field copied host->device before and
-device->host after every step.  Multi-GPU: realizations are split across
-ranks (block split, low ranks take the remainder) and every rank advances its
-own share independently -- weak scaling, no data-path collective.
+device->host after every step.  Multi-GPU: every rank advances its own batch
+of nr realizations (realizations rank*nr .. rank*nr+nr-1 of one parameter
+draw) independently -- weak scaling, no data-path collective; `value` is the
+cell-stages of all ranks over the slowest rank's time.
 
 At N = 1 the line also carries:
   "batched_vs_plain": realization-steps/s of the ragged batch, of one batch
@@ -137,12 +138,14 @@ class ClockSampler:
                 "power_w": statistics.median(pw) if pw else None}
 
 
-def make_inputs(wl: dict):
+def make_inputs(wl: dict, copies: int = 1):
+    """Grid, initial map and per-realization parameters of `copies` x nr
+    realizations (one batch of nr per GPU when the run is sharded)."""
     from hipft_b200 import synthetic as S
     t = S.refined_theta(wl["ntm"])
     p = S.uniform_phi(wl["npm1"])
     br = S.bipole_map(t, p, wl["seed"])
-    prm = S.batched_params(wl["nr"], wl["seed"])
+    prm = S.batched_params(wl["nr"] * copies, wl["seed"])
     return t, p, br, prm
 
 
@@ -310,8 +313,11 @@ def run_gpu(args, wl, name):
     from hipft_b200 import synthetic as S
     from hipft_b200.parallel import reduce_timing, split_realizations
 
-    t, p, br, prm = make_inputs(wl)
-    first, nrl = split_realizations(wl["nr"], world, rank)
+    # weak scaling: every GPU advances its own batch of nr realizations
+    # (realizations rank*nr .. rank*nr+nr-1 of one parameter draw); no
+    # collective touches the data path
+    t, p, br, prm = make_inputs(wl, copies=world)
+    first, nrl = split_realizations(wl["nr"] * world, world, rank)
     sl = slice(first, first + nrl)
     ragged = args.schedule == "ragged"
     g = make_handle(H, t, p, br, prm, sl, local, ragged, graph=args.step == "graph")
@@ -419,8 +425,9 @@ def run_gpu(args, wl, name):
         "metric": METRIC, "value": cells / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": name, "grid": [ntm, npm - 2], "realizations": wl["nr"],
-                   "realizations_per_gpu": nrl, "dt_hours": dt, "parallelism": f"realizations/{world}",
+        "config": {"workload": name, "grid": [ntm, npm - 2], "realizations": wl["nr"] * world,
+                   "realizations_per_gpu": nrl, "dt_hours": dt,
+                   "parallelism": f"replicas: {world} GPU(s), {nrl} realizations each",
                    "schedule": ("ragged: each realization its own Euler limit, PTL subcycles and RKG2 stage "
                                 "counts" if ragged else "shared (the reference's MIN/MAX schedule)"),
                    "method": "WENO3+SSPRK(4,3) Strang-split with RKG2 (PTL subcycles), DA every 24 h",
@@ -634,7 +641,7 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
     gc.enable()
     A = MisfitAdjoint(g, D, flow, checkpoint_every=checkpoint_every)
     A.run(f0, target, dts)  # warm-up: tuner, tape allocation (kept by the handle)
-    grad_runs = []
+    grad_runs, phases = [], []
     import gc
     for _ in range(5):
         gc.collect()
@@ -645,6 +652,9 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
         torch.cuda.synchronize()
         grad_runs.append(time.perf_counter() - w0)
         gc.enable()
+        phases.append({"forward_s": A.timing.get("forward_s"), "forward_parts": A.timing.get("forward_parts"),
+                       "reverse_s": A.timing.get("reverse_s"),
+                       "segments": A.timing.get("segments")})
     fwd_s, grad_s = statistics.median(fwd_runs), statistics.median(grad_runs)
     tape = ctypes.c_int64(0)
     g.L.hipft_adj_tape_fields(g.h, ctypes.byref(tape))
@@ -668,7 +678,7 @@ def measure_adjoint(args, local: int, days: float = 27.27, checkpoint_every: int
             "checkpoint_every": checkpoint_every, "segments": -(-len(dts) // checkpoint_every),
             "forward_ms": fwd_s * 1e3, "gradient_ms": grad_s * 1e3, "gradient_over_forward": grad_s / fwd_s,
             "runs": "median of 5 timed runs each", "forward_runs_ms": [x * 1e3 for x in fwd_runs],
-            "gradient_runs_ms": [x * 1e3 for x in grad_runs],
+            "gradient_runs_ms": [x * 1e3 for x in grad_runs], "gradient_phases": phases,
             "loss": loss, "grad_D": float(grads["D"][0]), "grad_f0_norm": float(np.linalg.norm(grads["f0"])),
             "tape_fields_peak": int(tape.value),
             "tape_gb_peak": int(tape.value) * ntm * (npm1 + 1) * 8 / 1e9,

@@ -268,8 +268,9 @@ class MisfitAdjoint:
         g.update_flow()
         self._fbytes = self._dev().numel() * 8
         self._est_fields = 16
-        self._free, self._total = torch.cuda.mem_get_info()
-        self._tape0 = self._tape_fields()
+        if not self._total:  # the first run; later runs find the same free memory (the tape is kept)
+            self._free, self._total = torch.cuda.mem_get_info()
+            self._tape0 = self._tape_fields()
         ckpt, recorded, states = {}, set(), {}
         last0 = ((n - 1) // self.k) * self.k
         taping = True
@@ -278,6 +279,8 @@ class MisfitAdjoint:
             if s % self.k == 0:
                 ckpt[s] = self._dev().clone()
             if s == last0:
+                torch.cuda.synchronize()
+                t_last = time.perf_counter()
                 self._segment_budget()
             if s >= last0 and taping and self._room_to_record():
                 self._record(s, dt)
@@ -289,7 +292,9 @@ class MisfitAdjoint:
             self._step(s, dt)
         fN = g.get_field()
         self._fwd = dict(dts=dts, ckpt=ckpt, recorded=recorded, states=states, last0=last0)
-        self.timing = {"forward_s": time.perf_counter() - t0}
+        t1 = time.perf_counter()
+        # forward_parts: seconds before the last segment, and of the (taped) last segment
+        self.timing = {"forward_s": t1 - t0, "forward_parts": (t_last - t0, t1 - t_last)}
         return fN
 
     def backward(self, gb) -> dict:

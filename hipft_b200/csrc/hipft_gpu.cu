@@ -165,7 +165,7 @@ struct hipft_gpu {
   size_t adj_rings_cap = 0, adj_rings_n = 0;
   int64_t adj_tape_limit = 0;             // fields the tape may use (0: half the free memory)
   int64_t adj_force_q = 0;                // stage-checkpoint spacing forced by the caller (0: automatic)
-  size_t adj_free_seen = 0;               // free device memory + 1 as seen by the current record (0: not yet)
+  size_t adj_free_seen = 0;               // free device memory + 1 as seen at the run's first record (0: not yet)
   double *adjw[8] = {};
   double *d_dpart = nullptr, *d_gring = nullptr, *d_gpart[2] = {};
   double *d_dpole = nullptr;  // [nr][adj_nch] D partials of the pole-row chunks
@@ -3453,7 +3453,7 @@ extern "C" int hipft_get_flux_noalloc(const double *f_dev, int ntm, int npm1, in
 static int64_t adj_stage_spacing(hipft_gpu *h, int64_t s) {
   int64_t budget = h->adj_tape_limit;
   if (budget <= 0) {
-    if (h->adj_free_seen == 0) {  // once per recorded step
+    if (h->adj_free_seen == 0) {  // once per run (reset by hipft_adj_clear / hipft_adj_release)
       size_t fr = 0, tot = 0;
       if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
       h->adj_free_seen = fr + 1;
@@ -3857,7 +3857,6 @@ static int adj_check(hipft_gpu *h) {
 static int adj_record(hipft_gpu *h, double dt) {
   TRY(adj_ensure(h));
   h->dring_valid = false;
-  h->adj_free_seen = 0;
   AdjRec R;
   R.dt = dt;
   R.first = h->adj_top;
@@ -3929,6 +3928,7 @@ extern "C" int hipft_adj_clear(hipft_gpu *h) {
   h->adj_recs.clear();
   h->adj_top = 0;
   h->adj_rings_n = 0;
+  h->adj_free_seen = 0;
   return HIPFT_OK;
 }
 
@@ -3979,6 +3979,7 @@ extern "C" int hipft_adj_release(hipft_gpu *h) {
   h->adj_recs.clear();
   h->adj_top = 0;
   h->adj_top_max = 0;
+  h->adj_free_seen = 0;
   h->adj_rings_n = 0;
   return HIPFT_OK;
 }
