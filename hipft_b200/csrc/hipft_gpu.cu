@@ -988,22 +988,52 @@ static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, co
   return HIPFT_OK;
 }
 
+// HIPFT_ADV_TILE=1 runs WENO3 stages with the tile kernel
+// (k_advection_stage<32, 8, true>) instead of the phi-marching kernel; both
+// give bitwise the same fields, and the tile kernel is kept as the marching
+// kernel's comparison in the tests.
+static bool adv_tile_weno() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("HIPFT_ADV_TILE");
+    v = (e && std::atoi(e) == 1) ? 1 : 0;
+  }
+  return v == 1;
+}
+
+// One explicit advection stage over nz realization slots (rlist maps slot z
+// to a realization when non-null; rdt scales each realization's step).
+// WENO3 stages march along phi (k_adv_weno_march); upwind stages take the
+// tile kernel.
+static void launch_adv_stage(const hipft_gpu *h, const Mesh &M, cudaStream_t s, unsigned nz, const double *x,
+                             const double *f0, double *out, AdvCombine cb, const int *rlist, const double *rdt) {
+  if (h->adv_space == 2 && !adv_tile_weno()) {
+    const unsigned groups = (unsigned)((h->ntm - 1) / 31 + 1);
+    const dim3 blk(32, kAdvWarps);
+    const dim3 grd((groups + kAdvWarps - 1) / kAdvWarps, (unsigned)((h->npm - 2 + kAdvCols - 1) / kAdvCols), nz);
+    auto kern = h->FL.flow2d ? (cb.mode == 0 ? k_adv_weno_march<true, 0> : k_adv_weno_march<true, 1>)
+                             : (cb.mode == 0 ? k_adv_weno_march<false, 0> : k_adv_weno_march<false, 1>);
+    kern<<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n, h->bc_flow_s, cb, rlist, rdt);
+    return;
+  }
+  const dim3 blk(33, 9);  // (TJ+1) x (TK+1) threads for a 32 x 8 tile
+  const dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), nz);
+  if (h->adv_space == 2)
+    k_advection_stage<32, 8, true><<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
+                                                        h->bc_flow_s, cb, rlist, rdt);
+  else
+    k_advection_stage<32, 8, false><<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
+                                                         h->bc_flow_s, cb, rlist, rdt);
+}
+
 static int advection_stage(hipft_gpu *h, const double *x, const double *f0, double *out, AdvCombine cb) {
   {
     ProfScope ps(h, HIPFT_K_RING);
     k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
     LAUNCHED(h);
   }
-  dim3 blk(33, 9);  // (TJ+1) x (TK+1) threads for a 32 x 8 tile
   ProfScope ps(h, HIPFT_K_ADV);
-  if (h->adv_space == 2)
-    k_advection_stage<32, 8, true><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out,
-                                                                                 h->d_ring, h->bc_flow_n,
-                                                                                 h->bc_flow_s, cb);
-  else
-    k_advection_stage<32, 8, false><<<stage_grid(h, 32, 8), blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out,
-                                                                                  h->d_ring, h->bc_flow_n,
-                                                                                  h->bc_flow_s, cb);
+  launch_adv_stage(h, h->M, h->stream, (unsigned)h->nr, x, f0, out, cb, nullptr, nullptr);
   LAUNCHED(h);
   h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * h->nr;
   return HIPFT_OK;
@@ -1172,6 +1202,19 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
     std::vector<size_t> wo;
     for (int q = 0; q < 7; ++q) { wo.push_back(pk.size()); pk.insert(pk.end(), wt[q].begin(), wt[q].end()); }
     for (int q = 0; q < 7; ++q) { wo.push_back(pk.size()); pk.insert(pk.end(), wp[q].begin(), wp[q].end()); }
+    // phi-face rows of the marching advection stage (Weno::ptab): faces
+    // 2..npm, face npm with face 2's weights (src/hipft.f90:7882)
+    const size_t tab0 = (pk.size() + 1) & ~(size_t)1;  // 16-byte aligned rows
+    pk.resize(tab0 + (size_t)(npm - 1) * kPhiTab, 0.0);
+    for (int kf = 2; kf <= npm; ++kf) {
+      const int kw = (kf >= npm) ? 2 : kf;
+      double *row = pk.data() + tab0 + (size_t)(kf - 2) * kPhiTab;
+      const double v[10] = {wp[1][kw - 1], wp[1][kw], wp[0][kw - 1], wp[0][kw], wp[4][kw - 1],
+                            wp[5][kw - 1], wp[2][kw], wp[3][kw],     wp[6][kw - 1], wp[6][kw]};
+      for (int q = 0; q < 10; ++q) row[q] = v[q];
+      row[10] = weno_consts_ok(v[4], v[5], v[6], v[7], v[8], v[9]) ? 1.0 : 0.0;
+      row[11] = (kf <= npm - 1) ? h->dp_i[kf] : 0.0;
+    }
     double *dw = nullptr;
     if ((rc = dalloc(h, &dw, pk.size()))) return bail(rc);
     if ((rc = upload(h, dw, pk))) return bail(rc);
@@ -1179,6 +1222,7 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
     h->W.pt = dw + wo[4]; h->W.mctt = dw + wo[5]; h->W.epst = dw + wo[6];
     h->W.cpp = dw + wo[7]; h->W.mcp = dw + wo[8]; h->W.mp = dw + wo[9]; h->W.cptp = dw + wo[10];
     h->W.pp = dw + wo[11]; h->W.mctp = dw + wo[12]; h->W.epsp = dw + wo[13];
+    h->W.ptab = dw + tab0;
     if ((rc = dalloc(h, &h->d_vt1, (size_t)nr * (nt + 1)))) return bail(rc);
     if ((rc = dalloc(h, &h->d_vp1, (size_t)nr * (ntm + 1)))) return bail(rc);
     if ((rc = dalloc(h, &h->d_at1, (size_t)nr * (ntm + 1)))) return bail(rc);
@@ -2143,16 +2187,8 @@ static int advection_stage_ragged(hipft_gpu *h, const double *x, const double *f
     k_ring_advection<<<h->nr, 256, 0, h->stream>>>(h->M, h->FL, x, h->d_ring);
     LAUNCHED(h);
   }
-  dim3 blk(33, 9);  // (TJ+1) x (TK+1) threads for a 32 x 8 tile
-  dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)n);
   ProfScope ps(h, HIPFT_K_ADV);
-  if (h->adv_space == 2)
-    k_advection_stage<32, 8, true><<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
-                                                               h->bc_flow_s, cb, h->d_rlist_adv, h->d_rdt);
-  else
-    k_advection_stage<32, 8, false><<<grd, blk, 0, h->stream>>>(h->M, h->FL, h->W, x, f0, out, h->d_ring,
-                                                                h->bc_flow_n, h->bc_flow_s, cb, h->d_rlist_adv,
-                                                                h->d_rdt);
+  launch_adv_stage(h, h->M, h->stream, (unsigned)n, x, f0, out, cb, h->d_rlist_adv, h->d_rdt);
   LAUNCHED(h);
   h->cell_updates += (int64_t)h->ntm * (h->npm - 2) * n;
   return HIPFT_OK;
@@ -2510,14 +2546,7 @@ static int graph_capture(hipft_gpu *h) {
   auto adv_stage = [&](cudaStream_t s, const double *x, const double *f0, double *out, AdvCombine cb) {
     k_ring_advection<<<nr, 256, 0, s>>>(M, h->FL, x, h->d_ring);
     peek();
-    const dim3 blk(33, 9);
-    const dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)nr);
-    if (h->adv_space == 2)
-      k_advection_stage<32, 8, true><<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
-                                                          h->bc_flow_s, cb, g.rl_adv, g.rdt);
-    else
-      k_advection_stage<32, 8, false><<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n,
-                                                           h->bc_flow_s, cb, g.rl_adv, g.rdt);
+    launch_adv_stage(h, M, s, (unsigned)nr, x, f0, out, cb, g.rl_adv, g.rdt);
     peek();
   };
   auto advection = [&](double frac) {

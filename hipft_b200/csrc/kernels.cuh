@@ -345,7 +345,13 @@ __device__ __forceinline__ double ap_at(const Mesh &m, const Flow &fl, int j, in
 struct Weno {
   const double *cpt, *mct, *mt, *cptt, *pt, *mctt, *epst;  // theta: D_C_CPt, D_C_MCt, D_M_Tt, D_CP_Tt, D_P_Tt, D_MC_Tt, eps
   const double *cpp, *mcp, *mp, *cptp, *pp, *mctp, *epsp;  // phi
+  // Phi faces k = 2..npm, kPhiTab doubles each at ptab[(k-2)*kPhiTab]: the ten
+  // weights in weno_face's argument order (face npm takes face 2's), a flag
+  // (1.0 when the linear weights and eps lie in weno_face_nr's range) and
+  // dp_i(k) (the cell divergence factor of column k).
+  const double *ptab;
 };
+constexpr int kPhiTab = 12;
 
 // WENO3 face flux (src/hipft.f90:7775-7801).  LN*: LN(j-2), LN(j-1), LN(j);
 // LP*: LP(j-1), LP(j), LP(j+1); weights at indices j-1 (m1) and j (0).
@@ -373,6 +379,73 @@ __device__ __forceinline__ double weno_face(double LNm2, double LNm1, double LN0
   double um = (w0m / sm) * p0m + (w1m / sm) * p1m;
   double up = (w0p / sp) * p0p + (w1p / sp) * p1p;
   return up + um;
+}
+
+// Division by Newton-Raphson refinement, for the marching advection stage.
+// recip_nr(b): 1/b rounded to nearest, from the hardware reciprocal estimate
+// and three steps y' = y + y (1 - b y), the last of which is Markstein's
+// correctly rounding step; quot_nr(a, b, y): a/b rounded to nearest, from
+// q = a y and two corrections q' = q + (a - b q) y whose residuals the fused
+// multiply-add computes exactly (P. Markstein, IBM J. Res. Dev. 34(1), 1990;
+// J.-M. Muller et al., Handbook of Floating-Point Arithmetic, ch. 4).  The
+// quotient of two doubles is never a rounding midpoint, so the result is the
+// IEEE quotient whenever operands, reciprocals and quotients stay well inside
+// the normal range; weno_face_nr checks that range and its caller falls back
+// to weno_face otherwise.  Compared bit for bit with the IEEE division by the
+// tile-kernel comparison in tests/test_gpu_adv_march.py.
+__device__ __forceinline__ double recip_nr(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = fma(-b, y, kOne);
+  y = fma(y, e, y);
+  e = fma(-b, y, kOne);
+  y = fma(y, e, y);
+  e = fma(-b, y, kOne);
+  return fma(y, e, y);
+}
+__device__ __forceinline__ double quot_nr(double a, double b, double y) {
+  double q = a * y;
+  double r = fma(-b, q, a);
+  q = fma(r, y, q);
+  r = fma(-b, q, a);
+  return fma(r, y, q);
+}
+
+// weno_face with the divisions of quot_nr (the two normalising divisions of
+// each side share one reciprocal).  The smoothness denominators are
+// e = eps + 4 t^2 >= eps; ok is cleared unless every e is at most 2^100.  With
+// eps and the linear weights in [2^-100, 2^100] (weno_consts_ok, checked by
+// the caller) every operand, reciprocal and quotient is then a normal double
+// and the face equals weno_face's bit for bit.
+__device__ __forceinline__ double weno_face_nr(double LNm2, double LNm1, double LN0, double LPm1, double LP0,
+                                               double LPp1, double DCMC_m1, double DCMC_0, double DCCP_m1,
+                                               double DCCP_0, double DPT_m1, double DMCT_m1, double DMT_0,
+                                               double DCPT_0, double eps_m1, double eps_0, bool &ok) {
+  double p0m = (kOne + DCMC_m1) * LNm1 - DCMC_m1 * LNm2;
+  double p1m = DCMC_0 * LNm1 + DCCP_m1 * LN0;
+  double p0p = (kOne + DCCP_0) * LP0 - DCCP_0 * LPp1;
+  double p1p = DCCP_m1 * LP0 + DCMC_0 * LPm1;
+  double t0 = DCMC_m1 * (LNm1 - LNm2), t1 = DCCP_m1 * (LN0 - LNm1);
+  double t2 = DCCP_0 * (LPp1 - LP0), t3 = DCMC_0 * (LP0 - LPm1);
+  double e0 = eps_m1 + kFour * (t0 * t0), e1 = eps_m1 + kFour * (t1 * t1);
+  double e2 = eps_0 + kFour * (t2 * t2), e3 = eps_0 + kFour * (t3 * t3);
+  ok = fmax(fmax(e0, e1), fmax(e2, e3)) <= 0x1p100;
+  const double s0 = e0 * e0, s1 = e1 * e1, s2 = e2 * e2, s3 = e3 * e3;
+  double w0m = quot_nr(DPT_m1, s0, recip_nr(s0)), w1m = quot_nr(DMCT_m1, s1, recip_nr(s1));
+  double w0p = quot_nr(DMT_0, s2, recip_nr(s2)), w1p = quot_nr(DCPT_0, s3, recip_nr(s3));
+  double sm = w0m + w1m, sp = w0p + w1p;
+  const double ym = recip_nr(sm), yp = recip_nr(sp);
+  double um = quot_nr(w0m, sm, ym) * p0m + quot_nr(w1m, sm, ym) * p1m;
+  double up = quot_nr(w0p, sp, yp) * p0p + quot_nr(w1p, sp, yp) * p1p;
+  return up + um;
+}
+
+// A face's linear weights (DPT_m1, DMCT_m1, DMT_0, DCPT_0) and epsilons within
+// [2^-100, 2^100], weno_face_nr's range.
+__host__ __device__ inline bool weno_consts_ok(double a, double b, double c, double d, double e, double f) {
+  const double lo = 0x1p-100, hi = 0x1p100;
+  return a >= lo && a <= hi && b >= lo && b <= hi && c >= lo && c <= hi && d >= lo && d <= hi && e >= lo &&
+         e <= hi && f >= lo && f <= hi;
 }
 
 // First-order upwind face flux (src/hipft.f90:7649-7651, 7809-7815).
@@ -599,6 +672,237 @@ __global__ void __launch_bounds__((TJ + 1) * (TK + 1)) k_advection_stage(
   out[q] = y;
   if (k == 2) out[q + (int64_t)(npm - 2) * m.ldt] = y;
   if (k == npm - 1) out[q - (int64_t)(npm - 2) * m.ldt] = y;
+}
+
+// One WENO3 advection stage that marches along phi (the same faces,
+// divergence, pole rows, seam and combine as k_advection_stage<., ., true>,
+// with the same values: bitwise the same results).  The eight divisions per
+// face bound this stage; the faces divide by Newton-Raphson refinement
+// (weno_face_nr: correctly rounded, so the IEEE quotients; weno_face where
+// its range check fails), which ran at 1.8x the IEEE routine's throughput.
+//
+// Each warp owns a group of theta rows and a chunk of kAdvCols phi columns:
+// lane l holds row r = j0 - 1 + l (j0 = 1 + 31 g for row group g), so lanes
+// 1..31 own the cells of rows j0..j0+30 and lane 0's row, which belongs to the
+// group below, only supplies the theta face between rows j0-1 and j0.  Per
+// column k every lane computes one theta face (the face between its row and
+// the next) and one phi face (between columns k and k+1 of its row): each face
+// once, two per cell.  The theta face's LN/LP terms of the neighbouring rows
+// come by warp shuffles (lanes 31, 0 and 1 also load the halo rows j0-2,
+// j0+31 and j0+32), the phi face's from a sliding window of the row's last
+// columns, and the cell takes the lower theta face from lane l-1 and the
+// lower phi face from the previous column.  Both faces are evaluated before
+// either range check, so the scheduler has two independent chains.  The phi
+// face's weights and the column's dp_i come as six 16-byte loads of one
+// table row (Weno::ptab), the same address across the warp.  The next
+// column's inputs are loaded one column ahead.  No block barrier: warps are
+// independent.
+constexpr int kAdvCols = 64;   // phi columns per warp
+constexpr int kAdvWarps = 2;   // row groups per block (8 blocks per SM: at most 128 registers)
+
+template <bool FLOW2D, int MODE>
+__global__ void __launch_bounds__(32 * kAdvWarps, 8) k_adv_weno_march(
+    Mesh m, Flow fl, Weno wn, const double *__restrict__ x, const double *__restrict__ f0, double *out,
+    const double *__restrict__ ring, double bcn, double bcs, AdvCombine cb, const int *__restrict__ rlist,
+    const double *__restrict__ rdt) {
+  const int l = threadIdx.x;
+  const int ntm = m.ntm, npm = m.npm;
+  const int j0 = 1 + 31 * (int)(blockIdx.x * kAdvWarps + threadIdx.y);
+  const int kc0 = 2 + (int)blockIdx.y * kAdvCols;
+  if (j0 > ntm || kc0 > npm - 1) return;  // uniform per warp
+  if (rlist && rlist[blockIdx.z] < 0) return;
+  const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
+  if (rdt) cb.C = cb.C * rdt[i - 1];
+  const int kc1 = min(kc0 + kAdvCols - 1, npm - 1);
+  const int r = j0 - 1 + l;
+  const int hr = (l == 31) ? j0 - 2 : (l == 0) ? j0 + 31 : (l == 1) ? j0 + 32 : 0;  // halo row (0: none)
+  const bool rin = r >= 1 && r <= ntm, hin = hr >= 1 && hr <= ntm;
+  const int64_t pbase = (int64_t)(i - 1) * m.plane;
+  const int ldt = m.ldt, ldv = fl.ldv;
+  // this lane's row and halo row of realization i (clamped into the plane
+  // when out of range; such lanes use zeros instead of their loads)
+  const double *xr = x + pbase + (rin ? r - 1 : 0);
+  const double *xh = x + pbase + (hin ? hr - 1 : 0);
+
+  // theta face jf = r + 1: none, first-order upwind (faces 2 and ntm) or WENO3
+  const int jf = r + 1;
+  const bool tface = jf >= 2 && jf <= ntm;
+  const bool tup = tface && (jf == 2 || jf == ntm);
+  const bool wup = __any_sync(0xffffffffu, tup);
+  const int jw = min(max(jf, 2), m.nt - 1);
+  const double w0 = wn.mct[jw - 1], w1 = wn.mct[jw], w2 = wn.cpt[jw - 1], w3 = wn.cpt[jw], w4 = wn.pt[jw - 1];
+  const double w5 = wn.mctt[jw - 1], w6 = wn.mt[jw], w7 = wn.cptt[jw], w8 = wn.epst[jw - 1], w9 = wn.epst[jw];
+  const bool tok = weno_consts_ok(w4, w5, w6, w7, w8, w9);
+  // divergence factors of row r
+  const int rc = min(max(r, 1), ntm);
+  const double sth0 = m.sth[rc], sth1 = m.sth[rc + 1], sti = m.st_i[rc], dti = m.dt_i[rc];
+  const bool cell = l >= 1 && rin;
+  const bool pface = r >= 2 && r <= ntm - 1;
+  const double apole = (r == 1) ? ring[2 * (i - 1)] * bcn : -ring[2 * (i - 1) + 1] * bcs;
+  const bool pole = r == 1 || r == ntm;
+
+  // LN(c) = half x(c) (vt(c)+at(c)) and LP(c) = half x(c) (vt(c+1)-at(c)) are
+  // formed as x(c) * (half (vt(c)+at(c))) etc.: halving is exact, so the
+  // products are the reference's (for |x| above 2^-1021, i.e. any map).
+  // 1-D flows: the halved theta terms of the row and the halo row, and the
+  // halved phi terms vp(j)+ap(j), vp(j)-ap(j), per row.
+  double tn = 0.0, tp = 0.0, htn = 0.0, htp = 0.0, pn = 0.0, pp = 0.0, vtu = 0.0;
+  if (!FLOW2D) {
+    const double *vt = fl.vt1 + (int64_t)(i - 1) * (m.nt + 1), *at = fl.at1 + (int64_t)(i - 1) * (m.ntm + 1);
+    const double *vp = fl.vp1 + (int64_t)(i - 1) * (m.ntm + 1), *ap = fl.ap1 + (int64_t)(i - 1) * (m.ntm + 1);
+    if (rin) {
+      tn = kHalf * (vt[r] + at[r]);
+      tp = kHalf * (vt[r + 1] - at[r]);
+      pn = kHalf * (vp[r] + ap[r]);
+      pp = kHalf * (vp[r] - ap[r]);
+    }
+    if (hin) {
+      htn = kHalf * (vt[hr] + at[hr]);
+      htp = kHalf * (vt[hr + 1] - at[hr]);
+    }
+    if (tup) vtu = vt[jf];
+  }
+  // 2-D flows: this lane's row of the planes of realization i (theta stride ldv)
+  const int64_t vbase = (int64_t)(i - 1) * fl.vplane;
+  const double *vtr = fl.vt + vbase + (rin ? r - 1 : 0), *atr = fl.at + vbase + (rin ? r - 1 : 0);
+  const double *vth = fl.vt + vbase + (hin ? hr - 1 : 0), *ath = fl.at + vbase + (hin ? hr - 1 : 0);
+  const double *vpr = fl.vp + vbase + (rin ? r - 1 : 0), *apr = fl.ap + vbase + (rin ? r - 1 : 0);
+
+  // column c (wrapped onto 1..npm-1) of the row: x, and the halved phi terms
+  auto xload = [&](int c) -> double {
+    const int cw = wrap_cell(m, c);
+    return rin ? xr[(int64_t)(cw - 1) * ldt] : 0.0;
+  };
+  auto vN = [&](int c) -> double {
+    if (!FLOW2D) return pn;
+    const int cw = wrap_cell(m, c);
+    return rin ? kHalf * (vpr[(int64_t)(cw - 1) * ldv] + apr[(int64_t)(cw - 1) * ldv]) : 0.0;
+  };
+  auto vP = [&](int c) -> double {
+    if (!FLOW2D) return pp;
+    const int cw = wrap_cell(m, c);
+    return rin ? kHalf * (vpr[(int64_t)cw * ldv] - apr[(int64_t)(cw - 1) * ldv]) : 0.0;
+  };
+  // the phi-face table row of face kf (2..npm)
+  auto ptab = [&](int kf) -> const double2 * {
+    return reinterpret_cast<const double2 *>(wn.ptab + (int64_t)(kf - 2) * kPhiTab);
+  };
+
+  // window: LN at k-1, k, k+1; LP at k, k+1; x at k, k+1; the lower phi face
+  // of column k and dp_i(k)
+  double LN0, LN1, LN2, LP0, LP1, xk, xk1, Fplo, dpk;
+  {
+    const double xm2 = xload(kc0 - 2), xm1 = xload(kc0 - 1), x0 = xload(kc0), x1 = xload(kc0 + 1);
+    const double LNm2 = xm2 * vN(kc0 - 2);
+    LN0 = xm1 * vN(kc0 - 1);
+    LN1 = x0 * vN(kc0);
+    LN2 = x1 * vN(kc0 + 1);
+    const double LPm1 = xm1 * vP(kc0 - 1);
+    LP0 = x0 * vP(kc0);
+    LP1 = x1 * vP(kc0 + 1);
+    const double2 *T = ptab(kc0);
+    const double2 q0 = T[0], q1 = T[1], q2 = T[2], q3 = T[3], q4 = T[4], q5 = T[5];
+    bool ok;
+    double F = weno_face_nr(LNm2, LN0, LN1, LPm1, LP0, LP1, q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y, q4.x,
+                            q4.y, ok);
+    if (!(ok && q5.x != 0.0))
+      F = weno_face(LNm2, LN0, LN1, LPm1, LP0, LP1, q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y, q4.x, q4.y);
+    Fplo = pface ? F : 0.0;
+    dpk = q5.y;
+    xk = x0;
+    xk1 = x1;
+  }
+  // loads one column ahead: x(r, k+2) for the phi window, the halo row at
+  // column k, f0 at column k, and the 2-D flows (theta at column k, phi at
+  // column k+2); the last iteration's loads reach column npm at most, which
+  // is inside the planes
+  double xn = xload(kc0 + 2);
+  double xhn = hin ? xh[(int64_t)(kc0 - 1) * ldt] : 0.0;
+  double fv = (MODE != 0 && cell) ? f0[pbase + (int64_t)(kc0 - 1) * ldt + (r - 1)] : 0.0;
+  double vt0 = 0.0, vt1 = 0.0, at0 = 0.0, vh0 = 0.0, vh1 = 0.0, ah0 = 0.0, vNn = pn, vPn = pp;
+  if (FLOW2D) {
+    const int64_t o = (int64_t)(kc0 - 1) * ldv;
+    vt0 = rin ? vtr[o] : 0.0;
+    vt1 = rin ? vtr[o + 1] : 0.0;
+    at0 = rin ? atr[o] : 0.0;
+    vh0 = hin ? vth[o] : 0.0;
+    vh1 = hin ? vth[o + 1] : 0.0;
+    ah0 = hin ? ath[o] : 0.0;
+    vNn = vN(kc0 + 2);
+    vPn = vP(kc0 + 2);
+  }
+
+  for (int k = kc0; k <= kc1; ++k) {
+    const double xc2 = xn, xhc = xhn, fc = fv;
+    double ctn = tn, ctp = tp, chn = htn, chp = htp, cvu = vtu;
+    const double cN = vNn, cP = vPn;
+    if (FLOW2D) {
+      ctn = kHalf * (vt0 + at0);
+      ctp = kHalf * (vt1 - at0);
+      chn = kHalf * (vh0 + ah0);
+      chp = kHalf * (vh1 - ah0);
+      cvu = vt1;
+    }
+    xn = xload(k + 3);
+    xhn = hin ? xh[(int64_t)k * ldt] : 0.0;
+    if (MODE != 0 && cell) fv = f0[pbase + (int64_t)k * ldt + (r - 1)];
+    if (FLOW2D) {
+      const int64_t o = (int64_t)k * ldv;
+      vt0 = rin ? vtr[o] : 0.0;
+      vt1 = rin ? vtr[o + 1] : 0.0;
+      at0 = rin ? atr[o] : 0.0;
+      vh0 = hin ? vth[o] : 0.0;
+      vh1 = hin ? vth[o + 1] : 0.0;
+      ah0 = hin ? ath[o] : 0.0;
+      vNn = vN(k + 3);
+      vPn = vP(k + 3);
+    }
+    const double2 *T = ptab(k + 1);
+    const double2 q0 = T[0], q1 = T[1], q2 = T[2], q3 = T[3], q4 = T[4], q5 = T[5];
+    // phi face k+1: LN at k-1, k, k+1; LP at k, k+1, k+2
+    const double LN3 = xc2 * cN, LP2 = xc2 * cP;
+    // theta face r+1 of column k: LN at r-1, r, r+1; LP at r, r+1, r+2
+    const double LNt = xk * ctn, LPt = xk * ctp;
+    const double LNh = xhc * chn, LPh = xhc * chp;
+    const double LNrm = __shfl_sync(0xffffffffu, l == 31 ? LNh : LNt, (l + 31) & 31);
+    const double LNrp = __shfl_sync(0xffffffffu, l == 0 ? LNh : LNt, (l + 1) & 31);
+    const double LPrp = __shfl_sync(0xffffffffu, l == 0 ? LPh : LPt, (l + 1) & 31);
+    const double LPrpp = __shfl_sync(0xffffffffu, l <= 1 ? LPh : LPt, (l + 2) & 31);
+    // both faces first (independent work for the scheduler), then the rare
+    // IEEE-division recomputations
+    bool okp, okt;
+    double Fphi = weno_face_nr(LN0, LN1, LN2, LP0, LP1, LP2, q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y, q4.x,
+                               q4.y, okp);
+    double Ft = weno_face_nr(LNrm, LNt, LNrp, LPt, LPrp, LPrpp, w0, w1, w2, w3, w4, w5, w6, w7, w8, w9, okt);
+    if (!(okp && q5.x != 0.0))
+      Fphi = weno_face(LN0, LN1, LN2, LP0, LP1, LP2, q0.x, q0.y, q1.x, q1.y, q2.x, q2.y, q3.x, q3.y, q4.x, q4.y);
+    if (!(okt && tok)) Ft = weno_face(LNrm, LNt, LNrp, LPt, LPrp, LPrpp, w0, w1, w2, w3, w4, w5, w6, w7, w8, w9);
+    if (!pface) Fphi = 0.0;
+    if (wup) {  // x(r+1) for the upwind faces 2 and ntm
+      const double xr1 = __shfl_sync(0xffffffffu, l == 0 ? xhc : xk, (l + 1) & 31);
+      if (tup) Ft = upwind_flux(cvu, fl.upwind, xr1, xk);
+    }
+    if (!tface) Ft = 0.0;
+    const double Ftlo = __shfl_sync(0xffffffffu, Ft, (l + 31) & 31);
+    const double aop = pole ? apole : ((sth1 * Ft - sth0 * Ftlo) * sti * dti + (Fphi - Fplo) * sti * dpk);
+    const double y = MODE == 0 ? xk - cb.C * aop : cb.A * fc + cb.B * xk - cb.C * aop;
+    if (cell) {
+      double *o = out + pbase + (int64_t)(k - 1) * ldt + (r - 1);
+      *o = y;
+      if (k == 2) o[(int64_t)(npm - 2) * ldt] = y;
+      if (k == npm - 1) o[-(int64_t)(npm - 2) * ldt] = y;
+    }
+    // slide the window
+    Fplo = Fphi;
+    dpk = q5.y;
+    LN0 = LN1;
+    LN1 = LN2;
+    LN2 = LN3;
+    LP0 = LP1;
+    LP1 = LP2;
+    xk = xk1;
+    xk1 = xc2;
+  }
 }
 
 // CFL limit, get_flow_dtmax (src/hipft.f90:7321-7327): min over interior
