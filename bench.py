@@ -62,9 +62,9 @@ METRIC = "FP64 Gcell-updates/s"
 UNIT = "Gcell-updates/s"
 STS_BYTES_PER_CELL = 40  # RKG2 stage k>=2: read Y_{k-1}, Y_{k-2}, u0, dty0; write Y_k
 # two-stage kernel per HIPFT_STS_PAIR value (the library's default is 5); the
-# timed region of a "launch" is the kernel plus, for 4 and 5, its pole-row launch
-STS_KERNELS = {"1": "k_sts_pair", "2": "k_sts_pair_p", "3": "k_sts_pair_march",
-               "4": "k_sts_pair_ws+k_pair_poles", "5": "k_sts_pair_ws<rows2>+k_pair_poles"}
+# timed region of a "launch" is the kernel plus its pole-row launch
+STS_KERNELS = {"4": "k_sts_pair_ws+k_pair_poles", "5": "k_sts_pair_ws<rows2>+k_pair_poles",
+               "6": "k_sts_pair_ws<rows2, bulk stores>+k_pair_poles"}
 
 WORKLOADS = {
     "batched64_1024x2048": dict(ntm=1024, npm1=2049, nr=64, seed=1),

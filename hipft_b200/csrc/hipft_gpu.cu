@@ -51,10 +51,9 @@ constexpr int kNBuf = 8;  // current field + scratch: u0, dty0, two inputs and u
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
 // Two-stage kernel kinds (see the autotuner) and the plan a handle uses.
-enum { PK_SINGLE = 0, PK_TILE = 1, PK_WS_ROWS1 = 4, PK_WS_ROWS2 = 5, PK_WS_BULK = 6, PK_WS_QUAD = 7 };
+enum { PK_SINGLE = 0, PK_WS_ROWS1 = 4, PK_WS_ROWS2 = 5, PK_WS_BULK = 6, PK_WS_QUAD = 7 };
 struct PairPlan {
   int kind = -1;    // PK_*; -1: not chosen yet
-  int shape = 0;    // kPairShapes index (PK_TILE)
   int ctas_per_sm = 2;
   double ms = 0.0;  // timed ms per launch pair (0: not timed)
   int candidates = 0;
@@ -567,53 +566,6 @@ static WsMaps ws_maps(hipft_gpu *h, const double *ykm1, const double *ykm2, cons
   return tm;
 }
 
-// Tile shapes of the one-CTA-per-tile two-stage kernel (theta rows x phi
-// columns).
-struct PairShape {
-  const char *name;
-  int tj, tk;
-  size_t smem;
-  void (*launch)(dim3, cudaStream_t, const Mesh &, const double *, const double *, const double *, const double *,
-                 const double *, double *, double *, const double *, double, double, const PairArgs &,
-                 const RingOut &);
-};
-
-template <int TJ, int TK, int MINB>
-static void launch_pair(dim3 g, cudaStream_t s, const Mesh &m, const double *dfac, const double *ykm1,
-                        const double *ykm2, const double *u0, const double *dty0, double *ok, double *ok1,
-                        const double *rin, double bcn, double bcs, const PairArgs &pa, const RingOut &ro) {
-  k_sts_pair<TJ, TK, MINB><<<g, kPThreads, pair_smem_bytes<TJ, TK>(), s>>>(m, dfac, ykm1, ykm2, u0, dty0, ok, ok1,
-                                                                          rin, bcn, bcs, pa, ro);
-}
-
-template <int TJ, int TK, int MINB>
-static cudaError_t pair_attr() {
-  return cudaFuncSetAttribute(k_sts_pair<TJ, TK, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)pair_smem_bytes<TJ, TK>());
-}
-
-static const PairShape kPairShapes[] = {
-    {"128x8", 128, 8, pair_smem_bytes<128, 8>(), launch_pair<128, 8, 4>},
-    {"128x4", 128, 4, pair_smem_bytes<128, 4>(), launch_pair<128, 4, 4>},
-    {"64x8", 64, 8, pair_smem_bytes<64, 8>(), launch_pair<64, 8, 4>},
-    {"64x16", 64, 16, pair_smem_bytes<64, 16>(), launch_pair<64, 16, 4>},
-    {"128x16", 128, 16, pair_smem_bytes<128, 16>(), launch_pair<128, 16, 2>},
-    {"256x8", 256, 8, pair_smem_bytes<256, 8>(), launch_pair<256, 8, 2>},
-    {"256x4", 256, 4, pair_smem_bytes<256, 4>(), launch_pair<256, 4, 3>},
-};
-constexpr int kNPairShapes = (int)(sizeof(kPairShapes) / sizeof(kPairShapes[0]));
-
-static cudaError_t pair_attrs_all() {
-  cudaError_t e;
-  if ((e = pair_attr<128, 8, 4>()) != cudaSuccess) return e;
-  if ((e = pair_attr<128, 4, 4>()) != cudaSuccess) return e;
-  if ((e = pair_attr<64, 8, 4>()) != cudaSuccess) return e;
-  if ((e = pair_attr<64, 16, 4>()) != cudaSuccess) return e;
-  if ((e = pair_attr<128, 16, 2>()) != cudaSuccess) return e;
-  if ((e = pair_attr<256, 8, 2>()) != cudaSuccess) return e;
-  return pair_attr<256, 4, 3>();
-}
-
 // ------------------------------------------------------------ autotuner
 // The two-stage launch has several implementations whose speed depends on
 // the grid and the batch.  The persistent warp-specialised family shares one
@@ -623,20 +575,16 @@ static cudaError_t pair_attrs_all() {
 // stores (PK_WS_BULK), one row per thread (PK_WS_ROWS1).  On the first
 // two-stage super-step of a grid size (ntm, npm, nr) on a device the library
 // times each of them over a few launches on the handle's own buffers and
-// keeps the fastest for the process.  The one-CTA-per-tile kernels (PK_TILE,
-// seven tile shapes) sum the pole rings in another order, so they are not
-// candidates -- a run's result must not depend on timing noise -- and are
-// selected explicitly: HIPFT_STS_PAIR (0: one stage per launch, 1: tiles of
-// HIPFT_PAIR_TILE, 4/5/6: the warp-specialised kinds, 7: four stages per pass
-// on the interior theta blocks) fixes the choice, and HIPFT_TUNE=0 takes
-// PK_WS_ROWS2 at 2 CTAs per SM without timing.  The four-stage path
-// (PK_WS_QUAD, sts_quad_ws.cuh) computes the same cell values and is a
-// candidate whenever the grid has interior blocks.
+// keeps the fastest for the process.  HIPFT_STS_PAIR (0: one stage per
+// launch, 4/5/6: the warp-specialised kinds, 7: four stages per pass on the
+// interior theta blocks) fixes the choice, and HIPFT_TUNE=0 takes PK_WS_ROWS2
+// at 2 CTAs per SM without timing.  The four-stage path (PK_WS_QUAD,
+// sts_quad_ws.cuh) computes the same cell values and is a candidate whenever
+// the grid has interior blocks.
 
 static const char *pair_kind_name(int k) {
   switch (k) {
     case PK_SINGLE: return "single-stage";
-    case PK_TILE: return "tile";
     case PK_WS_ROWS1: return "ws-rows1";
     case PK_WS_ROWS2: return "ws-rows2";
     case PK_WS_BULK: return "ws-bulk";
@@ -652,12 +600,7 @@ static bool env_plan(PairPlan &p) {
   const char *e = std::getenv("HIPFT_STS_PAIR");
   if (e) {
     const int v = std::atoi(e);
-    p.kind = (v == 0 || v == 1 || v == 4 || v == 6 || v == 7) ? v : PK_WS_ROWS2;
-    if (p.kind == PK_TILE) {
-      const char *t = std::getenv("HIPFT_PAIR_TILE");
-      for (int q = 0; t && q < kNPairShapes; ++q)
-        if (std::strcmp(t, kPairShapes[q].name) == 0) p.shape = q;
-    }
+    p.kind = (v == 0 || v == 4 || v == 6 || v == 7) ? v : PK_WS_ROWS2;
     return true;
   }
   const char *t = std::getenv("HIPFT_TUNE");
@@ -683,51 +626,42 @@ static int sts_pair_plan(hipft_gpu *h, const PairPlan &pl, const double *ykm1, c
   static_assert(kWK == kPK && kWJ == kPJ, "the two-stage kernels share one tile shape");
   {
     ProfScope ps(h, HIPFT_K_STS);
-    if (pl.kind != PK_TILE) {
-      const int nkt = (h->npm - 2 + kWK - 1) / kWK;
-      RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
-      const int grid = std::min(h->ptab.ntiles, pl.ctas_per_sm * h->num_sms);
-      const PairArgs pa{ca, cb, h->d_err};
-      const double *rin = h->d_ringbuf[h->ring_cur];
-      const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
-      // programmatic dependent launch: may overlap the previous pair's
-      // k_pair_poles (the kernel's pole tiles wait for it)
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3((unsigned)grid);
-      cfg.blockDim = dim3(kWThreads);
-      cfg.dynamicSmemBytes = kWSmem;
-      cfg.stream = h->stream;
-      cudaLaunchAttribute attr[1];
-      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
-      cfg.attrs = attr;
-      cfg.numAttrs = 1;
-      cudaError_t le;
-      // bulk stores need 16-byte aligned output columns (ldt and the plane
-      // are multiples of 16 elements)
-      const bool aligned = ((reinterpret_cast<uintptr_t>(out_k) | reinterpret_cast<uintptr_t>(out_k1)) & 15) == 0;
-      if (pl.kind == PK_WS_BULK && aligned)
-        le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true, true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
-                                dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
-      else if (pl.kind == PK_WS_ROWS1)
-        le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0,
-                                out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
-      else
-        le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0,
-                                out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
-      if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
-      LAUNCHED(h);
-      dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
-      k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
-                                                       h->bc_diff_n, h->bc_diff_s, pa, ro, h->pole);
-    } else {
-      const PairShape &sh = kPairShapes[pl.shape];
-      const int nkt = (h->npm - 2 + sh.tk - 1) / sh.tk;
-      RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
-      dim3 grd((unsigned)((h->ntm + sh.tj - 1) / sh.tj), (unsigned)nkt, (unsigned)h->nr);
-      sh.launch(grd, h->stream, h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k, out_k1, h->d_ringbuf[h->ring_cur],
-                h->bc_diff_n, h->bc_diff_s, PairArgs{ca, cb, h->d_err}, ro);
-    }
+    const int nkt = (h->npm - 2 + kWK - 1) / kWK;
+    RingOut ro{h->d_ringbuf[1 - h->ring_cur], h->d_rpart, h->d_rcount, nkt};
+    const int grid = std::min(h->ptab.ntiles, pl.ctas_per_sm * h->num_sms);
+    const PairArgs pa{ca, cb, h->d_err};
+    const double *rin = h->d_ringbuf[h->ring_cur];
+    const WsMaps tmaps = ws_maps(h, ykm1, ykm2, u0, dty0);
+    // programmatic dependent launch: may overlap the previous pair's
+    // k_pair_poles (the kernel's pole tiles wait for it)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3(kWThreads);
+    cfg.dynamicSmemBytes = kWSmem;
+    cfg.stream = h->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = (ws_pdl() && overlap_prev) ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t le;
+    // bulk stores need 16-byte aligned output columns (ldt and the plane
+    // are multiples of 16 elements)
+    const bool aligned = ((reinterpret_cast<uintptr_t>(out_k) | reinterpret_cast<uintptr_t>(out_k1)) & 15) == 0;
+    if (pl.kind == PK_WS_BULK && aligned)
+      le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true, true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0,
+                              dty0, out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+    else if (pl.kind == PK_WS_ROWS1)
+      le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<false>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0,
+                              out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+    else
+      le = cudaLaunchKernelEx(&cfg, k_sts_pair_ws<true>, h->M, (const double *)h->DC.dfac, ykm1, ykm2, u0, dty0,
+                              out_k, out_k1, rin, h->bc_diff_n, h->bc_diff_s, pa, ro, h->ptab, tmaps);
+    if (le != cudaSuccess) return fail(h, HIPFT_ECUDA, "k_sts_pair_ws launch: %s", cudaGetErrorString(le));
+    LAUNCHED(h);
+    dim3 pg((unsigned)h->nr, (unsigned)h->pole_nch);
+    k_pair_poles<<<pg, kPoleThreads, 0, h->stream>>>(h->M, h->DC.dfac, ykm1, ykm2, u0, dty0, out_k1, rin,
+                                                     h->bc_diff_n, h->bc_diff_s, pa, ro, h->pole);
     LAUNCHED(h);
   }
   h->ring_cur = 1 - h->ring_cur;
@@ -988,33 +922,43 @@ static int diffusion_stage(hipft_gpu *h, const double *x, const double *ykm2, co
   return HIPFT_OK;
 }
 
-// HIPFT_ADV_TILE=1 runs WENO3 stages with the tile kernel
-// (k_advection_stage<32, 8, true>) instead of the phi-marching kernel; both
-// give bitwise the same fields, and the tile kernel is kept as the marching
-// kernel's comparison in the tests.
-static bool adv_tile_weno() {
+// HIPFT_ADV_KERNEL selects the WENO3 stage kernel: "tile" the tile kernel
+// (k_advection_stage<32, 8, true>), "march" the phi-marching kernel on any
+// grid; unset, the library decides by grid size.  Both give bitwise the same
+// fields; the tests compare the two.
+static int adv_kernel_env() {
   static int v = -1;
   if (v < 0) {
-    const char *e = std::getenv("HIPFT_ADV_TILE");
-    v = (e && std::atoi(e) == 1) ? 1 : 0;
+    const char *e = std::getenv("HIPFT_ADV_KERNEL");
+    v = (e && std::strcmp(e, "tile") == 0) ? 1 : (e && std::strcmp(e, "march") == 0) ? 2 : 0;
   }
-  return v == 1;
+  return v;
 }
 
 // One explicit advection stage over nz realization slots (rlist maps slot z
 // to a realization when non-null; rdt scales each realization's step).
-// WENO3 stages march along phi (k_adv_weno_march); upwind stages take the
-// tile kernel.
+// WENO3 stages march along phi (k_adv_weno_march) when the grid, in chunks of
+// 64 or 32 phi columns, holds 1.5 waves of warps (16 resident per SM): on one
+// 1024 x 2048 realization the tile kernel is faster (0.090 against 0.102 ms),
+// on 64 of them the marching kernel (3.97 against 5.57 ms).  Upwind stages
+// take the tile kernel.
 static void launch_adv_stage(const hipft_gpu *h, const Mesh &M, cudaStream_t s, unsigned nz, const double *x,
                              const double *f0, double *out, AdvCombine cb, const int *rlist, const double *rdt) {
-  if (h->adv_space == 2 && !adv_tile_weno()) {
-    const unsigned groups = (unsigned)((h->ntm - 1) / 31 + 1);
-    const dim3 blk(32, kAdvWarps);
-    const dim3 grd((groups + kAdvWarps - 1) / kAdvWarps, (unsigned)((h->npm - 2 + kAdvCols - 1) / kAdvCols), nz);
-    auto kern = h->FL.flow2d ? (cb.mode == 0 ? k_adv_weno_march<true, 0> : k_adv_weno_march<true, 1>)
-                             : (cb.mode == 0 ? k_adv_weno_march<false, 0> : k_adv_weno_march<false, 1>);
-    kern<<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n, h->bc_flow_s, cb, rlist, rdt);
-    return;
+  if (h->adv_space == 2 && adv_kernel_env() != 1) {
+    const int64_t groups = (h->ntm - 1) / 31 + 1, fill = 24LL * h->num_sms;
+    auto warps = [&](int ncol) { return groups * ((h->npm - 2 + ncol - 1) / ncol) * (int64_t)nz; };
+    int ncol = kAdvColsMax;
+    while (ncol > 8 && warps(ncol) < fill) ncol /= 2;
+    if (ncol >= 32 || adv_kernel_env() == 2) {
+      const dim3 blk(32, kAdvWarps);
+      const dim3 grd((unsigned)((groups + kAdvWarps - 1) / kAdvWarps), (unsigned)((h->npm - 2 + ncol - 1) / ncol),
+                     nz);
+      auto kern = h->FL.flow2d ? (cb.mode == 0 ? k_adv_weno_march<true, 0> : k_adv_weno_march<true, 1>)
+                               : (cb.mode == 0 ? k_adv_weno_march<false, 0> : k_adv_weno_march<false, 1>);
+      kern<<<grd, blk, 0, s>>>(M, h->FL, h->W, x, f0, out, h->d_ring, h->bc_flow_n, h->bc_flow_s, cb, rlist, rdt,
+                               ncol);
+      return;
+    }
   }
   const dim3 blk(33, 9);  // (TJ+1) x (TK+1) threads for a 32 x 8 tile
   const dim3 grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), nz);
@@ -1122,8 +1066,7 @@ extern "C" int hipft_gpu_create(const hipft_grid *g, const hipft_params *prm, hi
   if ((rc = dalloc(h, &h->d_rcount, (size_t)nr))) return bail(rc);
   if ((rc = dalloc(h, &h->d_err, 1))) return bail(rc);
   if (cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream) != cudaSuccess) return bail(HIPFT_ECUDA);
-  if (pair_attrs_all() != cudaSuccess ||
-      cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
+  if (cudaFuncSetAttribute(k_sts_pair_ws<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
       cudaFuncSetAttribute(k_sts_pair_ws<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kWSmem) !=
           cudaSuccess ||
@@ -3220,8 +3163,6 @@ extern "C" int hipft_gpu_describe(hipft_gpu *h, char *buf, size_t len) {
   char kind[128];
   if (p.kind < 0)
     std::snprintf(kind, sizeof kind, "not chosen yet");
-  else if (p.kind == PK_TILE)
-    std::snprintf(kind, sizeof kind, "tile %s", kPairShapes[p.shape].name);
   else if (p.kind == PK_SINGLE)
     std::snprintf(kind, sizeof kind, "%s", pair_kind_name(p.kind));
   else

@@ -681,7 +681,7 @@ __global__ void __launch_bounds__((TJ + 1) * (TK + 1)) k_advection_stage(
 // (weno_face_nr: correctly rounded, so the IEEE quotients; weno_face where
 // its range check fails), which ran at 1.8x the IEEE routine's throughput.
 //
-// Each warp owns a group of theta rows and a chunk of kAdvCols phi columns:
+// Each warp owns a group of theta rows and a chunk of ncol phi columns:
 // lane l holds row r = j0 - 1 + l (j0 = 1 + 31 g for row group g), so lanes
 // 1..31 own the cells of rows j0..j0+30 and lane 0's row, which belongs to the
 // group below, only supplies the theta face between rows j0-1 and j0.  Per
@@ -697,23 +697,23 @@ __global__ void __launch_bounds__((TJ + 1) * (TK + 1)) k_advection_stage(
 // table row (Weno::ptab), the same address across the warp.  The next
 // column's inputs are loaded one column ahead.  No block barrier: warps are
 // independent.
-constexpr int kAdvCols = 64;   // phi columns per warp
+constexpr int kAdvColsMax = 64;  // phi columns per warp (fewer when the grid would not fill the GPU)
 constexpr int kAdvWarps = 2;   // row groups per block (8 blocks per SM: at most 128 registers)
 
 template <bool FLOW2D, int MODE>
 __global__ void __launch_bounds__(32 * kAdvWarps, 8) k_adv_weno_march(
     Mesh m, Flow fl, Weno wn, const double *__restrict__ x, const double *__restrict__ f0, double *out,
     const double *__restrict__ ring, double bcn, double bcs, AdvCombine cb, const int *__restrict__ rlist,
-    const double *__restrict__ rdt) {
+    const double *__restrict__ rdt, int ncol) {
   const int l = threadIdx.x;
   const int ntm = m.ntm, npm = m.npm;
   const int j0 = 1 + 31 * (int)(blockIdx.x * kAdvWarps + threadIdx.y);
-  const int kc0 = 2 + (int)blockIdx.y * kAdvCols;
+  const int kc0 = 2 + (int)blockIdx.y * ncol;
   if (j0 > ntm || kc0 > npm - 1) return;  // uniform per warp
   if (rlist && rlist[blockIdx.z] < 0) return;
   const int i = (rlist ? rlist[blockIdx.z] : (int)blockIdx.z) + 1;
   if (rdt) cb.C = cb.C * rdt[i - 1];
-  const int kc1 = min(kc0 + kAdvCols - 1, npm - 1);
+  const int kc1 = min(kc0 + ncol - 1, npm - 1);
   const int r = j0 - 1 + l;
   const int hr = (l == 31) ? j0 - 2 : (l == 0) ? j0 + 31 : (l == 1) ? j0 + 32 : 0;  // halo row (0: none)
   const bool rin = r >= 1 && r <= ntm, hin = hr >= 1 && hr <= ntm;
@@ -1641,33 +1641,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t phase,
 }
 
 // ------------------------------------------- two RKG2 stages per launch
-// Temporal blocking of stages k and k+1 (src/hipft.f90:5222-5237) for a
-// constant-per-realization D.  A CTA owns a tile of TJ theta rows x TK phi
-// columns.  Phase 1 stages, with 1-D TMA copies of whole theta runs, Y_{k-1}
-// on the tile plus a halo of 2 and Y_{k-2}, u0, dty0 plus a halo of 1 in
-// shared memory (phi halos wrap periodically; theta runs are clipped at the
-// poles).  Phase 2 computes Y_k on the tile plus a halo of 1 in shared memory
-// (in place of Y_{k-2}) and writes its tile; phase 3 computes Y_{k+1} on the
-// tile from shared memory and writes it.  Per cell and stage pair the HBM
-// traffic is 4 reads + 2 writes instead of 2 x (4 reads + 1 write).
-//
-// The pole rows of Y_{k+1} need ring sums over all phi of the intermediate
-// Y_k (src/hipft.f90:7969-7979).  CTAs holding rows 1-2 / ntm-1..ntm publish
-// per-tile partials of those sums; the last of them (atomic counter, no
-// waiting) reduces the partials in tile order, computes both pole rows of
-// Y_{k+1} for every phi column, then the ring sums of Y_{k+1} for the next
-// launch.
-constexpr int kPJ = 128;          // theta rows per tile (default shape)
+// Launch arguments of the two-stage kernel k_sts_pair_ws (sts_pair_ws.cuh):
+// temporal blocking of stages k and k+1 (src/hipft.f90:5222-5237) over tiles
+// of kPJ theta rows x kPK phi columns.
+constexpr int kPJ = 128;          // theta rows per tile
 constexpr int kPK = 8;            // phi columns per tile
-constexpr int kPR = kPJ + 4;      // shared rows per column (halo 2 each side)
-constexpr int kPC = kPK + 4;      // shared columns (halo 2 each side)
-constexpr int kPThreads = 256;
-// 4 staged arrays, per-row tables (st_i, c2, c4), per-column tables (P1, P5), mbarrier
-template <int TJ, int TK>
-constexpr size_t pair_smem_bytes() {
-  return ((size_t)4 * (TK + 4) * (TJ + 4) + 3 * (TJ + 4) + 2 * (TK + 4)) * sizeof(double) + 64;
-}
-constexpr size_t kPairSmem = pair_smem_bytes<kPJ, kPK>();
 
 struct PairArgs {
   StageCoef ca, cb;     // stages k and k+1
@@ -1685,234 +1663,5 @@ struct PairArgs {
   const int *dnact = nullptr;
   int dstride = 0;
 };
-
-template <int TJ, int TK, int MINB>
-__global__ void __launch_bounds__(kPThreads, MINB) k_sts_pair(Mesh m, const double *__restrict__ dfac,
-                                                           const double *__restrict__ ykm1,
-                                                           const double *__restrict__ ykm2,
-                                                           const double *__restrict__ u0,
-                                                           const double *__restrict__ dty0, double *out_k,
-                                                           double *out_k1, const double *__restrict__ ring_in,
-                                                           double bcn, double bcs, PairArgs pa, RingOut ro) {
-  constexpr int PR = TJ + 4, PC = TK + 4;
-  extern __shared__ __align__(128) double psm[];
-  double *sX1 = psm;                   // Y_{k-1}
-  double *sYk = psm + PC * PR;       // Y_{k-2}, overwritten by Y_k
-  double *sU = psm + 2 * PC * PR;    // u0
-  double *sD = psm + 3 * PC * PR;    // dty0
-  double *tST = psm + 4 * PC * PR;   // st_i(j) per shared row
-  double *tC2 = tST + PR;             // c2(j)
-  double *tC4 = tC2 + PR;             // c4(j)
-  double *tP1 = tC4 + PR;             // (Dh*dph_i(k))*dp_i(k) per shared column
-  double *tP5 = tP1 + PC;             // (Dh*dph_i(k+1))*dp_i(k)
-  uint64_t *bar = reinterpret_cast<uint64_t *>(tP5 + PC);
-  __shared__ double red[2][kPThreads / 32];
-  __shared__ double s_ring[2];
-  __shared__ int s_last;
-
-  const int tid = threadIdx.x;
-  const int ntm = m.ntm, npm = m.npm;
-  const int64_t ld = m.ldt;
-  const int j0 = blockIdx.x * TJ + 1;
-  const int kt = blockIdx.y;
-  const int k0 = kt * TK + 2;
-  const int i = blockIdx.z + 1;
-  const int nk = min(TK, npm - 1 - k0 + 1);  // interior columns of this tile
-  const int64_t pbase = (int64_t)(i - 1) * m.plane;
-#define SIDX(c, r) ((c) * PR + (r))       // c: column k0-2+c, r: row j0-2+r
-  auto wrapc = [&](int c) {
-    if (c < 1) return c + (npm - 2);
-    if (c > npm) return c - (npm - 2);
-    return c;
-  };
-
-  // ---- phase 1: TMA loads of whole theta runs
-  const int rs = max(1, j0 - 2);
-  const int re = min((int)ld, j0 + TJ + 1);
-  const uint32_t run_bytes = (uint32_t)(re - rs + 1) * 8u;
-  const int roff = rs - (j0 - 2);
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (tid == 0) {
-    const uint32_t ncopy = (uint32_t)(nk + 4) + 3u * (uint32_t)(nk + 2);
-    mbar_expect_tx(bar, ncopy * run_bytes);
-    for (int c = 0; c < nk + 4; ++c) {
-      const int kg = wrapc(k0 - 2 + c);
-      bulk_load(&sX1[SIDX(c, roff)], ykm1 + pbase + (int64_t)(kg - 1) * ld + (rs - 1), run_bytes, bar);
-    }
-    for (int c = 1; c < nk + 3; ++c) {
-      const int kg = wrapc(k0 - 2 + c);
-      const int64_t g = pbase + (int64_t)(kg - 1) * ld + (rs - 1);
-      bulk_load(&sYk[SIDX(c, roff)], ykm2 + g, run_bytes, bar);
-      bulk_load(&sU[SIDX(c, roff)], u0 + g, run_bytes, bar);
-      bulk_load(&sD[SIDX(c, roff)], dty0 + g, run_bytes, bar);
-    }
-  }
-  const double Dr = dfac[i];
-  const double Dh = kHalf * (Dr + Dr);
-  const double ax_n = ring_in[2 * (i - 1)] * bcn;
-  const double ax_s = -ring_in[2 * (i - 1) + 1] * bcs;
-  // coefficient tables, in load_diffusion_matrix's operation order, while the copies fly
-  for (int r = tid; r < PR; r += kPThreads) {
-    const int j = j0 - 2 + r;
-    double st = 0.0, c2 = 0.0, c4 = 0.0;
-    if (j >= 2 && j <= ntm - 1) {
-      st = m.st_i[j];
-      c2 = Dh * m.dth_i[j] * m.dt_i[j] * st * m.sth[j];
-      c4 = Dh * m.dth_i[j + 1] * m.dt_i[j] * st * m.sth[j + 1];
-    }
-    tST[r] = st;
-    tC2[r] = c2;
-    tC4[r] = c4;
-  }
-  for (int c = tid; c < PC; c += kPThreads) {
-    const int kc = wrapc(k0 - 2 + c);
-    const int kw = kc == npm ? 2 : (kc == 1 ? npm - 1 : kc);  // seam columns take their twins' metrics
-    tP1[c] = Dh * m.dph_i[kw] * m.dp_i[kw];
-    tP5[c] = Dh * m.dph_i[kw + 1] * m.dp_i[kw];
-  }
-  const bool landed = mbar_wait_bounded(bar, 0, 1u << 22);
-  if (!landed) {
-    if (tid == 0) atomicExch(pa.err, 1);
-    mbar_wait_bounded(bar, 0, 1u << 22);  // let copies still in flight land before exiting
-    return;
-  }
-  __syncthreads();  // tables visible
-
-  // ---- phase 2: Y_k on rows j0-1..j0+TJ, columns k0-1..k0+nk (shared, in place of Y_{k-2})
-  const int nr2 = TJ + 2, nc2 = nk + 2;
-  const StageCoef sa = pa.ca;
-  for (int e = tid; e < nr2 * nc2; e += kPThreads) {
-    const int r = 1 + e % nr2;  // shared row
-    const int c = 1 + e / nr2;  // shared column
-    const int j = j0 - 2 + r;
-    if (j < 1 || j > ntm) continue;
-    double ax;
-    if (j == 1) {
-      ax = ax_n;
-    } else if (j == ntm) {
-      ax = ax_s;
-    } else {
-      const double sti = tST[r];
-      const double c1 = tP1[c] * sti * sti;
-      const double c2 = tC2[r];
-      const double c4 = tC4[r];
-      const double c5 = tP5[c] * sti * sti;
-      const double c3 = -(c1 + c2 + c4 + c5);
-      ax = c1 * sX1[SIDX(c - 1, r)] + c2 * sX1[SIDX(c, r - 1)] + c3 * sX1[SIDX(c, r)] +
-           c4 * sX1[SIDX(c, r + 1)] + c5 * sX1[SIDX(c + 1, r)];
-    }
-    const double y = sa.a * sX1[SIDX(c, r)] + sa.b * sYk[SIDX(c, r)] + sa.c * sU[SIDX(c, r)] + sa.d * ax +
-                     sa.e * sD[SIDX(c, r)];
-    sYk[SIDX(c, r)] = y;
-    if (r >= 2 && r < 2 + TJ && c >= 2 && c < 2 + nk) {  // tile interior goes to HBM (+ seam copies)
-      const int k = k0 - 2 + c;
-      const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
-      out_k[q] = y;
-      if (k == 2) out_k[q + (int64_t)(npm - 2) * ld] = y;
-      if (k == npm - 1) out_k[q - (int64_t)(npm - 2) * ld] = y;
-    }
-  }
-  __syncthreads();
-
-  // ---- ring partials of Y_k over this tile's columns.  The CTAs whose tile
-  // holds row 2 (north) or row ntm-1 (south) publish; they also write rows 2
-  // and ntm-1 of Y_{k+1}, which the last of them reads back below.
-  const bool has_n = (j0 == 1);
-  const bool has_s = (ntm - 1 >= j0 && ntm - 1 <= j0 + TJ - 1);
-  if (tid == 0 && (has_n || has_s)) {
-    if (has_n) {
-      double acc = 0.0;
-      for (int c = 2; c < 2 + nk; ++c)
-        acc = acc + (Dr + Dr) * (sYk[SIDX(c, 3)] - sYk[SIDX(c, 2)]) * m.dp[k0 - 2 + c];
-      ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
-    }
-    if (has_s) {
-      const int rS = ntm - (j0 - 2);
-      double acc = 0.0;
-      for (int c = 2; c < 2 + nk; ++c)
-        acc = acc + (Dr + Dr) * (sYk[SIDX(c, rS)] - sYk[SIDX(c, rS - 1)]) * m.dp[k0 - 2 + c];
-      ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + kt] = acc;
-    }
-  }
-
-  // ---- phase 3: Y_{k+1} on the tile interior (pole rows are finished below)
-  const StageCoef sb = pa.cb;
-  for (int e = tid; e < TJ * nk; e += kPThreads) {
-    const int r = 2 + e % TJ;
-    const int c = 2 + e / TJ;
-    const int j = j0 - 2 + r;
-    if (j < 2 || j > ntm - 1) continue;
-    const int k = k0 - 2 + c;
-    const double sti = tST[r];
-    const double c1 = tP1[c] * sti * sti;
-    const double c2 = tC2[r];
-    const double c4 = tC4[r];
-    const double c5 = tP5[c] * sti * sti;
-    const double c3 = -(c1 + c2 + c4 + c5);
-    const double ax = c1 * sYk[SIDX(c - 1, r)] + c2 * sYk[SIDX(c, r - 1)] + c3 * sYk[SIDX(c, r)] +
-                      c4 * sYk[SIDX(c, r + 1)] + c5 * sYk[SIDX(c + 1, r)];
-    const double y = sb.a * sYk[SIDX(c, r)] + sb.b * sX1[SIDX(c, r)] + sb.c * sU[SIDX(c, r)] + sb.d * ax +
-                     sb.e * sD[SIDX(c, r)];
-    const int64_t q = pbase + (int64_t)(k - 1) * ld + (j - 1);
-    out_k1[q] = y;
-    if (k == 2) out_k1[q + (int64_t)(npm - 2) * ld] = y;
-    if (k == npm - 1) out_k1[q - (int64_t)(npm - 2) * ld] = y;
-  }
-#undef SIDX
-
-  // ---- publish: the last pole-holding CTA of realization i finishes the poles
-  const int contrib = (has_n ? 1 : 0) + (has_s ? 1 : 0);
-  if (contrib == 0) return;
-  __threadfence();
-  __syncthreads();
-  if (tid == 0) {
-    const unsigned int old = atomicAdd(&ro.count[i - 1], (unsigned)contrib);
-    s_last = (old + (unsigned)contrib == 2u * (unsigned)ro.nkb) ? 1 : 0;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  // ring sums of Y_k in tile order (fixed tree)
-  double sn = 0.0, ss = 0.0;
-  for (int b = tid; b < ro.nkb; b += kPThreads) {
-    sn = sn + __ldcg(&ro.part[((int64_t)0 * m.nr + (i - 1)) * ro.nkb + b]);
-    ss = ss + __ldcg(&ro.part[((int64_t)1 * m.nr + (i - 1)) * ro.nkb + b]);
-  }
-  block_sum2(sn, ss, &red[0][0]);
-  if (tid == 0) {
-    s_ring[0] = sn;
-    s_ring[1] = ss;
-  }
-  __syncthreads();
-  const double axn1 = s_ring[0] * bcn, axs1 = -s_ring[1] * bcs;
-  // pole rows of Y_{k+1} for every column, then the ring sums of Y_{k+1}
-  double rn = 0.0, rsum = 0.0;
-  for (int k = 1 + tid; k <= npm; k += kPThreads) {
-    const int64_t qn = pbase + (int64_t)(k - 1) * ld;  // row 1
-    const int64_t qs = qn + (ntm - 1);                 // row ntm
-    // Y_k at the pole rows, recomputed from the inputs (stage k's pole rows
-    // use the input's ring sums), so no other CTA's stores are needed here
-    const double ykn = sa.a * ykm1[qn] + sa.b * ykm2[qn] + sa.c * u0[qn] + sa.d * ax_n + sa.e * dty0[qn];
-    const double yks = sa.a * ykm1[qs] + sa.b * ykm2[qs] + sa.c * u0[qs] + sa.d * ax_s + sa.e * dty0[qs];
-    const double yn = sb.a * ykn + sb.b * ykm1[qn] + sb.c * u0[qn] + sb.d * axn1 + sb.e * dty0[qn];
-    const double ys = sb.a * yks + sb.b * ykm1[qs] + sb.c * u0[qs] + sb.d * axs1 + sb.e * dty0[qs];
-    out_k1[qn] = yn;
-    out_k1[qs] = ys;
-    if (k >= 2 && k <= npm - 1) {
-      rn = rn + (Dr + Dr) * (__ldcg(&out_k1[qn + 1]) - yn) * m.dp[k];
-      rsum = rsum + (Dr + Dr) * (ys - __ldcg(&out_k1[qs - 1])) * m.dp[k];
-    }
-  }
-  block_sum2(rn, rsum, &red[0][0]);
-  if (tid == 0) {
-    ro.ring[2 * (i - 1)] = rn;
-    ro.ring[2 * (i - 1) + 1] = rsum;
-    ro.count[i - 1] = 0u;
-  }
-}
 
 }  // namespace hipft

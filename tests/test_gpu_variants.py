@@ -2,11 +2,12 @@
 stage per launch, against the oracle.
 
 The library fixes its RKG2 kernel from the environment when asked
-(HIPFT_STS_PAIR=1: one CTA per tile, shape HIPFT_PAIR_TILE; =4: persistent
-warp-specialised CTAs with one theta row per consumer thread; =5: two rows
-per thread; =6: the same with the outputs leaving by bulk stores; =7: four
-stages per pass on the interior theta blocks; =0: one stage per launch), so each variant runs the standalone driver in a fresh
-subprocess; final fields must match the oracle to FIELD_TOL.  The "tuned"
+(HIPFT_STS_PAIR=4: persistent warp-specialised CTAs with one theta row per
+consumer thread; =5: two rows per thread; =6: the same with the outputs
+leaving by bulk stores; =7: four stages per pass on the interior theta
+blocks; =0: one stage per launch), so each variant runs the standalone
+driver in a fresh subprocess; final fields must match the oracle to
+FIELD_TOL.  The "tuned"
 variant lets the autotuner choose."""
 import os
 import subprocess
@@ -23,9 +24,7 @@ pytestmark = pytest.mark.gpu
 
 FIELD_TOL = 1e-12
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-VARIANTS = {"pair": {"HIPFT_STS_PAIR": "1"}, "pair_64x16": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "64x16"},
-            "pair_256x4": {"HIPFT_STS_PAIR": "1", "HIPFT_PAIR_TILE": "256x4"},
-            "pair_ws": {"HIPFT_STS_PAIR": "4"}, "pair_ws_rowpairs": {"HIPFT_STS_PAIR": "5"},
+VARIANTS = {"pair_ws": {"HIPFT_STS_PAIR": "4"}, "pair_ws_rowpairs": {"HIPFT_STS_PAIR": "5"},
             "pair_ws_bulkst": {"HIPFT_STS_PAIR": "6"}, "quad_ws": {"HIPFT_STS_PAIR": "7"},
             "single_v3": {"HIPFT_STS_PAIR": "0"}, "tuned": {}}
 RUNS = ["diffuse_soccer", "rkg2_auto_ntm33", "rkg2_auto_ntm161", "rkg2_ntm129_np65", "rkg2_ntm130_np96",
@@ -54,7 +53,7 @@ def test_stage_kernel_variant_parity(variant, name, tmp_path):
     code = ("import sys, numpy as np; sys.path.insert(0, %r); import hipft_b200 as H; "
             "np.save(%r, H.run_field(%r, %r, %r))" % (ROOT, str(out), str(tmp_path / "hipft.in"), str(tmp_path),
                                                       tuple(r["f"].shape)))
-    env = {k: v for k, v in os.environ.items() if k not in ("HIPFT_STS_PAIR", "HIPFT_PAIR_TILE", "HIPFT_TUNE")}
+    env = {k: v for k, v in os.environ.items() if k not in ("HIPFT_STS_PAIR", "HIPFT_TUNE")}
     env.update(VARIANTS[variant])
     res = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
