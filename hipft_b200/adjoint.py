@@ -157,8 +157,9 @@ class MisfitAdjoint:
     assim: optional {step index s: (map3, options)}, an assimilation of the
     (3, ntm, npm1) map with HipftGPU.assimilate's keyword options right after
     step s (apply_data_assimilation, src/hipft.f90:4148-4306), differentiated
-    by hipft_adj_assimilate (blend and additive forms; not the balanced
-    increment).
+    by hipft_adj_assimilate_at (blend and additive forms, and the balanced
+    increment, for which the field before each such assimilation of the
+    segment being reversed is kept: one field per balanced assimilation).
 
     Device memory: one field per checkpoint (every `checkpoint_every` steps)
     and the tapes of one segment's steps, as many as fit while
@@ -178,6 +179,7 @@ class MisfitAdjoint:
                      for k in FLOW_KEYS}
         self.k = max(1, int(checkpoint_every))
         self.assim = dict(assim or {})
+        self._preda = {}  # step -> field before its balanced assimilation
         self.mesh = mesh_1d(gpu.t, gpu.p)
         self.w = misfit_weights(self.mesh)
         self.timing = {}
@@ -203,11 +205,18 @@ class MisfitAdjoint:
                    int(opts.get("balance_flux", False)), float(opts.get("mult_fac", 1.0)), *[_p(a) for a in v])
         return o, v
 
-    def _step(self, s: int, dt: float):
-        self.gpu.flux_transport_step(dt)
+    def _assimilate(self, s: int, keep: bool):
+        """The assimilation after step s, if any; keep: hold the field before
+        a balanced increment for the reverse pass."""
         if s in self.assim:
             m3, opts = self.assim[s]
+            if keep and opts.get("balance_flux", False) and not opts.get("add", False):
+                self._preda[s] = self._dev().clone()
             self.gpu.assimilate(m3, **opts)
+
+    def _step(self, s: int, dt: float, keep: bool = False):
+        self.gpu.flux_transport_step(dt)
+        self._assimilate(s, keep)
 
     def loss_and_cotangent(self, fN: np.ndarray, target: np.ndarray):
         """Misfit and its folded cotangent (nr, npm, ntm)."""
@@ -250,9 +259,7 @@ class MisfitAdjoint:
         _, u1 = self._recorded()
         self._est_fields = max(self._est_fields, u1 - u0)
         self._budget -= (u1 - u0) * self._fbytes
-        if s in self.assim:
-            m3, opts = self.assim[s]
-            self.gpu.assimilate(m3, **opts)
+        self._assimilate(s, True)
 
     def forward(self, f0: np.ndarray, dts: Sequence[float]) -> np.ndarray:
         """The forward run with its checkpoints, the last segment taped;
@@ -264,6 +271,7 @@ class MisfitAdjoint:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g._ck(g.L.hipft_adj_clear(g.h), "hipft_adj_clear")  # steps left by an earlier run; the tape memory stays
+        self._preda = {}
         g.set_field(f0)
         g.update_flow()
         self._fbytes = self._dev().numel() * 8
@@ -289,7 +297,7 @@ class MisfitAdjoint:
             if s >= last0:
                 taping = False
                 states[s] = self._dev().clone()
-            self._step(s, dt)
+            self._step(s, dt, keep=s >= last0)
         fN = g.get_field()
         self._fwd = dict(dts=dts, ckpt=ckpt, recorded=recorded, states=states, last0=last0)
         t1 = time.perf_counter()
@@ -338,7 +346,7 @@ class MisfitAdjoint:
                     taping = False
                     states[s] = self._dev().clone()
                     if s < s1 - 1:
-                        self._step(s, dts[s])
+                        self._step(s, dts[s], keep=True)
             torch.cuda.synchronize()
             tb = time.perf_counter()
             for s in range(s1 - 1, s0 - 1, -1):
@@ -346,8 +354,10 @@ class MisfitAdjoint:
                     m3, opts = self.assim[s]
                     o, keep = self._da_opts(opts)
                     m3 = np.ascontiguousarray(m3, dtype=np.float64)
-                    g._ck(g.L.hipft_adj_assimilate(g.h, m3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                                   ctypes.byref(o), ptr(fbar)), "hipft_adj_assimilate")
+                    fpre = self._preda.pop(s, None)
+                    g._ck(g.L.hipft_adj_assimilate_at(g.h, m3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                      ctypes.byref(o), None if fpre is None else ptr(fpre),
+                                                      ptr(fbar)), "hipft_adj_assimilate_at")
                 if s not in recorded:
                     self._set(states.pop(s))
                     g._ck(g.L.hipft_adj_record(g.h, float(dts[s])), "hipft_adj_record")

@@ -465,6 +465,54 @@ __global__ void k_adj_da(Mesh m, DAArgs a, double *fbar) {
   fbar[q] = (kOne - w) * fbar[q];
 }
 
+// Reverse of the balanced increment (balance_flux of D = w (d - f),
+// src/hipft.f90:8752-8807, applied at 4125-4141).  Forward: B(D) = D / r where
+// D > 0, D r elsewhere, r = sqrt(|F+ / F-|), F+- get_flux's area-weighted
+// sums of the positive and the other cells (columns 1..npm-1, column 1 the
+// seam copy of npm-1).  With b the folded cotangent of f after the step,
+//   Dbar = g b + S dr/dD,  g = 1/r (D > 0) or r,
+//   S = sum b D dg/dr = -SP / r^2 + SN,  SP, SN = sum of b D over D > 0, D <= 0,
+//   dr/dD = A r / (2 F+) (D > 0) or -A r / (2 F-),
+// A the cell's get_flux area (column npm-1 twice: itself and its seam copy),
+// and fbar = b - w Dbar.  k_adj_bal_partial: per-block partials of SP, SN
+// over core columns (the host sums them in block order); k_adj_da_bal: the
+// pointwise pass with coef[i] = {1/r, r, S r / (2 F+), -S r / (2 F-)}.
+__global__ void k_adj_bal_partial(Mesh m, const double *__restrict__ delta, const double *__restrict__ fbar,
+                                  int cols_per_block, double *part) {
+  __shared__ double sh[64];
+  const int i = blockIdx.y + 1;
+  const int kb = 2 + blockIdx.x * cols_per_block;
+  const int ke = min(kb + cols_per_block - 1, m.npm - 1);
+  double sp = 0.0, sn = 0.0;
+  const int ncell = (ke - kb + 1) * m.ntm;
+  for (int e = threadIdx.x; e < ncell; e += blockDim.x) {
+    const int k = kb + e / m.ntm, j = 1 + e % m.ntm;
+    const int64_t q = fidx(m, j, k, i);
+    const double d = delta[q], v = fbar[q] * d;
+    if (d > 0.0) sp = sp + v; else sn = sn + v;
+  }
+  block_sum2(sp, sn, sh);
+  if (threadIdx.x == 0) {
+    part[((int64_t)(i - 1) * gridDim.x + blockIdx.x) * 2] = sp;
+    part[((int64_t)(i - 1) * gridDim.x + blockIdx.x) * 2 + 1] = sn;
+  }
+}
+
+__global__ void k_adj_da_bal(Mesh m, DAArgs a, const double *__restrict__ delta, const double *__restrict__ da_t,
+                             const double *__restrict__ da_p, const double *__restrict__ coef, double *fbar) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int k = blockIdx.y * blockDim.y + threadIdx.y + 2;
+  const int i = blockIdx.z + 1;
+  if (j > m.ntm || k > m.npm - 1) return;
+  const double *c = coef + 4 * (i - 1);
+  const int64_t q = fidx(m, j, k, i);
+  const double d = delta[q], b = fbar[q];
+  double A = da_t[j] * da_p[k];
+  if (k == m.npm - 1) A = A + da_t[j] * da_p[1];
+  const double dbar = (d > 0.0) ? c[0] * b + c[2] * A : c[1] * b + c[3] * A;
+  fbar[q] = b - da_weight(m, a, j, k, i) * dbar;
+}
+
 // dacc[i] += scale * (sum of realization i's block partials and pole-row
 // chunk partials), fixed order.
 __global__ void k_adj_dsum(const double *__restrict__ dpart, int nblk, const double *__restrict__ dpole, int nch,

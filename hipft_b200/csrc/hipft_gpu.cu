@@ -207,6 +207,7 @@ struct hipft_gpu {
   double *h_pin = nullptr;
   // analysis
   double *d_anw = nullptr;
+  double *d_adj_delta = nullptr;  // increment of a balanced assimilation, recomputed by its reverse
   unsigned char *d_masks = nullptr;
   std::vector<double> da_t, da_p;
   int vmode = 0;
@@ -3964,6 +3965,75 @@ extern "C" int hipft_adj_assimilate(hipft_gpu *h, const double *data3_pt, const 
   TRY(da_args(h, data3_pt, o, a));
   dim3 blk(32, 8), grd((unsigned)((h->ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)h->nr);
   k_adj_da<<<grd, blk, 0, h->stream>>>(h->M, a, fbar);
+  LAUNCHED(h);
+  CK(h, cudaStreamSynchronize(h->stream));
+  return HIPFT_OK;
+}
+
+extern "C" int hipft_adj_assimilate_at(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o,
+                                       const double *f_pre, double *fbar) {
+  if (!h || !data3_pt || !o || !fbar) return HIPFT_EINVAL;
+  if (!o->balance_flux || o->add) {
+    // the plain blend, or an increment that does not depend on f
+    hipft_da_opts o2 = *o;
+    o2.balance_flux = 0;
+    return hipft_adj_assimilate(h, data3_pt, &o2, fbar);
+  }
+  if (!f_pre) return fail(h, HIPFT_EINVAL, "adj_assimilate_at: the balanced increment needs the field it was applied to");
+  if (!o->lat_limit || (o->custom_from_mu && (!o->mu_power || !o->mu_limit)))
+    return fail(h, HIPFT_EINVAL, "adj_assimilate_at: missing per-realization options");
+  CK(h, cudaSetDevice(h->dev));
+  const int ntm = h->ntm, npm1 = h->npm1, nr = h->nr;
+  DAArgs a;
+  TRY(da_args(h, data3_pt, o, a));
+  if (!h->d_adj_delta) TRY(dalloc(h, &h->d_adj_delta, h->fieldn));
+  double *delta = h->d_adj_delta;
+  dim3 blk(32, 8), grd((unsigned)((ntm + 31) / 32), (unsigned)((npm1 + 31) / 32), (unsigned)nr);
+  k_da_delta<<<grd, blk, 0, h->stream>>>(h->M, a, f_pre, delta);
+  LAUNCHED(h);
+  // F+, F- exactly as the forward's balance (same kernel, same block order),
+  // then SP, SN over the core columns
+  const int cpb = 16, nb = (h->npm - 1 + cpb - 1) / cpb, nb2 = (h->npm - 2 + cpb - 1) / cpb;
+  TRY(ensure_part(h, (size_t)nr * (nb + nb2) * 2 + 4 * (size_t)nr));
+  const double *da_t = h->d_anw, *da_p = h->d_anw + 3 * ((size_t)std::max(ntm, h->npm) + 1);
+  double *pf = h->d_part, *ps = h->d_part + (size_t)nr * nb * 2, *dcoef = ps + (size_t)nr * nb2 * 2;
+  k_flux_partial<<<dim3((unsigned)nb, (unsigned)nr), 256, 0, h->stream>>>(h->M, da_t, da_p, delta, 1, pf, cpb);
+  LAUNCHED(h);
+  k_adj_bal_partial<<<dim3((unsigned)nb2, (unsigned)nr), 256, 0, h->stream>>>(h->M, delta, fbar, cpb, ps);
+  LAUNCHED(h);
+  std::vector<double> part((size_t)nr * (nb + nb2) * 2);
+  CK(h, cudaMemcpyAsync(part.data(), h->d_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(h, cudaStreamSynchronize(h->stream));
+  std::vector<double> coef(4 * (size_t)nr);
+  for (int i = 0; i < nr; ++i) {
+    double fp = 0.0, fm = 0.0, sp = 0.0, sn = 0.0;
+    for (int q = 0; q < nb; ++q) {
+      fp = fp + part[((size_t)i * nb + q) * 2];
+      fm = fm + part[((size_t)i * nb + q) * 2 + 1];
+    }
+    const double *p2 = part.data() + (size_t)nr * nb * 2;
+    for (int q = 0; q < nb2; ++q) {
+      sp = sp + p2[((size_t)i * nb2 + q) * 2];
+      sn = sn + p2[((size_t)i * nb2 + q) * 2 + 1];
+    }
+    double *c = coef.data() + 4 * (size_t)i;
+    if (fm + fp == 0.0) {  // the forward leaves the increment as it is
+      c[0] = c[1] = 1.0;
+      c[2] = c[3] = 0.0;
+      continue;
+    }
+    if (fp == 0.0 || fm == 0.0)
+      return fail(h, HIPFT_ESTATE, "adj_assimilate_at: realization %d: one-signed balanced increment", i + 1);
+    const double r = std::sqrt(std::fabs(fp / fm));
+    const double S = -sp / (r * r) + sn;
+    c[0] = 1.0 / r;
+    c[1] = r;
+    c[2] = S * r / (2.0 * fp);
+    c[3] = -S * r / (2.0 * fm);
+  }
+  TRY(upload(h, dcoef, coef));
+  dim3 g2((unsigned)((ntm + 31) / 32), (unsigned)((h->npm - 2 + 7) / 8), (unsigned)nr);
+  k_adj_da_bal<<<g2, blk, 0, h->stream>>>(h->M, a, delta, da_t, da_p, dcoef, fbar);
   LAUNCHED(h);
   CK(h, cudaStreamSynchronize(h->stream));
   return HIPFT_OK;

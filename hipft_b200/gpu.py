@@ -145,6 +145,8 @@ SIGNATURES = [
     ("hipft_adj_set_tape_limit", ctypes.c_int, [_H, ctypes.c_int64, ctypes.c_int64]),
     ("hipft_adj_release", ctypes.c_int, [_H]),
     ("hipft_adj_assimilate", ctypes.c_int, [_H, DPTR, ctypes.POINTER(DAOpts), ctypes.c_void_p]),
+    ("hipft_adj_assimilate_at", ctypes.c_int, [_H, DPTR, ctypes.POINTER(DAOpts), ctypes.c_void_p,
+                                               ctypes.c_void_p]),
     ("hipft_gpu_describe", ctypes.c_int, [_H, ctypes.c_char_p, ctypes.c_size_t]),
     ("hipft_gpu_set_ragged", ctypes.c_int, [_H, ctypes.c_int]),
     ("hipft_gpu_set_graph", ctypes.c_int, [_H, ctypes.c_int]),

@@ -434,9 +434,21 @@ int hipft_adj_release(hipft_gpu *h);
  * src/hipft.f90:4116-4141, same map and options as the forward call):
  * fbar (device, the handle's layout, folded) becomes (1 - w) fbar on every
  * core cell for the blend f += w (d - f), and is unchanged for the additive
- * form f += w d.  The balanced increment (balance_flux, 8794-8801) is not
- * differentiated (HIPFT_ESTATE). */
+ * form f += w d.  The balanced increment (balance_flux, 8794-8801) needs
+ * the field it was applied to: hipft_adj_assimilate_at (here HIPFT_ESTATE). */
 int hipft_adj_assimilate(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o, double *fbar);
+/* Reverse of one data-assimilation step given the field it was applied to,
+ * the balanced increment included (apply_data_assimilation,
+ * src/hipft.f90:4116-4141, with balance_flux of the increment, 8752-8807):
+ * f_pre (device, the handle's layout) is the field before the assimilation.
+ * The forward scales the increment D = w (d - f) by 1/r where D > 0 and by r
+ * elsewhere, r = sqrt(|F+/F-|) of get_flux's area-weighted sums; the reverse
+ * also differentiates r through both sums (one reduction pass over D and
+ * fbar, one pointwise pass).  A one-signed increment (F+ or F- zero, F+ + F-
+ * nonzero) is not differentiated (HIPFT_ESTATE).  Without balance_flux, or
+ * for the additive form, this is hipft_adj_assimilate (f_pre may be NULL). */
+int hipft_adj_assimilate_at(hipft_gpu *h, const double *data3_pt, const hipft_da_opts *o, const double *f_pre,
+                            double *fbar);
 
 /* ---- map files ------------------------------------------------------------- */
 

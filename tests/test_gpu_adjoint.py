@@ -170,14 +170,17 @@ def _da_map(seed=3):
     return np.stack([data, np.zeros_like(mu), mu])
 
 
-def test_adjoint_through_assimilation_matches_restatement():
-    """An assimilation blend (mu^4 weights, mu > 0.1) after the first step:
-    the hand-written reverse of the blend (hipft_adj_assimilate) against
-    autograd of the restatement with the same blend."""
+@pytest.mark.parametrize("balance", [False, True])
+def test_adjoint_through_assimilation_matches_restatement(balance):
+    """An assimilation blend (mu^4 weights, mu > 0.1) after the first step,
+    with and without flux balancing of the increment (balance_flux,
+    src/hipft.f90:8752-8807): the hand-written reverse
+    (hipft_adj_assimilate_at) against autograd of the restatement with the
+    same blend."""
     f0, target, dts, D, coef = _inputs()
     t, p = C.mesh_tp()
     m3 = _da_map()
-    opts = dict(custom_from_mu=True, mu_power=4.0, mu_limit=0.1)
+    opts = dict(custom_from_mu=True, mu_power=4.0, mu_limit=0.1, balance_flux=balance)
     with _handle(D, coef) as g:
         A = MisfitAdjoint(g, D, coef, checkpoint_every=2, assim={0: (m3, opts)})
         loss, grads = A.run(f0, target, dts)
@@ -192,7 +195,18 @@ def test_adjoint_through_assimilation_matches_restatement():
     w = np.where(mu > 0.1, mu ** 4.0, 0.0)          # (ntm, npm1): map column c is field column c (0-based)
     Wc = torch.tensor(w[:, 1:].T)[None]             # core field columns 1..npm-2 (0-based)
     Dd = torch.tensor(m3[0][:, 1:].T)[None]
-    core = f[:, 1:-1] + Wc * (Dd - f[:, 1:-1])
+    delta = Wc * (Dd - f[:, 1:-1])
+    if balance:
+        # get_flux's areas over columns 1..npm-1 (column 1 the seam copy of npm-1)
+        A = torch.tensor(misfit_weights(mesh_1d(t, p)))[None]
+        full = S._seam(delta)
+        pos = full > 0
+        fp = (full * A * pos).sum(dim=(1, 2))
+        fm = (full * A * ~pos).sum(dim=(1, 2))
+        assert (fp > 0).all() and (fm < 0).all()
+        r = torch.sqrt(torch.abs(fp / fm))[:, None, None]
+        delta = torch.where(delta > 0, delta / r, delta * r)
+    core = f[:, 1:-1] + delta
     f = S._seam(core)
     f = S.run(f, dts[1:], Dv, cv, sc, S.euler_dt(D))
     L = S.misfit(f, torch.tensor(target))
