@@ -355,6 +355,14 @@ class MisfitAdjoint:
                     o, keep = self._da_opts(opts)
                     m3 = np.ascontiguousarray(m3, dtype=np.float64)
                     fpre = self._preda.pop(s, None)
+                    if (fpre is None and opts.get("balance_flux", False) and not opts.get("add", False)
+                            and s in states):
+                        # a step the recompute did not run (taping stopped before
+                        # the segment's last step): its output, once more
+                        self._set(states[s])
+                        g.flux_transport_step(dts[s])
+                        fpre = self._dev().clone()
+                        torch.cuda.synchronize()
                     g._ck(g.L.hipft_adj_assimilate_at(g.h, m3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                       ctypes.byref(o), None if fpre is None else ptr(fpre),
                                                       ptr(fbar)), "hipft_adj_assimilate_at")

@@ -216,6 +216,27 @@ def test_adjoint_through_assimilation_matches_restatement(balance):
     _check_against_reference(loss, grads, L.item(), gr)
 
 
+def test_balanced_assimilation_without_room_to_tape():
+    """A balanced assimilation after the last step of a recomputed segment,
+    with no device memory left for tapes (every step recorded one at a time
+    in the reverse pass, so the recompute never runs that step and its output
+    is computed again for the balance's reverse): the same gradient as with
+    the segment taped."""
+    f0, target, dts, D, coef = _inputs()
+    assert len(dts) >= 3
+    m3 = _da_map()
+    opts = dict(custom_from_mu=True, mu_power=4.0, mu_limit=0.1, balance_flux=True)
+    out = []
+    for reserve in (0.15, 0.9999):
+        with _handle(D, coef) as g:
+            A = MisfitAdjoint(g, D, coef, checkpoint_every=2, assim={1: (m3, opts)}, reserve_frac=reserve)
+            out.append(A.run(f0, target, dts))
+    (l0, g0), (l1, g1) = out
+    assert l0 == l1
+    for k in g0:
+        np.testing.assert_allclose(g1[k], g0[k], rtol=1e-13, atol=0.0, err_msg=k)
+
+
 def test_stage_checkpoints_do_not_change_the_gradient():
     """Stage checkpoints inside the RKG2 super-steps (the reverse recomputes
     each block of q stages from its pair) give bitwise the gradient of the
