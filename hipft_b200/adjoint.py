@@ -161,6 +161,12 @@ class MisfitAdjoint:
     increment, for which the field before each such assimilation of the
     segment being reversed is kept: one field per balanced assimilation).
 
+    Flows: analytic (gradients of f0, D and p0..p5), or a 2-D flow from
+    files with or without analytic parts (gpu.set_flow_from_files; gradients
+    of f0 and D only: the flow is a constant of the step, and the LLF alpha
+    of a 2-D flow is not chained to the coefficients).  Attenuated flows,
+    which depend on the field, are not differentiated.
+
     Device memory: one field per checkpoint (every `checkpoint_every` steps)
     and the tapes of one segment's steps, as many as fit while
     `reserve_frac` of the device memory stays free (the other steps of the
@@ -309,7 +315,8 @@ class MisfitAdjoint:
         """Reverse pass from the folded cotangent gb (nr, npm, ntm) of f_N
         (numpy or torch; seam columns ignored).  Returns grads["f0"] (nr,
         npm, ntm) (folded: seam columns zero, their share in columns npm-1
-        and 2), grads["D"] (nr,) and grads["p0".."p5"] (nr,)."""
+        and 2), grads["D"] (nr,) and, for analytic flows, grads["p0".."p5"]
+        (nr,)."""
         import torch
         if self._fwd is None:
             raise RuntimeError("backward() needs a forward() first")
@@ -380,7 +387,8 @@ class MisfitAdjoint:
         grads["f0"][:, 0] = 0.0
         grads["f0"][:, self.npm - 1] = 0.0
         grads["D"] = dacc.cpu().numpy() / self.D
-        grads.update(self._flow_grads(gflow))
+        if not getattr(g, "file_flow", False):
+            grads.update(self._flow_grads(gflow))
         self.timing["reverse_s"] = time.perf_counter() - t1
         # per segment: (first step, recompute seconds, reverse seconds)
         self.timing["segments"] = seg_times

@@ -3814,8 +3814,13 @@ static int adj_diff_rev(hipft_gpu *h, const AdjSub &S, double *&W, double *dacc)
 
 static int adj_check(hipft_gpu *h) {
   if (!h->field_set) return fail(h, HIPFT_ESTATE, "adjoint step before set_field");
-  if (h->P.advance_flow && (h->adv_time != 3 || h->adv_space != 2 || h->FL.flow2d))
-    return fail(h, HIPFT_ESTATE, "adjoint: advection must be WENO3+SSPRK(4,3) with analytic flows");
+  if (h->P.advance_flow && (h->adv_time != 3 || h->adv_space != 2))
+    return fail(h, HIPFT_ESTATE, "adjoint: advection must be WENO3+SSPRK(4,3)");
+  // flows from files (with or without analytic parts) do not depend on the
+  // field; attenuated flows do (through |Br|), and the rotated rigid rotation
+  // is NaN on most grids
+  if (h->P.advance_flow && h->have_flow && (h->fdef.flow_attenuate || h->fdef.flow_rigid_omega != 0.0))
+    return fail(h, HIPFT_ESTATE, "adjoint: attenuated or rotated flows are not differentiated");
   if (h->P.advance_diffusion && (h->P.diffusion_num_method != 3 || h->DC.grid))
     return fail(h, HIPFT_ESTATE, "adjoint: diffusion must be RKG2 with per-realization constant coefficients");
   if (h->P.advance_source) return fail(h, HIPFT_ESTATE, "adjoint: sources are not differentiated");

@@ -261,6 +261,7 @@ class HipftGPU:
                      int(advance_diffusion), int(diffusion_num_method), int(diffusion_subcycles),
                      int(diffusion_coef_grid), float(diffusion_coef_factor), _p(self._dc),
                      float(pole_flux_lat_limit), int(verbose))
+        self.file_flow = False  # a 2-D flow from files is set
         self.h = ctypes.c_void_p()
         rc = self.L.hipft_gpu_create(ctypes.byref(g), ctypes.byref(prm), ctypes.byref(self.h))
         if rc:
@@ -341,6 +342,7 @@ class HipftGPU:
         b = np.ascontiguousarray(vp, dtype=np.float64)
         assert a.shape == (self.ntm + 1, self.npm1) and b.shape == (self.ntm, self.npm1 + 1), (a.shape, b.shape)
         self._ck(self.L.hipft_gpu_set_flow_from_files(self.h, _p(a), _p(b), int(at_load)), "set_flow_from_files")
+        self.file_flow = True
 
     def update_flow(self) -> bool:
         """update_flow (src/hipft.f90:3371); True when the flow changed."""

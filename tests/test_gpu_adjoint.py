@@ -141,6 +141,53 @@ def test_adjoint_matches_finite_differences_of_library_forward():
     assert abs(float(np.sum(grads["f0"] * dirn)) - fd) <= FD_TOL * abs(fd), (np.sum(grads["f0"] * dirn), fd)
 
 
+def _file_flow(t, p):
+    """A smooth 2-D flow in m/s on the test grid: vt (nt, npm1) on theta
+    faces, vp (ntm, np) on phi faces (set_flow_from_files' shapes)."""
+    th = np.concatenate([[t[0]], 0.5 * (t[1:] + t[:-1]), [t[-1]]])   # nt faces
+    ph = np.concatenate([p, [p[-1] + (p[-1] - p[-2])]])               # np faces
+    vt = 25.0 * np.sin(th)[:, None] ** 2 * np.sin(2.0 * p + 0.3)[None, :]
+    vp = 40.0 * np.sin(t)[:, None] * np.cos(ph - 0.7)[None, :] ** 2
+    return vt, vp
+
+
+def test_adjoint_with_flows_from_files_matches_finite_differences():
+    """A 2-D flow from files added to the analytic flows (a constant of the
+    step): the gradients of f0 (a random direction) and D against central
+    differences of the library's forward with the same flows."""
+    f0, target, dts, D, coef = _inputs()
+    t, p = C.mesh_tp()
+    vt, vp = _file_flow(t, p)
+    with _handle(D, coef) as g:
+        g.set_flow_from_files(vt, vp)
+        A = MisfitAdjoint(g, D, coef, checkpoint_every=2)
+        loss, grads = A.run(f0, target, dts)
+    assert set(grads) == {"f0", "D"}
+
+    def loss_at(Dd, f0d):
+        with _handle(Dd, coef) as g:
+            g.set_flow_from_files(vt, vp)
+            g.set_field(f0d)
+            g.update_flow()
+            for dt in dts:
+                g.flux_transport_step(float(dt))
+            return A.loss_and_cotangent(g.get_field(), target)[0]
+
+    for i in range(len(D)):
+        h = 1e-6 * abs(D[i])
+        Dp, Dm = D.copy(), D.copy()
+        Dp[i] += h
+        Dm[i] -= h
+        fd = (loss_at(Dp, f0) - loss_at(Dm, f0)) / (2 * h)
+        assert abs(grads["D"][i] - fd) <= FD_TOL * abs(fd), (i, grads["D"][i], fd)
+    dirn = np.random.default_rng(11).standard_normal(f0.shape)
+    dirn[:, 0] = dirn[:, -2]
+    dirn[:, -1] = dirn[:, 1]
+    h = 1e-6 * np.max(np.abs(f0))
+    fd = (loss_at(D, f0 + h * dirn) - loss_at(D, f0 - h * dirn)) / (2 * h)
+    assert abs(float(np.sum(grads["f0"] * dirn)) - fd) <= FD_TOL * abs(fd), (np.sum(grads["f0"] * dirn), fd)
+
+
 def test_autograd_function_matches_restatement():
     """FluxTransport (torch.autograd.Function over the library's forward and
     adjoint) inside an ordinary torch loss: its gradients equal the
