@@ -33,7 +33,8 @@ At N = 1 the line also carries:
       an L2 flush before each step (its fields fit in L2);
   "adjoint": gradient / forward cost on the adjoint configuration;
   "cpu_baseline": the CPU oracle's timing build on several realizations.
-`--c5` adds the 16-realization 2048 x 4096 forward leg.
+`--c5` adds the 16-realization 2048 x 4096 forward leg, `--c5-adjoint` the
+gradient / forward cost on one of its realizations (flows from files).
 
 `--impl reference` times the CPU oracle (the restatement of the reference's
 solver in oracle/, its timing build, all host threads) on a bounded sample
@@ -466,6 +467,8 @@ def run_gpu(args, wl, name):
         out["adjoint"] = measure_adjoint(args, local, days=args.adjoint_days)
     if rank == 0 and world == 1 and args.c5:
         out["c5"] = measure_c5(args, local)
+    if rank == 0 and world == 1 and args.c5_adjoint:
+        out["c5_adjoint"] = measure_c5_adjoint(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle as O
         idx = [0, 1, 2, 3]
@@ -741,6 +744,82 @@ def measure_c5(args, local: int, steps: int = 2):
     return out
 
 
+def measure_c5_adjoint(args, local: int, steps: int = 6, checkpoint_every: int = 2, runs: int = 3):
+    """Gradient / forward cost on one realization of the 16-realization
+    2048 x 4096 configuration (its realization 0: D, differential rotation and
+    meridional flow of seed 2, the supergranular flow of day 0 from files),
+    plain schedule with PTL subcycling, `steps` steps at the CFL-limited dt,
+    a checkpoint every `checkpoint_every` steps.  The batch's gradient runs
+    realization by realization: a stage-checkpointed step tape of one
+    realization is about 2 + 2 sqrt(2 s) fields of 67 MB.  Target: the same
+    run with D x 1.2."""
+    import torch
+    import hipft_b200 as H
+    from hipft_b200 import synthetic as S
+    from hipft_b200.adjoint import MisfitAdjoint
+    ntm, npm1, seed = 2048, 4097, 2
+    t = S.refined_theta(ntm)
+    p = S.uniform_phi(npm1)
+    br = S.bipole_map(t, p, seed)
+    prm = S.batched_params(16, seed)
+    flow = {"p0": prm["dr_p0"][:1], "p2": prm["dr_p2"][:1], "p4": prm["dr_p4"][:1], "p1": prm["mf_p1"][:1],
+            "p3": prm["mf_p3"][:1], "p5": prm["mf_p5"][:1]}
+    vt, vp = S.supergranular_flow(t, p, seed, day=0, coarse=(256, 513))
+    D = prm["diffusion_coef_constants"][:1]
+
+    def handle(Dv):
+        g = H.HipftGPU(t, p, 1, device=local, advance_flow=True, flow_num_method=4, strang_splitting=True,
+                       advance_diffusion=True, diffusion_coef_constants=Dv)
+        g.set_flow_from_files(vt, vp, at_load=True)
+        g.set_flow(dr_model=1, mf_model=1, dr_p0=flow["p0"], dr_p2=flow["p2"], dr_p4=flow["p4"],
+                   mf_p1=flow["p1"], mf_p3=flow["p3"], mf_p5=flow["p5"])
+        return g
+
+    g = handle(D)
+    g.load_initial_map(br[None])
+    f0 = g.get_field()
+    g.update_flow()
+    dts = [g.flow_dtmax()] * steps
+
+    def forward(gg, f):
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        gg.set_field(f)
+        gg.update_flow()
+        for d in dts:
+            gg.flux_transport_step(d)
+        out = gg.get_field()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - w0
+
+    gt = handle(D * 1.2)
+    target, _ = forward(gt, f0)
+    gt.close()
+    forward(g, f0)
+    fwd_runs = [forward(g, f0)[1] for _ in range(runs)]
+    A = MisfitAdjoint(g, D, flow, checkpoint_every=checkpoint_every)
+    A.run(f0, target, dts)  # warm-up: tuner, tape allocation
+    grad_runs = []
+    for _ in range(runs):
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        A.run(f0, target, dts)
+        torch.cuda.synchronize()
+        grad_runs.append(time.perf_counter() - w0)
+    tape = A._tape_fields()
+    info = g.info()
+    fbytes = A._fbytes
+    A.release()
+    g.close()
+    fw, gr = statistics.median(fwd_runs), statistics.median(grad_runs)
+    return {"workload": "adjoint_c5_realization0_2048x4096", "grid": [ntm, npm1 - 1], "realizations": 1,
+            "steps": steps, "dt_hours": dts[0], "checkpoint_every": checkpoint_every,
+            "flows": "supergranular flow of day 0 from files + analytic differential rotation and meridional flow",
+            "forward_ms": fw * 1e3, "gradient_ms": gr * 1e3, "gradient_over_forward": gr / fw,
+            "runs": f"median of {runs}", "tape_fields": int(tape), "field_bytes": int(fbytes),
+            "tape_gb": tape * fbytes / 1e9, "handle_device_gb": info.device_bytes / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -752,6 +831,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain (one realization) leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the gradient / forward cost leg")
     ap.add_argument("--c5", action="store_true", help="add the 16-realization 2048 x 4096 forward leg")
+    ap.add_argument("--c5-adjoint", action="store_true",
+                    help="add the gradient / forward cost on one realization of the 2048 x 4096 configuration")
     ap.add_argument("--adjoint-days", type=float, default=27.27,
                     help="model days of the adjoint leg (27.27: the adjoint configuration)")
     ap.add_argument("--adjoint-kernels", action="store_true",
