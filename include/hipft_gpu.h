@@ -392,9 +392,11 @@ int hipft_run_shard(const char *namelist_path, const char *run_dir, int device, 
  *         (vp+ap), phi LP (vp-ap), each already multiplied by x/2.
  * The step is replayed from f_in with every stage input kept; its schedule
  * (PTL subcycle dts, RKG2 stage counts) is the forward's and is held fixed.
- * Requires WENO3+SSPRK(4,3) with analytic flows, RKG2 with per-realization
- * constant diffusion coefficients and no sources (else HIPFT_ESTATE).  The
- * current field becomes the step's output. */
+ * Requires WENO3+SSPRK(4,3) with analytic flows or flows from files (not
+ * attenuated or rotated flows, which depend on the field or are NaN; with a
+ * 2-D flow the gflow cotangents are per cell of that flow), RKG2 with
+ * per-realization constant diffusion coefficients and no sources (else
+ * HIPFT_ESTATE).  The current field becomes the step's output. */
 int hipft_adj_step(hipft_gpu *h, double dt, const double *f_in, double *fbar, double *dacc, double *gflow);
 /* hipft_adj_step in two halves, for checkpoint segments that are taped once:
  * hipft_adj_record runs one flux_transport_step of the current field (the
