@@ -199,6 +199,15 @@ class MisfitAdjoint:
     def _dev(self):
         return self.gpu.field_tensor()
 
+    def _snapshot(self):
+        """A copy of the current field, complete on return: the library's
+        stream does not wait for torch's, and its next launch may overwrite
+        the field in place."""
+        import torch
+        x = self._dev().clone()
+        torch.cuda.current_stream().synchronize()
+        return x
+
     def _set(self, x):
         self.gpu._ck(self.gpu.L.hipft_gpu_set_field_device(self.gpu.h, ctypes.c_void_p(x.data_ptr())),
                      "set_field_device")
@@ -217,7 +226,7 @@ class MisfitAdjoint:
         if s in self.assim:
             m3, opts = self.assim[s]
             if keep and opts.get("balance_flux", False) and not opts.get("add", False):
-                self._preda[s] = self._dev().clone()
+                self._preda[s] = self._snapshot()
             self.gpu.assimilate(m3, **opts)
 
     def _step(self, s: int, dt: float, keep: bool = False):
@@ -291,7 +300,7 @@ class MisfitAdjoint:
         self._budget = 0.0
         for s, dt in enumerate(dts):
             if s % self.k == 0:
-                ckpt[s] = self._dev().clone()
+                ckpt[s] = self._snapshot()
             if s == last0:
                 torch.cuda.synchronize()
                 t_last = time.perf_counter()
@@ -302,7 +311,7 @@ class MisfitAdjoint:
                 continue
             if s >= last0:
                 taping = False
-                states[s] = self._dev().clone()
+                states[s] = self._snapshot()
             self._step(s, dt, keep=s >= last0)
         fN = g.get_field()
         self._fwd = dict(dts=dts, ckpt=ckpt, recorded=recorded, states=states, last0=last0)
@@ -351,7 +360,7 @@ class MisfitAdjoint:
                         recorded.add(s)
                         continue
                     taping = False
-                    states[s] = self._dev().clone()
+                    states[s] = self._snapshot()
                     if s < s1 - 1:
                         self._step(s, dts[s], keep=True)
             torch.cuda.synchronize()
@@ -368,8 +377,7 @@ class MisfitAdjoint:
                         # the segment's last step): its output, once more
                         self._set(states[s])
                         g.flux_transport_step(dts[s])
-                        fpre = self._dev().clone()
-                        torch.cuda.synchronize()
+                        fpre = self._snapshot()
                     g._ck(g.L.hipft_adj_assimilate_at(g.h, m3.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                                       ctypes.byref(o), None if fpre is None else ptr(fpre),
                                                       ptr(fbar)), "hipft_adj_assimilate_at")
