@@ -1349,7 +1349,8 @@ extern "C" int hipft_gpu_set_flow(hipft_gpu *h, const hipft_flow_def *def) {
   h->fdef = *def;
   h->have_flow = true;
   h->flow_needs_updating = true;
-  h->flow2d = def->flow_attenuate || def->flow_rigid_omega != 0.0;
+  // a flow from files, set before or after, stays the base of vt, vp
+  h->flow2d = h->have_file_flow || def->flow_attenuate || def->flow_rigid_omega != 0.0;
   return HIPFT_OK;
 }
 

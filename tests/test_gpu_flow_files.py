@@ -79,3 +79,34 @@ def test_flow_from_files_matches_oracle(name, tmp_path):
     # the steps were cut at the flow times 1.5, 3.0 and, after the wrap, 4.5
     times = set(np.round(r["sol"][:, 0, 1], 9))
     assert {1.5, 3.0, 4.5}.issubset(times)
+
+
+def test_file_flow_survives_a_later_set_flow():
+    """The flow from files stays the base of vt, vp whichever of
+    hipft_gpu_set_flow and hipft_gpu_set_flow_from_files is called first:
+    both orders give bitwise the same step, and it differs from the step
+    without the file flow."""
+    import hipft_b200 as H
+    ntm, npm1, nr = 40, 81, 2
+    t = np.linspace(0.0, np.pi, ntm)
+    p = np.linspace(0.0, 2.0 * np.pi, npm1)
+    th = np.concatenate([[t[0]], 0.5 * (t[1:] + t[:-1]), [t[-1]]])
+    vt = 30.0 * np.sin(th)[:, None] ** 2 * np.cos(p)[None, :]
+    vp = 60.0 * np.sin(t)[:, None] * np.ones((1, npm1 + 1))
+    core = np.cos(t)[None, None, :] * (1.0 + 0.1 * np.sin(3.0 * p[:-1]))[None, :, None] * np.ones((nr, 1, 1))
+    f0 = np.concatenate([core[:, -1:], core, core[:, :1]], axis=1)  # (nr, npm, ntm), periodic seam
+    flow = dict(dr_model=1, mf_model=1, dr_p2=-300.0, mf_p1=20.0, mf_p3=-20.0)
+    out = []
+    for order in ("flow_first", "files_first", "no_files"):
+        with H.HipftGPU(t, p, nr, advance_flow=True) as g:
+            if order == "files_first":
+                g.set_flow_from_files(vt, vp)
+            g.set_flow(**flow)
+            if order == "flow_first":
+                g.set_flow_from_files(vt, vp)
+            g.set_field(f0)
+            g.update_flow()
+            g.advection_step(0.5)
+            out.append(g.get_field())
+    assert np.array_equal(out[0].view(np.uint64), out[1].view(np.uint64))
+    assert np.abs(out[0] - out[2]).max() > 1e-6
